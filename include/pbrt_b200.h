@@ -1,0 +1,202 @@
+/*
+ * pbrt_b200.h — C ABI of the B200 wavefront path tracer.
+ *
+ * This is the drop-in boundary for nmichel/pbrt's data-parallel hot path: ray/BVH
+ * traversal (Möller–Trumbore triangles, analytic spheres and cylinders) and the path
+ * integrator's bounce loop with BSDF sampling/evaluation and light sampling. The reference
+ * is a Rust crate whose seams are traits; a Rust binding would declare exactly these
+ * functions in an `extern "C"` block. Each entry point names the
+ * reference interface it replaces, as `path:line` inside nmichel/pbrt.
+ *
+ * Conventions
+ *   - Every function returns a pbrt_status; 0 is success. pbrt_last_error() gives a
+ *     human-readable message for the last failure on a context.
+ *   - A context belongs to one host thread at a time; callers serialise per context.
+ *   - Buffers passed to trace/render calls may live in host memory (pageable or pinned) or
+ *     in device memory of the context's GPU; the library detects which. Host buffers are
+ *     always complete when the call returns. Device buffers are complete when the call
+ *     returns unless a stream was set with pbrt_ctx_set_stream(), in which case the work is
+ *     ordered on that stream and pbrt_ctx_sync() reports any device-side error.
+ *   - The library copies every scene description it is given; the caller keeps ownership
+ *     of its arrays.
+ *   - Rays are eight SoA planes of n floats each, one after another:
+ *       ox[n] oy[n] oz[n] dx[n] dy[n] dz[n] tmin[n] tmax[n]
+ *     Directions are used as given: they must be normalised the way the reference's
+ *     Ray::new does it (src/geom/ray.rs:10-18: d * (1 / sqrt(dx*dx + dy*dy + dz*dz))).
+ *   - All arithmetic on the path is IEEE FP32 with no fused multiply-add, in the
+ *     reference's operation order; films are accumulated in FP64.
+ */
+#ifndef PBRT_B200_H
+#define PBRT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pbrt_status {
+  PBRT_OK = 0,
+  PBRT_ERR_INVALID_ARGUMENT = 1,
+  PBRT_ERR_OUT_OF_MEMORY = 2,
+  PBRT_ERR_CUDA = 3,
+  PBRT_ERR_DEVICE_BUDGET = 4, /* a device loop ran out of its iteration budget */
+  PBRT_ERR_CAPACITY = 5,      /* a tree too deep for the traversal stack, a queue overflow */
+  PBRT_ERR_UNSUPPORTED = 6
+} pbrt_status;
+
+typedef struct pbrt_ctx pbrt_ctx;
+typedef struct pbrt_scene pbrt_scene;
+
+/* Missing-hit marker written to prim_id / object_id. */
+#define PBRT_MISS 0xFFFFFFFFu
+
+/* ---------------------------------------------------------------------------------- */
+/* Context                                                                              */
+/* ---------------------------------------------------------------------------------- */
+
+/* Opens a context on CUDA device `device`. No reference counterpart: the reference runs on
+ * host threads (src/renderers/mt.rs:23-110). */
+int pbrt_ctx_create(int device, pbrt_ctx** out);
+void pbrt_ctx_destroy(pbrt_ctx* ctx);
+/* Message of the last failure on `ctx` (never NULL; "" when none). */
+const char* pbrt_last_error(const pbrt_ctx* ctx);
+/* Orders subsequent device-buffer calls on `stream` (a cudaStream_t) without a host
+ * synchronisation; NULL restores synchronous calls. */
+int pbrt_ctx_set_stream(pbrt_ctx* ctx, void* stream);
+/* Waits for the context's work and reports device-side errors raised since the last sync. */
+int pbrt_ctx_sync(pbrt_ctx* ctx);
+
+/* ---------------------------------------------------------------------------------- */
+/* Scene description (flat POD; replaces building Scene/Object/Shape/Material/Light     */
+/* trait objects: src/scene.rs:89-115, src/objects/*.rs, src/shapes/*.rs)              */
+/* ---------------------------------------------------------------------------------- */
+
+typedef enum pbrt_shape_kind {
+  PBRT_SHAPE_MESH = 0,     /* TriangleMesh (src/shapes/triangle_mesh/triangle_mesh.rs:11-41) */
+  PBRT_SHAPE_SPHERE = 1,   /* Sphere of `radius` at the origin (src/shapes/sphere.rs:11-23) */
+  PBRT_SHAPE_CYLINDER = 2  /* Cylinder along y, `radius`, `height` (src/shapes/cylinder.rs:7-21) */
+} pbrt_shape_kind;
+
+typedef enum pbrt_material_kind {
+  PBRT_MAT_LAMBERTIAN = 0,    /* src/materials/lambertian.rs */
+  PBRT_MAT_METAL = 1,         /* src/materials/metal.rs (fuzz) */
+  PBRT_MAT_DIELECTRIC = 2,    /* src/materials/dielectric.rs (ior, albedo) */
+  PBRT_MAT_DIFFUSE_LIGHT = 3  /* src/materials/diffuse_light.rs (emission in `color`) */
+} pbrt_material_kind;
+
+typedef enum pbrt_light_kind {
+  PBRT_LIGHT_POINT = 0,               /* src/lights/point_light.rs */
+  PBRT_LIGHT_UNIFORM_INFINITE = 1,    /* src/lights/uniform_infinite_light.rs */
+  PBRT_LIGHT_BACKGROUND_INFINITE = 2, /* src/lights/background_infinite_light.rs */
+  PBRT_LIGHT_AREA = 3                 /* the emissive surface of an object (the reference's
+                                         planned AreaLight, ideas/area_light.md) */
+} pbrt_light_kind;
+
+typedef struct pbrt_mesh_desc {
+  const float* vertices;    /* 3 * vertex_count floats, xyz */
+  uint32_t vertex_count;
+  const uint32_t* indices;  /* 3 * triangle_count vertex indices */
+  uint32_t triangle_count;
+} pbrt_mesh_desc;
+
+typedef struct pbrt_material_desc {
+  uint32_t kind;  /* pbrt_material_kind */
+  float color[3]; /* albedo (lambertian, metal, dielectric) or emitted radiance (diffuse light) */
+  float fuzz;     /* metal */
+  float ior;      /* dielectric */
+} pbrt_material_desc;
+
+typedef struct pbrt_object_desc {
+  uint32_t shape;          /* pbrt_shape_kind */
+  uint32_t mesh;           /* index into meshes, PBRT_SHAPE_MESH only */
+  float radius, height;    /* sphere, cylinder */
+  uint32_t material;       /* index into materials */
+  uint32_t transformed;    /* 0: Simple (src/objects/simple.rs); 1: Transformed(Simple)
+                              (src/objects/transformed.rs) with the two matrices below */
+  float to_world[12];      /* row-major 3x4 of Transform::mat (src/geom/transform.rs:7-10) */
+  float to_local[12];      /* row-major 3x4 of Transform::inv_mat */
+} pbrt_object_desc;
+
+typedef struct pbrt_light_desc {
+  uint32_t kind;           /* pbrt_light_kind */
+  float position[3];       /* point light, world space */
+  float radiance[3];       /* point: intensity I; uniform infinite: L */
+  float bottom[3], top[3]; /* background gradient: `f` at dir.y = -1, `t` at dir.y = +1 */
+  uint32_t object;         /* area light: the emitting object (its material is DIFFUSE_LIGHT) */
+} pbrt_light_desc;
+
+typedef struct pbrt_scene_desc {
+  const pbrt_mesh_desc* meshes;
+  uint32_t mesh_count;
+  const pbrt_material_desc* materials;
+  uint32_t material_count;
+  const pbrt_object_desc* objects;
+  uint32_t object_count;
+  const pbrt_light_desc* lights;
+  uint32_t light_count;
+  /* Mesh BVH build (src/shapes/triangle_mesh/bvh.rs:221-309): binned SAH with `bvh_bins`
+   * bins (0 = the reference's 8) that stops splitting nodes of at most `bvh_max_leaf`
+   * triangles (0 = the reference's 1, i.e. split while the SAH says so). */
+  uint32_t bvh_bins;
+  uint32_t bvh_max_leaf;
+} pbrt_scene_desc;
+
+/* Builds the acceleration structures on the host and uploads the scene. Replaces
+ * Scene::commit (src/scene.rs:101-115), BVH::new (src/bvh.rs:109-132) and
+ * TriangleMesh::new / BVHTree::build (src/shapes/triangle_mesh/triangle_mesh.rs:27-41,
+ * bvh.rs:221-230). */
+int pbrt_scene_create(pbrt_ctx* ctx, const pbrt_scene_desc* desc, pbrt_scene** out);
+void pbrt_scene_destroy(pbrt_scene* scene);
+
+/* Host-only: builds one mesh's BVH exactly as pbrt_scene_create does and copies out the
+ * flattened layout the GPU reads, without touching a GPU. `nodes` receives node_capacity
+ * 32-byte records {float bmin[3]; uint32 left_first; float bmax[3]; uint32 count} in GPU
+ * numbering (index 0 = root, index 1 = padding, sibling pairs at even indices);
+ * `tri_order` receives triangle_count original triangle indices in leaf order. Call with
+ * nodes = NULL to learn the node count through *node_count. Replaces BVHTree::new + build
+ * (src/shapes/triangle_mesh/bvh.rs:179-230) for callers that inspect the tree. */
+int pbrt_mesh_bvh_build_host(const pbrt_mesh_desc* mesh, uint32_t bvh_bins, uint32_t bvh_max_leaf, void* nodes,
+                             uint64_t node_capacity, uint32_t* tri_order, uint64_t* node_count);
+
+typedef struct pbrt_scene_info {
+  uint64_t triangle_count;
+  uint64_t mesh_node_count;  /* summed over meshes, reference numbering (no padding) */
+  uint64_t mesh_leaf_count;
+  uint32_t mesh_max_depth;   /* root = depth 1, as BuildStats::max_depth (bvh.rs:70) */
+  uint32_t mesh_max_leaf_tris;
+  uint64_t object_count;
+  uint64_t device_bytes;     /* device memory held by the scene */
+} pbrt_scene_info;
+int pbrt_scene_get_info(const pbrt_scene* scene, pbrt_scene_info* info);
+
+/* ---------------------------------------------------------------------------------- */
+/* Batched ray casting                                                                  */
+/* ---------------------------------------------------------------------------------- */
+
+/* Nearest hit per ray: replaces Scene::intersect (src/scene.rs:118-120, 186-220) and, for
+ * a scene made of one untransformed mesh, TriangleMesh::intersect / BVHTree::query
+ * (src/shapes/triangle_mesh/triangle_mesh.rs:73-132, bvh.rs:350-352, 450-526).
+ * prim_id: triangle index within its mesh (or 0 for an analytic shape), PBRT_MISS on a miss.
+ * t: hit distance, +inf on a miss. object_id may be NULL. */
+int pbrt_trace_closest(pbrt_scene* scene, const float* rays, uint64_t n, uint32_t* prim_id, float* t,
+                       uint32_t* object_id);
+
+/* pbrt_trace_closest plus the traversal's work counters summed over all rays:
+ * stats[0] nodes visited, stats[1] ray/box tests, stats[2] ray/triangle tests. Replaces
+ * TriangleMesh::intersect_instrumented (src/shapes/triangle_mesh/triangle_mesh.rs:49-53)
+ * and BVHTree::query_instrumented (bvh.rs:359-361); the counts are those of
+ * TraversalStats (bvh.rs:18-47), so they equal the reference's for the same tree. */
+int pbrt_trace_closest_instrumented(pbrt_scene* scene, const float* rays, uint64_t n, uint32_t* prim_id, float* t,
+                                    uint64_t* stats);
+
+/* Whether anything blocks each ray within [tmin, tmax]: replaces Scene::intersect_p
+ * (src/scene.rs:143-168) and BVHTree::intersect_p (src/shapes/triangle_mesh/bvh.rs:381-420). */
+int pbrt_trace_any(pbrt_scene* scene, const float* rays, uint64_t n, uint8_t* occluded);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PBRT_B200_H */

@@ -1,0 +1,195 @@
+"""CPU oracle for the pbrt_b200 hot path — TEST INFRASTRUCTURE, NOT THE PRODUCT.
+
+A C++ restatement (pbrt_oracle.hpp) of nmichel/pbrt's CPU traversal, intersection and
+path-integration code, loaded here through ctypes. It is the checker of the CUDA path:
+only tests/, __graft_entry__.smoke() and the cpu_baseline leg of bench.py may use it,
+and nothing on the product path calls into it.
+
+Parity pinning: the FP64 instantiation reproduces, to the unit, the hit counts and the
+per-ray box/triangle test counts that the reference publishes for its mesh-mode traversal
+benchmark (docs/mesures_bvh.md:706-713, produced by src/bin/bvh_stats.rs:345-401); see
+tests/test_oracle_kat.py and tests/golden/bvh_stats_published.json.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+MISS = 0xFFFFFFFF
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so from its sources with the Makefile beside it."""
+    srcs = [os.path.join(_HERE, f) for f in os.listdir(_HERE) if f.endswith((".cpp", ".hpp"))]
+    if force or not os.path.exists(_LIB_PATH) or any(
+        os.path.getmtime(s) > os.path.getmtime(_LIB_PATH) for s in srcs
+    ):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def _declare(L):
+    vp, sz, i32, u32 = C.c_void_p, C.c_size_t, C.c_int, C.c_uint32
+    L.oracle_last_error.restype = C.c_char_p
+    L.oracle_ply_read.argtypes = [C.c_char_p, i32, C.POINTER(C.POINTER(C.c_double)), C.POINTER(sz),
+                                  C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(sz)]
+    L.oracle_free.argtypes = [vp]
+    for suf in ("f64", "f32"):
+        getattr(L, f"oracle_mesh_new_{suf}").restype = vp
+        getattr(L, f"oracle_mesh_new_{suf}").argtypes = [vp, sz, vp, sz, i32, u32]
+        getattr(L, f"oracle_mesh_free_{suf}").argtypes = [vp]
+        getattr(L, f"oracle_mesh_build_stats_{suf}").argtypes = [vp, vp]
+        getattr(L, f"oracle_mesh_node_count_{suf}").restype = sz
+        getattr(L, f"oracle_mesh_node_count_{suf}").argtypes = [vp]
+        getattr(L, f"oracle_mesh_nodes_{suf}").argtypes = [vp, vp, vp, vp]
+        getattr(L, f"oracle_mesh_tri_idx_{suf}").argtypes = [vp, vp]
+        getattr(L, f"oracle_mesh_trace_{suf}").argtypes = [vp, vp, sz, vp, vp, vp, i32]
+        getattr(L, f"oracle_mesh_occluded_{suf}").argtypes = [vp, vp, sz, vp, i32]
+        getattr(L, f"oracle_mesh_brute_{suf}").argtypes = [vp, vp, sz, vp, vp, i32]
+        getattr(L, f"oracle_mesh_orbit_rays_{suf}").argtypes = [vp, vp]
+        getattr(L, f"oracle_box_hit_{suf}").argtypes = [vp, vp, C.c_double if suf == "f64" else C.c_float,
+                                                        C.c_double if suf == "f64" else C.c_float, vp]
+        getattr(L, f"oracle_make_ray_{suf}").argtypes = [vp, vp, vp]
+    L.oracle_slab_widening_f64.restype = C.c_double
+    L.oracle_slab_widening_f32.restype = C.c_float
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def read_ply(path: str, reverse: bool = False):
+    """Vertices (f64, values of the f32 text) and flat triangle indices of an ASCII PLY."""
+    L = lib()
+    vp = C.POINTER(C.c_double)()
+    ip = C.POINTER(C.c_uint32)()
+    nv, ni = C.c_size_t(), C.c_size_t()
+    if L.oracle_ply_read(path.encode(), int(reverse), C.byref(vp), C.byref(nv), C.byref(ip), C.byref(ni)) != 0:
+        raise IOError(L.oracle_last_error().decode())
+    verts = np.ctypeslib.as_array(vp, shape=(max(1, nv.value * 3),))[: nv.value * 3].copy()
+    idx = np.ctypeslib.as_array(ip, shape=(max(1, ni.value),))[: ni.value].copy()
+    L.oracle_free(C.cast(vp, C.c_void_p))
+    L.oracle_free(C.cast(ip, C.c_void_p))
+    return verts.reshape(-1, 3), idx.reshape(-1, 3)
+
+
+class MeshBVH:
+    """The reference's mesh BVH (src/shapes/triangle_mesh/bvh.rs), built and traversed on
+    the CPU in f64 (`dtype=np.float64`) or in the f32 restatement (`np.float32`).
+
+    bins=8, max_leaf=1 is the reference's own build; bins=16, max_leaf=4 is the
+    GPU configuration of the 327,680-triangle ray-cast workload."""
+
+    def __init__(self, vertices, indices, dtype=np.float64, bins: int = 8, max_leaf: int = 1):
+        self.dtype = np.dtype(dtype)
+        self.suf = "f64" if self.dtype == np.float64 else "f32"
+        self._v = np.ascontiguousarray(vertices, dtype=self.dtype).reshape(-1)
+        self._i = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1)
+        L = lib()
+        self._h = getattr(L, f"oracle_mesh_new_{self.suf}")(_ptr(self._v), self._v.size // 3, _ptr(self._i),
+                                                            self._i.size // 3, bins, max_leaf)
+        if not self._h:
+            raise ValueError(L.oracle_last_error().decode())
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            getattr(_lib, f"oracle_mesh_free_{self.suf}")(h)
+            self._h = None
+
+    def build_stats(self) -> dict:
+        out = np.zeros(5, np.uint64)
+        getattr(lib(), f"oracle_mesh_build_stats_{self.suf}")(self._h, _ptr(out))
+        keys = ("node_count", "leaf_count", "max_depth", "max_leaf_tri_count", "total_leaf_tri_count")
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def nodes(self):
+        n = getattr(lib(), f"oracle_mesh_node_count_{self.suf}")(self._h)
+        boxes = np.zeros((n, 6), self.dtype)
+        lf = np.zeros(n, np.uint64)
+        cnt = np.zeros(n, np.uint64)
+        getattr(lib(), f"oracle_mesh_nodes_{self.suf}")(self._h, _ptr(boxes), _ptr(lf), _ptr(cnt))
+        return boxes, lf, cnt
+
+    def tri_idx(self):
+        out = np.zeros(self._i.size // 3, np.uint32)
+        getattr(lib(), f"oracle_mesh_tri_idx_{self.suf}")(self._h, _ptr(out))
+        return out
+
+    def _rays(self, rays):
+        rays = np.ascontiguousarray(rays, dtype=self.dtype)
+        assert rays.ndim == 2 and rays.shape[0] == 8, "rays are 8 SoA planes: ox oy oz dx dy dz tmin tmax"
+        return rays
+
+    def trace(self, rays, threads: int = os.cpu_count() or 1):
+        """Nearest hit per ray: (prim_id uint32 with 0xFFFFFFFF for a miss, t, counters)."""
+        rays = self._rays(rays)
+        n = rays.shape[1]
+        prim = np.empty(n, np.uint32)
+        t = np.empty(n, self.dtype)
+        stats = np.zeros(3, np.uint64)
+        if getattr(lib(), f"oracle_mesh_trace_{self.suf}")(self._h, _ptr(rays), n, _ptr(prim), _ptr(t),
+                                                             _ptr(stats), threads) != 0:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return prim, t, dict(nodes_visited=int(stats[0]), box_tests=int(stats[1]), triangle_tests=int(stats[2]))
+
+    def occluded(self, rays, threads: int = os.cpu_count() or 1):
+        rays = self._rays(rays)
+        n = rays.shape[1]
+        occ = np.empty(n, np.uint8)
+        if getattr(lib(), f"oracle_mesh_occluded_{self.suf}")(self._h, _ptr(rays), n, _ptr(occ), threads) != 0:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return occ
+
+    def brute_force(self, rays, threads: int = os.cpu_count() or 1):
+        rays = self._rays(rays)
+        n = rays.shape[1]
+        prim = np.empty(n, np.uint32)
+        t = np.empty(n, self.dtype)
+        getattr(lib(), f"oracle_mesh_brute_{self.suf}")(self._h, _ptr(rays), n, _ptr(prim), _ptr(t), threads)
+        return prim, t
+
+    def orbit_rays(self):
+        """The mesh-mode ray set of src/bin/bvh_stats.rs:345-382 (240,000 rays)."""
+        out = np.zeros((8, 6 * 200 * 200), self.dtype)
+        getattr(lib(), f"oracle_mesh_orbit_rays_{self.suf}")(self._h, _ptr(out))
+        return out
+
+
+def box_hit(bmin, bmax, origin, direction, tmin, tmax, dtype=np.float64):
+    """AABoundingBox::hit (src/geom/aabound.rs:323-355): entry distance or None. The
+    direction is used as given (the reference's Ray::new normalises it; use make_ray)."""
+    dt = np.dtype(dtype)
+    suf = "f64" if dt == np.float64 else "f32"
+    box = np.array(list(bmin) + list(bmax), dt)
+    ray = np.array(list(origin) + list(direction), dt)
+    entry = np.zeros(1, dt)
+    hit = getattr(lib(), f"oracle_box_hit_{suf}")(_ptr(box), _ptr(ray), float(tmin), float(tmax), _ptr(entry))
+    return float(entry[0]) if hit else None
+
+
+def make_ray(origin, direction, dtype=np.float64):
+    """Ray::new (src/geom/ray.rs:10-18): (origin, normalised direction)."""
+    dt = np.dtype(dtype)
+    suf = "f64" if dt == np.float64 else "f32"
+    o = np.array(origin, dt)
+    d = np.array(direction, dt)
+    out = np.zeros(6, dt)
+    getattr(lib(), f"oracle_make_ray_{suf}")(_ptr(o), _ptr(d), _ptr(out))
+    return out[:3].copy(), out[3:].copy()

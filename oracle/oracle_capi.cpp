@@ -1,0 +1,285 @@
+// oracle_capi.cpp — TEST INFRASTRUCTURE, NOT THE PRODUCT.
+//
+// extern "C" surface of the CPU oracle (pbrt_oracle.hpp) for the Python tests and the
+// cpu_baseline leg of bench.py. Rays cross this boundary as eight SoA planes of n values:
+// ox, oy, oz, dx, dy, dz, tmin, tmax.
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "pbrt_oracle.hpp"
+
+
+using namespace oracle;
+
+namespace {
+
+template <class F>
+void parallel_for(size_t n, int threads, F&& f) {
+  if (threads <= 1 || n < 4096) {
+    f(size_t(0), n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  std::atomic<size_t> next{0};
+  const size_t chunk = 4096;
+  for (int t = 0; t < threads; ++t) {
+    pool.emplace_back([&]() {
+      for (;;) {
+        size_t b = next.fetch_add(chunk);
+        if (b >= n) break;
+        f(b, std::min(n, b + chunk));
+      }
+    });
+  }
+  for (auto& th : pool) th.join();
+}
+
+template <class R>
+Ray<R> load_ray(const R* rays, size_t n, size_t i, R* tmin, R* tmax) {
+  Ray<R> r;
+  r.o = {rays[i], rays[n + i], rays[2 * n + i]};
+  r.d = {rays[3 * n + i], rays[4 * n + i], rays[5 * n + i]};
+  *tmin = rays[6 * n + i];
+  *tmax = rays[7 * n + i];
+  return r;
+}
+
+template <class R>
+int trace(const MeshBVH<R>* m, const R* rays, size_t n, uint32_t* prim, R* t, uint64_t* stats, int threads) {
+  std::atomic<uint64_t> nv{0}, bt{0}, tt{0};
+  parallel_for(n, threads, [&](size_t b, size_t e) {
+    TraversalStats st;
+    for (size_t i = b; i < e; ++i) {
+      R tmin, tmax;
+      Ray<R> r = load_ray(rays, n, i, &tmin, &tmax);
+      TriHit<R> h;
+      uint32_t id;
+      if (m->traverse(r, tmin, tmax, &h, &id, &st)) {
+        prim[i] = id;
+        t[i] = h.t;
+      } else {
+        prim[i] = 0xFFFFFFFFu;
+        t[i] = std::numeric_limits<R>::infinity();
+      }
+    }
+    nv += st.nodes_visited;
+    bt += st.box_tests;
+    tt += st.triangle_tests;
+  });
+  if (stats) {
+    stats[0] = nv;
+    stats[1] = bt;
+    stats[2] = tt;
+  }
+  return 0;
+}
+
+template <class R>
+int occluded(const MeshBVH<R>* m, const R* rays, size_t n, uint8_t* occ, int threads) {
+  parallel_for(n, threads, [&](size_t b, size_t e) {
+    for (size_t i = b; i < e; ++i) {
+      R tmin, tmax;
+      Ray<R> r = load_ray(rays, n, i, &tmin, &tmax);
+      occ[i] = m->intersect_p(r, tmin, tmax) ? 1 : 0;
+    }
+  });
+  return 0;
+}
+
+template <class R>
+int brute(const MeshBVH<R>* m, const R* rays, size_t n, uint32_t* prim, R* t, int threads) {
+  parallel_for(n, threads, [&](size_t b, size_t e) {
+    for (size_t i = b; i < e; ++i) {
+      R tmin, tmax;
+      Ray<R> r = load_ray(rays, n, i, &tmin, &tmax);
+      R tt;
+      uint32_t id;
+      if (m->brute_force(r, tmin, tmax, &tt, &id)) {
+        prim[i] = id;
+        t[i] = tt;
+      } else {
+        prim[i] = 0xFFFFFFFFu;
+        t[i] = std::numeric_limits<R>::infinity();
+      }
+    }
+  });
+  return 0;
+}
+
+// Mesh-mode ray set of the traversal benchmark (bvh_stats.rs:345-382): 6 orbit cameras
+// around the vertex bounds, 200x200 pixel-centre primary rays each, near 1e-4, far 1000.
+template <class R>
+void orbit_rays(const MeshBVH<R>* m, R* out) {
+  const size_t n = 6 * 200 * 200;
+  AABB<R> b = m->vertex_bounds();
+  V3<R> c = b.centroid();
+  const R PI = R(3.141592653589793238462643383279502884L);
+  const R fov = R(40) * PI / R(180);
+  R radius = length(b.bmax - b.bmin) * R(0.5);
+  R dist = radius / std::sin(fov / R(2));
+  size_t i = 0;
+  for (int v = 0; v < 6; ++v) {
+    PinHoleCamera<R> cam = orbit_camera<R>(v, c, dist);
+    for (uint32_t py = 0; py < 200; ++py)
+      for (uint32_t px = 0; px < 200; ++px, ++i) {
+        Ray<R> r = cam.get_ray(R(px) + R(0.5), R(py) + R(0.5));
+        out[i] = r.o.x; out[n + i] = r.o.y; out[2 * n + i] = r.o.z;
+        out[3 * n + i] = r.d.x; out[4 * n + i] = r.d.y; out[5 * n + i] = r.d.z;
+        out[6 * n + i] = R(0.0001); out[7 * n + i] = R(1000);
+      }
+  }
+}
+
+thread_local std::string g_err;
+
+}  // namespace
+
+extern "C" {
+
+const char* oracle_last_error() { return g_err.c_str(); }
+void oracle_free(void* p) { std::free(p); }
+
+// ASCII PLY reader with the reference's semantics (src/loader/ply/ply_loader.rs,
+// src/loader/mesh_loader.rs:13-91): float properties parse as f32 and widen to f64,
+// vertex_indices lists are appended as they come (reversed when `reverse`).
+int oracle_ply_read(const char* path, int reverse, double** verts_out, size_t* nv_out, uint32_t** idx_out, size_t* nidx_out) {
+  std::ifstream f(path);
+  if (!f) { g_err = std::string("cannot open ") + path; return -1; }
+  std::string line;
+  struct Prop { std::string name; std::string type; bool list; std::string count_type; };
+  struct Elem { std::string name; size_t count; std::vector<Prop> props; };
+  std::vector<Elem> elems;
+  std::getline(f, line);
+  if (line.rfind("ply", 0) != 0) { g_err = "not a ply file"; return -1; }
+  while (std::getline(f, line)) {
+    std::istringstream ss(line);
+    std::string kw;
+    ss >> kw;
+    if (kw == "format") {
+      std::string fmt;
+      ss >> fmt;
+      if (fmt != "ascii") { g_err = "only ascii ply is supported"; return -1; }
+    } else if (kw == "element") {
+      Elem e;
+      ss >> e.name >> e.count;
+      elems.push_back(e);
+    } else if (kw == "property") {
+      Prop p;
+      std::string t;
+      ss >> t;
+      if (t == "list") { p.list = true; ss >> p.count_type >> p.type >> p.name; }
+      else { p.list = false; p.type = t; ss >> p.name; }
+      if (elems.empty()) { g_err = "property before element"; return -1; }
+      elems.back().props.push_back(p);
+    } else if (kw == "end_header") {
+      break;
+    }
+  }
+  std::vector<double> verts;
+  std::vector<uint32_t> idx;
+  for (const Elem& e : elems) {
+    for (size_t r = 0; r < e.count; ++r) {
+      if (!std::getline(f, line)) { g_err = "truncated ply: element " + e.name + " row " + std::to_string(r) + " of " + std::to_string(e.count); return -1; }
+      std::istringstream ss(line);
+      for (const Prop& p : e.props) {
+        if (p.list) {
+          size_t cnt;
+          ss >> cnt;
+          std::vector<long long> vals(cnt);
+          for (size_t k = 0; k < cnt; ++k) ss >> vals[k];
+          if (e.name == "face" && (p.name == "vertex_indices" || p.name == "vertex_index")) {
+            if (reverse) for (size_t k = cnt; k-- > 0;) idx.push_back(uint32_t(vals[k]));
+            else for (size_t k = 0; k < cnt; ++k) idx.push_back(uint32_t(vals[k]));
+          }
+        } else {
+          std::string tok;
+          ss >> tok;
+          if (e.name == "vertex" && (p.name == "x" || p.name == "y" || p.name == "z")) {
+            double v;
+            if (p.type == "float" || p.type == "float32") v = double(std::strtof(tok.c_str(), nullptr));
+            else v = std::strtod(tok.c_str(), nullptr);
+            verts.push_back(v);
+          }
+        }
+      }
+    }
+  }
+  *nv_out = verts.size() / 3;
+  *nidx_out = idx.size();
+  *verts_out = (double*)std::malloc(sizeof(double) * std::max<size_t>(1, verts.size()));
+  *idx_out = (uint32_t*)std::malloc(sizeof(uint32_t) * std::max<size_t>(1, idx.size()));
+  std::memcpy(*verts_out, verts.data(), sizeof(double) * verts.size());
+  std::memcpy(*idx_out, idx.data(), sizeof(uint32_t) * idx.size());
+  return 0;
+}
+
+#define ORACLE_MESH_API(SUF, R)                                                                              \
+  void* oracle_mesh_new_##SUF(const R* v, size_t nv, const uint32_t* idx, size_t nt, int bins, uint32_t max_leaf) { \
+    try {                                                                                                    \
+      return new MeshBVH<R>(v, nv, idx, nt, bins, max_leaf);                                                 \
+    } catch (const std::exception& e) {                                                                      \
+      g_err = e.what();                                                                                      \
+      return nullptr;                                                                                        \
+    }                                                                                                        \
+  }                                                                                                          \
+  void oracle_mesh_free_##SUF(void* m) { delete (MeshBVH<R>*)m; }                                            \
+  void oracle_mesh_build_stats_##SUF(void* m, uint64_t* out) {                                               \
+    BuildStats s = ((MeshBVH<R>*)m)->build_stats();                                                          \
+    out[0] = s.node_count; out[1] = s.leaf_count; out[2] = s.max_depth;                                      \
+    out[3] = s.max_leaf_tri_count; out[4] = s.total_leaf_tri_count;                                          \
+  }                                                                                                          \
+  size_t oracle_mesh_node_count_##SUF(void* m) { return ((MeshBVH<R>*)m)->nodes().size(); }                  \
+  void oracle_mesh_nodes_##SUF(void* m, R* boxes, uint64_t* left_first, uint64_t* count) {                   \
+    const auto& ns = ((MeshBVH<R>*)m)->nodes();                                                              \
+    for (size_t i = 0; i < ns.size(); ++i) {                                                                 \
+      boxes[6 * i + 0] = ns[i].box.bmin.x; boxes[6 * i + 1] = ns[i].box.bmin.y; boxes[6 * i + 2] = ns[i].box.bmin.z; \
+      boxes[6 * i + 3] = ns[i].box.bmax.x; boxes[6 * i + 4] = ns[i].box.bmax.y; boxes[6 * i + 5] = ns[i].box.bmax.z; \
+      left_first[i] = ns[i].left_first; count[i] = ns[i].count;                                              \
+    }                                                                                                        \
+  }                                                                                                          \
+  void oracle_mesh_tri_idx_##SUF(void* m, uint32_t* out) {                                                   \
+    const auto& t = ((MeshBVH<R>*)m)->tri_idx();                                                             \
+    std::memcpy(out, t.data(), t.size() * sizeof(uint32_t));                                                 \
+  }                                                                                                          \
+  int oracle_mesh_trace_##SUF(void* m, const R* rays, size_t n, uint32_t* prim, R* t, uint64_t* stats, int threads) { \
+    try {                                                                                                    \
+      return trace((MeshBVH<R>*)m, rays, n, prim, t, stats, threads);                                        \
+    } catch (const std::exception& e) {                                                                      \
+      g_err = e.what();                                                                                      \
+      return -1;                                                                                             \
+    }                                                                                                        \
+  }                                                                                                          \
+  int oracle_mesh_occluded_##SUF(void* m, const R* rays, size_t n, uint8_t* occ, int threads) {              \
+    try {                                                                                                    \
+      return occluded((MeshBVH<R>*)m, rays, n, occ, threads);                                                \
+    } catch (const std::exception& e) {                                                                      \
+      g_err = e.what();                                                                                      \
+      return -1;                                                                                             \
+    }                                                                                                        \
+  }                                                                                                          \
+  int oracle_mesh_brute_##SUF(void* m, const R* rays, size_t n, uint32_t* prim, R* t, int threads) {         \
+    return brute((MeshBVH<R>*)m, rays, n, prim, t, threads);                                                 \
+  }                                                                                                          \
+  void oracle_mesh_orbit_rays_##SUF(void* m, R* out) { orbit_rays((MeshBVH<R>*)m, out); }                    \
+  R oracle_slab_widening_##SUF() { return Limits<R>::slab_widening(); }                                      \
+  int oracle_box_hit_##SUF(const R* box, const R* ray, R tmin, R tmax, R* entry) {                           \
+    AABB<R> b{{box[0], box[1], box[2]}, {box[3], box[4], box[5]}};                                           \
+    Ray<R> r{{ray[0], ray[1], ray[2]}, {ray[3], ray[4], ray[5]}};                                            \
+    return box_hit(b, r, tmin, tmax, entry) ? 1 : 0;                                                         \
+  }                                                                                                          \
+  void oracle_make_ray_##SUF(const R* o, const R* d, R* out) {                                               \
+    Ray<R> r = make_ray(V3<R>{o[0], o[1], o[2]}, V3<R>{d[0], d[1], d[2]});                                   \
+    out[0] = r.o.x; out[1] = r.o.y; out[2] = r.o.z; out[3] = r.d.x; out[4] = r.d.y; out[5] = r.d.z;           \
+  }
+
+ORACLE_MESH_API(f64, double)
+ORACLE_MESH_API(f32, float)
+
+}  // extern "C"

@@ -1,0 +1,105 @@
+"""ctypes declarations of the C ABI in include/pbrt_b200.h.
+
+Loading fails loudly: there is no CPU fallback for anything this library computes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpbrt_b200.so")
+
+PBRT_MISS = 0xFFFFFFFF
+
+STATUS = {
+    0: "PBRT_OK",
+    1: "PBRT_ERR_INVALID_ARGUMENT",
+    2: "PBRT_ERR_OUT_OF_MEMORY",
+    3: "PBRT_ERR_CUDA",
+    4: "PBRT_ERR_DEVICE_BUDGET",
+    5: "PBRT_ERR_CAPACITY",
+    6: "PBRT_ERR_UNSUPPORTED",
+}
+
+SHAPE_MESH, SHAPE_SPHERE, SHAPE_CYLINDER = 0, 1, 2
+MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_DIFFUSE_LIGHT = 0, 1, 2, 3
+LIGHT_POINT, LIGHT_UNIFORM_INFINITE, LIGHT_BACKGROUND_INFINITE, LIGHT_AREA = 0, 1, 2, 3
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("vertex_count", C.c_uint32), ("indices", C.c_void_p),
+                ("triangle_count", C.c_uint32)]
+
+
+class MaterialDesc(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("color", C.c_float * 3), ("fuzz", C.c_float), ("ior", C.c_float)]
+
+
+class ObjectDesc(C.Structure):
+    _fields_ = [("shape", C.c_uint32), ("mesh", C.c_uint32), ("radius", C.c_float), ("height", C.c_float),
+                ("material", C.c_uint32), ("transformed", C.c_uint32), ("to_world", C.c_float * 12),
+                ("to_local", C.c_float * 12)]
+
+
+class LightDesc(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("position", C.c_float * 3), ("radiance", C.c_float * 3),
+                ("bottom", C.c_float * 3), ("top", C.c_float * 3), ("object", C.c_uint32)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("meshes", C.POINTER(MeshDesc)), ("mesh_count", C.c_uint32),
+                ("materials", C.POINTER(MaterialDesc)), ("material_count", C.c_uint32),
+                ("objects", C.POINTER(ObjectDesc)), ("object_count", C.c_uint32),
+                ("lights", C.POINTER(LightDesc)), ("light_count", C.c_uint32),
+                ("bvh_bins", C.c_uint32), ("bvh_max_leaf", C.c_uint32)]
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [("triangle_count", C.c_uint64), ("mesh_node_count", C.c_uint64), ("mesh_leaf_count", C.c_uint64),
+                ("mesh_max_depth", C.c_uint32), ("mesh_max_leaf_tris", C.c_uint32), ("object_count", C.c_uint64),
+                ("device_bytes", C.c_uint64)]
+
+
+# Every symbol the header declares, with its signature. tests/test_capi_symbols.py checks
+# the library exports each of them.
+SIGNATURES = {
+    "pbrt_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "pbrt_ctx_destroy": (None, [C.c_void_p]),
+    "pbrt_last_error": (C.c_char_p, [C.c_void_p]),
+    "pbrt_ctx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "pbrt_ctx_sync": (C.c_int, [C.c_void_p]),
+    "pbrt_scene_create": (C.c_int, [C.c_void_p, C.POINTER(SceneDesc), C.POINTER(C.c_void_p)]),
+    "pbrt_scene_destroy": (None, [C.c_void_p]),
+    "pbrt_scene_get_info": (C.c_int, [C.c_void_p, C.POINTER(SceneInfo)]),
+    "pbrt_mesh_bvh_build_host": (C.c_int, [C.POINTER(MeshDesc), C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64,
+                                           C.c_void_p, C.POINTER(C.c_uint64)]),
+    "pbrt_trace_closest": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pbrt_trace_closest_instrumented": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                                                  C.c_void_p]),
+    "pbrt_trace_any": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libpbrt_b200.so (raises if it is missing: build it with pbrt_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing; build it with `python -m pbrt_b200.build` (there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+class PbrtError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code

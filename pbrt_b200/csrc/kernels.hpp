@@ -1,0 +1,19 @@
+// kernels.hpp — host-side launchers of the device kernels (no device code here).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pbrt {
+
+struct MeshView;
+
+// Ray buffers: eight planes (ox oy oz dx dy dz tmin tmax) of `stride` floats each, of which
+// the first `n` are used.
+cudaError_t launch_mesh_closest(const MeshView& m, const float* rays, uint64_t stride, uint64_t n, uint32_t* prim,
+                                float* t, uint32_t* obj, unsigned long long* counters, uint32_t* err, int sm_count,
+                                cudaStream_t s);
+cudaError_t launch_mesh_any(const MeshView& m, const float* rays, uint64_t stride, uint64_t n, uint8_t* occ,
+                            uint32_t* err, int sm_count, cudaStream_t s);
+
+}  // namespace pbrt

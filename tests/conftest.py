@@ -1,0 +1,81 @@
+"""Shared fixtures. GPU tests are marked `gpu`; everything else runs on a CPU-only host."""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+REFERENCE_ROOT = os.environ.get("PBRT_REFERENCE_ROOT", "/root/reference")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 (sm_100) GPU and the built libpbrt_b200.so")
+
+
+@pytest.fixture(scope="session")
+def golden_meshes():
+    d = np.load(os.path.join(GOLDEN, "meshes.npz"))
+    return {k: d[k] for k in d.files}
+
+
+@pytest.fixture(scope="session")
+def published():
+    with open(os.path.join(GOLDEN, "bvh_stats_published.json")) as f:
+        return json.load(f)["meshes"]
+
+
+@pytest.fixture(scope="session")
+def reference_test_files():
+    p = os.path.join(REFERENCE_ROOT, "test_files")
+    if not os.path.isdir(p):
+        pytest.skip("the reference checkout (test_files/) is not mounted here")
+    return p
+
+
+def unbuilt_grid_mesh(side: int):
+    """side³ small slanted triangles, one per grid cell (src/shapes/triangle_mesh/bvh.rs:746-766)."""
+    verts, idx = [], []
+    for ix in range(side):
+        for iy in range(side):
+            for iz in range(side):
+                x, y, z = float(ix), float(iy), float(iz)
+                first = len(verts)
+                verts += [[x, y, z], [x + 0.4, y + 0.1, z], [x + 0.1, y + 0.4, z + 0.3]]
+                idx.append([first, first + 1, first + 2])
+    return np.array(verts, np.float64), np.array(idx, np.uint32)
+
+
+def grid_ray_set(vertices, indices, make_ray, dtype):
+    """Rays aimed at every centroid from three origins plus axis pencils
+    (src/shapes/triangle_mesh/bvh.rs:828-854), normalised with the oracle's Ray::new."""
+    origins = [(-6.0, -7.0, -8.0), (9.0, -6.0, 7.0), (-5.0, 8.0, -9.0)]
+    rays = []
+    dt = np.dtype(dtype)
+    v = vertices.astype(dt)
+    for tri in indices:
+        # tri_centroid: ((v0 + v1) + v2) * (1/3) in the working precision (bvh.rs:578-584)
+        c = ((v[tri[0]] + v[tri[1]]) + v[tri[2]]) * (dt.type(1) / dt.type(3))
+        for o in origins:
+            oo = np.array(o, dt)
+            rays.append(make_ray(oo, c - oo, dt))
+    for a in range(7):
+        for b in range(7):
+            u, w = -1.0 + a * 0.7, -1.0 + b * 0.7
+            rays.append(make_ray((-5.0, u, w), (1.0, 0.0, 0.0), dt))
+            rays.append(make_ray((u, -5.0, w), (0.0, 1.0, 0.0), dt))
+            rays.append(make_ray((u, w, -5.0), (0.0, 0.0, 1.0), dt))
+    out = np.zeros((8, len(rays)), dt)
+    for k, (o, d) in enumerate(rays):
+        out[0:3, k] = o
+        out[3:6, k] = d
+    out[6] = dt.type(0.0001)
+    out[7] = dt.type(1000.0)
+    return out

@@ -1,0 +1,130 @@
+"""GPU parity of the ray-cast path against the FP32 oracle (bit-exact ids and t).
+
+The oracle restates the reference's traversal (src/shapes/triangle_mesh/bvh.rs:381-526)
+and Möller–Trumbore (triangle_mesh.rs:183-217) in FP32 without FMA; the CUDA kernels walk
+the same tree in the same order with the same roundings, so the nearest triangle, its t,
+the occlusion answer and even the work counters must be identical.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from conftest import grid_ray_set, unbuilt_grid_mesh
+import pbrt_b200 as pb
+from pbrt_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene(v, f, bins=8, max_leaf=1):
+    s = pb.Scene()
+    s.add_object(pb.Simple(pb.TriangleMesh(v, f)))
+    return s.commit(bvh_bins=bins, bvh_max_leaf=max_leaf)
+
+
+def _assert_parity(scene, m, rays, counters=True):
+    prim, t, st = scene.intersect_instrumented(rays) if counters else (*scene.intersect(rays), None)
+    oprim, ot, ost = m.trace(rays)
+    assert np.array_equal(prim, oprim), f"{(prim != oprim).sum()} ids differ"
+    hit = oprim != oracle.MISS
+    assert np.array_equal(t[hit], ot[hit]), "t must be bit-identical on hits"
+    assert np.all(np.isinf(t[~hit]))
+    if counters:
+        assert st == ost, (st, ost)
+    occ = scene.intersect_p(rays)
+    assert np.array_equal(occ, m.occluded(rays))
+    return hit
+
+
+def test_grid_fixture_parity():
+    v, i = unbuilt_grid_mesh(3)
+    v = v.astype(np.float32)
+    rays = grid_ray_set(v, i, oracle.make_ray, np.float32)
+    s = _scene(v, i)
+    m = oracle.MeshBVH(v, i, np.float32)
+    hit = _assert_parity(s, m, rays)
+    assert hit.sum() > 20
+    # far swept across the nearest hit (bvh.rs:937-975)
+    prim, t = s.intersect(rays)
+    h = prim != pb.PBRT_MISS
+    for factor in (0.5, 0.99, 0.999999, 1.0, 1.000001):
+        r = rays[:, h].copy()
+        r[7] = (t[h] * factor).astype(np.float32)
+        _assert_parity(s, m, r)
+
+
+@pytest.mark.parametrize("bins,max_leaf", [(8, 1), (16, 4)])
+def test_reference_mesh_orbit_rays(golden_meshes, bins, max_leaf):
+    v = golden_meshes["bun_zipper_res4_vertices"].astype(np.float32)
+    i = golden_meshes["bun_zipper_res4_indices"]
+    m = oracle.MeshBVH(v, i, np.float32, bins=bins, max_leaf=max_leaf)
+    rays = m.orbit_rays()
+    hit = _assert_parity(_scene(v, i, bins, max_leaf), m, rays)
+    assert hit.sum() > 40_000
+
+
+@pytest.mark.parametrize("bins,max_leaf", [(16, 4), (8, 1)])
+def test_displaced_icosphere_incoherent(bins, max_leaf):
+    v, f = W.displaced_icosphere(6, seed=11)
+    rays = W.incoherent_rays(1 << 20, v.min(0), v.max(0), seed=12)
+    # plus rays aimed into the mesh so most of them traverse deep
+    rng = np.random.default_rng(13)
+    aim = rays[:, : 1 << 18].copy()
+    tgt = (rng.random((3, aim.shape[1])) - 0.5).astype(np.float32)
+    aim[3:6] = W.normalize_f32(tgt - aim[0:3])
+    rays = np.concatenate([rays, aim], axis=1)
+    m = oracle.MeshBVH(v, f, np.float32, bins=bins, max_leaf=max_leaf)
+    hit = _assert_parity(_scene(v, f, bins, max_leaf), m, rays)
+    assert hit.sum() > 100_000
+
+
+def test_host_and_device_buffers_agree_across_chunks():
+    v, f = W.displaced_icosphere(5, seed=21)
+    n = (1 << 21) * 2 + 12345  # three pipelined chunks, the last one partial
+    rays = W.incoherent_rays(n, v.min(0), v.max(0), seed=22)
+    s = _scene(v, f, 16, 4)
+    hp, ht = s.intersect(rays)
+    dr = torch.from_numpy(rays).cuda()
+    dp, dt = s.intersect(dr)
+    assert np.array_equal(hp, dp.cpu().numpy().view(np.uint32))
+    assert np.array_equal(ht, dt.cpu().numpy())
+    occ_h = s.intersect_p(rays)
+    occ_d = s.intersect_p(dr).cpu().numpy()
+    assert np.array_equal(occ_h, occ_d)
+    m = oracle.MeshBVH(v, f, np.float32, bins=16, max_leaf=4)
+    op, ot, _ = m.trace(rays)
+    assert np.array_equal(hp, op)
+
+
+def test_edge_cases():
+    v, f = W.displaced_icosphere(3, seed=31)
+    s = _scene(v, f)
+    m = oracle.MeshBVH(v, f, np.float32)
+    rays = []
+    # axis-aligned directions (zero components take the parallel-slab branch)
+    for d in [(1, 0, 0), (0, 1, 0), (0, 0, 1), (-1, 0, 0), (0, -1, 0), (0, 0, -1)]:
+        for o in [(-3, 0.1, 0.05), (0.1, -3, 0.05), (0.05, 0.1, -3), (3, 0.1, 0.05), (0, 0, 0), (2, 2, 2)]:
+            rays.append((o, d, 1e-4, 1e30))
+    # starting inside the mesh, empty interval, interval ending before the surface, negative far
+    rays += [((0, 0, 0), (0.3, 0.4, 0.5), 1e-4, 1e30), ((0, 0, 0), (0.3, 0.4, 0.5), 5.0, 1.0),
+             ((0, 0, 0), (0.3, 0.4, 0.5), 1e-4, 0.5), ((-3, 0, 0), (1, 0, 0), 1e-4, -1.0),
+             ((0, 0, -5), (0, 0, 1), 0.0, 1e30)]
+    arr = np.zeros((8, len(rays)), np.float32)
+    for k, (o, d, a, b) in enumerate(rays):
+        ro, rd = oracle.make_ray(o, d, np.float32)
+        arr[0:3, k], arr[3:6, k], arr[6, k], arr[7, k] = ro, rd, a, b
+    _assert_parity(s, m, arr)
+    # n = 0 is a no-op
+    p, t = s.intersect(np.zeros((8, 0), np.float32))
+    assert p.size == 0 and t.size == 0
+
+
+def test_unsupported_and_invalid_inputs_raise():
+    with pytest.raises(pb.PbrtError):
+        pb.Scene().add_object(pb.Simple(pb.TriangleMesh(np.zeros((3, 3), np.float32), np.zeros((0, 3))))).commit()
+    v, f = W.icosphere(1)
+    bad = f.copy()
+    bad[0, 0] = 9999
+    with pytest.raises(pb.PbrtError):
+        pb.Scene().add_object(pb.Simple(pb.TriangleMesh(v, bad))).commit()
