@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -23,6 +24,7 @@ namespace {
 
 constexpr uint64_t kSlotRays = uint64_t(1) << 21;  // rays per pipelined chunk (64 MiB of rays)
 constexpr int kSlots = 3;
+constexpr uint64_t kDevChunk = uint64_t(1) << 24;  // rays per launch pair on device buffers
 
 struct DeviceGuard {
   int prev = -1;
@@ -56,6 +58,8 @@ struct Slot {
   float* t = nullptr;
   uint32_t* obj = nullptr;
   uint8_t* occ = nullptr;
+  uint32_t* queue = nullptr;            // survivor queue of the two-stage nearest-hit pass
+  unsigned long long* fetch = nullptr;  // [queue length, fetch position] of that pass
 };
 
 }  // namespace
@@ -67,7 +71,9 @@ struct pbrt_ctx {
   cudaStream_t user = nullptr;    // caller's stream (asynchronous device-buffer calls)
   std::string err;
   uint32_t* d_err = nullptr;
-  unsigned long long* d_counters = nullptr;
+  unsigned long long* d_counters = nullptr;  // [0..2] traversal counters, [4..5] queue length / fetch position
+  uint32_t* queue = nullptr;                  // survivor queue for device-buffer calls (kDevChunk entries)
+  bool persistent = true;                     // persistent dynamic-fetch traversal (default)
   Slot slots[kSlots];
   bool slots_ready = false;
   std::vector<void*> allocs;
@@ -117,9 +123,16 @@ int ensure_slots(pbrt_ctx* c) {
     PBRT_TRY(c->cuda(cudaMalloc(&s.t, sizeof(float) * kSlotRays), "cudaMalloc(staging)"));
     PBRT_TRY(c->cuda(cudaMalloc(&s.obj, sizeof(uint32_t) * kSlotRays), "cudaMalloc(staging)"));
     PBRT_TRY(c->cuda(cudaMalloc(&s.occ, kSlotRays), "cudaMalloc(staging)"));
+    PBRT_TRY(c->cuda(cudaMalloc(&s.queue, sizeof(uint32_t) * kSlotRays), "cudaMalloc(staging)"));
+    PBRT_TRY(c->cuda(cudaMalloc(&s.fetch, 2 * sizeof(unsigned long long)), "cudaMalloc(staging)"));
   }
   c->slots_ready = true;
   return PBRT_OK;
+}
+
+int ensure_queue(pbrt_ctx* c) {
+  if (c->queue) return PBRT_OK;
+  return c->cuda(cudaMalloc(&c->queue, sizeof(uint32_t) * kDevChunk), "cudaMalloc(survivor queue)");
 }
 
 // Reads and clears the device error word after the work that may have raised it.
@@ -166,11 +179,13 @@ int pbrt_ctx_create(int device, pbrt_ctx** out) {
   if (c->cuda(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties") != PBRT_OK) return PBRT_ERR_CUDA;
   if (prop.major < 10) return PBRT_ERR_UNSUPPORTED;  // built for sm_100a only
   c->sm_count = prop.multiProcessorCount;
+  // PBRT_TRACE_KERNEL=simple selects the one-thread-per-ray kernel (same results) for A/B runs.
+  if (const char* k = std::getenv("PBRT_TRACE_KERNEL")) c->persistent = std::strcmp(k, "simple") != 0;
   if (c->cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate") != PBRT_OK)
     return PBRT_ERR_CUDA;
   if (c->cuda(cudaMalloc(&c->d_err, sizeof(uint32_t)), "cudaMalloc") != PBRT_OK) return PBRT_ERR_OUT_OF_MEMORY;
   if (c->cuda(cudaMemset(c->d_err, 0, sizeof(uint32_t)), "cudaMemset") != PBRT_OK) return PBRT_ERR_CUDA;
-  if (c->cuda(cudaMalloc(&c->d_counters, 4 * sizeof(unsigned long long)), "cudaMalloc") != PBRT_OK)
+  if (c->cuda(cudaMalloc(&c->d_counters, 8 * sizeof(unsigned long long)), "cudaMalloc") != PBRT_OK)
     return PBRT_ERR_OUT_OF_MEMORY;
   *out = c.release();
   return PBRT_OK;
@@ -187,10 +202,13 @@ void pbrt_ctx_destroy(pbrt_ctx* c) {
     cudaFree(s.t);
     cudaFree(s.obj);
     cudaFree(s.occ);
+    cudaFree(s.queue);
+    cudaFree(s.fetch);
     if (s.s) cudaStreamDestroy(s.s);
   }
   cudaFree(c->d_err);
   cudaFree(c->d_counters);
+  cudaFree(c->queue);
   cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -332,9 +350,22 @@ int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, flo
 
   if (kr == MemKind::Device) {
     cudaStream_t st = c->work_stream();
-    cudaError_t e = occ ? launch_mesh_any(mv, rays, n, n, occ, c->d_err, c->sm_count, st)
-                        : launch_mesh_closest(mv, rays, n, n, prim, t, obj, counters, c->d_err, c->sm_count, st);
-    PBRT_TRY(c->cuda(e, "kernel launch"));
+    if (occ) {
+      PBRT_TRY(c->cuda(launch_mesh_any(mv, rays, n, n, occ, c->d_err, c->sm_count, st), "kernel launch"));
+    } else if (c->persistent && !counters) {
+      // Chunks of at most kDevChunk rays bound the survivor queue (scratch) to 64 MiB.
+      PBRT_TRY(ensure_queue(c));
+      for (uint64_t base = 0; base < n; base += kDevChunk) {
+        const uint64_t m = std::min<uint64_t>(kDevChunk, n - base);
+        PBRT_TRY(c->cuda(launch_mesh_closest_persistent(mv, rays + base, n, m, prim + base, t + base,
+                                                        obj ? obj + base : nullptr, c->queue, c->d_counters + 4,
+                                                        c->d_err, c->sm_count, st),
+                         "kernel launch"));
+      }
+    } else {
+      PBRT_TRY(c->cuda(launch_mesh_closest(mv, rays, n, n, prim, t, obj, counters, c->d_err, c->sm_count, st),
+                       "kernel launch"));
+    }
     if (stats) {
       unsigned long long h[3];
       PBRT_TRY(c->cuda(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, st), "cudaMemcpy"));
@@ -361,9 +392,15 @@ int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, flo
       PBRT_TRY(c->cuda(cudaMemcpyAsync(sl.rays + p * kSlotRays, rays + p * n + base, m * sizeof(float),
                                        cudaMemcpyHostToDevice, sl.s),
                        "cudaMemcpyAsync(rays)"));
-    cudaError_t e = occ ? launch_mesh_any(mv, sl.rays, kSlotRays, m, sl.occ, c->d_err, c->sm_count, sl.s)
-                        : launch_mesh_closest(mv, sl.rays, kSlotRays, m, sl.prim, sl.t, obj ? sl.obj : nullptr,
-                                              counters, c->d_err, c->sm_count, sl.s);
+    cudaError_t e;
+    if (occ)
+      e = launch_mesh_any(mv, sl.rays, kSlotRays, m, sl.occ, c->d_err, c->sm_count, sl.s);
+    else if (c->persistent && !counters)
+      e = launch_mesh_closest_persistent(mv, sl.rays, kSlotRays, m, sl.prim, sl.t, obj ? sl.obj : nullptr, sl.queue,
+                                         sl.fetch, c->d_err, c->sm_count, sl.s);
+    else
+      e = launch_mesh_closest(mv, sl.rays, kSlotRays, m, sl.prim, sl.t, obj ? sl.obj : nullptr, counters, c->d_err,
+                              c->sm_count, sl.s);
     PBRT_TRY(c->cuda(e, "kernel launch"));
     if (occ) {
       PBRT_TRY(c->cuda(cudaMemcpyAsync(occ + base, sl.occ, m, cudaMemcpyDeviceToHost, sl.s), "cudaMemcpyAsync"));

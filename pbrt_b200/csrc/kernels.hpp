@@ -13,6 +13,13 @@ struct MeshView;
 cudaError_t launch_mesh_closest(const MeshView& m, const float* rays, uint64_t stride, uint64_t n, uint32_t* prim,
                                 float* t, uint32_t* obj, unsigned long long* counters, uint32_t* err, int sm_count,
                                 cudaStream_t s);
+// Two-stage nearest hit: a streaming root-box cull that answers misses and compacts the
+// survivors' indices into `queue` (scratch, capacity >= n, n < 2^32), then the persistent
+// dynamic-fetch traversal over the queue. `counters` is two 64-bit words of scratch (queue
+// length, fetch position), zeroed on `s` by the launcher.
+cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays, uint64_t stride, uint64_t n,
+                                           uint32_t* prim, float* t, uint32_t* obj, uint32_t* queue,
+                                           unsigned long long* counters, uint32_t* err, int sm_count, cudaStream_t s);
 cudaError_t launch_mesh_any(const MeshView& m, const float* rays, uint64_t stride, uint64_t n, uint8_t* occ,
                             uint32_t* err, int sm_count, cudaStream_t s);
 

@@ -1,8 +1,18 @@
 // kernels_trace.cu — batched ray-cast kernels (nearest hit / any hit) over one mesh.
 //
-// One thread per ray. Ray planes are read and results written with streaming cache
-// hints (each byte is touched once), so L1/L2 stay dedicated to the tree and triangles,
-// which every ray revisits.
+// Ray planes are read and results written with streaming cache hints (each byte is touched
+// once), so L1/L2 stay dedicated to the tree and triangles, which every ray revisits.
+//
+// The nearest-hit pass on a batch runs in two stages:
+//   1. k_cull_root streams every ray once (four rays per thread, 16-byte loads), tests the
+//      root box, writes a miss for every ray, and appends the rays that enter the root to a
+//      queue with one atomicAdd per block;
+//   2. k_mesh_closest_persistent runs persistent warps over the queue, refilling idle lanes
+//      with ballot/popc and one atomicAdd per warp, and walks interior nodes until each lane
+//      reaches a leaf before any lane tests triangles (so a leaf of one lane does not
+//      serialise the warp at every step). Each lane still visits its nodes in the
+//      reference's order, so ids and t stay bit-exact.
+// k_mesh_closest (one thread per ray) is the instrumented form that counts the work.
 #include <cfloat>
 #include <cstdint>
 
@@ -57,6 +67,247 @@ __global__ void __launch_bounds__(128) k_mesh_any(MeshView m, const float* __res
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// Stage 1: root-box cull and compaction.
+// ---------------------------------------------------------------------------------------
+constexpr int kCullThreads = 256;
+constexpr int kCullRays = 4;  // rays per thread and iteration
+
+// kVec: every plane and every output pointer is 16-byte aligned and the plane stride is a
+// multiple of 4, so a thread's four rays are one float4 per plane.
+template <bool kVec>
+__global__ void __launch_bounds__(kCullThreads) k_cull_root(MeshView m, const float* __restrict__ rays, uint64_t stride,
+                                                            uint64_t n, uint32_t* __restrict__ prim,
+                                                            float* __restrict__ tout, uint32_t* __restrict__ obj,
+                                                            uint32_t* __restrict__ queue,
+                                                            unsigned long long* __restrict__ queue_count) {
+  __shared__ uint32_t warp_off[2][kCullThreads / 32];
+  __shared__ unsigned long long blk_base[2];
+  const float4 rlo = __ldg(&m.nodes[0]);
+  const float4 rhi = __ldg(&m.nodes[1]);
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint64_t per_iter = uint64_t(gridDim.x) * kCullThreads * kCullRays;
+  const uint64_t iters = (n + per_iter - 1) / per_iter;  // uniform across the grid: __syncthreads is safe
+  for (uint64_t it = 0; it < iters; ++it) {
+    const uint64_t i0 = it * per_iter + (uint64_t(blockIdx.x) * kCullThreads + threadIdx.x) * kCullRays;
+    float v[8][kCullRays];
+    const bool full = i0 + kCullRays <= n;
+    if (kVec && full) {
+#pragma unroll
+      for (int p = 0; p < 8; ++p) {
+        const float4 q = __ldcs(reinterpret_cast<const float4*>(rays + p * stride + i0));
+        v[p][0] = q.x; v[p][1] = q.y; v[p][2] = q.z; v[p][3] = q.w;
+      }
+    } else {
+#pragma unroll
+      for (int p = 0; p < 8; ++p)
+#pragma unroll
+        for (int j = 0; j < kCullRays; ++j) v[p][j] = (i0 + j < n) ? __ldcs(rays + p * stride + i0 + j) : 0.f;
+    }
+    unsigned enter = 0;
+#pragma unroll
+    for (int j = 0; j < kCullRays; ++j) {
+      if (i0 + j < n) {
+        float entry;
+        const PRay r = prepare_ray(mk3(v[0][j], v[1][j], v[2][j]), mk3(v[3][j], v[4][j], v[5][j]));
+        // entered, and not dropped at its first pop for entry >= min_t = FLT_MAX (bvh.rs:462-472)
+        if (box_hit(r, rlo, rhi, v[6][j], v[7][j], entry) && entry < FLT_MAX) enter |= 1u << j;
+      }
+    }
+    // Every ray gets the miss answer now; stage 2 overwrites the rays it traverses.
+    if (kVec && full) {
+      __stcs(reinterpret_cast<uint4*>(prim + i0), make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu));
+      const float inf = __int_as_float(0x7f800000);
+      __stcs(reinterpret_cast<float4*>(tout + i0), make_float4(inf, inf, inf, inf));
+      if (obj)
+        __stcs(reinterpret_cast<uint4*>(obj + i0), make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu));
+    } else {
+      for (int j = 0; j < kCullRays; ++j)
+        if (i0 + j < n) {
+          __stcs(prim + i0 + j, 0xFFFFFFFFu);
+          __stcs(tout + i0 + j, __int_as_float(0x7f800000));
+          if (obj) __stcs(obj + i0 + j, 0xFFFFFFFFu);
+        }
+    }
+    // Block-wide exclusive scan of the survivor counts: one atomicAdd per block.
+    const uint32_t c = __popc(enter);
+    uint32_t incl = c;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= unsigned(off)) incl += y;
+    }
+    const int buf = int(it & 1);
+    if (lane == 31) warp_off[buf][warp] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t run = 0;
+      for (int w = 0; w < kCullThreads / 32; ++w) {
+        const uint32_t t = warp_off[buf][w];
+        warp_off[buf][w] = run;
+        run += t;
+      }
+      blk_base[buf] = run ? atomicAdd(queue_count, (unsigned long long)run) : 0ull;
+    }
+    __syncthreads();
+    uint64_t pos = blk_base[buf] + warp_off[buf][warp] + (incl - c);
+#pragma unroll
+    for (int j = 0; j < kCullRays; ++j)
+      if (enter & (1u << j)) queue[pos++] = uint32_t(i0 + j);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Stage 2: persistent traversal of the survivors.
+// ---------------------------------------------------------------------------------------
+struct TraversalStack {
+  uint32_t lf[kTraceStack];
+  uint32_t cnt[kTraceStack];
+  float e[kTraceStack];
+};
+
+// Next node to visit after a leaf or a node with no child worth visiting: pops, dropping
+// entries whose entry distance is >= min_t (bvh.rs:470-472). False when the stack is empty.
+PBRT_DEV bool pop_next(TraversalStack& s, int& sp, float min_t, uint32_t& lf, uint32_t& count) {
+  while (sp > 0) {
+    --sp;
+    if (s.e[sp] < min_t) {
+      lf = s.lf[sp];
+      count = s.cnt[sp];
+      return true;
+    }
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(128) k_mesh_closest_persistent(MeshView m, const float* __restrict__ rays,
+                                                                 uint64_t stride, const uint32_t* __restrict__ queue,
+                                                                 const unsigned long long* __restrict__ queue_count,
+                                                                 uint32_t* __restrict__ prim,
+                                                                 float* __restrict__ tout, uint32_t* __restrict__ obj,
+                                                                 unsigned long long* __restrict__ next_ray,
+                                                                 uint32_t* __restrict__ err) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const uint64_t n = *queue_count;
+  bool active = false;
+  uint32_t idx = 0;
+  PRay r;
+  float near = 0.f, far = 0.f, min_t = FLT_MAX;
+  uint32_t best = 0xFFFFFFFFu, lf = 0, count = 0, budget = 0;
+  int sp = 0;
+  TraversalStack stk;
+  const uint32_t root_lf = __float_as_uint(__ldg(&m.nodes[0]).w);
+  const uint32_t root_cnt = __float_as_uint(__ldg(&m.nodes[1]).w);
+
+  for (;;) {
+    // Refill the lanes whose ray is finished: one atomicAdd per warp.
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    bool exhausted = false;
+    if (idle) {
+      const int leader = __ffs(idle) - 1;
+      unsigned long long base = 0;
+      if (int(lane) == leader) base = atomicAdd(next_ray, (unsigned long long)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      exhausted = base + __popc(idle) >= n;
+      if (!active) {
+        const uint64_t k = base + __popc(idle & lt_mask);
+        if (k < n) {
+          idx = __ldg(queue + k);
+          const F3 o = mk3(__ldg(rays + idx), __ldg(rays + stride + idx), __ldg(rays + 2 * stride + idx));
+          const F3 d = mk3(__ldg(rays + 3 * stride + idx), __ldg(rays + 4 * stride + idx),
+                           __ldg(rays + 5 * stride + idx));
+          near = __ldg(rays + 6 * stride + idx);
+          far = __ldg(rays + 7 * stride + idx);
+          r = prepare_ray(o, d);
+          min_t = FLT_MAX;
+          best = 0xFFFFFFFFu;
+          lf = root_lf;  // the root entered the ray's interval in stage 1 (bvh.rs:458-461)
+          count = root_cnt;
+          sp = 0;
+          budget = m.node_count;
+          active = true;
+        }
+      }
+    }
+    if (__ballot_sync(0xffffffffu, active) == 0) {
+      if (exhausted) break;
+      continue;
+    }
+    if (active) {
+      bool done = false;
+      // Interior walk until this lane stands on a leaf (or its ray is finished).
+      while (count == 0) {
+        if (budget-- == 0) {
+          atomicOr(err, kErrBudget);
+          done = true;
+          break;
+        }
+        const float4 l0 = __ldg(&m.nodes[2 * lf]);
+        const float4 l1 = __ldg(&m.nodes[2 * lf + 1]);
+        const float4 r0 = __ldg(&m.nodes[2 * lf + 2]);
+        const float4 r1 = __ldg(&m.nodes[2 * lf + 3]);
+        float dl, dr;
+        const bool hl = box_hit(r, l0, l1, near, far, dl);
+        const bool hr = box_hit(r, r0, r1, near, far, dr);
+        const bool swap = hl && hr && dr < dl;  // right first only when strictly nearer
+        const bool hn = swap ? hr : hl, hf = swap ? hl : hr;
+        const float dn = swap ? dr : dl, df = swap ? dl : dr;
+        const bool take_f = hf && df < min_t;
+        const bool take_n = hn && dn < min_t;
+        if (take_n) {
+          if (take_f) {
+            if (sp >= kTraceStack) {
+              atomicOr(err, kErrStack);
+              done = true;
+              break;
+            }
+            stk.lf[sp] = __float_as_uint(swap ? l0.w : r0.w);
+            stk.cnt[sp] = __float_as_uint(swap ? l1.w : r1.w);
+            stk.e[sp] = df;
+            ++sp;
+          }
+          lf = __float_as_uint(swap ? r0.w : l0.w);
+          count = __float_as_uint(swap ? r1.w : l1.w);
+        } else if (take_f) {
+          lf = __float_as_uint(swap ? l0.w : r0.w);
+          count = __float_as_uint(swap ? l1.w : r1.w);
+        } else if (!pop_next(stk, sp, min_t, lf, count)) {
+          done = true;
+          break;
+        }
+      }
+      // Leaf: every lane that reached one tests its triangles in the same pass.
+      if (!done) {
+        if (budget-- == 0) {
+          atomicOr(err, kErrBudget);
+          done = true;
+        } else {
+          for (uint32_t k = lf; k < lf + count; ++k) {
+            const float4 A = __ldg(&m.tri_a[k]);
+            const float4 B = __ldg(&m.tri_b[k]);
+            const float2 C = __ldg(&m.tri_c[k]);
+            float t;
+            if (tri_hit(r, A, B, C.x, t) && t < min_t && t >= near && t <= far) {
+              min_t = t;
+              best = __float_as_uint(C.y);
+            }
+          }
+          if (!pop_next(stk, sp, min_t, lf, count)) done = true;
+        }
+      }
+      if (done) {
+        if (best != 0xFFFFFFFFu) {  // stage 1 already wrote the miss answer
+          __stcs(prim + idx, best);
+          __stcs(tout + idx, min_t);
+          if (obj) __stcs(obj + idx, 0u);
+        }
+        active = false;
+      }
+    }
+  }
+}
+
 static unsigned grid_for(uint64_t n, int threads, int sm_count) {
   const uint64_t want = (n + threads - 1) / threads;
   const uint64_t cap = uint64_t(sm_count) * 64;  // grid-stride beyond this
@@ -72,6 +323,36 @@ cudaError_t launch_mesh_closest(const MeshView& m, const float* rays, uint64_t s
     k_mesh_closest<true><<<g, 128, 0, s>>>(m, rays, stride, n, prim, t, obj, counters, err);
   else
     k_mesh_closest<false><<<g, 128, 0, s>>>(m, rays, stride, n, prim, t, obj, nullptr, err);
+  return cudaGetLastError();
+}
+
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays, uint64_t stride, uint64_t n,
+                                           uint32_t* prim, float* t, uint32_t* obj, uint32_t* queue,
+                                           unsigned long long* counters, uint32_t* err, int sm_count, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  static int blocks_per_sm = 0;
+  if (blocks_per_sm == 0) {
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_mesh_closest_persistent, 128, 0);
+    if (e != cudaSuccess || blocks_per_sm <= 0) blocks_per_sm = 8;
+  }
+  cudaError_t e = cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  const bool vec = stride % 4 == 0 && aligned16(rays) && aligned16(prim) && aligned16(t) && (!obj || aligned16(obj));
+  const uint64_t per_block = uint64_t(kCullThreads) * kCullRays;
+  const uint64_t cull_need = (n + per_block - 1) / per_block, cull_cap = uint64_t(sm_count) * 8;
+  const unsigned cg = unsigned(cull_need < cull_cap ? cull_need : cull_cap);
+  if (vec)
+    k_cull_root<true><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters);
+  else
+    k_cull_root<false><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const uint64_t full = uint64_t(sm_count) * blocks_per_sm;
+  const uint64_t need = (n + 127) / 128;
+  const unsigned g = unsigned(need < full ? need : full);
+  k_mesh_closest_persistent<<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj, counters + 1, err);
   return cudaGetLastError();
 }
 

@@ -75,7 +75,26 @@ PBRT_DEV void slab_axis(float o, float inv, bool neg, bool zero, float lo, float
   tmax = fminf(t1, tmax);
 }
 
+// One slab with no parallel axis: the branch-free form used whenever no direction
+// component is zero (every incoherent ray in practice).
+PBRT_DEV void slab_axis_fast(float o, float inv, bool neg, float lo, float hi, float& tmin, float& tmax) {
+  const float W = PBRT_SLAB_WIDENING_F32;
+  float t0 = fm(fs(neg ? hi : lo, o), inv);
+  float t1 = fm(fs(neg ? lo : hi, o), inv);
+  t0 = fs(t0, fm(fabsf(t0), W));
+  t1 = fa(t1, fm(fabsf(t1), W));
+  tmin = fmaxf(t0, tmin);
+  tmax = fminf(t1, tmax);
+}
+
 PBRT_DEV bool box_hit(const PRay& r, const float4& lo, const float4& hi, float tmin, float tmax, float& entry) {
+  if (r.zero == 0u) {
+    slab_axis_fast(r.o.x, r.inv.x, r.neg & 1u, lo.x, hi.x, tmin, tmax);
+    slab_axis_fast(r.o.y, r.inv.y, r.neg & 2u, lo.y, hi.y, tmin, tmax);
+    slab_axis_fast(r.o.z, r.inv.z, r.neg & 4u, lo.z, hi.z, tmin, tmax);
+    entry = tmin;
+    return !(tmax < tmin);
+  }
   bool miss = false;
   slab_axis(r.o.x, r.inv.x, r.neg & 1u, r.zero & 1u, lo.x, hi.x, tmin, tmax, miss);
   slab_axis(r.o.y, r.inv.y, r.neg & 2u, r.zero & 2u, lo.y, hi.y, tmin, tmax, miss);
@@ -118,7 +137,8 @@ PBRT_DEV uint32_t mesh_closest(const MeshView& m, const PRay& r, float near, flo
   const float4 rhi = __ldg(&m.nodes[1]);
   float entry;
   if (kCount) cnt->box_tests++;
-  if (box_hit(r, rlo, rhi, near, far, entry)) {
+  // The root is pushed, then dropped at pop if its entry is >= min_t = FLT_MAX (bvh.rs:462-472).
+  if (box_hit(r, rlo, rhi, near, far, entry) && entry < FLT_MAX) {
     uint32_t lf = __float_as_uint(rlo.w), count = __float_as_uint(rhi.w);
     uint32_t stk_lf[kTraceStack], stk_cnt[kTraceStack];
     float stk_e[kTraceStack];
