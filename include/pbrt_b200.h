@@ -191,6 +191,25 @@ int pbrt_trace_closest(pbrt_scene* scene, const float* rays, uint64_t n, uint32_
 int pbrt_trace_closest_instrumented(pbrt_scene* scene, const float* rays, uint64_t n, uint32_t* prim_id, float* t,
                                     uint64_t* stats);
 
+/* pbrt_trace_closest for callers that cannot call cudaMalloc — a host application that
+ * owns every device allocation through its own pool and budget (a renderer embedding this
+ * tracer as a plugin), or code on a latency-critical path where cudaMalloc's implicit
+ * synchronisation and unpredictable cost are not acceptable. No counterpart in the
+ * reference. It allocates nothing: its scratch (survivor queue, counters, error word) is a
+ * fixed static device array of PBRT_NOALLOC_MAX_RAYS queue entries (4 MiB + 256 B) that
+ * every GPU which loads the library holds until the process exits.
+ *   - rays, prim_id and t must be device memory of the context's GPU; n must not exceed
+ *     PBRT_NOALLOC_MAX_RAYS (PBRT_ERR_CAPACITY otherwise; split larger batches).
+ *   - The first call on a device looks the array's address up there; make that first call
+ *     before any stream capture.
+ *   - Every call shares the one array: calls that overlap on the GPU (other streams, other
+ *     threads, other contexts on the same device) race and corrupt each other's results.
+ *   - It runs on the context's stream (pbrt_ctx_set_stream) and returns when its results
+ *     are complete, with device-side errors reported in its status.
+ * Results are identical to pbrt_trace_closest's. */
+#define PBRT_NOALLOC_MAX_RAYS 1048576u
+int pbrt_trace_closest_noalloc(pbrt_scene* scene, const float* rays, uint64_t n, uint32_t* prim_id, float* t);
+
 /* Whether anything blocks each ray within [tmin, tmax]: replaces Scene::intersect_p
  * (src/scene.rs:143-168) and BVHTree::intersect_p (src/shapes/triangle_mesh/bvh.rs:381-420). */
 int pbrt_trace_any(pbrt_scene* scene, const float* rays, uint64_t n, uint8_t* occluded);

@@ -78,6 +78,7 @@ SIGNATURES = {
     "pbrt_trace_closest_instrumented": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
                                                   C.c_void_p]),
     "pbrt_trace_any": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
+    "pbrt_trace_closest_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

@@ -439,6 +439,38 @@ int pbrt_trace_closest_instrumented(pbrt_scene* s, const float* rays, uint64_t n
   return trace_impl(s, rays, n, prim_id, t, nullptr, nullptr, stats);
 }
 
+static_assert(kNoAllocMaxRays == PBRT_NOALLOC_MAX_RAYS, "header and kernels disagree on the no-alloc capacity");
+
+// For callers that cannot call cudaMalloc (see the header): the same two kernels as the
+// device-buffer path of pbrt_trace_closest, with their scratch in a static __device__ array.
+int pbrt_trace_closest_noalloc(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim_id, float* t) {
+  if (!s) return PBRT_ERR_INVALID_ARGUMENT;
+  pbrt_ctx* c = s->ctx;
+  DeviceGuard g(c->device);
+  if (n > kNoAllocMaxRays)
+    return c->fail(PBRT_ERR_CAPACITY, "pbrt_trace_closest_noalloc: n = " + std::to_string(n) +
+                                          " exceeds its fixed scratch capacity of " + std::to_string(kNoAllocMaxRays) +
+                                          " rays; split the batch or use pbrt_trace_closest");
+  if (n > 0) {
+    if (!rays || !prim_id || !t) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "ray or result buffer is NULL");
+    if (mem_kind(rays) != MemKind::Device || mem_kind(prim_id) != MemKind::Device || mem_kind(t) != MemKind::Device)
+      return c->fail(PBRT_ERR_INVALID_ARGUMENT,
+                     "pbrt_trace_closest_noalloc takes device buffers only (host buffers need staging memory)");
+  }
+  const MeshView& mv = s->meshes[s->single_mesh].view;
+  cudaStream_t st = c->work_stream();
+  uint32_t* scratch = nullptr;
+  PBRT_TRY(c->cuda(launch_mesh_closest_noalloc(mv, rays, n, prim_id, t, c->device, c->sm_count, st, &scratch),
+                   "pbrt_trace_closest_noalloc"));
+  if (n == 0) return PBRT_OK;
+  PBRT_TRY(c->cuda(cudaStreamSynchronize(st), "kernel execution"));
+  uint32_t h = 0;
+  PBRT_TRY(c->cuda(cudaMemcpy(&h, scratch + 4, sizeof(h), cudaMemcpyDeviceToHost), "cudaMemcpy(error word)"));
+  if (h & kErrStack) return c->fail(PBRT_ERR_CAPACITY, "traversal stack capacity exceeded");
+  if (h) return c->fail(PBRT_ERR_DEVICE_BUDGET, "a traversal exceeded its iteration budget (malformed tree)");
+  return PBRT_OK;
+}
+
 int pbrt_trace_any(pbrt_scene* s, const float* rays, uint64_t n, uint8_t* occluded) {
   if (!occluded) return s ? s->ctx->fail(PBRT_ERR_INVALID_ARGUMENT, "occluded is NULL") : PBRT_ERR_INVALID_ARGUMENT;
   return trace_impl(s, rays, n, nullptr, nullptr, nullptr, occluded, nullptr);

@@ -15,6 +15,7 @@
 // k_mesh_closest (one thread per ray) is the instrumented form that counts the work.
 #include <cfloat>
 #include <cstdint>
+#include <mutex>
 
 #include "kernels.hpp"
 #include "trace_mesh.cuh"
@@ -353,6 +354,75 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
   const uint64_t need = (n + 127) / 128;
   const unsigned g = unsigned(need < full ? need : full);
   k_mesh_closest_persistent<<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj, counters + 1, err);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free variant of the two-stage nearest-hit pass.
+//
+// Its scratch (the two 64-bit counters, the device error word and the survivor queue) is
+// this file-scope array instead of memory the context allocates: 256 header bytes plus
+// kNoAllocMaxRays queue entries, i.e. 4 MiB + 256 B that every GPU which loads the library
+// holds until the process exits. Header layout in 32-bit words: [0..1] queue length,
+// [2..3] fetch position, [4] error word; the queue starts at word 64.
+// ---------------------------------------------------------------------------------------
+static __device__ __align__(256) uint32_t g_noalloc_scratch[64 + kNoAllocMaxRays];
+
+// Device address of g_noalloc_scratch on `device`, looked up once per device with that
+// device current (host code cannot use the symbol itself as a device address).
+static cudaError_t noalloc_scratch_address(int device, uint32_t** out) {
+  static std::mutex mu;
+  static uint32_t* addr[kMaxDevices] = {};
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[device]) {
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) return e;
+    if (cur != device) return cudaErrorInvalidDevice;  // the caller makes `device` current
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    addr[device] = static_cast<uint32_t*>(p);
+  }
+  *out = addr[device];
+  return cudaSuccess;
+}
+
+cudaError_t launch_mesh_closest_noalloc(const MeshView& m, const float* rays, uint64_t n, uint32_t* prim, float* t,
+                                        int device, int sm_count, cudaStream_t s, uint32_t** scratch_out) {
+  uint32_t* scratch = nullptr;
+  cudaError_t e = noalloc_scratch_address(device, &scratch);
+  if (e != cudaSuccess) return e;
+  *scratch_out = scratch;
+  if (n == 0) return cudaSuccess;
+  if (n > kNoAllocMaxRays) return cudaErrorInvalidValue;
+  // The array keeps the previous call's contents: the counters and the error word must
+  // start at zero; the queue is written before it is read.
+  e = cudaMemsetAsync(scratch, 0, 64 * sizeof(uint32_t), s);
+  if (e != cudaSuccess) return e;
+  unsigned long long* counters = reinterpret_cast<unsigned long long*>(scratch);
+  uint32_t* err = scratch + 4;
+  uint32_t* queue = scratch + 64;
+  static int blocks_per_sm = 0;
+  if (blocks_per_sm == 0) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_mesh_closest_persistent, 128, 0);
+    if (e != cudaSuccess || blocks_per_sm <= 0) blocks_per_sm = 8;
+  }
+  const bool vec = n % 4 == 0 && aligned16(rays) && aligned16(prim) && aligned16(t);
+  const uint64_t per_block = uint64_t(kCullThreads) * kCullRays;
+  const uint64_t cull_need = (n + per_block - 1) / per_block, cull_cap = uint64_t(sm_count) * 8;
+  const unsigned cg = unsigned(cull_need < cull_cap ? cull_need : cull_cap);
+  if (vec)
+    k_cull_root<true><<<cg, kCullThreads, 0, s>>>(m, rays, n, n, prim, t, nullptr, queue, counters);
+  else
+    k_cull_root<false><<<cg, kCullThreads, 0, s>>>(m, rays, n, n, prim, t, nullptr, queue, counters);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const uint64_t full = uint64_t(sm_count) * blocks_per_sm;
+  const uint64_t need = (n + 127) / 128;
+  const unsigned g = unsigned(need < full ? need : full);
+  k_mesh_closest_persistent<<<g, 128, 0, s>>>(m, rays, n, queue, counters, prim, t, nullptr, counters + 1, err);
   return cudaGetLastError();
 }
 
