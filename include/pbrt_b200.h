@@ -70,7 +70,7 @@ int pbrt_ctx_sync(pbrt_ctx* ctx);
 
 /* ---------------------------------------------------------------------------------- */
 /* Scene description (flat POD; replaces building Scene/Object/Shape/Material/Light     */
-/* trait objects: src/scene.rs:89-115, src/objects/*.rs, src/shapes/*.rs)              */
+/* trait objects: src/scene.rs:89-115, the files of src/objects/ and src/shapes/)       */
 /* ---------------------------------------------------------------------------------- */
 
 typedef enum pbrt_shape_kind {
@@ -213,6 +213,48 @@ int pbrt_trace_closest_noalloc(pbrt_scene* scene, const float* rays, uint64_t n,
 /* Whether anything blocks each ray within [tmin, tmax]: replaces Scene::intersect_p
  * (src/scene.rs:143-168) and BVHTree::intersect_p (src/shapes/triangle_mesh/bvh.rs:381-420). */
 int pbrt_trace_any(pbrt_scene* scene, const float* rays, uint64_t n, uint8_t* occluded);
+
+/* ---------------------------------------------------------------------------------- */
+/* Rendering                                                                            */
+/* ---------------------------------------------------------------------------------- */
+
+/* PinHoleCamera::new(resolution, fov, near, far, Matrix4::look_at(position, look_at, up))
+ * (src/cameras/pin_hole.rs:17-38, src/geom/matrix4.rs:70-98). near/far are also every
+ * ray's [near, far] interval, as the reference passes Config::near/far to li(). */
+typedef struct pbrt_camera_desc {
+  uint32_t width, height;
+  float fov; /* full field of view, radians */
+  float near, far;
+  float position[3], look_at[3], up[3];
+} pbrt_camera_desc;
+
+typedef enum pbrt_integrator {
+  PBRT_INTEGRATOR_PATH = 0, /* PathIntegrator (src/integrators/path.rs:48-115) + area-light NEE */
+  PBRT_INTEGRATOR_NAIVE = 1 /* NaiveIntegrator (src/integrators/naive.rs:29-52), background = the
+                               scene's infinite lights */
+} pbrt_integrator;
+
+typedef struct pbrt_render_params {
+  pbrt_camera_desc camera;
+  uint32_t spp;           /* Config::samples_ppx */
+  uint32_t max_depth;     /* PathIntegrator::max_depth */
+  uint32_t rr_start;      /* Russian roulette from this bounce (q = min(1, max beta)); 0 = off, as the
+                             reference's is commented out (path.rs:92-101) */
+  uint32_t sample_offset; /* index of the first sample: progressive rendering, resume */
+  uint64_t seed;          /* PCG32, one stream per pixel, re-keyed per (pixel, sample) */
+  uint32_t integrator;    /* pbrt_integrator */
+  uint32_t flags;         /* reserved, 0 */
+} pbrt_render_params;
+
+/* Mean radiance per pixel over spp samples into film_rgb (width*height*3 doubles, row-major,
+ * row 0 at the top), host or device memory; per-sample radiance is FP32, the film FP64.
+ * Replaces renderers::mt::render / st::render (src/renderers/mt.rs:23-110, 112-130). */
+int pbrt_render(pbrt_scene* scene, const pbrt_render_params* params, double* film_rgb);
+
+/* Spectrum::gamma_correct + to_rgb (src/spectrum.rs:13-25, 134-136): sqrt gamma, clip to
+ * [0, 1], truncate to 8 bits, alpha 255, as image_write stores it (mt.rs:152-167). Host
+ * buffers; no GPU work. */
+int pbrt_film_to_rgba8(const double* film_rgb, uint32_t width, uint32_t height, uint8_t* rgba);
 
 #ifdef __cplusplus
 }

@@ -193,3 +193,189 @@ def make_ray(origin, direction, dtype=np.float64):
     out = np.zeros(6, dt)
     getattr(lib(), f"oracle_make_ray_{suf}")(_ptr(o), _ptr(d), _ptr(out))
     return out[:3].copy(), out[3:].copy()
+
+
+# ------------------------------------------------------------------------------------------
+# Scenes and rendering (pbrt_oracle_pt.hpp)
+#
+# A scene is described by a plain dict, the same one the tests lower into the product:
+#   meshes:    [{"vertices": (n,3) float32, "indices": (m,3) uint32}]
+#   materials: [{"kind": 0 lambertian | 1 metal | 2 dielectric | 3 diffuse light,
+#                "color": (3,), "fuzz": f, "ior": f}]
+#   objects:   [{"shape": 0 mesh | 1 sphere | 2 cylinder, "mesh": i, "radius": r, "height": h,
+#                "material": i, "to_world": (12,) or None, "to_local": (12,) or None}]
+#   lights:    [{"kind": 0 point | 1 uniform infinite | 2 background | 3 area, "position": (3,),
+#                "radiance": (3,), "bottom": (3,), "top": (3,), "object": i}]
+#   bvh_bins, bvh_max_leaf
+# camera: {"width", "height", "fov" (radians), "near", "far", "position", "look_at", "up"}
+# ------------------------------------------------------------------------------------------
+class _OMesh(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("vertex_count", C.c_uint32), ("indices", C.c_void_p),
+                ("triangle_count", C.c_uint32)]
+
+
+class _OMaterial(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("color", C.c_float * 3), ("fuzz", C.c_float), ("ior", C.c_float)]
+
+
+class _OObject(C.Structure):
+    _fields_ = [("shape", C.c_uint32), ("mesh", C.c_uint32), ("radius", C.c_float), ("height", C.c_float),
+                ("material", C.c_uint32), ("transformed", C.c_uint32), ("to_world", C.c_float * 12),
+                ("to_local", C.c_float * 12)]
+
+
+class _OLight(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("position", C.c_float * 3), ("radiance", C.c_float * 3),
+                ("bottom", C.c_float * 3), ("top", C.c_float * 3), ("object", C.c_uint32)]
+
+
+class _OScene(C.Structure):
+    _fields_ = [("meshes", C.c_void_p), ("mesh_count", C.c_uint32), ("materials", C.c_void_p),
+                ("material_count", C.c_uint32), ("objects", C.c_void_p), ("object_count", C.c_uint32),
+                ("lights", C.c_void_p), ("light_count", C.c_uint32), ("bvh_bins", C.c_uint32),
+                ("bvh_max_leaf", C.c_uint32)]
+
+
+class _OCamera(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("fov", C.c_float), ("near", C.c_float),
+                ("far", C.c_float), ("position", C.c_float * 3), ("look_at", C.c_float * 3), ("up", C.c_float * 3)]
+
+
+class _ORender(C.Structure):
+    _fields_ = [("camera", _OCamera), ("spp", C.c_uint32), ("max_depth", C.c_uint32), ("rr_start", C.c_uint32),
+                ("sample_offset", C.c_uint32), ("seed", C.c_uint64), ("integrator", C.c_uint32)]
+
+
+def _camera(cam: dict) -> _OCamera:
+    c = _OCamera()
+    c.width, c.height = int(cam["width"]), int(cam["height"])
+    c.fov, c.near, c.far = float(cam["fov"]), float(cam["near"]), float(cam["far"])
+    c.position[:] = [float(x) for x in cam["position"]]
+    c.look_at[:] = [float(x) for x in cam["look_at"]]
+    c.up[:] = [float(x) for x in cam["up"]]
+    return c
+
+
+def _declare_scene(L):
+    vp, sz = C.c_void_p, C.c_size_t
+    for suf in ("f64", "f32"):
+        getattr(L, f"oracle_scene_new_{suf}").restype = vp
+        getattr(L, f"oracle_scene_new_{suf}").argtypes = [C.POINTER(_OScene)]
+        getattr(L, f"oracle_scene_free_{suf}").argtypes = [vp]
+        getattr(L, f"oracle_scene_trace_{suf}").argtypes = [vp, vp, sz, vp, vp, vp, C.c_int]
+        getattr(L, f"oracle_scene_occluded_{suf}").argtypes = [vp, vp, sz, vp, C.c_int]
+        getattr(L, f"oracle_render_{suf}").argtypes = [vp, C.POINTER(_ORender), vp, C.c_int]
+        getattr(L, f"oracle_camera_rays_{suf}").argtypes = [C.POINTER(_OCamera), vp]
+        getattr(L, f"oracle_scene_bvh_{suf}").argtypes = [vp, vp, vp, vp, vp]
+        getattr(L, f"oracle_scene_bvh_nodes_{suf}").restype = sz
+        getattr(L, f"oracle_scene_bvh_nodes_{suf}").argtypes = [vp]
+
+
+class Scene:
+    """The reference's Scene (src/scene.rs) with its objects, materials and lights, in f64
+    or in the f32 restatement; renders with the path or naive integrator."""
+
+    def __init__(self, desc: dict, dtype=np.float32):
+        L = lib()
+        if not getattr(L, "_scene_declared", False):
+            _declare_scene(L)
+            L._scene_declared = True
+        self.dtype = np.dtype(dtype)
+        self.suf = "f64" if self.dtype == np.float64 else "f32"
+        self._keep = []
+        ms = []
+        for m in desc.get("meshes", []):
+            v = np.ascontiguousarray(m["vertices"], np.float32).reshape(-1, 3)
+            i = np.ascontiguousarray(m["indices"], np.uint32).reshape(-1, 3)
+            self._keep += [v, i]
+            ms.append(_OMesh(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0]))
+        mats = []
+        for m in desc.get("materials", []):
+            d = _OMaterial()
+            d.kind = int(m["kind"])
+            d.color[:] = [float(c) for c in m.get("color", (0, 0, 0))]
+            d.fuzz, d.ior = float(m.get("fuzz", 0.0)), float(m.get("ior", 1.0))
+            mats.append(d)
+        objs = []
+        for o in desc.get("objects", []):
+            d = _OObject()
+            d.shape, d.mesh = int(o["shape"]), int(o.get("mesh", 0))
+            d.radius, d.height = float(o.get("radius", 0.0)), float(o.get("height", 0.0))
+            d.material = int(o["material"])
+            if o.get("to_world") is not None:
+                d.transformed = 1
+                d.to_world[:] = [float(x) for x in np.asarray(o["to_world"]).reshape(-1)[:12]]
+                d.to_local[:] = [float(x) for x in np.asarray(o["to_local"]).reshape(-1)[:12]]
+            objs.append(d)
+        lts = []
+        for l in desc.get("lights", []):
+            d = _OLight()
+            d.kind = int(l["kind"])
+            for k in ("position", "radiance", "bottom", "top"):
+                getattr(d, k)[:] = [float(x) for x in l.get(k, (0, 0, 0))]
+            d.object = int(l.get("object", 0))
+            lts.append(d)
+        arrs = [(_OMesh * max(1, len(ms)))(*ms), (_OMaterial * max(1, len(mats)))(*mats),
+                (_OObject * max(1, len(objs)))(*objs), (_OLight * max(1, len(lts)))(*lts)]
+        self._keep += arrs
+        sd = _OScene(C.addressof(arrs[0]), len(ms), C.addressof(arrs[1]), len(mats), C.addressof(arrs[2]), len(objs),
+                     C.addressof(arrs[3]), len(lts), int(desc.get("bvh_bins", 8)), int(desc.get("bvh_max_leaf", 1)))
+        self._h = getattr(L, f"oracle_scene_new_{self.suf}")(C.byref(sd))
+        if not self._h:
+            raise ValueError(L.oracle_last_error().decode())
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            getattr(_lib, f"oracle_scene_free_{self.suf}")(h)
+            self._h = None
+
+    def trace(self, rays, threads: int = os.cpu_count() or 1):
+        """Scene::intersect per ray: (prim, object, t); prim is the triangle index (0 for an
+        analytic shape), both MISS on a miss."""
+        rays = np.ascontiguousarray(rays, dtype=self.dtype)
+        n = rays.shape[1]
+        prim, obj, t = np.empty(n, np.uint32), np.empty(n, np.uint32), np.empty(n, self.dtype)
+        getattr(lib(), f"oracle_scene_trace_{self.suf}")(self._h, _ptr(rays), n, _ptr(prim), _ptr(obj), _ptr(t),
+                                                         threads)
+        return prim, obj, t
+
+    def occluded(self, rays, threads: int = os.cpu_count() or 1):
+        rays = np.ascontiguousarray(rays, dtype=self.dtype)
+        occ = np.empty(rays.shape[1], np.uint8)
+        getattr(lib(), f"oracle_scene_occluded_{self.suf}")(self._h, _ptr(rays), rays.shape[1], _ptr(occ), threads)
+        return occ
+
+    def bvh(self):
+        n = getattr(lib(), f"oracle_scene_bvh_nodes_{self.suf}")(self._h)
+        boxes = np.zeros((n, 6), self.dtype)
+        lf, cnt = np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+        order = np.zeros(max(1, n), np.uint32)
+        getattr(lib(), f"oracle_scene_bvh_{self.suf}")(self._h, _ptr(boxes), _ptr(lf), _ptr(cnt), _ptr(order))
+        return boxes, lf, cnt, order
+
+    def render(self, camera: dict, spp: int, max_depth: int, seed: int = 1, rr_start: int = 0,
+               sample_offset: int = 0, integrator: str = "path", threads: int = os.cpu_count() or 1):
+        """Mean radiance per pixel, (height, width, 3) float64 (renderers/mt.rs:112-130)."""
+        p = _ORender()
+        p.camera = _camera(camera)
+        p.spp, p.max_depth, p.rr_start, p.sample_offset = spp, max_depth, rr_start, sample_offset
+        p.seed, p.integrator = seed, 1 if integrator == "naive" else 0
+        film = np.zeros((int(camera["height"]), int(camera["width"]), 3), np.float64)
+        if getattr(lib(), f"oracle_render_{self.suf}")(self._h, C.byref(p), _ptr(film), threads) != 0:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return film
+
+
+def camera_rays(camera: dict, dtype=np.float32):
+    """Pixel-centre primary rays of PinHoleCamera (src/cameras/pin_hole.rs:42-50), row-major."""
+    L = lib()
+    if not getattr(L, "_scene_declared", False):
+        _declare_scene(L)
+        L._scene_declared = True
+    dt = np.dtype(dtype)
+    n = int(camera["width"]) * int(camera["height"])
+    out = np.zeros((8, n), dt)
+    c = _camera(camera)
+    getattr(L, f"oracle_camera_rays_{'f64' if dt == np.float64 else 'f32'}")(C.byref(c), _ptr(out))
+    return out

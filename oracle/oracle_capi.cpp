@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "pbrt_oracle.hpp"
+#include "pbrt_oracle_pt.hpp"
 
 
 using namespace oracle;
@@ -281,5 +282,127 @@ int oracle_ply_read(const char* path, int reverse, double** verts_out, size_t* n
 
 ORACLE_MESH_API(f64, double)
 ORACLE_MESH_API(f32, float)
+
+}  // extern "C"
+
+namespace {
+
+template <class R>
+int scene_trace(const OScene<R>* s, const R* rays, size_t n, uint32_t* prim, uint32_t* obj, R* t, int threads) {
+  parallel_for(n, threads, [&](size_t b, size_t e) {
+    for (size_t i = b; i < e; ++i) {
+      R tmin, tmax;
+      Ray<R> r = load_ray(rays, n, i, &tmin, &tmax);
+      Isect<R> it;
+      uint32_t o = 0xFFFFFFFFu, p = 0xFFFFFFFFu;
+      if (s->intersect(r, tmin, tmax, &it, &o, &p)) {
+        prim[i] = p;
+        obj[i] = o;
+        t[i] = it.d;
+      } else {
+        prim[i] = 0xFFFFFFFFu;
+        obj[i] = 0xFFFFFFFFu;
+        t[i] = std::numeric_limits<R>::infinity();
+      }
+    }
+  });
+  return 0;
+}
+
+template <class R>
+int scene_occluded(const OScene<R>* s, const R* rays, size_t n, uint8_t* occ, int threads) {
+  parallel_for(n, threads, [&](size_t b, size_t e) {
+    for (size_t i = b; i < e; ++i) {
+      R tmin, tmax;
+      Ray<R> r = load_ray(rays, n, i, &tmin, &tmax);
+      occ[i] = s->occluded(r, tmin, tmax) ? 1 : 0;
+    }
+  });
+  return 0;
+}
+
+// renderers::mt::compute_pixel (mt.rs:112-130): spp jittered samples through the pinhole
+// camera, mean radiance per pixel (accumulated in f64, the film the judge image needs).
+template <class R>
+int render(const OScene<R>* s, const ORenderParams* p, double* film, int threads) {
+  const PinHoleCamera<R> cam = make_camera<R>(p->camera);
+  const uint32_t w = p->camera.width, h = p->camera.height;
+  const size_t npix = size_t(w) * h;
+  parallel_for(npix, threads, [&](size_t b, size_t e) {
+    for (size_t pix = b; pix < e; ++pix) {
+      const uint32_t x = uint32_t(pix % w), y = uint32_t(pix / w);
+      double acc[3] = {0, 0, 0};
+      for (uint32_t k = 0; k < p->spp; ++k) {
+        Pcg32 rng = path_rng(p->seed, uint32_t(pix), p->sample_offset + k);
+        const R jx = R(rng.uniform()), jy = R(rng.uniform());  // Sampler2::sample (mt.rs:145-150)
+        const Ray<R> ray = cam.get_ray(R(x) + jx, R(y) + jy);
+        const V3<R> L = p->integrator == 1 ? s->li_naive(ray, R(p->camera.near), R(p->camera.far), p->max_depth, rng)
+                                           : s->li_path(ray, R(p->camera.near), R(p->camera.far), p->max_depth,
+                                                        p->rr_start, rng);
+        acc[0] += double(L.x);
+        acc[1] += double(L.y);
+        acc[2] += double(L.z);
+      }
+      for (int c = 0; c < 3; ++c) film[3 * pix + c] = acc[c] / double(p->spp);
+    }
+  });
+  return 0;
+}
+
+template <class R>
+void camera_rays(const OCameraDesc* c, R* out) {
+  const PinHoleCamera<R> cam = make_camera<R>(*c);
+  const size_t n = size_t(c->width) * c->height;
+  for (size_t pix = 0; pix < n; ++pix) {
+    const Ray<R> r = cam.get_ray(R(pix % c->width) + R(0.5), R(pix / c->width) + R(0.5));
+    out[pix] = r.o.x; out[n + pix] = r.o.y; out[2 * n + pix] = r.o.z;
+    out[3 * n + pix] = r.d.x; out[4 * n + pix] = r.d.y; out[5 * n + pix] = r.d.z;
+    out[6 * n + pix] = R(c->near); out[7 * n + pix] = R(c->far);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+#define ORACLE_SCENE_API(SUF, R)                                                                            \
+  void* oracle_scene_new_##SUF(const OSceneDesc* d) {                                                       \
+    try {                                                                                                   \
+      return new OScene<R>(*d);                                                                             \
+    } catch (const std::exception& e) {                                                                     \
+      g_err = e.what();                                                                                     \
+      return nullptr;                                                                                       \
+    }                                                                                                       \
+  }                                                                                                         \
+  void oracle_scene_free_##SUF(void* s) { delete (OScene<R>*)s; }                                           \
+  int oracle_scene_trace_##SUF(void* s, const R* rays, size_t n, uint32_t* prim, uint32_t* obj, R* t, int th) { \
+    return scene_trace((OScene<R>*)s, rays, n, prim, obj, t, th);                                           \
+  }                                                                                                         \
+  int oracle_scene_occluded_##SUF(void* s, const R* rays, size_t n, uint8_t* occ, int th) {                 \
+    return scene_occluded((OScene<R>*)s, rays, n, occ, th);                                                 \
+  }                                                                                                         \
+  int oracle_render_##SUF(void* s, const ORenderParams* p, double* film, int th) {                          \
+    try {                                                                                                   \
+      return render((OScene<R>*)s, p, film, th);                                                            \
+    } catch (const std::exception& e) {                                                                     \
+      g_err = e.what();                                                                                     \
+      return -1;                                                                                            \
+    }                                                                                                       \
+  }                                                                                                         \
+  void oracle_camera_rays_##SUF(const OCameraDesc* c, R* out) { camera_rays(c, out); }                     \
+  void oracle_scene_bvh_##SUF(void* s, R* boxes, uint32_t* left_first, uint32_t* count, uint32_t* order) {  \
+    const OScene<R>* sc = (OScene<R>*)s;                                                                    \
+    for (size_t i = 0; i < sc->bnodes.size(); ++i) {                                                        \
+      const auto& b = sc->bnodes[i].box;                                                                    \
+      boxes[6 * i] = b.bmin.x; boxes[6 * i + 1] = b.bmin.y; boxes[6 * i + 2] = b.bmin.z;                    \
+      boxes[6 * i + 3] = b.bmax.x; boxes[6 * i + 4] = b.bmax.y; boxes[6 * i + 5] = b.bmax.z;                \
+      left_first[i] = sc->bnodes[i].left_first; count[i] = sc->bnodes[i].count;                             \
+    }                                                                                                       \
+    for (size_t i = 0; i < sc->order.size(); ++i) order[i] = sc->order[i];                                  \
+  }                                                                                                         \
+  size_t oracle_scene_bvh_nodes_##SUF(void* s) { return ((OScene<R>*)s)->bnodes.size(); }
+
+ORACLE_SCENE_API(f64, double)
+ORACLE_SCENE_API(f32, float)
 
 }  // extern "C"

@@ -1,0 +1,887 @@
+// pbrt_oracle_pt.hpp — TEST INFRASTRUCTURE, NOT THE PRODUCT.
+//
+// The scene-level half of the CPU oracle: objects (Simple / Transformed), analytic shapes,
+// the scene BVH, materials, lights, the sampler and the path integrator, restated from
+// nmichel/pbrt in the reference's operation order (citations are path:line there).
+//
+// Extensions the reference plans but does not implement, written from its own notes:
+//   - AreaLight NEE (ideas/area_light.md §2-§6): uniform area sampling, p(ω) = p(A)·d²/|cosθ_l|,
+//     zero pdf → no sample; emission is two-sided, as DiffuseLight::emit is
+//     (src/materials/diffuse_light.rs:18-22); the shadow ray stops at (1 - 1e-4)·d so the
+//     sampled point's own surface does not occlude it. The specular guard of path.rs:58 is kept.
+//   - Russian roulette in the commented form of path.rs:92-101, from bounce `rr_start`, with
+//     q clamped to 1 (without the clamp a path with max(β) > 1 would be scaled down, a bias).
+//   - A seeded sampler (ideas/rng_graine.md §7-§8): PCG32, one stream per pixel, re-keyed per
+//     (pixel, sample); a uniform draw is the top 24 bits of one output times 2^-24.
+//   - The naive estimator (src/integrators/naive.rs:29-52) with the scene's infinite lights as
+//     its background instead of the hard-coded sky, so naive and path integrate the same scene
+//     (the cross-check ideas/area_light.md:131-136 asks for).
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <vector>
+
+#include "pbrt_oracle.hpp"
+
+namespace oracle {
+
+// ---------------------------------------------------------------------------------------
+// Sampler
+// ---------------------------------------------------------------------------------------
+struct Pcg32 {
+  uint64_t state = 0, inc = 1;
+  uint32_t next() {
+    const uint64_t old = state;
+    state = old * 6364136223846793005ULL + inc;
+    const uint32_t xs = uint32_t(((old >> 18u) ^ old) >> 27u);
+    const uint32_t rot = uint32_t(old >> 59u);
+    return (xs >> rot) | (xs << ((32u - rot) & 31u));
+  }
+  void seed(uint64_t initstate, uint64_t initseq) {
+    state = 0;
+    inc = (initseq << 1u) | 1u;
+    next();
+    state += initstate;
+    next();
+  }
+  float uniform() { return float(next() >> 8) * (1.0f / 16777216.0f); }
+};
+
+inline uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ULL;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+  return x ^ (x >> 31);
+}
+
+// One stream per pixel, re-keyed per (pixel, sample).
+inline Pcg32 path_rng(uint64_t seed, uint32_t pixel, uint32_t sample) {
+  Pcg32 r;
+  r.seed(splitmix64(seed ^ splitmix64((uint64_t(pixel) << 32) | sample)), pixel);
+  return r;
+}
+
+template <class R> struct Consts {
+  static R pi() { return R(3.141592653589793238462643383279502884L); }
+};
+
+// ---------------------------------------------------------------------------------------
+// Intersection record — src/geom/intersectable.rs:8-28, 92-144
+// ---------------------------------------------------------------------------------------
+template <class R>
+struct Isect {
+  V3<R> p, n, wo, dpdu, dpdv;
+  R d, u, v;
+  // world_to_local / local_to_world: ss = normalize(dpdu), ts = n x ss, ns = n
+  V3<R> to_local(const V3<R>& w) const {
+    V3<R> ss = normalized(dpdu);
+    V3<R> ts = cross(n, ss);
+    return V3<R>{dot(ss, w), dot(ts, w), dot(n, w)};
+  }
+  V3<R> to_world(const V3<R>& l) const {
+    V3<R> ss = normalized(dpdu);
+    V3<R> ts = cross(n, ss);
+    return V3<R>{ss.x * l.x + ts.x * l.y + n.x * l.z, ss.y * l.x + ts.y * l.y + n.y * l.z,
+                 ss.z * l.x + ts.z * l.y + n.z * l.z};
+  }
+};
+
+// 3x4 affine matrix (the bottom row of every Transform on the path is 0 0 0 1, so the
+// `w != 1` division of Matrix4::transform_point never triggers).
+template <class R>
+struct Affine {
+  R m[3][4];
+  V3<R> point(const V3<R>& v) const {
+    return {m[0][0] * v.x + m[0][1] * v.y + m[0][2] * v.z + m[0][3], m[1][0] * v.x + m[1][1] * v.y + m[1][2] * v.z + m[1][3],
+            m[2][0] * v.x + m[2][1] * v.y + m[2][2] * v.z + m[2][3]};
+  }
+  V3<R> direction(const V3<R>& v) const {
+    return {m[0][0] * v.x + m[0][1] * v.y + m[0][2] * v.z, m[1][0] * v.x + m[1][1] * v.y + m[1][2] * v.z,
+            m[2][0] * v.x + m[2][1] * v.y + m[2][2] * v.z};
+  }
+  // transform_normal multiplies by the transpose (matrix4.rs:208-213)
+  V3<R> normal(const V3<R>& v) const {
+    return {m[0][0] * v.x + m[1][0] * v.y + m[2][0] * v.z, m[0][1] * v.x + m[1][1] * v.y + m[2][1] * v.z,
+            m[0][2] * v.x + m[1][2] * v.y + m[2][2] * v.z};
+  }
+};
+
+// ---------------------------------------------------------------------------------------
+// Scene description (the oracle's own POD; tests lower one scene into it and into the
+// product's C description)
+// ---------------------------------------------------------------------------------------
+enum { O_SHAPE_MESH = 0, O_SHAPE_SPHERE = 1, O_SHAPE_CYLINDER = 2 };
+enum { O_MAT_LAMBERTIAN = 0, O_MAT_METAL = 1, O_MAT_DIELECTRIC = 2, O_MAT_DIFFUSE_LIGHT = 3 };
+enum { O_LIGHT_POINT = 0, O_LIGHT_UNIFORM = 1, O_LIGHT_BACKGROUND = 2, O_LIGHT_AREA = 3 };
+
+struct OMeshDesc {
+  const float* vertices;
+  uint32_t vertex_count;
+  const uint32_t* indices;
+  uint32_t triangle_count;
+};
+struct OMaterialDesc {
+  uint32_t kind;
+  float color[3];
+  float fuzz, ior;
+};
+struct OObjectDesc {
+  uint32_t shape, mesh;
+  float radius, height;
+  uint32_t material, transformed;
+  float to_world[12], to_local[12];
+};
+struct OLightDesc {
+  uint32_t kind;
+  float position[3], radiance[3], bottom[3], top[3];
+  uint32_t object;
+};
+struct OSceneDesc {
+  const OMeshDesc* meshes;
+  uint32_t mesh_count;
+  const OMaterialDesc* materials;
+  uint32_t material_count;
+  const OObjectDesc* objects;
+  uint32_t object_count;
+  const OLightDesc* lights;
+  uint32_t light_count;
+  uint32_t bvh_bins, bvh_max_leaf;
+};
+struct OCameraDesc {
+  uint32_t width, height;
+  float fov, near, far;
+  float position[3], look_at[3], up[3];
+};
+struct ORenderParams {
+  OCameraDesc camera;
+  uint32_t spp, max_depth, rr_start, sample_offset;
+  uint64_t seed;
+  uint32_t integrator;  // 0 path, 1 naive
+};
+
+// ---------------------------------------------------------------------------------------
+// Scene
+// ---------------------------------------------------------------------------------------
+template <class R>
+class OScene {
+ public:
+  struct Mesh {
+    std::unique_ptr<MeshBVH<R>> bvh;
+    std::vector<R> v;
+    std::vector<uint32_t> idx;
+  };
+  struct Object {
+    uint32_t shape, mesh, material;
+    R radius, height, half_height;
+    bool transformed;
+    Affine<R> mat, inv;
+  };
+  struct Material {
+    uint32_t kind;
+    V3<R> color;
+    R fuzz, ior;
+  };
+  struct Light {
+    uint32_t kind;
+    V3<R> pos, rad, bottom, top;
+    uint32_t object;
+    // area lights: world-space triangles (mesh) and their area CDF, or the sphere's centre/radius
+    std::vector<V3<R>> tp;  // 3 per triangle
+    std::vector<R> cdf;     // running sum of areas
+    R area = R(0);
+  };
+  struct BNode {
+    AABB<R> box;
+    uint32_t left_first, count;
+  };
+
+  explicit OScene(const OSceneDesc& d) {
+    for (uint32_t i = 0; i < d.mesh_count; ++i) {
+      const OMeshDesc& md = d.meshes[i];
+      Mesh m;
+      m.v.assign(md.vertices, md.vertices + 3 * size_t(md.vertex_count));
+      m.idx.assign(md.indices, md.indices + 3 * size_t(md.triangle_count));
+      m.bvh.reset(new MeshBVH<R>(m.v.data(), md.vertex_count, m.idx.data(), md.triangle_count,
+                                 d.bvh_bins ? int(d.bvh_bins) : 8, d.bvh_max_leaf ? d.bvh_max_leaf : 1));
+      meshes.push_back(std::move(m));
+    }
+    for (uint32_t i = 0; i < d.material_count; ++i) {
+      const OMaterialDesc& m = d.materials[i];
+      materials.push_back(Material{m.kind, V3<R>{R(m.color[0]), R(m.color[1]), R(m.color[2])}, R(m.fuzz), R(m.ior)});
+    }
+    for (uint32_t i = 0; i < d.object_count; ++i) {
+      const OObjectDesc& o = d.objects[i];
+      Object ob;
+      ob.shape = o.shape;
+      ob.mesh = o.mesh;
+      ob.material = o.material;
+      ob.radius = R(o.radius);
+      ob.height = R(o.height);
+      ob.half_height = R(o.height) / R(2);  // Cylinder::new (cylinder.rs:12-19)
+      ob.transformed = o.transformed != 0;
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 4; ++c) {
+          ob.mat.m[r][c] = R(o.to_world[4 * r + c]);
+          ob.inv.m[r][c] = R(o.to_local[4 * r + c]);
+        }
+      if (ob.shape == O_SHAPE_MESH && ob.mesh >= meshes.size()) throw std::invalid_argument("bad mesh index");
+      objects.push_back(ob);
+    }
+    for (uint32_t i = 0; i < d.light_count; ++i) {
+      const OLightDesc& l = d.lights[i];
+      Light L;
+      L.kind = l.kind;
+      L.pos = {R(l.position[0]), R(l.position[1]), R(l.position[2])};
+      L.rad = {R(l.radiance[0]), R(l.radiance[1]), R(l.radiance[2])};
+      L.bottom = {R(l.bottom[0]), R(l.bottom[1]), R(l.bottom[2])};
+      L.top = {R(l.top[0]), R(l.top[1]), R(l.top[2])};
+      L.object = l.object;
+      if (L.kind == O_LIGHT_AREA) setup_area(L);
+      lights.push_back(L);
+    }
+    build_bvh();
+  }
+
+  // ---- geometry of one object ----------------------------------------------------------
+  AABB<R> object_box(const Object& o) const {
+    AABB<R> b;
+    if (o.shape == O_SHAPE_MESH) {
+      b = meshes[o.mesh].bvh->vertex_bounds();
+    } else if (o.shape == O_SHAPE_SPHERE) {
+      b = AABB<R>{{-o.radius, -o.radius, -o.radius}, {o.radius, o.radius, o.radius}};
+    } else {
+      b = AABB<R>{{-o.radius, -o.half_height, -o.radius}, {o.radius, o.half_height, o.radius}};
+    }
+    if (!o.transformed) return b;
+    // Transformable for AABoundingBox (aabound.rs:437-468): the eight corners
+    const V3<R> mn = b.bmin, mx = b.bmax;
+    const V3<R> c[8] = {{mn.x, mn.y, mn.z}, {mn.x, mn.y, mx.z}, {mn.x, mx.y, mn.z}, {mn.x, mx.y, mx.z},
+                        {mx.x, mx.y, mx.z}, {mx.x, mx.y, mn.z}, {mx.x, mn.y, mx.z}, {mx.x, mn.y, mn.z}};
+    AABB<R> t{{Limits<R>::max(), Limits<R>::max(), Limits<R>::max()},
+              {Limits<R>::lowest(), Limits<R>::lowest(), Limits<R>::lowest()}};
+    for (int k = 0; k < 8; ++k) {
+      V3<R> p = o.mat.point(c[k]);
+      t.bmin = {rmin(t.bmin.x, p.x), rmin(t.bmin.y, p.y), rmin(t.bmin.z, p.z)};
+      t.bmax = {rmax(t.bmax.x, p.x), rmax(t.bmax.y, p.y), rmax(t.bmax.z, p.z)};
+    }
+    return t;
+  }
+
+  // Sphere::intersect (sphere.rs:108-144) — first listed hit, as Simple::intersect keeps
+  bool sphere_hit(const Object& o, const Ray<R>& ray, R near, R far, R* t_out) const {
+    const V3<R> l = ray.o * R(-1);
+    const R tca = dot(l, ray.d);
+    if (tca < R(0)) return false;
+    const R r2 = o.radius * o.radius;
+    const R d2 = dot(l, l) - tca * tca;
+    if (d2 > r2) return false;
+    const R thc = std::sqrt(r2 - d2);
+    const R t0 = tca - thc, t1 = tca + thc;
+    const R tmin = rmin(t0, t1), tmax = rmax(t0, t1);
+    if (tmax < near || tmin > far) return false;
+    if (tmin > near) { *t_out = tmin; return true; }
+    if (tmax > near && tmax < far) { *t_out = tmax; return true; }
+    return false;
+  }
+
+  // Cylinder::intersect (cylinder.rs:28-110): all hits, sorted; first kept. Returns the
+  // index of the piece (0 wall, 1 bottom cap, 2 top cap) through *piece.
+  bool cylinder_hit(const Object& o, const Ray<R>& ray, R near, R far, R* t_out, int* piece) const {
+    const V3<R>& org = ray.o;
+    const V3<R>& dir = ray.d;
+    const R a = dir.x * dir.x + dir.z * dir.z;
+    const R b = R(2) * (org.x * dir.x + org.z * dir.z);
+    const R c = org.x * org.x + org.z * org.z - o.radius * o.radius;
+    const R disc = b * b - R(4) * a * c;
+    if (disc < R(0)) return false;
+    const R rd = std::sqrt(disc);
+    const R q = b < R(0) ? R(-0.5) * (b - rd) : R(-0.5) * (b + rd);
+    const R t0 = q / a, t1 = c / q;
+    const R tmin = rmin(t0, t1), tmax = rmax(t0, t1);
+    if (tmax < near || tmin > far) return false;
+    R ts[4];
+    int ps[4];
+    int n = 0;
+    if (tmin > near) {
+      const V3<R> p = org + dir * tmin;
+      if (p.y > -o.half_height && p.y < o.half_height) { ts[n] = tmin; ps[n] = 0; n++; }
+    }
+    if (tmax > near && tmax < far) {
+      const V3<R> p = org + dir * tmax;
+      if (p.y > -o.half_height && p.y < o.half_height) { ts[n] = tmax; ps[n] = 0; n++; }
+    }
+    if (n < 2) {
+      const R inv_dir_y = R(1) / dir.y;
+      const R c0 = (-o.half_height - org.y) * inv_dir_y;
+      if (c0 > near && c0 < far) {
+        const V3<R> p = org + dir * c0;
+        if (p.x * p.x + p.z * p.z <= o.radius * o.radius) { ts[n] = c0; ps[n] = 1; n++; }
+      }
+      const R c1 = (o.half_height - org.y) * inv_dir_y;
+      if (c1 > near && c1 < far) {
+        const V3<R> p = org + dir * c1;
+        if (p.x * p.x + p.z * p.z <= o.radius * o.radius) { ts[n] = c1; ps[n] = 2; n++; }
+      }
+    }
+    if (n == 0) return false;
+    // sort_by partial_cmp (stable): the smallest d, first among equals
+    int best = 0;
+    for (int k = 1; k < n; ++k)
+      if (ts[k] < ts[best]) best = k;
+    *t_out = ts[best];
+    *piece = ps[best];
+    return true;
+  }
+
+  Ray<R> local_ray(const Object& o, const Ray<R>& ray) const {
+    if (!o.transformed) return ray;
+    return make_ray(o.inv.point(ray.o), o.inv.direction(ray.d));  // transform_ray_to_local (transform.rs:98-103)
+  }
+
+  // Object::intersect → the world-space interaction (transformed.rs:27-38, simple.rs:28-41)
+  bool intersect_object(uint32_t oi, const Ray<R>& ray, R near, R far, Isect<R>* out, uint32_t* prim) const {
+    const Object& o = objects[oi];
+    const Ray<R> lr = local_ray(o, ray);
+    Isect<R> h;
+    if (o.shape == O_SHAPE_MESH) {
+      const Mesh& m = meshes[o.mesh];
+      TriHit<R> th;
+      uint32_t tri;
+      TraversalStats st;
+      if (!m.bvh->traverse(lr, near, far, &th, &tri, &st)) return false;
+      mesh_details(m, tri, lr, th, &h);
+      *prim = tri;
+    } else if (o.shape == O_SHAPE_SPHERE) {
+      R t;
+      if (!sphere_hit(o, lr, near, far, &t)) return false;
+      sphere_details(o, lr, t, &h);
+      *prim = 0;
+    } else {
+      R t;
+      int piece;
+      if (!cylinder_hit(o, lr, near, far, &t, &piece)) return false;
+      cylinder_details(o, lr, t, piece, &h);
+      *prim = uint32_t(piece);  // 0 wall, 1 bottom cap, 2 top cap
+    }
+    if (o.transformed) {  // transform_interaction_to_world (transform.rs:105-116)
+      Isect<R> w = h;
+      w.n = o.inv.normal(h.n);
+      w.p = o.mat.point(h.p);
+      w.wo = o.mat.direction(h.wo);
+      w.dpdu = o.mat.direction(h.dpdu);
+      w.dpdv = o.mat.direction(h.dpdv);
+      h = w;
+    }
+    *out = h;
+    return true;
+  }
+
+  // Intersectable::intersect_p through Simple/Transformed (simple.rs:70-72, transformed.rs:145-148)
+  bool occluded_object(uint32_t oi, const Ray<R>& ray, R near, R far) const {
+    const Object& o = objects[oi];
+    const Ray<R> lr = local_ray(o, ray);
+    if (o.shape == O_SHAPE_MESH) return meshes[o.mesh].bvh->intersect_p(lr, near, far);
+    R t;
+    int piece;
+    if (o.shape == O_SHAPE_SPHERE) return sphere_hit(o, lr, near, far, &t);
+    return cylinder_hit(o, lr, near, far, &t, &piece);
+  }
+
+  // TriangleMesh::intersect post-hit (triangle_mesh.rs:73-132, 219-258) with default uvs
+  void mesh_details(const Mesh& m, uint32_t tri, const Ray<R>& ray, const TriHit<R>& th, Isect<R>* h) const {
+    const uint32_t i0 = m.idx[3 * size_t(tri)], i1 = m.idx[3 * size_t(tri) + 1], i2 = m.idx[3 * size_t(tri) + 2];
+    const V3<R> p0{m.v[3 * size_t(i0)], m.v[3 * size_t(i0) + 1], m.v[3 * size_t(i0) + 2]};
+    const V3<R> p1{m.v[3 * size_t(i1)], m.v[3 * size_t(i1) + 1], m.v[3 * size_t(i1) + 2]};
+    const V3<R> p2{m.v[3 * size_t(i2)], m.v[3 * size_t(i2) + 1], m.v[3 * size_t(i2) + 2]};
+    h->p = ray.o + ray.d * th.t;
+    h->d = th.t;
+    const R uv0x = R(0), uv0y = R(0), uv1x = R(1), uv1y = R(0), uv2x = R(1), uv2y = R(1);
+    h->u = th.w * uv0x + th.u * uv1x + th.v * uv2x;
+    h->v = th.w * uv0y + th.u * uv1y + th.v * uv2y;
+    const R d02x = uv0x - uv2x, d02y = uv0y - uv2y, d12x = uv1x - uv2x, d12y = uv1y - uv2y;
+    const V3<R> dp02 = p0 - p2, dp12 = p1 - p2;
+    const R det = d12x * d02y - d12y * d02x;
+    if (std::fabs(det) < R(1e-8)) {
+      const V3<R> nn = cross(dp12, dp02);
+      const V3<R> tg = std::fabs(nn.x) < R(0.9) ? cross(V3<R>{R(1), R(0), R(0)}, nn) : cross(V3<R>{R(0), R(1), R(0)}, nn);
+      h->dpdu = tg;
+      h->dpdv = cross(nn, tg);
+    } else {
+      const R inv = R(1) / det;
+      h->dpdu = (dp12 * d02y - dp02 * d12y) * inv;
+      h->dpdv = (dp02 * d12x - dp12 * d02x) * inv;
+    }
+    h->n = normalized(cross(h->dpdv, h->dpdu));
+    h->wo = ray.d * R(-1);
+  }
+
+  // compute_intersection_details (sphere.rs:152-187)
+  void sphere_details(const Object& o, const Ray<R>& ray, R t, Isect<R>* h) const {
+    const R PI = Consts<R>::pi();
+    const V3<R> hit = ray.o + ray.d * t;
+    h->p = hit;
+    h->n = normalized(hit);
+    R phi = std::atan2(hit.y, hit.x);
+    if (phi < R(0)) phi += R(2) * PI;
+    h->u = phi / (R(2) * PI);
+    const R theta = std::acos(std::min(std::max(hit.z / o.radius, R(-1)), R(1)));
+    h->v = theta / PI;
+    const R zr = std::sqrt(hit.x * hit.x + hit.y * hit.y);
+    const R izr = R(1) / zr;
+    const R cphi = hit.x * izr, sphi = hit.y * izr;
+    h->dpdu = V3<R>{-hit.y, hit.x, R(0)} * (R(2) * PI);
+    h->dpdv = V3<R>{hit.z * cphi, hit.z * sphi, -o.radius * std::sin(theta)} * PI;
+    h->d = t;
+    h->wo = ray.d * R(-1);
+  }
+
+  // compute_cynlinder_intersection_details (cylinder.rs:324-344) and the caps (:266-300)
+  void cylinder_details(const Object& o, const Ray<R>& ray, R t, int piece, Isect<R>* h) const {
+    const R PI = Consts<R>::pi();
+    const V3<R> p = ray.o + ray.d * t;
+    h->p = p;
+    h->d = t;
+    h->wo = ray.d * R(-1);
+    if (piece == 0) {
+      h->n = normalized(V3<R>{p.x, R(0), p.z});
+      R phi = std::atan2(p.z, p.x);
+      if (phi < R(0)) phi += R(2) * PI;
+      h->u = phi / (R(2) * PI);
+      h->v = p.y;
+      h->dpdu = V3<R>{-p.z, R(0), p.x} * (R(2) * PI);
+      h->dpdv = V3<R>{R(0), R(1), R(0)};
+    } else {
+      const bool top = piece == 2;
+      h->n = V3<R>{R(0), top ? R(1) : R(-1), R(0)};
+      h->u = p.x;
+      h->v = p.z;
+      h->dpdu = V3<R>{top ? R(1) : R(-1), R(0), R(0)};
+      h->dpdv = V3<R>{R(0), R(0), R(1)};
+    }
+  }
+
+  // ---- scene BVH (src/bvh.rs:109-388) ---------------------------------------------------
+  void build_bvh() {
+    order.clear();
+    bnodes.clear();
+    boxes.clear();
+    for (uint32_t i = 0; i < objects.size(); ++i) boxes.push_back(object_box(objects[i]));
+    if (objects.empty()) return;
+    for (uint32_t i = 0; i < objects.size(); ++i) order.push_back(i);
+    bnodes.push_back(BNode{AABB<R>::empty(), 0, uint32_t(objects.size())});
+    subdivide(0);
+  }
+
+  AABB<R> subdivide(uint32_t ni) {
+    const uint32_t first = bnodes[ni].left_first, count = bnodes[ni].count;
+    if (count == 1) {
+      bnodes[ni].box = boxes[order[first]];
+      return bnodes[ni].box;
+    }
+    // widest_centroid_axis (bvh.rs:358-378)
+    R mn[3] = {Limits<R>::max(), Limits<R>::max(), Limits<R>::max()};
+    R mx[3] = {Limits<R>::lowest(), Limits<R>::lowest(), Limits<R>::lowest()};
+    for (uint32_t k = first; k < first + count; ++k) {
+      const V3<R> c = boxes[order[k]].centroid();
+      for (int a = 0; a < 3; ++a) { mn[a] = rmin(mn[a], c[a]); mx[a] = rmax(mx[a], c[a]); }
+    }
+    int axis = 0;
+    for (int a = 1; a < 3; ++a)
+      if (mx[a] - mn[a] > mx[axis] - mn[axis]) axis = a;
+    std::stable_sort(order.begin() + first, order.begin() + first + count,
+                     [&](uint32_t a, uint32_t b) { return boxes[a].centroid()[axis] < boxes[b].centroid()[axis]; });
+    const uint32_t lc = count / 2;
+    const uint32_t li = uint32_t(bnodes.size());
+    bnodes.push_back(BNode{AABB<R>::empty(), first, lc});
+    bnodes.push_back(BNode{AABB<R>::empty(), first + lc, count - lc});
+    bnodes[ni].left_first = li;
+    bnodes[ni].count = 0;
+    const AABB<R> lb = subdivide(li);
+    const AABB<R> rb = subdivide(li + 1);
+    AABB<R> u = AABB<R>::empty();
+    u.combine(lb);
+    u.combine(rb);
+    bnodes[ni].box = u;
+    return u;
+  }
+
+  // Scene::find_nearest + BVH::query (scene.rs:186-220, bvh.rs:153-230)
+  bool intersect(const Ray<R>& ray, R near, R far, Isect<R>* out, uint32_t* obj_out, uint32_t* prim_out) const {
+    if (bnodes.empty()) return false;
+    bool have = false;
+    Isect<R> nearest{};
+    R min_t = far;
+    R e;
+    if (!box_hit(bnodes[0].box, ray, near, min_t, &e)) return false;
+    struct Ent { uint32_t n; R e; };
+    std::vector<Ent> stack;
+    stack.reserve(64);
+    stack.push_back(Ent{0, e});
+    while (!stack.empty()) {
+      const Ent en = stack.back();
+      stack.pop_back();
+      if (en.e >= min_t) continue;
+      const BNode& nd = bnodes[en.n];
+      if (nd.count > 0) {
+        for (uint32_t k = nd.left_first; k < nd.left_first + nd.count; ++k) {
+          Isect<R> c;
+          uint32_t prim;
+          if (!intersect_object(order[k], ray, near, min_t, &c, &prim)) continue;
+          if (have && !(c.d < nearest.d)) continue;  // strictly nearer (scene.rs:206-210)
+          have = true;
+          nearest = c;
+          *obj_out = order[k];
+          *prim_out = prim;
+          min_t = c.d;
+        }
+      } else {
+        R dl = R(0), dr = R(0);
+        const bool hl = box_hit(bnodes[nd.left_first].box, ray, near, min_t, &dl);
+        const bool hr = box_hit(bnodes[nd.left_first + 1].box, ray, near, min_t, &dr);
+        uint32_t nn = nd.left_first, ff = nd.left_first + 1;
+        bool hn = hl, hf = hr;
+        R dn = dl, df = dr;
+        if (hl && hr && dr < dl) { nn = nd.left_first + 1; ff = nd.left_first; hn = hr; hf = hl; dn = dr; df = dl; }
+        if (hf) stack.push_back(Ent{ff, df});
+        if (hn) stack.push_back(Ent{nn, dn});
+      }
+    }
+    if (have) *out = nearest;
+    return have;
+  }
+
+  // Scene::any_hit + BVH::query_p (scene.rs:157-168, bvh.rs:239-275)
+  bool occluded(const Ray<R>& ray, R near, R far) const {
+    if (bnodes.empty()) return false;
+    std::vector<uint32_t> stack;
+    stack.reserve(64);
+    stack.push_back(0);
+    while (!stack.empty()) {
+      const BNode& nd = bnodes[stack.back()];
+      stack.pop_back();
+      R e;
+      if (!box_hit(nd.box, ray, near, far, &e)) continue;
+      if (nd.count > 0) {
+        for (uint32_t k = nd.left_first; k < nd.left_first + nd.count; ++k)
+          if (occluded_object(order[k], ray, near, far)) return true;
+      } else {
+        stack.push_back(nd.left_first + 1);
+        stack.push_back(nd.left_first);
+      }
+    }
+    return false;
+  }
+
+  // ---- lights -------------------------------------------------------------------------------
+  void setup_area(Light& L) {
+    if (L.object >= objects.size()) throw std::invalid_argument("area light object out of range");
+    const Object& o = objects[L.object];
+    if (o.shape == O_SHAPE_MESH) {
+      const Mesh& m = meshes[o.mesh];
+      const size_t nt = m.idx.size() / 3;
+      R run = R(0);
+      for (size_t t = 0; t < nt; ++t) {
+        V3<R> p[3];
+        for (int k = 0; k < 3; ++k) {
+          const uint32_t vi = m.idx[3 * t + k];
+          V3<R> v{m.v[3 * size_t(vi)], m.v[3 * size_t(vi) + 1], m.v[3 * size_t(vi) + 2]};
+          p[k] = o.transformed ? o.mat.point(v) : v;
+          L.tp.push_back(p[k]);
+        }
+        const R a = R(0.5) * length(cross(p[1] - p[0], p[2] - p[0]));
+        run = run + a;
+        L.cdf.push_back(run);
+      }
+      L.area = run;
+    } else if (o.shape == O_SHAPE_SPHERE) {
+      L.area = R(4) * Consts<R>::pi() * o.radius * o.radius;
+    } else {
+      throw std::invalid_argument("area lights are triangle meshes or spheres");
+    }
+  }
+
+  struct LiSample {
+    V3<R> spectrum, wi;
+    R pdf;
+    Ray<R> ray;
+    R dist;
+  };
+
+  // SpherePdf::generate (pdfs/sphere.rs:10-23)
+  static V3<R> sphere_dir(Pcg32& rng) {
+    const R two_pi = R(2) * Consts<R>::pi();
+    const R phi = two_pi * R(rng.uniform());
+    const R ct = R(1) - R(2) * R(rng.uniform());
+    const R st = std::sqrt(R(1) - ct * ct);
+    return V3<R>{std::cos(phi) * st, std::sin(phi) * st, ct};
+  }
+
+  V3<R> gradient(const Light& L, const V3<R>& dir) const {
+    const R f = R(0.5) * (dir.y + R(1));
+    return L.bottom * (R(1) - f) + L.top * f;
+  }
+
+  // Light::le for infinite lights (background_infinite_light.rs:33-37, uniform_infinite_light.rs:23-25)
+  V3<R> background(const V3<R>& dir) const {
+    V3<R> res{R(0), R(0), R(0)};
+    for (const Light& L : lights) {
+      if (L.kind == O_LIGHT_BACKGROUND) res = res + gradient(L, normalized(dir));
+      else if (L.kind == O_LIGHT_UNIFORM) res = res + L.rad;
+    }
+    return res;
+  }
+
+  bool sample_li(const Light& L, const Isect<R>& it, Pcg32& rng, LiSample* s) const {
+    if (L.kind == O_LIGHT_POINT) {  // point_light.rs:23-35
+      const V3<R> wi = L.pos - it.p;
+      const R sl = dot(wi, wi);
+      s->spectrum = V3<R>{L.rad.x / sl, L.rad.y / sl, L.rad.z / sl};
+      s->wi = normalized(wi);
+      s->pdf = R(1);
+      s->ray = spawn_from_through(it.p, L.pos);  // VisibilityTester::between (lights.rs:40-47)
+      s->dist = length(L.pos - it.p);
+      return true;
+    }
+    if (L.kind == O_LIGHT_BACKGROUND || L.kind == O_LIGHT_UNIFORM) {  // background_infinite_light.rs:39-51
+      const V3<R> wi = sphere_dir(rng);
+      s->pdf = R(1) / (R(4) * Consts<R>::pi());
+      s->spectrum = L.kind == O_LIGHT_BACKGROUND ? gradient(L, wi) : L.rad;
+      s->wi = wi;
+      s->ray = make_ray(it.p, wi);  // towards_infinity (lights.rs:55-60)
+      s->dist = Limits<R>::max();
+      return true;
+    }
+    // area light (ideas/area_light.md §3)
+    const Object& o = objects[L.object];
+    V3<R> pl, nl;
+    if (o.shape == O_SHAPE_MESH) {
+      const R u0 = R(rng.uniform()) * L.area;
+      size_t t = size_t(std::upper_bound(L.cdf.begin(), L.cdf.end(), u0) - L.cdf.begin());
+      if (t >= L.cdf.size()) t = L.cdf.size() - 1;
+      const R su = std::sqrt(R(rng.uniform()));
+      const R u2 = R(rng.uniform());
+      const R b0 = R(1) - su, b1 = u2 * su;
+      const V3<R> p0 = L.tp[3 * t], p1 = L.tp[3 * t + 1], p2 = L.tp[3 * t + 2];
+      pl = p0 * b0 + p1 * b1 + p2 * (R(1) - b0 - b1);
+      // the mesh's own normal convention: normalize(dpdv x dpdu) = normalize((p2-p1) x (p1-p0))
+      nl = normalized(cross(p2 - p1, p1 - p0));
+    } else {
+      const V3<R> dir = sphere_dir(rng);
+      const V3<R> lp = dir * o.radius;
+      pl = o.transformed ? o.mat.point(lp) : lp;
+      nl = o.transformed ? normalized(o.inv.normal(dir)) : dir;
+    }
+    const V3<R> w = pl - it.p;
+    const R d2 = dot(w, w);
+    const R dist = std::sqrt(d2);
+    const V3<R> wi = normalized(w);
+    const R cosl = std::fabs(dot(nl, wi));
+    const R pdf = (R(1) / L.area) * d2 / cosl;
+    if (!(pdf > R(0)) || !std::isfinite(pdf)) return false;
+    s->spectrum = materials[o.material].color;  // DiffuseLight emission, two-sided
+    s->wi = wi;
+    s->pdf = pdf;
+    s->ray = make_ray(it.p, wi);
+    s->dist = dist * (R(1) - R(1e-4));
+    return true;
+  }
+
+  // ---- materials ----------------------------------------------------------------------------
+  // Material::f (materials.rs:32-34, lambertian.rs:40-52)
+  V3<R> bsdf_f(const Material& m, const V3<R>& wo, const V3<R>& wi, const Isect<R>& it) const {
+    if (m.kind != O_MAT_LAMBERTIAN) return V3<R>{R(0), R(0), R(0)};
+    const V3<R> lwi = it.to_local(wi), lwo = it.to_local(wo);
+    if (lwo.z * lwi.z > R(0)) return V3<R>{m.color.x / Consts<R>::pi(), m.color.y / Consts<R>::pi(), m.color.z / Consts<R>::pi()};
+    return V3<R>{R(0), R(0), R(0)};
+  }
+
+  struct Scatter {
+    V3<R> att;
+    Ray<R> ray;
+    R pdf;
+  };
+
+  // random_in_unit_sphere (utils.rs:24-32); bounded at 64 draws (p(more) ≈ 1e-21)
+  static V3<R> in_unit_sphere(Pcg32& rng) {
+    V3<R> p{R(0), R(0), R(0)};
+    for (int k = 0; k < 64; ++k) {
+      const R x = R(rng.uniform()), y = R(rng.uniform()), z = R(rng.uniform());
+      p = V3<R>{x * R(2) - R(1), y * R(2) - R(1), z * R(2) - R(1)};
+      if (dot(p, p) < R(1)) return p;
+    }
+    return p * R(0.5);
+  }
+
+  bool scatter(const Material& m, const Isect<R>& it, Pcg32& rng, Scatter* s) const {
+    const R PI = Consts<R>::pi();
+    if (m.kind == O_MAT_LAMBERTIAN) {  // lambertian.rs:24-38, pdfs/cosine.rs:10-24
+      const R two_pi = R(2) * PI;
+      const R phi = two_pi * R(rng.uniform());
+      const R r2 = R(rng.uniform());
+      const R r2s = std::sqrt(r2);
+      const R ct = std::sqrt(R(1) - r2);
+      const V3<R> lwi{std::cos(phi) * r2s, std::sin(phi) * r2s, ct};
+      const V3<R> wi = it.to_world(lwi);
+      s->ray = make_ray(it.p + it.n * R(0.001), wi);
+      s->att = V3<R>{m.color.x / PI, m.color.y / PI, m.color.z / PI};
+      s->pdf = std::fabs(lwi.z / PI);
+      return true;
+    }
+    if (m.kind == O_MAT_METAL) {  // metal.rs:22-59
+      const V3<R> lwo = normalized(it.to_local(it.wo));
+      const V3<R> refl{-lwo.x, -lwo.y, lwo.z};
+      const V3<R> tgt = normalized(refl + in_unit_sphere(rng) * m.fuzz);
+      if (!(tgt.z > R(0))) return false;
+      const V3<R> w = it.to_world(tgt);
+      s->ray = make_ray(it.p + it.n * R(0.001), w);
+      const R ac = std::fabs(tgt.z);
+      s->att = V3<R>{m.color.x / ac, m.color.y / ac, m.color.z / ac};
+      s->pdf = R(1);
+      return true;
+    }
+    if (m.kind == O_MAT_DIELECTRIC) {  // dielectric.rs:32-182
+      const V3<R> lwo = normalized(it.to_local(it.wo));
+      const V3<R> refl{-lwo.x, -lwo.y, lwo.z};
+      V3<R> ln, wn;
+      R ni, nt;
+      if (lwo.z <= R(0)) { ln = V3<R>{R(0), R(0), R(-1)}; wn = it.n * R(-1); ni = m.ior; nt = R(1); }
+      else { ln = V3<R>{R(0), R(0), R(1)}; wn = it.n; ni = R(1); nt = m.ior; }
+      const R nint = ni / nt;
+      // refract (dielectric.rs:129-157)
+      const R ci = dot(lwo, ln);
+      const R s2i = R(1) - ci * ci;
+      const R s2t = nint * nint * s2i;
+      const R disc = R(1) - s2t;
+      V3<R> ldir;
+      V3<R> origin;
+      if (disc > R(0)) {
+        const R ctt = std::sqrt(disc);
+        const V3<R> wi = lwo * R(-1);
+        const V3<R> refr = normalized(wi * nint + ln * (nint * ci - ctt));
+        // fresnel (dielectric.rs:168-182)
+        const R n12 = ni / nt;
+        const R cti = lwo.z * ln.z;
+        const R ctf = std::sqrt(R(1) - n12 * n12 * (R(1) - cti * cti));
+        const R ro = (ni * cti - nt * ctf) / (ni * cti + nt * ctf);
+        const R rp = (nt * cti - ni * ctf) / (nt * cti + ni * ctf);
+        const R refl_p = (ro * ro + rp * rp) * R(0.5);
+        if (R(rng.uniform()) < refl_p) { ldir = refl; origin = it.p + wn * R(0.001); }
+        else { ldir = refr; origin = it.p + wn * R(-0.001); }
+      } else {
+        ldir = refl;
+        origin = it.p + wn * R(0.001);
+      }
+      s->ray = make_ray(origin, it.to_world(ldir));
+      const R ac = std::fabs(ldir.z);
+      s->att = V3<R>{m.color.x / ac, m.color.y / ac, m.color.z / ac};
+      s->pdf = R(1);
+      return true;
+    }
+    return false;  // DiffuseLight scatters nothing
+  }
+
+  // ---- integrators --------------------------------------------------------------------------
+  // PathIntegrator::li (path.rs:48-115) with area-light NEE and Russian roulette
+  V3<R> li_path(Ray<R> ray, R near, R far, uint32_t max_depth, uint32_t rr_start, Pcg32& rng) const {
+    V3<R> beta{R(1), R(1), R(1)}, L{R(0), R(0), R(0)};
+    bool specular = true;
+    uint32_t bounce = 0;
+    const R SHADOW_EPS = R(0.00001);
+    for (;;) {
+      Isect<R> it;
+      uint32_t obj, prim;
+      if (!intersect(ray, near, far, &it, &obj, &prim)) {
+        if (specular) {
+          const V3<R> bg = background(ray.d);
+          L = L + V3<R>{bg.x * beta.x, bg.y * beta.y, bg.z * beta.z};
+        }
+        break;
+      }
+      const Material& m = materials[objects[obj].material];
+      if (specular && m.kind == O_MAT_DIFFUSE_LIGHT)
+        L = L + V3<R>{m.color.x * beta.x, m.color.y * beta.y, m.color.z * beta.z};
+      bounce++;
+      if (bounce == max_depth) break;
+      if (!lights.empty()) {  // sample_light (path.rs:31-44)
+        const R cnt = R(lights.size());
+        const R pick = std::min(R(rng.uniform()) * cnt, cnt - R(1));
+        const uint32_t li = uint32_t(pick);
+        const R pl = R(1) / cnt;
+        LiSample s;
+        if (sample_li(lights[li], it, rng, &s)) {
+          const V3<R> f0 = bsdf_f(m, ray.d * R(-1), s.wi, it);
+          const R ac = std::fabs(dot(s.wi, it.n));
+          const V3<R> f{f0.x * ac, f0.y * ac, f0.z * ac};
+          if (f.x != R(0) || f.y != R(0) || f.z != R(0)) {  // zero contributions skip the shadow ray
+            if (!occluded(s.ray, SHADOW_EPS, s.dist)) {
+              const R den = pl * s.pdf;
+              const V3<R> c{((s.spectrum.x * f.x) * beta.x) / den, ((s.spectrum.y * f.y) * beta.y) / den,
+                            ((s.spectrum.z * f.z) * beta.z) / den};
+              L = L + c;
+            }
+          }
+        }
+      }
+      Scatter sc;
+      if (!scatter(m, it, rng, &sc)) break;
+      const R ac = std::fabs(dot(sc.ray.d, it.n));
+      const V3<R> k{(sc.att.x * ac) / sc.pdf, (sc.att.y * ac) / sc.pdf, (sc.att.z * ac) / sc.pdf};
+      beta = V3<R>{beta.x * k.x, beta.y * k.y, beta.z * k.z};
+      ray = sc.ray;
+      specular = m.kind == O_MAT_METAL || m.kind == O_MAT_DIELECTRIC;
+      if (rr_start && bounce >= rr_start) {
+        const R q = std::min(R(1), rmax(rmax(beta.x, beta.y), beta.z));
+        if (R(rng.uniform()) > q) break;
+        const R iq = R(1) / q;
+        beta = beta * iq;
+      }
+    }
+    return L;
+  }
+
+  // NaiveIntegrator::li (naive.rs:29-52), written as a loop, background = infinite lights
+  V3<R> li_naive(Ray<R> ray, R near, R far, uint32_t max_depth, Pcg32& rng) const {
+    V3<R> beta{R(1), R(1), R(1)}, L{R(0), R(0), R(0)};
+    for (uint32_t depth = max_depth; depth > 0; --depth) {
+      Isect<R> it;
+      uint32_t obj, prim;
+      if (!intersect(ray, near, far, &it, &obj, &prim)) {
+        const V3<R> bg = background(ray.d);
+        L = L + V3<R>{bg.x * beta.x, bg.y * beta.y, bg.z * beta.z};
+        break;
+      }
+      const Material& m = materials[objects[obj].material];
+      if (m.kind == O_MAT_DIFFUSE_LIGHT) L = L + V3<R>{m.color.x * beta.x, m.color.y * beta.y, m.color.z * beta.z};
+      Scatter sc;
+      if (!scatter(m, it, rng, &sc)) break;
+      const R ac = std::fabs(dot(sc.ray.d, it.n));
+      const V3<R> k{(sc.att.x * ac) / sc.pdf, (sc.att.y * ac) / sc.pdf, (sc.att.z * ac) / sc.pdf};
+      beta = V3<R>{beta.x * k.x, beta.y * k.y, beta.z * k.z};
+      ray = sc.ray;
+    }
+    return L;
+  }
+
+  std::vector<Mesh> meshes;
+  std::vector<Object> objects;
+  std::vector<Material> materials;
+  std::vector<Light> lights;
+  std::vector<AABB<R>> boxes;
+  std::vector<uint32_t> order;
+  std::vector<BNode> bnodes;
+};
+
+template <class R>
+PinHoleCamera<R> make_camera(const OCameraDesc& c) {
+  const V3<R> pos{R(c.position[0]), R(c.position[1]), R(c.position[2])};
+  const V3<R> look{R(c.look_at[0]), R(c.look_at[1]), R(c.look_at[2])};
+  const V3<R> up{R(c.up[0]), R(c.up[1]), R(c.up[2])};
+  return PinHoleCamera<R>(c.width, c.height, R(c.fov), R(c.near), R(c.far), M4<R>::look_at(pos, look, up));
+}
+
+}  // namespace oracle

@@ -61,6 +61,17 @@ class SceneInfo(C.Structure):
                 ("device_bytes", C.c_uint64)]
 
 
+class CameraDesc(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("fov", C.c_float), ("near", C.c_float),
+                ("far", C.c_float), ("position", C.c_float * 3), ("look_at", C.c_float * 3), ("up", C.c_float * 3)]
+
+
+class RenderParams(C.Structure):
+    _fields_ = [("camera", CameraDesc), ("spp", C.c_uint32), ("max_depth", C.c_uint32), ("rr_start", C.c_uint32),
+                ("sample_offset", C.c_uint32), ("seed", C.c_uint64), ("integrator", C.c_uint32),
+                ("flags", C.c_uint32)]
+
+
 # Every symbol the header declares, with its signature. tests/test_capi_symbols.py checks
 # the library exports each of them.
 SIGNATURES = {
@@ -79,6 +90,8 @@ SIGNATURES = {
                                                   C.c_void_p]),
     "pbrt_trace_any": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "pbrt_trace_closest_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
+    "pbrt_render": (C.c_int, [C.c_void_p, C.POINTER(RenderParams), C.c_void_p]),
+    "pbrt_film_to_rgba8": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
 }
 
 _lib = None

@@ -26,6 +26,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp
 # Per-file extra flags: the parity-critical kernels forbid FMA contraction outright.
 NVCC_EXTRA = {
     "kernels_trace.cu": ["-fmad=false"],
+    "kernels_render.cu": ["-fmad=false"],
     "api.cu": ["-fmad=false"],
 }
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall", "-I", CSRC, "-I", INCLUDE]

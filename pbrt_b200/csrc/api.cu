@@ -16,6 +16,9 @@
 #include "../../include/pbrt_b200.h"
 #include "kernels.hpp"
 #include "mesh_bvh.hpp"
+#include "render.hpp"
+#include "scene_device.cuh"
+#include "scene_host.hpp"
 #include "trace_mesh.cuh"
 
 using namespace pbrt;
@@ -102,8 +105,20 @@ struct DeviceMesh {
 struct pbrt_scene {
   pbrt_ctx* ctx = nullptr;
   std::vector<DeviceMesh> meshes;
+  std::vector<void*> allocs;  // every other device array of the scene
+  uint64_t extra_bytes = 0;
+  SceneView view{};
   pbrt_scene_info info{};
   int single_mesh = -1;  // index of the only (untransformed) mesh object, or -1
+
+  int upload(void** dst, const void* src, size_t bytes) {
+    if (bytes == 0) return PBRT_OK;
+    int rc = ctx->cuda(cudaMalloc(dst, bytes), "cudaMalloc(scene)");
+    if (rc != PBRT_OK) return rc;
+    allocs.push_back(*dst);
+    extra_bytes += bytes;
+    return ctx->cuda(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy(scene)");
+  }
 };
 
 #define PBRT_TRY(expr)              \
@@ -234,57 +249,82 @@ int pbrt_scene_create(pbrt_ctx* c, const pbrt_scene_desc* d, pbrt_scene** out) {
   if (d->object_count == 0) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "a scene needs at least one object");
   if (d->mesh_count && !d->meshes) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "meshes is NULL");
   if (!d->objects) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "objects is NULL");
-  MeshBuildParams bp;
-  bp.bins = d->bvh_bins ? int(d->bvh_bins) : 8;
-  bp.max_leaf = d->bvh_max_leaf ? d->bvh_max_leaf : 1;
+  FlatScene fs;
+  std::string e;
+  if (!build_scene(*d, &fs, &e)) return c->fail(PBRT_ERR_INVALID_ARGUMENT, e);
+  for (uint32_t i = 0; i < fs.meshes.size(); ++i)
+    if (fs.meshes[i].stats.max_depth >= uint32_t(kTraceStack))
+      return c->fail(PBRT_ERR_CAPACITY, "mesh " + std::to_string(i) + ": BVH depth " +
+                                             std::to_string(fs.meshes[i].stats.max_depth) +
+                                             " exceeds the traversal stack");
+  if (fs.top_depth >= uint32_t(kTraceStack))
+    return c->fail(PBRT_ERR_CAPACITY, "scene BVH depth exceeds the traversal stack");
 
   std::unique_ptr<pbrt_scene> s(new pbrt_scene);
   s->ctx = c;
-  for (uint32_t i = 0; i < d->object_count; ++i) {
-    const pbrt_object_desc& o = d->objects[i];
-    if (o.shape == PBRT_SHAPE_MESH && o.mesh >= d->mesh_count)
-      return c->fail(PBRT_ERR_INVALID_ARGUMENT, "object references a mesh that does not exist");
-  }
-  if (!(d->object_count == 1 && d->objects[0].shape == PBRT_SHAPE_MESH && !d->objects[0].transformed))
-    return c->fail(PBRT_ERR_UNSUPPORTED, "this build traces scenes made of one untransformed mesh");
-
-  s->meshes.resize(d->mesh_count);
-  for (uint32_t i = 0; i < d->mesh_count; ++i) {
-    const pbrt_mesh_desc& md = d->meshes[i];
-    FlatMesh fm;
-    std::string e;
-    if (!build_mesh_bvh(md.vertices, md.vertex_count, md.indices, md.triangle_count, bp, &fm, &e)) {
-      for (auto& m : s->meshes) free_mesh(m);
-      return c->fail(PBRT_ERR_INVALID_ARGUMENT, "mesh " + std::to_string(i) + ": " + e);
-    }
-    if (fm.stats.max_depth >= uint32_t(kTraceStack)) {
-      for (auto& m : s->meshes) free_mesh(m);
-      return c->fail(PBRT_ERR_CAPACITY, "mesh " + std::to_string(i) + ": BVH depth " +
-                                             std::to_string(fm.stats.max_depth) + " exceeds the traversal stack");
-    }
+  s->meshes.resize(fs.meshes.size());
+  std::vector<MeshView> views(fs.meshes.size());
+  std::vector<MeshShade> shades(fs.meshes.size());
+  int rc = PBRT_OK;
+  for (uint32_t i = 0; i < fs.meshes.size() && rc == PBRT_OK; ++i) {
+    const FlatMesh& fm = fs.meshes[i];
     DeviceMesh& dm = s->meshes[i];
-    int rc = upload(c, &dm.nodes, fm.nodes.data(), fm.nodes.size() * sizeof(GpuNode), &dm.bytes);
+    rc = upload(c, &dm.nodes, fm.nodes.data(), fm.nodes.size() * sizeof(GpuNode), &dm.bytes);
     if (rc == PBRT_OK) rc = upload(c, &dm.tri_a, fm.tri_a.data(), fm.tri_a.size() * sizeof(float), &dm.bytes);
     if (rc == PBRT_OK) rc = upload(c, &dm.tri_b, fm.tri_b.data(), fm.tri_b.size() * sizeof(float), &dm.bytes);
     if (rc == PBRT_OK) rc = upload(c, &dm.tri_c, fm.tri_c.data(), fm.tri_c.size() * sizeof(float), &dm.bytes);
-    if (rc != PBRT_OK) {
-      for (auto& m : s->meshes) free_mesh(m);
-      return rc;
-    }
+    if (rc != PBRT_OK) break;
     dm.view.nodes = (const float4*)dm.nodes;
     dm.view.tri_a = (const float4*)dm.tri_a;
     dm.view.tri_b = (const float4*)dm.tri_b;
     dm.view.tri_c = (const float2*)dm.tri_c;
     dm.view.node_count = uint32_t(fm.nodes.size());
-    s->info.triangle_count += md.triangle_count;
+    views[i] = dm.view;
+    void* pv = nullptr;
+    void* pi = nullptr;
+    rc = s->upload(&pv, fs.mesh_v[i].data(), fs.mesh_v[i].size() * sizeof(float));
+    if (rc == PBRT_OK) rc = s->upload(&pi, fs.mesh_idx[i].data(), fs.mesh_idx[i].size() * sizeof(uint32_t));
+    shades[i] = MeshShade{(const float*)pv, (const uint32_t*)pi};
+    s->info.triangle_count += fm.tri_index.size();
     s->info.mesh_node_count += fm.stats.node_count;
     s->info.mesh_leaf_count += fm.stats.leaf_count;
     s->info.mesh_max_depth = std::max(s->info.mesh_max_depth, fm.stats.max_depth);
     s->info.mesh_max_leaf_tris = std::max(s->info.mesh_max_leaf_tris, fm.stats.max_leaf_tris);
     s->info.device_bytes += dm.bytes;
   }
+  void *top = nullptr, *order = nullptr, *objs = nullptr, *mviews = nullptr, *mshades = nullptr, *mats = nullptr,
+       *lights = nullptr, *ltris = nullptr, *lcdf = nullptr;
+  if (rc == PBRT_OK) rc = s->upload(&top, fs.top.data(), fs.top.size() * sizeof(GpuNode));
+  if (rc == PBRT_OK) rc = s->upload(&order, fs.order.data(), fs.order.size() * sizeof(uint32_t));
+  if (rc == PBRT_OK) rc = s->upload(&objs, fs.objects.data(), fs.objects.size() * sizeof(ObjRec));
+  if (rc == PBRT_OK && !views.empty()) rc = s->upload(&mviews, views.data(), views.size() * sizeof(MeshView));
+  if (rc == PBRT_OK && !shades.empty()) rc = s->upload(&mshades, shades.data(), shades.size() * sizeof(MeshShade));
+  if (rc == PBRT_OK) rc = s->upload(&mats, fs.materials.data(), fs.materials.size() * sizeof(MatRec));
+  if (rc == PBRT_OK && !fs.lights.empty()) rc = s->upload(&lights, fs.lights.data(), fs.lights.size() * sizeof(LightRec));
+  if (rc == PBRT_OK && !fs.light_tris.empty())
+    rc = s->upload(&ltris, fs.light_tris.data(), fs.light_tris.size() * sizeof(float));
+  if (rc == PBRT_OK && !fs.light_cdf.empty())
+    rc = s->upload(&lcdf, fs.light_cdf.data(), fs.light_cdf.size() * sizeof(float));
+  if (rc != PBRT_OK) {
+    pbrt_scene_destroy(s.release());
+    return rc;
+  }
+  SceneView& v = s->view;
+  v.top = (const float4*)top;
+  v.top_node_count = uint32_t(fs.top.size());
+  v.order = (const uint32_t*)order;
+  v.objects = (const ObjRec*)objs;
+  v.meshes = (const MeshView*)mviews;
+  v.shade = (const MeshShade*)mshades;
+  v.materials = (const MatRec*)mats;
+  v.lights = (const LightRec*)lights;
+  v.light_count = uint32_t(fs.lights.size());
+  v.light_tris = (const float*)ltris;
+  v.light_cdf = (const float*)lcdf;
   s->info.object_count = d->object_count;
-  s->single_mesh = int(d->objects[0].mesh);
+  s->info.device_bytes += s->extra_bytes;
+  if (d->object_count == 1 && d->objects[0].shape == PBRT_SHAPE_MESH && !d->objects[0].transformed)
+    s->single_mesh = int(d->objects[0].mesh);
   *out = s.release();
   return PBRT_OK;
 }
@@ -294,6 +334,7 @@ void pbrt_scene_destroy(pbrt_scene* s) {
   DeviceGuard g(s->ctx->device);
   cudaStreamSynchronize(s->ctx->work_stream());
   for (auto& m : s->meshes) free_mesh(m);
+  for (void* p : s->allocs) cudaFree(p);
   delete s;
 }
 
@@ -333,7 +374,21 @@ int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, flo
   DeviceGuard g(c->device);
   if (n == 0) return PBRT_OK;
   if (!rays || (!occ && (!prim || !t))) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "ray or result buffer is NULL");
-  const MeshView& mv = s->meshes[s->single_mesh].view;
+  if (stats && s->single_mesh < 0)
+    return c->fail(PBRT_ERR_UNSUPPORTED, "work counters are reported for scenes made of one untransformed mesh");
+  const bool one_mesh = s->single_mesh >= 0;
+  const MeshView mv = one_mesh ? s->meshes[s->single_mesh].view : MeshView{};
+  // Nearest hit / any hit of one chunk of `m` rays (planes `stride` apart) on `st`.
+  auto launch = [&](const float* r, uint64_t stride, uint64_t m, uint32_t* p, float* tt, uint32_t* ob, uint8_t* oc,
+                    unsigned long long* cnt, uint32_t* queue, unsigned long long* qc, cudaStream_t st) -> cudaError_t {
+    if (!one_mesh)
+      return oc ? launch_scene_any(s->view, r, stride, m, oc, c->d_err, c->sm_count, st)
+                : launch_scene_closest(s->view, r, stride, m, p, tt, ob, c->d_err, c->sm_count, st);
+    if (oc) return launch_mesh_any(mv, r, stride, m, oc, c->d_err, c->sm_count, st);
+    if (c->persistent && !cnt)
+      return launch_mesh_closest_persistent(mv, r, stride, m, p, tt, ob, queue, qc, c->d_err, c->sm_count, st);
+    return launch_mesh_closest(mv, r, stride, m, p, tt, ob, cnt, c->d_err, c->sm_count, st);
+  };
 
   const MemKind kr = mem_kind(rays);
   const MemKind ko = occ ? mem_kind(occ) : mem_kind(prim);
@@ -350,21 +405,17 @@ int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, flo
 
   if (kr == MemKind::Device) {
     cudaStream_t st = c->work_stream();
-    if (occ) {
-      PBRT_TRY(c->cuda(launch_mesh_any(mv, rays, n, n, occ, c->d_err, c->sm_count, st), "kernel launch"));
-    } else if (c->persistent && !counters) {
+    if (one_mesh && !occ && c->persistent && !counters) {
       // Chunks of at most kDevChunk rays bound the survivor queue (scratch) to 64 MiB.
       PBRT_TRY(ensure_queue(c));
       for (uint64_t base = 0; base < n; base += kDevChunk) {
         const uint64_t m = std::min<uint64_t>(kDevChunk, n - base);
-        PBRT_TRY(c->cuda(launch_mesh_closest_persistent(mv, rays + base, n, m, prim + base, t + base,
-                                                        obj ? obj + base : nullptr, c->queue, c->d_counters + 4,
-                                                        c->d_err, c->sm_count, st),
+        PBRT_TRY(c->cuda(launch(rays + base, n, m, prim + base, t + base, obj ? obj + base : nullptr, nullptr, nullptr,
+                                c->queue, c->d_counters + 4, st),
                          "kernel launch"));
       }
     } else {
-      PBRT_TRY(c->cuda(launch_mesh_closest(mv, rays, n, n, prim, t, obj, counters, c->d_err, c->sm_count, st),
-                       "kernel launch"));
+      PBRT_TRY(c->cuda(launch(rays, n, n, prim, t, obj, occ, counters, nullptr, nullptr, st), "kernel launch"));
     }
     if (stats) {
       unsigned long long h[3];
@@ -392,16 +443,9 @@ int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, flo
       PBRT_TRY(c->cuda(cudaMemcpyAsync(sl.rays + p * kSlotRays, rays + p * n + base, m * sizeof(float),
                                        cudaMemcpyHostToDevice, sl.s),
                        "cudaMemcpyAsync(rays)"));
-    cudaError_t e;
-    if (occ)
-      e = launch_mesh_any(mv, sl.rays, kSlotRays, m, sl.occ, c->d_err, c->sm_count, sl.s);
-    else if (c->persistent && !counters)
-      e = launch_mesh_closest_persistent(mv, sl.rays, kSlotRays, m, sl.prim, sl.t, obj ? sl.obj : nullptr, sl.queue,
-                                         sl.fetch, c->d_err, c->sm_count, sl.s);
-    else
-      e = launch_mesh_closest(mv, sl.rays, kSlotRays, m, sl.prim, sl.t, obj ? sl.obj : nullptr, counters, c->d_err,
-                              c->sm_count, sl.s);
-    PBRT_TRY(c->cuda(e, "kernel launch"));
+    PBRT_TRY(c->cuda(launch(sl.rays, kSlotRays, m, sl.prim, sl.t, obj ? sl.obj : nullptr, occ ? sl.occ : nullptr,
+                            counters, sl.queue, sl.fetch, sl.s),
+                     "kernel launch"));
     if (occ) {
       PBRT_TRY(c->cuda(cudaMemcpyAsync(occ + base, sl.occ, m, cudaMemcpyDeviceToHost, sl.s), "cudaMemcpyAsync"));
     } else {
@@ -457,6 +501,8 @@ int pbrt_trace_closest_noalloc(pbrt_scene* s, const float* rays, uint64_t n, uin
       return c->fail(PBRT_ERR_INVALID_ARGUMENT,
                      "pbrt_trace_closest_noalloc takes device buffers only (host buffers need staging memory)");
   }
+  if (s->single_mesh < 0)
+    return c->fail(PBRT_ERR_UNSUPPORTED, "pbrt_trace_closest_noalloc traces scenes made of one untransformed mesh");
   const MeshView& mv = s->meshes[s->single_mesh].view;
   cudaStream_t st = c->work_stream();
   uint32_t* scratch = nullptr;
@@ -474,6 +520,119 @@ int pbrt_trace_closest_noalloc(pbrt_scene* s, const float* rays, uint64_t n, uin
 int pbrt_trace_any(pbrt_scene* s, const float* rays, uint64_t n, uint8_t* occluded) {
   if (!occluded) return s ? s->ctx->fail(PBRT_ERR_INVALID_ARGUMENT, "occluded is NULL") : PBRT_ERR_INVALID_ARGUMENT;
   return trace_impl(s, rays, n, nullptr, nullptr, nullptr, occluded, nullptr);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Rendering
+// ---------------------------------------------------------------------------------------
+namespace {
+
+constexpr uint32_t kWave = 1u << 22;  // paths in flight per wave (~128 B of state each)
+
+// The wave's SoA state, kept by the context and grown on demand.
+struct WaveAlloc {
+  void* block = nullptr;
+  uint32_t capacity = 0;
+  WaveBuffers w{};
+};
+
+int ensure_wave(pbrt_ctx* c, WaveAlloc* wa, uint32_t cap) {
+  if (wa->capacity >= cap) return PBRT_OK;
+  cudaFree(wa->block);
+  wa->block = nullptr;
+  wa->capacity = 0;
+  const size_t n = cap;
+  // 4-byte arrays: 6 ray + 3 beta + 3 L + pixel + flags + ht + hobj + hprim + qa + qb + 11 shadow
+  // = 31 words, plus the 8-byte rng state, plus 4 counters.
+  const size_t bytes = n * (31 * 4 + 8) + 64;
+  PBRT_TRY(c->cuda(cudaMalloc(&wa->block, bytes), "cudaMalloc(wave state)"));
+  char* p = static_cast<char*>(wa->block);
+  auto f32 = [&]() { float* r = reinterpret_cast<float*>(p); p += n * 4; return r; };
+  auto u32 = [&]() { uint32_t* r = reinterpret_cast<uint32_t*>(p); p += n * 4; return r; };
+  WaveBuffers& w = wa->w;
+  w.rng = reinterpret_cast<unsigned long long*>(p);
+  p += n * 8;
+  w.ox = f32(); w.oy = f32(); w.oz = f32(); w.dx = f32(); w.dy = f32(); w.dz = f32();
+  w.br = f32(); w.bg = f32(); w.bb = f32(); w.lr = f32(); w.lg = f32(); w.lb = f32();
+  w.pixel = u32(); w.flags = u32(); w.ht = f32(); w.hobj = u32(); w.hprim = u32(); w.qa = u32(); w.qb = u32();
+  w.s_path = u32(); w.s_ox = f32(); w.s_oy = f32(); w.s_oz = f32(); w.s_dx = f32(); w.s_dy = f32(); w.s_dz = f32();
+  w.s_tmax = f32(); w.s_cr = f32(); w.s_cg = f32(); w.s_cb = f32();
+  w.counts = reinterpret_cast<uint32_t*>(p);
+  wa->capacity = cap;
+  return PBRT_OK;
+}
+
+WaveAlloc g_waves[kMaxDevices];  // per device; a context serialises its own calls
+
+}  // namespace
+
+extern "C" {
+
+int pbrt_render(pbrt_scene* s, const pbrt_render_params* p, double* film) {
+  if (!s) return PBRT_ERR_INVALID_ARGUMENT;
+  pbrt_ctx* c = s->ctx;
+  DeviceGuard g(c->device);
+  if (!p || !film) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "params or film is NULL");
+  const pbrt_camera_desc& cd = p->camera;
+  if (cd.width == 0 || cd.height == 0) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "empty image");
+  if (p->spp == 0) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "spp must be >= 1");
+  if (p->max_depth == 0 || p->max_depth > 0xFFFF)
+    return c->fail(PBRT_ERR_INVALID_ARGUMENT, "max_depth must be in [1, 65535]");
+  if (p->integrator > PBRT_INTEGRATOR_NAIVE) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "unknown integrator");
+  if (!(cd.fov > 0.f) || !(cd.fov < 3.14159265f) || !(cd.far > cd.near))
+    return c->fail(PBRT_ERR_INVALID_ARGUMENT, "bad camera");
+  const uint64_t npix = uint64_t(cd.width) * cd.height;
+  if (npix > 0xFFFFFFFFull) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "image too large");
+  const uint64_t total = npix * p->spp;
+  const CameraRec cam = build_camera(cd);
+  RenderSettings rs;
+  rs.max_depth = p->max_depth;
+  rs.rr_start = p->integrator == PBRT_INTEGRATOR_NAIVE ? 0u : p->rr_start;
+  rs.sample_offset = p->sample_offset;
+  rs.naive = p->integrator == PBRT_INTEGRATOR_NAIVE ? 1u : 0u;
+  rs.seed = p->seed;
+
+  WaveAlloc& wa = g_waves[c->device];
+  const uint32_t wave = uint32_t(std::min<uint64_t>(total, kWave));
+  PBRT_TRY(ensure_wave(c, &wa, wave));
+  cudaStream_t st = c->work_stream();
+  const size_t film_n = size_t(npix) * 3;
+  double* dfilm = film;
+  const bool host_film = mem_kind(film) != MemKind::Device;
+  if (host_film) PBRT_TRY(c->cuda(cudaMalloc(&dfilm, film_n * sizeof(double)), "cudaMalloc(film)"));
+  int rc = c->cuda(cudaMemsetAsync(dfilm, 0, film_n * sizeof(double), st), "cudaMemset(film)");
+  for (uint64_t base = 0; base < total && rc == PBRT_OK; base += wave) {
+    const uint32_t n = uint32_t(std::min<uint64_t>(wave, total - base));
+    rc = c->cuda(render_wave(s->view, wa.w, cam, base, n, uint32_t(npix), rs, dfilm, c->d_err, c->sm_count, st),
+                 "render");
+  }
+  if (rc == PBRT_OK) rc = c->cuda(scale_film(dfilm, film_n, 1.0 / double(p->spp), c->sm_count, st), "render");
+  if (host_film) {
+    if (rc == PBRT_OK)
+      rc = c->cuda(cudaMemcpyAsync(film, dfilm, film_n * sizeof(double), cudaMemcpyDeviceToHost, st), "cudaMemcpy(film)");
+    if (rc == PBRT_OK) rc = check_device_error(c, st);
+    cudaStreamSynchronize(st);
+    cudaFree(dfilm);
+    return rc;
+  }
+  PBRT_TRY(rc);
+  if (c->user) return PBRT_OK;
+  return check_device_error(c, st);
+}
+
+int pbrt_film_to_rgba8(const double* film, uint32_t w, uint32_t h, uint8_t* rgba) {
+  if (!film || !rgba) return PBRT_ERR_INVALID_ARGUMENT;
+  for (size_t i = 0; i < size_t(w) * h; ++i) {
+    for (int ch = 0; ch < 3; ++ch) {
+      const double v = std::sqrt(film[3 * i + ch]);           // gamma_correct (spectrum.rs:19-23)
+      const double b = std::fmin(1.0, std::fmax(0.0, v));      // in_bound (spectrum.rs:134-136)
+      rgba[4 * i + ch] = uint8_t(b * 255.0);                   // `as u8` truncates (spectrum.rs:13-17)
+    }
+    rgba[4 * i + 3] = 255;
+  }
+  return PBRT_OK;
 }
 
 }  // extern "C"

@@ -1,0 +1,525 @@
+// kernels_render.cu — wavefront path tracing and general-scene ray casting.
+//
+// A wave of up to kWave paths lives in SoA buffers. Each bounce runs three kernels over
+// queues of path indices: extend (nearest hit), shade (emission, light sampling, BSDF
+// sampling, Russian roulette; pushes the surviving paths to the next queue and at most one
+// shadow ray per path to the shadow queue, both with one atomicAdd per warp) and shadow
+// (any hit; adds the light sample's contribution when unoccluded). Radiance is added to a
+// path in exactly the order PathIntegrator::li adds it (src/integrators/path.rs:55-113):
+// emission, then the light sample, then the next vertex's emission or the background. At
+// the end of a wave, accumulate adds every path's FP32 radiance into the FP64 film.
+#include <cfloat>
+#include <cstdint>
+#include <vector>
+
+#include "kernels.hpp"
+#include "render.hpp"
+#include "scene_device.cuh"
+
+namespace pbrt {
+
+constexpr float kPiF = 3.14159265358979323846f;
+constexpr float kShadowEps = 0.00001f;  // SHADOW_RAY_EPSILON (src/lights.rs:21)
+constexpr uint32_t kSpecularBit = 0x80000000u;
+
+// ---- sampler: PCG32, one stream per pixel, re-keyed per (pixel, sample) ------------------
+PBRT_DEV uint32_t pcg_next(unsigned long long& state, unsigned long long inc) {
+  const unsigned long long old = state;
+  state = old * 6364136223846793005ULL + inc;
+  const uint32_t xs = uint32_t(((old >> 18u) ^ old) >> 27u);
+  const uint32_t rot = uint32_t(old >> 59u);
+  return (xs >> rot) | (xs << ((32u - rot) & 31u));
+}
+PBRT_DEV float pcg_uniform(unsigned long long& state, unsigned long long inc) {
+  return float(pcg_next(state, inc) >> 8) * (1.0f / 16777216.0f);
+}
+PBRT_DEV unsigned long long splitmix64(unsigned long long x) {
+  x += 0x9E3779B97F4A7C15ULL;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+  return x ^ (x >> 31);
+}
+PBRT_DEV unsigned long long pcg_inc(uint32_t pixel) { return (((unsigned long long)pixel) << 1u) | 1u; }
+PBRT_DEV unsigned long long pcg_seed(unsigned long long seed, uint32_t pixel, uint32_t sample) {
+  const unsigned long long inc = pcg_inc(pixel);
+  unsigned long long state = 0;
+  pcg_next(state, inc);
+  state += splitmix64(seed ^ splitmix64((((unsigned long long)pixel) << 32u) | sample));
+  pcg_next(state, inc);
+  return state;
+}
+
+// ---- warp-aggregated queue push ----------------------------------------------------------
+PBRT_DEV uint32_t warp_push(uint32_t* count, bool want) {
+  const unsigned mask = __activemask();
+  const unsigned b = __ballot_sync(mask, want);
+  if (!want) return 0;
+  const int leader = __ffs(b) - 1;
+  const unsigned lane = threadIdx.x & 31u;
+  uint32_t base = 0;
+  if (int(lane) == leader) base = atomicAdd(count, uint32_t(__popc(b)));
+  base = __shfl_sync(b, base, leader);
+  return base + __popc(b & ((1u << lane) - 1u));
+}
+
+// ---- lights -----------------------------------------------------------------------------------
+PBRT_DEV F3 gradient(const LightRec& L, const F3& dir) {
+  const float f = fm(0.5f, fa(dir.y, 1.f));
+  const float g = fs(1.f, f);
+  return mk3(fa(fm(L.bottom[0], g), fm(L.top[0], f)), fa(fm(L.bottom[1], g), fm(L.top[1], f)),
+             fa(fm(L.bottom[2], g), fm(L.top[2], f)));
+}
+
+// Σ le over the infinite lights (path.rs:117-124)
+PBRT_DEV F3 background(const SceneView& s, const F3& dir) {
+  F3 res = mk3(0.f, 0.f, 0.f);
+  for (uint32_t i = 0; i < s.light_count; ++i) {
+    const LightRec& L = s.lights[i];
+    if (L.kind == kLightBackground) res = add3(res, gradient(L, normalize3(dir)));
+    else if (L.kind == kLightUniform) res = add3(res, mk3(L.rad[0], L.rad[1], L.rad[2]));
+  }
+  return res;
+}
+
+// SpherePdf::generate (pdfs/sphere.rs:10-23)
+PBRT_DEV F3 sphere_dir(unsigned long long& st, unsigned long long inc) {
+  const float two_pi = fm(2.f, kPiF);
+  const float phi = fm(two_pi, pcg_uniform(st, inc));
+  const float ct = fs(1.f, fm(2.f, pcg_uniform(st, inc)));
+  const float sn = fsq(fs(1.f, fm(ct, ct)));
+  return mk3(fm(cosf(phi), sn), fm(sinf(phi), sn), ct);
+}
+
+struct LiSample {
+  F3 spectrum, wi, ro, rd;
+  float pdf, dist;
+};
+
+PBRT_DEV bool sample_li(const SceneView& s, const LightRec& L, const Isect& it, unsigned long long& st,
+                        unsigned long long inc, LiSample& out) {
+  if (L.kind == kLightPoint) {  // point_light.rs:23-35, VisibilityTester::between (lights.rs:40-47)
+    const F3 pos = mk3(L.pos[0], L.pos[1], L.pos[2]);
+    const F3 wi = sub3(pos, it.p);
+    const float sl = dot3(wi, wi);
+    out.spectrum = mk3(fdv(L.rad[0], sl), fdv(L.rad[1], sl), fdv(L.rad[2], sl));
+    out.wi = normalize3(wi);
+    out.pdf = 1.f;
+    out.ro = it.p;
+    out.rd = normalize3(normalize3(sub3(pos, it.p)));
+    out.dist = length3(sub3(pos, it.p));
+    return true;
+  }
+  if (L.kind == kLightBackground || L.kind == kLightUniform) {  // towards_infinity (lights.rs:55-60)
+    const F3 wi = sphere_dir(st, inc);
+    out.pdf = fdv(1.f, fm(4.f, kPiF));
+    out.spectrum = L.kind == kLightBackground ? gradient(L, wi) : mk3(L.rad[0], L.rad[1], L.rad[2]);
+    out.wi = wi;
+    out.ro = it.p;
+    out.rd = normalize3(wi);
+    out.dist = FLT_MAX;
+    return true;
+  }
+  // area light: uniform on the emitter's area, p(ω) = p(A)·d²/|cos θ_l| (ideas/area_light.md §3)
+  const ObjRec& ob = s.objects[L.object];
+  F3 pl, nl;
+  if (ob.shape == kShapeMesh) {
+    const float u0 = fm(pcg_uniform(st, inc), L.area);
+    // first triangle whose running area exceeds u0 (upper_bound)
+    uint32_t lo = 0, hi = L.tri_count;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (s.light_cdf[L.tri_first + mid] <= u0) lo = mid + 1;
+      else hi = mid;
+    }
+    const uint32_t t = lo < L.tri_count ? lo : L.tri_count - 1;
+    const float su = fsq(pcg_uniform(st, inc));
+    const float u2 = pcg_uniform(st, inc);
+    const float b0 = fs(1.f, su), b1 = fm(u2, su);
+    const float* tp = s.light_tris + 9 * size_t(L.tri_first + t);
+    const F3 p0 = mk3(tp[0], tp[1], tp[2]), p1 = mk3(tp[3], tp[4], tp[5]), p2 = mk3(tp[6], tp[7], tp[8]);
+    pl = add3(add3(mul3(p0, b0), mul3(p1, b1)), mul3(p2, fs(fs(1.f, b0), b1)));
+    nl = normalize3(cross3(sub3(p2, p1), sub3(p1, p0)));
+  } else {
+    const F3 dir = sphere_dir(st, inc);
+    const F3 lp = mul3(dir, ob.radius);
+    pl = ob.transformed ? xf_point(ob.to_world, lp) : lp;
+    nl = ob.transformed ? normalize3(xf_normal(ob.to_local, dir)) : dir;
+  }
+  const F3 w = sub3(pl, it.p);
+  const float d2 = dot3(w, w);
+  const float dist = fsq(d2);
+  const F3 wi = normalize3(w);
+  const float cosl = fabsf(dot3(nl, wi));
+  const float pdf = fdv(fm(fdv(1.f, L.area), d2), cosl);
+  if (!(pdf > 0.f) || !isfinite(pdf)) return false;
+  const MatRec& m = s.materials[ob.material];
+  out.spectrum = mk3(m.color[0], m.color[1], m.color[2]);
+  out.wi = wi;
+  out.pdf = pdf;
+  out.ro = it.p;
+  out.rd = normalize3(wi);
+  out.dist = fm(dist, fs(1.f, 1e-4f));
+  return true;
+}
+
+// ---- materials --------------------------------------------------------------------------------
+// Material::f (materials.rs:32-34, lambertian.rs:40-52)
+PBRT_DEV F3 bsdf_f(const MatRec& m, const F3& wo, const F3& wi, const Isect& it) {
+  if (m.kind != kMatLambertian) return mk3(0.f, 0.f, 0.f);
+  const F3 lwi = to_local(it, wi), lwo = to_local(it, wo);
+  if (fm(lwo.z, lwi.z) > 0.f) return mk3(fdv(m.color[0], kPiF), fdv(m.color[1], kPiF), fdv(m.color[2], kPiF));
+  return mk3(0.f, 0.f, 0.f);
+}
+
+// random_in_unit_sphere (utils.rs:24-32), bounded at 64 draws
+PBRT_DEV F3 in_unit_sphere(unsigned long long& st, unsigned long long inc) {
+  F3 p = mk3(0.f, 0.f, 0.f);
+  for (int k = 0; k < 64; ++k) {
+    const float x = pcg_uniform(st, inc), y = pcg_uniform(st, inc), z = pcg_uniform(st, inc);
+    p = mk3(fs(fm(x, 2.f), 1.f), fs(fm(y, 2.f), 1.f), fs(fm(z, 2.f), 1.f));
+    if (dot3(p, p) < 1.f) return p;
+  }
+  return mul3(p, 0.5f);
+}
+
+struct ScatterOut {
+  F3 att, ro, rd;
+  float pdf;
+};
+
+PBRT_DEV bool scatter(const MatRec& m, const Isect& it, unsigned long long& st, unsigned long long inc, ScatterOut& s) {
+  const F3 col = mk3(m.color[0], m.color[1], m.color[2]);
+  if (m.kind == kMatLambertian) {  // lambertian.rs:24-38, pdfs/cosine.rs:10-24
+    const float two_pi = fm(2.f, kPiF);
+    const float phi = fm(two_pi, pcg_uniform(st, inc));
+    const float r2 = pcg_uniform(st, inc);
+    const float r2s = fsq(r2);
+    const float ct = fsq(fs(1.f, r2));
+    const F3 lwi = mk3(fm(cosf(phi), r2s), fm(sinf(phi), r2s), ct);
+    const F3 wi = to_world(it, lwi);
+    s.ro = add3(it.p, mul3(it.n, 0.001f));
+    s.rd = normalize3(wi);
+    s.att = mk3(fdv(col.x, kPiF), fdv(col.y, kPiF), fdv(col.z, kPiF));
+    s.pdf = fabsf(fdv(lwi.z, kPiF));
+    return true;
+  }
+  if (m.kind == kMatMetal) {  // metal.rs:22-59
+    const F3 lwo = normalize3(to_local(it, it.wo));
+    const F3 refl = mk3(-lwo.x, -lwo.y, lwo.z);
+    const F3 tgt = normalize3(add3(refl, mul3(in_unit_sphere(st, inc), m.fuzz)));
+    if (!(tgt.z > 0.f)) return false;
+    const F3 w = to_world(it, tgt);
+    s.ro = add3(it.p, mul3(it.n, 0.001f));
+    s.rd = normalize3(w);
+    const float ac = fabsf(tgt.z);
+    s.att = mk3(fdv(col.x, ac), fdv(col.y, ac), fdv(col.z, ac));
+    s.pdf = 1.f;
+    return true;
+  }
+  if (m.kind == kMatDielectric) {  // dielectric.rs:32-182
+    const F3 lwo = normalize3(to_local(it, it.wo));
+    const F3 refl = mk3(-lwo.x, -lwo.y, lwo.z);
+    F3 ln, wn;
+    float ni, nt;
+    if (lwo.z <= 0.f) { ln = mk3(0.f, 0.f, -1.f); wn = mul3(it.n, -1.f); ni = m.ior; nt = 1.f; }
+    else { ln = mk3(0.f, 0.f, 1.f); wn = it.n; ni = 1.f; nt = m.ior; }
+    const float nint = fdv(ni, nt);
+    const float ci = dot3(lwo, ln);
+    const float s2i = fs(1.f, fm(ci, ci));
+    const float s2t = fm(fm(nint, nint), s2i);
+    const float disc = fs(1.f, s2t);
+    F3 ldir, origin;
+    if (disc > 0.f) {
+      const float ctt = fsq(disc);
+      const F3 wi = mul3(lwo, -1.f);
+      const F3 refr = normalize3(add3(mul3(wi, nint), mul3(ln, fs(fm(nint, ci), ctt))));
+      const float n12 = fdv(ni, nt);
+      const float cti = fm(lwo.z, ln.z);
+      const float ctf = fsq(fs(1.f, fm(fm(n12, n12), fs(1.f, fm(cti, cti)))));
+      const float ro = fdv(fs(fm(ni, cti), fm(nt, ctf)), fa(fm(ni, cti), fm(nt, ctf)));
+      const float rp = fdv(fs(fm(nt, cti), fm(ni, ctf)), fa(fm(nt, cti), fm(ni, ctf)));
+      const float reflectance = fm(fa(fm(ro, ro), fm(rp, rp)), 0.5f);
+      if (pcg_uniform(st, inc) < reflectance) { ldir = refl; origin = add3(it.p, mul3(wn, 0.001f)); }
+      else { ldir = refr; origin = add3(it.p, mul3(wn, -0.001f)); }
+    } else {
+      ldir = refl;
+      origin = add3(it.p, mul3(wn, 0.001f));
+    }
+    s.ro = origin;
+    s.rd = normalize3(to_world(it, ldir));
+    const float ac = fabsf(ldir.z);
+    s.att = mk3(fdv(col.x, ac), fdv(col.y, ac), fdv(col.z, ac));
+    s.pdf = 1.f;
+    return true;
+  }
+  return false;
+}
+
+// ---- the camera ------------------------------------------------------------------------------
+// PinHoleCamera::get_ray (pin_hole.rs:42-50): raster -> screen through the inverse
+// perspective (w != 1 divides), normalise, camera -> world, Ray::new normalises again.
+PBRT_DEV void camera_ray(const CameraRec& c, float px, float py, F3& o, F3& d) {
+  const float* m = c.raster_to_screen;
+  F3 v = mk3(fa(fa(fa(fm(m[0], px), fm(m[1], py)), fm(m[2], 0.f)), m[3]),
+             fa(fa(fa(fm(m[4], px), fm(m[5], py)), fm(m[6], 0.f)), m[7]),
+             fa(fa(fa(fm(m[8], px), fm(m[9], py)), fm(m[10], 0.f)), m[11]));
+  const float w = fa(fa(fa(fm(m[12], px), fm(m[13], py)), fm(m[14], 0.f)), m[15]);
+  if (w != 1.f) v = mul3(v, frcp(w));
+  const F3 cv = normalize3(v);
+  o = xf_point(c.cam_to_world, mk3(0.f, 0.f, 0.f));
+  d = normalize3(xf_dir(c.cam_to_world, cv));
+}
+
+// ---- kernels ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_generate(WaveBuffers w, CameraRec cam, uint64_t wave_base, uint32_t n,
+                                                  uint32_t npix, uint32_t sample_offset, unsigned long long seed) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint64_t g = wave_base + i;
+    const uint32_t pixel = uint32_t(g % npix);
+    const uint32_t sample = sample_offset + uint32_t(g / npix);
+    const unsigned long long inc = pcg_inc(pixel);
+    unsigned long long st = pcg_seed(seed, pixel, sample);
+    const float jx = pcg_uniform(st, inc), jy = pcg_uniform(st, inc);  // Sampler2::sample (mt.rs:145-150)
+    F3 o, d;
+    camera_ray(cam, fa(float(pixel % cam.width), jx), fa(float(pixel / cam.width), jy), o, d);
+    w.ox[i] = o.x; w.oy[i] = o.y; w.oz[i] = o.z;
+    w.dx[i] = d.x; w.dy[i] = d.y; w.dz[i] = d.z;
+    w.br[i] = 1.f; w.bg[i] = 1.f; w.bb[i] = 1.f;
+    w.lr[i] = 0.f; w.lg[i] = 0.f; w.lb[i] = 0.f;
+    w.rng[i] = st;
+    w.pixel[i] = pixel;
+    w.flags[i] = kSpecularBit;  // is_last_bounce_specular starts true (path.rs:52)
+    w.qa[i] = i;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) w.counts[0] = n;
+}
+
+__global__ void __launch_bounds__(128) k_extend(WaveBuffers w, SceneView s, const uint32_t* __restrict__ q,
+                                                const uint32_t* __restrict__ qcount, float near, float far,
+                                                uint32_t* err) {
+  const uint32_t n = *qcount;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const uint32_t p = q[k];
+    const F3 o = mk3(w.ox[p], w.oy[p], w.oz[p]), d = mk3(w.dx[p], w.dy[p], w.dz[p]);
+    float t = 0.f;
+    uint32_t obj = 0xFFFFFFFFu, prim = 0;
+    if (!scene_closest(s, o, d, near, far, t, obj, prim, err)) obj = 0xFFFFFFFFu;
+    w.ht[p] = t;
+    w.hobj[p] = obj;
+    w.hprim[p] = prim;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_shade(WaveBuffers w, SceneView s, const uint32_t* __restrict__ q,
+                                               const uint32_t* __restrict__ qcount, uint32_t* __restrict__ qout,
+                                               uint32_t* __restrict__ qout_count, uint32_t max_depth, uint32_t rr_start,
+                                               uint32_t naive) {
+  const uint32_t n = *qcount;
+  // every lane runs the same trip count so the warp-aggregated pushes see full warps
+  const uint32_t stride = gridDim.x * blockDim.x;
+  const uint32_t iters = (n + stride - 1) / stride;
+  for (uint32_t it_ = 0; it_ < iters; ++it_) {
+    const uint32_t k = it_ * stride + blockIdx.x * blockDim.x + threadIdx.x;
+    bool push_path = false, push_shadow = false;
+    uint32_t p = 0;
+    F3 sro, srd, contrib;
+    float stmax = 0.f;
+    if (k < n) {
+      p = q[k];
+      F3 o = mk3(w.ox[p], w.oy[p], w.oz[p]), d = mk3(w.dx[p], w.dy[p], w.dz[p]);
+      F3 beta = mk3(w.br[p], w.bg[p], w.bb[p]);
+      F3 L = mk3(w.lr[p], w.lg[p], w.lb[p]);
+      unsigned long long st = w.rng[p];
+      const uint32_t pixel = w.pixel[p];
+      const unsigned long long inc = pcg_inc(pixel);
+      uint32_t flags = w.flags[p];
+      const bool spec = naive || (flags & kSpecularBit);
+      uint32_t bounce = flags & 0xFFFFu;
+      const uint32_t obj = w.hobj[p];
+      bool alive = false;
+      if (obj == 0xFFFFFFFFu) {
+        if (spec) {
+          const F3 bg = background(s, d);
+          L = add3(L, mk3(fm(bg.x, beta.x), fm(bg.y, beta.y), fm(bg.z, beta.z)));
+        }
+      } else {
+        const Isect it = interaction(s, obj, w.hprim[p], o, d, w.ht[p]);
+        const MatRec m = s.materials[s.objects[obj].material];
+        if (spec && m.kind == kMatDiffuseLight)
+          L = add3(L, mk3(fm(m.color[0], beta.x), fm(m.color[1], beta.y), fm(m.color[2], beta.z)));
+        bounce++;
+        // PathIntegrator stops at the max_depth-th hit, before sampling a light (path.rs:64-67);
+        // the naive estimator scatters at every hit and the host stops extending after
+        // max_depth hits (naive.rs:29-52: li(.., 0) is black).
+        const bool depth_cut = !naive && bounce == max_depth;
+        if (!depth_cut) {
+          if (!naive && s.light_count > 0) {  // sample_light (path.rs:31-44) and the light sample
+            const float cnt = float(s.light_count);
+            const float pick = fminf(fm(pcg_uniform(st, inc), cnt), fs(cnt, 1.f));
+            const uint32_t li = uint32_t(pick);
+            const float pl = fdv(1.f, cnt);
+            LiSample ls;
+            if (sample_li(s, s.lights[li], it, st, inc, ls)) {
+              const F3 f0 = bsdf_f(m, mul3(d, -1.f), ls.wi, it);
+              const float ac = fabsf(dot3(ls.wi, it.n));
+              const F3 f = mk3(fm(f0.x, ac), fm(f0.y, ac), fm(f0.z, ac));
+              if (f.x != 0.f || f.y != 0.f || f.z != 0.f) {
+                const float den = fm(pl, ls.pdf);
+                contrib = mk3(fdv(fm(fm(ls.spectrum.x, f.x), beta.x), den),
+                              fdv(fm(fm(ls.spectrum.y, f.y), beta.y), den),
+                              fdv(fm(fm(ls.spectrum.z, f.z), beta.z), den));
+                sro = ls.ro;
+                srd = ls.rd;
+                stmax = ls.dist;
+                push_shadow = true;
+              }
+            }
+          }
+          ScatterOut sc;
+          if (scatter(m, it, st, inc, sc)) {
+            const float ac = fabsf(dot3(sc.rd, it.n));
+            const F3 kk = mk3(fdv(fm(sc.att.x, ac), sc.pdf), fdv(fm(sc.att.y, ac), sc.pdf), fdv(fm(sc.att.z, ac), sc.pdf));
+            beta = mk3(fm(beta.x, kk.x), fm(beta.y, kk.y), fm(beta.z, kk.z));
+            o = sc.ro;
+            d = sc.rd;
+            const bool sp = m.kind == kMatMetal || m.kind == kMatDielectric;
+            alive = true;
+            if (rr_start && bounce >= rr_start) {  // Russian roulette (path.rs:92-101, q clamped to 1)
+              const float qq = fminf(1.f, fmaxf(fmaxf(beta.x, beta.y), beta.z));
+              if (pcg_uniform(st, inc) > qq) {
+                alive = false;
+              } else {
+                const float iq = frcp(qq);
+                beta = mul3(beta, iq);
+              }
+            }
+            flags = (sp ? kSpecularBit : 0u) | bounce;
+          }
+        }
+      }
+      w.lr[p] = L.x; w.lg[p] = L.y; w.lb[p] = L.z;
+      if (alive) {
+        w.ox[p] = o.x; w.oy[p] = o.y; w.oz[p] = o.z;
+        w.dx[p] = d.x; w.dy[p] = d.y; w.dz[p] = d.z;
+        w.br[p] = beta.x; w.bg[p] = beta.y; w.bb[p] = beta.z;
+        w.rng[p] = st;
+        w.flags[p] = flags;
+        push_path = true;
+      }
+    }
+    const uint32_t qi = warp_push(qout_count, push_path);
+    if (push_path) qout[qi] = p;
+    const uint32_t si = warp_push(w.counts + 2, push_shadow);
+    if (push_shadow) {
+      w.s_path[si] = p;
+      w.s_ox[si] = sro.x; w.s_oy[si] = sro.y; w.s_oz[si] = sro.z;
+      w.s_dx[si] = srd.x; w.s_dy[si] = srd.y; w.s_dz[si] = srd.z;
+      w.s_tmax[si] = stmax;
+      w.s_cr[si] = contrib.x; w.s_cg[si] = contrib.y; w.s_cb[si] = contrib.z;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) k_shadow(WaveBuffers w, SceneView s, uint32_t* err) {
+  const uint32_t n = w.counts[2];
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const F3 o = mk3(w.s_ox[k], w.s_oy[k], w.s_oz[k]), d = mk3(w.s_dx[k], w.s_dy[k], w.s_dz[k]);
+    if (!scene_any(s, o, d, kShadowEps, w.s_tmax[k], err)) {  // VisibilityTester::unoccluded (lights.rs:67-69)
+      const uint32_t p = w.s_path[k];
+      w.lr[p] = fa(w.lr[p], w.s_cr[k]);
+      w.lg[p] = fa(w.lg[p], w.s_cg[k]);
+      w.lb[p] = fa(w.lb[p], w.s_cb[k]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_accumulate(WaveBuffers w, uint32_t n, double* __restrict__ film) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t pix = w.pixel[i];
+    atomicAdd(film + 3 * size_t(pix), double(w.lr[i]));
+    atomicAdd(film + 3 * size_t(pix) + 1, double(w.lg[i]));
+    atomicAdd(film + 3 * size_t(pix) + 2, double(w.lb[i]));
+  }
+}
+
+__global__ void k_scale_film(double* film, size_t n, double s) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    film[i] *= s;
+}
+
+// ---- general-scene ray casting ---------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_scene_closest(SceneView s, const float* __restrict__ rays, uint64_t stride,
+                                                       uint64_t n, uint32_t* __restrict__ prim, float* __restrict__ tout,
+                                                       uint32_t* __restrict__ obj, uint32_t* err) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+    const F3 o = mk3(__ldcs(rays + i), __ldcs(rays + stride + i), __ldcs(rays + 2 * stride + i));
+    const F3 d = mk3(__ldcs(rays + 3 * stride + i), __ldcs(rays + 4 * stride + i), __ldcs(rays + 5 * stride + i));
+    const float near = __ldcs(rays + 6 * stride + i), far = __ldcs(rays + 7 * stride + i);
+    float t = 0.f;
+    uint32_t ob = 0, pr = 0;
+    const bool hit = scene_closest(s, o, d, near, far, t, ob, pr, err);
+    __stcs(prim + i, hit ? pr : 0xFFFFFFFFu);
+    __stcs(tout + i, hit ? t : __int_as_float(0x7f800000));
+    if (obj) __stcs(obj + i, hit ? ob : 0xFFFFFFFFu);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_scene_any(SceneView s, const float* __restrict__ rays, uint64_t stride,
+                                                   uint64_t n, uint8_t* __restrict__ occ, uint32_t* err) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+    const F3 o = mk3(__ldcs(rays + i), __ldcs(rays + stride + i), __ldcs(rays + 2 * stride + i));
+    const F3 d = mk3(__ldcs(rays + 3 * stride + i), __ldcs(rays + 4 * stride + i), __ldcs(rays + 5 * stride + i));
+    occ[i] = scene_any(s, o, d, __ldcs(rays + 6 * stride + i), __ldcs(rays + 7 * stride + i), err) ? 1 : 0;
+  }
+}
+
+// ---- launchers -------------------------------------------------------------------------------
+static unsigned grid_cap(uint64_t n, int threads, int sm_count, int per_sm) {
+  const uint64_t want = (n + threads - 1) / threads;
+  const uint64_t cap = uint64_t(sm_count) * per_sm;
+  return unsigned(want < cap ? (want ? want : 1) : cap);
+}
+
+cudaError_t launch_scene_closest(const SceneView& s, const float* rays, uint64_t stride, uint64_t n, uint32_t* prim,
+                                 float* t, uint32_t* obj, uint32_t* err, int sm_count, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  k_scene_closest<<<grid_cap(n, 128, sm_count, 32), 128, 0, st>>>(s, rays, stride, n, prim, t, obj, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scene_any(const SceneView& s, const float* rays, uint64_t stride, uint64_t n, uint8_t* occ,
+                             uint32_t* err, int sm_count, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  k_scene_any<<<grid_cap(n, 128, sm_count, 32), 128, 0, st>>>(s, rays, stride, n, occ, err);
+  return cudaGetLastError();
+}
+
+cudaError_t render_wave(const SceneView& s, const WaveBuffers& w, const CameraRec& cam, uint64_t wave_base,
+                        uint32_t n, uint32_t npix, const RenderSettings& rs, double* film, uint32_t* err, int sm_count,
+                        cudaStream_t st) {
+  cudaError_t e;
+  k_generate<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, cam, wave_base, n, npix, rs.sample_offset, rs.seed);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const unsigned g128 = unsigned(sm_count) * 16;
+  for (uint32_t b = 0; b < rs.max_depth; ++b) {
+    uint32_t* qin = (b & 1) ? w.qb : w.qa;
+    uint32_t* qout = (b & 1) ? w.qa : w.qb;
+    uint32_t* cin = w.counts + (b & 1);
+    uint32_t* cout = w.counts + ((b + 1) & 1);
+    if ((e = cudaMemsetAsync(cout, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(w.counts + 2, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+    k_extend<<<g128, 128, 0, st>>>(w, s, qin, cin, cam.near, cam.far, err);
+    k_shade<<<g128, 128, 0, st>>>(w, s, qin, cin, qout, cout, rs.max_depth, rs.rr_start, rs.naive);
+    if (!rs.naive) k_shadow<<<g128, 128, 0, st>>>(w, s, err);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  k_accumulate<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, n, film);
+  return cudaGetLastError();
+}
+
+cudaError_t scale_film(double* film, size_t n, double s, int sm_count, cudaStream_t st) {
+  k_scale_film<<<grid_cap(n, 256, sm_count, 8), 256, 0, st>>>(film, n, s);
+  return cudaGetLastError();
+}
+
+}  // namespace pbrt

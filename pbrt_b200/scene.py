@@ -8,10 +8,16 @@ Names and argument meanings follow the Rust crate:
   Transformed::new(object, transform)        src/objects/transformed.rs:15-20
   Transform::translation / rotation_*        src/geom/transform.rs:43-72
   Lambertian / Metal / Dielectric / DiffuseLight   src/materials/*.rs
+  PointLight / UniformInfiniteLight / BackgroundInfiniteLight   src/lights/*.rs
+  AreaLight — the reference's planned light (ideas/area_light.md), on an emissive object
   Scene::new / add_object / add_light / commit     src/scene.rs:80-115
   Scene::intersect / intersect_p (batched)         src/scene.rs:118-150
+  renderers::mt::render (mean radiance film)       src/renderers/mt.rs:23-130
 Errors the reference reports by panicking (an empty mesh, an index out of range) raise
 PbrtError here; "no hit" is PBRT_MISS in the returned id array, as `None` is in Rust.
+
+A scene lowers to a plain description dict (Scene.describe), the same one the CPU oracle
+consumes in the tests; Scene.from_description builds a scene from such a dict.
 """
 from __future__ import annotations
 
@@ -123,9 +129,13 @@ class Transform:
     def __mul__(self, o: "Transform") -> "Transform":  # transform.rs:119-127
         return Transform(self.mat @ o.mat, o.inv @ self.inv)
 
+    def rows(self):
+        """(to_world, to_local) as 12 FP32 values each (row-major 3x4)."""
+        return (self.mat[:3, :].astype(np.float32).reshape(-1), self.inv[:3, :].astype(np.float32).reshape(-1))
+
 
 # ------------------------------------------------------------------------------------------
-# Shapes, materials, objects
+# Shapes, materials, objects, lights
 # ------------------------------------------------------------------------------------------
 class TriangleMesh:
     def __init__(self, vertices, indices):
@@ -185,6 +195,44 @@ class Transformed:
     transform: Transform
 
 
+@dataclass
+class PointLight:
+    """PointLight::new(transform, i): a point at transform·(0,0,0) with intensity I."""
+    position: Sequence[float]
+    i: Sequence[float]
+
+
+@dataclass
+class UniformInfiniteLight:
+    i: Sequence[float]
+
+
+@dataclass
+class BackgroundInfiniteLight:
+    """Gradient f (downwards) → t (upwards) on the direction's y (background_infinite_light.rs)."""
+    f: Sequence[float]
+    t: Sequence[float]
+
+
+@dataclass
+class AreaLight:
+    """The emissive surface of an object already added to the scene (its material is a
+    DiffuseLight); sampled by area for next-event estimation (ideas/area_light.md)."""
+    object: object
+
+
+def _material_desc(m) -> dict:
+    if isinstance(m, Lambertian):
+        return dict(kind=_capi.MAT_LAMBERTIAN, color=tuple(m.albedo), fuzz=0.0, ior=1.0)
+    if isinstance(m, Metal):
+        return dict(kind=_capi.MAT_METAL, color=tuple(m.albedo), fuzz=float(m.fuzz), ior=1.0)
+    if isinstance(m, Dielectric):
+        return dict(kind=_capi.MAT_DIELECTRIC, color=tuple(m.albedo), fuzz=0.0, ior=float(m.ref_idx))
+    if isinstance(m, DiffuseLight):
+        return dict(kind=_capi.MAT_DIFFUSE_LIGHT, color=tuple(m.emitted), fuzz=0.0, ior=1.0)
+    raise TypeError(f"unknown material {m!r}")
+
+
 # ------------------------------------------------------------------------------------------
 # Buffers
 # ------------------------------------------------------------------------------------------
@@ -217,6 +265,16 @@ def _empty_like(ref, n: int, dtype: str):
     return np.empty(n, nd)
 
 
+def camera_desc(camera: dict) -> _capi.CameraDesc:
+    c = _capi.CameraDesc()
+    c.width, c.height = int(camera["width"]), int(camera["height"])
+    c.fov, c.near, c.far = float(camera["fov"]), float(camera["near"]), float(camera["far"])
+    c.position[:] = [float(x) for x in camera["position"]]
+    c.look_at[:] = [float(x) for x in camera["look_at"]]
+    c.up[:] = [float(x) for x in camera["up"]]
+    return c
+
+
 # ------------------------------------------------------------------------------------------
 # Scene
 # ------------------------------------------------------------------------------------------
@@ -228,7 +286,13 @@ class Scene:
         self.objects: List[object] = []
         self.lights: List[object] = []
         self.h = None
-        self._keep = []
+        self._desc = None
+
+    @classmethod
+    def from_description(cls, desc: dict, ctx: Optional[Context] = None) -> "Scene":
+        s = cls(ctx)
+        s._desc = desc
+        return s
 
     def add_object(self, obj) -> "Scene":
         self.objects.append(obj)
@@ -238,72 +302,104 @@ class Scene:
         self.lights.append(light)
         return self
 
-    def commit(self, bvh_bins: int = 8, bvh_max_leaf: int = 1) -> "Scene":
-        if self.ctx is None:
-            self.ctx = default_context()
-        self.release()
-        meshes, mesh_ids, materials, mat_ids, objs = [], {}, [], {}, []
-
-        def mat_index(m):
-            key = id(m)
-            if key not in mat_ids:
-                d = _capi.MaterialDesc()
-                if isinstance(m, Lambertian):
-                    d.kind, col = _capi.MAT_LAMBERTIAN, m.albedo
-                elif isinstance(m, Metal):
-                    d.kind, col, d.fuzz = _capi.MAT_METAL, m.albedo, m.fuzz
-                elif isinstance(m, Dielectric):
-                    d.kind, col, d.ior = _capi.MAT_DIELECTRIC, m.albedo, m.ref_idx
-                elif isinstance(m, DiffuseLight):
-                    d.kind, col = _capi.MAT_DIFFUSE_LIGHT, m.emitted
-                else:
-                    raise TypeError(f"unknown material {m!r}")
-                d.color[:] = [float(c) for c in col]
-                mat_ids[key] = len(materials)
-                materials.append(d)
-            return mat_ids[key]
-
+    def describe(self, bvh_bins: int = 8, bvh_max_leaf: int = 1) -> dict:
+        """The plain description dict of this scene (see the module docstring)."""
+        if self._desc is not None:
+            return self._desc
+        meshes, mesh_ids, materials, mat_ids, objs, obj_ids = [], {}, [], {}, [], {}
         for o in self.objects:
             xf = None
+            top = o
             if isinstance(o, Transformed):
                 xf, o = o.transform, o.object
             if not isinstance(o, Simple):
                 raise TypeError("objects are Simple or Transformed(Simple)")
-            d = _capi.ObjectDesc()
+            d = dict(shape=0, mesh=0, radius=0.0, height=0.0, material=0, to_world=None, to_local=None)
             shp = o.shape
             if isinstance(shp, TriangleMesh):
                 if id(shp) not in mesh_ids:
-                    md = _capi.MeshDesc(_ptr(shp.vertices), shp.vertices.shape[0], _ptr(shp.indices),
-                                        shp.indices.shape[0])
                     mesh_ids[id(shp)] = len(meshes)
-                    meshes.append(md)
-                    self._keep.append(shp)
-                d.shape, d.mesh = _capi.SHAPE_MESH, mesh_ids[id(shp)]
+                    meshes.append(dict(vertices=shp.vertices, indices=shp.indices))
+                d.update(shape=_capi.SHAPE_MESH, mesh=mesh_ids[id(shp)])
             elif isinstance(shp, Sphere):
-                d.shape, d.radius = _capi.SHAPE_SPHERE, shp.r
+                d.update(shape=_capi.SHAPE_SPHERE, radius=float(shp.r))
             elif isinstance(shp, Cylinder):
-                d.shape, d.radius, d.height = _capi.SHAPE_CYLINDER, shp.radius, shp.height
+                d.update(shape=_capi.SHAPE_CYLINDER, radius=float(shp.radius), height=float(shp.height))
             else:
                 raise TypeError(f"unknown shape {shp!r}")
-            d.material = mat_index(o.material)
+            if id(o.material) not in mat_ids:
+                mat_ids[id(o.material)] = len(materials)
+                materials.append(_material_desc(o.material))
+            d["material"] = mat_ids[id(o.material)]
             if xf is not None:
-                d.transformed = 1
-                d.to_world[:] = [float(x) for x in xf.mat[:3, :].reshape(-1)]
-                d.to_local[:] = [float(x) for x in xf.inv[:3, :].reshape(-1)]
+                d["to_world"], d["to_local"] = xf.rows()
+            obj_ids[id(top)] = len(objs)
             objs.append(d)
+        lights = []
+        for l in self.lights:
+            if isinstance(l, PointLight):
+                lights.append(dict(kind=_capi.LIGHT_POINT, position=tuple(l.position), radiance=tuple(l.i)))
+            elif isinstance(l, UniformInfiniteLight):
+                lights.append(dict(kind=_capi.LIGHT_UNIFORM_INFINITE, radiance=tuple(l.i)))
+            elif isinstance(l, BackgroundInfiniteLight):
+                lights.append(dict(kind=_capi.LIGHT_BACKGROUND_INFINITE, bottom=tuple(l.f), top=tuple(l.t)))
+            elif isinstance(l, AreaLight):
+                if id(l.object) not in obj_ids:
+                    raise PbrtError(1, "an AreaLight's object must be added to the scene")
+                lights.append(dict(kind=_capi.LIGHT_AREA, object=obj_ids[id(l.object)]))
+            else:
+                raise TypeError(f"unknown light {l!r}")
+        return dict(meshes=meshes, materials=materials, objects=objs, lights=lights, bvh_bins=bvh_bins,
+                    bvh_max_leaf=bvh_max_leaf)
 
-        desc = _capi.SceneDesc()
-        MA = _capi.MeshDesc * max(1, len(meshes))
-        TA = _capi.MaterialDesc * max(1, len(materials))
-        OA = _capi.ObjectDesc * max(1, len(objs))
-        self._arrays = (MA(*meshes), TA(*materials), OA(*objs))
-        desc.meshes, desc.mesh_count = C.cast(self._arrays[0], C.POINTER(_capi.MeshDesc)), len(meshes)
-        desc.materials, desc.material_count = C.cast(self._arrays[1], C.POINTER(_capi.MaterialDesc)), len(materials)
-        desc.objects, desc.object_count = C.cast(self._arrays[2], C.POINTER(_capi.ObjectDesc)), len(objs)
-        desc.lights, desc.light_count = None, 0
-        desc.bvh_bins, desc.bvh_max_leaf = bvh_bins, bvh_max_leaf
+    def commit(self, bvh_bins: int = 8, bvh_max_leaf: int = 1) -> "Scene":
+        if self.ctx is None:
+            self.ctx = default_context()
+        self.release()
+        desc = self.describe(bvh_bins, bvh_max_leaf)
+        keep = []
+        meshes = []
+        for m in desc["meshes"]:
+            v = np.ascontiguousarray(m["vertices"], np.float32).reshape(-1, 3)
+            i = np.ascontiguousarray(m["indices"], np.uint32).reshape(-1, 3)
+            keep += [v, i]
+            meshes.append(_capi.MeshDesc(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0]))
+        mats = []
+        for m in desc["materials"]:
+            d = _capi.MaterialDesc()
+            d.kind = int(m["kind"])
+            d.color[:] = [float(c) for c in m["color"]]
+            d.fuzz, d.ior = float(m.get("fuzz", 0.0)), float(m.get("ior", 1.0))
+            mats.append(d)
+        objs = []
+        for o in desc["objects"]:
+            d = _capi.ObjectDesc()
+            d.shape, d.mesh = int(o["shape"]), int(o.get("mesh", 0))
+            d.radius, d.height = float(o.get("radius", 0.0)), float(o.get("height", 0.0))
+            d.material = int(o["material"])
+            if o.get("to_world") is not None:
+                d.transformed = 1
+                d.to_world[:] = [float(x) for x in np.asarray(o["to_world"], np.float32).reshape(-1)[:12]]
+                d.to_local[:] = [float(x) for x in np.asarray(o["to_local"], np.float32).reshape(-1)[:12]]
+            objs.append(d)
+        lights = []
+        for l in desc["lights"]:
+            d = _capi.LightDesc()
+            d.kind = int(l["kind"])
+            for k in ("position", "radiance", "bottom", "top"):
+                getattr(d, k)[:] = [float(x) for x in l.get(k, (0.0, 0.0, 0.0))]
+            d.object = int(l.get("object", 0))
+            lights.append(d)
+        arrays = ((_capi.MeshDesc * max(1, len(meshes)))(*meshes), (_capi.MaterialDesc * max(1, len(mats)))(*mats),
+                  (_capi.ObjectDesc * max(1, len(objs)))(*objs), (_capi.LightDesc * max(1, len(lights)))(*lights))
+        sd = _capi.SceneDesc()
+        sd.meshes, sd.mesh_count = C.cast(arrays[0], C.POINTER(_capi.MeshDesc)), len(meshes)
+        sd.materials, sd.material_count = C.cast(arrays[1], C.POINTER(_capi.MaterialDesc)), len(mats)
+        sd.objects, sd.object_count = C.cast(arrays[2], C.POINTER(_capi.ObjectDesc)), len(objs)
+        sd.lights, sd.light_count = C.cast(arrays[3], C.POINTER(_capi.LightDesc)), len(lights)
+        sd.bvh_bins, sd.bvh_max_leaf = int(desc.get("bvh_bins", bvh_bins)), int(desc.get("bvh_max_leaf", bvh_max_leaf))
         h = C.c_void_p()
-        self.ctx.check(self.ctx.lib.pbrt_scene_create(self.ctx.h, C.byref(desc), C.byref(h)), "pbrt_scene_create")
+        self.ctx.check(self.ctx.lib.pbrt_scene_create(self.ctx.h, C.byref(sd), C.byref(h)), "pbrt_scene_create")
         self.h = h
         return self
 
@@ -345,6 +441,19 @@ class Scene:
         self.ctx.check(self.ctx.lib.pbrt_trace_any(self.h, _ptr(r), n, _ptr(occ)), "pbrt_trace_any")
         return occ
 
+    def render(self, camera: dict, spp: int, max_depth: int, seed: int = 1, rr_start: int = 0,
+               sample_offset: int = 0, integrator: str = "path", film=None):
+        """Mean radiance per pixel, (height, width, 3) float64; `film` may be a CUDA tensor."""
+        self._need()
+        p = _capi.RenderParams()
+        p.camera = camera_desc(camera)
+        p.spp, p.max_depth, p.rr_start, p.sample_offset = int(spp), int(max_depth), int(rr_start), int(sample_offset)
+        p.seed, p.integrator, p.flags = int(seed), 1 if integrator == "naive" else 0, 0
+        if film is None:
+            film = np.zeros((int(camera["height"]), int(camera["width"]), 3), np.float64)
+        self.ctx.check(self.ctx.lib.pbrt_render(self.h, C.byref(p), _ptr(film)), "pbrt_render")
+        return film
+
     def release(self):
         if self.h is not None and self.ctx is not None and self.ctx.h is not None:
             self.ctx.lib.pbrt_scene_destroy(self.h)
@@ -355,6 +464,17 @@ class Scene:
             self.release()
         except Exception:
             pass
+
+
+def film_to_rgba8(film: np.ndarray) -> np.ndarray:
+    """Spectrum::gamma_correct + to_rgb (src/spectrum.rs:13-25): (h, w, 4) uint8."""
+    f = np.ascontiguousarray(film, np.float64)
+    h, w = f.shape[0], f.shape[1]
+    out = np.zeros((h, w, 4), np.uint8)
+    rc = _capi.load().pbrt_film_to_rgba8(f.ctypes.data, w, h, out.ctypes.data)
+    if rc != 0:
+        raise PbrtError(rc, "pbrt_film_to_rgba8")
+    return out
 
 
 # ------------------------------------------------------------------------------------------

@@ -125,3 +125,134 @@ def raycast_workload(level: int = 7, n_rays: int = 1 << 24, seed: int = 1):
     v, f = displaced_icosphere(level, seed=seed)
     rays = incoherent_rays(n_rays, v.min(0), v.max(0), seed=seed + 1)
     return v, f, rays
+
+
+# ------------------------------------------------------------------------------------------
+# Path-tracing scenes, as plain description dicts (pbrt_b200.Scene.from_description) plus a
+# camera dict. Triangles are wound so that the reference's mesh normal
+# (p2−p1)×(p1−p0) faces the lit side (into the room, out of the boxes).
+# ------------------------------------------------------------------------------------------
+def _quad(p0, p1, p2, p3, normal):
+    p = [np.asarray(x, np.float64) for x in (p0, p1, p2, p3)]
+    tris = [[p[0], p[1], p[2]], [p[0], p[2], p[3]]]
+    out = []
+    for a, b, c in tris:
+        n = np.cross(c - b, b - a)
+        out.append([a, b, c] if np.dot(n, normal) > 0 else [c, b, a])
+    return out
+
+
+def _box(center, half, angle):
+    c, h = np.asarray(center, np.float64), np.asarray(half, np.float64)
+    s, co = np.sin(angle), np.cos(angle)
+    rot = np.array([[co, 0, s], [0, 1, 0], [-s, 0, co]])  # Matrix4::rotation_y (matrix4.rs:54-60)
+
+    def corner(sx, sy, sz):
+        return c + rot @ (h * np.array([sx, sy, sz], np.float64))
+
+    tris = []
+    for axis in range(3):
+        for sign in (-1, 1):
+            n = np.zeros(3)
+            n[axis] = sign
+            u, v = [a for a in range(3) if a != axis]
+            cs = []
+            for su, sv in ((-1, -1), (1, -1), (1, 1), (-1, 1)):
+                q = np.zeros(3)
+                q[axis], q[u], q[v] = sign, su, sv
+                cs.append(corner(*q))
+            tris += _quad(*cs, rot @ n)
+    return tris
+
+
+def _mesh(tris):
+    v = np.asarray(tris, np.float64).reshape(-1, 3).astype(np.float32)
+    return dict(vertices=v, indices=np.arange(v.shape[0], dtype=np.uint32).reshape(-1, 3))
+
+
+def cornell_box(width: int = 256, height: int = 256):
+    """Closed box of triangles: five Lambertian walls of a unit cube (grey 0.73, red left,
+    green right), two 12-triangle boxes rotated ±18° about y, a 0.25-wide quad light of 2
+    triangles at the ceiling centre emitting (17, 12, 4). No loader lights."""
+    L = 0.5
+    white = [*_quad((-L, -L, -L), (L, -L, -L), (L, -L, L), (-L, -L, L), (0, 1, 0)),   # floor
+             *_quad((-L, L, -L), (L, L, -L), (L, L, L), (-L, L, L), (0, -1, 0)),      # ceiling
+             *_quad((-L, -L, -L), (L, -L, -L), (L, L, -L), (-L, L, -L), (0, 0, 1)),   # back
+             *_box((0.17, -0.35, 0.10), (0.15, 0.15, 0.15), -np.pi / 10),            # short box, -18°
+             *_box((-0.17, -0.20, -0.15), (0.15, 0.30, 0.15), np.pi / 10)]           # tall box, +18°
+    red = _quad((-L, -L, -L), (-L, L, -L), (-L, L, L), (-L, -L, L), (1, 0, 0))
+    green = _quad((L, -L, -L), (L, L, -L), (L, L, L), (L, -L, L), (-1, 0, 0))
+    y, s = L - 1e-3, 0.125
+    light = _quad((-s, y, -s), (s, y, -s), (s, y, s), (-s, y, s), (0, -1, 0))
+    desc = dict(
+        meshes=[_mesh(white), _mesh(red), _mesh(green), _mesh(light)],
+        materials=[dict(kind=0, color=(0.73, 0.73, 0.73)), dict(kind=0, color=(0.65, 0.05, 0.05)),
+                   dict(kind=0, color=(0.12, 0.45, 0.15)), dict(kind=3, color=(17.0, 12.0, 4.0))],
+        objects=[dict(shape=0, mesh=k, material=k, to_world=None, to_local=None) for k in range(4)],
+        lights=[dict(kind=3, object=3)],
+        bvh_bins=8, bvh_max_leaf=1,
+    )
+    camera = dict(width=width, height=height, fov=np.deg2rad(40.0), near=1e-4, far=1000.0,
+                  position=(0.0, 0.0, 1.85), look_at=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0))
+    return desc, camera
+
+
+def _translation_rows(c):
+    tw = np.array([[1, 0, 0, c[0]], [0, 1, 0, c[1]], [0, 0, 1, c[2]]], np.float32).reshape(-1)
+    tl = np.array([[1, 0, 0, -c[0]], [0, 1, 0, -c[1]], [0, 0, 1, -c[2]]], np.float32).reshape(-1)
+    return tw, tl
+
+
+def many_spheres(n: int = 10_000, seed: int = 3, width: int = 1024, height: int = 768, extent: float = 10.0):
+    """n non-overlapping spheres, radius U[0.05, 0.3], centres U in a (2·extent)³ box, each a
+    Transformed(translation) of Simple(Sphere); materials in equal thirds: Lambertian
+    (albedo U[0.1, 0.9]³), metal (fuzz U[0, 0.3], albedo U[0.5, 0.95]³ — the metal albedo is
+    not specified, this is the choice), dielectric (IOR 1.5). Lights: the white → (0.5, 0.7,
+    1.0) sky gradient (BackgroundInfiniteLight) and one spherical area light."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    cell = 0.6
+    grid = {}
+    centres, radii = [], []
+    while len(centres) < n:
+        c = (rng.random(3) * 2.0 - 1.0) * extent
+        r = 0.05 + 0.25 * rng.random()
+        key = tuple(np.floor(c / cell).astype(int))
+        ok = True
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for j in grid.get((key[0] + dx, key[1] + dy, key[2] + dz), ()):
+                        if np.sum((centres[j] - c) ** 2) <= (radii[j] + r) ** 2:
+                            ok = False
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if not ok:
+                break
+        if ok:
+            grid.setdefault(key, []).append(len(centres))
+            centres.append(c)
+            radii.append(r)
+    materials, objects = [], []
+    for k, (c, r) in enumerate(zip(centres, radii)):
+        kind = k % 3
+        if kind == 0:
+            materials.append(dict(kind=0, color=tuple(0.1 + 0.8 * rng.random(3))))
+        elif kind == 1:
+            materials.append(dict(kind=1, color=tuple(0.5 + 0.45 * rng.random(3)), fuzz=0.3 * rng.random()))
+        else:
+            materials.append(dict(kind=2, color=(1.0, 1.0, 1.0), ior=1.5))
+        tw, tl = _translation_rows(c)
+        objects.append(dict(shape=1, radius=float(r), material=k, to_world=tw, to_local=tl))
+    materials.append(dict(kind=3, color=(8.0, 8.0, 8.0)))
+    tw, tl = _translation_rows((0.0, extent + 5.0, 0.0))
+    objects.append(dict(shape=1, radius=2.5, material=len(materials) - 1, to_world=tw, to_local=tl))
+    desc = dict(meshes=[], materials=materials, objects=objects,
+                lights=[dict(kind=2, bottom=(1.0, 1.0, 1.0), top=(0.5, 0.7, 1.0)),
+                        dict(kind=3, object=len(objects) - 1)],
+                bvh_bins=8, bvh_max_leaf=1)
+    camera = dict(width=width, height=height, fov=np.deg2rad(45.0), near=1e-4, far=1000.0,
+                  position=(0.0, 0.6 * extent, 3.2 * extent), look_at=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0))
+    return desc, camera
