@@ -251,6 +251,48 @@ typedef struct pbrt_render_params {
  * Replaces renderers::mt::render / st::render (src/renderers/mt.rs:23-110, 112-130). */
 int pbrt_render(pbrt_scene* scene, const pbrt_render_params* params, double* film_rgb);
 
+/* ---------------------------------------------------------------------------------- */
+/* Learned radiance cache (no counterpart in the reference: an extension of the path    */
+/* integrator, src/integrators/path.rs:48-115, that ends paths into a network)          */
+/* ---------------------------------------------------------------------------------- */
+
+typedef struct pbrt_cache pbrt_cache;
+
+/* Network: 82 features (12-band sin/cos encoding of the position normalised to the scene
+ * box, 72 values; outgoing direction, normal, albedo, roughness) -> 5 x 64 ReLU -> RGB, no
+ * biases, BF16 weights, FP32 accumulation on the tensor cores; relative-L2 loss; Adam. */
+#define PBRT_CACHE_PARAMS 23552u /* weights, row-major out x in per layer, last layer padded to 16 rows */
+#define PBRT_CACHE_RECORD 16u    /* floats per query record: p.xyz, roughness, wo.xyz, 0, n.xyz, 0, albedo.xyz, 0 */
+
+typedef struct pbrt_cache_params {
+  uint64_t seed;            /* weight initialisation */
+  float learning_rate;      /* Adam step size; 0 = 1e-2 */
+  float beta1, beta2;       /* 0 = 0.9, 0.99 */
+  float epsilon;            /* 0 = 1e-8 */
+  float scene_min[3], scene_max[3]; /* the box positions are normalised to */
+  uint32_t terminate_bounce; /* paths end into the cache at this hit; 0 = 2 */
+  uint32_t train_samples;    /* training samples per cached frame; 0 = 65536 */
+  uint32_t train_steps;      /* Adam steps per cached frame; 0 = 4 */
+} pbrt_cache_params;
+
+int pbrt_cache_create(pbrt_ctx* ctx, const pbrt_cache_params* params, pbrt_cache** out);
+void pbrt_cache_destroy(pbrt_cache* cache);
+/* Back to the seeded initial weights, zero Adam moments. */
+int pbrt_cache_reset(pbrt_cache* cache);
+int pbrt_cache_get_weights(pbrt_cache* cache, float* weights /* PBRT_CACHE_PARAMS */);
+int pbrt_cache_set_weights(pbrt_cache* cache, const float* weights);
+/* rgb[3*i..3*i+2] = network(record i); host or device buffers. */
+int pbrt_cache_query(pbrt_cache* cache, const float* records, uint64_t n, float* rgb);
+/* Gradient of the mean relative-L2 loss over a batch (grad: PBRT_CACHE_PARAMS floats); the
+ * loss is reported through *loss when not NULL. Weights are not changed. */
+int pbrt_cache_gradient(pbrt_cache* cache, const float* records, const float* targets, uint64_t n, float* grad,
+                        float* loss);
+/* One Adam step on a batch. */
+int pbrt_cache_train_step(pbrt_cache* cache, const float* records, const float* targets, uint64_t n, float* loss);
+/* Checkpoint of the weights and Adam state (pass buf = NULL to learn the size). */
+int pbrt_cache_save(pbrt_cache* cache, void* buf, uint64_t capacity, uint64_t* size);
+int pbrt_cache_load(pbrt_cache* cache, const void* buf, uint64_t size);
+
 /* Spectrum::gamma_correct + to_rgb (src/spectrum.rs:13-25, 134-136): sqrt gamma, clip to
  * [0, 1], truncate to 8 bits, alpha 255, as image_write stores it (mt.rs:152-167). Host
  * buffers; no GPU work. */

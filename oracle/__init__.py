@@ -379,3 +379,65 @@ def camera_rays(camera: dict, dtype=np.float32):
     c = _camera(camera)
     getattr(L, f"oracle_camera_rays_{'f64' if dt == np.float64 else 'f32'}")(C.byref(c), _ptr(out))
     return out
+
+
+# ------------------------------------------------------------------------------------------
+# The radiance cache's network (mlp_oracle.hpp)
+# ------------------------------------------------------------------------------------------
+MLP_PARAMS = 23552
+
+
+def _declare_mlp(L):
+    vp = C.c_void_p
+    L.oracle_mlp_forward.argtypes = [vp, vp, vp, C.c_size_t, vp, C.c_int, C.c_int]
+    L.oracle_mlp_gradient.argtypes = [vp, vp, vp, vp, C.c_size_t, vp, vp, C.c_int]
+    L.oracle_mlp_forward_f64.argtypes = [vp, vp, vp, C.c_size_t, vp]
+    L.oracle_mlp_adam.argtypes = [vp, vp, vp, vp, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float]
+
+
+def _mlp_lib():
+    L = lib()
+    if not getattr(L, "_mlp_declared", False):
+        _declare_mlp(L)
+        L._mlp_declared = True
+    return L
+
+
+def mlp_forward(weights, bounds, records, emulate=True, threads: int = os.cpu_count() or 1):
+    """Network outputs (n, 3); bounds = (min xyz, max xyz) of the position normalisation."""
+    w = np.ascontiguousarray(weights, np.float32)
+    b = np.ascontiguousarray(bounds, np.float32).reshape(6)
+    r = np.ascontiguousarray(records, np.float32).reshape(-1, 16)
+    out = np.zeros((r.shape[0], 3), np.float32)
+    _mlp_lib().oracle_mlp_forward(_ptr(w), _ptr(b), _ptr(r), r.shape[0], _ptr(out), int(emulate), threads)
+    return out
+
+
+def mlp_forward_f64(weights, bounds, records):
+    """Exact-mode network outputs (n, 3) in float64."""
+    w = np.ascontiguousarray(weights, np.float32)
+    b = np.ascontiguousarray(bounds, np.float32).reshape(6)
+    r = np.ascontiguousarray(records, np.float32).reshape(-1, 16)
+    out = np.zeros((r.shape[0], 3), np.float64)
+    _mlp_lib().oracle_mlp_forward_f64(_ptr(w), _ptr(b), _ptr(r), r.shape[0], _ptr(out))
+    return out
+
+
+def mlp_gradient(weights, bounds, records, targets, emulate=True):
+    """(gradient (23552,) float64, mean loss) of the relative-L2 loss over the batch."""
+    w = np.ascontiguousarray(weights, np.float32)
+    b = np.ascontiguousarray(bounds, np.float32).reshape(6)
+    r = np.ascontiguousarray(records, np.float32).reshape(-1, 16)
+    t = np.ascontiguousarray(targets, np.float32).reshape(-1, 3)
+    g = np.zeros(MLP_PARAMS, np.float64)
+    loss = np.zeros(1, np.float64)
+    _mlp_lib().oracle_mlp_gradient(_ptr(w), _ptr(b), _ptr(r), _ptr(t), r.shape[0], _ptr(g), _ptr(loss), int(emulate))
+    return g, float(loss[0])
+
+
+def mlp_adam(w, m, v, g, step, lr=1e-2, b1=0.9, b2=0.99, eps=1e-8):
+    """One Adam step in place on float32 arrays."""
+    for a in (w, m, v):
+        assert a.dtype == np.float32 and a.flags.c_contiguous
+    gg = np.ascontiguousarray(g, np.float32)
+    _mlp_lib().oracle_mlp_adam(_ptr(w), _ptr(m), _ptr(v), _ptr(gg), step, lr, b1, b2, eps)

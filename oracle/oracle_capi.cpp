@@ -406,3 +406,73 @@ ORACLE_SCENE_API(f64, double)
 ORACLE_SCENE_API(f32, float)
 
 }  // extern "C"
+
+// ---- the radiance cache's network (mlp_oracle.hpp) ----------------------------------------
+#include "mlp_oracle.hpp"
+
+extern "C" {
+
+static void mlp_bounds(const float* b6, float* lo, float* inv) {
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = b6[a];
+    const float ext = b6[3 + a] - b6[a];
+    inv[a] = ext > 0.f ? 1.0f / ext : 1.0f;
+  }
+}
+
+int oracle_mlp_forward(const float* weights, const float* bounds6, const float* records, size_t n, float* out,
+                       int emulate, int threads) {
+  const oracle::mlp::Net net(weights, emulate != 0);
+  float lo[3], inv[3];
+  mlp_bounds(bounds6, lo, inv);
+  parallel_for(n, threads, [&](size_t b, size_t e) {
+    for (size_t i = b; i < e; ++i) {
+      double f[oracle::mlp::kInPad], o[oracle::mlp::kOutPad];
+      std::vector<std::vector<double>> acts;
+      oracle::mlp::encode(records + i * oracle::mlp::kRecord, lo, inv, f);
+      net.forward(f, acts, o);
+      for (int c = 0; c < 3; ++c) out[3 * i + c] = float(o[c]);
+    }
+  });
+  return 0;
+}
+
+// Exact-mode (FP64) outputs, for finite-difference checks of the gradient.
+int oracle_mlp_forward_f64(const float* weights, const float* bounds6, const float* records, size_t n,
+                           double* out) {
+  const oracle::mlp::Net net(weights, false);
+  float lo[3], inv[3];
+  mlp_bounds(bounds6, lo, inv);
+  for (size_t i = 0; i < n; ++i) {
+    double f[oracle::mlp::kInPad], o[oracle::mlp::kOutPad];
+    std::vector<std::vector<double>> acts;
+    oracle::mlp::encode(records + i * oracle::mlp::kRecord, lo, inv, f);
+    net.forward(f, acts, o);
+    for (int c = 0; c < 3; ++c) out[3 * i + c] = o[c];
+  }
+  return 0;
+}
+
+int oracle_mlp_gradient(const float* weights, const float* bounds6, const float* records, const float* targets,
+                        size_t n, double* grad, double* loss, int emulate) {
+  const oracle::mlp::Net net(weights, emulate != 0);
+  float lo[3], inv[3];
+  mlp_bounds(bounds6, lo, inv);
+  for (int p = 0; p < oracle::mlp::kParams; ++p) grad[p] = 0.0;
+  const double scale = 1.0 / (double(n) * 3.0);
+  double l = 0.0;
+  for (size_t i = 0; i < n; ++i) {
+    double f[oracle::mlp::kInPad];
+    oracle::mlp::encode(records + i * oracle::mlp::kRecord, lo, inv, f);
+    l += net.backward(f, targets + 3 * i, scale, grad);
+  }
+  *loss = l * scale;
+  return 0;
+}
+
+void oracle_mlp_adam(float* w, float* m, float* v, const float* g, uint32_t step, float lr, float b1, float b2,
+                     float eps) {
+  oracle::mlp::adam(w, m, v, g, step, lr, b1, b2, eps);
+}
+
+}  // extern "C"

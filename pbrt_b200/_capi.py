@@ -72,6 +72,12 @@ class RenderParams(C.Structure):
                 ("flags", C.c_uint32)]
 
 
+class CacheParams(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("learning_rate", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
+                ("epsilon", C.c_float), ("scene_min", C.c_float * 3), ("scene_max", C.c_float * 3),
+                ("terminate_bounce", C.c_uint32), ("train_samples", C.c_uint32), ("train_steps", C.c_uint32)]
+
+
 # Every symbol the header declares, with its signature. tests/test_capi_symbols.py checks
 # the library exports each of them.
 SIGNATURES = {
@@ -91,6 +97,16 @@ SIGNATURES = {
     "pbrt_trace_any": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "pbrt_trace_closest_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     "pbrt_render": (C.c_int, [C.c_void_p, C.POINTER(RenderParams), C.c_void_p]),
+    "pbrt_cache_create": (C.c_int, [C.c_void_p, C.POINTER(CacheParams), C.POINTER(C.c_void_p)]),
+    "pbrt_cache_destroy": (None, [C.c_void_p]),
+    "pbrt_cache_reset": (C.c_int, [C.c_void_p]),
+    "pbrt_cache_get_weights": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "pbrt_cache_set_weights": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "pbrt_cache_query": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
+    "pbrt_cache_gradient": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
+    "pbrt_cache_train_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
+    "pbrt_cache_save": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "pbrt_cache_load": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "pbrt_film_to_rgba8": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
 }
 

@@ -1,0 +1,30 @@
+// cache.hpp — the radiance cache object behind the C ABI's pbrt_cache handle (host code).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/pbrt_b200.h"
+#include "mlp.hpp"
+
+struct pbrt_cache {
+  pbrt_ctx* ctx = nullptr;
+  pbrt_cache_params params{};
+  float *w = nullptr, *m = nullptr, *v = nullptr, *grad = nullptr, *loss = nullptr;
+  uint16_t *wfwd = nullptr, *wbwd = nullptr;
+  float *partials = nullptr, *tile_loss = nullptr;
+  uint32_t tile_cap = 0;
+  uint32_t step = 0;
+  std::vector<void*> train_bufs;  // the cached render's training-record buffers
+
+  int device_arrays();
+  int ensure_tiles(uint32_t tiles);
+  int reset();
+  pbrt::mlp::Bounds bounds() const;
+  int gradient_device(const float* records, const float* targets, uint64_t n, cudaStream_t s);
+  int adam_device(cudaStream_t s);
+  int query_device(const float* records, uint64_t n, float* rgb, cudaStream_t s);
+  void release();
+};

@@ -1,0 +1,137 @@
+// context.hpp — the library's internal state behind the C ABI's opaque handles (host
+// code only): the context with its streams, staging slots and error word, the scene with
+// its device arrays, and the helpers every entry point shares.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/pbrt_b200.h"
+#include "scene_device.cuh"
+#include "trace_mesh.cuh"
+
+namespace pbrt {
+namespace api {
+
+constexpr uint64_t kSlotRays = uint64_t(1) << 21;  // rays per pipelined chunk (64 MiB of rays)
+constexpr int kSlots = 3;
+constexpr uint64_t kDevChunk = uint64_t(1) << 24;  // rays per launch pair on device buffers
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+enum class MemKind { Host, Device, Null };
+
+inline MemKind mem_kind(const void* p) {
+  if (!p) return MemKind::Null;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return MemKind::Host;
+  }
+  if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return MemKind::Device;
+  return MemKind::Host;
+}
+
+struct Slot {
+  cudaStream_t s = nullptr;
+  float* rays = nullptr;     // 8 planes of kSlotRays
+  uint32_t* prim = nullptr;
+  float* t = nullptr;
+  uint32_t* obj = nullptr;
+  uint8_t* occ = nullptr;
+  uint32_t* queue = nullptr;            // survivor queue of the two-stage nearest-hit pass
+  unsigned long long* fetch = nullptr;  // [queue length, fetch position] of that pass
+};
+
+}  // namespace api
+}  // namespace pbrt
+
+struct pbrt_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;  // internal stream
+  cudaStream_t user = nullptr;    // caller's stream (asynchronous device-buffer calls)
+  std::string err;
+  uint32_t* d_err = nullptr;
+  unsigned long long* d_counters = nullptr;  // [0..2] traversal counters, [4..5] queue length / fetch position
+  uint32_t* queue = nullptr;                  // survivor queue for device-buffer calls (kDevChunk entries)
+  bool persistent = true;                     // persistent dynamic-fetch traversal (default)
+  pbrt::api::Slot slots[pbrt::api::kSlots];
+  bool slots_ready = false;
+  std::vector<void*> allocs;
+
+  int fail(int code, const std::string& msg) {
+    err = msg;
+    return code;
+  }
+  int cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return PBRT_OK;
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? PBRT_ERR_OUT_OF_MEMORY : PBRT_ERR_CUDA;
+  }
+  cudaStream_t work_stream() const { return user ? user : stream; }
+};
+
+struct DeviceMesh {
+  void* nodes = nullptr;
+  void* tri_a = nullptr;
+  void* tri_b = nullptr;
+  void* tri_c = nullptr;
+  pbrt::MeshView view{};
+  uint64_t bytes = 0;
+};
+
+struct pbrt_scene {
+  pbrt_ctx* ctx = nullptr;
+  std::vector<DeviceMesh> meshes;
+  std::vector<void*> allocs;  // every other device array of the scene
+  uint64_t extra_bytes = 0;
+  pbrt::SceneView view{};
+  pbrt_scene_info info{};
+  int single_mesh = -1;  // index of the only (untransformed) mesh object, or -1
+
+  int upload(void** dst, const void* src, size_t bytes) {
+    if (bytes == 0) return PBRT_OK;
+    int rc = ctx->cuda(cudaMalloc(dst, bytes), "cudaMalloc(scene)");
+    if (rc != PBRT_OK) return rc;
+    allocs.push_back(*dst);
+    extra_bytes += bytes;
+    return ctx->cuda(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy(scene)");
+  }
+};
+
+#define PBRT_TRY(expr)              \
+  do {                              \
+    int _rc = (expr);               \
+    if (_rc != PBRT_OK) return _rc; \
+  } while (0)
+
+namespace pbrt {
+namespace api {
+
+// Reads and clears the device error word after the work that may have raised it.
+inline int check_device_error(pbrt_ctx* c, cudaStream_t s) {
+  PBRT_TRY(c->cuda(cudaStreamSynchronize(s), "kernel execution"));
+  uint32_t h = 0;
+  PBRT_TRY(c->cuda(cudaMemcpy(&h, c->d_err, sizeof(h), cudaMemcpyDeviceToHost), "cudaMemcpy(error word)"));
+  if (h == 0) return PBRT_OK;
+  PBRT_TRY(c->cuda(cudaMemset(c->d_err, 0, sizeof(uint32_t)), "cudaMemset(error word)"));
+  if (h & kErrStack) return c->fail(PBRT_ERR_CAPACITY, "traversal stack capacity exceeded");
+  return c->fail(PBRT_ERR_DEVICE_BUDGET, "a traversal exceeded its iteration budget (malformed tree)");
+}
+
+}  // namespace api
+}  // namespace pbrt

@@ -1,0 +1,423 @@
+// mlp.cu — forward (inference), per-tile backward, gradient reduction and Adam for the
+// radiance cache's network; see mlp.hpp for the network and tcgen05.cuh for the layouts.
+//
+// One CTA of 128 threads owns a tile of 128 samples: thread r encodes sample r into row r of
+// the BF16 input tile in shared memory; for every layer, thread 0 issues the tcgen05.mma
+// chain (M = 128, N = 64 or 16, K = 96 or 64 in steps of 16) into a TMEM accumulator of 64
+// FP32 columns and commits it to an mbarrier; every thread then reads its own accumulator
+// row (TMEM lane = sample), applies ReLU and writes the BF16 activations back to shared
+// memory as the next layer's A operand. The weights of all six layers (47 KB of BF16) stay
+// resident in shared memory for the CTA's lifetime.
+//
+// Training: the same forward keeps every layer's activations; the loss gradient dO is
+// written as a BF16 tile; for each layer the data gradient dA = G·W runs on the tensor cores
+// (W transposed in its own pack) while the weight gradient dW = Gᵀ·A runs on the CUDA
+// cores from the same shared-memory tiles; per-tile partial gradients are reduced by a
+// second kernel and Adam updates the FP32 master weights and rewrites both BF16 packs.
+#include <cuda_bf16.h>
+
+#include <cstdint>
+
+#include "mlp.hpp"
+#include "tcgen05.cuh"
+
+namespace pbrt {
+namespace mlp {
+
+constexpr uint32_t kErrMma = 4u;  // a tensor-core completion wait ran out of its budget
+constexpr uint32_t kWBytes = kParams * 2;           // 47,104
+constexpr uint32_t kXBytes = kTile * kInPad * 2;    // 24,576
+constexpr uint32_t kHBytes = kTile * kHidden * 2;   // 16,384
+constexpr uint32_t kG16Bytes = kTile * kOutPad * 2;  // 4,096
+constexpr uint32_t kTmemCols = 64;
+
+__device__ __forceinline__ uint16_t to_bf16(float f) { return __bfloat16_as_ushort(__float2bfloat16_rn(f)); }
+__device__ __forceinline__ float from_bf16(uint16_t b) { return __uint_as_float(uint32_t(b) << 16); }
+__device__ __forceinline__ uint32_t pack2(float a, float b) {
+  return uint32_t(to_bf16(a)) | (uint32_t(to_bf16(b)) << 16);
+}
+
+// Encodes one query record into 96 features (82 used, zero padded).
+__device__ void encode(const float* __restrict__ rec, const Bounds& b, float* f) {
+  const float4 q0 = __ldg(reinterpret_cast<const float4*>(rec));
+  const float4 q1 = __ldg(reinterpret_cast<const float4*>(rec) + 1);
+  const float4 q2 = __ldg(reinterpret_cast<const float4*>(rec) + 2);
+  const float4 q3 = __ldg(reinterpret_cast<const float4*>(rec) + 3);
+  const float p[3] = {q0.x, q0.y, q0.z};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float x = (p[a] - b.lo[a]) * b.inv_extent[a];
+#pragma unroll
+    for (int j = 0; j < 12; ++j) {
+      float s, c;
+      sincospif(x, &s, &c);
+      f[a * 24 + 2 * j] = s;
+      f[a * 24 + 2 * j + 1] = c;
+      x = x * 2.0f;
+    }
+  }
+  f[72] = q1.x; f[73] = q1.y; f[74] = q1.z;
+  f[75] = q2.x; f[76] = q2.y; f[77] = q2.z;
+  f[78] = q3.x; f[79] = q3.y; f[80] = q3.z;
+  f[81] = q0.w;
+#pragma unroll
+  for (int k = kIn; k < kInPad; ++k) f[k] = 0.f;
+}
+
+// Writes `n` (multiple of 8) values of row r into an R=128-row tile as BF16.
+__device__ __forceinline__ void store_row(uint8_t* tile, uint32_t r, const float* v, int n) {
+  for (int c = 0; c < n; c += 8) {
+    uint4 q;
+    q.x = pack2(v[c], v[c + 1]);
+    q.y = pack2(v[c + 2], v[c + 3]);
+    q.z = pack2(v[c + 4], v[c + 5]);
+    q.w = pack2(v[c + 6], v[c + 7]);
+    *reinterpret_cast<uint4*>(tile + tc::tile_offset(r, uint32_t(c), kTile)) = q;
+  }
+}
+
+__device__ __forceinline__ float tile_at(const uint8_t* tile, uint32_t r, uint32_t k, uint32_t rows) {
+  return from_bf16(*reinterpret_cast<const uint16_t*>(tile + tc::tile_offset(r, k, rows)));
+}
+
+// D[128 x n] = A[128 x k] · B[n x k]^T, both K-major in the core-matrix layout; thread 0 only.
+__device__ __forceinline__ void issue_gemm(const uint8_t* a, const uint8_t* b, uint32_t n, uint32_t k, uint32_t tmem,
+                                           uint64_t* mbar) {
+  const uint32_t a_addr = tc::smem_u32(a), b_addr = tc::smem_u32(b);
+  const uint32_t lbo_a = (kTile / 8) * 128, lbo_b = (n / 8) * 128;
+  const uint32_t idesc = tc::idesc_bf16(kTile, n);
+  for (uint32_t s = 0; s < k / 16; ++s)
+    tc::mma_bf16(tmem, tc::make_desc(a_addr + s * 2 * lbo_a, lbo_a, 128), tc::make_desc(b_addr + s * 2 * lbo_b, lbo_b, 128),
+                 idesc, s > 0 ? 1u : 0u);
+  tc::mma_commit(mbar);
+}
+
+// All threads: waits for the committed GEMM; false (and the error bit) if it never completes.
+__device__ __forceinline__ bool wait_gemm(uint64_t* mbar, uint32_t& phase, uint32_t* err) {
+  bool ok = tc::mbar_wait(mbar, phase);
+  ok = __syncthreads_and(ok);
+  if (!ok && threadIdx.x == 0) atomicOr(err, kErrMma);
+  phase ^= 1u;
+  tc::fence_after_sync();
+  return ok;
+}
+
+// This thread's 64 accumulator columns (its TMEM lane is its row).
+__device__ __forceinline__ void read_acc64(uint32_t tmem, float* v) {
+  const uint32_t lane = (threadIdx.x >> 5) * 32u;
+#pragma unroll
+  for (int c = 0; c < 64; c += 16) tc::tmem_ld16(tmem + (lane << 16) + uint32_t(c), v + c);
+}
+
+__device__ __forceinline__ void load_smem(uint8_t* dst, const uint16_t* src, uint32_t bytes) {
+  const uint4* s = reinterpret_cast<const uint4*>(src);
+  uint4* d = reinterpret_cast<uint4*>(dst);
+  for (uint32_t i = threadIdx.x; i < bytes / 16; i += blockDim.x) d[i] = __ldg(s + i);
+}
+
+__device__ __forceinline__ void setup_tmem(uint64_t* mbar, uint32_t* tslot) {
+  if (threadIdx.x == 0) tc::mbar_init(mbar, 1);
+  if ((threadIdx.x >> 5) == 0) {
+    tc::tmem_alloc(tslot, kTmemCols);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+}
+
+__device__ __forceinline__ void release_tmem(uint32_t tmem, uint64_t* mbar, uint32_t phase, bool ok) {
+  if (!ok) tc::mbar_wait(mbar, phase, 1u << 20);  // one more bounded wait for a GEMM still in flight
+  tc::fence_before_sync();
+  __syncthreads();
+  if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(tmem, kTmemCols);
+}
+
+__global__ void __launch_bounds__(kTile, 1) k_mlp_infer(Net net, Bounds b, const float* __restrict__ rec, uint64_t n,
+                                                         float* __restrict__ out, uint32_t* err) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* sW = smem;
+  uint8_t* sX = sW + kWBytes;
+  uint8_t* sH = sX + kXBytes;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sH + kHBytes);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+  load_smem(sW, net.wpk_fwd, kWBytes);
+  setup_tmem(mbar, tslot);
+  const uint32_t tmem = *tslot;
+  uint32_t phase = 0;
+  bool ok = true;
+  const uint64_t tiles = (n + kTile - 1) / kTile;
+  for (uint64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    const uint64_t row = tile * kTile + threadIdx.x;
+    float f[kInPad];
+    if (row < n) {
+      encode(rec + row * kRecord, b, f);
+    } else {
+#pragma unroll
+      for (int k = 0; k < kInPad; ++k) f[k] = 0.f;
+    }
+    store_row(sX, threadIdx.x, f, kInPad);
+    tc::fence_smem_to_async();
+    __syncthreads();
+    for (int l = 0; l < kLayers && ok; ++l) {
+      if (threadIdx.x == 0) {
+        tc::fence_after_sync();
+        issue_gemm(l == 0 ? sX : sH, sW + 2 * layer_off(l), uint32_t(layer_n(l)), uint32_t(layer_k(l)), tmem, mbar);
+      }
+      ok = wait_gemm(mbar, phase, err);
+      if (!ok) break;
+      if (l < kLayers - 1) {
+        float v[64];
+        read_acc64(tmem, v);
+#pragma unroll
+        for (int c = 0; c < 64; ++c) v[c] = fmaxf(v[c], 0.f);
+        store_row(sH, threadIdx.x, v, 64);
+        tc::fence_before_sync();
+        tc::fence_smem_to_async();
+        __syncthreads();
+      } else {
+        float v[16];
+        tc::tmem_ld16(tmem + (((threadIdx.x >> 5) * 32u) << 16), v);
+        if (row < n) {
+          out[3 * row] = v[0];
+          out[3 * row + 1] = v[1];
+          out[3 * row + 2] = v[2];
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+      }
+    }
+  }
+  release_tmem(tmem, mbar, phase, ok);
+}
+
+__global__ void __launch_bounds__(kTile, 1) k_mlp_grad(Net net, Bounds b, const float* __restrict__ rec,
+                                                        const float* __restrict__ tgt, uint64_t n, float grad_scale,
+                                                        float* __restrict__ partials, float* __restrict__ tile_loss,
+                                                        uint32_t* err) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* sWf = smem;
+  uint8_t* sWb = sWf + kWBytes;
+  uint8_t* sX = sWb + kWBytes;
+  uint8_t* sA = sX + kXBytes;          // activations A_1..A_5, kHBytes each
+  uint8_t* sG = sA + 5 * kHBytes;      // layer gradient (64 wide)
+  uint8_t* sG16 = sG + kHBytes;        // output gradient (16 wide)
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sG16 + kG16Bytes);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+  float* s_loss = reinterpret_cast<float*>(tslot + 1);
+  load_smem(sWf, net.wpk_fwd, kWBytes);
+  load_smem(sWb, net.wpk_bwd, kWBytes);
+  if (threadIdx.x == 0) *s_loss = 0.f;
+  setup_tmem(mbar, tslot);
+  const uint32_t tmem = *tslot;
+  uint32_t phase = 0;
+  bool ok = true;
+  const uint64_t tile = blockIdx.x;
+  const uint32_t r = threadIdx.x;
+  const uint64_t row = tile * kTile + r;
+  auto act = [&](int l) -> uint8_t* { return l == 0 ? sX : sA + (l - 1) * kHBytes; };
+
+  {
+    float f[kInPad];
+    if (row < n) {
+      encode(rec + row * kRecord, b, f);
+    } else {
+#pragma unroll
+      for (int k = 0; k < kInPad; ++k) f[k] = 0.f;
+    }
+    store_row(sX, r, f, kInPad);
+    tc::fence_smem_to_async();
+    __syncthreads();
+  }
+  // forward, keeping every activation
+  float o[3] = {0.f, 0.f, 0.f};
+  for (int l = 0; l < kLayers && ok; ++l) {
+    if (threadIdx.x == 0) {
+      tc::fence_after_sync();
+      issue_gemm(act(l), sWf + 2 * layer_off(l), uint32_t(layer_n(l)), uint32_t(layer_k(l)), tmem, mbar);
+    }
+    ok = wait_gemm(mbar, phase, err);
+    if (!ok) break;
+    if (l < kLayers - 1) {
+      float v[64];
+      read_acc64(tmem, v);
+#pragma unroll
+      for (int c = 0; c < 64; ++c) v[c] = fmaxf(v[c], 0.f);
+      store_row(act(l + 1), r, v, 64);
+      tc::fence_before_sync();
+      tc::fence_smem_to_async();
+      __syncthreads();
+    } else {
+      float v[16];
+      tc::tmem_ld16(tmem + (((threadIdx.x >> 5) * 32u) << 16), v);
+      o[0] = v[0]; o[1] = v[1]; o[2] = v[2];
+      tc::fence_before_sync();
+      __syncthreads();
+    }
+  }
+  if (ok) {
+    // relative L2 loss and its gradient (the denominator is held constant)
+    float g[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) g[c] = 0.f;
+    float loss = 0.f;
+    if (row < n) {
+      for (int c = 0; c < 3; ++c) {
+        const float d = o[c] - __ldg(tgt + 3 * row + c);
+        const float w = 1.0f / (o[c] * o[c] + 0.01f);
+        loss += d * d * w;
+        g[c] = 2.0f * d * w * grad_scale;
+      }
+    }
+    for (int off = 16; off > 0; off >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(s_loss, loss);
+    store_row(sG16, r, g, 16);
+    tc::fence_smem_to_async();
+    __syncthreads();
+  }
+  // backward
+  for (int l = kLayers - 1; l >= 0 && ok; --l) {
+    const int N = layer_n(l), K = layer_k(l);
+    const uint8_t* G = (l == kLayers - 1) ? sG16 : sG;
+    const uint8_t* A = act(l);
+    if (l > 0 && threadIdx.x == 0) {  // dA_l = G_l · W_l on the tensor cores, (128 x K) with K = 64
+      tc::fence_after_sync();
+      issue_gemm(G, sWb + 2 * layer_off(l), uint32_t(K), uint32_t(N), tmem, mbar);
+    }
+    // dW_l = G_lᵀ · A_l on the CUDA cores: thread t owns outputs o in [o0, o0 + ob), i in [i0, i0 + ib)
+    {
+      const int groups_o = 16, groups_i = 8;  // 128 threads
+      const int ob = N / groups_o, ib = K / groups_i;
+      const int o0 = (threadIdx.x / groups_i) * ob, i0 = (threadIdx.x % groups_i) * ib;
+      float acc[4 * 12];
+      for (int j = 0; j < ob * ib; ++j) acc[j] = 0.f;
+      for (int bb = 0; bb < kTile; ++bb) {
+        float gv[4], av[12];
+        for (int j = 0; j < ob; ++j) gv[j] = tile_at(G, uint32_t(bb), uint32_t(o0 + j), kTile);
+        for (int k = 0; k < ib; ++k) av[k] = tile_at(A, uint32_t(bb), uint32_t(i0 + k), kTile);
+        for (int j = 0; j < ob; ++j)
+          for (int k = 0; k < ib; ++k) acc[j * ib + k] += gv[j] * av[k];
+      }
+      float* dst = partials + tile * uint64_t(kParams) + layer_off(l);
+      for (int j = 0; j < ob; ++j)
+        for (int k = 0; k < ib; ++k) dst[(o0 + j) * K + (i0 + k)] = acc[j * ib + k];
+    }
+    __syncthreads();  // every thread is done reading G_l
+    if (l > 0) {
+      ok = wait_gemm(mbar, phase, err);
+      if (!ok) break;
+      float v[64];
+      read_acc64(tmem, v);
+#pragma unroll
+      for (int c = 0; c < 64; ++c) v[c] = tile_at(A, r, uint32_t(c), kTile) > 0.f ? v[c] : 0.f;
+      store_row(sG, r, v, 64);
+      tc::fence_before_sync();
+      tc::fence_smem_to_async();
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) tile_loss[tile] = *s_loss;
+  release_tmem(tmem, mbar, phase, ok);
+}
+
+__global__ void k_reduce(const float* __restrict__ partials, const float* __restrict__ tile_loss, uint32_t tiles,
+                         float* __restrict__ grad, float* __restrict__ loss) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < uint32_t(kParams)) {
+    float s = 0.f;
+    for (uint32_t t = 0; t < tiles; ++t) s += partials[uint64_t(t) * kParams + p];
+    grad[p] = s;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    float s = 0.f;
+    for (uint32_t t = 0; t < tiles; ++t) s += tile_loss[t];
+    *loss = s;
+  }
+}
+
+__device__ __forceinline__ void pack_one(uint32_t p, float w, uint16_t* fwd, uint16_t* bwd) {
+  int l = 0;
+  while (l + 1 < kLayers && uint32_t(layer_off(l + 1)) <= p) ++l;
+  const uint32_t local = p - uint32_t(layer_off(l));
+  const uint32_t K = uint32_t(layer_k(l)), N = uint32_t(layer_n(l));
+  const uint32_t o = local / K, i = local % K;
+  const uint16_t bits = to_bf16(w);
+  fwd[layer_off(l) + tc::tile_offset(o, i, N) / 2] = bits;
+  bwd[layer_off(l) + tc::tile_offset(i, o, K) / 2] = bits;
+}
+
+__global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                       const float* __restrict__ grad, float c1, float c2, float lr, float b1, float b2, float eps,
+                       uint16_t* fwd, uint16_t* bwd) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= uint32_t(kParams)) return;
+  // Rounded operations spelled out (no contraction) so the step is reproducible on the host.
+  const float g = grad[p];
+  const float mm = __fadd_rn(__fmul_rn(b1, m[p]), __fmul_rn(1.0f - b1, g));
+  const float vv = __fadd_rn(__fmul_rn(b2, v[p]), __fmul_rn(__fmul_rn(1.0f - b2, g), g));
+  m[p] = mm;
+  v[p] = vv;
+  const float step = __fdiv_rn(__fmul_rn(lr, __fdiv_rn(mm, c1)), __fadd_rn(__fsqrt_rn(__fdiv_rn(vv, c2)), eps));
+  const float ww = __fsub_rn(w[p], step);
+  w[p] = ww;
+  pack_one(p, ww, fwd, bwd);
+}
+
+__global__ void k_pack(const float* __restrict__ w, uint16_t* fwd, uint16_t* bwd) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < uint32_t(kParams)) pack_one(p, w[p], fwd, bwd);
+}
+
+size_t infer_smem_bytes() { return kWBytes + kXBytes + kHBytes + 64; }
+size_t train_smem_bytes() { return 2 * kWBytes + kXBytes + 5 * kHBytes + kHBytes + kG16Bytes + 64; }
+
+cudaError_t launch_infer(const Net& net, const Bounds& b, const float* records, uint64_t n, float* out, uint32_t* err,
+                         int sm_count, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, int(infer_smem_bytes()));
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const uint64_t tiles = (n + kTile - 1) / kTile;
+  const uint64_t cap = uint64_t(sm_count) * 2;
+  k_mlp_infer<<<unsigned(tiles < cap ? tiles : cap), kTile, infer_smem_bytes(), s>>>(net, b, records, n, out, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grad_tiles(const Net& net, const Bounds& b, const float* records, const float* targets, uint64_t n,
+                              float grad_scale, float* partials, float* tile_loss, uint32_t* err, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, int(train_smem_bytes()));
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const uint64_t tiles = (n + kTile - 1) / kTile;
+  k_mlp_grad<<<unsigned(tiles), kTile, train_smem_bytes(), s>>>(net, b, records, targets, n, grad_scale, partials,
+                                                                 tile_loss, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce(const float* partials, const float* tile_loss, uint32_t tiles, float* grad, float* loss,
+                          cudaStream_t s) {
+  k_reduce<<<(kParams + 255) / 256, 256, 0, s>>>(partials, tile_loss, tiles, grad, loss);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adam(float* w, float* m, float* v, const float* grad, uint32_t step, float lr, float beta1,
+                        float beta2, float eps, uint16_t* wpk_fwd, uint16_t* wpk_bwd, cudaStream_t s) {
+  const float c1 = 1.0f - powf(beta1, float(step)), c2 = 1.0f - powf(beta2, float(step));
+  k_adam<<<(kParams + 255) / 256, 256, 0, s>>>(w, m, v, grad, c1, c2, lr, beta1, beta2, eps, wpk_fwd, wpk_bwd);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack(const float* w, uint16_t* wpk_fwd, uint16_t* wpk_bwd, cudaStream_t s) {
+  k_pack<<<(kParams + 255) / 256, 256, 0, s>>>(w, wpk_fwd, wpk_bwd);
+  return cudaGetLastError();
+}
+
+}  // namespace mlp
+}  // namespace pbrt
