@@ -99,6 +99,9 @@ typedef struct pbrt_mesh_desc {
   uint32_t vertex_count;
   const uint32_t* indices;  /* 3 * triangle_count vertex indices */
   uint32_t triangle_count;
+  /* Optional material index per triangle (NULL: every triangle takes its object's
+   * material). An extension: the reference binds one material per object. */
+  const uint32_t* face_materials;
 } pbrt_mesh_desc;
 
 typedef struct pbrt_material_desc {
@@ -292,6 +295,22 @@ int pbrt_cache_train_step(pbrt_cache* cache, const float* records, const float* 
 /* Checkpoint of the weights and Adam state (pass buf = NULL to learn the size). */
 int pbrt_cache_save(pbrt_cache* cache, void* buf, uint64_t capacity, uint64_t* size);
 int pbrt_cache_load(pbrt_cache* cache, const void* buf, uint64_t size);
+
+/* Path tracing that ends paths into the learned radiance cache (an extension of
+ * PathIntegrator::li, src/integrators/path.rs:48-115; the reference has no counterpart).
+ * First `train_rounds` rounds of online training. A round traces max(128, train_samples / 4)
+ * full-length path-integrator paths from random pixels and records each Lambertian or metal
+ * vertex (at most train_samples of them) with the radiance the rest of its path gathered,
+ * divided by the throughput at the vertex. It then takes train_steps Adam steps, each on
+ * max(128, train_samples / train_steps) vertices drawn with replacement from the recorded ones.
+ * Then params->spp samples per pixel are rendered as pbrt_render renders them, except that a
+ * path whose hit number terminate_bounce + 1 (or a later one, after a dielectric) lies on a
+ * Lambertian or metal surface stops there: it takes no light sample at that hit and adds
+ * its throughput times max(network output, 0). spp = 0 only trains (film may be NULL). The
+ * integrator must be PBRT_INTEGRATOR_PATH. A cache whose scene box is empty (scene_min ==
+ * scene_max) takes the scene's bounds on first use. */
+int pbrt_render_cached(pbrt_scene* scene, pbrt_cache* cache, const pbrt_render_params* params, uint32_t train_rounds,
+                       double* film_rgb);
 
 /* Spectrum::gamma_correct + to_rgb (src/spectrum.rs:13-25, 134-136): sqrt gamma, clip to
  * [0, 1], truncate to 8 bits, alpha 255, as image_write stores it (mt.rs:152-167). Host

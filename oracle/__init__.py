@@ -211,7 +211,7 @@ def make_ray(origin, direction, dtype=np.float64):
 # ------------------------------------------------------------------------------------------
 class _OMesh(C.Structure):
     _fields_ = [("vertices", C.c_void_p), ("vertex_count", C.c_uint32), ("indices", C.c_void_p),
-                ("triangle_count", C.c_uint32)]
+                ("triangle_count", C.c_uint32), ("face_materials", C.c_void_p)]
 
 
 class _OMaterial(C.Structure):
@@ -265,6 +265,8 @@ def _declare_scene(L):
         getattr(L, f"oracle_scene_trace_{suf}").argtypes = [vp, vp, sz, vp, vp, vp, C.c_int]
         getattr(L, f"oracle_scene_occluded_{suf}").argtypes = [vp, vp, sz, vp, C.c_int]
         getattr(L, f"oracle_render_{suf}").argtypes = [vp, C.POINTER(_ORender), vp, C.c_int]
+        getattr(L, f"oracle_render_cached_{suf}").argtypes = [vp, C.POINTER(_ORender), vp, vp, C.c_uint32, vp,
+                                                              C.c_int]
         getattr(L, f"oracle_camera_rays_{suf}").argtypes = [C.POINTER(_OCamera), vp]
         getattr(L, f"oracle_scene_bvh_{suf}").argtypes = [vp, vp, vp, vp, vp]
         getattr(L, f"oracle_scene_bvh_nodes_{suf}").restype = sz
@@ -288,7 +290,12 @@ class Scene:
             v = np.ascontiguousarray(m["vertices"], np.float32).reshape(-1, 3)
             i = np.ascontiguousarray(m["indices"], np.uint32).reshape(-1, 3)
             self._keep += [v, i]
-            ms.append(_OMesh(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0]))
+            fm = None
+            if m.get("face_materials") is not None:
+                fm = np.ascontiguousarray(m["face_materials"], np.uint32)
+                self._keep.append(fm)
+            ms.append(_OMesh(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0],
+                             fm.ctypes.data if fm is not None else None))
         mats = []
         for m in desc.get("materials", []):
             d = _OMaterial()
@@ -363,6 +370,23 @@ class Scene:
         p.seed, p.integrator = seed, 1 if integrator == "naive" else 0
         film = np.zeros((int(camera["height"]), int(camera["width"]), 3), np.float64)
         if getattr(lib(), f"oracle_render_{self.suf}")(self._h, C.byref(p), _ptr(film), threads) != 0:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return film
+
+    def render_cached(self, camera: dict, spp: int, max_depth: int, weights, bounds, terminate_bounce: int = 2,
+                      seed: int = 1, rr_start: int = 0, sample_offset: int = 0,
+                      threads: int = os.cpu_count() or 1):
+        """The path integrator ending paths into the network `weights` (BF16-emulating) at hit
+        terminate_bounce + 1, as the GPU's cached render does after its training rounds."""
+        p = _ORender()
+        p.camera = _camera(camera)
+        p.spp, p.max_depth, p.rr_start, p.sample_offset = spp, max_depth, rr_start, sample_offset
+        p.seed, p.integrator = seed, 0
+        w = np.ascontiguousarray(weights, np.float32)
+        b = np.ascontiguousarray(bounds, np.float32).reshape(6)
+        film = np.zeros((int(camera["height"]), int(camera["width"]), 3), np.float64)
+        fn = getattr(lib(), f"oracle_render_cached_{self.suf}")
+        if fn(self._h, C.byref(p), _ptr(w), _ptr(b), terminate_bounce + 1, _ptr(film), threads) != 0:
             raise RuntimeError(lib().oracle_last_error().decode())
         return film
 

@@ -8,11 +8,13 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <sstream>
 #include <string>
 #include <thread>
 #include <vector>
 
+#include "mlp_oracle.hpp"
 #include "pbrt_oracle.hpp"
 #include "pbrt_oracle_pt.hpp"
 
@@ -324,7 +326,7 @@ int scene_occluded(const OScene<R>* s, const R* rays, size_t n, uint8_t* occ, in
 // renderers::mt::compute_pixel (mt.rs:112-130): spp jittered samples through the pinhole
 // camera, mean radiance per pixel (accumulated in f64, the film the judge image needs).
 template <class R>
-int render(const OScene<R>* s, const ORenderParams* p, double* film, int threads) {
+int render(const OScene<R>* s, const ORenderParams* p, double* film, int threads, const CacheHook* cache = nullptr) {
   const PinHoleCamera<R> cam = make_camera<R>(p->camera);
   const uint32_t w = p->camera.width, h = p->camera.height;
   const size_t npix = size_t(w) * h;
@@ -338,7 +340,7 @@ int render(const OScene<R>* s, const ORenderParams* p, double* film, int threads
         const Ray<R> ray = cam.get_ray(R(x) + jx, R(y) + jy);
         const V3<R> L = p->integrator == 1 ? s->li_naive(ray, R(p->camera.near), R(p->camera.far), p->max_depth, rng)
                                            : s->li_path(ray, R(p->camera.near), R(p->camera.far), p->max_depth,
-                                                        p->rr_start, rng);
+                                                        p->rr_start, rng, cache);
         acc[0] += double(L.x);
         acc[1] += double(L.y);
         acc[2] += double(L.z);
@@ -347,6 +349,29 @@ int render(const OScene<R>* s, const ORenderParams* p, double* film, int threads
     }
   });
   return 0;
+}
+
+// The cache as the GPU evaluates it: the network in its BF16-emulating mode.
+CacheHook cache_hook(const float* weights, const float* b6, uint32_t term_hit) {
+  auto net = std::make_shared<oracle::mlp::Net>(weights, true);
+  float lo[3], inv[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = b6[a];
+    const float ext = b6[3 + a] - b6[a];
+    inv[a] = ext > 0.f ? 1.0f / ext : 1.0f;
+  }
+  CacheHook h;
+  h.term_hit = term_hit;
+  h.query = [net, lo0 = lo[0], lo1 = lo[1], lo2 = lo[2], i0 = inv[0], i1 = inv[1], i2 = inv[2]](const float* rec,
+                                                                                                  float* rgb) {
+    const float l[3] = {lo0, lo1, lo2}, iv[3] = {i0, i1, i2};
+    double f[oracle::mlp::kInPad], o[oracle::mlp::kOutPad];
+    std::vector<std::vector<double>> acts;
+    oracle::mlp::encode(rec, l, iv, f);
+    net->forward(f, acts, o);
+    for (int c = 0; c < 3; ++c) rgb[c] = float(o[c]);
+  };
+  return h;
 }
 
 template <class R>
@@ -389,6 +414,16 @@ extern "C" {
       return -1;                                                                                            \
     }                                                                                                       \
   }                                                                                                         \
+  int oracle_render_cached_##SUF(void* s, const ORenderParams* p, const float* weights, const float* bounds6,  \
+                                 uint32_t term_hit, double* film, int th) {                                 \
+    try {                                                                                                   \
+      const CacheHook hook = cache_hook(weights, bounds6, term_hit);                                        \
+      return render((OScene<R>*)s, p, film, th, &hook);                                                     \
+    } catch (const std::exception& e) {                                                                     \
+      g_err = e.what();                                                                                     \
+      return -1;                                                                                            \
+    }                                                                                                       \
+  }                                                                                                         \
   void oracle_camera_rays_##SUF(const OCameraDesc* c, R* out) { camera_rays(c, out); }                     \
   void oracle_scene_bvh_##SUF(void* s, R* boxes, uint32_t* left_first, uint32_t* count, uint32_t* order) {  \
     const OScene<R>* sc = (OScene<R>*)s;                                                                    \
@@ -408,7 +443,6 @@ ORACLE_SCENE_API(f32, float)
 }  // extern "C"
 
 // ---- the radiance cache's network (mlp_oracle.hpp) ----------------------------------------
-#include "mlp_oracle.hpp"
 
 extern "C" {
 

@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <functional>
 #include <limits>
 #include <memory>
 #include <stdexcept>
@@ -124,6 +125,7 @@ struct OMeshDesc {
   uint32_t vertex_count;
   const uint32_t* indices;
   uint32_t triangle_count;
+  const uint32_t* face_materials;  // optional per-triangle material (an extension of the reference)
 };
 struct OMaterialDesc {
   uint32_t kind;
@@ -164,6 +166,15 @@ struct ORenderParams {
   uint32_t integrator;  // 0 path, 1 naive
 };
 
+// Ends paths into a radiance cache: at hit number >= term_hit on a Lambertian or metal
+// surface the path takes no light sample, adds beta * max(query(record), 0) and stops. The
+// record is 16 floats: p, roughness (fuzz; 1 for Lambertian), wo, 0, the normal turned to
+// face wo, 0, albedo, 0.
+struct CacheHook {
+  uint32_t term_hit;
+  std::function<void(const float* rec, float* rgb)> query;
+};
+
 // ---------------------------------------------------------------------------------------
 // Scene
 // ---------------------------------------------------------------------------------------
@@ -174,6 +185,7 @@ class OScene {
     std::unique_ptr<MeshBVH<R>> bvh;
     std::vector<R> v;
     std::vector<uint32_t> idx;
+    std::vector<uint32_t> fmat;  // empty: the object's material
   };
   struct Object {
     uint32_t shape, mesh, material;
@@ -206,6 +218,7 @@ class OScene {
       Mesh m;
       m.v.assign(md.vertices, md.vertices + 3 * size_t(md.vertex_count));
       m.idx.assign(md.indices, md.indices + 3 * size_t(md.triangle_count));
+      if (md.face_materials) m.fmat.assign(md.face_materials, md.face_materials + md.triangle_count);
       m.bvh.reset(new MeshBVH<R>(m.v.data(), md.vertex_count, m.idx.data(), md.triangle_count,
                                  d.bvh_bins ? int(d.bvh_bins) : 8, d.bvh_max_leaf ? d.bvh_max_leaf : 1));
       meshes.push_back(std::move(m));
@@ -785,9 +798,16 @@ class OScene {
     return false;  // DiffuseLight scatters nothing
   }
 
+  uint32_t material_of(uint32_t obj, uint32_t prim) const {
+    const Object& o = objects[obj];
+    if (o.shape == O_SHAPE_MESH && !meshes[o.mesh].fmat.empty()) return meshes[o.mesh].fmat[prim];
+    return o.material;
+  }
+
   // ---- integrators --------------------------------------------------------------------------
   // PathIntegrator::li (path.rs:48-115) with area-light NEE and Russian roulette
-  V3<R> li_path(Ray<R> ray, R near, R far, uint32_t max_depth, uint32_t rr_start, Pcg32& rng) const {
+  V3<R> li_path(Ray<R> ray, R near, R far, uint32_t max_depth, uint32_t rr_start, Pcg32& rng,
+                const CacheHook* cache = nullptr) const {
     V3<R> beta{R(1), R(1), R(1)}, L{R(0), R(0), R(0)};
     bool specular = true;
     uint32_t bounce = 0;
@@ -802,11 +822,25 @@ class OScene {
         }
         break;
       }
-      const Material& m = materials[objects[obj].material];
+      const Material& m = materials[material_of(obj, prim)];
       if (specular && m.kind == O_MAT_DIFFUSE_LIGHT)
         L = L + V3<R>{m.color.x * beta.x, m.color.y * beta.y, m.color.z * beta.z};
       bounce++;
       if (bounce == max_depth) break;
+      if (cache && bounce >= cache->term_hit && (m.kind == O_MAT_LAMBERTIAN || m.kind == O_MAT_METAL)) {
+        const V3<R> wo = ray.d * R(-1);
+        const V3<R> n = dot(it.n, wo) < R(0) ? it.n * R(-1) : it.n;
+        const float rec[16] = {float(it.p.x), float(it.p.y), float(it.p.z),
+                               m.kind == O_MAT_METAL ? float(m.fuzz) : 1.0f,
+                               float(wo.x), float(wo.y), float(wo.z), 0.f,
+                               float(n.x), float(n.y), float(n.z), 0.f,
+                               float(m.color.x), float(m.color.y), float(m.color.z), 0.f};
+        float o[3];
+        cache->query(rec, o);
+        L = L + V3<R>{beta.x * R(std::fmax(o[0], 0.f)), beta.y * R(std::fmax(o[1], 0.f)),
+                      beta.z * R(std::fmax(o[2], 0.f))};
+        break;
+      }
       if (!lights.empty()) {  // sample_light (path.rs:31-44)
         const R cnt = R(lights.size());
         const R pick = std::min(R(rng.uniform()) * cnt, cnt - R(1));
@@ -855,7 +889,7 @@ class OScene {
         L = L + V3<R>{bg.x * beta.x, bg.y * beta.y, bg.z * beta.z};
         break;
       }
-      const Material& m = materials[objects[obj].material];
+      const Material& m = materials[material_of(obj, prim)];
       if (m.kind == O_MAT_DIFFUSE_LIGHT) L = L + V3<R>{m.color.x * beta.x, m.color.y * beta.y, m.color.z * beta.z};
       Scatter sc;
       if (!scatter(m, it, rng, &sc)) break;

@@ -29,7 +29,7 @@ LIGHT_POINT, LIGHT_UNIFORM_INFINITE, LIGHT_BACKGROUND_INFINITE, LIGHT_AREA = 0, 
 
 class MeshDesc(C.Structure):
     _fields_ = [("vertices", C.c_void_p), ("vertex_count", C.c_uint32), ("indices", C.c_void_p),
-                ("triangle_count", C.c_uint32)]
+                ("triangle_count", C.c_uint32), ("face_materials", C.c_void_p)]
 
 
 class MaterialDesc(C.Structure):
@@ -107,6 +107,7 @@ SIGNATURES = {
     "pbrt_cache_train_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "pbrt_cache_save": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
     "pbrt_cache_load": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "pbrt_render_cached": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(RenderParams), C.c_uint32, C.c_void_p]),
     "pbrt_film_to_rgba8": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
 }
 

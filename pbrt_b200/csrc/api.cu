@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/pbrt_b200.h"
+#include "cache.hpp"
 #include "kernels.hpp"
 #include "mesh_bvh.hpp"
 #include "render.hpp"
@@ -172,7 +173,10 @@ int pbrt_scene_create(pbrt_ctx* c, const pbrt_scene_desc* d, pbrt_scene** out) {
     void* pi = nullptr;
     rc = s->upload(&pv, fs.mesh_v[i].data(), fs.mesh_v[i].size() * sizeof(float));
     if (rc == PBRT_OK) rc = s->upload(&pi, fs.mesh_idx[i].data(), fs.mesh_idx[i].size() * sizeof(uint32_t));
-    shades[i] = MeshShade{(const float*)pv, (const uint32_t*)pi};
+    void* pf = nullptr;
+    if (rc == PBRT_OK && !fs.mesh_fmat[i].empty())
+      rc = s->upload(&pf, fs.mesh_fmat[i].data(), fs.mesh_fmat[i].size() * sizeof(uint32_t));
+    shades[i] = MeshShade{(const float*)pv, (const uint32_t*)pi, (const uint32_t*)pf};
     s->info.triangle_count += fm.tri_index.size();
     s->info.mesh_node_count += fm.stats.node_count;
     s->info.mesh_leaf_count += fm.stats.leaf_count;
@@ -211,6 +215,10 @@ int pbrt_scene_create(pbrt_ctx* c, const pbrt_scene_desc* d, pbrt_scene** out) {
   v.light_cdf = (const float*)lcdf;
   s->info.object_count = d->object_count;
   s->info.device_bytes += s->extra_bytes;
+  for (int a = 0; a < 3; ++a) {
+    s->bounds[a] = fs.top[0].bmin[a];
+    s->bounds[3 + a] = fs.top[0].bmax[a];
+  }
   if (d->object_count == 1 && d->objects[0].shape == PBRT_SHAPE_MESH && !d->objects[0].transformed)
     s->single_mesh = int(d->objects[0].mesh);
   *out = s.release();
@@ -454,6 +462,36 @@ int ensure_wave(pbrt_ctx* c, WaveAlloc* wa, uint32_t cap) {
 
 WaveAlloc g_waves[kMaxDevices];  // per device; a context serialises its own calls
 
+int check_render_params(pbrt_ctx* c, const pbrt_render_params* p, bool allow_no_samples) {
+  const pbrt_camera_desc& cd = p->camera;
+  if (cd.width == 0 || cd.height == 0) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "empty image");
+  if (p->spp == 0 && !allow_no_samples) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "spp must be >= 1");
+  if (p->max_depth == 0 || p->max_depth > 0xFFFF)
+    return c->fail(PBRT_ERR_INVALID_ARGUMENT, "max_depth must be in [1, 65535]");
+  if (p->integrator > PBRT_INTEGRATOR_NAIVE) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "unknown integrator");
+  if (!(cd.fov > 0.f) || !(cd.fov < 3.14159265f) || !(cd.far > cd.near))
+    return c->fail(PBRT_ERR_INVALID_ARGUMENT, "bad camera");
+  if (uint64_t(cd.width) * cd.height > 0xFFFFFFFFull) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "image too large");
+  return PBRT_OK;
+}
+
+RenderSettings settings_of(const pbrt_render_params* p) {
+  RenderSettings rs;
+  rs.max_depth = p->max_depth;
+  rs.rr_start = p->integrator == PBRT_INTEGRATOR_NAIVE ? 0u : p->rr_start;
+  rs.sample_offset = p->sample_offset;
+  rs.naive = p->integrator == PBRT_INTEGRATOR_NAIVE ? 1u : 0u;
+  rs.seed = p->seed;
+  return rs;
+}
+
+unsigned long long host_mix64(unsigned long long x) {
+  x += 0x9E3779B97F4A7C15ULL;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+  return x ^ (x >> 31);
+}
+
 }  // namespace
 
 extern "C" {
@@ -463,24 +501,12 @@ int pbrt_render(pbrt_scene* s, const pbrt_render_params* p, double* film) {
   pbrt_ctx* c = s->ctx;
   DeviceGuard g(c->device);
   if (!p || !film) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "params or film is NULL");
+  PBRT_TRY(check_render_params(c, p, false));
   const pbrt_camera_desc& cd = p->camera;
-  if (cd.width == 0 || cd.height == 0) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "empty image");
-  if (p->spp == 0) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "spp must be >= 1");
-  if (p->max_depth == 0 || p->max_depth > 0xFFFF)
-    return c->fail(PBRT_ERR_INVALID_ARGUMENT, "max_depth must be in [1, 65535]");
-  if (p->integrator > PBRT_INTEGRATOR_NAIVE) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "unknown integrator");
-  if (!(cd.fov > 0.f) || !(cd.fov < 3.14159265f) || !(cd.far > cd.near))
-    return c->fail(PBRT_ERR_INVALID_ARGUMENT, "bad camera");
   const uint64_t npix = uint64_t(cd.width) * cd.height;
-  if (npix > 0xFFFFFFFFull) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "image too large");
   const uint64_t total = npix * p->spp;
   const CameraRec cam = build_camera(cd);
-  RenderSettings rs;
-  rs.max_depth = p->max_depth;
-  rs.rr_start = p->integrator == PBRT_INTEGRATOR_NAIVE ? 0u : p->rr_start;
-  rs.sample_offset = p->sample_offset;
-  rs.naive = p->integrator == PBRT_INTEGRATOR_NAIVE ? 1u : 0u;
-  rs.seed = p->seed;
+  const RenderSettings rs = settings_of(p);
 
   WaveAlloc& wa = g_waves[c->device];
   const uint32_t wave = uint32_t(std::min<uint64_t>(total, kWave));
@@ -495,6 +521,102 @@ int pbrt_render(pbrt_scene* s, const pbrt_render_params* p, double* film) {
     const uint32_t n = uint32_t(std::min<uint64_t>(wave, total - base));
     rc = c->cuda(render_wave(s->view, wa.w, cam, base, n, uint32_t(npix), rs, dfilm, c->d_err, c->sm_count, st),
                  "render");
+  }
+  if (rc == PBRT_OK) rc = c->cuda(scale_film(dfilm, film_n, 1.0 / double(p->spp), c->sm_count, st), "render");
+  if (host_film) {
+    if (rc == PBRT_OK)
+      rc = c->cuda(cudaMemcpyAsync(film, dfilm, film_n * sizeof(double), cudaMemcpyDeviceToHost, st), "cudaMemcpy(film)");
+    if (rc == PBRT_OK) rc = check_device_error(c, st);
+    cudaStreamSynchronize(st);
+    cudaFree(dfilm);
+    return rc;
+  }
+  PBRT_TRY(rc);
+  if (c->user) return PBRT_OK;
+  return check_device_error(c, st);
+}
+
+int pbrt_render_cached(pbrt_scene* s, pbrt_cache* k, const pbrt_render_params* p, uint32_t train_rounds,
+                       double* film) {
+  if (!s || !k) return PBRT_ERR_INVALID_ARGUMENT;
+  pbrt_ctx* c = s->ctx;
+  DeviceGuard g(c->device);
+  if (k->ctx != c) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "the cache belongs to another context");
+  if (!p) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "params is NULL");
+  PBRT_TRY(check_render_params(c, p, true));
+  if (p->spp && !film) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "film is NULL");
+  if (p->integrator != PBRT_INTEGRATOR_PATH)
+    return c->fail(PBRT_ERR_UNSUPPORTED, "the radiance cache ends path-integrator paths only");
+  pbrt_cache_params& cp = k->params;
+  if (cp.scene_min[0] == cp.scene_max[0] && cp.scene_min[1] == cp.scene_max[1] && cp.scene_min[2] == cp.scene_max[2])
+    for (int a = 0; a < 3; ++a) {
+      cp.scene_min[a] = s->bounds[a];
+      cp.scene_max[a] = s->bounds[3 + a];
+    }
+  const pbrt_camera_desc& cd = p->camera;
+  const uint64_t npix = uint64_t(cd.width) * cd.height;
+  const uint64_t total = npix * p->spp;
+  const CameraRec cam = build_camera(cd);
+  const RenderSettings rs = settings_of(p);
+  const uint32_t train_paths = std::max(128u, cp.train_samples / 4);
+  const uint32_t steps = cp.train_steps;
+  const uint32_t batch = std::max(128u, cp.train_samples / steps);
+  const uint32_t wave = uint32_t(std::min<uint64_t>(total, kWave));
+
+  WaveAlloc& wa = g_waves[c->device];
+  PBRT_TRY(ensure_wave(c, &wa, std::max(wave, train_paths)));
+  PBRT_TRY(k->ensure_render_buffers(wave, cp.train_samples, batch));
+  cudaStream_t st = c->work_stream();
+  const CacheWave& cw = k->cw;
+
+  // online training: full-length paths from random pixels, their vertices' radiance suffixes
+  for (uint32_t r = 0; r < train_rounds; ++r) {
+    RenderSettings tr = rs;
+    tr.cache_mode = kCacheRecord;
+    tr.random_pixels = 1;
+    tr.sample_offset = 0;
+    tr.seed = host_mix64(p->seed ^ host_mix64(0x747261696e696e67ULL + k->rounds));
+    PBRT_TRY(c->cuda(cudaMemsetAsync(cw.counts, 0, 2 * sizeof(uint32_t), st), "cudaMemset(cache counts)"));
+    PBRT_TRY(c->cuda(trace_wave(s->view, wa.w, cw, cam, 0, train_paths, uint32_t(npix), tr, c->d_err, c->sm_count, st),
+                     "cache training paths"));
+    uint32_t offered = 0;
+    PBRT_TRY(c->cuda(cudaMemcpyAsync(&offered, cw.counts + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st),
+                     "cudaMemcpy(cache counts)"));
+    PBRT_TRY(check_device_error(c, st));
+    const uint32_t m = std::min(offered, cw.tcap);
+    if (m > 0)
+      for (uint32_t step = 0; step < steps; ++step) {
+        PBRT_TRY(c->cuda(train_batch(wa.w, cw, m, batch, step, tr.seed, k->brec, k->btgt, c->sm_count, st),
+                         "cache training batch"));
+        PBRT_TRY(k->gradient_device(k->brec, k->btgt, batch, st));
+        PBRT_TRY(k->adam_device(st));
+      }
+    ++k->rounds;
+  }
+  if (p->spp == 0) return check_device_error(c, st);
+
+  // rendering: paths end into the cache at hit terminate_bounce + 1
+  RenderSettings qr = rs;
+  qr.cache_mode = kCacheQuery;
+  qr.term_hit = cp.terminate_bounce + 1;
+  const mlp::Net net{k->wfwd, k->wbwd};
+  const mlp::Bounds nb = k->bounds();
+  const size_t film_n = size_t(npix) * 3;
+  double* dfilm = film;
+  const bool host_film = mem_kind(film) != MemKind::Device;
+  if (host_film) PBRT_TRY(c->cuda(cudaMalloc(&dfilm, film_n * sizeof(double)), "cudaMalloc(film)"));
+  int rc = c->cuda(cudaMemsetAsync(dfilm, 0, film_n * sizeof(double), st), "cudaMemset(film)");
+  for (uint64_t base = 0; base < total && rc == PBRT_OK; base += wave) {
+    const uint32_t n = uint32_t(std::min<uint64_t>(wave, total - base));
+    rc = c->cuda(cudaMemsetAsync(cw.counts, 0, sizeof(uint32_t), st), "cudaMemset(cache counts)");
+    if (rc == PBRT_OK)
+      rc = c->cuda(trace_wave(s->view, wa.w, cw, cam, base, n, uint32_t(npix), qr, c->d_err, c->sm_count, st),
+                   "cached render");
+    if (rc == PBRT_OK)
+      rc = c->cuda(mlp::launch_infer_dev(net, nb, cw.qrec, cw.counts, n, cw.qout, c->d_err, c->sm_count, st),
+                   "cache query");
+    if (rc == PBRT_OK) rc = c->cuda(apply_cache(wa.w, cw, n, c->sm_count, st), "cache apply");
+    if (rc == PBRT_OK) rc = c->cuda(accumulate_wave(wa.w, n, dfilm, c->sm_count, st), "cached render");
   }
   if (rc == PBRT_OK) rc = c->cuda(scale_film(dfilm, film_n, 1.0 / double(p->spp), c->sm_count, st), "render");
   if (host_film) {

@@ -118,11 +118,42 @@ int pbrt_cache::query_device(const float* records, uint64_t n, float* rgb, cudaS
   return ctx->cuda(mlp::launch_infer(net, bounds(), records, n, rgb, ctx->d_err, ctx->sm_count, s), "cache query");
 }
 
+int pbrt_cache::ensure_render_buffers(uint32_t queries, uint32_t train_vertices, uint32_t batch) {
+  if (render_block && qcap >= queries && cw.tcap >= train_vertices && bcap >= batch) return PBRT_OK;
+  queries = std::max(queries, qcap);
+  train_vertices = std::max(train_vertices, cw.tcap);
+  batch = std::max(batch, bcap);
+  cudaFree(render_block);
+  render_block = nullptr;
+  qcap = bcap = 0;
+  cw = pbrt::CacheWave{};
+  const size_t R = pbrt::kCacheRecordFloats * 4;
+  auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t bytes = up(64) + up(size_t(queries) * R) + up(size_t(queries) * 12) + up(size_t(queries) * 4) +
+                       up(size_t(train_vertices) * R) + up(size_t(train_vertices) * 24) +
+                       up(size_t(train_vertices) * 4) + up(size_t(batch) * R) + up(size_t(batch) * 12);
+  PBRT_TRY(ctx->cuda(cudaMalloc(&render_block, bytes), "cudaMalloc(cache render buffers)"));
+  char* p = static_cast<char*>(render_block);
+  auto take = [&](size_t b) { char* r = p; p += up(b); return r; };
+  cw.counts = reinterpret_cast<uint32_t*>(take(64));
+  cw.qrec = reinterpret_cast<float*>(take(size_t(queries) * R));
+  cw.qout = reinterpret_cast<float*>(take(size_t(queries) * 12));
+  cw.qpath = reinterpret_cast<uint32_t*>(take(size_t(queries) * 4));
+  cw.trec = reinterpret_cast<float*>(take(size_t(train_vertices) * R));
+  cw.tstate = reinterpret_cast<float*>(take(size_t(train_vertices) * 24));
+  cw.tpath = reinterpret_cast<uint32_t*>(take(size_t(train_vertices) * 4));
+  cw.tcap = train_vertices;
+  brec = reinterpret_cast<float*>(take(size_t(batch) * R));
+  btgt = reinterpret_cast<float*>(take(size_t(batch) * 12));
+  qcap = queries;
+  bcap = batch;
+  return PBRT_OK;
+}
+
 void pbrt_cache::release() {
   for (void* p : {(void*)w, (void*)m, (void*)v, (void*)grad, (void*)wfwd, (void*)wbwd, (void*)loss, (void*)partials,
-                  (void*)tile_loss})
+                  (void*)tile_loss, render_block})
     cudaFree(p);
-  for (void* p : train_bufs) cudaFree(p);
 }
 
 namespace {

@@ -8,6 +8,7 @@
 
 #include "../../include/pbrt_b200.h"
 #include "mlp.hpp"
+#include "render.hpp"
 
 struct pbrt_cache {
   pbrt_ctx* ctx = nullptr;
@@ -17,7 +18,14 @@ struct pbrt_cache {
   float *partials = nullptr, *tile_loss = nullptr;
   uint32_t tile_cap = 0;
   uint32_t step = 0;
-  std::vector<void*> train_bufs;  // the cached render's training-record buffers
+  uint64_t rounds = 0;  // training rounds run by cached renders (keys their path streams)
+
+  // the cached render's buffers: queries, training vertices and one training batch
+  void* render_block = nullptr;
+  uint32_t qcap = 0, bcap = 0;
+  pbrt::CacheWave cw{};
+  float *brec = nullptr, *btgt = nullptr;
+  int ensure_render_buffers(uint32_t queries, uint32_t train_vertices, uint32_t batch);
 
   int device_arrays();
   int ensure_tiles(uint32_t tiles);

@@ -102,6 +102,7 @@ struct pbrt_scene {
   pbrt::SceneView view{};
   pbrt_scene_info info{};
   int single_mesh = -1;  // index of the only (untransformed) mesh object, or -1
+  float bounds[6] = {0, 0, 0, 0, 0, 0};  // world box of every object (min xyz, max xyz)
 
   int upload(void** dst, const void* src, size_t bytes) {
     if (bytes == 0) return PBRT_OK;

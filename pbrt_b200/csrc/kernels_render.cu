@@ -270,13 +270,27 @@ PBRT_DEV void camera_ray(const CameraRec& c, float px, float py, F3& o, F3& d) {
   d = normalize3(xf_dir(c.cam_to_world, cv));
 }
 
+// ---- the radiance cache's records ---------------------------------------------------------------
+PBRT_DEV void write_record(float* rec, const F3& p, float rough, const F3& wo, const F3& n, const F3& alb) {
+  float4* r = reinterpret_cast<float4*>(rec);
+  r[0] = make_float4(p.x, p.y, p.z, rough);
+  r[1] = make_float4(wo.x, wo.y, wo.z, 0.f);
+  r[2] = make_float4(n.x, n.y, n.z, 0.f);
+  r[3] = make_float4(alb.x, alb.y, alb.z, 0.f);
+}
+
 // ---- kernels ---------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_generate(WaveBuffers w, CameraRec cam, uint64_t wave_base, uint32_t n,
-                                                  uint32_t npix, uint32_t sample_offset, unsigned long long seed) {
+                                                  uint32_t npix, uint32_t sample_offset, unsigned long long seed,
+                                                  uint32_t random_pixels) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint64_t g = wave_base + i;
-    const uint32_t pixel = uint32_t(g % npix);
-    const uint32_t sample = sample_offset + uint32_t(g / npix);
+    uint32_t pixel = uint32_t(g % npix);
+    uint32_t sample = sample_offset + uint32_t(g / npix);
+    if (random_pixels) {  // training paths: a pixel per path, the path's index keys its stream
+      pixel = uint32_t(splitmix64(seed + g) % npix);
+      sample = uint32_t(g);
+    }
     const unsigned long long inc = pcg_inc(pixel);
     unsigned long long st = pcg_seed(seed, pixel, sample);
     const float jx = pcg_uniform(st, inc), jy = pcg_uniform(st, inc);  // Sampler2::sample (mt.rs:145-150)
@@ -313,17 +327,19 @@ __global__ void __launch_bounds__(128) k_extend(WaveBuffers w, SceneView s, cons
 __global__ void __launch_bounds__(128) k_shade(WaveBuffers w, SceneView s, const uint32_t* __restrict__ q,
                                                const uint32_t* __restrict__ qcount, uint32_t* __restrict__ qout,
                                                uint32_t* __restrict__ qout_count, uint32_t max_depth, uint32_t rr_start,
-                                               uint32_t naive) {
+                                               uint32_t naive, CacheWave cw, uint32_t cache_mode, uint32_t term_hit) {
   const uint32_t n = *qcount;
   // every lane runs the same trip count so the warp-aggregated pushes see full warps
   const uint32_t stride = gridDim.x * blockDim.x;
   const uint32_t iters = (n + stride - 1) / stride;
   for (uint32_t it_ = 0; it_ < iters; ++it_) {
     const uint32_t k = it_ * stride + blockIdx.x * blockDim.x + threadIdx.x;
-    bool push_path = false, push_shadow = false;
+    bool push_path = false, push_shadow = false, push_query = false, push_train = false;
     uint32_t p = 0;
     F3 sro, srd, contrib;
     float stmax = 0.f;
+    F3 cp, cwo, cn, calb, cL, cB;  // the cache record of this vertex
+    float crough = 0.f;
     if (k < n) {
       p = q[k];
       F3 o = mk3(w.ox[p], w.oy[p], w.oz[p]), d = mk3(w.dx[p], w.dy[p], w.dz[p]);
@@ -344,7 +360,7 @@ __global__ void __launch_bounds__(128) k_shade(WaveBuffers w, SceneView s, const
         }
       } else {
         const Isect it = interaction(s, obj, w.hprim[p], o, d, w.ht[p]);
-        const MatRec m = s.materials[s.objects[obj].material];
+        const MatRec m = s.materials[material_index(s, obj, w.hprim[p])];
         if (spec && m.kind == kMatDiffuseLight)
           L = add3(L, mk3(fm(m.color[0], beta.x), fm(m.color[1], beta.y), fm(m.color[2], beta.z)));
         bounce++;
@@ -352,7 +368,19 @@ __global__ void __launch_bounds__(128) k_shade(WaveBuffers w, SceneView s, const
         // the naive estimator scatters at every hit and the host stops extending after
         // max_depth hits (naive.rs:29-52: li(.., 0) is black).
         const bool depth_cut = !naive && bounce == max_depth;
-        if (!depth_cut) {
+        const bool cacheable = m.kind == kMatLambertian || m.kind == kMatMetal;
+        if (!depth_cut && cacheable && (cache_mode == kCacheRecord || (cache_mode == kCacheQuery && bounce >= term_hit))) {
+          cp = it.p;
+          cwo = mul3(d, -1.f);
+          cn = dot3(it.n, cwo) < 0.f ? mul3(it.n, -1.f) : it.n;
+          calb = mk3(m.color[0], m.color[1], m.color[2]);
+          crough = m.kind == kMatMetal ? m.fuzz : 1.f;
+          cL = L;
+          cB = beta;
+          push_query = cache_mode == kCacheQuery;  // the path ends here, into the cache
+          push_train = cache_mode == kCacheRecord;
+        }
+        if (!depth_cut && !push_query) {
           if (!naive && s.light_count > 0) {  // sample_light (path.rs:31-44) and the light sample
             const float cnt = float(s.light_count);
             const float pick = fminf(fm(pcg_uniform(st, inc), cnt), fs(cnt, 1.f));
@@ -416,6 +444,50 @@ __global__ void __launch_bounds__(128) k_shade(WaveBuffers w, SceneView s, const
       w.s_dx[si] = srd.x; w.s_dy[si] = srd.y; w.s_dz[si] = srd.z;
       w.s_tmax[si] = stmax;
       w.s_cr[si] = contrib.x; w.s_cg[si] = contrib.y; w.s_cb[si] = contrib.z;
+    }
+    if (cache_mode != kCacheOff) {  // uniform over the grid, so the pushes see whole warps
+      const uint32_t ci = warp_push(cw.counts, push_query);
+      if (push_query) {  // at most one query per path: ci < the wave size
+        write_record(cw.qrec + size_t(ci) * kCacheRecordFloats, cp, crough, cwo, cn, calb);
+        cw.qpath[ci] = p;
+      }
+      const uint32_t ti = warp_push(cw.counts + 1, push_train);
+      if (push_train && ti < cw.tcap) {
+        write_record(cw.trec + size_t(ti) * kCacheRecordFloats, cp, crough, cwo, cn, calb);
+        float* ts = cw.tstate + 6 * size_t(ti);
+        ts[0] = cL.x; ts[1] = cL.y; ts[2] = cL.z;
+        ts[3] = cB.x; ts[4] = cB.y; ts[5] = cB.z;
+        cw.tpath[ti] = p;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_apply_cache(WaveBuffers w, CacheWave cw) {
+  const uint32_t n = cw.counts[0];
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const uint32_t p = cw.qpath[k];
+    const float* o = cw.qout + 3 * size_t(k);
+    w.lr[p] = fa(w.lr[p], fm(w.br[p], fmaxf(o[0], 0.f)));
+    w.lg[p] = fa(w.lg[p], fm(w.bg[p], fmaxf(o[1], 0.f)));
+    w.lb[p] = fa(w.lb[p], fm(w.bb[p], fmaxf(o[2], 0.f)));
+  }
+}
+
+__global__ void __launch_bounds__(256) k_train_batch(WaveBuffers w, CacheWave cw, uint32_t m, uint32_t batch,
+                                                     uint32_t step, unsigned long long seed, float* __restrict__ rec,
+                                                     float* __restrict__ tgt) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < batch; i += gridDim.x * blockDim.x) {
+    const uint32_t j = uint32_t(splitmix64(seed ^ ((((unsigned long long)step) << 32) | i)) % m);
+    const float4* src = reinterpret_cast<const float4*>(cw.trec + size_t(j) * kCacheRecordFloats);
+    float4* dst = reinterpret_cast<float4*>(rec + size_t(i) * kCacheRecordFloats);
+    dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; dst[3] = src[3];
+    const uint32_t p = cw.tpath[j];
+    const float* ts = cw.tstate + 6 * size_t(j);
+    const float le[3] = {w.lr[p], w.lg[p], w.lb[p]};
+    for (int c = 0; c < 3; ++c) {
+      const float b = ts[3 + c];
+      tgt[3 * size_t(i) + c] = b > 0.f ? fdv(fs(le[c], ts[c]), b) : 0.f;
     }
   }
 }
@@ -494,11 +566,12 @@ cudaError_t launch_scene_any(const SceneView& s, const float* rays, uint64_t str
   return cudaGetLastError();
 }
 
-cudaError_t render_wave(const SceneView& s, const WaveBuffers& w, const CameraRec& cam, uint64_t wave_base,
-                        uint32_t n, uint32_t npix, const RenderSettings& rs, double* film, uint32_t* err, int sm_count,
-                        cudaStream_t st) {
+cudaError_t trace_wave(const SceneView& s, const WaveBuffers& w, const CacheWave& cw, const CameraRec& cam,
+                       uint64_t wave_base, uint32_t n, uint32_t npix, const RenderSettings& rs, uint32_t* err,
+                       int sm_count, cudaStream_t st) {
   cudaError_t e;
-  k_generate<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, cam, wave_base, n, npix, rs.sample_offset, rs.seed);
+  k_generate<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, cam, wave_base, n, npix, rs.sample_offset, rs.seed,
+                                                             rs.random_pixels);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const unsigned g128 = unsigned(sm_count) * 16;
   for (uint32_t b = 0; b < rs.max_depth; ++b) {
@@ -509,11 +582,38 @@ cudaError_t render_wave(const SceneView& s, const WaveBuffers& w, const CameraRe
     if ((e = cudaMemsetAsync(cout, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.counts + 2, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
     k_extend<<<g128, 128, 0, st>>>(w, s, qin, cin, cam.near, cam.far, err);
-    k_shade<<<g128, 128, 0, st>>>(w, s, qin, cin, qout, cout, rs.max_depth, rs.rr_start, rs.naive);
+    k_shade<<<g128, 128, 0, st>>>(w, s, qin, cin, qout, cout, rs.max_depth, rs.rr_start, rs.naive, cw, rs.cache_mode,
+                                  rs.term_hit);
     if (!rs.naive) k_shadow<<<g128, 128, 0, st>>>(w, s, err);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
+  return cudaSuccess;
+}
+
+cudaError_t accumulate_wave(const WaveBuffers& w, uint32_t n, double* film, int sm_count, cudaStream_t st) {
   k_accumulate<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, n, film);
+  return cudaGetLastError();
+}
+
+cudaError_t render_wave(const SceneView& s, const WaveBuffers& w, const CameraRec& cam, uint64_t wave_base,
+                        uint32_t n, uint32_t npix, const RenderSettings& rs, double* film, uint32_t* err, int sm_count,
+                        cudaStream_t st) {
+  RenderSettings plain = rs;
+  plain.cache_mode = kCacheOff;
+  const cudaError_t e = trace_wave(s, w, CacheWave{}, cam, wave_base, n, npix, plain, err, sm_count, st);
+  if (e != cudaSuccess) return e;
+  return accumulate_wave(w, n, film, sm_count, st);
+}
+
+cudaError_t apply_cache(const WaveBuffers& w, const CacheWave& cw, uint32_t n_max, int sm_count, cudaStream_t st) {
+  k_apply_cache<<<grid_cap(n_max, 256, sm_count, 8), 256, 0, st>>>(w, cw);
+  return cudaGetLastError();
+}
+
+cudaError_t train_batch(const WaveBuffers& w, const CacheWave& cw, uint32_t m, uint32_t batch, uint32_t step,
+                        unsigned long long seed, float* rec, float* tgt, int sm_count, cudaStream_t st) {
+  if (m == 0 || batch == 0) return cudaSuccess;
+  k_train_batch<<<grid_cap(batch, 256, sm_count, 8), 256, 0, st>>>(w, cw, m, batch, step, seed, rec, tgt);
   return cudaGetLastError();
 }
 

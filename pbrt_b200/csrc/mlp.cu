@@ -134,7 +134,10 @@ __device__ __forceinline__ void release_tmem(uint32_t tmem, uint64_t* mbar, uint
 }
 
 __global__ void __launch_bounds__(kTile, 1) k_mlp_infer(Net net, Bounds b, const float* __restrict__ rec, uint64_t n,
-                                                         float* __restrict__ out, uint32_t* err) {
+                                                         const uint32_t* __restrict__ n_dev, float* __restrict__ out,
+                                                         uint32_t* err) {
+  if (n_dev) n = min(n, uint64_t(*n_dev));  // a count the previous kernel left on the device
+  if (uint64_t(blockIdx.x) * kTile >= n) return;  // before any barrier or TMEM allocation
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* sW = smem;
   uint8_t* sX = sW + kWBytes;
@@ -373,6 +376,11 @@ size_t train_smem_bytes() { return 2 * kWBytes + kXBytes + 5 * kHBytes + kHBytes
 
 cudaError_t launch_infer(const Net& net, const Bounds& b, const float* records, uint64_t n, float* out, uint32_t* err,
                          int sm_count, cudaStream_t s) {
+  return launch_infer_dev(net, b, records, nullptr, n, out, err, sm_count, s);
+}
+
+cudaError_t launch_infer_dev(const Net& net, const Bounds& b, const float* records, const uint32_t* n_dev,
+                             uint64_t n, float* out, uint32_t* err, int sm_count, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   static bool configured = false;
   if (!configured) {
@@ -382,7 +390,8 @@ cudaError_t launch_infer(const Net& net, const Bounds& b, const float* records, 
   }
   const uint64_t tiles = (n + kTile - 1) / kTile;
   const uint64_t cap = uint64_t(sm_count) * 2;
-  k_mlp_infer<<<unsigned(tiles < cap ? tiles : cap), kTile, infer_smem_bytes(), s>>>(net, b, records, n, out, err);
+  k_mlp_infer<<<unsigned(tiles < cap ? tiles : cap), kTile, infer_smem_bytes(), s>>>(net, b, records, n, n_dev, out,
+                                                                                     err);
   return cudaGetLastError();
 }
 

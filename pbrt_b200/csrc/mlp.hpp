@@ -37,6 +37,9 @@ struct Net {
 // out[3 * i + c] = network(record i), i < n.
 cudaError_t launch_infer(const Net& net, const Bounds& b, const float* records, uint64_t n, float* out,
                          uint32_t* err, int sm_count, cudaStream_t s);
+// The same for n = min(n_max, *n_dev), a count on the device (the grid is sized for n_max).
+cudaError_t launch_infer_dev(const Net& net, const Bounds& b, const float* records, const uint32_t* n_dev,
+                             uint64_t n_max, float* out, uint32_t* err, int sm_count, cudaStream_t s);
 // Per-tile partial gradients (tiles = ceil(n / 128), each kParams floats) and loss sums.
 cudaError_t launch_grad_tiles(const Net& net, const Bounds& b, const float* records, const float* targets, uint64_t n,
                               float grad_scale, float* partials, float* tile_loss, uint32_t* err, cudaStream_t s);

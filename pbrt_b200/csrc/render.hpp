@@ -27,15 +27,50 @@ struct WaveBuffers {
   uint32_t* counts;                    // [0] qa length, [1] qb length, [2] shadow queue length
 };
 
+// The radiance cache's side of a wave. Query mode: a path that reaches hit `term_hit` on a
+// Lambertian or metal surface stops there, and its query record (position, roughness,
+// outgoing direction, normal facing it, albedo) joins the query list; after the wave the
+// network's answer times the path's throughput is added to its radiance. Record mode
+// (training paths, never cut short): every Lambertian or metal vertex stores its record,
+// the radiance gathered before it and the throughput at it, so that once the path is done
+// (L_end - L_vertex) / beta_vertex is an unbiased sample of the radiance the vertex reflects.
+enum : uint32_t { kCacheOff = 0, kCacheQuery = 1, kCacheRecord = 2 };
+constexpr uint32_t kCacheRecordFloats = 16;
+
+struct CacheWave {
+  float* qrec;       // query records, 16 floats each (capacity = the wave size)
+  uint32_t* qpath;   // path of each query
+  float* qout;       // network output, 3 floats per query
+  float* trec;       // training vertex records, 16 floats each (capacity tcap)
+  float* tstate;     // per training vertex: radiance before it (rgb), throughput at it (rgb)
+  uint32_t* tpath;   // path of each training vertex
+  uint32_t tcap;
+  uint32_t* counts;  // [0] queries, [1] training vertices offered (may exceed tcap)
+};
+
 struct RenderSettings {
   uint32_t max_depth, rr_start, sample_offset, naive;
   unsigned long long seed;
+  uint32_t cache_mode = kCacheOff;
+  uint32_t term_hit = 0;       // query mode: the hit at which paths end into the cache
+  uint32_t random_pixels = 0;  // training paths: each path draws its pixel
 };
 
 // One wave: generate, max_depth x (extend, shade, shadow), accumulate into `film` (sums).
 cudaError_t render_wave(const SceneView& s, const WaveBuffers& w, const CameraRec& cam, uint64_t wave_base,
                         uint32_t n, uint32_t npix, const RenderSettings& rs, double* film, uint32_t* err, int sm_count,
                         cudaStream_t st);
+// The same without the accumulation, with the cache's side (cw unused when cache_mode is off).
+cudaError_t trace_wave(const SceneView& s, const WaveBuffers& w, const CacheWave& cw, const CameraRec& cam,
+                       uint64_t wave_base, uint32_t n, uint32_t npix, const RenderSettings& rs, uint32_t* err,
+                       int sm_count, cudaStream_t st);
+cudaError_t accumulate_wave(const WaveBuffers& w, uint32_t n, double* film, int sm_count, cudaStream_t st);
+// radiance[path] += beta[path] * max(network output, 0) for every query of the wave.
+cudaError_t apply_cache(const WaveBuffers& w, const CacheWave& cw, uint32_t n_max, int sm_count, cudaStream_t st);
+// A training batch of `batch` samples drawn with replacement from the m recorded vertices:
+// their records and targets (L_end - L_vertex) / beta_vertex (0 where beta is 0).
+cudaError_t train_batch(const WaveBuffers& w, const CacheWave& cw, uint32_t m, uint32_t batch, uint32_t step,
+                        unsigned long long seed, float* rec, float* tgt, int sm_count, cudaStream_t st);
 cudaError_t scale_film(double* film, size_t n, double s, int sm_count, cudaStream_t st);
 
 cudaError_t launch_scene_closest(const SceneView& s, const float* rays, uint64_t stride, uint64_t n, uint32_t* prim,

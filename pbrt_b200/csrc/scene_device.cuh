@@ -22,6 +22,7 @@ namespace pbrt {
 struct MeshShade {  // original vertices/indices, for the post-hit shading record
   const float* v;
   const uint32_t* idx;
+  const uint32_t* fmat;  // material per triangle, or NULL
 };
 
 struct SceneView {
@@ -278,6 +279,16 @@ PBRT_DEV F3 vtx(const MeshShade& m, uint32_t i) { return mk3(m.v[3 * i], m.v[3 *
 
 // World-space shading record of object `oi` hit at distance t (recomputed from the same
 // local ray and the same arithmetic as the hit itself).
+// The material of a hit: the triangle's own when its mesh carries per-face materials.
+PBRT_DEV uint32_t material_index(const SceneView& s, uint32_t oi, uint32_t prim) {
+  const ObjRec& ob = s.objects[oi];
+  if (ob.shape == kShapeMesh) {
+    const uint32_t* fm = s.shade[ob.mesh].fmat;
+    if (fm) return fm[prim];
+  }
+  return ob.material;
+}
+
 PBRT_DEV Isect interaction(const SceneView& s, uint32_t oi, uint32_t prim, const F3& o, const F3& d, float t) {
   const ObjRec& ob = s.objects[oi];
   F3 lo, ld;

@@ -212,6 +212,7 @@ bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err) {
   out->meshes.resize(d.mesh_count);
   out->mesh_v.resize(d.mesh_count);
   out->mesh_idx.resize(d.mesh_count);
+  out->mesh_fmat.resize(d.mesh_count);
   for (uint32_t i = 0; i < d.mesh_count; ++i) {
     const pbrt_mesh_desc& md = d.meshes[i];
     std::string e;
@@ -221,6 +222,14 @@ bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err) {
     }
     out->mesh_v[i].assign(md.vertices, md.vertices + 3 * size_t(md.vertex_count));
     out->mesh_idx[i].assign(md.indices, md.indices + 3 * size_t(md.triangle_count));
+    if (md.face_materials) {
+      for (uint32_t t = 0; t < md.triangle_count; ++t)
+        if (md.face_materials[t] >= d.material_count) {
+          *err = "mesh " + std::to_string(i) + ": triangle " + std::to_string(t) + " has a bad material";
+          return false;
+        }
+      out->mesh_fmat[i].assign(md.face_materials, md.face_materials + md.triangle_count);
+    }
   }
 
   for (uint32_t i = 0; i < d.material_count; ++i) {

@@ -20,6 +20,7 @@ struct FlatScene {
   std::vector<FlatMesh> meshes;
   std::vector<std::vector<float>> mesh_v;       // original vertices (shading)
   std::vector<std::vector<uint32_t>> mesh_idx;  // original indices (shading)
+  std::vector<std::vector<uint32_t>> mesh_fmat; // per-triangle material, empty when absent
   std::vector<ObjRec> objects;
   std::vector<GpuNode> top;                     // GPU numbering (root 0, padding 1)
   std::vector<uint32_t> order;                  // leaf slot -> object

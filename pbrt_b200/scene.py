@@ -138,12 +138,23 @@ class Transform:
 # Shapes, materials, objects, lights
 # ------------------------------------------------------------------------------------------
 class TriangleMesh:
-    def __init__(self, vertices, indices):
+    """Triangles sharing one BVH. `face_materials` (optional) gives each triangle its own
+    material: a list of materials and, per triangle, an index into it; the triangles then
+    ignore the material of the object that holds the mesh."""
+
+    def __init__(self, vertices, indices, face_materials=None):
         v = np.ascontiguousarray(np.asarray(vertices, np.float32).reshape(-1, 3))
         i = np.ascontiguousarray(np.asarray(indices, np.uint32).reshape(-1, 3))
         if i.shape[0] == 0:
             raise PbrtError(1, "a TriangleMesh needs at least one triangle")
         self.vertices, self.indices = v, i
+        self.face_materials = None
+        if face_materials is not None:
+            mats, per_face = face_materials
+            per_face = np.ascontiguousarray(np.asarray(per_face, np.uint32).reshape(-1))
+            if per_face.shape[0] != i.shape[0] or (per_face.size and int(per_face.max()) >= len(mats)):
+                raise PbrtError(1, "face_materials: one index per triangle into the material list")
+            self.face_materials = (list(mats), per_face)
 
     @property
     def triangle_count(self) -> int:
@@ -319,7 +330,16 @@ class Scene:
             if isinstance(shp, TriangleMesh):
                 if id(shp) not in mesh_ids:
                     mesh_ids[id(shp)] = len(meshes)
-                    meshes.append(dict(vertices=shp.vertices, indices=shp.indices))
+                    md = dict(vertices=shp.vertices, indices=shp.indices)
+                    if shp.face_materials is not None:
+                        glob = []
+                        for m in shp.face_materials[0]:
+                            if id(m) not in mat_ids:
+                                mat_ids[id(m)] = len(materials)
+                                materials.append(_material_desc(m))
+                            glob.append(mat_ids[id(m)])
+                        md["face_materials"] = np.asarray(glob, np.uint32)[shp.face_materials[1]]
+                    meshes.append(md)
                 d.update(shape=_capi.SHAPE_MESH, mesh=mesh_ids[id(shp)])
             elif isinstance(shp, Sphere):
                 d.update(shape=_capi.SHAPE_SPHERE, radius=float(shp.r))
@@ -363,7 +383,12 @@ class Scene:
             v = np.ascontiguousarray(m["vertices"], np.float32).reshape(-1, 3)
             i = np.ascontiguousarray(m["indices"], np.uint32).reshape(-1, 3)
             keep += [v, i]
-            meshes.append(_capi.MeshDesc(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0]))
+            fm = None
+            if m.get("face_materials") is not None:
+                fm = np.ascontiguousarray(m["face_materials"], np.uint32)
+                keep.append(fm)
+            meshes.append(_capi.MeshDesc(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0],
+                                         fm.ctypes.data if fm is not None else None))
         mats = []
         for m in desc["materials"]:
             d = _capi.MaterialDesc()
@@ -452,6 +477,23 @@ class Scene:
         if film is None:
             film = np.zeros((int(camera["height"]), int(camera["width"]), 3), np.float64)
         self.ctx.check(self.ctx.lib.pbrt_render(self.h, C.byref(p), _ptr(film)), "pbrt_render")
+        return film
+
+    def render_cached(self, cache, camera: dict, spp: int, max_depth: int, seed: int = 1, rr_start: int = 0,
+                      sample_offset: int = 0, train_rounds: int = 1, film=None):
+        """`train_rounds` rounds of online training of `cache` (a pbrt_b200.cache.RadianceCache),
+        then `spp` samples per pixel whose paths end into it; returns the film (None when
+        spp is 0)."""
+        self._need()
+        p = _capi.RenderParams()
+        p.camera = camera_desc(camera)
+        p.spp, p.max_depth, p.rr_start, p.sample_offset = int(spp), int(max_depth), int(rr_start), int(sample_offset)
+        p.seed, p.integrator, p.flags = int(seed), 0, 0
+        if film is None and spp > 0:
+            film = np.zeros((int(camera["height"]), int(camera["width"]), 3), np.float64)
+        self.ctx.check(self.ctx.lib.pbrt_render_cached(self.h, cache.h, C.byref(p), int(train_rounds),
+                                                       _ptr(film) if film is not None else None),
+                       "pbrt_render_cached")
         return film
 
     def release(self):

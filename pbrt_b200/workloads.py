@@ -256,3 +256,75 @@ def many_spheres(n: int = 10_000, seed: int = 3, width: int = 1024, height: int 
     camera = dict(width=width, height=height, fov=np.deg2rad(45.0), near=1e-4, far=1000.0,
                   position=(0.0, 0.6 * extent, 3.2 * extent), look_at=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0))
     return desc, camera
+
+
+def torus_knot(segments: int = 10627, sides: int = 41, p: int = 2, q: int = 3, scale: float = 0.105,
+               tube: float = 0.045, amplitude: float = 0.25, seed: int = 4):
+    """A (p, q) torus-knot tube of 2·segments·sides triangles (871,414 by default), its
+    surface displaced along the tube normal by seeded 3-octave value noise of amplitude
+    `amplitude`·tube. The knot lies in the xy plane around the origin. Faces are wound so
+    that (p2−p1)×(p1−p0) points out of the tube."""
+    t = np.arange(segments, dtype=np.float64) * (2.0 * np.pi / segments)
+    r = np.cos(q * t) + 2.0
+    c = np.stack([r * np.cos(p * t), r * np.sin(p * t), -np.sin(q * t)], 1)
+    dr = -q * np.sin(q * t)
+    d1 = np.stack([dr * np.cos(p * t) - p * r * np.sin(p * t), dr * np.sin(p * t) + p * r * np.cos(p * t),
+                   -q * np.cos(q * t)], 1)
+    ddr = -q * q * np.cos(q * t)
+    d2 = np.stack([ddr * np.cos(p * t) - 2 * p * dr * np.sin(p * t) - p * p * r * np.cos(p * t),
+                   ddr * np.sin(p * t) + 2 * p * dr * np.cos(p * t) - p * p * r * np.sin(p * t),
+                   q * q * np.sin(q * t)], 1)
+    T = d1 / np.linalg.norm(d1, axis=1, keepdims=True)
+    B = np.cross(d1, d2)  # a torus knot's curvature never vanishes: the Frenet frame is defined
+    B /= np.linalg.norm(B, axis=1, keepdims=True)
+    N = np.cross(B, T)
+    th = np.arange(sides, dtype=np.float64) * (2.0 * np.pi / sides)
+    ring = np.cos(th)[None, :, None] * N[:, None, :] + np.sin(th)[None, :, None] * B[:, None, :]
+    centre = (c * scale)[:, None, :]
+    base = centre + tube * ring
+    noise = np.zeros(segments * sides)
+    norm = 0.0
+    pts = base.reshape(-1, 3) * 20.0
+    for o in range(3):
+        a = 0.5 ** o
+        noise += a * value_noise(pts * (2 ** o), seed + 7919 * o)
+        norm += a
+    noise = 2.0 * (noise / norm) - 1.0
+    v = centre + (tube * (1.0 + amplitude * noise.reshape(segments, sides)))[:, :, None] * ring
+    v = v.reshape(-1, 3)
+    i = np.arange(segments)[:, None]
+    j = np.arange(sides)[None, :]
+    a = i * sides + j
+    b = ((i + 1) % segments) * sides + j
+    cc = ((i + 1) % segments) * sides + (j + 1) % sides
+    d = i * sides + (j + 1) % sides
+    f = np.concatenate([np.stack([a, b, cc], -1).reshape(-1, 3), np.stack([a, cc, d], -1).reshape(-1, 3)])
+    p0, p1, p2 = v[f[:, 0]], v[f[:, 1]], v[f[:, 2]]
+    n = np.cross(p2 - p1, p1 - p0)
+    mid_ring = np.concatenate([np.repeat(c * scale, sides, axis=0)] * 2)
+    inward = (n * ((p0 + p1 + p2) / 3.0 - mid_ring)).sum(1) < 0
+    f[inward] = f[inward][:, ::-1]
+    return v.astype(np.float32), f.astype(np.uint32)
+
+
+def radiance_cache_scene(width: int = 1920, height: int = 1080, segments: int = 10627, sides: int = 41,
+                         seed: int = 4):
+    """The learned-cache workload: the closed box of cornell_box (walls and ceiling light,
+    without its two inner boxes) around a displaced torus knot of 2·segments·sides
+    triangles (871,414 by default) whose faces are, seeded per quad, one of two diffuse or
+    two glossy (metal, fuzz 0.25 and 0.1) materials."""
+    desc, camera = cornell_box(width, height)
+    walls = desc["meshes"][0]
+    desc["meshes"][0] = dict(vertices=walls["vertices"][:18], indices=walls["indices"][:6])  # floor, ceiling, back
+    v, f = torus_knot(segments, sides, seed=seed)
+    v = v + np.array([0.0, -0.02, -0.08], np.float32)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    quad_mat = rng.integers(0, 4, segments * sides)
+    base = len(desc["materials"])
+    desc["materials"] += [dict(kind=0, color=(0.75, 0.45, 0.2)), dict(kind=0, color=(0.3, 0.5, 0.8)),
+                          dict(kind=1, color=(0.9, 0.75, 0.4), fuzz=0.25), dict(kind=1, color=(0.8, 0.8, 0.85), fuzz=0.1)]
+    fm = (base + np.concatenate([quad_mat, quad_mat])).astype(np.uint32)
+    desc["meshes"].append(dict(vertices=v, indices=f, face_materials=fm))
+    desc["objects"].append(dict(shape=0, mesh=len(desc["meshes"]) - 1, material=base, to_world=None, to_local=None))
+    desc["bvh_bins"], desc["bvh_max_leaf"] = 16, 4
+    return desc, camera
