@@ -17,6 +17,11 @@ stream, max over ranks). `e2e` is the same metric through the public C ABI with 
 buffers: every step copies the rays in and the ids/distances out. `--impl reference` times
 the CPU restatement of the reference's traversal (the oracle; the Rust reference cannot be
 built on this image) on all host cores.
+
+At N = 1 the line also carries `cache`: the learned radiance cache's workload (a displaced
+torus knot of 871,414 triangles in the closed box, 1920x1080), timed as seconds of device
+time for the cached and for the plain path tracer to reach relMSE 1e-3 against a deep plain
+render (see cache_race). `--no-cache-race` skips it.
 """
 from __future__ import annotations
 
@@ -124,6 +129,119 @@ def _traffic_per_launch(n_rays: int):
     return float(d["dram_bytes_per_launch"]) * n_rays / float(d["rays_per_launch"])
 
 
+# The learned-cache workload: time to relMSE 1e-3 of the cached and of the plain path tracer.
+CACHE_W, CACHE_H, CACHE_DEPTH = 1920, 1080, 32
+JUDGE_SPP, JUDGE_STRIDE, JUDGE_CHUNK = 32768, 4, 256
+TARGET = 1e-3
+PLAIN_SPP_PER_FRAME, CACHED_SPP_PER_FRAME, CACHE_WARMUP_ROUNDS = 8, 4, 50
+RACE_LIMIT_S = 90.0
+
+
+def cache_race(pb, W, ctx, device):
+    """Both arms render the full 1920x1080 image frame after frame into a running FP64 mean;
+    the error is measured on every JUDGE_STRIDE-th pixel in x and y against a plain render
+    of those pixels (same pixel footprints) with JUDGE_SPP samples. relMSE =
+    mean((x - ref)^2 / (ref^2 + 0.01)); `trimmed` drops the 0.1% largest per-pixel terms
+    (caustic fireflies of the glossy faces, which even the judge has not averaged out).
+    Times are device times (CUDA events) of the render calls, training included; error
+    evaluation is outside them."""
+    import torch
+    from pbrt_b200.cache import RadianceCache
+    from pbrt_b200.scene import film_shape
+
+    desc, cam = W.radiance_cache_scene(CACHE_W, CACHE_H)
+    scene = pb.Scene.from_description(desc, ctx).commit(bvh_bins=16, bvh_max_leaf=4)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    fshape = film_shape(cam, JUDGE_STRIDE)
+    ja = torch.zeros(fshape, dtype=torch.float64, device=device)
+    jb = torch.zeros_like(ja)
+    chunk = torch.zeros_like(ja)
+    t0 = time.perf_counter()
+    n_chunks = JUDGE_SPP // JUDGE_CHUNK
+    for k in range(n_chunks):
+        scene.render(cam, spp=JUDGE_CHUNK, max_depth=CACHE_DEPTH, seed=1000, rr_start=4,
+                     sample_offset=JUDGE_CHUNK * k, film=chunk, pixel_stride=JUDGE_STRIDE)
+        (ja if k % 2 == 0 else jb).add_(chunk)
+    ja /= n_chunks // 2
+    jb /= n_chunks // 2
+    judge = (ja + jb) / 2
+    torch.cuda.synchronize()
+    judge_s = time.perf_counter() - t0
+
+    def terms(x, ref):
+        return ((x - ref) ** 2 / (ref * ref + 1e-2)).reshape(-1)
+
+    def trimmed(e):
+        k = int(e.numel() * 0.999)
+        return float(torch.sort(e).values[:k].mean())
+
+    half = terms(ja, jb)
+    judge_err = {"raw": float(half.mean()) / 4, "trimmed": trimmed(half) / 4}
+
+    def race(frame, spp_per_frame, setup=None):
+        full = torch.zeros((CACHE_H, CACHE_W, 3), dtype=torch.float64, device=device)
+        acc = torch.zeros_like(full)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        dev_ms, n, hit, hist = 0.0, 0, None, []
+        if setup:
+            ev0.record(stream)
+            setup()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            dev_ms += ev0.elapsed_time(ev1)
+        wall0 = time.perf_counter()
+        while time.perf_counter() - wall0 < RACE_LIMIT_S:
+            ev0.record(stream)
+            frame(full, n)
+            ev1.record(stream)
+            acc.add_(full, alpha=spp_per_frame)
+            n += spp_per_frame
+            torch.cuda.synchronize()
+            dev_ms += ev0.elapsed_time(ev1)
+            e = terms(acc[::JUDGE_STRIDE, ::JUDGE_STRIDE] / n, judge)
+            tr = trimmed(e)
+            hist.append((n, dev_ms))
+            if tr <= TARGET:
+                mean = acc / n
+                hit = {"seconds": round(dev_ms / 1e3, 3), "spp": n, "relmse_trimmed": tr, "relmse_raw": float(e.mean()),
+                       "energy_bias": float(mean[::JUDGE_STRIDE, ::JUDGE_STRIDE].mean() / judge.mean() - 1.0)}
+                break
+        if hit is None:
+            mean = acc / max(n, 1)
+            e = terms(mean[::JUDGE_STRIDE, ::JUDGE_STRIDE], judge)
+            hit = {"seconds": None, "spp": n, "device_seconds_spent": round(dev_ms / 1e3, 3),
+                   "relmse_trimmed": trimmed(e), "relmse_raw": float(e.mean())}
+        hit["ms_per_spp"] = round(dev_ms / max(n, 1), 3)
+        return hit
+
+    plain = race(lambda film, n: scene.render(cam, spp=PLAIN_SPP_PER_FRAME, max_depth=CACHE_DEPTH, seed=7, rr_start=4,
+                                              sample_offset=n, film=film), PLAIN_SPP_PER_FRAME)
+    cache = RadianceCache((0, 0, 0), (0, 0, 0), seed=1, terminate_bounce=2, train_samples=1 << 16, train_steps=4,
+                          ctx=ctx)
+    cached = race(lambda film, n: scene.render_cached(cache, cam, spp=CACHED_SPP_PER_FRAME, max_depth=CACHE_DEPTH,
+                                                      seed=9, sample_offset=n, train_rounds=1, film=film),
+                  CACHED_SPP_PER_FRAME,
+                  setup=lambda: scene.render_cached(cache, cam, spp=0, max_depth=CACHE_DEPTH, seed=5,
+                                                    train_rounds=CACHE_WARMUP_ROUNDS))
+    ctx.set_stream(None)
+    speedup = None
+    if plain["seconds"] and cached["seconds"]:
+        speedup = round(plain["seconds"] / cached["seconds"], 3)
+    return {
+        "metric": "seconds to relMSE 1e-3 (trimmed: 0.1% largest per-pixel terms dropped), cached vs plain PT",
+        "workload": "displaced torus knot (871,414 triangles, glossy/diffuse per face) in the closed box with its "
+                    f"area light; {CACHE_W}x{CACHE_H}, max depth {CACHE_DEPTH}",
+        "plain": plain, "cached": cached, "speedup_plain_over_cached": speedup,
+        "plain_settings": f"path integrator, Russian roulette from bounce 4, {PLAIN_SPP_PER_FRAME} spp per frame",
+        "cached_settings": f"paths end into the cache at hit 3; per frame {CACHED_SPP_PER_FRAME} spp + 1 training "
+                           f"round (2^16 samples, 4 Adam steps, lr 1e-2); {CACHE_WARMUP_ROUNDS} warm-up rounds counted",
+        "judge": {"spp": JUDGE_SPP, "pixels": f"every {JUDGE_STRIDE}th pixel in x and y ({fshape[0] * fshape[1]})",
+                  "integrator": "plain path tracer, Russian roulette from bounce 4, FP64 film",
+                  "seconds": round(judge_s, 1), "own_error_estimate": judge_err},
+    }
+
+
 def run_reference(args, rank):
     """The CPU restatement of the reference's traversal, all host threads, one pass per step."""
     if rank != 0:
@@ -162,6 +280,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cache-race", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = _dist()
@@ -284,9 +403,11 @@ def main():
                          "peak_kind": peak_kind, "kernel": "k_mesh_closest",
                          "algorithmic_bytes_per_ray": round(bytes_per_ray, 2), "box_tests_per_ray": round(box_pr, 4),
                          "triangle_tests_per_ray": round(tri_pr, 4), "avg_launch_ms": round(launch_ms, 4)},
-            "gpu_launches": args.steps,
+            "gpu_launches": 2 * args.steps,  # per pbrt_trace_closest: the root cull and the persistent traversal
             "clocks": clocks,
         }
+        if ws == 1 and not args.no_cache_race:
+            line["cache"] = cache_race(pb, W, ctx, rays_d.device)
         if ws == 1 and not args.no_cpu_baseline:
             import oracle
 

@@ -246,11 +246,14 @@ typedef struct pbrt_render_params {
   uint32_t sample_offset; /* index of the first sample: progressive rendering, resume */
   uint64_t seed;          /* PCG32, one stream per pixel, re-keyed per (pixel, sample) */
   uint32_t integrator;    /* pbrt_integrator */
-  uint32_t flags;         /* reserved, 0 */
+  uint32_t pixel_stride;  /* 0 or 1: every pixel. s > 1: only the pixels (s*i, s*j), each rendered
+                             exactly as a full render renders it (same sample streams); the film
+                             is then ceil(width/s) x ceil(height/s) */
 } pbrt_render_params;
 
 /* Mean radiance per pixel over spp samples into film_rgb (width*height*3 doubles, row-major,
- * row 0 at the top), host or device memory; per-sample radiance is FP32, the film FP64.
+ * row 0 at the top; see pixel_stride), host or device memory; per-sample radiance is FP32,
+ * the film FP64.
  * Replaces renderers::mt::render / st::render (src/renderers/mt.rs:23-110, 112-130). */
 int pbrt_render(pbrt_scene* scene, const pbrt_render_params* params, double* film_rgb);
 
@@ -299,14 +302,19 @@ int pbrt_cache_load(pbrt_cache* cache, const void* buf, uint64_t size);
 /* Path tracing that ends paths into the learned radiance cache (an extension of
  * PathIntegrator::li, src/integrators/path.rs:48-115; the reference has no counterpart).
  * First `train_rounds` rounds of online training. A round traces max(128, train_samples / 4)
- * full-length path-integrator paths from random pixels and records each Lambertian or metal
- * vertex (at most train_samples of them) with the radiance the rest of its path gathered,
- * divided by the throughput at the vertex. It then takes train_steps Adam steps, each on
- * max(128, train_samples / train_steps) vertices drawn with replacement from the recorded ones.
+ * path-integrator paths from random pixels; each ends into the cache itself three hits after
+ * the render's cache hit (the cache's answer there closes the path), and each Lambertian or
+ * metal vertex before that (at most train_samples of them) is recorded with the radiance the
+ * rest of its path gathered, divided by the throughput at the vertex. The round then takes
+ * train_steps Adam steps, each on max(128, train_samples / train_steps) vertices drawn with
+ * replacement from the recorded ones (no step when none were recorded).
  * Then params->spp samples per pixel are rendered as pbrt_render renders them, except that a
  * path whose hit number terminate_bounce + 1 (or a later one, after a dielectric) lies on a
  * Lambertian or metal surface stops there: it takes no light sample at that hit and adds
- * its throughput times max(network output, 0). spp = 0 only trains (film may be NULL). The
+ * its throughput times the network's output clamped to [0, Lmax]. Lmax is the largest
+ * radiance an emitter of the scene gives off (diffuse-light materials, infinite lights;
+ * unbounded with a point light): no energy-conserving surface reflects more. Training
+ * targets are clamped the same way. spp = 0 only trains (film may be NULL). The
  * integrator must be PBRT_INTEGRATOR_PATH. A cache whose scene box is empty (scene_min ==
  * scene_max) takes the scene's bounds on first use. */
 int pbrt_render_cached(pbrt_scene* scene, pbrt_cache* cache, const pbrt_render_params* params, uint32_t train_rounds,

@@ -417,7 +417,8 @@ extern "C" {
   int oracle_render_cached_##SUF(void* s, const ORenderParams* p, const float* weights, const float* bounds6,  \
                                  uint32_t term_hit, double* film, int th) {                                 \
     try {                                                                                                   \
-      const CacheHook hook = cache_hook(weights, bounds6, term_hit);                                        \
+      CacheHook hook = cache_hook(weights, bounds6, term_hit);                                              \
+      hook.max_radiance = ((OScene<R>*)s)->max_radiance;                                                    \
       return render((OScene<R>*)s, p, film, th, &hook);                                                     \
     } catch (const std::exception& e) {                                                                     \
       g_err = e.what();                                                                                     \

@@ -172,6 +172,7 @@ struct ORenderParams {
 // face wo, 0, albedo, 0.
 struct CacheHook {
   uint32_t term_hit;
+  float max_radiance;  // answers are clamped to [0, max_radiance]
   std::function<void(const float* rec, float* rgb)> query;
 };
 
@@ -226,6 +227,8 @@ class OScene {
     for (uint32_t i = 0; i < d.material_count; ++i) {
       const OMaterialDesc& m = d.materials[i];
       materials.push_back(Material{m.kind, V3<R>{R(m.color[0]), R(m.color[1]), R(m.color[2])}, R(m.fuzz), R(m.ior)});
+      if (m.kind == O_MAT_DIFFUSE_LIGHT)
+        for (int c = 0; c < 3; ++c) max_radiance = std::max(max_radiance, m.color[c]);
     }
     for (uint32_t i = 0; i < d.object_count; ++i) {
       const OObjectDesc& o = d.objects[i];
@@ -256,6 +259,11 @@ class OScene {
       L.object = l.object;
       if (L.kind == O_LIGHT_AREA) setup_area(L);
       lights.push_back(L);
+      if (l.kind == O_LIGHT_POINT) max_radiance = std::numeric_limits<float>::infinity();
+      for (int c = 0; c < 3; ++c) {
+        if (l.kind == O_LIGHT_UNIFORM) max_radiance = std::max(max_radiance, l.radiance[c]);
+        if (l.kind == O_LIGHT_BACKGROUND) max_radiance = std::max(max_radiance, std::max(l.bottom[c], l.top[c]));
+      }
     }
     build_bvh();
   }
@@ -837,8 +845,9 @@ class OScene {
                                float(m.color.x), float(m.color.y), float(m.color.z), 0.f};
         float o[3];
         cache->query(rec, o);
-        L = L + V3<R>{beta.x * R(std::fmax(o[0], 0.f)), beta.y * R(std::fmax(o[1], 0.f)),
-                      beta.z * R(std::fmax(o[2], 0.f))};
+        const float mx = cache->max_radiance;
+        L = L + V3<R>{beta.x * R(std::fmin(std::fmax(o[0], 0.f), mx)), beta.y * R(std::fmin(std::fmax(o[1], 0.f), mx)),
+                      beta.z * R(std::fmin(std::fmax(o[2], 0.f), mx))};
         break;
       }
       if (!lights.empty()) {  // sample_light (path.rs:31-44)
@@ -901,6 +910,7 @@ class OScene {
     return L;
   }
 
+  float max_radiance = 0.f;  // the largest emitted radiance (+inf with a point light)
   std::vector<Mesh> meshes;
   std::vector<Object> objects;
   std::vector<Material> materials;

@@ -69,7 +69,7 @@ class CameraDesc(C.Structure):
 class RenderParams(C.Structure):
     _fields_ = [("camera", CameraDesc), ("spp", C.c_uint32), ("max_depth", C.c_uint32), ("rr_start", C.c_uint32),
                 ("sample_offset", C.c_uint32), ("seed", C.c_uint64), ("integrator", C.c_uint32),
-                ("flags", C.c_uint32)]
+                ("pixel_stride", C.c_uint32)]
 
 
 class CacheParams(C.Structure):

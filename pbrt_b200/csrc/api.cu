@@ -215,6 +215,8 @@ int pbrt_scene_create(pbrt_ctx* c, const pbrt_scene_desc* d, pbrt_scene** out) {
   v.light_cdf = (const float*)lcdf;
   s->info.object_count = d->object_count;
   s->info.device_bytes += s->extra_bytes;
+  s->max_radiance = fs.max_radiance;
+  s->has_dielectric = fs.has_dielectric;
   for (int a = 0; a < 3; ++a) {
     s->bounds[a] = fs.top[0].bmin[a];
     s->bounds[3 + a] = fs.top[0].bmax[a];
@@ -462,6 +464,10 @@ int ensure_wave(pbrt_ctx* c, WaveAlloc* wa, uint32_t cap) {
 
 WaveAlloc g_waves[kMaxDevices];  // per device; a context serialises its own calls
 
+// Training paths of the cached render go this many hits past the render's cache hit before
+// they end into the cache themselves.
+constexpr uint32_t kTrainTail = 3;
+
 int check_render_params(pbrt_ctx* c, const pbrt_render_params* p, bool allow_no_samples) {
   const pbrt_camera_desc& cd = p->camera;
   if (cd.width == 0 || cd.height == 0) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "empty image");
@@ -472,6 +478,8 @@ int check_render_params(pbrt_ctx* c, const pbrt_render_params* p, bool allow_no_
   if (!(cd.fov > 0.f) || !(cd.fov < 3.14159265f) || !(cd.far > cd.near))
     return c->fail(PBRT_ERR_INVALID_ARGUMENT, "bad camera");
   if (uint64_t(cd.width) * cd.height > 0xFFFFFFFFull) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "image too large");
+  if (p->pixel_stride > cd.width || p->pixel_stride > cd.height)
+    return c->fail(PBRT_ERR_INVALID_ARGUMENT, "pixel_stride exceeds the image");
   return PBRT_OK;
 }
 
@@ -482,7 +490,14 @@ RenderSettings settings_of(const pbrt_render_params* p) {
   rs.sample_offset = p->sample_offset;
   rs.naive = p->integrator == PBRT_INTEGRATOR_NAIVE ? 1u : 0u;
   rs.seed = p->seed;
+  rs.stride = p->pixel_stride > 1 ? p->pixel_stride : 1u;
+  rs.film_w = (p->camera.width + rs.stride - 1) / rs.stride;
   return rs;
+}
+
+// Film pixels of a render: the image's, or the strided subset's.
+uint64_t film_pixels(const pbrt_render_params* p, const RenderSettings& rs) {
+  return uint64_t(rs.film_w) * ((p->camera.height + rs.stride - 1) / rs.stride);
 }
 
 unsigned long long host_mix64(unsigned long long x) {
@@ -503,10 +518,10 @@ int pbrt_render(pbrt_scene* s, const pbrt_render_params* p, double* film) {
   if (!p || !film) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "params or film is NULL");
   PBRT_TRY(check_render_params(c, p, false));
   const pbrt_camera_desc& cd = p->camera;
-  const uint64_t npix = uint64_t(cd.width) * cd.height;
-  const uint64_t total = npix * p->spp;
   const CameraRec cam = build_camera(cd);
   const RenderSettings rs = settings_of(p);
+  const uint64_t npix = film_pixels(p, rs);
+  const uint64_t total = npix * p->spp;
 
   WaveAlloc& wa = g_waves[c->device];
   const uint32_t wave = uint32_t(std::min<uint64_t>(total, kWave));
@@ -554,10 +569,10 @@ int pbrt_render_cached(pbrt_scene* s, pbrt_cache* k, const pbrt_render_params* p
       cp.scene_max[a] = s->bounds[3 + a];
     }
   const pbrt_camera_desc& cd = p->camera;
-  const uint64_t npix = uint64_t(cd.width) * cd.height;
-  const uint64_t total = npix * p->spp;
   const CameraRec cam = build_camera(cd);
   const RenderSettings rs = settings_of(p);
+  const uint64_t npix = film_pixels(p, rs);
+  const uint64_t total = npix * p->spp;
   const uint32_t train_paths = std::max(128u, cp.train_samples / 4);
   const uint32_t steps = cp.train_steps;
   const uint32_t batch = std::max(128u, cp.train_samples / steps);
@@ -565,42 +580,51 @@ int pbrt_render_cached(pbrt_scene* s, pbrt_cache* k, const pbrt_render_params* p
 
   WaveAlloc& wa = g_waves[c->device];
   PBRT_TRY(ensure_wave(c, &wa, std::max(wave, train_paths)));
-  PBRT_TRY(k->ensure_render_buffers(wave, cp.train_samples, batch));
+  // one query per path at most: the render wave's and the training paths'
+  PBRT_TRY(k->ensure_render_buffers(std::max(wave, train_paths), cp.train_samples, batch));
   cudaStream_t st = c->work_stream();
   const CacheWave& cw = k->cw;
 
-  // online training: full-length paths from random pixels, their vertices' radiance suffixes
+  // Online training. Training paths start at random pixels, go kTrainTail hits past the
+  // render's cache hit and end into the cache there; their earlier Lambertian and metal
+  // vertices become training samples. No host synchronisation: counts stay on the device.
+  const uint32_t term_hit = cp.terminate_bounce + 1;
+  const uint32_t tail_hit = term_hit + kTrainTail;
+  const mlp::Net net{k->wfwd, k->wbwd};
+  const mlp::Bounds nb = k->bounds();
   for (uint32_t r = 0; r < train_rounds; ++r) {
     RenderSettings tr = rs;
     tr.cache_mode = kCacheRecord;
+    tr.term_hit = tail_hit;
     tr.random_pixels = 1;
     tr.sample_offset = 0;
     tr.seed = host_mix64(p->seed ^ host_mix64(0x747261696e696e67ULL + k->rounds));
-    PBRT_TRY(c->cuda(cudaMemsetAsync(cw.counts, 0, 2 * sizeof(uint32_t), st), "cudaMemset(cache counts)"));
+    if (!s->has_dielectric) tr.loop_depth = std::min(rs.max_depth, tail_hit);
+    PBRT_TRY(c->cuda(cudaMemsetAsync(cw.counts, 0, 3 * sizeof(uint32_t), st), "cudaMemset(cache counts)"));
     PBRT_TRY(c->cuda(trace_wave(s->view, wa.w, cw, cam, 0, train_paths, uint32_t(npix), tr, c->d_err, c->sm_count, st),
                      "cache training paths"));
-    uint32_t offered = 0;
-    PBRT_TRY(c->cuda(cudaMemcpyAsync(&offered, cw.counts + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st),
-                     "cudaMemcpy(cache counts)"));
-    PBRT_TRY(check_device_error(c, st));
-    const uint32_t m = std::min(offered, cw.tcap);
-    if (m > 0)
-      for (uint32_t step = 0; step < steps; ++step) {
-        PBRT_TRY(c->cuda(train_batch(wa.w, cw, m, batch, step, tr.seed, k->brec, k->btgt, c->sm_count, st),
-                         "cache training batch"));
-        PBRT_TRY(k->gradient_device(k->brec, k->btgt, batch, st));
-        PBRT_TRY(k->adam_device(st));
-      }
+    PBRT_TRY(c->cuda(mlp::launch_infer_dev(net, nb, cw.qrec, cw.counts, train_paths, cw.qout, c->d_err, c->sm_count,
+                                           st),
+                     "cache training tails"));
+    PBRT_TRY(c->cuda(apply_cache(wa.w, cw, train_paths, s->max_radiance, c->sm_count, st), "cache training tails"));
+    for (uint32_t step = 0; step < steps; ++step) {
+      PBRT_TRY(c->cuda(train_batch(wa.w, cw, batch, step, tr.seed, s->max_radiance, k->brec, k->btgt, c->sm_count, st),
+                       "cache training batch"));
+      PBRT_TRY(k->gradient_device(k->brec, k->btgt, batch, st));
+      PBRT_TRY(k->adam_device(st, cw.counts + 2));
+    }
     ++k->rounds;
   }
-  if (p->spp == 0) return check_device_error(c, st);
+  if (p->spp == 0) {
+    if (c->user) return PBRT_OK;
+    return check_device_error(c, st);
+  }
 
   // rendering: paths end into the cache at hit terminate_bounce + 1
   RenderSettings qr = rs;
   qr.cache_mode = kCacheQuery;
-  qr.term_hit = cp.terminate_bounce + 1;
-  const mlp::Net net{k->wfwd, k->wbwd};
-  const mlp::Bounds nb = k->bounds();
+  qr.term_hit = term_hit;
+  if (!s->has_dielectric) qr.loop_depth = std::min(rs.max_depth, term_hit);
   const size_t film_n = size_t(npix) * 3;
   double* dfilm = film;
   const bool host_film = mem_kind(film) != MemKind::Device;
@@ -615,8 +639,8 @@ int pbrt_render_cached(pbrt_scene* s, pbrt_cache* k, const pbrt_render_params* p
     if (rc == PBRT_OK)
       rc = c->cuda(mlp::launch_infer_dev(net, nb, cw.qrec, cw.counts, n, cw.qout, c->d_err, c->sm_count, st),
                    "cache query");
-    if (rc == PBRT_OK) rc = c->cuda(apply_cache(wa.w, cw, n, c->sm_count, st), "cache apply");
-    if (rc == PBRT_OK) rc = c->cuda(accumulate_wave(wa.w, n, dfilm, c->sm_count, st), "cached render");
+    if (rc == PBRT_OK) rc = c->cuda(apply_cache(wa.w, cw, n, s->max_radiance, c->sm_count, st), "cache apply");
+    if (rc == PBRT_OK) rc = c->cuda(accumulate_wave(wa.w, n, dfilm, cd.width, qr, c->sm_count, st), "cached render");
   }
   if (rc == PBRT_OK) rc = c->cuda(scale_film(dfilm, film_n, 1.0 / double(p->spp), c->sm_count, st), "render");
   if (host_film) {

@@ -106,10 +106,10 @@ int pbrt_cache::gradient_device(const float* records, const float* targets, uint
   return ctx->cuda(mlp::launch_reduce(partials, tile_loss, tiles, grad, loss, s), "cache gradient");
 }
 
-int pbrt_cache::adam_device(cudaStream_t s) {
+int pbrt_cache::adam_device(cudaStream_t s, const uint32_t* active) {
   ++step;
   return ctx->cuda(mlp::launch_adam(w, m, v, grad, step, params.learning_rate, params.beta1, params.beta2,
-                                    params.epsilon, wfwd, wbwd, s),
+                                    params.epsilon, wfwd, wbwd, s, active),
                    "cache adam");
 }
 
@@ -143,6 +143,7 @@ int pbrt_cache::ensure_render_buffers(uint32_t queries, uint32_t train_vertices,
   cw.tstate = reinterpret_cast<float*>(take(size_t(train_vertices) * 24));
   cw.tpath = reinterpret_cast<uint32_t*>(take(size_t(train_vertices) * 4));
   cw.tcap = train_vertices;
+  cw.qcap = queries;
   brec = reinterpret_cast<float*>(take(size_t(batch) * R));
   btgt = reinterpret_cast<float*>(take(size_t(batch) * 12));
   qcap = queries;

@@ -32,7 +32,7 @@ struct pbrt_cache {
   int reset();
   pbrt::mlp::Bounds bounds() const;
   int gradient_device(const float* records, const float* targets, uint64_t n, cudaStream_t s);
-  int adam_device(cudaStream_t s);
+  int adam_device(cudaStream_t s, const uint32_t* active = nullptr);
   int query_device(const float* records, uint64_t n, float* rgb, cudaStream_t s);
   void release();
 };

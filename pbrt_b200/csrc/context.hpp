@@ -103,6 +103,8 @@ struct pbrt_scene {
   pbrt_scene_info info{};
   int single_mesh = -1;  // index of the only (untransformed) mesh object, or -1
   float bounds[6] = {0, 0, 0, 0, 0, 0};  // world box of every object (min xyz, max xyz)
+  float max_radiance = 0.f;              // bound of reflected radiance (see FlatScene)
+  bool has_dielectric = false;
 
   int upload(void** dst, const void* src, size_t bytes) {
     if (bytes == 0) return PBRT_OK;

@@ -282,13 +282,14 @@ PBRT_DEV void write_record(float* rec, const F3& p, float rough, const F3& wo, c
 // ---- kernels ---------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_generate(WaveBuffers w, CameraRec cam, uint64_t wave_base, uint32_t n,
                                                   uint32_t npix, uint32_t sample_offset, unsigned long long seed,
-                                                  uint32_t random_pixels) {
+                                                  uint32_t random_pixels, uint32_t stride, uint32_t film_w) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint64_t g = wave_base + i;
-    uint32_t pixel = uint32_t(g % npix);
+    const uint32_t q = uint32_t(g % npix);  // film pixel
+    uint32_t pixel = (q / film_w) * stride * cam.width + (q % film_w) * stride;
     uint32_t sample = sample_offset + uint32_t(g / npix);
     if (random_pixels) {  // training paths: a pixel per path, the path's index keys its stream
-      pixel = uint32_t(splitmix64(seed + g) % npix);
+      pixel = uint32_t(splitmix64(seed + g) % (unsigned long long)(cam.width * cam.height));
       sample = uint32_t(g);
     }
     const unsigned long long inc = pcg_inc(pixel);
@@ -369,7 +370,7 @@ __global__ void __launch_bounds__(128) k_shade(WaveBuffers w, SceneView s, const
         // max_depth hits (naive.rs:29-52: li(.., 0) is black).
         const bool depth_cut = !naive && bounce == max_depth;
         const bool cacheable = m.kind == kMatLambertian || m.kind == kMatMetal;
-        if (!depth_cut && cacheable && (cache_mode == kCacheRecord || (cache_mode == kCacheQuery && bounce >= term_hit))) {
+        if (!depth_cut && cacheable && cache_mode != kCacheOff) {
           cp = it.p;
           cwo = mul3(d, -1.f);
           cn = dot3(it.n, cwo) < 0.f ? mul3(it.n, -1.f) : it.n;
@@ -377,8 +378,8 @@ __global__ void __launch_bounds__(128) k_shade(WaveBuffers w, SceneView s, const
           crough = m.kind == kMatMetal ? m.fuzz : 1.f;
           cL = L;
           cB = beta;
-          push_query = cache_mode == kCacheQuery;  // the path ends here, into the cache
-          push_train = cache_mode == kCacheRecord;
+          push_query = bounce >= term_hit;  // the path ends here, into the cache
+          push_train = cache_mode == kCacheRecord && !push_query;
         }
         if (!depth_cut && !push_query) {
           if (!naive && s.light_count > 0) {  // sample_light (path.rs:31-44) and the light sample
@@ -447,7 +448,7 @@ __global__ void __launch_bounds__(128) k_shade(WaveBuffers w, SceneView s, const
     }
     if (cache_mode != kCacheOff) {  // uniform over the grid, so the pushes see whole warps
       const uint32_t ci = warp_push(cw.counts, push_query);
-      if (push_query) {  // at most one query per path: ci < the wave size
+      if (push_query && ci < cw.qcap) {  // at most one query per path, and qcap covers the wave
         write_record(cw.qrec + size_t(ci) * kCacheRecordFloats, cp, crough, cwo, cn, calb);
         cw.qpath[ci] = p;
       }
@@ -463,21 +464,33 @@ __global__ void __launch_bounds__(128) k_shade(WaveBuffers w, SceneView s, const
   }
 }
 
-__global__ void __launch_bounds__(256) k_apply_cache(WaveBuffers w, CacheWave cw) {
-  const uint32_t n = cw.counts[0];
+// The network's answer, clamped to [0, the scene's largest emitted radiance].
+PBRT_DEV float cache_value(float o, float max_l) { return fminf(fmaxf(o, 0.f), max_l); }
+
+__global__ void __launch_bounds__(256) k_apply_cache(WaveBuffers w, CacheWave cw, uint32_t paths, float max_l) {
+  const uint32_t n = min(cw.counts[0], cw.qcap);
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const uint32_t p = cw.qpath[k];
+    if (p >= paths) continue;
     const float* o = cw.qout + 3 * size_t(k);
-    w.lr[p] = fa(w.lr[p], fm(w.br[p], fmaxf(o[0], 0.f)));
-    w.lg[p] = fa(w.lg[p], fm(w.bg[p], fmaxf(o[1], 0.f)));
-    w.lb[p] = fa(w.lb[p], fm(w.bb[p], fmaxf(o[2], 0.f)));
+    w.lr[p] = fa(w.lr[p], fm(w.br[p], cache_value(o[0], max_l)));
+    w.lg[p] = fa(w.lg[p], fm(w.bg[p], cache_value(o[1], max_l)));
+    w.lb[p] = fa(w.lb[p], fm(w.bb[p], cache_value(o[2], max_l)));
   }
 }
 
-__global__ void __launch_bounds__(256) k_train_batch(WaveBuffers w, CacheWave cw, uint32_t m, uint32_t batch,
-                                                     uint32_t step, unsigned long long seed, float* __restrict__ rec,
+__global__ void __launch_bounds__(256) k_train_batch(WaveBuffers w, CacheWave cw, uint32_t batch, uint32_t step,
+                                                     unsigned long long seed, float max_l, float* __restrict__ rec,
                                                      float* __restrict__ tgt) {
+  const uint32_t m = min(cw.counts[1], cw.tcap);
+  if (blockIdx.x == 0 && threadIdx.x == 0) cw.counts[2] = m > 0 ? 1u : 0u;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < batch; i += gridDim.x * blockDim.x) {
+    if (m == 0) {
+      float4* dst = reinterpret_cast<float4*>(rec + size_t(i) * kCacheRecordFloats);
+      dst[0] = dst[1] = dst[2] = dst[3] = make_float4(0.f, 0.f, 0.f, 0.f);
+      tgt[3 * size_t(i)] = tgt[3 * size_t(i) + 1] = tgt[3 * size_t(i) + 2] = 0.f;
+      continue;
+    }
     const uint32_t j = uint32_t(splitmix64(seed ^ ((((unsigned long long)step) << 32) | i)) % m);
     const float4* src = reinterpret_cast<const float4*>(cw.trec + size_t(j) * kCacheRecordFloats);
     float4* dst = reinterpret_cast<float4*>(rec + size_t(i) * kCacheRecordFloats);
@@ -487,7 +500,7 @@ __global__ void __launch_bounds__(256) k_train_batch(WaveBuffers w, CacheWave cw
     const float le[3] = {w.lr[p], w.lg[p], w.lb[p]};
     for (int c = 0; c < 3; ++c) {
       const float b = ts[3 + c];
-      tgt[3 * size_t(i) + c] = b > 0.f ? fdv(fs(le[c], ts[c]), b) : 0.f;
+      tgt[3 * size_t(i) + c] = b > 0.f ? cache_value(fdv(fs(le[c], ts[c]), b), max_l) : 0.f;
     }
   }
 }
@@ -505,9 +518,11 @@ __global__ void __launch_bounds__(128) k_shadow(WaveBuffers w, SceneView s, uint
   }
 }
 
-__global__ void __launch_bounds__(256) k_accumulate(WaveBuffers w, uint32_t n, double* __restrict__ film) {
+__global__ void __launch_bounds__(256) k_accumulate(WaveBuffers w, uint32_t n, double* __restrict__ film,
+                                                    uint32_t image_w, uint32_t stride, uint32_t film_w) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t pix = w.pixel[i];
+    const uint32_t px = w.pixel[i];
+    const uint32_t pix = stride == 1 ? px : ((px / image_w) / stride) * film_w + (px % image_w) / stride;
     atomicAdd(film + 3 * size_t(pix), double(w.lr[i]));
     atomicAdd(film + 3 * size_t(pix) + 1, double(w.lg[i]));
     atomicAdd(film + 3 * size_t(pix) + 2, double(w.lb[i]));
@@ -571,10 +586,12 @@ cudaError_t trace_wave(const SceneView& s, const WaveBuffers& w, const CacheWave
                        int sm_count, cudaStream_t st) {
   cudaError_t e;
   k_generate<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, cam, wave_base, n, npix, rs.sample_offset, rs.seed,
-                                                             rs.random_pixels);
+                                                             rs.random_pixels, rs.stride,
+                                                             rs.film_w ? rs.film_w : cam.width);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const unsigned g128 = unsigned(sm_count) * 16;
-  for (uint32_t b = 0; b < rs.max_depth; ++b) {
+  const uint32_t loops = rs.loop_depth ? rs.loop_depth : rs.max_depth;
+  for (uint32_t b = 0; b < loops; ++b) {
     uint32_t* qin = (b & 1) ? w.qb : w.qa;
     uint32_t* qout = (b & 1) ? w.qa : w.qb;
     uint32_t* cin = w.counts + (b & 1);
@@ -590,8 +607,10 @@ cudaError_t trace_wave(const SceneView& s, const WaveBuffers& w, const CacheWave
   return cudaSuccess;
 }
 
-cudaError_t accumulate_wave(const WaveBuffers& w, uint32_t n, double* film, int sm_count, cudaStream_t st) {
-  k_accumulate<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, n, film);
+cudaError_t accumulate_wave(const WaveBuffers& w, uint32_t n, double* film, uint32_t image_w, const RenderSettings& rs,
+                            int sm_count, cudaStream_t st) {
+  k_accumulate<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, n, film, image_w, rs.stride,
+                                                               rs.film_w ? rs.film_w : image_w);
   return cudaGetLastError();
 }
 
@@ -602,18 +621,19 @@ cudaError_t render_wave(const SceneView& s, const WaveBuffers& w, const CameraRe
   plain.cache_mode = kCacheOff;
   const cudaError_t e = trace_wave(s, w, CacheWave{}, cam, wave_base, n, npix, plain, err, sm_count, st);
   if (e != cudaSuccess) return e;
-  return accumulate_wave(w, n, film, sm_count, st);
+  return accumulate_wave(w, n, film, cam.width, rs, sm_count, st);
 }
 
-cudaError_t apply_cache(const WaveBuffers& w, const CacheWave& cw, uint32_t n_max, int sm_count, cudaStream_t st) {
-  k_apply_cache<<<grid_cap(n_max, 256, sm_count, 8), 256, 0, st>>>(w, cw);
+cudaError_t apply_cache(const WaveBuffers& w, const CacheWave& cw, uint32_t n, float max_l, int sm_count,
+                        cudaStream_t st) {
+  k_apply_cache<<<grid_cap(n, 256, sm_count, 8), 256, 0, st>>>(w, cw, n, max_l);
   return cudaGetLastError();
 }
 
-cudaError_t train_batch(const WaveBuffers& w, const CacheWave& cw, uint32_t m, uint32_t batch, uint32_t step,
-                        unsigned long long seed, float* rec, float* tgt, int sm_count, cudaStream_t st) {
-  if (m == 0 || batch == 0) return cudaSuccess;
-  k_train_batch<<<grid_cap(batch, 256, sm_count, 8), 256, 0, st>>>(w, cw, m, batch, step, seed, rec, tgt);
+cudaError_t train_batch(const WaveBuffers& w, const CacheWave& cw, uint32_t batch, uint32_t step,
+                        unsigned long long seed, float max_l, float* rec, float* tgt, int sm_count, cudaStream_t st) {
+  if (batch == 0) return cudaSuccess;
+  k_train_batch<<<grid_cap(batch, 256, sm_count, 8), 256, 0, st>>>(w, cw, batch, step, seed, max_l, rec, tgt);
   return cudaGetLastError();
 }
 

@@ -351,9 +351,10 @@ __device__ __forceinline__ void pack_one(uint32_t p, float w, uint16_t* fwd, uin
 
 __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
                        const float* __restrict__ grad, float c1, float c2, float lr, float b1, float b2, float eps,
-                       uint16_t* fwd, uint16_t* bwd) {
+                       uint16_t* fwd, uint16_t* bwd, const uint32_t* __restrict__ active) {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= uint32_t(kParams)) return;
+  if (active && *active == 0) return;  // no training data this step
   // Rounded operations spelled out (no contraction) so the step is reproducible on the host.
   const float g = grad[p];
   const float mm = __fadd_rn(__fmul_rn(b1, m[p]), __fmul_rn(1.0f - b1, g));
@@ -417,9 +418,11 @@ cudaError_t launch_reduce(const float* partials, const float* tile_loss, uint32_
 }
 
 cudaError_t launch_adam(float* w, float* m, float* v, const float* grad, uint32_t step, float lr, float beta1,
-                        float beta2, float eps, uint16_t* wpk_fwd, uint16_t* wpk_bwd, cudaStream_t s) {
+                        float beta2, float eps, uint16_t* wpk_fwd, uint16_t* wpk_bwd, cudaStream_t s,
+                        const uint32_t* active) {
   const float c1 = 1.0f - powf(beta1, float(step)), c2 = 1.0f - powf(beta2, float(step));
-  k_adam<<<(kParams + 255) / 256, 256, 0, s>>>(w, m, v, grad, c1, c2, lr, beta1, beta2, eps, wpk_fwd, wpk_bwd);
+  k_adam<<<(kParams + 255) / 256, 256, 0, s>>>(w, m, v, grad, c1, c2, lr, beta1, beta2, eps, wpk_fwd, wpk_bwd,
+                                               active);
   return cudaGetLastError();
 }
 

@@ -46,9 +46,11 @@ cudaError_t launch_grad_tiles(const Net& net, const Bounds& b, const float* reco
 // grad[p] = sum over tiles of partials; loss[0] = sum of tile losses.
 cudaError_t launch_reduce(const float* partials, const float* tile_loss, uint32_t tiles, float* grad, float* loss,
                           cudaStream_t s);
-// One Adam step on the FP32 master weights, then the BF16 packs are rewritten.
+// One Adam step on the FP32 master weights, then the BF16 packs are rewritten; skipped
+// entirely when `active` is given and *active == 0.
 cudaError_t launch_adam(float* w, float* m, float* v, const float* grad, uint32_t step, float lr, float beta1,
-                        float beta2, float eps, uint16_t* wpk_fwd, uint16_t* wpk_bwd, cudaStream_t s);
+                        float beta2, float eps, uint16_t* wpk_fwd, uint16_t* wpk_bwd, cudaStream_t s,
+                        const uint32_t* active = nullptr);
 cudaError_t launch_pack(const float* w, uint16_t* wpk_fwd, uint16_t* wpk_bwd, cudaStream_t s);
 
 size_t infer_smem_bytes();

@@ -31,32 +31,38 @@ struct WaveBuffers {
 // Lambertian or metal surface stops there, and its query record (position, roughness,
 // outgoing direction, normal facing it, albedo) joins the query list; after the wave the
 // network's answer times the path's throughput is added to its radiance. Record mode
-// (training paths, never cut short): every Lambertian or metal vertex stores its record,
-// the radiance gathered before it and the throughput at it, so that once the path is done
-// (L_end - L_vertex) / beta_vertex is an unbiased sample of the radiance the vertex reflects.
+// (training paths): the same, with `term_hit` further along the path, and before that
+// every Lambertian or metal vertex stores its record, the radiance gathered before it and
+// the throughput at it, so that once the path (and its tail query) is done,
+// (L_end - L_vertex) / beta_vertex is the radiance sample the vertex is trained towards.
 enum : uint32_t { kCacheOff = 0, kCacheQuery = 1, kCacheRecord = 2 };
 constexpr uint32_t kCacheRecordFloats = 16;
 
 struct CacheWave {
-  float* qrec;       // query records, 16 floats each (capacity = the wave size)
+  float* qrec;       // query records, 16 floats each (capacity qcap)
   uint32_t* qpath;   // path of each query
   float* qout;       // network output, 3 floats per query
   float* trec;       // training vertex records, 16 floats each (capacity tcap)
   float* tstate;     // per training vertex: radiance before it (rgb), throughput at it (rgb)
   uint32_t* tpath;   // path of each training vertex
-  uint32_t tcap;
-  uint32_t* counts;  // [0] queries, [1] training vertices offered (may exceed tcap)
+  uint32_t qcap, tcap;
+  uint32_t* counts;  // [0] queries, [1] training vertices offered (may exceed tcap), [2] batch valid
 };
 
 struct RenderSettings {
   uint32_t max_depth, rr_start, sample_offset, naive;
   unsigned long long seed;
   uint32_t cache_mode = kCacheOff;
-  uint32_t term_hit = 0;       // query mode: the hit at which paths end into the cache
+  uint32_t term_hit = 0;       // the hit at which paths end into the cache
   uint32_t random_pixels = 0;  // training paths: each path draws its pixel
+  uint32_t loop_depth = 0;     // bounce iterations the host launches (0: max_depth); no path
+                               // may still be alive after them
+  uint32_t stride = 1;         // film pixel (i, j) is image pixel (stride*i, stride*j)
+  uint32_t film_w = 0;         // film columns (0: the image width)
 };
 
 // One wave: generate, max_depth x (extend, shade, shadow), accumulate into `film` (sums).
+// `npix` is the number of film pixels (the image's, or the strided subset's).
 cudaError_t render_wave(const SceneView& s, const WaveBuffers& w, const CameraRec& cam, uint64_t wave_base,
                         uint32_t n, uint32_t npix, const RenderSettings& rs, double* film, uint32_t* err, int sm_count,
                         cudaStream_t st);
@@ -64,13 +70,18 @@ cudaError_t render_wave(const SceneView& s, const WaveBuffers& w, const CameraRe
 cudaError_t trace_wave(const SceneView& s, const WaveBuffers& w, const CacheWave& cw, const CameraRec& cam,
                        uint64_t wave_base, uint32_t n, uint32_t npix, const RenderSettings& rs, uint32_t* err,
                        int sm_count, cudaStream_t st);
-cudaError_t accumulate_wave(const WaveBuffers& w, uint32_t n, double* film, int sm_count, cudaStream_t st);
-// radiance[path] += beta[path] * max(network output, 0) for every query of the wave.
-cudaError_t apply_cache(const WaveBuffers& w, const CacheWave& cw, uint32_t n_max, int sm_count, cudaStream_t st);
-// A training batch of `batch` samples drawn with replacement from the m recorded vertices:
-// their records and targets (L_end - L_vertex) / beta_vertex (0 where beta is 0).
-cudaError_t train_batch(const WaveBuffers& w, const CacheWave& cw, uint32_t m, uint32_t batch, uint32_t step,
-                        unsigned long long seed, float* rec, float* tgt, int sm_count, cudaStream_t st);
+cudaError_t accumulate_wave(const WaveBuffers& w, uint32_t n, double* film, uint32_t image_w, const RenderSettings& rs,
+                            int sm_count, cudaStream_t st);
+// radiance[path] += beta[path] * clamp(network output, 0, max_l) for every query of a wave of
+// n paths (queries beyond qcap were never written; path indices >= n are skipped).
+cudaError_t apply_cache(const WaveBuffers& w, const CacheWave& cw, uint32_t n, float max_l, int sm_count,
+                        cudaStream_t st);
+// A training batch of `batch` samples drawn with replacement from the m = min(counts[1],
+// tcap) recorded vertices (m read on the device): their records and targets
+// clamp((L_end - L_vertex) / beta_vertex, 0, max_l) (0 where beta is 0). Sets counts[2] to
+// 1 when m > 0, else 0 (and the batch is all zeros).
+cudaError_t train_batch(const WaveBuffers& w, const CacheWave& cw, uint32_t batch, uint32_t step,
+                        unsigned long long seed, float max_l, float* rec, float* tgt, int sm_count, cudaStream_t st);
 cudaError_t scale_film(double* film, size_t n, double s, int sm_count, cudaStream_t st);
 
 cudaError_t launch_scene_closest(const SceneView& s, const float* rays, uint64_t stride, uint64_t n, uint32_t* prim,

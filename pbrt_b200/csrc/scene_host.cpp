@@ -241,6 +241,9 @@ bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err) {
     r.ior = m.ior;
     for (int c = 0; c < 3; ++c) r.color[c] = m.color[c];
     out->materials.push_back(r);
+    if (m.kind == PBRT_MAT_DIFFUSE_LIGHT)
+      for (int c = 0; c < 3; ++c) out->max_radiance = std::max(out->max_radiance, m.color[c]);
+    if (m.kind == PBRT_MAT_DIELECTRIC) out->has_dielectric = true;
   }
 
   std::vector<Box3> boxes(d.object_count);
@@ -346,6 +349,12 @@ bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err) {
       if (!(r.area > 0.0f)) { *err = "light " + std::to_string(i) + ": zero area"; return false; }
     }
     out->lights.push_back(r);
+    if (l.kind == PBRT_LIGHT_POINT) out->max_radiance = INFINITY;
+    for (int c = 0; c < 3; ++c) {
+      if (l.kind == PBRT_LIGHT_UNIFORM_INFINITE) out->max_radiance = std::max(out->max_radiance, l.radiance[c]);
+      if (l.kind == PBRT_LIGHT_BACKGROUND_INFINITE)
+        out->max_radiance = std::max(out->max_radiance, std::max(l.bottom[c], l.top[c]));
+    }
   }
   return true;
 }

@@ -29,6 +29,10 @@ struct FlatScene {
   std::vector<LightRec> lights;
   std::vector<float> light_tris;                // 9 floats per area-light triangle (world space)
   std::vector<float> light_cdf;                 // running area per area-light triangle
+  // The largest radiance any emitter gives off (diffuse-light materials, infinite lights);
+  // +inf with a point light. With energy-conserving materials no surface reflects more.
+  float max_radiance = 0.f;
+  bool has_dielectric = false;  // a dielectric lets paths go on past a cache hit
 };
 
 bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err);

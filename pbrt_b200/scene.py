@@ -467,20 +467,22 @@ class Scene:
         return occ
 
     def render(self, camera: dict, spp: int, max_depth: int, seed: int = 1, rr_start: int = 0,
-               sample_offset: int = 0, integrator: str = "path", film=None):
-        """Mean radiance per pixel, (height, width, 3) float64; `film` may be a CUDA tensor."""
+               sample_offset: int = 0, integrator: str = "path", film=None, pixel_stride: int = 1):
+        """Mean radiance per pixel, (height, width, 3) float64; `film` may be a CUDA tensor.
+        pixel_stride s > 1 renders only the pixels (s*i, s*j), exactly as a full render does,
+        into a (ceil(height/s), ceil(width/s), 3) film."""
         self._need()
         p = _capi.RenderParams()
         p.camera = camera_desc(camera)
         p.spp, p.max_depth, p.rr_start, p.sample_offset = int(spp), int(max_depth), int(rr_start), int(sample_offset)
-        p.seed, p.integrator, p.flags = int(seed), 1 if integrator == "naive" else 0, 0
+        p.seed, p.integrator, p.pixel_stride = int(seed), 1 if integrator == "naive" else 0, int(pixel_stride)
         if film is None:
-            film = np.zeros((int(camera["height"]), int(camera["width"]), 3), np.float64)
+            film = np.zeros(film_shape(camera, pixel_stride), np.float64)
         self.ctx.check(self.ctx.lib.pbrt_render(self.h, C.byref(p), _ptr(film)), "pbrt_render")
         return film
 
     def render_cached(self, cache, camera: dict, spp: int, max_depth: int, seed: int = 1, rr_start: int = 0,
-                      sample_offset: int = 0, train_rounds: int = 1, film=None):
+                      sample_offset: int = 0, train_rounds: int = 1, film=None, pixel_stride: int = 1):
         """`train_rounds` rounds of online training of `cache` (a pbrt_b200.cache.RadianceCache),
         then `spp` samples per pixel whose paths end into it; returns the film (None when
         spp is 0)."""
@@ -488,9 +490,9 @@ class Scene:
         p = _capi.RenderParams()
         p.camera = camera_desc(camera)
         p.spp, p.max_depth, p.rr_start, p.sample_offset = int(spp), int(max_depth), int(rr_start), int(sample_offset)
-        p.seed, p.integrator, p.flags = int(seed), 0, 0
+        p.seed, p.integrator, p.pixel_stride = int(seed), 0, int(pixel_stride)
         if film is None and spp > 0:
-            film = np.zeros((int(camera["height"]), int(camera["width"]), 3), np.float64)
+            film = np.zeros(film_shape(camera, pixel_stride), np.float64)
         self.ctx.check(self.ctx.lib.pbrt_render_cached(self.h, cache.h, C.byref(p), int(train_rounds),
                                                        _ptr(film) if film is not None else None),
                        "pbrt_render_cached")
@@ -506,6 +508,12 @@ class Scene:
             self.release()
         except Exception:
             pass
+
+
+def film_shape(camera: dict, pixel_stride: int = 1):
+    """(rows, columns, 3) of the film a render with this camera and pixel stride fills."""
+    s = max(1, int(pixel_stride))
+    return (-(-int(camera["height"]) // s), -(-int(camera["width"]) // s), 3)
 
 
 def film_to_rgba8(film: np.ndarray) -> np.ndarray:

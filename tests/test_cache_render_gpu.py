@@ -80,15 +80,21 @@ def test_cached_render_matches_oracle(cornell, trained):
 
 def test_trained_cache_gain(cornell, trained):
     desc, cam, scene = cornell
-    judge = scene.render(cam, spp=2048, max_depth=16, seed=99)
-    spp = 8
-    cached = scene.render_cached(trained, cam, spp=spp, max_depth=16, seed=3, train_rounds=0)
-    cut = scene.render(cam, spp=spp, max_depth=TERM + 1, seed=3)
-    plain = scene.render(cam, spp=spp, max_depth=16, seed=3)
-    e_cached, e_cut, e_plain = relmse(cached, judge), relmse(cut, judge), relmse(plain, judge)
-    print(f"relMSE at {spp} spp: cached {e_cached:.3e}  cut without the network {e_cut:.3e}  plain {e_plain:.3e}")
-    assert e_cached < 0.25 * e_cut
-    assert e_cached < e_plain
+    judge = scene.render(cam, spp=4096, max_depth=16, seed=99)
+    out = {}
+    for spp in (8, 256):
+        cached = scene.render_cached(trained, cam, spp=spp, max_depth=16, seed=3, train_rounds=0)
+        cut = scene.render(cam, spp=spp, max_depth=TERM + 1, seed=3)
+        plain = scene.render(cam, spp=spp, max_depth=16, seed=3)
+        out[spp] = {k: (relmse(v, judge), float(v.mean() / judge.mean() - 1.0))
+                    for k, v in (("cached", cached), ("cut", cut), ("plain", plain))}
+        print(spp, "spp: relMSE / energy bias", out[spp])
+    # energy: pixel noise averages out over the image, what remains is bias
+    b = out[256]
+    assert abs(b["cached"][1]) < 0.25 * abs(b["cut"][1])
+    # the cut paths' missing light dominates their error; the network brings it back
+    assert b["cached"][0] < 0.5 * b["cut"][0]
+    assert out[8]["cached"][0] < out[8]["plain"][0]
 
 
 def test_rejects_naive_integrator_and_foreign_cache(cornell):

@@ -134,3 +134,19 @@ def test_progressive_samples_and_device_film():
     film = torch.zeros((32, 32, 3), dtype=torch.float64, device="cuda")
     s.render(cam, spp=8, max_depth=8, seed=2, film=film)
     assert np.array_equal(film.cpu().numpy(), a)
+
+
+@pytest.mark.parametrize("stride", [3, 4])
+def test_pixel_stride_renders_the_same_pixels(stride):
+    from pbrt_b200.cache import RadianceCache
+    from pbrt_b200.scene import film_shape
+    desc, cam = W.cornell_box(64, 50)
+    scene = pb.Scene.from_description(desc).commit()
+    full = scene.render(cam, spp=4, max_depth=6, seed=3, rr_start=3)
+    sub = scene.render(cam, spp=4, max_depth=6, seed=3, rr_start=3, pixel_stride=stride)
+    assert sub.shape == film_shape(cam, stride)
+    np.testing.assert_array_equal(sub, full[::stride, ::stride])
+    cache = RadianceCache((-0.5, -0.5, -0.5), (0.5, 0.5, 0.5), seed=2)
+    cfull = scene.render_cached(cache, cam, spp=4, max_depth=6, seed=3, train_rounds=0)
+    csub = scene.render_cached(cache, cam, spp=4, max_depth=6, seed=3, train_rounds=0, pixel_stride=stride)
+    np.testing.assert_array_equal(csub, cfull[::stride, ::stride])
