@@ -55,57 +55,76 @@ def _dist():
 
 
 class ClockSampler:
-    """Samples SM clocks and throttle reasons with nvidia-smi while the timed region runs."""
+    """Samples the SM clock and the clock-event (throttle) reasons every 5 ms while the timed
+    region runs, through NVML (read-only queries); nvidia-smi is the fallback."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+               "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+               "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+               "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
 
     def __init__(self, gpu: int):
         self.gpu = gpu
-        self.lines = []
-        self.proc = None
+        self.sm, self.reasons, self.smax = [], set(), None
+        self.stop_flag = threading.Event()
         self.t = None
+        self.nv = None
+        self.h = None
+
+    def _handle(self):
+        import pynvml as nv
+
+        nv.nvmlInit()
+        self.nv = nv
+        try:
+            import torch
+
+            p = torch.cuda.get_device_properties(self.gpu)
+            bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.gpu)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            self.h = self._handle()
+            self.smax = self.nv.nvmlDeviceGetMaxClockInfo(self.h, self.nv.NVML_CLOCK_SM)
         except Exception:
-            self.proc = None
+            self.h = None
+            return
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        nv = self.nv
+        masks = {k: getattr(nv, v, 0) for k, v in self.REASONS.items()}
+        while not self.stop_flag.is_set():
+            try:
+                self.sm.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for k, m in masks.items():
+                    if m and (r & m):
+                        self.reasons.add(k)
+            except Exception:
+                pass
+            self.stop_flag.wait(0.005)
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
+        if self.h is None:
+            return self._smi()
+        self.stop_flag.set()
         self.t.join(timeout=2)
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 8:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                smax.append(float(parts[1]))
-            except ValueError:
-                continue
-            for nm, val in zip(names, parts[4:8]):
-                if val.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.smax,
+                "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "nvml, 5 ms"}
+
+    def _smi(self):
+        try:
+            out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=clocks.sm,clocks.max.sm",
+                                  "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=10).stdout
+            sm, smax = [float(x) for x in out.strip().split(",")[:2]]
+            return {"sm_mhz": sm, "sm_max_mhz": smax, "reasons": [], "samples": 1, "source": "nvidia-smi, after"}
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"], "samples": 0}
 
 
 def _peaks():
@@ -215,6 +234,8 @@ def cache_race(pb, W, ctx, device):
         hit["ms_per_spp"] = round(dev_ms / max(n, 1), 3)
         return hit
 
+    sampler = ClockSampler(device.index or 0)
+    sampler.start()
     plain = race(lambda film, n: scene.render(cam, spp=PLAIN_SPP_PER_FRAME, max_depth=CACHE_DEPTH, seed=7, rr_start=4,
                                               sample_offset=n, film=film), PLAIN_SPP_PER_FRAME)
     cache = RadianceCache((0, 0, 0), (0, 0, 0), seed=1, terminate_bounce=2, train_samples=1 << 16, train_steps=4,
@@ -224,6 +245,7 @@ def cache_race(pb, W, ctx, device):
                   CACHED_SPP_PER_FRAME,
                   setup=lambda: scene.render_cached(cache, cam, spp=0, max_depth=CACHE_DEPTH, seed=5,
                                                     train_rounds=CACHE_WARMUP_ROUNDS))
+    clocks = sampler.stop()
     ctx.set_stream(None)
     speedup = None
     if plain["seconds"] and cached["seconds"]:
@@ -239,7 +261,76 @@ def cache_race(pb, W, ctx, device):
         "judge": {"spp": JUDGE_SPP, "pixels": f"every {JUDGE_STRIDE}th pixel in x and y ({fshape[0] * fshape[1]})",
                   "integrator": "plain path tracer, Russian roulette from bounce 4, FP64 film",
                   "seconds": round(judge_s, 1), "own_error_estimate": judge_err},
+        "clocks": clocks,
     }
+
+
+MLP_FLOP_PER_QUERY = 2 * (96 * 64 + 4 * 64 * 64 + 64 * 3)  # 45,440: forward multiply-adds x 2
+MLP_QUERIES, MLP_TRAIN_BATCH = 1 << 22, 1 << 14
+
+
+def run_mlp(args, local):
+    """The radiance cache's network alone: inference over 2^22 device-resident query records
+    and Adam steps on training batches of 2^14 samples (the size one step of a training
+    round takes), device time with CUDA events. Prints one JSON line."""
+    import torch
+
+    import pbrt_b200 as pb
+    from pbrt_b200.cache import RadianceCache, random_records
+
+    torch.cuda.set_device(local)
+    ctx = pb.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    cache = RadianceCache((-1, -1, -1), (1, 1, 1), seed=1, ctx=ctx)
+    dev = torch.device("cuda", local)
+    rec = torch.from_numpy(random_records(MLP_QUERIES, (-1, -1, -1), (1, 1, 1), seed=3)).to(dev)
+    out = torch.empty((MLP_QUERIES, 3), dtype=torch.float32, device=dev)
+    tgt = torch.rand((MLP_TRAIN_BATCH, 3), dtype=torch.float32, device=dev)
+    lib = ctx.lib
+
+    def query():
+        ctx.check(lib.pbrt_cache_query(cache.h, rec.data_ptr(), MLP_QUERIES, out.data_ptr()), "pbrt_cache_query")
+
+    def train():
+        ctx.check(lib.pbrt_cache_train_step(cache.h, rec.data_ptr(), tgt.data_ptr(), MLP_TRAIN_BATCH, None),
+                  "pbrt_cache_train_step")
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        total = 0.0
+        for _ in range(args.steps):
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            total += e0.elapsed_time(e1)
+        return total / args.steps
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    q_ms = timed(query)
+    t_ms = timed(train)
+    clocks = sampler.stop()
+    with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+        peak = float(json.load(f)["bf16_tflops"])
+    tflops = MLP_FLOP_PER_QUERY * MLP_QUERIES / (q_ms * 1e-3) / 1e12
+    line = {"metric": "radiance-cache network inference", "value": round(MLP_QUERIES / (q_ms * 1e-3) / 1e6, 2),
+            "unit": "Mqueries/s", "ms_per_step": round(q_ms, 4), "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "bf16 (fp32 accumulate)", "data": "synthetic",
+            "config": {"workload": f"{MLP_QUERIES} query records, 82->96 x 64^5 x 3(->16) ReLU MLP",
+                       "flop_per_query": MLP_FLOP_PER_QUERY},
+            "roofline": {"bound": "tensor", "achieved": round(tflops, 2), "peak": peak, "unit": "TFLOP/s",
+                         "frac": round(tflops / peak, 4), "peak_kind": "measured burst bf16", "kernel": "k_mlp_infer"},
+            "train_step": {"samples": MLP_TRAIN_BATCH, "ms": round(t_ms, 4),
+                           "samples_per_s": round(MLP_TRAIN_BATCH / (t_ms * 1e-3), 1),
+                           "includes": "forward + backward (tcgen05 data gradients, CUDA-core weight gradients), "
+                                       "tile reduction, Adam"},
+            "clocks": clocks}
+    print(json.dumps(line), flush=True)
 
 
 def run_reference(args, rank):
@@ -274,6 +365,7 @@ def run_reference(args, rank):
 
 
 def main():
+    global N_RAYS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
@@ -281,9 +373,16 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cache-race", action="store_true")
+    ap.add_argument("--rays", type=int, default=N_RAYS, help="rays per step (smaller cases for profiling)")
+    ap.add_argument("--workload", default="raycast", choices=["raycast", "mlp"],
+                    help="mlp: the radiance cache's network alone (not the headline line)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = _dist()
+    N_RAYS = args.rays
+    if args.workload == "mlp":
+        run_mlp(args, local)
+        return
 
     if args.impl == "reference":
         run_reference(args, rank)
@@ -327,8 +426,6 @@ def main():
         if rc != 0:
             ctx.check(rc, "pbrt_trace_closest")
 
-    sampler = ClockSampler(local)
-    sampler.start()
     for _ in range(args.warmup):
         step()
     ctx.sync()
@@ -336,6 +433,8 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     ev[0].record(stream)
     for k in range(args.steps):
@@ -343,12 +442,12 @@ def main():
         ev[k + 1].record(stream)
     torch.cuda.synchronize()
     ctx.sync()
+    clocks = sampler.stop()
     per_launch = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
     total_ms = ev[0].elapsed_time(ev[-1])
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = sampler.stop()
     tt = torch.tensor([total_ms], device=rays_d.device)
     if dist:
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
