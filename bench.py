@@ -265,6 +265,65 @@ def cache_race(pb, W, ctx, device):
     }
 
 
+# Path-tracing workloads timed beside the headline (configs 0 and 2) and for profiling.
+RENDER_CASES = {
+    "c0": ("closed box of triangles (34 triangles, quad area light), 256x256, 16 spp, max depth 8, no roulette",
+           lambda W: W.cornell_box(256, 256), dict(spp=16, max_depth=8, rr_start=0)),
+    "c2": ("10,000 non-overlapping spheres (Lambertian / metal / dielectric thirds), sky gradient + sphere light, "
+           "1024x768, 64 spp, max depth 16, roulette from bounce 4",
+           lambda W: W.many_spheres(10000, width=1024, height=768), dict(spp=64, max_depth=16, rr_start=4)),
+    "c4": ("displaced torus knot (871,414 triangles) in the closed box, 1920x1080, 4 spp, max depth 32, roulette "
+           "from bounce 4", lambda W: W.radiance_cache_scene(1920, 1080), dict(spp=4, max_depth=32, rr_start=4)),
+}
+
+
+def render_case(pb, W, ctx, case, reps=3, cpu=False, nvtx=False):
+    """Device time of one full render of a path-tracing workload (CUDA events on the
+    context's stream, after one warm-up render), with the rays it traced."""
+    import torch
+
+    what, make, kw = RENDER_CASES[case]
+    desc, cam = make(W)
+    scene = pb.Scene.from_description(desc, ctx).commit(bvh_bins=desc.get("bvh_bins", 8),
+                                                       bvh_max_leaf=desc.get("bvh_max_leaf", 1))
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    film = torch.zeros((cam["height"], cam["width"], 3), dtype=torch.float64, device="cuda")
+    scene.render(cam, seed=1, film=film, **kw)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if nvtx:
+        torch.cuda.nvtx.range_push("frame")
+    e0.record(stream)
+    for r in range(reps):
+        scene.render(cam, seed=2 + r, film=film, **kw)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if nvtx:
+        torch.cuda.nvtx.range_pop()
+    ms = e0.elapsed_time(e1) / reps
+    st = ctx.render_stats()
+    ctx.set_stream(None)
+    samples = cam["width"] * cam["height"] * kw["spp"]
+    rays = st["rays"] + st["shadow_rays"]
+    out = {"workload": what, "ms_per_frame": round(ms, 3), "samples_per_s": round(samples / (ms * 1e-3), 1),
+           "mrays_per_s": round(rays / (ms * 1e-3) / 1e6, 2), "rays_per_path": round(st["rays"] / st["paths"], 3),
+           "shadow_rays_per_path": round(st["shadow_rays"] / st["paths"], 3)}
+    if cpu:
+        import oracle
+
+        threads = os.cpu_count() or 1
+        o = oracle.Scene(desc, np.float32)
+        t0 = time.perf_counter()
+        o.render(cam, 1, kw["max_depth"], seed=1, rr_start=kw["rr_start"], threads=threads)
+        cs = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(cam["width"] * cam["height"] / cs, 1), "unit": "samples/s",
+                               "cores": threads, "kind": "port",
+                               "sample": "1 spp of the same image, FP32 C++ restatement of the reference's path "
+                                         "integrator and scene traversal (oracle), all host threads"}
+    return out
+
+
 MLP_FLOP_PER_QUERY = 2 * (96 * 64 + 4 * 64 * 64 + 64 * 3)  # 45,440: forward multiply-adds x 2
 MLP_QUERIES, MLP_TRAIN_BATCH = 1 << 22, 1 << 14
 
@@ -374,14 +433,26 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cache-race", action="store_true")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays per step (smaller cases for profiling)")
-    ap.add_argument("--workload", default="raycast", choices=["raycast", "mlp"],
-                    help="mlp: the radiance cache's network alone (not the headline line)")
+    ap.add_argument("--workload", default="raycast", choices=["raycast", "mlp", "render"],
+                    help="mlp: the radiance cache's network alone; render: one path-tracing case (--case); "
+                         "neither is the headline line")
+    ap.add_argument("--case", default="c0", choices=sorted(RENDER_CASES))
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = _dist()
     N_RAYS = args.rays
     if args.workload == "mlp":
         run_mlp(args, local)
+        return
+    if args.workload == "render":
+        import torch
+
+        import pbrt_b200 as pb
+        from pbrt_b200 import workloads as W
+
+        torch.cuda.set_device(local)
+        res = render_case(pb, W, pb.Context(local), args.case, reps=max(1, args.steps), nvtx=True)
+        print(json.dumps({"metric": f"path tracing {args.case}", **res}), flush=True)
         return
 
     if args.impl == "reference":
@@ -506,6 +577,7 @@ def main():
             "clocks": clocks,
         }
         if ws == 1 and not args.no_cache_race:
+            line["renders"] = {c: render_case(pb, W, ctx, c, cpu=not args.no_cpu_baseline) for c in ("c0", "c2")}
             line["cache"] = cache_race(pb, W, ctx, rays_d.device)
         if ws == 1 and not args.no_cpu_baseline:
             import oracle

@@ -152,6 +152,11 @@ typedef struct pbrt_scene_desc {
  * bvh.rs:221-230). */
 int pbrt_scene_create(pbrt_ctx* ctx, const pbrt_scene_desc* desc, pbrt_scene** out);
 void pbrt_scene_destroy(pbrt_scene* scene);
+/* n scenes at once: their host-side builds (BVHs) run on `threads` host threads (0: all
+ * cores), then they are uploaded in order; out[i] receives scene i. On failure no scene is
+ * left created. */
+int pbrt_scene_create_many(pbrt_ctx* ctx, const pbrt_scene_desc* descs, uint32_t n, uint32_t threads,
+                           pbrt_scene** out);
 
 /* Host-only: builds one mesh's BVH exactly as pbrt_scene_create does and copies out the
  * flattened layout the GPU reads, without touching a GPU. `nodes` receives node_capacity
@@ -319,6 +324,45 @@ int pbrt_cache_load(pbrt_cache* cache, const void* buf, uint64_t size);
  * scene_max) takes the scene's bounds on first use. */
 int pbrt_render_cached(pbrt_scene* scene, pbrt_cache* cache, const pbrt_render_params* params, uint32_t train_rounds,
                        double* film_rgb);
+
+/* ---------------------------------------------------------------------------------- */
+/* Tuning and batches of scenes                                                         */
+/* ---------------------------------------------------------------------------------- */
+
+/* Launch shape of the wavefront renderer (pbrt_render, pbrt_render_cached, batches created
+ * afterwards). Zero fields take the defaults. */
+typedef struct pbrt_tuning {
+  uint32_t wave_paths;          /* paths in flight per wave (the queues' capacity), [1024, 2^24]; 0 = 2^22 */
+  uint32_t trace_threads;       /* threads per block of the traversal kernels, multiple of 32 <= 256; 0 = 128 */
+  uint32_t trace_blocks_per_sm; /* their grid = SMs x this, [1, 64]; 0 = 16 */
+  uint32_t shade_threads;       /* the shading kernel's; 0 = 128 */
+  uint32_t shade_blocks_per_sm; /* 0 = 16 */
+} pbrt_tuning;
+
+int pbrt_ctx_set_tuning(pbrt_ctx* ctx, const pbrt_tuning* tuning /* NULL: defaults */);
+int pbrt_ctx_get_tuning(pbrt_ctx* ctx, pbrt_tuning* tuning);
+
+/* Many scenes rendered together (no counterpart in the reference, whose renderer takes one
+ * scene): the paths of all scenes share the waves, queues and kernel launches of one
+ * wavefront, scene by scene in the given order, and the launch sequence of one frame is
+ * recorded once in a CUDA graph that pbrt_batch_render replays. The scenes must belong to
+ * ctx and outlive the batch; params[i] (integrator path or naive) renders scenes[i]. */
+typedef struct pbrt_batch pbrt_batch;
+int pbrt_batch_create(pbrt_ctx* ctx, pbrt_scene* const* scenes, const pbrt_render_params* params, uint32_t n,
+                      pbrt_batch** out);
+/* Frame `frame`: scene i takes samples sample_offset + frame * spp ... + spp - 1 of every
+ * pixel. films[i] (host or device, scene i's film size; films or films[i] may be NULL)
+ * receives the mean radiance. scene_ms (optional, n floats): device milliseconds from the
+ * frame's start until the wave holding scene i's last paths finished. */
+int pbrt_batch_render(pbrt_batch* batch, uint32_t frame, double* const* films, float* scene_ms);
+void pbrt_batch_destroy(pbrt_batch* batch);
+/* pbrt_batch_create + pbrt_batch_render(frame 0) + pbrt_batch_destroy. */
+int pbrt_render_batch(pbrt_scene* const* scenes, const pbrt_render_params* params, uint32_t n, double* const* films);
+
+/* Work of the last pbrt_render / pbrt_render_cached / pbrt_batch_render on this context: stats[0] rays traced
+ * to their nearest hit (camera and bounce rays, training paths included), stats[1] shadow
+ * rays, stats[2] paths started. Synchronises the context's stream. */
+int pbrt_ctx_render_stats(pbrt_ctx* ctx, uint64_t* stats /* 3 */);
 
 /* Spectrum::gamma_correct + to_rgb (src/spectrum.rs:13-25, 134-136): sqrt gamma, clip to
  * [0, 1], truncate to 8 bits, alpha 255, as image_write stores it (mt.rs:152-167). Host

@@ -78,6 +78,11 @@ class CacheParams(C.Structure):
                 ("terminate_bounce", C.c_uint32), ("train_samples", C.c_uint32), ("train_steps", C.c_uint32)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("wave_paths", C.c_uint32), ("trace_threads", C.c_uint32), ("trace_blocks_per_sm", C.c_uint32),
+                ("shade_threads", C.c_uint32), ("shade_blocks_per_sm", C.c_uint32)]
+
+
 # Every symbol the header declares, with its signature. tests/test_capi_symbols.py checks
 # the library exports each of them.
 SIGNATURES = {
@@ -88,6 +93,7 @@ SIGNATURES = {
     "pbrt_ctx_sync": (C.c_int, [C.c_void_p]),
     "pbrt_scene_create": (C.c_int, [C.c_void_p, C.POINTER(SceneDesc), C.POINTER(C.c_void_p)]),
     "pbrt_scene_destroy": (None, [C.c_void_p]),
+    "pbrt_scene_create_many": (C.c_int, [C.c_void_p, C.POINTER(SceneDesc), C.c_uint32, C.c_uint32, C.c_void_p]),
     "pbrt_scene_get_info": (C.c_int, [C.c_void_p, C.POINTER(SceneInfo)]),
     "pbrt_mesh_bvh_build_host": (C.c_int, [C.POINTER(MeshDesc), C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64,
                                            C.c_void_p, C.POINTER(C.c_uint64)]),
@@ -108,6 +114,13 @@ SIGNATURES = {
     "pbrt_cache_save": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
     "pbrt_cache_load": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "pbrt_render_cached": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(RenderParams), C.c_uint32, C.c_void_p]),
+    "pbrt_ctx_render_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "pbrt_ctx_set_tuning": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "pbrt_ctx_get_tuning": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "pbrt_batch_create": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(RenderParams), C.c_uint32, C.POINTER(C.c_void_p)]),
+    "pbrt_batch_render": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "pbrt_batch_destroy": (None, [C.c_void_p]),
+    "pbrt_render_batch": (C.c_int, [C.c_void_p, C.POINTER(RenderParams), C.c_uint32, C.c_void_p]),
     "pbrt_film_to_rgba8": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
 }
 

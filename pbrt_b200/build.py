@@ -29,7 +29,7 @@ NVCC_EXTRA = {
     "kernels_render.cu": ["-fmad=false"],
     "api.cu": ["-fmad=false"],
 }
-CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall", "-I", CSRC, "-I", INCLUDE]
+CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall", "-I", CSRC, "-I", INCLUDE]
 
 
 def _sources():

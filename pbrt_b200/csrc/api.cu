@@ -12,6 +12,8 @@
 #include <memory>
 #include <string>
 #include <vector>
+#include <atomic>
+#include <thread>
 
 #include "../../include/pbrt_b200.h"
 #include "cache.hpp"
@@ -50,10 +52,13 @@ int ensure_queue(pbrt_ctx* c) {
 }
 
 
+// Host-to-device copies go on the context's own stream: a plain cudaMemcpy from pageable
+// memory may return before its DMA lands, and kernels on a non-blocking stream would not wait
+// for it. Scene creation synchronises that stream once all copies are queued.
 int upload(pbrt_ctx* c, void** dst, const void* src, size_t bytes, uint64_t* total) {
   PBRT_TRY(c->cuda(cudaMalloc(dst, bytes), "cudaMalloc(scene)"));
   *total += bytes;
-  return c->cuda(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy(scene)");
+  return c->cuda(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, c->stream), "cudaMemcpy(scene)");
 }
 
 void free_mesh(DeviceMesh& m) {
@@ -88,9 +93,14 @@ int pbrt_ctx_create(int device, pbrt_ctx** out) {
   if (c->cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate") != PBRT_OK)
     return PBRT_ERR_CUDA;
   if (c->cuda(cudaMalloc(&c->d_err, sizeof(uint32_t)), "cudaMalloc") != PBRT_OK) return PBRT_ERR_OUT_OF_MEMORY;
-  if (c->cuda(cudaMemset(c->d_err, 0, sizeof(uint32_t)), "cudaMemset") != PBRT_OK) return PBRT_ERR_CUDA;
-  if (c->cuda(cudaMalloc(&c->d_counters, 8 * sizeof(unsigned long long)), "cudaMalloc") != PBRT_OK)
+  if (c->cuda(cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), c->stream), "cudaMemset") != PBRT_OK)
+    return PBRT_ERR_CUDA;
+  if (c->cuda(cudaMalloc(&c->d_counters, 16 * sizeof(unsigned long long)), "cudaMalloc") != PBRT_OK)
     return PBRT_ERR_OUT_OF_MEMORY;
+  if (c->cuda(cudaMemsetAsync(c->d_counters, 0, 16 * sizeof(unsigned long long), c->stream), "cudaMemset") !=
+      PBRT_OK)
+    return PBRT_ERR_CUDA;
+  if (c->cuda(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize") != PBRT_OK) return PBRT_ERR_CUDA;
   *out = c.release();
   return PBRT_OK;
 }
@@ -131,16 +141,12 @@ int pbrt_ctx_sync(pbrt_ctx* c) {
   return check_device_error(c, c->work_stream());
 }
 
-int pbrt_scene_create(pbrt_ctx* c, const pbrt_scene_desc* d, pbrt_scene** out) {
-  if (!c || !d || !out) return PBRT_ERR_INVALID_ARGUMENT;
-  *out = nullptr;
-  DeviceGuard g(c->device);
-  if (d->object_count == 0) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "a scene needs at least one object");
-  if (d->mesh_count && !d->meshes) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "meshes is NULL");
-  if (!d->objects) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "objects is NULL");
-  FlatScene fs;
-  std::string e;
-  if (!build_scene(*d, &fs, &e)) return c->fail(PBRT_ERR_INVALID_ARGUMENT, e);
+}  // extern "C"
+
+namespace {
+
+// The device half of scene creation: checks the built structure, uploads it, fills the view.
+int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbrt_scene** out) {
   for (uint32_t i = 0; i < fs.meshes.size(); ++i)
     if (fs.meshes[i].stats.max_depth >= uint32_t(kTraceStack))
       return c->fail(PBRT_ERR_CAPACITY, "mesh " + std::to_string(i) + ": BVH depth " +
@@ -223,7 +229,71 @@ int pbrt_scene_create(pbrt_ctx* c, const pbrt_scene_desc* d, pbrt_scene** out) {
   }
   if (d->object_count == 1 && d->objects[0].shape == PBRT_SHAPE_MESH && !d->objects[0].transformed)
     s->single_mesh = int(d->objects[0].mesh);
+  const int rc2 = c->cuda(cudaStreamSynchronize(c->stream), "scene upload");
+  if (rc2 != PBRT_OK) {
+    pbrt_scene_destroy(s.release());
+    return rc2;
+  }
   *out = s.release();
+  return PBRT_OK;
+}
+
+int check_scene_desc(pbrt_ctx* c, const pbrt_scene_desc* d) {
+  if (!d) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "scene description is NULL");
+  if (d->object_count == 0) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "a scene needs at least one object");
+  if (d->mesh_count && !d->meshes) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "meshes is NULL");
+  if (!d->objects) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "objects is NULL");
+  return PBRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pbrt_scene_create(pbrt_ctx* c, const pbrt_scene_desc* d, pbrt_scene** out) {
+  if (!c || !d || !out) return PBRT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  DeviceGuard g(c->device);
+  PBRT_TRY(check_scene_desc(c, d));
+  FlatScene fs;
+  std::string e;
+  if (!build_scene(*d, &fs, &e)) return c->fail(PBRT_ERR_INVALID_ARGUMENT, e);
+  return upload_scene(c, d, fs, out);
+}
+
+int pbrt_scene_create_many(pbrt_ctx* c, const pbrt_scene_desc* descs, uint32_t n, uint32_t threads,
+                           pbrt_scene** out) {
+  if (!c || !descs || !out) return PBRT_ERR_INVALID_ARGUMENT;
+  DeviceGuard g(c->device);
+  for (uint32_t i = 0; i < n; ++i) out[i] = nullptr;
+  for (uint32_t i = 0; i < n; ++i) PBRT_TRY(check_scene_desc(c, descs + i));
+  // host builds on a pool of threads (no device calls), then uploads in order
+  std::vector<FlatScene> flat(n);
+  std::vector<std::string> errs(n);
+  std::vector<char> ok(n, 0);
+  std::atomic<uint32_t> next{0};
+  unsigned T = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
+  T = std::min<unsigned>(T, n);
+  auto work = [&]() {
+    for (uint32_t i = next++; i < n; i = next++) ok[i] = build_scene(descs[i], &flat[i], &errs[i]) ? 1 : 0;
+  };
+  std::vector<std::thread> pool;
+  for (unsigned t = 1; t < T; ++t) pool.emplace_back(work);
+  work();
+  for (std::thread& t : pool) t.join();
+  for (uint32_t i = 0; i < n; ++i)
+    if (!ok[i]) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "scene " + std::to_string(i) + ": " + errs[i]);
+  for (uint32_t i = 0; i < n; ++i) {
+    const int rc = upload_scene(c, descs + i, flat[i], out + i);
+    if (rc != PBRT_OK) {
+      for (uint32_t j = 0; j < i; ++j) {
+        pbrt_scene_destroy(out[j]);
+        out[j] = nullptr;
+      }
+      return rc;
+    }
+    FlatScene().meshes.swap(flat[i].meshes);  // release host copies as we go
+  }
   return PBRT_OK;
 }
 
@@ -425,26 +495,15 @@ int pbrt_trace_any(pbrt_scene* s, const float* rays, uint64_t n, uint8_t* occlud
 // ---------------------------------------------------------------------------------------
 // Rendering
 // ---------------------------------------------------------------------------------------
-namespace {
-
-constexpr uint32_t kWave = 1u << 22;  // paths in flight per wave (~128 B of state each)
-
-// The wave's SoA state, kept by the context and grown on demand.
-struct WaveAlloc {
-  void* block = nullptr;
-  uint32_t capacity = 0;
-  WaveBuffers w{};
-};
-
-int ensure_wave(pbrt_ctx* c, WaveAlloc* wa, uint32_t cap) {
+int pbrt::api::ensure_wave(pbrt_ctx* c, WaveAlloc* wa, uint32_t cap) {
   if (wa->capacity >= cap) return PBRT_OK;
   cudaFree(wa->block);
   wa->block = nullptr;
   wa->capacity = 0;
   const size_t n = cap;
-  // 4-byte arrays: 6 ray + 3 beta + 3 L + pixel + flags + ht + hobj + hprim + qa + qb + 11 shadow
-  // = 31 words, plus the 8-byte rng state, plus 4 counters.
-  const size_t bytes = n * (31 * 4 + 8) + 64;
+  // 4-byte arrays: 6 ray + 3 beta + 3 L + pixel + scene + flags + ht + hobj + hprim + qa + qb + 11 shadow
+  // = 32 words, plus the 8-byte rng state, plus 4 counters.
+  const size_t bytes = n * (32 * 4 + 8) + 64;
   PBRT_TRY(c->cuda(cudaMalloc(&wa->block, bytes), "cudaMalloc(wave state)"));
   char* p = static_cast<char*>(wa->block);
   auto f32 = [&]() { float* r = reinterpret_cast<float*>(p); p += n * 4; return r; };
@@ -454,7 +513,7 @@ int ensure_wave(pbrt_ctx* c, WaveAlloc* wa, uint32_t cap) {
   p += n * 8;
   w.ox = f32(); w.oy = f32(); w.oz = f32(); w.dx = f32(); w.dy = f32(); w.dz = f32();
   w.br = f32(); w.bg = f32(); w.bb = f32(); w.lr = f32(); w.lg = f32(); w.lb = f32();
-  w.pixel = u32(); w.flags = u32(); w.ht = f32(); w.hobj = u32(); w.hprim = u32(); w.qa = u32(); w.qb = u32();
+  w.pixel = u32(); w.scene = u32(); w.flags = u32(); w.ht = f32(); w.hobj = u32(); w.hprim = u32(); w.qa = u32(); w.qb = u32();
   w.s_path = u32(); w.s_ox = f32(); w.s_oy = f32(); w.s_oz = f32(); w.s_dx = f32(); w.s_dy = f32(); w.s_dz = f32();
   w.s_tmax = f32(); w.s_cr = f32(); w.s_cg = f32(); w.s_cb = f32();
   w.counts = reinterpret_cast<uint32_t*>(p);
@@ -462,13 +521,7 @@ int ensure_wave(pbrt_ctx* c, WaveAlloc* wa, uint32_t cap) {
   return PBRT_OK;
 }
 
-WaveAlloc g_waves[kMaxDevices];  // per device; a context serialises its own calls
-
-// Training paths of the cached render go this many hits past the render's cache hit before
-// they end into the cache themselves.
-constexpr uint32_t kTrainTail = 3;
-
-int check_render_params(pbrt_ctx* c, const pbrt_render_params* p, bool allow_no_samples) {
+int pbrt::api::check_render_params(pbrt_ctx* c, const pbrt_render_params* p, bool allow_no_samples) {
   const pbrt_camera_desc& cd = p->camera;
   if (cd.width == 0 || cd.height == 0) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "empty image");
   if (p->spp == 0 && !allow_no_samples) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "spp must be >= 1");
@@ -483,8 +536,10 @@ int check_render_params(pbrt_ctx* c, const pbrt_render_params* p, bool allow_no_
   return PBRT_OK;
 }
 
-RenderSettings settings_of(const pbrt_render_params* p) {
+RenderSettings pbrt::api::settings_of(pbrt_ctx* c, const pbrt_render_params* p) {
   RenderSettings rs;
+  rs.stats = c->d_counters + 8;
+  rs.shape = c->shape;
   rs.max_depth = p->max_depth;
   rs.rr_start = p->integrator == PBRT_INTEGRATOR_NAIVE ? 0u : p->rr_start;
   rs.sample_offset = p->sample_offset;
@@ -496,9 +551,17 @@ RenderSettings settings_of(const pbrt_render_params* p) {
 }
 
 // Film pixels of a render: the image's, or the strided subset's.
-uint64_t film_pixels(const pbrt_render_params* p, const RenderSettings& rs) {
+uint64_t pbrt::api::film_pixels(const pbrt_render_params* p, const RenderSettings& rs) {
   return uint64_t(rs.film_w) * ((p->camera.height + rs.stride - 1) / rs.stride);
 }
+
+namespace {
+
+WaveAlloc g_waves[kMaxDevices];  // per device; a context serialises its own calls
+
+// Training paths of the cached render go this many hits past the render's cache hit before
+// they end into the cache themselves.
+constexpr uint32_t kTrainTail = 3;
 
 unsigned long long host_mix64(unsigned long long x) {
   x += 0x9E3779B97F4A7C15ULL;
@@ -519,12 +582,12 @@ int pbrt_render(pbrt_scene* s, const pbrt_render_params* p, double* film) {
   PBRT_TRY(check_render_params(c, p, false));
   const pbrt_camera_desc& cd = p->camera;
   const CameraRec cam = build_camera(cd);
-  const RenderSettings rs = settings_of(p);
+  const RenderSettings rs = settings_of(c, p);
   const uint64_t npix = film_pixels(p, rs);
   const uint64_t total = npix * p->spp;
 
   WaveAlloc& wa = g_waves[c->device];
-  const uint32_t wave = uint32_t(std::min<uint64_t>(total, kWave));
+  const uint32_t wave = uint32_t(std::min<uint64_t>(total, c->wave_paths));
   PBRT_TRY(ensure_wave(c, &wa, wave));
   cudaStream_t st = c->work_stream();
   const size_t film_n = size_t(npix) * 3;
@@ -532,6 +595,7 @@ int pbrt_render(pbrt_scene* s, const pbrt_render_params* p, double* film) {
   const bool host_film = mem_kind(film) != MemKind::Device;
   if (host_film) PBRT_TRY(c->cuda(cudaMalloc(&dfilm, film_n * sizeof(double)), "cudaMalloc(film)"));
   int rc = c->cuda(cudaMemsetAsync(dfilm, 0, film_n * sizeof(double), st), "cudaMemset(film)");
+  if (rc == PBRT_OK) rc = c->cuda(cudaMemsetAsync(rs.stats, 0, 3 * sizeof(unsigned long long), st), "cudaMemset");
   for (uint64_t base = 0; base < total && rc == PBRT_OK; base += wave) {
     const uint32_t n = uint32_t(std::min<uint64_t>(wave, total - base));
     rc = c->cuda(render_wave(s->view, wa.w, cam, base, n, uint32_t(npix), rs, dfilm, c->d_err, c->sm_count, st),
@@ -570,13 +634,13 @@ int pbrt_render_cached(pbrt_scene* s, pbrt_cache* k, const pbrt_render_params* p
     }
   const pbrt_camera_desc& cd = p->camera;
   const CameraRec cam = build_camera(cd);
-  const RenderSettings rs = settings_of(p);
+  const RenderSettings rs = settings_of(c, p);
   const uint64_t npix = film_pixels(p, rs);
   const uint64_t total = npix * p->spp;
   const uint32_t train_paths = std::max(128u, cp.train_samples / 4);
   const uint32_t steps = cp.train_steps;
   const uint32_t batch = std::max(128u, cp.train_samples / steps);
-  const uint32_t wave = uint32_t(std::min<uint64_t>(total, kWave));
+  const uint32_t wave = uint32_t(std::min<uint64_t>(total, c->wave_paths));
 
   WaveAlloc& wa = g_waves[c->device];
   PBRT_TRY(ensure_wave(c, &wa, std::max(wave, train_paths)));
@@ -584,6 +648,7 @@ int pbrt_render_cached(pbrt_scene* s, pbrt_cache* k, const pbrt_render_params* p
   PBRT_TRY(k->ensure_render_buffers(std::max(wave, train_paths), cp.train_samples, batch));
   cudaStream_t st = c->work_stream();
   const CacheWave& cw = k->cw;
+  PBRT_TRY(c->cuda(cudaMemsetAsync(rs.stats, 0, 3 * sizeof(unsigned long long), st), "cudaMemset"));
 
   // Online training. Training paths start at random pixels, go kTrainTail hits past the
   // render's cache hit and end into the cache there; their earlier Lambertian and metal
@@ -654,6 +719,48 @@ int pbrt_render_cached(pbrt_scene* s, pbrt_cache* k, const pbrt_render_params* p
   PBRT_TRY(rc);
   if (c->user) return PBRT_OK;
   return check_device_error(c, st);
+}
+
+int pbrt_ctx_set_tuning(pbrt_ctx* c, const pbrt_tuning* t) {
+  if (!c) return PBRT_ERR_INVALID_ARGUMENT;
+  pbrt_tuning d{};
+  if (t) d = *t;
+  LaunchShape sh;
+  const uint32_t wave = d.wave_paths ? d.wave_paths : (1u << 22);
+  if (d.trace_threads) sh.trace_threads = d.trace_threads;
+  if (d.trace_blocks_per_sm) sh.trace_blocks_per_sm = d.trace_blocks_per_sm;
+  if (d.shade_threads) sh.shade_threads = d.shade_threads;
+  if (d.shade_blocks_per_sm) sh.shade_blocks_per_sm = d.shade_blocks_per_sm;
+  auto bad_threads = [](uint32_t x) { return x < 32 || x > 256 || x % 32 != 0; };
+  auto bad_blocks = [](uint32_t x) { return x < 1 || x > 64; };
+  if (bad_threads(sh.trace_threads) || bad_threads(sh.shade_threads))
+    return c->fail(PBRT_ERR_INVALID_ARGUMENT, "threads per block must be a multiple of 32 in [32, 256]");
+  if (bad_blocks(sh.trace_blocks_per_sm) || bad_blocks(sh.shade_blocks_per_sm))
+    return c->fail(PBRT_ERR_INVALID_ARGUMENT, "blocks per SM must be in [1, 64]");
+  if (wave < 1024 || wave > (1u << 24)) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "wave_paths must be in [1024, 2^24]");
+  c->shape = sh;
+  c->wave_paths = wave;
+  return PBRT_OK;
+}
+
+int pbrt_ctx_get_tuning(pbrt_ctx* c, pbrt_tuning* t) {
+  if (!c || !t) return PBRT_ERR_INVALID_ARGUMENT;
+  t->wave_paths = c->wave_paths;
+  t->trace_threads = c->shape.trace_threads;
+  t->trace_blocks_per_sm = c->shape.trace_blocks_per_sm;
+  t->shade_threads = c->shape.shade_threads;
+  t->shade_blocks_per_sm = c->shape.shade_blocks_per_sm;
+  return PBRT_OK;
+}
+
+int pbrt_ctx_render_stats(pbrt_ctx* c, uint64_t* stats) {
+  if (!c || !stats) return PBRT_ERR_INVALID_ARGUMENT;
+  DeviceGuard g(c->device);
+  PBRT_TRY(c->cuda(cudaStreamSynchronize(c->work_stream()), "sync"));
+  unsigned long long h[3];
+  PBRT_TRY(c->cuda(cudaMemcpy(h, c->d_counters + 8, sizeof(h), cudaMemcpyDeviceToHost), "cudaMemcpy(render stats)"));
+  for (int i = 0; i < 3; ++i) stats[i] = h[i];
+  return PBRT_OK;
 }
 
 int pbrt_film_to_rgba8(const double* film, uint32_t w, uint32_t h, uint8_t* rgba) {

@@ -1,0 +1,185 @@
+// batch.cu — many scenes rendered by one wavefront, its launch sequence recorded once in a
+// CUDA graph (pbrt_batch_* in include/pbrt_b200.h). Host code; the kernels are the wavefront
+// kernels of kernels_render.cu over the batch table.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <memory>
+#include <vector>
+
+#include "../../include/pbrt_b200.h"
+#include "context.hpp"
+#include "render.hpp"
+#include "scene_host.hpp"
+
+using namespace pbrt;
+using namespace pbrt::api;
+
+struct pbrt_batch {
+  pbrt_ctx* ctx = nullptr;
+  std::vector<BatchScene> table;  // host copy (film pointers are the batch's device films)
+  std::vector<size_t> film_n;     // doubles per film
+  BatchScene* d_table = nullptr;
+  uint32_t* d_frame = nullptr;
+  uint32_t frame_host = 0;
+  std::vector<double*> films;
+  WaveAlloc wave;
+  uint32_t wave_paths = 0, max_depth = 0;
+  bool any_path = false;
+  LaunchShape shape;
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t start = nullptr;
+  std::vector<cudaEvent_t> done;
+
+  void release() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cap) cudaStreamDestroy(cap);
+    if (start) cudaEventDestroy(start);
+    for (cudaEvent_t e : done) cudaEventDestroy(e);
+    for (double* f : films) cudaFree(f);
+    cudaFree(d_table);
+    cudaFree(d_frame);
+    cudaFree(wave.block);
+  }
+};
+
+namespace {
+
+// Records one frame's launches (all waves of all scenes) into b->graph and instantiates it.
+int capture(pbrt_batch* b) {
+  pbrt_ctx* c = b->ctx;
+  PBRT_TRY(c->cuda(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking), "cudaStreamCreate"));
+  PBRT_TRY(c->cuda(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture"));
+  cudaError_t e = cudaMemsetAsync(c->d_counters + 8, 0, 3 * sizeof(unsigned long long), b->cap);
+  if (e == cudaSuccess)
+    e = render_batch(b->d_table, b->table.data(), uint32_t(b->table.size()), b->wave.w, b->wave_paths, b->d_frame,
+                     b->max_depth, b->any_path, b->shape, c->d_counters + 8, c->d_err, c->sm_count, b->cap,
+                     b->done.data());
+  cudaGraph_t g = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(b->cap, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return c->cuda(e != cudaSuccess ? e : e2, "batch graph capture");
+  }
+  b->graph = g;
+  return c->cuda(cudaGraphInstantiate(&b->exec, b->graph, 0), "cudaGraphInstantiate");
+}
+
+}  // namespace
+
+extern "C" {
+
+int pbrt_batch_create(pbrt_ctx* c, pbrt_scene* const* scenes, const pbrt_render_params* params, uint32_t n,
+                      pbrt_batch** out) {
+  if (!c || !out) return PBRT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  DeviceGuard g(c->device);
+  if (n == 0 || !scenes || !params) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "empty batch");
+  std::unique_ptr<pbrt_batch> b(new pbrt_batch);
+  b->ctx = c;
+  b->shape = c->shape;
+  unsigned long long begin = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const pbrt_scene* s = scenes[i];
+    const pbrt_render_params* p = params + i;
+    if (!s || s->ctx != c) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "scene " + std::to_string(i) + " is NULL or "
+                                                                     "belongs to another context");
+    PBRT_TRY(check_render_params(c, p, false));
+    const RenderSettings rs = settings_of(c, p);
+    BatchScene e{};
+    e.view = s->view;
+    e.cam = build_camera(p->camera);
+    e.begin = begin;
+    e.seed = p->seed;
+    e.npix = uint32_t(film_pixels(p, rs));
+    e.spp = p->spp;
+    e.max_depth = rs.max_depth;
+    e.rr_start = rs.rr_start;
+    e.sample_offset = p->sample_offset;
+    e.naive = rs.naive;
+    e.stride = rs.stride;
+    e.film_w = rs.film_w;
+    const unsigned long long paths = (unsigned long long)e.npix * e.spp;
+    if (begin + paths < begin || begin + paths > (1ull << 62))
+      return c->fail(PBRT_ERR_INVALID_ARGUMENT, "too many paths in the batch");
+    begin += paths;
+    b->table.push_back(e);
+    b->film_n.push_back(size_t(e.npix) * 3);
+    b->max_depth = std::max(b->max_depth, e.max_depth);
+    b->any_path = b->any_path || !e.naive;
+  }
+  int rc = PBRT_OK;
+  for (uint32_t i = 0; i < n && rc == PBRT_OK; ++i) {
+    double* f = nullptr;
+    rc = c->cuda(cudaMalloc(&f, b->film_n[i] * sizeof(double)), "cudaMalloc(batch film)");
+    if (rc == PBRT_OK) {
+      b->films.push_back(f);
+      b->table[i].film = f;
+    }
+  }
+  if (rc == PBRT_OK) rc = c->cuda(cudaMalloc(&b->d_table, n * sizeof(BatchScene)), "cudaMalloc(batch table)");
+  if (rc == PBRT_OK)
+    rc = c->cuda(cudaMemcpyAsync(b->d_table, b->table.data(), n * sizeof(BatchScene), cudaMemcpyHostToDevice,
+                                 c->stream),
+                 "cudaMemcpy(batch table)");
+  if (rc == PBRT_OK) rc = c->cuda(cudaMalloc(&b->d_frame, sizeof(uint32_t)), "cudaMalloc(batch frame)");
+  if (rc == PBRT_OK) rc = c->cuda(cudaMemsetAsync(b->d_frame, 0, sizeof(uint32_t), c->stream), "cudaMemset(batch frame)");
+  if (rc == PBRT_OK) rc = c->cuda(cudaStreamSynchronize(c->stream), "batch upload");
+  b->wave_paths = uint32_t(std::min<unsigned long long>(begin, c->wave_paths));
+  if (rc == PBRT_OK) rc = ensure_wave(c, &b->wave, b->wave_paths);
+  if (rc == PBRT_OK) rc = c->cuda(cudaEventCreate(&b->start), "cudaEventCreate");
+  b->done.assign(n, nullptr);
+  for (uint32_t i = 0; i < n && rc == PBRT_OK; ++i) rc = c->cuda(cudaEventCreate(&b->done[i]), "cudaEventCreate");
+  if (rc == PBRT_OK) rc = capture(b.get());
+  if (rc != PBRT_OK) {
+    b->release();
+    return rc;
+  }
+  *out = b.release();
+  return PBRT_OK;
+}
+
+int pbrt_batch_render(pbrt_batch* b, uint32_t frame, double* const* films, float* scene_ms) {
+  if (!b) return PBRT_ERR_INVALID_ARGUMENT;
+  pbrt_ctx* c = b->ctx;
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->work_stream();
+  b->frame_host = frame;
+  PBRT_TRY(c->cuda(cudaMemcpyAsync(b->d_frame, &b->frame_host, sizeof(uint32_t), cudaMemcpyHostToDevice, st),
+                   "cudaMemcpy(batch frame)"));
+  PBRT_TRY(c->cuda(cudaEventRecord(b->start, st), "cudaEventRecord"));
+  PBRT_TRY(c->cuda(cudaGraphLaunch(b->exec, st), "cudaGraphLaunch"));
+  if (films)
+    for (size_t i = 0; i < b->films.size(); ++i)
+      if (films[i])
+        PBRT_TRY(c->cuda(cudaMemcpyAsync(films[i], b->films[i], b->film_n[i] * sizeof(double), cudaMemcpyDefault, st),
+                         "cudaMemcpy(batch film)"));
+  PBRT_TRY(check_device_error(c, st));
+  if (scene_ms)
+    for (size_t i = 0; i < b->done.size(); ++i)
+      PBRT_TRY(c->cuda(cudaEventElapsedTime(scene_ms + i, b->start, b->done[i]), "cudaEventElapsedTime"));
+  return PBRT_OK;
+}
+
+void pbrt_batch_destroy(pbrt_batch* b) {
+  if (!b) return;
+  DeviceGuard g(b->ctx->device);
+  cudaStreamSynchronize(b->ctx->work_stream());
+  b->release();
+  delete b;
+}
+
+int pbrt_render_batch(pbrt_scene* const* scenes, const pbrt_render_params* params, uint32_t n, double* const* films) {
+  if (!scenes || n == 0 || !scenes[0]) return PBRT_ERR_INVALID_ARGUMENT;
+  pbrt_batch* b = nullptr;
+  PBRT_TRY(pbrt_batch_create(scenes[0]->ctx, scenes, params, n, &b));
+  const int rc = pbrt_batch_render(b, 0, films, nullptr);
+  pbrt_batch_destroy(b);
+  return rc;
+}
+
+}  // extern "C"

@@ -172,7 +172,10 @@ struct DeviceIn {
       return PBRT_OK;
     }
     PBRT_TRY(c->cuda(cudaMalloc(&owned, std::max<size_t>(count, 1) * 4), "cudaMalloc(cache input)"));
-    PBRT_TRY(c->cuda(cudaMemcpy(owned, p, count * 4, cudaMemcpyHostToDevice), "cudaMemcpy(cache input)"));
+    // on the stream the kernels that read it run on (a plain cudaMemcpy from pageable memory
+    // may return before its DMA lands)
+    PBRT_TRY(c->cuda(cudaMemcpyAsync(owned, p, count * 4, cudaMemcpyHostToDevice, c->work_stream()),
+                     "cudaMemcpy(cache input)"));
     ptr = owned;
     return PBRT_OK;
   }
@@ -234,7 +237,7 @@ int pbrt_cache_set_weights(pbrt_cache* k, const float* w) {
   if (!k || !w) return PBRT_ERR_INVALID_ARGUMENT;
   DeviceGuard g(k->ctx->device);
   cudaStream_t s = k->ctx->work_stream();
-  PBRT_TRY(k->ctx->cuda(cudaMemcpy(k->w, w, mlp::kParams * 4, cudaMemcpyDefault), "cudaMemcpy(weights)"));
+  PBRT_TRY(k->ctx->cuda(cudaMemcpyAsync(k->w, w, mlp::kParams * 4, cudaMemcpyDefault, s), "cudaMemcpy(weights)"));
   PBRT_TRY(k->ctx->cuda(mlp::launch_pack(k->w, k->wfwd, k->wbwd, s), "cache pack"));
   return k->ctx->cuda(cudaStreamSynchronize(s), "cache pack");
 }
@@ -329,10 +332,11 @@ int pbrt_cache_load(pbrt_cache* k, const void* buf, uint64_t size) {
   if (magic != 0x43524e50u) return k->ctx->fail(PBRT_ERR_INVALID_ARGUMENT, "not a cache checkpoint");
   DeviceGuard g(k->ctx->device);
   cudaStream_t s = k->ctx->work_stream();
-  PBRT_TRY(k->ctx->cuda(cudaMemcpy(k->w, b + 8, mlp::kParams * 4, cudaMemcpyHostToDevice), "cudaMemcpy"));
-  PBRT_TRY(k->ctx->cuda(cudaMemcpy(k->m, b + 8 + mlp::kParams * 4, mlp::kParams * 4, cudaMemcpyHostToDevice), "cudaMemcpy"));
-  PBRT_TRY(k->ctx->cuda(cudaMemcpy(k->v, b + 8 + 2 * mlp::kParams * 4, mlp::kParams * 4, cudaMemcpyHostToDevice),
+  PBRT_TRY(k->ctx->cuda(cudaMemcpyAsync(k->w, b + 8, mlp::kParams * 4, cudaMemcpyHostToDevice, s), "cudaMemcpy"));
+  PBRT_TRY(k->ctx->cuda(cudaMemcpyAsync(k->m, b + 8 + mlp::kParams * 4, mlp::kParams * 4, cudaMemcpyHostToDevice, s),
                         "cudaMemcpy"));
+  PBRT_TRY(k->ctx->cuda(
+      cudaMemcpyAsync(k->v, b + 8 + 2 * mlp::kParams * 4, mlp::kParams * 4, cudaMemcpyHostToDevice, s), "cudaMemcpy"));
   k->step = step;
   PBRT_TRY(k->ctx->cuda(mlp::launch_pack(k->w, k->wfwd, k->wbwd, s), "cache pack"));
   return k->ctx->cuda(cudaStreamSynchronize(s), "cache pack");

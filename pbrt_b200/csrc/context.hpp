@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/pbrt_b200.h"
+#include "render.hpp"
 #include "scene_device.cuh"
 #include "trace_mesh.cuh"
 
@@ -56,6 +57,14 @@ struct Slot {
   unsigned long long* fetch = nullptr;  // [queue length, fetch position] of that pass
 };
 
+// The wave's SoA state, grown on demand (one per device for pbrt_render / pbrt_render_cached,
+// one per batch).
+struct WaveAlloc {
+  void* block = nullptr;
+  uint32_t capacity = 0;
+  WaveBuffers w{};
+};
+
 }  // namespace api
 }  // namespace pbrt
 
@@ -66,12 +75,15 @@ struct pbrt_ctx {
   cudaStream_t user = nullptr;    // caller's stream (asynchronous device-buffer calls)
   std::string err;
   uint32_t* d_err = nullptr;
-  unsigned long long* d_counters = nullptr;  // [0..2] traversal counters, [4..5] queue length / fetch position
+  unsigned long long* d_counters = nullptr;  // [0..2] traversal counters, [4..5] queue length / fetch position,
+                                             // [8..10] rays / shadow rays / paths of the last render
   uint32_t* queue = nullptr;                  // survivor queue for device-buffer calls (kDevChunk entries)
   bool persistent = true;                     // persistent dynamic-fetch traversal (default)
   pbrt::api::Slot slots[pbrt::api::kSlots];
   bool slots_ready = false;
   std::vector<void*> allocs;
+  pbrt::LaunchShape shape;          // wavefront launch shape (pbrt_ctx_set_tuning)
+  uint32_t wave_paths = 1u << 22;   // paths per wave
 
   int fail(int code, const std::string& msg) {
     err = msg;
@@ -112,7 +124,8 @@ struct pbrt_scene {
     if (rc != PBRT_OK) return rc;
     allocs.push_back(*dst);
     extra_bytes += bytes;
-    return ctx->cuda(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy(scene)");
+    // ordered on the context's stream (see upload in api.cu); scene creation synchronises it
+    return ctx->cuda(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream), "cudaMemcpy(scene)");
   }
 };
 
@@ -131,10 +144,25 @@ inline int check_device_error(pbrt_ctx* c, cudaStream_t s) {
   uint32_t h = 0;
   PBRT_TRY(c->cuda(cudaMemcpy(&h, c->d_err, sizeof(h), cudaMemcpyDeviceToHost), "cudaMemcpy(error word)"));
   if (h == 0) return PBRT_OK;
-  PBRT_TRY(c->cuda(cudaMemset(c->d_err, 0, sizeof(uint32_t)), "cudaMemset(error word)"));
+  PBRT_TRY(c->cuda(cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), s), "cudaMemset(error word)"));
+  PBRT_TRY(c->cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize"));
   if (h & kErrStack) return c->fail(PBRT_ERR_CAPACITY, "traversal stack capacity exceeded");
+  if (h & 4u) return c->fail(PBRT_ERR_DEVICE_BUDGET, "a tensor-core completion wait ran out of its budget");
   return c->fail(PBRT_ERR_DEVICE_BUDGET, "a traversal exceeded its iteration budget (malformed tree)");
 }
 
 }  // namespace api
 }  // namespace pbrt
+
+namespace pbrt {
+namespace api {
+int ensure_wave(pbrt_ctx* c, WaveAlloc* wa, uint32_t cap);
+// Validation of render parameters shared by every render entry point.
+int check_render_params(pbrt_ctx* c, const pbrt_render_params* p, bool allow_no_samples);
+// The kernels' settings for these parameters on this context (tuning, counters).
+RenderSettings settings_of(pbrt_ctx* c, const pbrt_render_params* p);
+// Film pixels of a render: the image's, or the strided subset's.
+uint64_t film_pixels(const pbrt_render_params* p, const RenderSettings& rs);
+}  // namespace api
+}  // namespace pbrt
+

@@ -1,6 +1,6 @@
 // kernels_render.cu — wavefront path tracing and general-scene ray casting.
 //
-// A wave of up to kWave paths lives in SoA buffers. Each bounce runs three kernels over
+// A wave of paths (up to the context's wave size, 2^22 by default) lives in SoA buffers. Each bounce runs three kernels over
 // queues of path indices: extend (nearest hit), shade (emission, light sampling, BSDF
 // sampling, Russian roulette; pushes the surviving paths to the next queue and at most one
 // shadow ray per path to the shadow queue, both with one atomicAdd per warp) and shadow
@@ -279,10 +279,54 @@ PBRT_DEV void write_record(float* rec, const F3& p, float rough, const F3& wo, c
   r[3] = make_float4(alb.x, alb.y, alb.z, 0.f);
 }
 
+// ---- where a path's scene comes from ------------------------------------------------------------
+// The wavefront kernels are written once over a scene source: one scene passed as a kernel
+// parameter (pbrt_render, the cached render), or the batch table indexed by the path's scene.
+struct PathSettings {
+  uint32_t max_depth, rr_start, naive;
+  float near, far;
+};
+
+struct OneScene {
+  SceneView v;
+  PathSettings ps;
+  PBRT_DEV const SceneView& view(const WaveBuffers&, uint32_t) const { return v; }
+  PBRT_DEV PathSettings settings(const WaveBuffers&, uint32_t) const { return ps; }
+};
+
+struct ManyScenes {
+  const BatchScene* b;
+  PBRT_DEV const SceneView& view(const WaveBuffers& w, uint32_t p) const { return b[w.scene[p]].view; }
+  PBRT_DEV PathSettings settings(const WaveBuffers& w, uint32_t p) const {
+    const BatchScene& e = b[w.scene[p]];
+    return PathSettings{e.max_depth, e.rr_start, e.naive, e.cam.near, e.cam.far};
+  }
+};
+
 // ---- kernels ---------------------------------------------------------------------------------
+// A new path for image pixel `pixel`, sample `sample`: jitter, camera ray, fresh state.
+PBRT_DEV void start_path(const WaveBuffers& w, uint32_t i, const CameraRec& cam, unsigned long long seed,
+                         uint32_t pixel, uint32_t sample) {
+  const unsigned long long inc = pcg_inc(pixel);
+  unsigned long long st = pcg_seed(seed, pixel, sample);
+  const float jx = pcg_uniform(st, inc), jy = pcg_uniform(st, inc);  // Sampler2::sample (mt.rs:145-150)
+  F3 o, d;
+  camera_ray(cam, fa(float(pixel % cam.width), jx), fa(float(pixel / cam.width), jy), o, d);
+  w.ox[i] = o.x; w.oy[i] = o.y; w.oz[i] = o.z;
+  w.dx[i] = d.x; w.dy[i] = d.y; w.dz[i] = d.z;
+  w.br[i] = 1.f; w.bg[i] = 1.f; w.bb[i] = 1.f;
+  w.lr[i] = 0.f; w.lg[i] = 0.f; w.lb[i] = 0.f;
+  w.rng[i] = st;
+  w.pixel[i] = pixel;
+  w.flags[i] = kSpecularBit;  // is_last_bounce_specular starts true (path.rs:52)
+  w.qa[i] = i;
+}
+
 __global__ void __launch_bounds__(256) k_generate(WaveBuffers w, CameraRec cam, uint64_t wave_base, uint32_t n,
                                                   uint32_t npix, uint32_t sample_offset, unsigned long long seed,
-                                                  uint32_t random_pixels, uint32_t stride, uint32_t film_w) {
+                                                  uint32_t random_pixels, uint32_t stride, uint32_t film_w,
+                                                  unsigned long long* stats) {
+  if (stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(stats + 2, (unsigned long long)n);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint64_t g = wave_base + i;
     const uint32_t q = uint32_t(g % npix);  // film pixel
@@ -292,43 +336,60 @@ __global__ void __launch_bounds__(256) k_generate(WaveBuffers w, CameraRec cam, 
       pixel = uint32_t(splitmix64(seed + g) % (unsigned long long)(cam.width * cam.height));
       sample = uint32_t(g);
     }
-    const unsigned long long inc = pcg_inc(pixel);
-    unsigned long long st = pcg_seed(seed, pixel, sample);
-    const float jx = pcg_uniform(st, inc), jy = pcg_uniform(st, inc);  // Sampler2::sample (mt.rs:145-150)
-    F3 o, d;
-    camera_ray(cam, fa(float(pixel % cam.width), jx), fa(float(pixel / cam.width), jy), o, d);
-    w.ox[i] = o.x; w.oy[i] = o.y; w.oz[i] = o.z;
-    w.dx[i] = d.x; w.dy[i] = d.y; w.dz[i] = d.z;
-    w.br[i] = 1.f; w.bg[i] = 1.f; w.bb[i] = 1.f;
-    w.lr[i] = 0.f; w.lg[i] = 0.f; w.lb[i] = 0.f;
-    w.rng[i] = st;
-    w.pixel[i] = pixel;
-    w.flags[i] = kSpecularBit;  // is_last_bounce_specular starts true (path.rs:52)
-    w.qa[i] = i;
+    start_path(w, i, cam, seed, pixel, sample);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) w.counts[0] = n;
 }
 
-__global__ void __launch_bounds__(128) k_extend(WaveBuffers w, SceneView s, const uint32_t* __restrict__ q,
-                                                const uint32_t* __restrict__ qcount, float near, float far,
-                                                uint32_t* err) {
+__global__ void __launch_bounds__(256) k_generate_batch(WaveBuffers w, const BatchScene* __restrict__ b,
+                                                        uint32_t nscenes, uint64_t wave_base, uint32_t n,
+                                                        const uint32_t* __restrict__ frame, unsigned long long* stats) {
+  if (stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(stats + 2, (unsigned long long)n);
+  const uint32_t f = *frame;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned long long g = wave_base + i;
+    uint32_t lo = 0, hi = nscenes - 1;  // the last scene whose range starts at or before g
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (b[mid].begin <= g) lo = mid;
+      else hi = mid - 1;
+    }
+    const BatchScene& e = b[lo];
+    const unsigned long long l = g - e.begin;
+    const uint32_t q = uint32_t(l % e.npix);
+    const uint32_t pixel = (q / e.film_w) * e.stride * e.cam.width + (q % e.film_w) * e.stride;
+    const uint32_t sample = e.sample_offset + f * e.spp + uint32_t(l / e.npix);
+    start_path(w, i, e.cam, e.seed, pixel, sample);
+    w.scene[i] = lo;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) w.counts[0] = n;
+}
+
+template <class Src>
+__global__ void __launch_bounds__(256) k_extend(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
+                                                const uint32_t* __restrict__ qcount, uint32_t* err,
+                                                unsigned long long* stats) {
   const uint32_t n = *qcount;
+  if (stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(stats, (unsigned long long)n);
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const uint32_t p = q[k];
+    const SceneView& s = src.view(w, p);
+    const PathSettings ps = src.settings(w, p);
     const F3 o = mk3(w.ox[p], w.oy[p], w.oz[p]), d = mk3(w.dx[p], w.dy[p], w.dz[p]);
     float t = 0.f;
     uint32_t obj = 0xFFFFFFFFu, prim = 0;
-    if (!scene_closest(s, o, d, near, far, t, obj, prim, err)) obj = 0xFFFFFFFFu;
+    if (!scene_closest(s, o, d, ps.near, ps.far, t, obj, prim, err)) obj = 0xFFFFFFFFu;
     w.ht[p] = t;
     w.hobj[p] = obj;
     w.hprim[p] = prim;
   }
 }
 
-__global__ void __launch_bounds__(128) k_shade(WaveBuffers w, SceneView s, const uint32_t* __restrict__ q,
+template <class Src>
+__global__ void __launch_bounds__(256) k_shade(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
                                                const uint32_t* __restrict__ qcount, uint32_t* __restrict__ qout,
-                                               uint32_t* __restrict__ qout_count, uint32_t max_depth, uint32_t rr_start,
-                                               uint32_t naive, CacheWave cw, uint32_t cache_mode, uint32_t term_hit) {
+                                               uint32_t* __restrict__ qout_count, CacheWave cw, uint32_t cache_mode,
+                                               uint32_t term_hit) {
   const uint32_t n = *qcount;
   // every lane runs the same trip count so the warp-aggregated pushes see full warps
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -343,6 +404,9 @@ __global__ void __launch_bounds__(128) k_shade(WaveBuffers w, SceneView s, const
     float crough = 0.f;
     if (k < n) {
       p = q[k];
+      const SceneView& s = src.view(w, p);
+      const PathSettings ps = src.settings(w, p);
+      const uint32_t max_depth = ps.max_depth, rr_start = ps.rr_start, naive = ps.naive;
       F3 o = mk3(w.ox[p], w.oy[p], w.oz[p]), d = mk3(w.dx[p], w.dy[p], w.dz[p]);
       F3 beta = mk3(w.br[p], w.bg[p], w.bb[p]);
       F3 L = mk3(w.lr[p], w.lg[p], w.lb[p]);
@@ -366,9 +430,10 @@ __global__ void __launch_bounds__(128) k_shade(WaveBuffers w, SceneView s, const
           L = add3(L, mk3(fm(m.color[0], beta.x), fm(m.color[1], beta.y), fm(m.color[2], beta.z)));
         bounce++;
         // PathIntegrator stops at the max_depth-th hit, before sampling a light (path.rs:64-67);
-        // the naive estimator scatters at every hit and the host stops extending after
-        // max_depth hits (naive.rs:29-52: li(.., 0) is black).
-        const bool depth_cut = !naive && bounce == max_depth;
+        // the naive estimator also ends there, its emission counted: after max_depth hits its
+        // recursion reaches li(.., 0), which is black (naive.rs:29-52). Paths of every scene of
+        // a batch stop at their own depth, whatever the number of bounce launches.
+        const bool depth_cut = bounce == max_depth;
         const bool cacheable = m.kind == kMatLambertian || m.kind == kMatMetal;
         if (!depth_cut && cacheable && cache_mode != kCacheOff) {
           cp = it.p;
@@ -505,12 +570,15 @@ __global__ void __launch_bounds__(256) k_train_batch(WaveBuffers w, CacheWave cw
   }
 }
 
-__global__ void __launch_bounds__(128) k_shadow(WaveBuffers w, SceneView s, uint32_t* err) {
+template <class Src>
+__global__ void __launch_bounds__(256) k_shadow(WaveBuffers w, Src src, uint32_t* err, unsigned long long* stats) {
   const uint32_t n = w.counts[2];
+  if (stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(stats + 1, (unsigned long long)n);
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const uint32_t p = w.s_path[k];
+    const SceneView& s = src.view(w, p);
     const F3 o = mk3(w.s_ox[k], w.s_oy[k], w.s_oz[k]), d = mk3(w.s_dx[k], w.s_dy[k], w.s_dz[k]);
     if (!scene_any(s, o, d, kShadowEps, w.s_tmax[k], err)) {  // VisibilityTester::unoccluded (lights.rs:67-69)
-      const uint32_t p = w.s_path[k];
       w.lr[p] = fa(w.lr[p], w.s_cr[k]);
       w.lg[p] = fa(w.lg[p], w.s_cg[k]);
       w.lb[p] = fa(w.lb[p], w.s_cb[k]);
@@ -527,6 +595,27 @@ __global__ void __launch_bounds__(256) k_accumulate(WaveBuffers w, uint32_t n, d
     atomicAdd(film + 3 * size_t(pix) + 1, double(w.lg[i]));
     atomicAdd(film + 3 * size_t(pix) + 2, double(w.lb[i]));
   }
+}
+
+__global__ void __launch_bounds__(256) k_accumulate_batch(WaveBuffers w, uint32_t n, const BatchScene* __restrict__ b) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const BatchScene& e = b[w.scene[i]];
+    const uint32_t px = w.pixel[i], iw = e.cam.width;
+    const uint32_t pix = e.stride == 1 ? px : ((px / iw) / e.stride) * e.film_w + (px % iw) / e.stride;
+    double* film = e.film + 3 * size_t(pix);
+    atomicAdd(film, double(w.lr[i]));
+    atomicAdd(film + 1, double(w.lg[i]));
+    atomicAdd(film + 2, double(w.lb[i]));
+  }
+}
+
+// Every scene's film: zero (scale 0) or divide the sums by spp; blockIdx.y is the scene.
+__global__ void k_films_batch(const BatchScene* __restrict__ b, int zero) {
+  const BatchScene& e = b[blockIdx.y];
+  const size_t n = size_t(e.npix) * 3;
+  const double s = zero ? 0.0 : 1.0 / double(e.spp);
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    e.film[i] = zero ? 0.0 : e.film[i] * s;
 }
 
 __global__ void k_scale_film(double* film, size_t n, double s) {
@@ -581,16 +670,13 @@ cudaError_t launch_scene_any(const SceneView& s, const float* rays, uint64_t str
   return cudaGetLastError();
 }
 
-cudaError_t trace_wave(const SceneView& s, const WaveBuffers& w, const CacheWave& cw, const CameraRec& cam,
-                       uint64_t wave_base, uint32_t n, uint32_t npix, const RenderSettings& rs, uint32_t* err,
-                       int sm_count, cudaStream_t st) {
+// extend -> shade -> shadow, `loops` times, over the ping-pong queues.
+template <class Src>
+static cudaError_t bounce_loop(const WaveBuffers& w, const Src& src, const CacheWave& cw, uint32_t loops, bool shadows,
+                               uint32_t cache_mode, uint32_t term_hit, const LaunchShape& sh, unsigned long long* stats,
+                               uint32_t* err, int sm_count, cudaStream_t st) {
   cudaError_t e;
-  k_generate<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, cam, wave_base, n, npix, rs.sample_offset, rs.seed,
-                                                             rs.random_pixels, rs.stride,
-                                                             rs.film_w ? rs.film_w : cam.width);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  const unsigned g128 = unsigned(sm_count) * 16;
-  const uint32_t loops = rs.loop_depth ? rs.loop_depth : rs.max_depth;
+  const unsigned gt = unsigned(sm_count) * sh.trace_blocks_per_sm, gs = unsigned(sm_count) * sh.shade_blocks_per_sm;
   for (uint32_t b = 0; b < loops; ++b) {
     uint32_t* qin = (b & 1) ? w.qb : w.qa;
     uint32_t* qout = (b & 1) ? w.qa : w.qb;
@@ -598,13 +684,61 @@ cudaError_t trace_wave(const SceneView& s, const WaveBuffers& w, const CacheWave
     uint32_t* cout = w.counts + ((b + 1) & 1);
     if ((e = cudaMemsetAsync(cout, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.counts + 2, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
-    k_extend<<<g128, 128, 0, st>>>(w, s, qin, cin, cam.near, cam.far, err);
-    k_shade<<<g128, 128, 0, st>>>(w, s, qin, cin, qout, cout, rs.max_depth, rs.rr_start, rs.naive, cw, rs.cache_mode,
-                                  rs.term_hit);
-    if (!rs.naive) k_shadow<<<g128, 128, 0, st>>>(w, s, err);
+    k_extend<Src><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, err, stats);
+    k_shade<Src><<<gs, sh.shade_threads, 0, st>>>(w, src, qin, cin, qout, cout, cw, cache_mode, term_hit);
+    if (shadows) k_shadow<Src><<<gt, sh.trace_threads, 0, st>>>(w, src, err, stats);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, uint32_t nscenes, const WaveBuffers& w,
+                         uint32_t wave, const uint32_t* frame, uint32_t max_depth, bool any_path_integrator,
+                         const LaunchShape& shape, unsigned long long* stats, uint32_t* err, int sm_count,
+                         cudaStream_t st, cudaEvent_t* done) {
+  cudaError_t e;
+  uint32_t max_npix = 0;
+  for (uint32_t i = 0; i < nscenes; ++i) max_npix = max_npix > host_table[i].npix ? max_npix : host_table[i].npix;
+  const dim3 fgrid(unsigned((size_t(max_npix) * 3 + 255) / 256 < 1024 ? (size_t(max_npix) * 3 + 255) / 256 : 1024),
+                   nscenes);
+  k_films_batch<<<fgrid, 256, 0, st>>>(table, 1);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const unsigned long long total =
+      host_table[nscenes - 1].begin + (unsigned long long)host_table[nscenes - 1].npix * host_table[nscenes - 1].spp;
+  const ManyScenes src{table};
+  uint32_t next_done = 0;
+  for (unsigned long long base = 0; base < total; base += wave) {
+    const uint32_t n = uint32_t(total - base < wave ? total - base : wave);
+    k_generate_batch<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, table, nscenes, base, n, frame, stats);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = bounce_loop(w, src, CacheWave{}, max_depth, any_path_integrator, kCacheOff, 0, shape, stats, err, sm_count,
+                         st)) != cudaSuccess)
+      return e;
+    k_accumulate_batch<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, n, table);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // scenes whose last path was in this wave are done
+    while (done && next_done < nscenes &&
+           host_table[next_done].begin + (unsigned long long)host_table[next_done].npix * host_table[next_done].spp <=
+               base + n) {
+      if ((e = cudaEventRecordWithFlags(done[next_done], st, cudaEventRecordExternal)) != cudaSuccess) return e;
+      ++next_done;
+    }
+  }
+  k_films_batch<<<fgrid, 256, 0, st>>>(table, 0);
+  return cudaGetLastError();
+}
+
+cudaError_t trace_wave(const SceneView& s, const WaveBuffers& w, const CacheWave& cw, const CameraRec& cam,
+                       uint64_t wave_base, uint32_t n, uint32_t npix, const RenderSettings& rs, uint32_t* err,
+                       int sm_count, cudaStream_t st) {
+  cudaError_t e;
+  k_generate<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, cam, wave_base, n, npix, rs.sample_offset, rs.seed,
+                                                             rs.random_pixels, rs.stride,
+                                                             rs.film_w ? rs.film_w : cam.width, rs.stats);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const OneScene src{s, PathSettings{rs.max_depth, rs.rr_start, rs.naive, cam.near, cam.far}};
+  return bounce_loop(w, src, cw, rs.loop_depth ? rs.loop_depth : rs.max_depth, !rs.naive, rs.cache_mode, rs.term_hit,
+                     rs.shape, rs.stats, err, sm_count, st);
 }
 
 cudaError_t accumulate_wave(const WaveBuffers& w, uint32_t n, double* film, uint32_t image_w, const RenderSettings& rs,

@@ -12,17 +12,23 @@
 namespace pbrt {
 namespace {
 
+// min / max with the tie rule of the C library's fmin / fmax (the first argument wins a tie,
+// which only matters for the sign of a zero); inputs are finite (checked before the build).
+inline float mn(float x, float y) { return y < x ? y : x; }
+inline float mx(float x, float y) { return x < y ? y : x; }
+
 struct Box {
   float lo[3], hi[3];
   void set_empty() {
     for (int a = 0; a < 3; ++a) { lo[a] = FLT_MAX; hi[a] = -FLT_MAX; }
   }
-  void grow(const Box& b) {
+  void grow(const float* l, const float* h) {
     for (int a = 0; a < 3; ++a) {
-      lo[a] = std::fmin(lo[a], b.lo[a]);
-      hi[a] = std::fmax(hi[a], b.hi[a]);
+      lo[a] = mn(lo[a], l[a]);
+      hi[a] = mx(hi[a], h[a]);
     }
   }
+  void grow(const Box& b) { grow(b.lo, b.hi); }
   bool empty() const { return lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]; }
   // AABoundingBox::half_area (src/geom/aabound.rs:123-130)
   float half_area() const {
@@ -39,35 +45,42 @@ struct RefNode {
   uint32_t depth;
 };
 
+// One triangle as the build sees it. The records themselves are permuted by the partition
+// (the same permutation the reference applies to its index list), so every pass over a
+// node's triangles reads memory in order.
+struct TriRef {
+  float c[3];          // centroid
+  float lo[3], hi[3];  // bounds
+  uint32_t id;
+};
+
 class Builder {
  public:
   Builder(const float* v, const uint32_t* idx, uint32_t n, const MeshBuildParams& p) : v_(v), idx_(idx), n_(n), p_(p) {}
 
   void run(std::vector<RefNode>* nodes_out, std::vector<uint32_t>* order_out) {
-    tri_box_.resize(n_);
-    for (int a = 0; a < 3; ++a) cen_[a].resize(n_);
+    refs_.resize(n_);
     const float third = 1.0f / 3.0f;
     for (uint32_t i = 0; i < n_; ++i) {
       const float* p0 = v_ + 3 * size_t(idx_[3 * size_t(i)]);
       const float* p1 = v_ + 3 * size_t(idx_[3 * size_t(i) + 1]);
       const float* p2 = v_ + 3 * size_t(idx_[3 * size_t(i) + 2]);
-      Box& b = tri_box_[i];
+      TriRef& r = refs_[i];
       for (int a = 0; a < 3; ++a) {
         // aabound_from_triangle (bvh.rs:564-572)
-        b.lo[a] = std::fmin(std::fmin(p0[a], p1[a]), p2[a]);
-        b.hi[a] = std::fmax(std::fmax(p0[a], p1[a]), p2[a]);
+        r.lo[a] = mn(mn(p0[a], p1[a]), p2[a]);
+        r.hi[a] = mx(mx(p0[a], p1[a]), p2[a]);
         // tri_centroid (bvh.rs:578-584)
         float c = p0[a];
         c = c + p1[a];
         c = c + p2[a];
-        cen_[a][i] = c * third;
+        r.c[a] = c * third;
       }
+      r.id = i;
     }
-    order_.resize(n_);
-    for (uint32_t i = 0; i < n_; ++i) order_[i] = i;
 
     nodes_.clear();
-    nodes_.reserve(size_t(2) * n_);
+    nodes_.reserve(size_t(2) * n_ / std::max<uint32_t>(1, p_.max_leaf) + 2);
     RefNode root;
     root.left_first = 0;
     root.count = n_;
@@ -76,52 +89,64 @@ class Builder {
     nodes_.push_back(root);
 
     // Depth-first, left child first: the same node numbering as the reference's recursion.
+    const int B = p_.bins, S = B - 1;
     std::vector<uint32_t> stack;
     stack.push_back(0);
-    std::vector<Box> bin_box(p_.bins);
-    std::vector<uint32_t> bin_cnt(p_.bins);
-    std::vector<float> la(p_.bins), ra(p_.bins);
-    std::vector<uint32_t> lc(p_.bins), rc(p_.bins);
+    std::vector<Box> bin_box(size_t(3) * B);
+    std::vector<uint32_t> bin_cnt(size_t(3) * B);
+    std::vector<float> la(B), ra(B);
+    std::vector<uint32_t> lc(B), rc(B);
     while (!stack.empty()) {
       const uint32_t ni = stack.back();
       stack.pop_back();
       const uint32_t first = nodes_[ni].left_first, count = nodes_[ni].count;
       if (count <= p_.max_leaf) continue;
       const float leaf_cost = nodes_[ni].box.half_area() * float(count);
+      const TriRef* rr = refs_.data() + first;
+
+      // centroid extent of every axis in one pass
+      float cmin[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, cmax[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+      for (uint32_t k = 0; k < count; ++k)
+        for (int a = 0; a < 3; ++a) {
+          cmin[a] = mn(cmin[a], rr[k].c[a]);
+          cmax[a] = mx(cmax[a], rr[k].c[a]);
+        }
+      bool use[3];
+      float width[3];
+      for (int a = 0; a < 3; ++a) {
+        use[a] = !(cmin[a] == cmax[a]);
+        width[a] = (cmax[a] - cmin[a]) / float(B);
+        for (int b = 0; b < B; ++b) {
+          bin_box[a * B + b].set_empty();
+          bin_cnt[a * B + b] = 0;
+        }
+      }
+      // the bins of every splittable axis in one pass
+      for (uint32_t k = 0; k < count; ++k)
+        for (int a = 0; a < 3; ++a) {
+          if (!use[a]) continue;
+          const int b = a * B + bin_of(rr[k].c[a], cmin[a], width[a]);
+          bin_box[b].grow(rr[k].lo, rr[k].hi);
+          bin_cnt[b]++;
+        }
 
       bool have = false;
       int best_axis = 0, best_boundary = 0;
-      float best_cmin = 0, best_width = 0, best_cost = 0;
+      float best_cost = 0;
       for (int a = 0; a < 3; ++a) {
-        const std::vector<float>& c = cen_[a];
-        float cmin = FLT_MAX, cmax = -FLT_MAX;
-        for (uint32_t k = first; k < first + count; ++k) {
-          const float x = c[order_[k]];
-          cmin = std::fmin(cmin, x);
-          cmax = std::fmax(cmax, x);
-        }
-        if (cmin == cmax) continue;
-        const float width = (cmax - cmin) / float(p_.bins);
-        for (int b = 0; b < p_.bins; ++b) { bin_box[b].set_empty(); bin_cnt[b] = 0; }
-        for (uint32_t k = first; k < first + count; ++k) {
-          const uint32_t t = order_[k];
-          const int b = bin_of(c[t], cmin, width);
-          bin_box[b].grow(tri_box_[t]);
-          bin_cnt[b]++;
-        }
-        const int S = p_.bins - 1;
+        if (!use[a]) continue;
         Box lb, rb;
         lb.set_empty();
         rb.set_empty();
         uint32_t ls = 0, rs = 0;
         for (int i = 0; i < S; ++i) {
-          lb.grow(bin_box[i]);
-          ls += bin_cnt[i];
+          lb.grow(bin_box[a * B + i]);
+          ls += bin_cnt[a * B + i];
           la[i] = lb.half_area();
           lc[i] = ls;
           const int m = S - 1 - i;
-          rb.grow(bin_box[m + 1]);
-          rs += bin_cnt[m + 1];
+          rb.grow(bin_box[a * B + m + 1]);
+          rs += bin_cnt[a * B + m + 1];
           ra[m] = rb.half_area();
           rc[m] = rs;
         }
@@ -132,20 +157,19 @@ class Builder {
             have = true;
             best_axis = a;
             best_boundary = b;
-            best_cmin = cmin;
-            best_width = width;
             best_cost = cost;
           }
         }
       }
       if (!have || !(best_cost < leaf_cost)) continue;
 
-      // Forward-swap partition by bin index (bvh.rs:260-267).
-      const std::vector<float>& c = cen_[best_axis];
+      // Forward-swap partition by bin index (bvh.rs:260-267), children's boxes on the way.
+      TriRef* w = refs_.data();
+      const float bmin = cmin[best_axis], bw = width[best_axis];
       uint32_t left_end = first;
       for (uint32_t k = first; k < first + count; ++k) {
-        if (bin_of(c[order_[k]], best_cmin, best_width) <= best_boundary) {
-          std::swap(order_[k], order_[left_end]);
+        if (bin_of(w[k].c[best_axis], bmin, bw) <= best_boundary) {
+          std::swap(w[k], w[left_end]);
           left_end++;
         }
       }
@@ -170,31 +194,31 @@ class Builder {
       stack.push_back(li);
     }
     nodes_out->swap(nodes_);
-    order_out->swap(order_);
+    order_out->resize(n_);
+    for (uint32_t k = 0; k < n_; ++k) (*order_out)[k] = refs_[k].id;
   }
 
  private:
-  // bin_index (bvh.rs:173-176) with Rust's saturating float-to-usize cast.
+  // bin_index (bvh.rs:173-176): floor, then Rust's saturating float-to-usize cast. For
+  // 0 <= q < bins - 1 the floor is the truncation; q < 0 and NaN give 0, q >= bins - 1 the
+  // last bin (floor(q) >= bins - 1 exactly when q >= bins - 1, bins - 1 being an integer).
   int bin_of(float pos, float cmin, float width) const {
     const float q = (pos - cmin) / width;
-    const float f = std::floor(q);
-    if (!(f >= 0.0f)) return 0;
-    if (f >= float(p_.bins - 1)) return p_.bins - 1;
-    return int(f);
+    if (!(q >= 0.0f)) return 0;
+    if (q >= float(p_.bins - 1)) return p_.bins - 1;
+    return int(q);
   }
 
   void bounds(uint32_t first, uint32_t count, Box* out) const {
     out->set_empty();
-    for (uint32_t k = first; k < first + count; ++k) out->grow(tri_box_[order_[k]]);
+    for (uint32_t k = first; k < first + count; ++k) out->grow(refs_[k].lo, refs_[k].hi);
   }
 
   const float* v_;
   const uint32_t* idx_;
   uint32_t n_;
   MeshBuildParams p_;
-  std::vector<Box> tri_box_;
-  std::vector<float> cen_[3];
-  std::vector<uint32_t> order_;
+  std::vector<TriRef> refs_;
   std::vector<RefNode> nodes_;
 };
 

@@ -5,11 +5,10 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "scene_device.cuh"
 #include "scene_types.hpp"
 
 namespace pbrt {
-
-struct SceneView;
 
 // SoA state of one wave of paths (capacity = the wave size) and its queues.
 struct WaveBuffers {
@@ -18,6 +17,7 @@ struct WaveBuffers {
   float *lr, *lg, *lb;                 // radiance gathered so far (FP32 per sample)
   unsigned long long* rng;             // PCG32 state (the increment derives from the pixel)
   uint32_t* pixel;
+  uint32_t* scene;                     // batched renders: the path's scene (index into the batch table)
   uint32_t* flags;                     // bounce count (low 16 bits) | last-bounce-specular (bit 31)
   float* ht;                           // nearest hit of the current ray
   uint32_t *hobj, *hprim;
@@ -49,6 +49,13 @@ struct CacheWave {
   uint32_t* counts;  // [0] queries, [1] training vertices offered (may exceed tcap), [2] batch valid
 };
 
+// Launch shape of the wavefront kernels: threads per block and the resident-block target per
+// SM of the grid-stride traversal kernels (extend, shadow) and of the shading kernel.
+struct LaunchShape {
+  uint32_t trace_threads = 128, trace_blocks_per_sm = 16;
+  uint32_t shade_threads = 128, shade_blocks_per_sm = 16;
+};
+
 struct RenderSettings {
   uint32_t max_depth, rr_start, sample_offset, naive;
   unsigned long long seed;
@@ -58,8 +65,30 @@ struct RenderSettings {
   uint32_t loop_depth = 0;     // bounce iterations the host launches (0: max_depth); no path
                                // may still be alive after them
   uint32_t stride = 1;         // film pixel (i, j) is image pixel (stride*i, stride*j)
+  unsigned long long* stats = nullptr;  // when set: += rays traced, shadow rays, paths
   uint32_t film_w = 0;         // film columns (0: the image width)
+  LaunchShape shape;
 };
+
+// One scene of a batched render (device table entry). Global path index g belongs to the
+// scene with begin <= g < begin + npix * spp; its local index l = g - begin renders film
+// pixel l % npix, sample sample_offset + frame * spp + l / npix.
+struct BatchScene {
+  SceneView view;
+  CameraRec cam;
+  double* film;       // sums; scaled by 1 / spp at the end
+  unsigned long long begin, seed;
+  uint32_t npix, spp, max_depth, rr_start, sample_offset, naive, stride, film_w;
+};
+
+// A batched frame: waves of `wave` paths over all scenes' paths (scenes in table order); the
+// kernels read the frame number from `frame` (device memory), so a captured graph of these
+// launches renders any frame. `done[s]`, when given, is recorded (as an external event, so it
+// survives stream capture) right after the wave that completes scene s.
+cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, uint32_t nscenes, const WaveBuffers& w,
+                         uint32_t wave, const uint32_t* frame, uint32_t max_depth, bool any_path_integrator,
+                         const LaunchShape& shape, unsigned long long* stats, uint32_t* err, int sm_count,
+                         cudaStream_t st, cudaEvent_t* done);
 
 // One wave: generate, max_depth x (extend, shade, shadow), accumulate into `film` (sums).
 // `npix` is the number of film pixels (the image's, or the strided subset's).

@@ -62,6 +62,24 @@ class Context:
     def sync(self):
         self.check(self.lib.pbrt_ctx_sync(self.h), "pbrt_ctx_sync")
 
+    def set_tuning(self, wave_paths: int = 0, trace_threads: int = 0, trace_blocks_per_sm: int = 0,
+                   shade_threads: int = 0, shade_blocks_per_sm: int = 0):
+        """Launch shape of the wavefront (zeros: defaults); applies to later renders/batches."""
+        t = _capi.Tuning(int(wave_paths), int(trace_threads), int(trace_blocks_per_sm), int(shade_threads),
+                         int(shade_blocks_per_sm))
+        self.check(self.lib.pbrt_ctx_set_tuning(self.h, C.byref(t)), "pbrt_ctx_set_tuning")
+
+    def tuning(self) -> dict:
+        t = _capi.Tuning()
+        self.check(self.lib.pbrt_ctx_get_tuning(self.h, C.byref(t)), "pbrt_ctx_get_tuning")
+        return {k: getattr(t, k) for k, _ in _capi.Tuning._fields_}
+
+    def render_stats(self) -> dict:
+        """Rays, shadow rays and paths of the last render on this context."""
+        out = np.zeros(3, np.uint64)
+        self.check(self.lib.pbrt_ctx_render_stats(self.h, out.ctypes.data), "pbrt_ctx_render_stats")
+        return dict(rays=int(out[0]), shadow_rays=int(out[1]), paths=int(out[2]))
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.pbrt_ctx_destroy(self.h)
@@ -377,52 +395,7 @@ class Scene:
             self.ctx = default_context()
         self.release()
         desc = self.describe(bvh_bins, bvh_max_leaf)
-        keep = []
-        meshes = []
-        for m in desc["meshes"]:
-            v = np.ascontiguousarray(m["vertices"], np.float32).reshape(-1, 3)
-            i = np.ascontiguousarray(m["indices"], np.uint32).reshape(-1, 3)
-            keep += [v, i]
-            fm = None
-            if m.get("face_materials") is not None:
-                fm = np.ascontiguousarray(m["face_materials"], np.uint32)
-                keep.append(fm)
-            meshes.append(_capi.MeshDesc(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0],
-                                         fm.ctypes.data if fm is not None else None))
-        mats = []
-        for m in desc["materials"]:
-            d = _capi.MaterialDesc()
-            d.kind = int(m["kind"])
-            d.color[:] = [float(c) for c in m["color"]]
-            d.fuzz, d.ior = float(m.get("fuzz", 0.0)), float(m.get("ior", 1.0))
-            mats.append(d)
-        objs = []
-        for o in desc["objects"]:
-            d = _capi.ObjectDesc()
-            d.shape, d.mesh = int(o["shape"]), int(o.get("mesh", 0))
-            d.radius, d.height = float(o.get("radius", 0.0)), float(o.get("height", 0.0))
-            d.material = int(o["material"])
-            if o.get("to_world") is not None:
-                d.transformed = 1
-                d.to_world[:] = [float(x) for x in np.asarray(o["to_world"], np.float32).reshape(-1)[:12]]
-                d.to_local[:] = [float(x) for x in np.asarray(o["to_local"], np.float32).reshape(-1)[:12]]
-            objs.append(d)
-        lights = []
-        for l in desc["lights"]:
-            d = _capi.LightDesc()
-            d.kind = int(l["kind"])
-            for k in ("position", "radiance", "bottom", "top"):
-                getattr(d, k)[:] = [float(x) for x in l.get(k, (0.0, 0.0, 0.0))]
-            d.object = int(l.get("object", 0))
-            lights.append(d)
-        arrays = ((_capi.MeshDesc * max(1, len(meshes)))(*meshes), (_capi.MaterialDesc * max(1, len(mats)))(*mats),
-                  (_capi.ObjectDesc * max(1, len(objs)))(*objs), (_capi.LightDesc * max(1, len(lights)))(*lights))
-        sd = _capi.SceneDesc()
-        sd.meshes, sd.mesh_count = C.cast(arrays[0], C.POINTER(_capi.MeshDesc)), len(meshes)
-        sd.materials, sd.material_count = C.cast(arrays[1], C.POINTER(_capi.MaterialDesc)), len(mats)
-        sd.objects, sd.object_count = C.cast(arrays[2], C.POINTER(_capi.ObjectDesc)), len(objs)
-        sd.lights, sd.light_count = C.cast(arrays[3], C.POINTER(_capi.LightDesc)), len(lights)
-        sd.bvh_bins, sd.bvh_max_leaf = int(desc.get("bvh_bins", bvh_bins)), int(desc.get("bvh_max_leaf", bvh_max_leaf))
+        sd, keep = _lower_description(desc, bvh_bins, bvh_max_leaf)
         h = C.c_void_p()
         self.ctx.check(self.ctx.lib.pbrt_scene_create(self.ctx.h, C.byref(sd), C.byref(h)), "pbrt_scene_create")
         self.h = h
@@ -506,6 +479,128 @@ class Scene:
     def __del__(self):
         try:
             self.release()
+        except Exception:
+            pass
+
+
+def _lower_description(desc: dict, bvh_bins: int = 8, bvh_max_leaf: int = 1):
+    """The C pbrt_scene_desc of a description dict, with the arrays it points into."""
+    keep = []
+    meshes = []
+    for m in desc["meshes"]:
+        v = np.ascontiguousarray(m["vertices"], np.float32).reshape(-1, 3)
+        i = np.ascontiguousarray(m["indices"], np.uint32).reshape(-1, 3)
+        keep += [v, i]
+        fm = None
+        if m.get("face_materials") is not None:
+            fm = np.ascontiguousarray(m["face_materials"], np.uint32)
+            keep.append(fm)
+        meshes.append(_capi.MeshDesc(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0],
+                                     fm.ctypes.data if fm is not None else None))
+    mats = []
+    for m in desc["materials"]:
+        d = _capi.MaterialDesc()
+        d.kind = int(m["kind"])
+        d.color[:] = [float(c) for c in m["color"]]
+        d.fuzz, d.ior = float(m.get("fuzz", 0.0)), float(m.get("ior", 1.0))
+        mats.append(d)
+    objs = []
+    for o in desc["objects"]:
+        d = _capi.ObjectDesc()
+        d.shape, d.mesh = int(o["shape"]), int(o.get("mesh", 0))
+        d.radius, d.height = float(o.get("radius", 0.0)), float(o.get("height", 0.0))
+        d.material = int(o["material"])
+        if o.get("to_world") is not None:
+            d.transformed = 1
+            d.to_world[:] = [float(x) for x in np.asarray(o["to_world"], np.float32).reshape(-1)[:12]]
+            d.to_local[:] = [float(x) for x in np.asarray(o["to_local"], np.float32).reshape(-1)[:12]]
+        objs.append(d)
+    lights = []
+    for l in desc["lights"]:
+        d = _capi.LightDesc()
+        d.kind = int(l["kind"])
+        for k in ("position", "radiance", "bottom", "top"):
+            getattr(d, k)[:] = [float(x) for x in l.get(k, (0.0, 0.0, 0.0))]
+        d.object = int(l.get("object", 0))
+        lights.append(d)
+    arrays = ((_capi.MeshDesc * max(1, len(meshes)))(*meshes), (_capi.MaterialDesc * max(1, len(mats)))(*mats),
+              (_capi.ObjectDesc * max(1, len(objs)))(*objs), (_capi.LightDesc * max(1, len(lights)))(*lights))
+    sd = _capi.SceneDesc()
+    sd.meshes, sd.mesh_count = C.cast(arrays[0], C.POINTER(_capi.MeshDesc)), len(meshes)
+    sd.materials, sd.material_count = C.cast(arrays[1], C.POINTER(_capi.MaterialDesc)), len(mats)
+    sd.objects, sd.object_count = C.cast(arrays[2], C.POINTER(_capi.ObjectDesc)), len(objs)
+    sd.lights, sd.light_count = C.cast(arrays[3], C.POINTER(_capi.LightDesc)), len(lights)
+    sd.bvh_bins, sd.bvh_max_leaf = int(desc.get("bvh_bins", bvh_bins)), int(desc.get("bvh_max_leaf", bvh_max_leaf))
+    keep.append(arrays)
+    return sd, keep
+
+
+def create_scenes(descs, ctx: Optional[Context] = None, threads: int = 0, bvh_bins: int = 8,
+                  bvh_max_leaf: int = 1) -> list:
+    """Committed Scenes of many descriptions at once: the host-side BVH builds run on
+    `threads` threads (0: all cores) inside pbrt_scene_create_many."""
+    ctx = ctx or default_context()
+    lowered = [_lower_description(d, bvh_bins, bvh_max_leaf) for d in descs]
+    arr = (_capi.SceneDesc * len(lowered))(*[sd for sd, _ in lowered])
+    hs = (C.c_void_p * len(lowered))()
+    ctx.check(ctx.lib.pbrt_scene_create_many(ctx.h, arr, len(lowered), int(threads), hs), "pbrt_scene_create_many")
+    out = []
+    for d, h in zip(descs, hs):
+        sc = Scene.from_description(d, ctx)
+        sc.h = C.c_void_p(h)
+        out.append(sc)
+    return out
+
+
+def render_params(camera: dict, spp: int, max_depth: int, seed: int = 1, rr_start: int = 0, sample_offset: int = 0,
+                  integrator: str = "path", pixel_stride: int = 1) -> "_capi.RenderParams":
+    p = _capi.RenderParams()
+    p.camera = camera_desc(camera)
+    p.spp, p.max_depth, p.rr_start, p.sample_offset = int(spp), int(max_depth), int(rr_start), int(sample_offset)
+    p.seed, p.integrator, p.pixel_stride = int(seed), 1 if integrator == "naive" else 0, int(pixel_stride)
+    return p
+
+
+class Batch:
+    """Many committed scenes rendered together (pbrt_batch): one wavefront over all their
+    paths, its launch sequence recorded once in a CUDA graph. `params` are render_params()
+    per scene."""
+
+    def __init__(self, scenes, params, ctx: Optional[Context] = None):
+        self.ctx = ctx or scenes[0].ctx
+        self.scenes = list(scenes)  # kept alive: the batch refers to their device data
+        self.params = list(params)
+        hs = (C.c_void_p * len(scenes))(*[s.h.value if isinstance(s.h, C.c_void_p) else s.h for s in scenes])
+        ps = (_capi.RenderParams * len(params))(*params)
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.pbrt_batch_create(self.ctx.h, hs, ps, len(scenes), C.byref(h)), "pbrt_batch_create")
+        self.h = h
+
+    def film_shapes(self):
+        out = []
+        for p in self.params:
+            s = max(1, p.pixel_stride)
+            out.append((-(-p.camera.height // s), -(-p.camera.width // s), 3))
+        return out
+
+    def render(self, frame: int = 0, films=None, scene_times: bool = False):
+        """Films (numpy float64 by default, or the given host/device arrays) and, with
+        scene_times, each scene's completion time in ms from the frame's start."""
+        if films is None:
+            films = [np.zeros(sh, np.float64) for sh in self.film_shapes()]
+        fp = (C.c_void_p * len(films))(*[_ptr(f) if f is not None else None for f in films])
+        ms = (C.c_float * len(self.scenes))() if scene_times else None
+        self.ctx.check(self.ctx.lib.pbrt_batch_render(self.h, int(frame), fp, ms), "pbrt_batch_render")
+        return (films, list(ms)) if scene_times else films
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.ctx.h is not None:
+            self.ctx.lib.pbrt_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass
 

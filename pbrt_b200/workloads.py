@@ -328,3 +328,35 @@ def radiance_cache_scene(width: int = 1920, height: int = 1080, segments: int = 
     desc["objects"].append(dict(shape=0, mesh=len(desc["meshes"]) - 1, material=base, to_world=None, to_local=None))
     desc["bvh_bins"], desc["bvh_max_leaf"] = 16, 4
     return desc, camera
+
+
+def batch_scenes(n: int = 64, seed: int = 3, width: int = 512, height: int = 512, max_depth: int = 8,
+                 levels=(3, 9), spp=(4, 64)):
+    """The batched-rendering workload: n independent scenes, each the closed box of
+    cornell_box (walls and ceiling light, without its inner boxes) around a displaced
+    icosphere (radius 0.3, value-noise amplitude 0.1·r) of level U{levels}, rendered at
+    width x height with U{spp} samples per pixel and max depth max_depth. Scenes of the same
+    level share one seeded mesh; each scene is still committed (and its BVH built) on its
+    own. Returns [(description, camera, spp)] in scene order."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    lv = rng.integers(levels[0], levels[1] + 1, n)
+    sp = rng.integers(spp[0], spp[1] + 1, n)
+    meshes = {}
+    out = []
+    for i in range(n):
+        level = int(lv[i])
+        if level not in meshes:
+            v, f = displaced_icosphere(level, seed=seed * 1000 + level, radius=0.3, amplitude=0.1)
+            meshes[level] = ((v + np.array([0.0, -0.18, -0.05], np.float32)).astype(np.float32), f)
+        desc, cam = cornell_box(width, height)
+        walls = desc["meshes"][0]
+        desc["meshes"][0] = dict(vertices=walls["vertices"][:18], indices=walls["indices"][:6])
+        v, f = meshes[level]
+        desc["materials"].append(dict(kind=0, color=(0.4, 0.5, 0.8)))
+        desc["meshes"].append(dict(vertices=v, indices=f))
+        desc["objects"].append(dict(shape=0, mesh=len(desc["meshes"]) - 1, material=len(desc["materials"]) - 1,
+                                    to_world=None, to_local=None))
+        desc["bvh_bins"], desc["bvh_max_leaf"] = 16, 4
+        desc["level"] = level
+        out.append((desc, cam, int(sp[i])))
+    return out

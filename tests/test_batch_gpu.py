@@ -1,0 +1,127 @@
+"""Batched multi-scene rendering (pbrt_batch): one wavefront over many scenes, replayed as a
+CUDA graph. Each scene's paths are the paths pbrt_render traces for it alone (same sample
+streams, same kernels), so every film must equal the scene's own render, whatever the wave
+size and launch shape."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import pbrt_b200 as pb
+from pbrt_b200 import PbrtError
+from pbrt_b200 import workloads as W
+from pbrt_b200.scene import Batch, create_scenes, render_params
+
+pytestmark = pytest.mark.gpu
+
+
+def _specs():
+    d0, c0 = W.cornell_box(32, 24)
+    d1, c1 = W.many_spheres(300, width=40, height=30)
+    d2, c2 = W.radiance_cache_scene(48, 27, segments=200, sides=10)
+    d3, c3 = W.cornell_box(20, 20)
+    return [(d0, c0, dict(spp=3, max_depth=6)), (d1, c1, dict(spp=2, max_depth=8, rr_start=3)),
+            (d2, c2, dict(spp=2, max_depth=5, pixel_stride=2)), (d3, c3, dict(spp=4, max_depth=4, integrator="naive"))]
+
+
+@pytest.fixture(scope="module")
+def built():
+    specs = _specs()
+    scenes = create_scenes([d for d, _, _ in specs])
+    singles = [s.render(cam, seed=5, **kw) for s, (_, cam, kw) in zip(scenes, specs)]
+    params = [render_params(cam, seed=5, **kw) for _, cam, kw in specs]
+    return specs, scenes, singles, params
+
+
+def _close(a, b):
+    np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-15)
+
+
+def test_batch_films_equal_single_renders(built):
+    specs, scenes, singles, params = built
+    b = Batch(scenes, params)
+    films, ms = b.render(0, scene_times=True)
+    for f, s in zip(films, singles):
+        assert f.shape == s.shape
+        _close(f, s)
+    assert all(t > 0 for t in ms)
+    assert all(ms[i] <= ms[i + 1] + 1e-3 for i in range(len(ms) - 1))  # scenes finish in table order
+    # replaying the graph gives the same frame
+    again = b.render(0)
+    for f, s in zip(again, singles):
+        _close(f, s)
+    b.close()
+
+
+def test_frames_continue_the_sample_sequence(built):
+    specs, scenes, singles, params = built
+    b = Batch(scenes, params)
+    films = b.render(2)
+    for sc, f, (_, cam, kw) in zip(scenes, films, specs):
+        ref = sc.render(cam, seed=5, sample_offset=2 * kw["spp"], **kw)
+        _close(f, ref)
+    b.close()
+
+
+@pytest.mark.parametrize("tuning", [dict(wave_paths=4096), dict(trace_threads=64, trace_blocks_per_sm=32),
+                                    dict(trace_threads=256, trace_blocks_per_sm=4, shade_threads=256,
+                                         shade_blocks_per_sm=2)])
+def test_results_do_not_depend_on_the_launch_shape(built, tuning):
+    specs, scenes, singles, params = built
+    ctx = scenes[0].ctx
+    ctx.set_tuning(**tuning)
+    try:
+        b = Batch(scenes, params)
+        for f, s in zip(b.render(0), singles):
+            _close(f, s)
+        b.close()
+        # single-scene renders follow the context's tuning too
+        _close(scenes[0].render(specs[0][1], seed=5, **specs[0][2]), singles[0])
+    finally:
+        ctx.set_tuning()
+
+
+def test_device_films_and_one_shot(built):
+    torch = pytest.importorskip("torch")
+    specs, scenes, singles, params = built
+    b = Batch(scenes, params)
+    films = [torch.zeros(sh, dtype=torch.float64, device="cuda") for sh in b.film_shapes()]
+    b.render(0, films)
+    for f, s in zip(films, singles):
+        _close(f.cpu().numpy(), s)
+    b.close()
+    import ctypes as C
+    from pbrt_b200 import _capi
+    ctx = scenes[0].ctx
+    hs = (C.c_void_p * 2)(scenes[0].h.value, scenes[1].h.value)
+    ps = (_capi.RenderParams * 2)(params[0], params[1])
+    outs = [np.zeros(s.shape) for s in singles[:2]]
+    fp = (C.c_void_p * 2)(outs[0].ctypes.data, outs[1].ctypes.data)
+    ctx.check(ctx.lib.pbrt_render_batch(hs, ps, 2, fp), "pbrt_render_batch")
+    _close(outs[0], singles[0])
+    _close(outs[1], singles[1])
+
+
+def test_invalid_batches_and_tuning_are_refused(built):
+    specs, scenes, singles, params = built
+    other = pb.Context(0)
+    with pytest.raises(PbrtError):
+        Batch(scenes[:2], params[:2], ctx=other)
+    with pytest.raises(PbrtError):
+        other.set_tuning(trace_threads=48)
+    with pytest.raises(PbrtError):
+        other.set_tuning(wave_paths=10)
+    bad = render_params(specs[0][1], spp=0, max_depth=4)
+    with pytest.raises(PbrtError):
+        Batch(scenes[:1], [bad])
+    other.close()
+
+
+def test_batch_render_stats(built):
+    specs, scenes, singles, params = built
+    b = Batch(scenes, params)
+    b.render(0)
+    st = scenes[0].ctx.render_stats()
+    want = sum(int(np.prod(sh[:2])) * p.spp for sh, p in zip(b.film_shapes(), params))
+    assert st["paths"] == want
+    b.close()

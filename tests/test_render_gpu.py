@@ -150,3 +150,14 @@ def test_pixel_stride_renders_the_same_pixels(stride):
     cfull = scene.render_cached(cache, cam, spp=4, max_depth=6, seed=3, train_rounds=0)
     csub = scene.render_cached(cache, cam, spp=4, max_depth=6, seed=3, train_rounds=0, pixel_stride=stride)
     np.testing.assert_array_equal(csub, cfull[::stride, ::stride])
+
+
+def test_render_stats_count_the_work():
+    desc, cam = W.cornell_box(32, 24)
+    scene = pb.Scene.from_description(desc).commit()
+    scene.render(cam, spp=3, max_depth=5, seed=1)
+    st = scene.ctx.render_stats()
+    assert st["paths"] == 32 * 24 * 3
+    # every path traces its camera ray, at most max_depth rays in all, one shadow ray per hit
+    assert st["paths"] <= st["rays"] <= 5 * st["paths"]
+    assert 0 < st["shadow_rays"] <= 4 * st["paths"]

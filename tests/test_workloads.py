@@ -41,3 +41,16 @@ def test_rays_are_deterministic_and_normalised_like_ray_new():
         # the generator applies the same FP32 normalisation to the raw direction
         assert np.allclose(d, raw, rtol=0, atol=2e-7)
     assert np.all(a[6] == np.float32(1e-4)) and np.all(a[7] == np.float32(1e30))
+
+
+def test_batch_scenes_are_seeded_and_in_range():
+    from pbrt_b200 import workloads as W
+    a = W.batch_scenes(n=6, levels=(3, 5), spp=(4, 64))
+    b = W.batch_scenes(n=6, levels=(3, 5), spp=(4, 64))
+    assert [(d["level"], s) for d, _, s in a] == [(d["level"], s) for d, _, s in b]
+    for d, cam, s in a:
+        assert 3 <= d["level"] <= 5 and 4 <= s <= 64
+        assert cam["width"] == 512 and cam["height"] == 512
+        assert d["meshes"][-1]["indices"].shape[0] == 20 * 4 ** d["level"]
+        v = d["meshes"][-1]["vertices"]
+        assert v.min() > -0.5 and v.max() < 0.5  # inside the box
