@@ -324,6 +324,76 @@ def render_case(pb, W, ctx, case, reps=3, cpu=False, nvtx=False):
     return out
 
 
+def batch_race(pb, W, ctx, device):
+    """Batched rendering of 64 scenes (displaced icosphere of level U{3..9} in the closed box,
+    512x512, U{4..64} spp, max depth 8): the autotuner picks leaf size, wave size and launch
+    shape on a sample of the scenes, then one frame of all 64 scenes is rendered as one CUDA
+    graph replay (device time to the last scene's last wave, and each scene's completion
+    time), and the same scenes are rendered one after another with pbrt_render (device time
+    of each, and the completion times that sequence gives)."""
+    import torch
+    from pbrt_b200.autotune import autotune
+    from pbrt_b200.scene import Batch, create_scenes, render_params
+
+    t0 = time.perf_counter()
+    specs = W.batch_scenes(64, seed=3)
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tune = autotune(specs, ctx, sample=8, trial_spp=1, reps=2, leaf_sizes=(1, 2, 4))
+    tune_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    scenes = create_scenes([dict(d, bvh_max_leaf=tune["leaf"]) for d, _, _ in specs], ctx)
+    build_s = time.perf_counter() - t0
+    params = [render_params(cam, spp, 8, seed=100 + i) for i, (_, cam, spp) in enumerate(specs)]
+    samples = sum(cam["width"] * cam["height"] * spp for _, cam, spp in specs)
+    batch = Batch(scenes, params, ctx)
+    none = [None] * len(scenes)
+    batch.render(0, none)
+    frames = []
+    for f in (1, 2):
+        _, ms = batch.render(f, none, scene_times=True)
+        frames.append(ms)
+    batch.close()
+    best = min(frames, key=max)
+    frame_ms = max(best)
+    # the same scenes one after another, each its own pbrt_render
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    seq = []
+    for sc, p, (_, cam, spp) in zip(scenes, params, specs):
+        film = torch.empty((cam["height"], cam["width"], 3), dtype=torch.float64, device=device)
+        sc.render(cam, spp=spp, max_depth=8, seed=p.seed, film=film)  # warm-up (this scene's first launch)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sc.render(cam, spp=spp, max_depth=8, seed=p.seed, film=film)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        seq.append(e0.elapsed_time(e1))
+    ctx.set_stream(None)
+    ctx.set_tuning()
+    cum = list(np.cumsum(seq))
+    for sc in scenes:
+        sc.release()
+    levels = [d["level"] for d, _, _ in specs]
+    return {
+        "metric": "aggregate samples/s and per-scene latency, one batched graph frame vs sequential launches",
+        "workload": "64 scenes: displaced icosphere level U{3..9} in the closed box (area light), 512x512, "
+                    "U{4..64} spp, max depth 8 (seeded)",
+        "scenes": len(specs), "samples_per_frame": samples, "triangles": sum(20 * 4 ** l for l in levels),
+        "batched": {"frame_ms": round(frame_ms, 2), "samples_per_s": round(samples / (frame_ms * 1e-3), 1),
+                    "scene_latency_ms": {"mean": round(float(np.mean(best)), 2), "max": round(float(max(best)), 2)},
+                    "graph_launches_per_frame": 1},
+        "sequential": {"total_ms": round(float(cum[-1]), 2), "samples_per_s": round(samples / (cum[-1] * 1e-3), 1),
+                       "scene_latency_ms": {"mean": round(float(np.mean(cum)), 2), "max": round(float(cum[-1]), 2)},
+                       "note": "same scenes and tuning, one pbrt_render each (launches not captured)"},
+        "speedup_aggregate": round(cum[-1] / frame_ms, 3),
+        "tuning": {k: tune[k] for k in ("leaf", "wave_paths", "trace_threads", "trace_blocks_per_sm",
+                                          "shade_threads", "shade_blocks_per_sm")},
+        "autotune": {"trials": len(tune["trials"]), "sample_scenes": tune["sample_scenes"], "seconds": round(tune_s, 1)},
+        "setup_s": {"generate": round(gen_s, 1), "build_64_scenes": round(build_s, 1)},
+    }
+
+
 MLP_FLOP_PER_QUERY = 2 * (96 * 64 + 4 * 64 * 64 + 64 * 3)  # 45,440: forward multiply-adds x 2
 MLP_QUERIES, MLP_TRAIN_BATCH = 1 << 22, 1 << 14
 
@@ -433,7 +503,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cache-race", action="store_true")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays per step (smaller cases for profiling)")
-    ap.add_argument("--workload", default="raycast", choices=["raycast", "mlp", "render"],
+    ap.add_argument("--workload", default="raycast", choices=["raycast", "mlp", "render", "batch"],
                     help="mlp: the radiance cache's network alone; render: one path-tracing case (--case); "
                          "neither is the headline line")
     ap.add_argument("--case", default="c0", choices=sorted(RENDER_CASES))
@@ -443,6 +513,15 @@ def main():
     N_RAYS = args.rays
     if args.workload == "mlp":
         run_mlp(args, local)
+        return
+    if args.workload == "batch":
+        import torch
+
+        import pbrt_b200 as pb
+        from pbrt_b200 import workloads as W
+
+        torch.cuda.set_device(local)
+        print(json.dumps(batch_race(pb, W, pb.Context(local), torch.device("cuda", local))), flush=True)
         return
     if args.workload == "render":
         import torch
@@ -579,6 +658,7 @@ def main():
         if ws == 1 and not args.no_cache_race:
             line["renders"] = {c: render_case(pb, W, ctx, c, cpu=not args.no_cpu_baseline) for c in ("c0", "c2")}
             line["cache"] = cache_race(pb, W, ctx, rays_d.device)
+            line["batch"] = batch_race(pb, W, ctx, rays_d.device)
         if ws == 1 and not args.no_cpu_baseline:
             import oracle
 
