@@ -47,6 +47,27 @@ WORKLOAD = ("raycast: displaced icosphere level 7 (327,680 FP32 triangles, value
             "BVH binned SAH 16 bins leaf<=4, nearest-hit id + t per ray")
 
 
+def rank_ray_seed(rank: int) -> int:
+    """Each rank casts its own seeded rays against its own copy of the mesh (replicas)."""
+    return 2 + 1000 * rank
+
+
+def max_over_ranks(x: float, dist, device) -> float:
+    """The slowest rank's value (all ranks take this collective, in the same order)."""
+    if not dist:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world_size: int, units_per_rank: int, seconds: float) -> float:
+    """Units all ranks processed per second of the slowest rank's time."""
+    return world_size * units_per_rank / seconds
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -553,7 +574,7 @@ def main():
     from pbrt_b200 import workloads as W
 
     v, f = W.displaced_icosphere(LEVEL, seed=1)
-    rays_h = W.incoherent_rays(N_RAYS, v.min(0), v.max(0), seed=2 + 1000 * rank)
+    rays_h = W.incoherent_rays(N_RAYS, v.min(0), v.max(0), seed=rank_ray_seed(rank))
     ctx = pb.Context(local)
     scene = pb.Scene(ctx).add_object(pb.Simple(pb.TriangleMesh(v, f))).commit(bvh_bins=BINS, bvh_max_leaf=MAX_LEAF)
     info = scene.info()
@@ -598,11 +619,8 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    tt = torch.tensor([total_ms], device=rays_d.device)
-    if dist:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    ms_per_step = float(tt.item()) / args.steps
-    value = ws * N_RAYS / (ms_per_step * 1e-3) / 1e6
+    ms_per_step = max_over_ranks(total_ms, dist, rays_d.device) / args.steps
+    value = whole_job_rate(ws, N_RAYS, ms_per_step * 1e-3) / 1e6
 
     # End to end through the public API with pinned host buffers (copies inside the region).
     ctx.set_stream(None)
@@ -624,10 +642,7 @@ def main():
     for _ in range(e2e_steps):
         step_e2e()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    te = torch.tensor([e2e_s], device=rays_d.device)
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = ws * N_RAYS / float(te.item()) / 1e6
+    e2e_value = whole_job_rate(ws, N_RAYS, max_over_ranks(e2e_s, dist, rays_d.device)) / 1e6
     # the host path must agree with the device path
     assert torch.equal(prim_pin, prim_d.cpu()), "host-buffer results differ from device-buffer results"
 

@@ -40,6 +40,7 @@ int ensure_slots(pbrt_ctx* c) {
     PBRT_TRY(c->cuda(cudaMalloc(&s.obj, sizeof(uint32_t) * kSlotRays), "cudaMalloc(staging)"));
     PBRT_TRY(c->cuda(cudaMalloc(&s.occ, kSlotRays), "cudaMalloc(staging)"));
     PBRT_TRY(c->cuda(cudaMalloc(&s.queue, sizeof(uint32_t) * kSlotRays), "cudaMalloc(staging)"));
+    PBRT_TRY(c->cuda(cudaMalloc(&s.rec, sizeof(float4) * 2 * kSlotRays), "cudaMalloc(staging)"));
     PBRT_TRY(c->cuda(cudaMalloc(&s.fetch, 2 * sizeof(unsigned long long)), "cudaMalloc(staging)"));
   }
   c->slots_ready = true;
@@ -47,8 +48,9 @@ int ensure_slots(pbrt_ctx* c) {
 }
 
 int ensure_queue(pbrt_ctx* c) {
-  if (c->queue) return PBRT_OK;
-  return c->cuda(cudaMalloc(&c->queue, sizeof(uint32_t) * kDevChunk), "cudaMalloc(survivor queue)");
+  if (c->queue && c->queue_rec) return PBRT_OK;
+  if (!c->queue) PBRT_TRY(c->cuda(cudaMalloc(&c->queue, sizeof(uint32_t) * kDevChunk), "cudaMalloc(survivor queue)"));
+  return c->cuda(cudaMalloc(&c->queue_rec, sizeof(float4) * 2 * kDevChunk), "cudaMalloc(survivor records)");
 }
 
 
@@ -118,11 +120,13 @@ void pbrt_ctx_destroy(pbrt_ctx* c) {
     cudaFree(s.occ);
     cudaFree(s.queue);
     cudaFree(s.fetch);
+    cudaFree(s.rec);
     if (s.s) cudaStreamDestroy(s.s);
   }
   cudaFree(c->d_err);
   cudaFree(c->d_counters);
   cudaFree(c->queue);
+  cudaFree(c->queue_rec);
   cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -348,13 +352,14 @@ int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, flo
   const MeshView mv = one_mesh ? s->meshes[s->single_mesh].view : MeshView{};
   // Nearest hit / any hit of one chunk of `m` rays (planes `stride` apart) on `st`.
   auto launch = [&](const float* r, uint64_t stride, uint64_t m, uint32_t* p, float* tt, uint32_t* ob, uint8_t* oc,
-                    unsigned long long* cnt, uint32_t* queue, unsigned long long* qc, cudaStream_t st) -> cudaError_t {
+                    unsigned long long* cnt, uint32_t* queue, unsigned long long* qc, float4* rec,
+                    cudaStream_t st) -> cudaError_t {
     if (!one_mesh)
       return oc ? launch_scene_any(s->view, r, stride, m, oc, c->d_err, c->sm_count, st)
                 : launch_scene_closest(s->view, r, stride, m, p, tt, ob, c->d_err, c->sm_count, st);
     if (oc) return launch_mesh_any(mv, r, stride, m, oc, c->d_err, c->sm_count, st);
     if (c->persistent && !cnt)
-      return launch_mesh_closest_persistent(mv, r, stride, m, p, tt, ob, queue, qc, c->d_err, c->sm_count, st);
+      return launch_mesh_closest_persistent(mv, r, stride, m, p, tt, ob, queue, qc, c->d_err, c->sm_count, st, rec);
     return launch_mesh_closest(mv, r, stride, m, p, tt, ob, cnt, c->d_err, c->sm_count, st);
   };
 
@@ -379,11 +384,11 @@ int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, flo
       for (uint64_t base = 0; base < n; base += kDevChunk) {
         const uint64_t m = std::min<uint64_t>(kDevChunk, n - base);
         PBRT_TRY(c->cuda(launch(rays + base, n, m, prim + base, t + base, obj ? obj + base : nullptr, nullptr, nullptr,
-                                c->queue, c->d_counters + 4, st),
+                                c->queue, c->d_counters + 4, c->queue_rec, st),
                          "kernel launch"));
       }
     } else {
-      PBRT_TRY(c->cuda(launch(rays, n, n, prim, t, obj, occ, counters, nullptr, nullptr, st), "kernel launch"));
+      PBRT_TRY(c->cuda(launch(rays, n, n, prim, t, obj, occ, counters, nullptr, nullptr, nullptr, st), "kernel launch"));
     }
     if (stats) {
       unsigned long long h[3];
@@ -412,7 +417,7 @@ int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, flo
                                        cudaMemcpyHostToDevice, sl.s),
                        "cudaMemcpyAsync(rays)"));
     PBRT_TRY(c->cuda(launch(sl.rays, kSlotRays, m, sl.prim, sl.t, obj ? sl.obj : nullptr, occ ? sl.occ : nullptr,
-                            counters, sl.queue, sl.fetch, sl.s),
+                            counters, sl.queue, sl.fetch, sl.rec, sl.s),
                      "kernel launch"));
     if (occ) {
       PBRT_TRY(c->cuda(cudaMemcpyAsync(occ + base, sl.occ, m, cudaMemcpyDeviceToHost, sl.s), "cudaMemcpyAsync"));

@@ -54,6 +54,7 @@ struct Slot {
   uint32_t* obj = nullptr;
   uint8_t* occ = nullptr;
   uint32_t* queue = nullptr;            // survivor queue of the two-stage nearest-hit pass
+  float4* rec = nullptr;                // the survivors' ray records (32 bytes each)
   unsigned long long* fetch = nullptr;  // [queue length, fetch position] of that pass
 };
 
@@ -78,6 +79,7 @@ struct pbrt_ctx {
   unsigned long long* d_counters = nullptr;  // [0..2] traversal counters, [4..5] queue length / fetch position,
                                              // [8..10] rays / shadow rays / paths of the last render
   uint32_t* queue = nullptr;                  // survivor queue for device-buffer calls (kDevChunk entries)
+  float4* queue_rec = nullptr;                // and their ray records (kDevChunk x 32 bytes)
   bool persistent = true;                     // persistent dynamic-fetch traversal (default)
   pbrt::api::Slot slots[pbrt::api::kSlots];
   bool slots_ready = false;

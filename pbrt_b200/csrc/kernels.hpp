@@ -16,10 +16,12 @@ cudaError_t launch_mesh_closest(const MeshView& m, const float* rays, uint64_t s
 // Two-stage nearest hit: a streaming root-box cull that answers misses and compacts the
 // survivors' indices into `queue` (scratch, capacity >= n, n < 2^32), then the persistent
 // dynamic-fetch traversal over the queue. `counters` is two 64-bit words of scratch (queue
-// length, fetch position), zeroed on `s` by the launcher.
+// length, fetch position), zeroed on `s` by the launcher. `rec` (optional scratch, 2 x n
+// float4): the survivors' rays copied beside their queue entries, read back coalesced.
 cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays, uint64_t stride, uint64_t n,
                                            uint32_t* prim, float* t, uint32_t* obj, uint32_t* queue,
-                                           unsigned long long* counters, uint32_t* err, int sm_count, cudaStream_t s);
+                                           unsigned long long* counters, uint32_t* err, int sm_count, cudaStream_t s,
+                                           float4* rec = nullptr);
 // Allocation-free form of launch_mesh_closest_persistent for device buffers (plane stride
 // = n): its scratch is a file-scope __device__ array of kNoAllocMaxRays queue entries
 // shared by every call on a device. Looks the array's address up on `device` (which must be

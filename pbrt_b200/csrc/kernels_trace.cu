@@ -6,7 +6,9 @@
 // The nearest-hit pass on a batch runs in two stages:
 //   1. k_cull_root streams every ray once (four rays per thread, 16-byte loads), tests the
 //      root box, writes a miss for every ray, and appends the rays that enter the root to a
-//      queue with one atomicAdd per block;
+//      queue with one atomicAdd per block, each with a 32-byte copy of the ray beside its
+//      index (when a record buffer is given), so that stage 2 reads its rays coalesced
+//      instead of gathering eight planes per ray;
 //   2. k_mesh_closest_persistent runs persistent warps over the queue, refilling idle lanes
 //      with ballot/popc and one atomicAdd per warp, and walks interior nodes until each lane
 //      reaches a leaf before any lane tests triangles (so a leaf of one lane does not
@@ -81,7 +83,8 @@ __global__ void __launch_bounds__(kCullThreads) k_cull_root(MeshView m, const fl
                                                             uint64_t n, uint32_t* __restrict__ prim,
                                                             float* __restrict__ tout, uint32_t* __restrict__ obj,
                                                             uint32_t* __restrict__ queue,
-                                                            unsigned long long* __restrict__ queue_count) {
+                                                            unsigned long long* __restrict__ queue_count,
+                                                            float4* __restrict__ rec) {
   __shared__ uint32_t warp_off[2][kCullThreads / 32];
   __shared__ unsigned long long blk_base[2];
   const float4 rlo = __ldg(&m.nodes[0]);
@@ -154,7 +157,13 @@ __global__ void __launch_bounds__(kCullThreads) k_cull_root(MeshView m, const fl
     uint64_t pos = blk_base[buf] + warp_off[buf][warp] + (incl - c);
 #pragma unroll
     for (int j = 0; j < kCullRays; ++j)
-      if (enter & (1u << j)) queue[pos++] = uint32_t(i0 + j);
+      if (enter & (1u << j)) {
+        if (rec) {  // read back soon by stage 2: default caching, the planes stream past
+          rec[2 * pos] = make_float4(v[0][j], v[1][j], v[2][j], v[6][j]);
+          rec[2 * pos + 1] = make_float4(v[3][j], v[4][j], v[5][j], v[7][j]);
+        }
+        queue[pos++] = uint32_t(i0 + j);
+      }
   }
 }
 
@@ -181,13 +190,15 @@ PBRT_DEV bool pop_next(TraversalStack& s, int& sp, float min_t, uint32_t& lf, ui
   return false;
 }
 
+template <bool kRec>
 __global__ void __launch_bounds__(128) k_mesh_closest_persistent(MeshView m, const float* __restrict__ rays,
                                                                  uint64_t stride, const uint32_t* __restrict__ queue,
                                                                  const unsigned long long* __restrict__ queue_count,
                                                                  uint32_t* __restrict__ prim,
                                                                  float* __restrict__ tout, uint32_t* __restrict__ obj,
                                                                  unsigned long long* __restrict__ next_ray,
-                                                                 uint32_t* __restrict__ err) {
+                                                                 uint32_t* __restrict__ err,
+                                                                 const float4* __restrict__ rec) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
   const uint64_t n = *queue_count;
@@ -215,11 +226,19 @@ __global__ void __launch_bounds__(128) k_mesh_closest_persistent(MeshView m, con
         const uint64_t k = base + __popc(idle & lt_mask);
         if (k < n) {
           idx = __ldg(queue + k);
-          const F3 o = mk3(__ldg(rays + idx), __ldg(rays + stride + idx), __ldg(rays + 2 * stride + idx));
-          const F3 d = mk3(__ldg(rays + 3 * stride + idx), __ldg(rays + 4 * stride + idx),
-                           __ldg(rays + 5 * stride + idx));
-          near = __ldg(rays + 6 * stride + idx);
-          far = __ldg(rays + 7 * stride + idx);
+          F3 o, d;
+          if (kRec) {  // the copy stage 1 wrote: consecutive lanes read consecutive records
+            const float4 a = __ldcs(rec + 2 * k), b = __ldcs(rec + 2 * k + 1);
+            o = mk3(a.x, a.y, a.z);
+            d = mk3(b.x, b.y, b.z);
+            near = a.w;
+            far = b.w;
+          } else {
+            o = mk3(__ldg(rays + idx), __ldg(rays + stride + idx), __ldg(rays + 2 * stride + idx));
+            d = mk3(__ldg(rays + 3 * stride + idx), __ldg(rays + 4 * stride + idx), __ldg(rays + 5 * stride + idx));
+            near = __ldg(rays + 6 * stride + idx);
+            far = __ldg(rays + 7 * stride + idx);
+          }
           r = prepare_ray(o, d);
           min_t = FLT_MAX;
           best = 0xFFFFFFFFu;
@@ -331,11 +350,13 @@ static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 
 
 cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays, uint64_t stride, uint64_t n,
                                            uint32_t* prim, float* t, uint32_t* obj, uint32_t* queue,
-                                           unsigned long long* counters, uint32_t* err, int sm_count, cudaStream_t s) {
+                                           unsigned long long* counters, uint32_t* err, int sm_count, cudaStream_t s,
+                                           float4* rec) {
   if (n == 0) return cudaSuccess;
   static int blocks_per_sm = 0;
   if (blocks_per_sm == 0) {
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_mesh_closest_persistent, 128, 0);
+    cudaError_t e =
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_mesh_closest_persistent<true>, 128, 0);
     if (e != cudaSuccess || blocks_per_sm <= 0) blocks_per_sm = 8;
   }
   cudaError_t e = cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), s);
@@ -345,15 +366,20 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
   const uint64_t cull_need = (n + per_block - 1) / per_block, cull_cap = uint64_t(sm_count) * 8;
   const unsigned cg = unsigned(cull_need < cull_cap ? cull_need : cull_cap);
   if (vec)
-    k_cull_root<true><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters);
+    k_cull_root<true><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec);
   else
-    k_cull_root<false><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters);
+    k_cull_root<false><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const uint64_t full = uint64_t(sm_count) * blocks_per_sm;
   const uint64_t need = (n + 127) / 128;
   const unsigned g = unsigned(need < full ? need : full);
-  k_mesh_closest_persistent<<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj, counters + 1, err);
+  if (rec)
+    k_mesh_closest_persistent<true><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj, counters + 1, err,
+                                                      rec);
+  else
+    k_mesh_closest_persistent<false><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj, counters + 1,
+                                                       err, nullptr);
   return cudaGetLastError();
 }
 
@@ -406,7 +432,7 @@ cudaError_t launch_mesh_closest_noalloc(const MeshView& m, const float* rays, ui
   uint32_t* queue = scratch + 64;
   static int blocks_per_sm = 0;
   if (blocks_per_sm == 0) {
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_mesh_closest_persistent, 128, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_mesh_closest_persistent<false>, 128, 0);
     if (e != cudaSuccess || blocks_per_sm <= 0) blocks_per_sm = 8;
   }
   const bool vec = n % 4 == 0 && aligned16(rays) && aligned16(prim) && aligned16(t);
@@ -414,15 +440,16 @@ cudaError_t launch_mesh_closest_noalloc(const MeshView& m, const float* rays, ui
   const uint64_t cull_need = (n + per_block - 1) / per_block, cull_cap = uint64_t(sm_count) * 8;
   const unsigned cg = unsigned(cull_need < cull_cap ? cull_need : cull_cap);
   if (vec)
-    k_cull_root<true><<<cg, kCullThreads, 0, s>>>(m, rays, n, n, prim, t, nullptr, queue, counters);
+    k_cull_root<true><<<cg, kCullThreads, 0, s>>>(m, rays, n, n, prim, t, nullptr, queue, counters, nullptr);
   else
-    k_cull_root<false><<<cg, kCullThreads, 0, s>>>(m, rays, n, n, prim, t, nullptr, queue, counters);
+    k_cull_root<false><<<cg, kCullThreads, 0, s>>>(m, rays, n, n, prim, t, nullptr, queue, counters, nullptr);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const uint64_t full = uint64_t(sm_count) * blocks_per_sm;
   const uint64_t need = (n + 127) / 128;
   const unsigned g = unsigned(need < full ? need : full);
-  k_mesh_closest_persistent<<<g, 128, 0, s>>>(m, rays, n, queue, counters, prim, t, nullptr, counters + 1, err);
+  k_mesh_closest_persistent<false><<<g, 128, 0, s>>>(m, rays, n, queue, counters, prim, t, nullptr, counters + 1, err,
+                                                     nullptr);
   return cudaGetLastError();
 }
 
