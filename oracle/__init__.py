@@ -201,12 +201,20 @@ def make_ray(origin, direction, dtype=np.float64):
 # A scene is described by a plain dict, the same one the tests lower into the product:
 #   meshes:    [{"vertices": (n,3) float32, "indices": (m,3) uint32}]
 #   materials: [{"kind": 0 lambertian | 1 metal | 2 dielectric | 3 diffuse light,
-#                "color": (3,), "fuzz": f, "ior": f}]
-#   objects:   [{"shape": 0 mesh | 1 sphere | 2 cylinder, "mesh": i, "radius": r, "height": h,
-#                "material": i, "to_world": (12,) or None, "to_local": (12,) or None}]
+#                "color": (3,), "fuzz": f, "ior": f,
+#                optional "texture": 1 checkerboard with "color2": (3,), "scale": f}]
+#   objects:   [{"shape": 0 mesh | 1 sphere | 2 cylinder | 3 rectangle | 4 aabox | 5 plane,
+#                "mesh": i, "radius": r, "height": h, "extent": (3,), "material": i,
+#                "to_world": (12,) or None, "to_local": (12,) or None}]
+#              (rectangle: radius = width, height = height; aabox: extent = full size)
 #   lights:    [{"kind": 0 point | 1 uniform infinite | 2 background | 3 area, "position": (3,),
 #                "radiance": (3,), "bottom": (3,), "top": (3,), "object": i}]
+#   optional object tree: "nodes": [{"kind": 0 simple | 1 transformed | 2 compound,
+#                "object": i (simple), "children": [node, ...], "to_world", "to_local"
+#                (transformed)}], "roots": [node, ...] (the scene's primitives, in order)
 #   bvh_bins, bvh_max_leaf
+# Transforms are float64 here (the f64 oracle keeps them; the f32 oracle and the product
+# round them to float32).
 # camera: {"width", "height", "fov" (radians), "near", "far", "position", "look_at", "up"}
 # ------------------------------------------------------------------------------------------
 class _OMesh(C.Structure):
@@ -215,13 +223,19 @@ class _OMesh(C.Structure):
 
 
 class _OMaterial(C.Structure):
-    _fields_ = [("kind", C.c_uint32), ("color", C.c_float * 3), ("fuzz", C.c_float), ("ior", C.c_float)]
+    _fields_ = [("kind", C.c_uint32), ("color", C.c_float * 3), ("fuzz", C.c_float), ("ior", C.c_float),
+                ("texture", C.c_uint32), ("color2", C.c_float * 3), ("scale", C.c_float)]
 
 
 class _OObject(C.Structure):
-    _fields_ = [("shape", C.c_uint32), ("mesh", C.c_uint32), ("radius", C.c_float), ("height", C.c_float),
-                ("material", C.c_uint32), ("transformed", C.c_uint32), ("to_world", C.c_float * 12),
-                ("to_local", C.c_float * 12)]
+    _fields_ = [("shape", C.c_uint32), ("mesh", C.c_uint32), ("radius", C.c_double), ("height", C.c_double),
+                ("extent", C.c_double * 3), ("material", C.c_uint32), ("transformed", C.c_uint32),
+                ("to_world", C.c_double * 12), ("to_local", C.c_double * 12)]
+
+
+class _ONode(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("object", C.c_uint32), ("first", C.c_uint32), ("count", C.c_uint32),
+                ("to_world", C.c_double * 12), ("to_local", C.c_double * 12)]
 
 
 class _OLight(C.Structure):
@@ -233,12 +247,15 @@ class _OScene(C.Structure):
     _fields_ = [("meshes", C.c_void_p), ("mesh_count", C.c_uint32), ("materials", C.c_void_p),
                 ("material_count", C.c_uint32), ("objects", C.c_void_p), ("object_count", C.c_uint32),
                 ("lights", C.c_void_p), ("light_count", C.c_uint32), ("bvh_bins", C.c_uint32),
-                ("bvh_max_leaf", C.c_uint32)]
+                ("bvh_max_leaf", C.c_uint32), ("nodes", C.c_void_p), ("node_count", C.c_uint32),
+                ("children", C.c_void_p), ("child_count", C.c_uint32), ("roots", C.c_void_p),
+                ("root_count", C.c_uint32)]
 
 
 class _OCamera(C.Structure):
-    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("fov", C.c_float), ("near", C.c_float),
-                ("far", C.c_float), ("position", C.c_float * 3), ("look_at", C.c_float * 3), ("up", C.c_float * 3)]
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("fov", C.c_double), ("near", C.c_double),
+                ("far", C.c_double), ("position", C.c_double * 3), ("look_at", C.c_double * 3),
+                ("up", C.c_double * 3)]
 
 
 class _ORender(C.Structure):
@@ -271,6 +288,16 @@ def _declare_scene(L):
         getattr(L, f"oracle_scene_bvh_{suf}").argtypes = [vp, vp, vp, vp, vp]
         getattr(L, f"oracle_scene_bvh_nodes_{suf}").restype = sz
         getattr(L, f"oracle_scene_bvh_nodes_{suf}").argtypes = [vp]
+        getattr(L, f"oracle_scene_trace_stats_{suf}").argtypes = [vp, vp, sz, vp, vp, vp, C.c_int, vp]
+        getattr(L, f"oracle_scene_occluded_stats_{suf}").argtypes = [vp, vp, sz, vp, C.c_int, vp]
+        getattr(L, f"oracle_scene_cast_sets_{suf}").argtypes = [vp, C.POINTER(_OCamera), vp, C.c_double,
+                                                                C.c_double, C.c_double, vp, vp]
+        getattr(L, f"oracle_scene_counts_{suf}").argtypes = [vp, vp]
+
+
+def _xf12(m):
+    """A transform given as 12 row-major values or a 3x4 / 4x4 matrix, as 12 float64."""
+    return [float(x) for x in np.asarray(m, np.float64).reshape(-1)[:12]]
 
 
 class Scene:
@@ -302,18 +329,35 @@ class Scene:
             d.kind = int(m["kind"])
             d.color[:] = [float(c) for c in m.get("color", (0, 0, 0))]
             d.fuzz, d.ior = float(m.get("fuzz", 0.0)), float(m.get("ior", 1.0))
+            d.texture = int(m.get("texture", 0))
+            d.color2[:] = [float(c) for c in m.get("color2", (0, 0, 0))]
+            d.scale = float(m.get("scale", 1.0))
             mats.append(d)
         objs = []
         for o in desc.get("objects", []):
             d = _OObject()
             d.shape, d.mesh = int(o["shape"]), int(o.get("mesh", 0))
             d.radius, d.height = float(o.get("radius", 0.0)), float(o.get("height", 0.0))
+            d.extent[:] = [float(x) for x in o.get("extent", (0.0, 0.0, 0.0))]
             d.material = int(o["material"])
             if o.get("to_world") is not None:
                 d.transformed = 1
-                d.to_world[:] = [float(x) for x in np.asarray(o["to_world"]).reshape(-1)[:12]]
-                d.to_local[:] = [float(x) for x in np.asarray(o["to_local"]).reshape(-1)[:12]]
+                d.to_world[:] = _xf12(o["to_world"])
+                d.to_local[:] = _xf12(o["to_local"])
             objs.append(d)
+        nodes, kids = [], []
+        for n in desc.get("nodes", []) or []:
+            d = _ONode()
+            d.kind = int(n["kind"])
+            d.object = int(n.get("object", 0))
+            ch = [int(c) for c in n.get("children", [])]
+            d.first, d.count = len(kids), len(ch)
+            kids += ch
+            if n.get("to_world") is not None:
+                d.to_world[:] = _xf12(n["to_world"])
+                d.to_local[:] = _xf12(n["to_local"])
+            nodes.append(d)
+        roots = [int(r) for r in desc.get("roots", [])] if nodes else []
         lts = []
         for l in desc.get("lights", []):
             d = _OLight()
@@ -323,10 +367,14 @@ class Scene:
             d.object = int(l.get("object", 0))
             lts.append(d)
         arrs = [(_OMesh * max(1, len(ms)))(*ms), (_OMaterial * max(1, len(mats)))(*mats),
-                (_OObject * max(1, len(objs)))(*objs), (_OLight * max(1, len(lts)))(*lts)]
+                (_OObject * max(1, len(objs)))(*objs), (_OLight * max(1, len(lts)))(*lts),
+                (_ONode * max(1, len(nodes)))(*nodes), (C.c_uint32 * max(1, len(kids)))(*kids),
+                (C.c_uint32 * max(1, len(roots)))(*roots)]
         self._keep += arrs
         sd = _OScene(C.addressof(arrs[0]), len(ms), C.addressof(arrs[1]), len(mats), C.addressof(arrs[2]), len(objs),
-                     C.addressof(arrs[3]), len(lts), int(desc.get("bvh_bins", 8)), int(desc.get("bvh_max_leaf", 1)))
+                     C.addressof(arrs[3]), len(lts), int(desc.get("bvh_bins", 8)), int(desc.get("bvh_max_leaf", 1)),
+                     C.addressof(arrs[4]) if nodes else None, len(nodes), C.addressof(arrs[5]), len(kids),
+                     C.addressof(arrs[6]), len(roots))
         self._h = getattr(L, f"oracle_scene_new_{self.suf}")(C.byref(sd))
         if not self._h:
             raise ValueError(L.oracle_last_error().decode())
@@ -352,6 +400,51 @@ class Scene:
         occ = np.empty(rays.shape[1], np.uint8)
         getattr(lib(), f"oracle_scene_occluded_{self.suf}")(self._h, _ptr(rays), rays.shape[1], _ptr(occ), threads)
         return occ
+
+    def trace_instrumented(self, rays, threads: int = os.cpu_count() or 1):
+        """trace plus the scene query's counters summed over the rays: {nodes, boxes, objects}
+        as Scene::intersect_instrumented counts them (src/scene.rs:124-128)."""
+        rays = np.ascontiguousarray(rays, dtype=self.dtype)
+        n = rays.shape[1]
+        prim, obj, t = np.empty(n, np.uint32), np.empty(n, np.uint32), np.empty(n, self.dtype)
+        st = np.zeros(3, np.uint64)
+        getattr(lib(), f"oracle_scene_trace_stats_{self.suf}")(self._h, _ptr(rays), n, _ptr(prim), _ptr(obj),
+                                                               _ptr(t), threads, _ptr(st))
+        return prim, obj, t, dict(zip(("nodes", "boxes", "objects"), (int(x) for x in st)))
+
+    def occluded_instrumented(self, rays, threads: int = os.cpu_count() or 1):
+        """occluded plus Scene::intersect_p_instrumented's counters (src/scene.rs:148-153)."""
+        rays = np.ascontiguousarray(rays, dtype=self.dtype)
+        occ = np.empty(rays.shape[1], np.uint8)
+        st = np.zeros(3, np.uint64)
+        getattr(lib(), f"oracle_scene_occluded_stats_{self.suf}")(self._h, _ptr(rays), rays.shape[1], _ptr(occ),
+                                                                  threads, _ptr(st))
+        return occ, dict(zip(("nodes", "boxes", "objects"), (int(x) for x in st)))
+
+    def counts(self) -> dict:
+        """{bounded primitives (the BVH's), unbounded primitives, BVH nodes}."""
+        out = np.zeros(3, np.uint64)
+        getattr(lib(), f"oracle_scene_counts_{self.suf}")(self._h, _ptr(out))
+        return dict(zip(("primitives", "unbounded", "nodes"), (int(x) for x in out)))
+
+    def cast_sets(self, camera: dict, target=(0.0, 2.0, 1.0), near: float = 1e-4, far: float = 1000.0,
+                  shadow_near: float = 1e-5, shadow_rays: bool = False):
+        """The scene mode of the reference's traversal benchmark (src/bin/bvh_stats.rs:254-286):
+        pixel-centre primary rays, and from each hit a shadow ray towards `target`. Returns
+        {"primary": {rays, hits, nodes, boxes, objects}, "shadow": {...}} and, with
+        shadow_rays=True, the shadow rays (8 x pixels SoA, NaN rows for primary misses)."""
+        L = lib()
+        c = _camera(camera)
+        out = np.zeros(10, np.uint64)
+        tgt = np.asarray(target, np.float64)
+        n = int(camera["width"]) * int(camera["height"])
+        sr = np.zeros((8, n), self.dtype) if shadow_rays else None
+        getattr(L, f"oracle_scene_cast_sets_{self.suf}")(self._h, C.byref(c), _ptr(tgt), near, far, shadow_near,
+                                                         _ptr(out), _ptr(sr) if sr is not None else None)
+        keys = ("rays", "hits", "nodes", "boxes", "objects")
+        res = {"primary": {k: int(v) for k, v in zip(keys, out[:5])},
+               "shadow": {k: int(v) for k, v in zip(keys, out[5:])}}
+        return (res, sr) if shadow_rays else res
 
     def bvh(self):
         n = getattr(lib(), f"oracle_scene_bvh_nodes_{self.suf}")(self._h)

@@ -289,15 +289,32 @@ ORACLE_MESH_API(f32, float)
 
 namespace {
 
+// Sums per-chunk SceneStats into stats[3] = {nodes visited, box tests, object tests}.
+struct StatSum {
+  std::atomic<uint64_t> v[3] = {{0}, {0}, {0}};
+  void add(const SceneStats& st) {
+    v[0] += st.nodes_visited;
+    v[1] += st.box_tests;
+    v[2] += st.object_tests;
+  }
+  void out(uint64_t* stats) const {
+    if (stats)
+      for (int k = 0; k < 3; ++k) stats[k] = v[k].load();
+  }
+};
+
 template <class R>
-int scene_trace(const OScene<R>* s, const R* rays, size_t n, uint32_t* prim, uint32_t* obj, R* t, int threads) {
+int scene_trace(const OScene<R>* s, const R* rays, size_t n, uint32_t* prim, uint32_t* obj, R* t, int threads,
+                uint64_t* stats = nullptr) {
+  StatSum sum;
   parallel_for(n, threads, [&](size_t b, size_t e) {
+    SceneStats st;
     for (size_t i = b; i < e; ++i) {
       R tmin, tmax;
       Ray<R> r = load_ray(rays, n, i, &tmin, &tmax);
       Isect<R> it;
       uint32_t o = 0xFFFFFFFFu, p = 0xFFFFFFFFu;
-      if (s->intersect(r, tmin, tmax, &it, &o, &p)) {
+      if (s->intersect(r, tmin, tmax, &it, &o, &p, stats ? &st : nullptr)) {
         prim[i] = p;
         obj[i] = o;
         t[i] = it.d;
@@ -307,20 +324,66 @@ int scene_trace(const OScene<R>* s, const R* rays, size_t n, uint32_t* prim, uin
         t[i] = std::numeric_limits<R>::infinity();
       }
     }
+    sum.add(st);
   });
+  sum.out(stats);
   return 0;
 }
 
 template <class R>
-int scene_occluded(const OScene<R>* s, const R* rays, size_t n, uint8_t* occ, int threads) {
+int scene_occluded(const OScene<R>* s, const R* rays, size_t n, uint8_t* occ, int threads, uint64_t* stats = nullptr) {
+  StatSum sum;
   parallel_for(n, threads, [&](size_t b, size_t e) {
+    SceneStats st;
     for (size_t i = b; i < e; ++i) {
       R tmin, tmax;
       Ray<R> r = load_ray(rays, n, i, &tmin, &tmax);
-      occ[i] = s->occluded(r, tmin, tmax) ? 1 : 0;
+      occ[i] = s->occluded(r, tmin, tmax, stats ? &st : nullptr) ? 1 : 0;
     }
+    sum.add(st);
   });
+  sum.out(stats);
   return 0;
+}
+
+// The scene mode of the traversal benchmark (src/bin/bvh_stats.rs:254-286): one primary ray
+// per pixel centre through Scene::intersect_instrumented on [near, far]; from each hit, one
+// shadow ray spawned towards `target` (Ray::spawn_from_through) through
+// Scene::intersect_p_instrumented on [shadow_near, |target - p|].
+// out[0..4] = primary rays, hits, nodes, boxes, objects; out[5..9] the same for shadow rays.
+// With shadow_rays != NULL the shadow rays are written out (8 SoA planes of `primary rays`
+// entries; rows of missed pixels hold NaN) so that another implementation can cast them.
+template <class R>
+void scene_cast_sets(const OScene<R>* s, const OCameraDesc* c, const double* target, double near, double far,
+                     double shadow_near, uint64_t* out, R* shadow_rays) {
+  const PinHoleCamera<R> cam = make_camera<R>(*c);
+  const V3<R> tgt{R(target[0]), R(target[1]), R(target[2])};
+  SceneStats ps, ss;
+  uint64_t np = 0, hp = 0, ns = 0, hs = 0;
+  const size_t n = size_t(c->width) * c->height;
+  for (uint32_t y = 0; y < c->height; ++y)
+    for (uint32_t x = 0; x < c->width; ++x) {
+      const size_t i = size_t(y) * c->width + x;
+      const Ray<R> ray = cam.get_ray(R(x) + R(0.5), R(y) + R(0.5));
+      ++np;
+      Isect<R> it;
+      uint32_t o, p;
+      if (shadow_rays)
+        for (int k = 0; k < 8; ++k) shadow_rays[k * n + i] = std::numeric_limits<R>::quiet_NaN();
+      if (!s->intersect(ray, R(near), R(far), &it, &o, &p, &ps)) continue;
+      ++hp;
+      const Ray<R> sr = spawn_from_through(it.p, tgt);
+      const R dist = length(tgt - it.p);
+      ++ns;
+      if (shadow_rays) {
+        const R v[8] = {sr.o.x, sr.o.y, sr.o.z, sr.d.x, sr.d.y, sr.d.z, R(shadow_near), dist};
+        for (int k = 0; k < 8; ++k) shadow_rays[k * n + i] = v[k];
+      }
+      if (s->occluded(sr, R(shadow_near), dist, &ss)) ++hs;
+    }
+  const uint64_t v[10] = {np, hp, ps.nodes_visited, ps.box_tests, ps.object_tests,
+                          ns, hs, ss.nodes_visited, ss.box_tests, ss.object_tests};
+  for (int k = 0; k < 10; ++k) out[k] = v[k];
 }
 
 // renderers::mt::compute_pixel (mt.rs:112-130): spp jittered samples through the pinhole
@@ -406,6 +469,24 @@ extern "C" {
   int oracle_scene_occluded_##SUF(void* s, const R* rays, size_t n, uint8_t* occ, int th) {                 \
     return scene_occluded((OScene<R>*)s, rays, n, occ, th);                                                 \
   }                                                                                                         \
+  int oracle_scene_trace_stats_##SUF(void* s, const R* rays, size_t n, uint32_t* prim, uint32_t* obj, R* t,  \
+                                     int th, uint64_t* stats) {                                             \
+    return scene_trace((OScene<R>*)s, rays, n, prim, obj, t, th, stats);                                    \
+  }                                                                                                         \
+  int oracle_scene_occluded_stats_##SUF(void* s, const R* rays, size_t n, uint8_t* occ, int th,             \
+                                        uint64_t* stats) {                                                  \
+    return scene_occluded((OScene<R>*)s, rays, n, occ, th, stats);                                          \
+  }                                                                                                         \
+  void oracle_scene_cast_sets_##SUF(void* s, const OCameraDesc* c, const double* target, double near,       \
+                                    double far, double shadow_near, uint64_t* out, R* shadow_rays) {        \
+    scene_cast_sets((OScene<R>*)s, c, target, near, far, shadow_near, out, shadow_rays);                    \
+  }                                                                                                         \
+  void oracle_scene_counts_##SUF(void* s, uint64_t* out) {                                                  \
+    const OScene<R>* sc = (OScene<R>*)s;                                                                    \
+    out[0] = sc->prim_root.size();                                                                          \
+    out[1] = sc->unbounded.size();                                                                          \
+    out[2] = sc->bnodes.size();                                                                             \
+  }                                                                                                         \
   int oracle_render_##SUF(void* s, const ORenderParams* p, double* film, int th) {                          \
     try {                                                                                                   \
       return render((OScene<R>*)s, p, film, th);                                                            \
@@ -434,7 +515,7 @@ extern "C" {
       boxes[6 * i + 3] = b.bmax.x; boxes[6 * i + 4] = b.bmax.y; boxes[6 * i + 5] = b.bmax.z;                \
       left_first[i] = sc->bnodes[i].left_first; count[i] = sc->bnodes[i].count;                             \
     }                                                                                                       \
-    for (size_t i = 0; i < sc->order.size(); ++i) order[i] = sc->order[i];                                  \
+    for (size_t i = 0; i < sc->order.size(); ++i) order[i] = sc->prim_root[sc->order[i]];                  \
   }                                                                                                         \
   size_t oracle_scene_bvh_nodes_##SUF(void* s) { return ((OScene<R>*)s)->bnodes.size(); }
 

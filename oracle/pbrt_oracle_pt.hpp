@@ -116,9 +116,12 @@ struct Affine {
 // Scene description (the oracle's own POD; tests lower one scene into it and into the
 // product's C description)
 // ---------------------------------------------------------------------------------------
-enum { O_SHAPE_MESH = 0, O_SHAPE_SPHERE = 1, O_SHAPE_CYLINDER = 2 };
+enum { O_SHAPE_MESH = 0, O_SHAPE_SPHERE = 1, O_SHAPE_CYLINDER = 2, O_SHAPE_RECTANGLE = 3, O_SHAPE_AABOX = 4,
+       O_SHAPE_PLANE = 5 };
 enum { O_MAT_LAMBERTIAN = 0, O_MAT_METAL = 1, O_MAT_DIELECTRIC = 2, O_MAT_DIFFUSE_LIGHT = 3 };
 enum { O_LIGHT_POINT = 0, O_LIGHT_UNIFORM = 1, O_LIGHT_BACKGROUND = 2, O_LIGHT_AREA = 3 };
+enum { O_TEX_PLAIN = 0, O_TEX_CHECKERBOARD = 1 };
+enum { O_NODE_SIMPLE = 0, O_NODE_TRANSFORMED = 1, O_NODE_COMPOUND = 2 };
 
 struct OMeshDesc {
   const float* vertices;
@@ -131,12 +134,25 @@ struct OMaterialDesc {
   uint32_t kind;
   float color[3];
   float fuzz, ior;
+  uint32_t texture;  // O_TEX_*: PlainColor(color) or CheckerBoard(color, color2, scale)
+  float color2[3];
+  float scale;
 };
+// A Simple(shape, material) object, optionally wrapped in one Transformed. Sizes are the
+// reference's constructor arguments: sphere radius; cylinder radius, height; rectangle
+// width, height; aabox extent (full sizes; the shapes halve them).
 struct OObjectDesc {
   uint32_t shape, mesh;
-  float radius, height;
+  double radius, height;
+  double extent[3];
   uint32_t material, transformed;
-  float to_world[12], to_local[12];
+  double to_world[12], to_local[12];
+};
+// Object tree of a scene file (src/objects/*.rs): SIMPLE names an object; TRANSFORMED wraps
+// children[first]; COMPOUND holds children[first .. first + count).
+struct ONodeDesc {
+  uint32_t kind, object, first, count;
+  double to_world[12], to_local[12];
 };
 struct OLightDesc {
   uint32_t kind;
@@ -153,11 +169,18 @@ struct OSceneDesc {
   const OLightDesc* lights;
   uint32_t light_count;
   uint32_t bvh_bins, bvh_max_leaf;
+  // Optional tree (nodes == NULL: every object is one primitive of the scene, in order).
+  const ONodeDesc* nodes;
+  uint32_t node_count;
+  const uint32_t* children;
+  uint32_t child_count;
+  const uint32_t* roots;  // the scene's primitives in Scene::add_object order
+  uint32_t root_count;
 };
 struct OCameraDesc {
   uint32_t width, height;
-  float fov, near, far;
-  float position[3], look_at[3], up[3];
+  double fov, near, far;
+  double position[3], look_at[3], up[3];
 };
 struct ORenderParams {
   OCameraDesc camera;
@@ -179,6 +202,12 @@ struct CacheHook {
 // ---------------------------------------------------------------------------------------
 // Scene
 // ---------------------------------------------------------------------------------------
+// Work counters of a scene query (TraversalStats as Scene::intersect_instrumented and
+// Scene::intersect_p_instrumented fill them: src/scene.rs:124-153, src/bvh.rs:153-275).
+struct SceneStats {
+  uint64_t nodes_visited = 0, box_tests = 0, object_tests = 0;
+};
+
 template <class R>
 class OScene {
  public:
@@ -190,7 +219,9 @@ class OScene {
   };
   struct Object {
     uint32_t shape, mesh, material;
-    R radius, height, half_height;
+    R radius, height, half_height;  // sphere, cylinder
+    R half_w, half_h;               // rectangle (Rectangle::new halves width and height)
+    V3<R> amin, amax;               // aabox (AABox::new: min = 0 - extent/2, max = extent/2)
     bool transformed;
     Affine<R> mat, inv;
   };
@@ -198,6 +229,9 @@ class OScene {
     uint32_t kind;
     V3<R> color;
     R fuzz, ior;
+    uint32_t texture;
+    V3<R> color2;
+    R scale;
   };
   struct Light {
     uint32_t kind;
@@ -208,10 +242,22 @@ class OScene {
     std::vector<R> cdf;     // running sum of areas
     R area = R(0);
   };
+  struct Node {
+    uint32_t kind, object;
+    std::vector<uint32_t> kids;
+    Affine<R> mat, inv;
+  };
   struct BNode {
     AABB<R> box;
     uint32_t left_first, count;
   };
+
+  static Affine<R> affine(const double* m) {
+    Affine<R> a;
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 4; ++c) a.m[r][c] = R(m[4 * r + c]);
+    return a;
+  }
 
   explicit OScene(const OSceneDesc& d) {
     for (uint32_t i = 0; i < d.mesh_count; ++i) {
@@ -226,27 +272,73 @@ class OScene {
     }
     for (uint32_t i = 0; i < d.material_count; ++i) {
       const OMaterialDesc& m = d.materials[i];
-      materials.push_back(Material{m.kind, V3<R>{R(m.color[0]), R(m.color[1]), R(m.color[2])}, R(m.fuzz), R(m.ior)});
+      Material mm{m.kind, V3<R>{R(m.color[0]), R(m.color[1]), R(m.color[2])}, R(m.fuzz), R(m.ior), m.texture,
+                  V3<R>{R(m.color2[0]), R(m.color2[1]), R(m.color2[2])}, R(m.scale)};
+      if (m.texture > O_TEX_CHECKERBOARD) throw std::invalid_argument("unknown texture");
+      materials.push_back(mm);
       if (m.kind == O_MAT_DIFFUSE_LIGHT)
-        for (int c = 0; c < 3; ++c) max_radiance = std::max(max_radiance, m.color[c]);
+        for (int c = 0; c < 3; ++c) {
+          max_radiance = std::max(max_radiance, m.color[c]);
+          if (m.texture == O_TEX_CHECKERBOARD) max_radiance = std::max(max_radiance, m.color2[c]);
+        }
     }
     for (uint32_t i = 0; i < d.object_count; ++i) {
       const OObjectDesc& o = d.objects[i];
-      Object ob;
+      Object ob{};
       ob.shape = o.shape;
       ob.mesh = o.mesh;
       ob.material = o.material;
       ob.radius = R(o.radius);
       ob.height = R(o.height);
       ob.half_height = R(o.height) / R(2);  // Cylinder::new (cylinder.rs:12-19)
+      ob.half_w = R(o.radius) / R(2);       // Rectangle::new(width, height) (rectangle.rs:15-20)
+      ob.half_h = R(o.height) / R(2);
+      const V3<R> half = V3<R>{R(o.extent[0]), R(o.extent[1]), R(o.extent[2])} * R(0.5);  // AABox::new
+      ob.amin = V3<R>{R(0), R(0), R(0)} - half;
+      ob.amax = half;
       ob.transformed = o.transformed != 0;
-      for (int r = 0; r < 3; ++r)
-        for (int c = 0; c < 4; ++c) {
-          ob.mat.m[r][c] = R(o.to_world[4 * r + c]);
-          ob.inv.m[r][c] = R(o.to_local[4 * r + c]);
-        }
+      ob.mat = affine(o.to_world);
+      ob.inv = affine(o.to_local);
+      if (ob.shape > O_SHAPE_PLANE) throw std::invalid_argument("unknown shape");
       if (ob.shape == O_SHAPE_MESH && ob.mesh >= meshes.size()) throw std::invalid_argument("bad mesh index");
+      if (ob.material >= materials.size()) throw std::invalid_argument("bad material index");
       objects.push_back(ob);
+    }
+    if (d.nodes) {
+      for (uint32_t i = 0; i < d.node_count; ++i) {
+        const ONodeDesc& nd = d.nodes[i];
+        Node n{};
+        n.kind = nd.kind;
+        n.object = nd.object;
+        if (nd.kind == O_NODE_SIMPLE) {
+          if (nd.object >= objects.size()) throw std::invalid_argument("node names no object");
+        } else if (nd.kind == O_NODE_TRANSFORMED || nd.kind == O_NODE_COMPOUND) {
+          const uint32_t cnt = nd.kind == O_NODE_TRANSFORMED ? 1u : nd.count;
+          if (uint64_t(nd.first) + cnt > d.child_count) throw std::invalid_argument("node children out of range");
+          for (uint32_t k = 0; k < cnt; ++k) {
+            if (d.children[nd.first + k] >= d.node_count) throw std::invalid_argument("bad child node");
+            n.kids.push_back(d.children[nd.first + k]);
+          }
+          n.mat = affine(nd.to_world);
+          n.inv = affine(nd.to_local);
+        } else {
+          throw std::invalid_argument("unknown node kind");
+        }
+        nodes.push_back(std::move(n));
+      }
+      for (uint32_t i = 0; i < d.root_count; ++i) {
+        if (d.roots[i] >= nodes.size()) throw std::invalid_argument("bad root node");
+        roots.push_back(d.roots[i]);
+      }
+      check_acyclic();
+    } else {
+      for (uint32_t i = 0; i < objects.size(); ++i) {
+        Node n{};
+        n.kind = O_NODE_SIMPLE;
+        n.object = i;
+        nodes.push_back(n);
+        roots.push_back(i);
+      }
     }
     for (uint32_t i = 0; i < d.light_count; ++i) {
       const OLightDesc& l = d.lights[i];
@@ -265,34 +357,71 @@ class OScene {
         if (l.kind == O_LIGHT_BACKGROUND) max_radiance = std::max(max_radiance, std::max(l.bottom[c], l.top[c]));
       }
     }
-    build_bvh();
+    commit();
   }
 
-  // ---- geometry of one object ----------------------------------------------------------
-  AABB<R> object_box(const Object& o) const {
-    AABB<R> b;
-    if (o.shape == O_SHAPE_MESH) {
-      b = meshes[o.mesh].bvh->vertex_bounds();
-    } else if (o.shape == O_SHAPE_SPHERE) {
-      b = AABB<R>{{-o.radius, -o.radius, -o.radius}, {o.radius, o.radius, o.radius}};
-    } else {
-      b = AABB<R>{{-o.radius, -o.half_height, -o.radius}, {o.radius, o.half_height, o.radius}};
+  // A node may be shared (the reference holds objects in Arc), but the tree may not loop.
+  void check_acyclic() const {
+    std::vector<int> state(nodes.size(), 0);
+    std::function<void(uint32_t)> walk = [&](uint32_t n) {
+      if (state[n] == 1) throw std::invalid_argument("object tree has a cycle");
+      if (state[n] == 2) return;
+      state[n] = 1;
+      for (uint32_t k : nodes[n].kids) walk(k);
+      state[n] = 2;
+    };
+    for (uint32_t r : roots) walk(r);
+  }
+
+  // ---- bounds (src/geom/aabound.rs, the AABound impls of src/shapes and src/objects) -----
+  // AABoundingBox::transform (aabound.rs:437-468): the eight corners; unbounded stays unbounded
+  static AABB<R> transform_box(const AABB<R>& b, const Affine<R>& m) {
+    if (!b.is_bounded()) {
+      const R inf = std::numeric_limits<R>::infinity();
+      return AABB<R>{{-inf, -inf, -inf}, {inf, inf, inf}};
     }
-    if (!o.transformed) return b;
-    // Transformable for AABoundingBox (aabound.rs:437-468): the eight corners
     const V3<R> mn = b.bmin, mx = b.bmax;
     const V3<R> c[8] = {{mn.x, mn.y, mn.z}, {mn.x, mn.y, mx.z}, {mn.x, mx.y, mn.z}, {mn.x, mx.y, mx.z},
                         {mx.x, mx.y, mx.z}, {mx.x, mx.y, mn.z}, {mx.x, mn.y, mx.z}, {mx.x, mn.y, mn.z}};
-    AABB<R> t{{Limits<R>::max(), Limits<R>::max(), Limits<R>::max()},
-              {Limits<R>::lowest(), Limits<R>::lowest(), Limits<R>::lowest()}};
+    AABB<R> t = AABB<R>::empty();
     for (int k = 0; k < 8; ++k) {
-      V3<R> p = o.mat.point(c[k]);
+      const V3<R> p = m.point(c[k]);
       t.bmin = {rmin(t.bmin.x, p.x), rmin(t.bmin.y, p.y), rmin(t.bmin.z, p.z)};
       t.bmax = {rmax(t.bmax.x, p.x), rmax(t.bmax.y, p.y), rmax(t.bmax.z, p.z)};
     }
     return t;
   }
 
+  AABB<R> shape_box(const Object& o) const {
+    const R inf = std::numeric_limits<R>::infinity();
+    switch (o.shape) {
+      case O_SHAPE_MESH: return meshes[o.mesh].bvh->vertex_bounds();
+      case O_SHAPE_SPHERE: return AABB<R>{{-o.radius, -o.radius, -o.radius}, {o.radius, o.radius, o.radius}};
+      case O_SHAPE_CYLINDER:
+        return AABB<R>{{-o.radius, -o.half_height, -o.radius}, {o.radius, o.half_height, o.radius}};
+      case O_SHAPE_RECTANGLE: return AABB<R>{{-o.half_w, R(0), -o.half_h}, {o.half_w, R(0), o.half_h}};
+      case O_SHAPE_AABOX: return AABB<R>{o.amin, o.amax};
+      default: return AABB<R>{{-inf, -inf, -inf}, {inf, R(0), inf}};  // Plane (plane.rs:89-93)
+    }
+  }
+
+  AABB<R> object_box(const Object& o) const {
+    const AABB<R> b = shape_box(o);
+    return o.transformed ? transform_box(b, o.mat) : b;
+  }
+
+  // get_bounding_box of a node: Simple = its shape's; Transformed = the child's through the
+  // transform (transformed.rs:70-74); Compound = the union (compound.rs:57-64)
+  AABB<R> node_box(uint32_t n) const {
+    const Node& nd = nodes[n];
+    if (nd.kind == O_NODE_SIMPLE) return object_box(objects[nd.object]);
+    if (nd.kind == O_NODE_TRANSFORMED) return transform_box(node_box(nd.kids[0]), nd.mat);
+    AABB<R> u = AABB<R>::empty();
+    for (uint32_t k : nd.kids) u.combine(node_box(k));
+    return u;
+  }
+
+  // ---- the analytic shapes ------------------------------------------------------------------
   // Sphere::intersect (sphere.rs:108-144) — first listed hit, as Simple::intersect keeps
   bool sphere_hit(const Object& o, const Ray<R>& ray, R near, R far, R* t_out) const {
     const V3<R> l = ray.o * R(-1);
@@ -359,16 +488,79 @@ class OScene {
     return true;
   }
 
+  // Rectangle::intersect (rectangle.rs:25-60): the y = 0 plane within |x| <= hw, |z| <= hh
+  bool rectangle_hit(const Object& o, const Ray<R>& ray, R near, R far, R* t_out) const {
+    if (ray.d.y == R(0)) return false;
+    const R d = (ray.o.y * R(-1)) / ray.d.y;
+    if (d < near || d > far) return false;
+    V3<R> p = ray.o + ray.d * d;
+    p.y = R(0);
+    if (std::fabs(p.x) > o.half_w || std::fabs(p.z) > o.half_h) return false;
+    *t_out = d;
+    return true;
+  }
+
+  // Plane::intersect (plane.rs:19-45), its arithmetic as written: d = (o.y * -1) / (1 / dir.y)
+  static bool plane_hit(const Ray<R>& ray, R near, R far, R* t_out) {
+    const R inv_dir = R(1) / ray.d.y;
+    const R d = (ray.o.y * R(-1)) / inv_dir;
+    if (d < near || d > far) return false;
+    *t_out = d;
+    return true;
+  }
+
+  // AABox::intersect (aabox.rs:76-190): slabs with the entering/leaving face tracked; the
+  // first listed hit is the entry when it lies beyond near, else the exit. face: 0..5 for
+  // X_NEG, X_POS, Y_NEG, Y_POS, Z_NEG, Z_POS.
+  static bool aabox_hit(const Object& o, const Ray<R>& ray, R near, R far, R* t_out, int* face) {
+    const V3<R> inv{R(1) / ray.d.x, R(1) / ray.d.y, R(1) / ray.d.z};
+    R tmin, tmax;
+    int fmin, fmax;
+    if (inv.x >= R(0)) { tmin = (o.amin.x - ray.o.x) * inv.x; tmax = (o.amax.x - ray.o.x) * inv.x; fmin = 0; fmax = 1; }
+    else { tmin = (o.amax.x - ray.o.x) * inv.x; tmax = (o.amin.x - ray.o.x) * inv.x; fmin = 1; fmax = 0; }
+    R tymin, tymax;
+    int fymin, fymax;
+    if (inv.y >= R(0)) { tymin = (o.amin.y - ray.o.y) * inv.y; tymax = (o.amax.y - ray.o.y) * inv.y; fymin = 2; fymax = 3; }
+    else { tymin = (o.amax.y - ray.o.y) * inv.y; tymax = (o.amin.y - ray.o.y) * inv.y; fymin = 3; fymax = 2; }
+    if ((tmin > tymax) || (tymin > tmax)) return false;
+    if (tymin > tmin) { tmin = tymin; fmin = fymin; }
+    if (tymax < tmax) { tmax = tymax; fmax = fymax; }
+    R tzmin, tzmax;
+    int fzmin, fzmax;
+    if (inv.z >= R(0)) { tzmin = (o.amin.z - ray.o.z) * inv.z; tzmax = (o.amax.z - ray.o.z) * inv.z; fzmin = 4; fzmax = 5; }
+    else { tzmin = (o.amax.z - ray.o.z) * inv.z; tzmax = (o.amin.z - ray.o.z) * inv.z; fzmin = 5; fzmax = 4; }
+    if ((tmin > tzmax) || (tzmin > tmax)) return false;
+    if (tzmin > tmin) { tmin = tzmin; fmin = fzmin; }
+    if (tzmax < tmax) { tmax = tzmax; fmax = fzmax; }
+    if (tmax < near || tmin > far) return false;
+    if (tmin > near) { *t_out = tmin; *face = fmin; return true; }
+    if (tmax < far) { *t_out = tmax; *face = fmax; return true; }
+    return false;
+  }
+
   Ray<R> local_ray(const Object& o, const Ray<R>& ray) const {
     if (!o.transformed) return ray;
     return make_ray(o.inv.point(ray.o), o.inv.direction(ray.d));  // transform_ray_to_local (transform.rs:98-103)
   }
 
-  // Object::intersect → the world-space interaction (transformed.rs:27-38, simple.rs:28-41)
+  // transform_interaction_to_world (transform.rs:105-116): d, u, v are kept
+  static Isect<R> to_world_isect(const Isect<R>& h, const Affine<R>& mat, const Affine<R>& inv) {
+    Isect<R> w = h;
+    w.n = inv.normal(h.n);
+    w.p = mat.point(h.p);
+    w.wo = mat.direction(h.wo);
+    w.dpdu = mat.direction(h.dpdu);
+    w.dpdv = mat.direction(h.dpdv);
+    return w;
+  }
+
+  // Simple::intersect (simple.rs:28-41) of one object, through its own transform if any;
+  // prim = triangle index, cylinder piece or aabox face (0 otherwise)
   bool intersect_object(uint32_t oi, const Ray<R>& ray, R near, R far, Isect<R>* out, uint32_t* prim) const {
     const Object& o = objects[oi];
     const Ray<R> lr = local_ray(o, ray);
     Isect<R> h;
+    R t;
     if (o.shape == O_SHAPE_MESH) {
       const Mesh& m = meshes[o.mesh];
       TriHit<R> th;
@@ -378,39 +570,86 @@ class OScene {
       mesh_details(m, tri, lr, th, &h);
       *prim = tri;
     } else if (o.shape == O_SHAPE_SPHERE) {
-      R t;
       if (!sphere_hit(o, lr, near, far, &t)) return false;
       sphere_details(o, lr, t, &h);
       *prim = 0;
-    } else {
-      R t;
+    } else if (o.shape == O_SHAPE_CYLINDER) {
       int piece;
       if (!cylinder_hit(o, lr, near, far, &t, &piece)) return false;
       cylinder_details(o, lr, t, piece, &h);
       *prim = uint32_t(piece);  // 0 wall, 1 bottom cap, 2 top cap
+    } else if (o.shape == O_SHAPE_RECTANGLE || o.shape == O_SHAPE_PLANE) {
+      if (o.shape == O_SHAPE_RECTANGLE ? !rectangle_hit(o, lr, near, far, &t) : !plane_hit(lr, near, far, &t))
+        return false;
+      flat_details(lr, t, &h);
+      *prim = 0;
+    } else {
+      int face;
+      if (!aabox_hit(o, lr, near, far, &t, &face)) return false;
+      aabox_details(lr, t, face, &h);
+      *prim = uint32_t(face);
     }
-    if (o.transformed) {  // transform_interaction_to_world (transform.rs:105-116)
-      Isect<R> w = h;
-      w.n = o.inv.normal(h.n);
-      w.p = o.mat.point(h.p);
-      w.wo = o.mat.direction(h.wo);
-      w.dpdu = o.mat.direction(h.dpdu);
-      w.dpdv = o.mat.direction(h.dpdv);
-      h = w;
-    }
-    *out = h;
+    *out = o.transformed ? to_world_isect(h, o.mat, o.inv) : h;
     return true;
   }
 
-  // Intersectable::intersect_p through Simple/Transformed (simple.rs:70-72, transformed.rs:145-148)
+  // Intersectable::intersect_p through Simple (simple.rs:54-56): the shape's default
+  // `!intersect().is_empty()` (intersectable.rs:48-50), the mesh's own BVH any-hit
   bool occluded_object(uint32_t oi, const Ray<R>& ray, R near, R far) const {
     const Object& o = objects[oi];
     const Ray<R> lr = local_ray(o, ray);
-    if (o.shape == O_SHAPE_MESH) return meshes[o.mesh].bvh->intersect_p(lr, near, far);
     R t;
     int piece;
-    if (o.shape == O_SHAPE_SPHERE) return sphere_hit(o, lr, near, far, &t);
-    return cylinder_hit(o, lr, near, far, &t, &piece);
+    switch (o.shape) {
+      case O_SHAPE_MESH: return meshes[o.mesh].bvh->intersect_p(lr, near, far);
+      case O_SHAPE_SPHERE: return sphere_hit(o, lr, near, far, &t);
+      case O_SHAPE_CYLINDER: return cylinder_hit(o, lr, near, far, &t, &piece);
+      case O_SHAPE_RECTANGLE: return rectangle_hit(o, lr, near, far, &t);
+      case O_SHAPE_AABOX: return aabox_hit(o, lr, near, far, &t, &piece);
+      default: return plane_hit(lr, near, far, &t);
+    }
+  }
+
+  // Object::intersect of a tree node: Transformed (transformed.rs:27-38) moves the ray in
+  // and the interaction out; Compound (compound.rs:21-38) keeps the strictly nearest, the
+  // earlier member on a tie.
+  bool intersect_node(uint32_t n, const Ray<R>& ray, R near, R far, Isect<R>* out, uint32_t* obj,
+                      uint32_t* prim) const {
+    const Node& nd = nodes[n];
+    if (nd.kind == O_NODE_SIMPLE) {
+      if (!intersect_object(nd.object, ray, near, far, out, prim)) return false;
+      *obj = nd.object;
+      return true;
+    }
+    if (nd.kind == O_NODE_TRANSFORMED) {
+      const Ray<R> lr = make_ray(nd.inv.point(ray.o), nd.inv.direction(ray.d));
+      Isect<R> h;
+      if (!intersect_node(nd.kids[0], lr, near, far, &h, obj, prim)) return false;
+      *out = to_world_isect(h, nd.mat, nd.inv);
+      return true;
+    }
+    bool have = false;
+    for (uint32_t k : nd.kids) {
+      Isect<R> c;
+      uint32_t co, cp;
+      if (!intersect_node(k, ray, near, far, &c, &co, &cp)) continue;
+      if (have && !(c.d < out->d)) continue;
+      have = true;
+      *out = c;
+      *obj = co;
+      *prim = cp;
+    }
+    return have;
+  }
+
+  bool occluded_node(uint32_t n, const Ray<R>& ray, R near, R far) const {
+    const Node& nd = nodes[n];
+    if (nd.kind == O_NODE_SIMPLE) return occluded_object(nd.object, ray, near, far);
+    if (nd.kind == O_NODE_TRANSFORMED)
+      return occluded_node(nd.kids[0], make_ray(nd.inv.point(ray.o), nd.inv.direction(ray.d)), near, far);
+    for (uint32_t k : nd.kids)
+      if (occluded_node(k, ray, near, far)) return true;  // compound.rs:47-49
+    return false;
   }
 
   // TriangleMesh::intersect post-hit (triangle_mesh.rs:73-132, 219-258) with default uvs
@@ -486,15 +725,59 @@ class OScene {
     }
   }
 
-  // ---- scene BVH (src/bvh.rs:109-388) ---------------------------------------------------
-  void build_bvh() {
+  // Rectangle and Plane records (rectangle.rs:46-55, plane.rs:31-40): p on y = 0, n = +y,
+  // u = p.x, v = p.z, dpdu = +x, dpdv = +z
+  static void flat_details(const Ray<R>& ray, R t, Isect<R>* h) {
+    V3<R> p = ray.o + ray.d * t;
+    p.y = R(0);
+    h->p = p;
+    h->d = t;
+    h->n = V3<R>{R(0), R(1), R(0)};
+    h->wo = ray.d * R(-1);
+    h->u = p.x;
+    h->v = p.z;
+    h->dpdu = V3<R>{R(1), R(0), R(0)};
+    h->dpdv = V3<R>{R(0), R(0), R(1)};
+  }
+
+  // AABox face records (aabox.rs:29-63, 165-190): u = p·du, v = p·dv
+  static void aabox_details(const Ray<R>& ray, R t, int face, Isect<R>* h) {
+    static const R F[6][9] = {
+        {-1, 0, 0, 0, 0, -1, 0, 1, 0}, {1, 0, 0, 0, 0, 1, 0, 1, 0},  {0, -1, 0, -1, 0, 0, 0, 0, 1},
+        {0, 1, 0, 1, 0, 0, 0, 0, 1},   {0, 0, -1, 0, -1, 0, 1, 0, 0}, {0, 0, 1, 0, 1, 0, 1, 0, 0}};
+    const R* f = F[face];
+    const V3<R> p = ray.o + ray.d * t;
+    h->p = p;
+    h->d = t;
+    h->n = V3<R>{f[0], f[1], f[2]};
+    h->wo = ray.d * R(-1);
+    h->dpdu = V3<R>{f[3], f[4], f[5]};
+    h->dpdv = V3<R>{f[6], f[7], f[8]};
+    h->u = dot(p, h->dpdu);
+    h->v = dot(p, h->dpdv);
+  }
+
+  // ---- the scene: Scene::commit + BVH::new (scene.rs:101-115, bvh.rs:109-132, 291-357) ----
+  void commit() {
     order.clear();
     bnodes.clear();
     boxes.clear();
-    for (uint32_t i = 0; i < objects.size(); ++i) boxes.push_back(object_box(objects[i]));
-    if (objects.empty()) return;
-    for (uint32_t i = 0; i < objects.size(); ++i) order.push_back(i);
-    bnodes.push_back(BNode{AABB<R>::empty(), 0, uint32_t(objects.size())});
+    unbounded.clear();
+    std::vector<uint32_t> bounded;
+    for (uint32_t r : roots) {
+      const AABB<R> b = node_box(r);
+      if (b.is_bounded()) {
+        bounded.push_back(r);
+        boxes.push_back(b);
+      } else {
+        unbounded.push_back(r);
+      }
+    }
+    if (bounded.empty()) return;
+    // order[k] indexes `boxes`/`bounded`; prim_root maps it to the root node
+    prim_root = bounded;
+    for (uint32_t i = 0; i < bounded.size(); ++i) order.push_back(i);
+    bnodes.push_back(BNode{AABB<R>::empty(), 0, uint32_t(bounded.size())});
     subdivide(0);
   }
 
@@ -531,53 +814,80 @@ class OScene {
     return u;
   }
 
-  // Scene::find_nearest + BVH::query (scene.rs:186-220, bvh.rs:153-230)
-  bool intersect(const Ray<R>& ray, R near, R far, Isect<R>* out, uint32_t* obj_out, uint32_t* prim_out) const {
-    if (bnodes.empty()) return false;
+  bool hit_box(const BNode& nd, const Ray<R>& ray, R near, R far, R* e, SceneStats* st) const {
+    if (st) st->box_tests++;
+    return box_hit(nd.box, ray, near, far, e);
+  }
+
+  // Scene::find_nearest (scene.rs:186-235): the unbounded primitives first, then BVH::query
+  // (bvh.rs:153-230) over [near, nearest so far], adopting only strictly nearer hits.
+  bool intersect(const Ray<R>& ray, R near, R far, Isect<R>* out, uint32_t* obj_out, uint32_t* prim_out,
+                 SceneStats* st = nullptr) const {
     bool have = false;
     Isect<R> nearest{};
-    R min_t = far;
-    R e;
-    if (!box_hit(bnodes[0].box, ray, near, min_t, &e)) return false;
-    struct Ent { uint32_t n; R e; };
-    std::vector<Ent> stack;
-    stack.reserve(64);
-    stack.push_back(Ent{0, e});
-    while (!stack.empty()) {
-      const Ent en = stack.back();
-      stack.pop_back();
-      if (en.e >= min_t) continue;
-      const BNode& nd = bnodes[en.n];
-      if (nd.count > 0) {
-        for (uint32_t k = nd.left_first; k < nd.left_first + nd.count; ++k) {
-          Isect<R> c;
-          uint32_t prim;
-          if (!intersect_object(order[k], ray, near, min_t, &c, &prim)) continue;
-          if (have && !(c.d < nearest.d)) continue;  // strictly nearer (scene.rs:206-210)
-          have = true;
-          nearest = c;
-          *obj_out = order[k];
-          *prim_out = prim;
-          min_t = c.d;
+    for (uint32_t r : unbounded) {  // nearest_among + closer (scene.rs:222-249)
+      if (st) st->object_tests++;
+      Isect<R> c;
+      uint32_t o, p;
+      if (!intersect_node(r, ray, near, far, &c, &o, &p)) continue;
+      if (have && !(c.d < nearest.d)) continue;
+      have = true;
+      nearest = c;
+      *obj_out = o;
+      *prim_out = p;
+    }
+    if (!bnodes.empty()) {
+      R min_t = have ? nearest.d : far;
+      R e;
+      if (hit_box(bnodes[0], ray, near, min_t, &e, st)) {
+        struct Ent { uint32_t n; R e; };
+        std::vector<Ent> stack;
+        stack.reserve(64);
+        stack.push_back(Ent{0, e});
+        while (!stack.empty()) {
+          const Ent en = stack.back();
+          stack.pop_back();
+          if (en.e >= min_t) continue;
+          if (st) st->nodes_visited++;
+          const BNode& nd = bnodes[en.n];
+          if (nd.count > 0) {
+            for (uint32_t k = nd.left_first; k < nd.left_first + nd.count; ++k) {
+              if (st) st->object_tests++;
+              Isect<R> c;
+              uint32_t o, p;
+              if (!intersect_node(prim_root[order[k]], ray, near, min_t, &c, &o, &p)) continue;
+              if (have && !(c.d < nearest.d)) continue;  // strictly nearer (scene.rs:206-210)
+              have = true;
+              nearest = c;
+              *obj_out = o;
+              *prim_out = p;
+              min_t = c.d;
+            }
+          } else {
+            R dl = R(0), dr = R(0);
+            const bool hl = hit_box(bnodes[nd.left_first], ray, near, min_t, &dl, st);
+            const bool hr = hit_box(bnodes[nd.left_first + 1], ray, near, min_t, &dr, st);
+            uint32_t nn = nd.left_first, ff = nd.left_first + 1;
+            bool hn = hl, hf = hr;
+            R dn = dl, df = dr;
+            if (hl && hr && dr < dl) { nn = nd.left_first + 1; ff = nd.left_first; hn = hr; hf = hl; dn = dr; df = dl; }
+            if (hf) stack.push_back(Ent{ff, df});
+            if (hn) stack.push_back(Ent{nn, dn});
+          }
         }
-      } else {
-        R dl = R(0), dr = R(0);
-        const bool hl = box_hit(bnodes[nd.left_first].box, ray, near, min_t, &dl);
-        const bool hr = box_hit(bnodes[nd.left_first + 1].box, ray, near, min_t, &dr);
-        uint32_t nn = nd.left_first, ff = nd.left_first + 1;
-        bool hn = hl, hf = hr;
-        R dn = dl, df = dr;
-        if (hl && hr && dr < dl) { nn = nd.left_first + 1; ff = nd.left_first; hn = hr; hf = hl; dn = dr; df = dl; }
-        if (hf) stack.push_back(Ent{ff, df});
-        if (hn) stack.push_back(Ent{nn, dn});
       }
     }
     if (have) *out = nearest;
     return have;
   }
 
-  // Scene::any_hit + BVH::query_p (scene.rs:157-168, bvh.rs:239-275)
-  bool occluded(const Ray<R>& ray, R near, R far) const {
+  // Scene::any_hit (scene.rs:157-184): the unbounded primitives first, then BVH::query_p
+  // (bvh.rs:239-275): unordered, the box tested at pop, left popped first.
+  bool occluded(const Ray<R>& ray, R near, R far, SceneStats* st = nullptr) const {
+    for (uint32_t r : unbounded) {
+      if (st) st->object_tests++;
+      if (occluded_node(r, ray, near, far)) return true;
+    }
     if (bnodes.empty()) return false;
     std::vector<uint32_t> stack;
     stack.reserve(64);
@@ -586,10 +896,13 @@ class OScene {
       const BNode& nd = bnodes[stack.back()];
       stack.pop_back();
       R e;
-      if (!box_hit(nd.box, ray, near, far, &e)) continue;
+      if (!hit_box(nd, ray, near, far, &e, st)) continue;
+      if (st) st->nodes_visited++;
       if (nd.count > 0) {
-        for (uint32_t k = nd.left_first; k < nd.left_first + nd.count; ++k)
-          if (occluded_object(order[k], ray, near, far)) return true;
+        for (uint32_t k = nd.left_first; k < nd.left_first + nd.count; ++k) {
+          if (st) st->object_tests++;
+          if (occluded_node(prim_root[order[k]], ray, near, far)) return true;
+        }
       } else {
         stack.push_back(nd.left_first + 1);
         stack.push_back(nd.left_first);
@@ -601,7 +914,16 @@ class OScene {
   // ---- lights -------------------------------------------------------------------------------
   void setup_area(Light& L) {
     if (L.object >= objects.size()) throw std::invalid_argument("area light object out of range");
+    // the emitter must be one primitive of the scene (a root Simple node), so that its own
+    // transform is its whole placement
+    uint32_t refs = 0, root_refs = 0;
+    for (const Node& n : nodes) refs += n.kind == O_NODE_SIMPLE && n.object == L.object;
+    for (uint32_t r : roots) root_refs += nodes[r].kind == O_NODE_SIMPLE && nodes[r].object == L.object;
+    if (refs != 1 || root_refs != 1)
+      throw std::invalid_argument("an area light's object must be placed once, as a primitive of the scene");
     const Object& o = objects[L.object];
+    if (materials[o.material].texture != O_TEX_PLAIN)
+      throw std::invalid_argument("an area light's emission must be a plain color");
     if (o.shape == O_SHAPE_MESH) {
       const Mesh& m = meshes[o.mesh];
       const size_t nt = m.idx.size() / 3;
@@ -713,11 +1035,24 @@ class OScene {
   }
 
   // ---- materials ----------------------------------------------------------------------------
+  // Texture::shade at the interaction: PlainColor, or CheckerBoard::shade
+  // (textures/checker_board.rs:17-28) on the record's u, v (`%` is fmod; signum(±0) = ±1)
+  static V3<R> texel(const Material& m, const Isect<R>& it) {
+    if (m.texture == O_TEX_PLAIN) return m.color;
+    const R su = std::fmod(std::fabs(it.u) * m.scale, R(1));
+    const R sv = std::fmod(std::fabs(it.v) * m.scale, R(1));
+    const bool use_color = (su < R(0.5) && sv < R(0.5)) || (su >= R(0.5) && sv >= R(0.5));
+    const bool positive = !std::isnan(it.u) && !std::isnan(it.v) &&
+                          std::copysign(R(1), it.u) * std::copysign(R(1), it.v) >= R(0);
+    return (use_color != positive) ? m.color : m.color2;
+  }
+
   // Material::f (materials.rs:32-34, lambertian.rs:40-52)
   V3<R> bsdf_f(const Material& m, const V3<R>& wo, const V3<R>& wi, const Isect<R>& it) const {
     if (m.kind != O_MAT_LAMBERTIAN) return V3<R>{R(0), R(0), R(0)};
     const V3<R> lwi = it.to_local(wi), lwo = it.to_local(wo);
-    if (lwo.z * lwi.z > R(0)) return V3<R>{m.color.x / Consts<R>::pi(), m.color.y / Consts<R>::pi(), m.color.z / Consts<R>::pi()};
+    const V3<R> c = texel(m, it);
+    if (lwo.z * lwi.z > R(0)) return V3<R>{c.x / Consts<R>::pi(), c.y / Consts<R>::pi(), c.z / Consts<R>::pi()};
     return V3<R>{R(0), R(0), R(0)};
   }
 
@@ -740,6 +1075,7 @@ class OScene {
 
   bool scatter(const Material& m, const Isect<R>& it, Pcg32& rng, Scatter* s) const {
     const R PI = Consts<R>::pi();
+    const V3<R> col = texel(m, it);
     if (m.kind == O_MAT_LAMBERTIAN) {  // lambertian.rs:24-38, pdfs/cosine.rs:10-24
       const R two_pi = R(2) * PI;
       const R phi = two_pi * R(rng.uniform());
@@ -749,7 +1085,7 @@ class OScene {
       const V3<R> lwi{std::cos(phi) * r2s, std::sin(phi) * r2s, ct};
       const V3<R> wi = it.to_world(lwi);
       s->ray = make_ray(it.p + it.n * R(0.001), wi);
-      s->att = V3<R>{m.color.x / PI, m.color.y / PI, m.color.z / PI};
+      s->att = V3<R>{col.x / PI, col.y / PI, col.z / PI};
       s->pdf = std::fabs(lwi.z / PI);
       return true;
     }
@@ -761,7 +1097,7 @@ class OScene {
       const V3<R> w = it.to_world(tgt);
       s->ray = make_ray(it.p + it.n * R(0.001), w);
       const R ac = std::fabs(tgt.z);
-      s->att = V3<R>{m.color.x / ac, m.color.y / ac, m.color.z / ac};
+      s->att = V3<R>{col.x / ac, col.y / ac, col.z / ac};
       s->pdf = R(1);
       return true;
     }
@@ -799,7 +1135,7 @@ class OScene {
       }
       s->ray = make_ray(origin, it.to_world(ldir));
       const R ac = std::fabs(ldir.z);
-      s->att = V3<R>{m.color.x / ac, m.color.y / ac, m.color.z / ac};
+      s->att = V3<R>{col.x / ac, col.y / ac, col.z / ac};
       s->pdf = R(1);
       return true;
     }
@@ -831,18 +1167,21 @@ class OScene {
         break;
       }
       const Material& m = materials[material_of(obj, prim)];
-      if (specular && m.kind == O_MAT_DIFFUSE_LIGHT)
-        L = L + V3<R>{m.color.x * beta.x, m.color.y * beta.y, m.color.z * beta.z};
+      if (specular && m.kind == O_MAT_DIFFUSE_LIGHT) {  // DiffuseLight::emit (diffuse_light.rs:18-22)
+        const V3<R> e = texel(m, it);
+        L = L + V3<R>{e.x * beta.x, e.y * beta.y, e.z * beta.z};
+      }
       bounce++;
       if (bounce == max_depth) break;
       if (cache && bounce >= cache->term_hit && (m.kind == O_MAT_LAMBERTIAN || m.kind == O_MAT_METAL)) {
         const V3<R> wo = ray.d * R(-1);
         const V3<R> n = dot(it.n, wo) < R(0) ? it.n * R(-1) : it.n;
+        const V3<R> alb = texel(m, it);
         const float rec[16] = {float(it.p.x), float(it.p.y), float(it.p.z),
                                m.kind == O_MAT_METAL ? float(m.fuzz) : 1.0f,
                                float(wo.x), float(wo.y), float(wo.z), 0.f,
                                float(n.x), float(n.y), float(n.z), 0.f,
-                               float(m.color.x), float(m.color.y), float(m.color.z), 0.f};
+                               float(alb.x), float(alb.y), float(alb.z), 0.f};
         float o[3];
         cache->query(rec, o);
         const float mx = cache->max_radiance;
@@ -899,7 +1238,10 @@ class OScene {
         break;
       }
       const Material& m = materials[material_of(obj, prim)];
-      if (m.kind == O_MAT_DIFFUSE_LIGHT) L = L + V3<R>{m.color.x * beta.x, m.color.y * beta.y, m.color.z * beta.z};
+      if (m.kind == O_MAT_DIFFUSE_LIGHT) {
+        const V3<R> e = texel(m, it);
+        L = L + V3<R>{e.x * beta.x, e.y * beta.y, e.z * beta.z};
+      }
       Scatter sc;
       if (!scatter(m, it, rng, &sc)) break;
       const R ac = std::fabs(dot(sc.ray.d, it.n));
@@ -915,8 +1257,12 @@ class OScene {
   std::vector<Object> objects;
   std::vector<Material> materials;
   std::vector<Light> lights;
-  std::vector<AABB<R>> boxes;
-  std::vector<uint32_t> order;
+  std::vector<Node> nodes;
+  std::vector<uint32_t> roots;      // the scene's primitives (tree nodes), in add order
+  std::vector<uint32_t> unbounded;  // roots kept out of the BVH (Scene::commit)
+  std::vector<uint32_t> prim_root;  // BVH primitive -> root node
+  std::vector<AABB<R>> boxes;       // BVH primitive boxes
+  std::vector<uint32_t> order;      // leaf slot -> BVH primitive
   std::vector<BNode> bnodes;
 };
 

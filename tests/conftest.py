@@ -33,6 +33,36 @@ def published():
 
 
 @pytest.fixture(scope="session")
+def published_scenes():
+    with open(os.path.join(GOLDEN, "bvh_stats_published.json")) as f:
+        return json.load(f)["scenes"]
+
+
+def stage_text(name: str) -> str:
+    """A scene file of the reference's test_files/ (copied under tests/golden/stage/)."""
+    with open(os.path.join(GOLDEN, "stage", name)) as f:
+        return f.read()
+
+
+def fixture_mesh_loader(meshes: dict, reference_dir=None):
+    """load_ply_mesh(file, reverse) for scene files: the meshes of meshes.npz, else the
+    reference checkout's test_files/ when `reference_dir` is given. Faces reversed as
+    src/loader/mesh_loader.rs:60-70 does."""
+    import oracle
+
+    def load(name: str, reverse: bool):
+        key = os.path.basename(name).replace(".ply", "")
+        if key + "_vertices" in meshes:
+            v, i = meshes[key + "_vertices"], meshes[key + "_indices"]
+            return v, (i[:, ::-1] if reverse else i)
+        if reference_dir is None:
+            pytest.skip(f"{name} is not among the fixtures")
+        return oracle.read_ply(os.path.join(reference_dir, os.path.basename(name)), reverse)
+
+    return load
+
+
+@pytest.fixture(scope="session")
 def reference_test_files():
     p = os.path.join(REFERENCE_ROOT, "test_files")
     if not os.path.isdir(p):
