@@ -74,10 +74,28 @@ int pbrt_ctx_sync(pbrt_ctx* ctx);
 /* ---------------------------------------------------------------------------------- */
 
 typedef enum pbrt_shape_kind {
-  PBRT_SHAPE_MESH = 0,     /* TriangleMesh (src/shapes/triangle_mesh/triangle_mesh.rs:11-41) */
-  PBRT_SHAPE_SPHERE = 1,   /* Sphere of `radius` at the origin (src/shapes/sphere.rs:11-23) */
-  PBRT_SHAPE_CYLINDER = 2  /* Cylinder along y, `radius`, `height` (src/shapes/cylinder.rs:7-21) */
+  PBRT_SHAPE_MESH = 0,      /* TriangleMesh (src/shapes/triangle_mesh/triangle_mesh.rs:11-41) */
+  PBRT_SHAPE_SPHERE = 1,    /* Sphere of `radius` at the origin (src/shapes/sphere.rs:11-23) */
+  PBRT_SHAPE_CYLINDER = 2,  /* Cylinder along y, `radius`, `height` (src/shapes/cylinder.rs:7-21) */
+  PBRT_SHAPE_RECTANGLE = 3, /* Rectangle::new(width = `radius`, height = `height`): the y = 0 plane within
+                               |x| <= width/2, |z| <= height/2, facing +y (src/shapes/rectangle.rs:9-70) */
+  PBRT_SHAPE_AABOX = 4,     /* AABox::new(`extent`): the box [-extent/2, extent/2] (src/shapes/aabox.rs:9-203) */
+  PBRT_SHAPE_PLANE = 5      /* Plane: the y = 0 plane, unbounded (src/shapes/plane.rs:9-94); an unbounded
+                               primitive is kept out of the scene BVH and tested first (src/scene.rs:101-115) */
 } pbrt_shape_kind;
+
+typedef enum pbrt_texture_kind {
+  PBRT_TEXTURE_COLOR = 0,       /* PlainColor(color) (src/textures/plain_color.rs) */
+  PBRT_TEXTURE_CHECKERBOARD = 1 /* CheckerBoard(color, color2, scale) on the hit's u, v
+                                   (src/textures/checker_board.rs:17-28) */
+} pbrt_texture_kind;
+
+typedef enum pbrt_node_kind {
+  PBRT_NODE_SIMPLE = 0,      /* an object of `objects` (Simple, src/objects/simple.rs) */
+  PBRT_NODE_TRANSFORMED = 1, /* Transformed(child) (src/objects/transformed.rs) */
+  PBRT_NODE_COMPOUND = 2     /* Compound(children): the nearest member's hit, the first on a tie
+                                (src/objects/compound.rs:21-65) */
+} pbrt_node_kind;
 
 typedef enum pbrt_material_kind {
   PBRT_MAT_LAMBERTIAN = 0,    /* src/materials/lambertian.rs */
@@ -109,18 +127,34 @@ typedef struct pbrt_material_desc {
   float color[3]; /* albedo (lambertian, metal, dielectric) or emitted radiance (diffuse light) */
   float fuzz;     /* metal */
   float ior;      /* dielectric */
+  uint32_t texture; /* pbrt_texture_kind: where `color` comes from */
+  float color2[3];  /* checkerboard: the second colour */
+  float scale;      /* checkerboard: squares per unit of u and v */
 } pbrt_material_desc;
 
 typedef struct pbrt_object_desc {
   uint32_t shape;          /* pbrt_shape_kind */
   uint32_t mesh;           /* index into meshes, PBRT_SHAPE_MESH only */
-  float radius, height;    /* sphere, cylinder */
+  float radius, height;    /* sphere, cylinder; rectangle: width, height */
   uint32_t material;       /* index into materials */
   uint32_t transformed;    /* 0: Simple (src/objects/simple.rs); 1: Transformed(Simple)
                               (src/objects/transformed.rs) with the two matrices below */
   float to_world[12];      /* row-major 3x4 of Transform::mat (src/geom/transform.rs:7-10) */
   float to_local[12];      /* row-major 3x4 of Transform::inv_mat */
+  float extent[3];         /* aabox: full size along x, y, z */
 } pbrt_object_desc;
+
+/* One node of an object tree (the Object trait objects a scene file builds,
+ * src/loader/visitors/scene_builder.rs:95-116). TRANSFORMED wraps children[first] with
+ * the two matrices; COMPOUND holds children[first .. first + count); SIMPLE names
+ * objects[object] (whose own `transformed` matrices, if set, apply innermost). A node may be
+ * shared by several parents (the reference holds objects in Arc); the tree may not loop. */
+typedef struct pbrt_node_desc {
+  uint32_t kind;  /* pbrt_node_kind */
+  uint32_t object;
+  uint32_t first, count;
+  float to_world[12], to_local[12];
+} pbrt_node_desc;
 
 typedef struct pbrt_light_desc {
   uint32_t kind;           /* pbrt_light_kind */
@@ -144,6 +178,16 @@ typedef struct pbrt_scene_desc {
    * triangles (0 = the reference's 1, i.e. split while the SAH says so). */
   uint32_t bvh_bins;
   uint32_t bvh_max_leaf;
+  /* Optional object tree. nodes == NULL: every object is one primitive of the scene, in
+   * order (Scene::add_object for each). Otherwise the scene's primitives are the nodes
+   * listed in `roots`, in that order; children indexes into `node_children`. Object ids
+   * reported by the trace calls are indexes into `objects` (the Simple that was hit). */
+  const pbrt_node_desc* nodes;
+  uint32_t node_count;
+  const uint32_t* node_children;
+  uint32_t child_count;
+  const uint32_t* roots;
+  uint32_t root_count;
 } pbrt_scene_desc;
 
 /* Builds the acceleration structures on the host and uploads the scene. Replaces
@@ -174,7 +218,7 @@ typedef struct pbrt_scene_info {
   uint64_t mesh_leaf_count;
   uint32_t mesh_max_depth;   /* root = depth 1, as BuildStats::max_depth (bvh.rs:70) */
   uint32_t mesh_max_leaf_tris;
-  uint64_t object_count;
+  uint64_t object_count;     /* the scene's primitives (Scene::primitive_count plus the unbounded ones) */
   uint64_t device_bytes;     /* device memory held by the scene */
 } pbrt_scene_info;
 int pbrt_scene_get_info(const pbrt_scene* scene, pbrt_scene_info* info);
@@ -221,6 +265,16 @@ int pbrt_trace_closest_noalloc(pbrt_scene* scene, const float* rays, uint64_t n,
 /* Whether anything blocks each ray within [tmin, tmax]: replaces Scene::intersect_p
  * (src/scene.rs:143-168) and BVHTree::intersect_p (src/shapes/triangle_mesh/bvh.rs:381-420). */
 int pbrt_trace_any(pbrt_scene* scene, const float* rays, uint64_t n, uint8_t* occluded);
+
+/* The scene-level queries with the scene accelerator's work counters summed over all rays
+ * (any scene): stats[0] nodes visited, stats[1] ray/box tests, stats[2] object tests
+ * (primitives asked, the unbounded ones included), counted as TraversalStats counts them in
+ * Scene::intersect_instrumented / Scene::intersect_p_instrumented (src/scene.rs:124-153,
+ * src/bvh.rs:153-275). The meshes' inner traversals are not counted, as in the reference. */
+int pbrt_trace_closest_counted(pbrt_scene* scene, const float* rays, uint64_t n, uint32_t* prim_id, float* t,
+                               uint32_t* object_id, uint64_t* stats /* 3 */);
+int pbrt_trace_any_counted(pbrt_scene* scene, const float* rays, uint64_t n, uint8_t* occluded,
+                           uint64_t* stats /* 3 */);
 
 /* ---------------------------------------------------------------------------------- */
 /* Rendering                                                                            */
@@ -363,6 +417,51 @@ int pbrt_render_batch(pbrt_scene* const* scenes, const pbrt_render_params* param
  * to their nearest hit (camera and bounce rays, training paths included), stats[1] shadow
  * rays, stats[2] paths started. Synchronises the context's stream. */
 int pbrt_ctx_render_stats(pbrt_ctx* ctx, uint64_t* stats /* 3 */);
+
+/* ---------------------------------------------------------------------------------- */
+/* Scene files (host only, no GPU work)                                                 */
+/* ---------------------------------------------------------------------------------- */
+
+/* A parsed `.stage` scene file: Parser::parse + SceneBuilderVisitor
+ * (src/loader/parser.rs:13-367, src/loader/parser/lexer.rs, src/loader/visitors/scene_builder.rs)
+ * with its meshes read from ASCII PLY files (src/loader/mesh_loader.rs, src/loader/ply/). */
+typedef struct pbrt_stage pbrt_stage;
+
+/* The settings Loader::load_scene takes from its Config (src/config.rs:112-129); zero fields
+ * take the reference's defaults. */
+typedef struct pbrt_stage_options {
+  const char* base_dir;      /* mesh file names are read relative to it (NULL or "": as given) */
+  uint32_t width, height;    /* Config::output_width/height; 0 = 800 x 600 */
+  double fov_deg;            /* Config::fov_deg; 0 = 90 */
+  double near, far;          /* Config::near/far; 0 = 1e-4 / 1000 */
+  uint32_t no_loader_lights; /* 0: add the point light at (0, 2, 1) of intensity 15 and the white-to-
+                                (0.5, 0.7, 1.0) background light that Loader::load_scene adds to every
+                                scene (src/loader.rs:36-42); 1: add none */
+  uint32_t bvh_bins, bvh_max_leaf; /* copied into the scene description */
+} pbrt_stage_options;
+
+/* Parses `text` (a whole scene file) and reads its meshes. On failure returns
+ * PBRT_ERR_INVALID_ARGUMENT (a file the reference's parser rejects, or a shape outside the
+ * ported set: constructive solids) or PBRT_ERR_UNSUPPORTED, with a message in err. */
+int pbrt_stage_parse(const char* text, const pbrt_stage_options* options, pbrt_stage** out, char* err,
+                     size_t err_len);
+/* The scene description (pointing into arrays the stage owns, valid until
+ * pbrt_stage_destroy) and the camera (PinHoleCamera from the file's pos/look/up and the
+ * options; a thin_lens camera is described by its pinhole, see camera_lens). Either output
+ * may be NULL. camera_lens (2 floats, may be NULL) receives the thin lens' radius and focal
+ * distance (0, 0 for a pin_hole camera). */
+int pbrt_stage_describe(const pbrt_stage* stage, pbrt_scene_desc* desc, pbrt_camera_desc* camera,
+                        float* camera_lens);
+void pbrt_stage_destroy(pbrt_stage* stage);
+/* Loader::load_scene (src/loader.rs:29-45): parse + pbrt_scene_create. camera may be NULL. */
+int pbrt_scene_load(pbrt_ctx* ctx, const char* text, const pbrt_stage_options* options, pbrt_scene** scene,
+                    pbrt_camera_desc* camera);
+/* load_ply_mesh(path, reverse) (src/loader/mesh_loader.rs:13-24): vertices (3 floats each) and
+ * triangles (3 indices each; reversed winding when reverse != 0) of an ASCII PLY file,
+ * allocated with malloc (release with pbrt_free). Faces must be triangles. */
+int pbrt_ply_read(const char* path, int reverse, float** vertices, uint32_t* vertex_count, uint32_t** indices,
+                  uint32_t* triangle_count, char* err, size_t err_len);
+void pbrt_free(void* p);
 
 /* Spectrum::gamma_correct + to_rgb (src/spectrum.rs:13-25, 134-136): sqrt gamma, clip to
  * [0, 1], truncate to 8 bits, alpha 255, as image_write stores it (mt.rs:152-167). Host

@@ -10,15 +10,20 @@ from __future__ import annotations
 
 from ._capi import PBRT_MISS, PbrtError, load  # noqa: F401
 from .scene import (  # noqa: F401
+    AABox,
     AreaLight,
     BackgroundInfiniteLight,
+    CheckerBoard,
+    Compound,
     Context,
     Cylinder,
     Dielectric,
     DiffuseLight,
     Lambertian,
     Metal,
+    Plane,
     PointLight,
+    Rectangle,
     Scene,
     Simple,
     Sphere,
@@ -29,9 +34,11 @@ from .scene import (  # noqa: F401
     default_context,
     film_to_rgba8,
 )
+from .stage import Stage, load_scene, read_ply  # noqa: F401
 
 __all__ = [
     "PBRT_MISS", "PbrtError", "load", "Context", "default_context", "Scene", "TriangleMesh", "Sphere", "Cylinder",
     "Simple", "Transformed", "Transform", "Lambertian", "Metal", "Dielectric", "DiffuseLight", "PointLight",
-    "UniformInfiniteLight", "BackgroundInfiniteLight", "AreaLight", "film_to_rgba8",
+    "UniformInfiniteLight", "BackgroundInfiniteLight", "AreaLight", "film_to_rgba8", "Rectangle", "AABox", "Plane",
+    "CheckerBoard", "Compound", "Stage", "load_scene", "read_ply",
 ]

@@ -22,7 +22,9 @@ STATUS = {
     6: "PBRT_ERR_UNSUPPORTED",
 }
 
-SHAPE_MESH, SHAPE_SPHERE, SHAPE_CYLINDER = 0, 1, 2
+SHAPE_MESH, SHAPE_SPHERE, SHAPE_CYLINDER, SHAPE_RECTANGLE, SHAPE_AABOX, SHAPE_PLANE = 0, 1, 2, 3, 4, 5
+TEXTURE_COLOR, TEXTURE_CHECKERBOARD = 0, 1
+NODE_SIMPLE, NODE_TRANSFORMED, NODE_COMPOUND = 0, 1, 2
 MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_DIFFUSE_LIGHT = 0, 1, 2, 3
 LIGHT_POINT, LIGHT_UNIFORM_INFINITE, LIGHT_BACKGROUND_INFINITE, LIGHT_AREA = 0, 1, 2, 3
 
@@ -33,13 +35,19 @@ class MeshDesc(C.Structure):
 
 
 class MaterialDesc(C.Structure):
-    _fields_ = [("kind", C.c_uint32), ("color", C.c_float * 3), ("fuzz", C.c_float), ("ior", C.c_float)]
+    _fields_ = [("kind", C.c_uint32), ("color", C.c_float * 3), ("fuzz", C.c_float), ("ior", C.c_float),
+                ("texture", C.c_uint32), ("color2", C.c_float * 3), ("scale", C.c_float)]
 
 
 class ObjectDesc(C.Structure):
     _fields_ = [("shape", C.c_uint32), ("mesh", C.c_uint32), ("radius", C.c_float), ("height", C.c_float),
                 ("material", C.c_uint32), ("transformed", C.c_uint32), ("to_world", C.c_float * 12),
-                ("to_local", C.c_float * 12)]
+                ("to_local", C.c_float * 12), ("extent", C.c_float * 3)]
+
+
+class NodeDesc(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("object", C.c_uint32), ("first", C.c_uint32), ("count", C.c_uint32),
+                ("to_world", C.c_float * 12), ("to_local", C.c_float * 12)]
 
 
 class LightDesc(C.Structure):
@@ -52,7 +60,10 @@ class SceneDesc(C.Structure):
                 ("materials", C.POINTER(MaterialDesc)), ("material_count", C.c_uint32),
                 ("objects", C.POINTER(ObjectDesc)), ("object_count", C.c_uint32),
                 ("lights", C.POINTER(LightDesc)), ("light_count", C.c_uint32),
-                ("bvh_bins", C.c_uint32), ("bvh_max_leaf", C.c_uint32)]
+                ("bvh_bins", C.c_uint32), ("bvh_max_leaf", C.c_uint32),
+                ("nodes", C.POINTER(NodeDesc)), ("node_count", C.c_uint32),
+                ("node_children", C.POINTER(C.c_uint32)), ("child_count", C.c_uint32),
+                ("roots", C.POINTER(C.c_uint32)), ("root_count", C.c_uint32)]
 
 
 class SceneInfo(C.Structure):
@@ -76,6 +87,12 @@ class CacheParams(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("learning_rate", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
                 ("epsilon", C.c_float), ("scene_min", C.c_float * 3), ("scene_max", C.c_float * 3),
                 ("terminate_bounce", C.c_uint32), ("train_samples", C.c_uint32), ("train_steps", C.c_uint32)]
+
+
+class StageOptions(C.Structure):
+    _fields_ = [("base_dir", C.c_char_p), ("width", C.c_uint32), ("height", C.c_uint32), ("fov_deg", C.c_double),
+                ("near", C.c_double), ("far", C.c_double), ("no_loader_lights", C.c_uint32),
+                ("bvh_bins", C.c_uint32), ("bvh_max_leaf", C.c_uint32)]
 
 
 class Tuning(C.Structure):
@@ -102,6 +119,18 @@ SIGNATURES = {
                                                   C.c_void_p]),
     "pbrt_trace_any": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "pbrt_trace_closest_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
+    "pbrt_trace_closest_counted": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p]),
+    "pbrt_trace_any_counted": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
+    "pbrt_stage_parse": (C.c_int, [C.c_char_p, C.POINTER(StageOptions), C.POINTER(C.c_void_p), C.c_char_p,
+                                   C.c_size_t]),
+    "pbrt_stage_describe": (C.c_int, [C.c_void_p, C.POINTER(SceneDesc), C.POINTER(CameraDesc), C.c_void_p]),
+    "pbrt_stage_destroy": (None, [C.c_void_p]),
+    "pbrt_scene_load": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(StageOptions), C.POINTER(C.c_void_p),
+                                  C.POINTER(CameraDesc)]),
+    "pbrt_ply_read": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.POINTER(C.c_float)), C.POINTER(C.c_uint32),
+                                C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint32), C.c_char_p, C.c_size_t]),
+    "pbrt_free": (None, [C.c_void_p]),
     "pbrt_render": (C.c_int, [C.c_void_p, C.POINTER(RenderParams), C.c_void_p]),
     "pbrt_cache_create": (C.c_int, [C.c_void_p, C.POINTER(CacheParams), C.POINTER(C.c_void_p)]),
     "pbrt_cache_destroy": (None, [C.c_void_p]),

@@ -195,10 +195,14 @@ int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbr
     s->info.device_bytes += dm.bytes;
   }
   void *top = nullptr, *order = nullptr, *objs = nullptr, *mviews = nullptr, *mshades = nullptr, *mats = nullptr,
-       *lights = nullptr, *ltris = nullptr, *lcdf = nullptr;
-  if (rc == PBRT_OK) rc = s->upload(&top, fs.top.data(), fs.top.size() * sizeof(GpuNode));
-  if (rc == PBRT_OK) rc = s->upload(&order, fs.order.data(), fs.order.size() * sizeof(uint32_t));
+       *lights = nullptr, *ltris = nullptr, *lcdf = nullptr, *unb = nullptr, *xfs = nullptr, *grps = nullptr;
+  if (rc == PBRT_OK && !fs.top.empty()) rc = s->upload(&top, fs.top.data(), fs.top.size() * sizeof(GpuNode));
+  if (rc == PBRT_OK && !fs.order.empty()) rc = s->upload(&order, fs.order.data(), fs.order.size() * sizeof(uint32_t));
   if (rc == PBRT_OK) rc = s->upload(&objs, fs.objects.data(), fs.objects.size() * sizeof(ObjRec));
+  if (rc == PBRT_OK && !fs.unbounded.empty())
+    rc = s->upload(&unb, fs.unbounded.data(), fs.unbounded.size() * sizeof(uint32_t));
+  if (rc == PBRT_OK && !fs.xforms.empty()) rc = s->upload(&xfs, fs.xforms.data(), fs.xforms.size() * sizeof(XfRec));
+  if (rc == PBRT_OK && !fs.groups.empty()) rc = s->upload(&grps, fs.groups.data(), fs.groups.size() * sizeof(GroupRec));
   if (rc == PBRT_OK && !views.empty()) rc = s->upload(&mviews, views.data(), views.size() * sizeof(MeshView));
   if (rc == PBRT_OK && !shades.empty()) rc = s->upload(&mshades, shades.data(), shades.size() * sizeof(MeshShade));
   if (rc == PBRT_OK) rc = s->upload(&mats, fs.materials.data(), fs.materials.size() * sizeof(MatRec));
@@ -215,7 +219,11 @@ int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbr
   v.top = (const float4*)top;
   v.top_node_count = uint32_t(fs.top.size());
   v.order = (const uint32_t*)order;
+  v.unbounded = (const uint32_t*)unb;
+  v.unbounded_count = uint32_t(fs.unbounded.size());
   v.objects = (const ObjRec*)objs;
+  v.xforms = (const XfRec*)xfs;
+  v.groups = (const GroupRec*)grps;
   v.meshes = (const MeshView*)mviews;
   v.shade = (const MeshShade*)mshades;
   v.materials = (const MatRec*)mats;
@@ -223,16 +231,15 @@ int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbr
   v.light_count = uint32_t(fs.lights.size());
   v.light_tris = (const float*)ltris;
   v.light_cdf = (const float*)lcdf;
-  s->info.object_count = d->object_count;
+  s->info.object_count = fs.primitive_count;
   s->info.device_bytes += s->extra_bytes;
   s->max_radiance = fs.max_radiance;
   s->has_dielectric = fs.has_dielectric;
-  for (int a = 0; a < 3; ++a) {
-    s->bounds[a] = fs.top[0].bmin[a];
-    s->bounds[3 + a] = fs.top[0].bmax[a];
+  for (int a = 0; a < 3; ++a) {  // the bounded primitives' box (none: an empty box)
+    s->bounds[a] = fs.top.empty() ? 0.0f : fs.top[0].bmin[a];
+    s->bounds[3 + a] = fs.top.empty() ? 0.0f : fs.top[0].bmax[a];
   }
-  if (d->object_count == 1 && d->objects[0].shape == PBRT_SHAPE_MESH && !d->objects[0].transformed)
-    s->single_mesh = int(d->objects[0].mesh);
+  s->single_mesh = fs.single_mesh;
   const int rc2 = c->cuda(cudaStreamSynchronize(c->stream), "scene upload");
   if (rc2 != PBRT_OK) {
     pbrt_scene_destroy(s.release());
@@ -328,6 +335,22 @@ int pbrt_mesh_bvh_build_host(const pbrt_mesh_desc* md, uint32_t bins, uint32_t m
   return PBRT_OK;
 }
 
+// Loader::load_scene (src/loader.rs:29-45): the scene file parsed, then built like any scene.
+int pbrt_scene_load(pbrt_ctx* c, const char* text, const pbrt_stage_options* options, pbrt_scene** scene,
+                    pbrt_camera_desc* camera) {
+  if (!c || !scene) return PBRT_ERR_INVALID_ARGUMENT;
+  *scene = nullptr;
+  char err[512];
+  pbrt_stage* st = nullptr;
+  const int rc = pbrt_stage_parse(text, options, &st, err, sizeof(err));
+  if (rc != PBRT_OK) return c->fail(rc, std::string("scene file: ") + err);
+  pbrt_scene_desc d;
+  pbrt_stage_describe(st, &d, camera, nullptr);
+  const int rc2 = pbrt_scene_create(c, &d, scene);
+  pbrt_stage_destroy(st);
+  return rc2;
+}
+
 int pbrt_scene_get_info(const pbrt_scene* s, pbrt_scene_info* info) {
   if (!s || !info) return PBRT_ERR_INVALID_ARGUMENT;
   *info = s->info;
@@ -339,24 +362,26 @@ int pbrt_scene_get_info(const pbrt_scene* s, pbrt_scene_info* info) {
 namespace {
 
 // Runs the nearest-hit (or, with occ != NULL, any-hit) kernel over host or device buffers.
+// stats with scene_stats: the scene accelerator's counters (any scene); stats alone: the
+// mesh traversal's (scenes of one untransformed mesh).
 int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, float* t, uint32_t* obj, uint8_t* occ,
-               uint64_t* stats) {
+               uint64_t* stats, bool scene_stats = false) {
   if (!s) return PBRT_ERR_INVALID_ARGUMENT;
   pbrt_ctx* c = s->ctx;
   DeviceGuard g(c->device);
   if (n == 0) return PBRT_OK;
   if (!rays || (!occ && (!prim || !t))) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "ray or result buffer is NULL");
-  if (stats && s->single_mesh < 0)
+  if (stats && !scene_stats && s->single_mesh < 0)
     return c->fail(PBRT_ERR_UNSUPPORTED, "work counters are reported for scenes made of one untransformed mesh");
-  const bool one_mesh = s->single_mesh >= 0;
+  const bool one_mesh = s->single_mesh >= 0 && !scene_stats;
   const MeshView mv = one_mesh ? s->meshes[s->single_mesh].view : MeshView{};
   // Nearest hit / any hit of one chunk of `m` rays (planes `stride` apart) on `st`.
   auto launch = [&](const float* r, uint64_t stride, uint64_t m, uint32_t* p, float* tt, uint32_t* ob, uint8_t* oc,
                     unsigned long long* cnt, uint32_t* queue, unsigned long long* qc, float4* rec,
                     cudaStream_t st) -> cudaError_t {
     if (!one_mesh)
-      return oc ? launch_scene_any(s->view, r, stride, m, oc, c->d_err, c->sm_count, st)
-                : launch_scene_closest(s->view, r, stride, m, p, tt, ob, c->d_err, c->sm_count, st);
+      return oc ? launch_scene_any(s->view, r, stride, m, oc, cnt, c->d_err, c->sm_count, st)
+                : launch_scene_closest(s->view, r, stride, m, p, tt, ob, cnt, c->d_err, c->sm_count, st);
     if (oc) return launch_mesh_any(mv, r, stride, m, oc, c->d_err, c->sm_count, st);
     if (c->persistent && !cnt)
       return launch_mesh_closest_persistent(mv, r, stride, m, p, tt, ob, queue, qc, c->d_err, c->sm_count, st, rec);
@@ -493,6 +518,20 @@ int pbrt_trace_closest_noalloc(pbrt_scene* s, const float* rays, uint64_t n, uin
 int pbrt_trace_any(pbrt_scene* s, const float* rays, uint64_t n, uint8_t* occluded) {
   if (!occluded) return s ? s->ctx->fail(PBRT_ERR_INVALID_ARGUMENT, "occluded is NULL") : PBRT_ERR_INVALID_ARGUMENT;
   return trace_impl(s, rays, n, nullptr, nullptr, nullptr, occluded, nullptr);
+}
+
+int pbrt_trace_closest_counted(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim_id, float* t,
+                               uint32_t* object_id, uint64_t* stats) {
+  if (!stats) return s ? s->ctx->fail(PBRT_ERR_INVALID_ARGUMENT, "stats is NULL") : PBRT_ERR_INVALID_ARGUMENT;
+  for (int k = 0; k < 3; ++k) stats[k] = 0;
+  return trace_impl(s, rays, n, prim_id, t, object_id, nullptr, stats, true);
+}
+
+int pbrt_trace_any_counted(pbrt_scene* s, const float* rays, uint64_t n, uint8_t* occluded, uint64_t* stats) {
+  if (!occluded || !stats)
+    return s ? s->ctx->fail(PBRT_ERR_INVALID_ARGUMENT, "occluded or stats is NULL") : PBRT_ERR_INVALID_ARGUMENT;
+  for (int k = 0; k < 3; ++k) stats[k] = 0;
+  return trace_impl(s, rays, n, nullptr, nullptr, nullptr, occluded, stats, true);
 }
 
 }  // extern "C"

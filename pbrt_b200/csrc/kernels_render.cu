@@ -141,9 +141,9 @@ PBRT_DEV bool sample_li(const SceneView& s, const LightRec& L, const Isect& it, 
     nl = normalize3(cross3(sub3(p2, p1), sub3(p1, p0)));
   } else {
     const F3 dir = sphere_dir(st, inc);
-    const F3 lp = mul3(dir, ob.radius);
-    pl = ob.transformed ? xf_point(ob.to_world, lp) : lp;
-    nl = ob.transformed ? normalize3(xf_normal(ob.to_local, dir)) : dir;
+    const F3 lp = mul3(dir, ob.p[0]);
+    pl = ob.xf_count ? xf_point(ob.to_world, lp) : lp;  // emitters sit under at most one transform
+    nl = ob.xf_count ? normalize3(xf_normal(ob.to_local, dir)) : dir;
   }
   const F3 w = sub3(pl, it.p);
   const float d2 = dot3(w, w);
@@ -164,10 +164,10 @@ PBRT_DEV bool sample_li(const SceneView& s, const LightRec& L, const Isect& it, 
 
 // ---- materials --------------------------------------------------------------------------------
 // Material::f (materials.rs:32-34, lambertian.rs:40-52)
-PBRT_DEV F3 bsdf_f(const MatRec& m, const F3& wo, const F3& wi, const Isect& it) {
+PBRT_DEV F3 bsdf_f(const MatRec& m, const F3& alb, const F3& wo, const F3& wi, const Isect& it) {
   if (m.kind != kMatLambertian) return mk3(0.f, 0.f, 0.f);
   const F3 lwi = to_local(it, wi), lwo = to_local(it, wo);
-  if (fm(lwo.z, lwi.z) > 0.f) return mk3(fdv(m.color[0], kPiF), fdv(m.color[1], kPiF), fdv(m.color[2], kPiF));
+  if (fm(lwo.z, lwi.z) > 0.f) return mk3(fdv(alb.x, kPiF), fdv(alb.y, kPiF), fdv(alb.z, kPiF));
   return mk3(0.f, 0.f, 0.f);
 }
 
@@ -187,8 +187,8 @@ struct ScatterOut {
   float pdf;
 };
 
-PBRT_DEV bool scatter(const MatRec& m, const Isect& it, unsigned long long& st, unsigned long long inc, ScatterOut& s) {
-  const F3 col = mk3(m.color[0], m.color[1], m.color[2]);
+PBRT_DEV bool scatter(const MatRec& m, const F3& col, const Isect& it, unsigned long long& st, unsigned long long inc,
+                      ScatterOut& s) {
   if (m.kind == kMatLambertian) {  // lambertian.rs:24-38, pdfs/cosine.rs:10-24
     const float two_pi = fm(2.f, kPiF);
     const float phi = fm(two_pi, pcg_uniform(st, inc));
@@ -424,10 +424,10 @@ __global__ void __launch_bounds__(256) k_shade(WaveBuffers w, Src src, const uin
           L = add3(L, mk3(fm(bg.x, beta.x), fm(bg.y, beta.y), fm(bg.z, beta.z)));
         }
       } else {
-        const Isect it = interaction(s, obj, w.hprim[p], o, d, w.ht[p]);
         const MatRec m = s.materials[material_index(s, obj, w.hprim[p])];
-        if (spec && m.kind == kMatDiffuseLight)
-          L = add3(L, mk3(fm(m.color[0], beta.x), fm(m.color[1], beta.y), fm(m.color[2], beta.z)));
+        const Isect it = interaction(s, obj, w.hprim[p], o, d, w.ht[p], m.texture != kTexColor);
+        const F3 alb = texel(m, it);  // albedo, or emitted radiance (DiffuseLight::emit)
+        if (spec && m.kind == kMatDiffuseLight) L = add3(L, mk3(fm(alb.x, beta.x), fm(alb.y, beta.y), fm(alb.z, beta.z)));
         bounce++;
         // PathIntegrator stops at the max_depth-th hit, before sampling a light (path.rs:64-67);
         // the naive estimator also ends there, its emission counted: after max_depth hits its
@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(256) k_shade(WaveBuffers w, Src src, const uin
           cp = it.p;
           cwo = mul3(d, -1.f);
           cn = dot3(it.n, cwo) < 0.f ? mul3(it.n, -1.f) : it.n;
-          calb = mk3(m.color[0], m.color[1], m.color[2]);
+          calb = alb;
           crough = m.kind == kMatMetal ? m.fuzz : 1.f;
           cL = L;
           cB = beta;
@@ -454,7 +454,7 @@ __global__ void __launch_bounds__(256) k_shade(WaveBuffers w, Src src, const uin
             const float pl = fdv(1.f, cnt);
             LiSample ls;
             if (sample_li(s, s.lights[li], it, st, inc, ls)) {
-              const F3 f0 = bsdf_f(m, mul3(d, -1.f), ls.wi, it);
+              const F3 f0 = bsdf_f(m, alb, mul3(d, -1.f), ls.wi, it);
               const float ac = fabsf(dot3(ls.wi, it.n));
               const F3 f = mk3(fm(f0.x, ac), fm(f0.y, ac), fm(f0.z, ac));
               if (f.x != 0.f || f.y != 0.f || f.z != 0.f) {
@@ -470,7 +470,7 @@ __global__ void __launch_bounds__(256) k_shade(WaveBuffers w, Src src, const uin
             }
           }
           ScatterOut sc;
-          if (scatter(m, it, st, inc, sc)) {
+          if (scatter(m, alb, it, st, inc, sc)) {
             const float ac = fabsf(dot3(sc.rd, it.n));
             const F3 kk = mk3(fdv(fm(sc.att.x, ac), sc.pdf), fdv(fm(sc.att.y, ac), sc.pdf), fdv(fm(sc.att.z, ac), sc.pdf));
             beta = mk3(fm(beta.x, kk.x), fm(beta.y, kk.y), fm(beta.z, kk.z));
@@ -624,29 +624,57 @@ __global__ void k_scale_film(double* film, size_t n, double s) {
 }
 
 // ---- general-scene ray casting ---------------------------------------------------------------
+// Adds a thread's counters to cnt[0..2] (one atomic per warp and counter).
+PBRT_DEV void flush_counts(const SceneCount& c, unsigned long long* cnt) {
+  unsigned long long v[3] = {c.nodes, c.boxes, c.objects};
+  for (int k = 0; k < 3; ++k) {
+    for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xFFFFFFFFu, v[k], off);
+    if ((threadIdx.x & 31) == 0 && v[k]) atomicAdd(cnt + k, v[k]);
+  }
+}
+
+// Nearest hit per ray; object ids are the description's (the leaf's desc_id). kCount adds
+// the scene accelerator's counters (Scene::intersect_instrumented) into cnt.
+template <bool kCount>
 __global__ void __launch_bounds__(128) k_scene_closest(SceneView s, const float* __restrict__ rays, uint64_t stride,
                                                        uint64_t n, uint32_t* __restrict__ prim, float* __restrict__ tout,
-                                                       uint32_t* __restrict__ obj, uint32_t* err) {
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+                                                       uint32_t* __restrict__ obj, unsigned long long* cnt,
+                                                       uint32_t* err) {
+  SceneCount c{0, 0, 0};
+  // whole warps run the same trip count so the counter reduction sees full warps
+  const uint64_t step = uint64_t(gridDim.x) * blockDim.x;
+  const uint64_t iters = (n + step - 1) / step;
+  for (uint64_t it = 0; it < iters; ++it) {
+    const uint64_t i = it * step + uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) continue;
     const F3 o = mk3(__ldcs(rays + i), __ldcs(rays + stride + i), __ldcs(rays + 2 * stride + i));
     const F3 d = mk3(__ldcs(rays + 3 * stride + i), __ldcs(rays + 4 * stride + i), __ldcs(rays + 5 * stride + i));
     const float near = __ldcs(rays + 6 * stride + i), far = __ldcs(rays + 7 * stride + i);
     float t = 0.f;
-    uint32_t ob = 0, pr = 0;
-    const bool hit = scene_closest(s, o, d, near, far, t, ob, pr, err);
+    uint32_t leaf = 0, pr = 0;
+    const bool hit = scene_closest_t<kCount>(s, o, d, near, far, t, leaf, pr, err, &c);
     __stcs(prim + i, hit ? pr : 0xFFFFFFFFu);
     __stcs(tout + i, hit ? t : __int_as_float(0x7f800000));
-    if (obj) __stcs(obj + i, hit ? ob : 0xFFFFFFFFu);
+    if (obj) __stcs(obj + i, hit ? s.objects[leaf].desc_id : 0xFFFFFFFFu);
   }
+  if (kCount) flush_counts(c, cnt);
 }
 
+template <bool kCount>
 __global__ void __launch_bounds__(128) k_scene_any(SceneView s, const float* __restrict__ rays, uint64_t stride,
-                                                   uint64_t n, uint8_t* __restrict__ occ, uint32_t* err) {
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+                                                   uint64_t n, uint8_t* __restrict__ occ, unsigned long long* cnt,
+                                                   uint32_t* err) {
+  SceneCount c{0, 0, 0};
+  const uint64_t step = uint64_t(gridDim.x) * blockDim.x;
+  const uint64_t iters = (n + step - 1) / step;
+  for (uint64_t it = 0; it < iters; ++it) {
+    const uint64_t i = it * step + uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) continue;
     const F3 o = mk3(__ldcs(rays + i), __ldcs(rays + stride + i), __ldcs(rays + 2 * stride + i));
     const F3 d = mk3(__ldcs(rays + 3 * stride + i), __ldcs(rays + 4 * stride + i), __ldcs(rays + 5 * stride + i));
-    occ[i] = scene_any(s, o, d, __ldcs(rays + 6 * stride + i), __ldcs(rays + 7 * stride + i), err) ? 1 : 0;
+    occ[i] = scene_any_t<kCount>(s, o, d, __ldcs(rays + 6 * stride + i), __ldcs(rays + 7 * stride + i), err, &c) ? 1 : 0;
   }
+  if (kCount) flush_counts(c, cnt);
 }
 
 // ---- launchers -------------------------------------------------------------------------------
@@ -657,16 +685,21 @@ static unsigned grid_cap(uint64_t n, int threads, int sm_count, int per_sm) {
 }
 
 cudaError_t launch_scene_closest(const SceneView& s, const float* rays, uint64_t stride, uint64_t n, uint32_t* prim,
-                                 float* t, uint32_t* obj, uint32_t* err, int sm_count, cudaStream_t st) {
+                                 float* t, uint32_t* obj, unsigned long long* cnt, uint32_t* err, int sm_count,
+                                 cudaStream_t st) {
   if (n == 0) return cudaSuccess;
-  k_scene_closest<<<grid_cap(n, 128, sm_count, 32), 128, 0, st>>>(s, rays, stride, n, prim, t, obj, err);
+  const unsigned g = grid_cap(n, 128, sm_count, 32);
+  if (cnt) k_scene_closest<true><<<g, 128, 0, st>>>(s, rays, stride, n, prim, t, obj, cnt, err);
+  else k_scene_closest<false><<<g, 128, 0, st>>>(s, rays, stride, n, prim, t, obj, nullptr, err);
   return cudaGetLastError();
 }
 
 cudaError_t launch_scene_any(const SceneView& s, const float* rays, uint64_t stride, uint64_t n, uint8_t* occ,
-                             uint32_t* err, int sm_count, cudaStream_t st) {
+                             unsigned long long* cnt, uint32_t* err, int sm_count, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
-  k_scene_any<<<grid_cap(n, 128, sm_count, 32), 128, 0, st>>>(s, rays, stride, n, occ, err);
+  const unsigned g = grid_cap(n, 128, sm_count, 32);
+  if (cnt) k_scene_any<true><<<g, 128, 0, st>>>(s, rays, stride, n, occ, cnt, err);
+  else k_scene_any<false><<<g, 128, 0, st>>>(s, rays, stride, n, occ, nullptr, err);
   return cudaGetLastError();
 }
 

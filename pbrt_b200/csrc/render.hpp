@@ -113,9 +113,11 @@ cudaError_t train_batch(const WaveBuffers& w, const CacheWave& cw, uint32_t batc
                         unsigned long long seed, float max_l, float* rec, float* tgt, int sm_count, cudaStream_t st);
 cudaError_t scale_film(double* film, size_t n, double s, int sm_count, cudaStream_t st);
 
+// Scene-level ray casts; cnt (3 counters: nodes, boxes, objects) may be NULL.
 cudaError_t launch_scene_closest(const SceneView& s, const float* rays, uint64_t stride, uint64_t n, uint32_t* prim,
-                                 float* t, uint32_t* obj, uint32_t* err, int sm_count, cudaStream_t st);
+                                 float* t, uint32_t* obj, unsigned long long* cnt, uint32_t* err, int sm_count,
+                                 cudaStream_t st);
 cudaError_t launch_scene_any(const SceneView& s, const float* rays, uint64_t stride, uint64_t n, uint8_t* occ,
-                             uint32_t* err, int sm_count, cudaStream_t st);
+                             unsigned long long* cnt, uint32_t* err, int sm_count, cudaStream_t st);
 
 }  // namespace pbrt

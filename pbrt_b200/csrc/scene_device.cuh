@@ -1,14 +1,20 @@
-// scene_device.cuh — the scene on the GPU: objects, the top-level BVH over them, the
-// analytic shapes, and the interaction (shading record) of a hit.
+// scene_device.cuh — the scene on the GPU: placed objects ("leaves"), compounds, the
+// top-level BVH over the scene's primitives, the unbounded primitives, the analytic shapes,
+// and the interaction (shading record) of a hit.
 //
 // Semantics follow the reference operation for operation (FP32, no FMA):
-//   Scene::find_nearest + BVH::query      src/scene.rs:186-220, src/bvh.rs:153-230
-//   Scene::any_hit + BVH::query_p         src/scene.rs:157-168, src/bvh.rs:239-275
+//   Scene::find_nearest + BVH::query      src/scene.rs:186-249, src/bvh.rs:153-230
+//   Scene::any_hit + BVH::query_p         src/scene.rs:157-184, src/bvh.rs:239-275
 //   Transformed::intersect / intersect_p  src/objects/transformed.rs:27-38, 62-65
+//   Compound::intersect / intersect_p     src/objects/compound.rs:21-50
 //   Simple::intersect (first listed hit)  src/objects/simple.rs:28-41
 //   Sphere::intersect + details           src/shapes/sphere.rs:108-187
 //   Cylinder::intersect + details         src/shapes/cylinder.rs:28-110, 324-344
+//   Rectangle / Plane / AABox::intersect  src/shapes/rectangle.rs:25-60, plane.rs:19-45, aabox.rs:76-190
 //   TriangleMesh::intersect post-hit      src/shapes/triangle_mesh/triangle_mesh.rs:73-132, 219-258
+// A nested object tree is flattened on the host: each placed Simple is a leaf carrying the
+// chain of transforms above it (applied in turn, each renormalising the direction as
+// Ray::new does), and a Compound is a group of consecutive leaves.
 #pragma once
 
 #include <cfloat>
@@ -26,10 +32,14 @@ struct MeshShade {  // original vertices/indices, for the post-hit shading recor
 };
 
 struct SceneView {
-  const float4* top;        // top-level BVH nodes (GPU numbering, 2 float4 per node)
+  const float4* top;        // top-level BVH nodes (GPU numbering, 2 float4 per node); may be empty
   uint32_t top_node_count;
-  const uint32_t* order;    // leaf slot -> object index
-  const ObjRec* objects;
+  const uint32_t* order;    // leaf slot -> primitive (leaf index, or kGroupBit | group)
+  const uint32_t* unbounded;  // primitives kept out of the BVH, tested first
+  uint32_t unbounded_count;
+  const ObjRec* objects;    // leaves
+  const XfRec* xforms;      // transform chains beyond each leaf's first
+  const GroupRec* groups;   // compounds
   const MeshView* meshes;   // traversal views
   const MeshShade* shade;   // shading views
   const MatRec* materials;
@@ -41,7 +51,12 @@ struct SceneView {
 
 struct Isect {
   F3 p, n, wo, dpdu;
-  float d;
+  float d, u, v;
+};
+
+// Work counters of the scene-level queries (TraversalStats of Scene::intersect_instrumented).
+struct SceneCount {
+  uint32_t nodes, boxes, objects;
 };
 
 // ---- transforms (affine 3x4) -------------------------------------------------------------
@@ -123,61 +138,196 @@ PBRT_DEV bool cylinder_hit(float radius, float hh, const F3& o, const F3& d, flo
   return true;
 }
 
-// The object's local ray: transform_ray_to_local renormalises (transform.rs:98-103, ray.rs:10-18).
-PBRT_DEV void local_ray(const ObjRec& ob, const F3& o, const F3& d, F3& lo, F3& ld) {
-  if (ob.transformed) {
-    lo = xf_point(ob.to_local, o);
-    ld = normalize3(xf_dir(ob.to_local, d));
+// Rectangle::intersect: the y = 0 plane at d = (o.y * -1) / dir.y, within |x| <= hw, |z| <= hh
+PBRT_DEV bool rectangle_hit(float hw, float hh, const F3& o, const F3& d, float near, float far, float& t_out) {
+  if (d.y == 0.f) return false;
+  const float t = fdv(fm(o.y, -1.f), d.y);
+  if (t < near || t > far) return false;
+  const F3 p = add3(o, mul3(d, t));
+  if (fabsf(p.x) > hw || fabsf(p.z) > hh) return false;
+  t_out = t;
+  return true;
+}
+
+// Plane::intersect, its arithmetic as written: d = (o.y * -1) / (1 / dir.y)
+PBRT_DEV bool plane_hit(const F3& o, const F3& d, float near, float far, float& t_out) {
+  const float inv = frcp(d.y);
+  const float t = fdv(fm(o.y, -1.f), inv);
+  if (t < near || t > far) return false;
+  t_out = t;
+  return true;
+}
+
+// AABox::intersect over [-h, h] (min = 0 - h): the entry beyond near, else the exit before
+// far. face: 0..5 = X_NEG, X_POS, Y_NEG, Y_POS, Z_NEG, Z_POS.
+PBRT_DEV void aabox_axis(float o, float inv, float lo, float hi, int fneg, float& tmin, float& tmax, int& fmin,
+                         int& fmax) {
+  if (inv >= 0.f) {
+    tmin = fm(fs(lo, o), inv);
+    tmax = fm(fs(hi, o), inv);
+    fmin = fneg;
+    fmax = fneg + 1;
   } else {
-    lo = o;
-    ld = d;
+    tmin = fm(fs(hi, o), inv);
+    tmax = fm(fs(lo, o), inv);
+    fmin = fneg + 1;
+    fmax = fneg;
+  }
+}
+PBRT_DEV bool aabox_hit(const float* h, const F3& o, const F3& d, float near, float far, float& t_out, int& face) {
+  float tmin, tmax, tymin, tymax, tzmin, tzmax;
+  int fmin, fmax, fymin, fymax, fzmin, fzmax;
+  aabox_axis(o.x, frcp(d.x), fs(0.f, h[0]), h[0], 0, tmin, tmax, fmin, fmax);
+  aabox_axis(o.y, frcp(d.y), fs(0.f, h[1]), h[1], 2, tymin, tymax, fymin, fymax);
+  if ((tmin > tymax) || (tymin > tmax)) return false;
+  if (tymin > tmin) { tmin = tymin; fmin = fymin; }
+  if (tymax < tmax) { tmax = tymax; fmax = fymax; }
+  aabox_axis(o.z, frcp(d.z), fs(0.f, h[2]), h[2], 4, tzmin, tzmax, fzmin, fzmax);
+  if ((tmin > tzmax) || (tzmin > tmax)) return false;
+  if (tzmin > tmin) { tmin = tzmin; fmin = fzmin; }
+  if (tzmax < tmax) { tmax = tzmax; fmax = fzmax; }
+  if (tmax < near || tmin > far) return false;
+  if (tmin > near) { t_out = tmin; face = fmin; return true; }
+  if (tmax < far) { t_out = tmax; face = fmax; return true; }
+  return false;
+}
+
+// ---- leaves --------------------------------------------------------------------------------
+PBRT_DEV const float* leaf_to_local(const SceneView& s, const ObjRec& ob, uint32_t k) {
+  return k == 0 ? ob.to_local : s.xforms[ob.xf_rest + k - 1].to_local;
+}
+PBRT_DEV const float* leaf_to_world(const SceneView& s, const ObjRec& ob, uint32_t k) {
+  return k == 0 ? ob.to_world : s.xforms[ob.xf_rest + k - 1].to_world;
+}
+
+// The leaf's local ray: transform_ray_to_local at every level of its chain, outermost first;
+// each renormalises (transform.rs:98-103, ray.rs:10-18).
+PBRT_DEV void local_ray(const SceneView& s, const ObjRec& ob, const F3& o, const F3& d, F3& lo, F3& ld) {
+  lo = o;
+  ld = d;
+  for (uint32_t k = 0; k < ob.xf_count; ++k) {
+    const float* inv = leaf_to_local(s, ob, k);
+    lo = xf_point(inv, lo);
+    ld = normalize3(xf_dir(inv, ld));
   }
 }
 
-// Object::intersect distance within [near, far]; prim = triangle index (0 for analytic).
-PBRT_DEV bool object_closest(const SceneView& s, uint32_t oi, const F3& o, const F3& d, float near, float far,
-                             float& t, uint32_t& prim, uint32_t* err) {
-  const ObjRec& ob = s.objects[oi];
+// Object::intersect distance of one leaf within [near, far]; prim = triangle index, cylinder
+// piece or box face (0 for the other shapes).
+PBRT_DEV bool leaf_closest(const SceneView& s, uint32_t li, const F3& o, const F3& d, float near, float far,
+                           float& t, uint32_t& prim, uint32_t* err) {
+  const ObjRec& ob = s.objects[li];
   F3 lo, ld;
-  local_ray(ob, o, d, lo, ld);
-  if (ob.shape == kShapeMesh) {
-    const PRay r = prepare_ray(lo, ld);
-    TraceCounters c;
-    const uint32_t id = mesh_closest<false>(s.meshes[ob.mesh], r, near, far, &t, &c, err);
-    prim = id;
-    return id != 0xFFFFFFFFu;
-  }
+  local_ray(s, ob, o, d, lo, ld);
   prim = 0;
-  if (ob.shape == kShapeSphere) return sphere_hit(ob.radius, lo, ld, near, far, t);
-  int piece = 0;
-  const bool hit = cylinder_hit(ob.radius, ob.half_height, lo, ld, near, far, t, piece);
-  prim = uint32_t(piece);  // cylinders report which piece was hit: 0 wall, 1 bottom cap, 2 top cap
-  return hit;
+  switch (ob.shape) {
+    case kShapeMesh: {
+      const PRay r = prepare_ray(lo, ld);
+      TraceCounters c;
+      const uint32_t id = mesh_closest<false>(s.meshes[ob.mesh], r, near, far, &t, &c, err);
+      prim = id;
+      return id != 0xFFFFFFFFu;
+    }
+    case kShapeSphere: return sphere_hit(ob.p[0], lo, ld, near, far, t);
+    case kShapeCylinder: {
+      int piece = 0;
+      const bool hit = cylinder_hit(ob.p[0], ob.p[1], lo, ld, near, far, t, piece);
+      prim = uint32_t(piece);
+      return hit;
+    }
+    case kShapeRectangle: return rectangle_hit(ob.p[0], ob.p[1], lo, ld, near, far, t);
+    case kShapeAABox: {
+      int face = 0;
+      const bool hit = aabox_hit(ob.p, lo, ld, near, far, t, face);
+      prim = uint32_t(face);
+      return hit;
+    }
+    default: return plane_hit(lo, ld, near, far, t);
+  }
 }
 
-PBRT_DEV bool object_any(const SceneView& s, uint32_t oi, const F3& o, const F3& d, float near, float far,
-                         uint32_t* err) {
-  const ObjRec& ob = s.objects[oi];
+PBRT_DEV bool leaf_any(const SceneView& s, uint32_t li, const F3& o, const F3& d, float near, float far,
+                       uint32_t* err) {
+  const ObjRec& ob = s.objects[li];
   F3 lo, ld;
-  local_ray(ob, o, d, lo, ld);
-  if (ob.shape == kShapeMesh) return mesh_any(s.meshes[ob.mesh], prepare_ray(lo, ld), near, far, err);
+  local_ray(s, ob, o, d, lo, ld);
   float t;
-  if (ob.shape == kShapeSphere) return sphere_hit(ob.radius, lo, ld, near, far, t);
-  int piece;
-  return cylinder_hit(ob.radius, ob.half_height, lo, ld, near, far, t, piece);
+  int k;
+  switch (ob.shape) {
+    case kShapeMesh: return mesh_any(s.meshes[ob.mesh], prepare_ray(lo, ld), near, far, err);
+    case kShapeSphere: return sphere_hit(ob.p[0], lo, ld, near, far, t);
+    case kShapeCylinder: return cylinder_hit(ob.p[0], ob.p[1], lo, ld, near, far, t, k);
+    case kShapeRectangle: return rectangle_hit(ob.p[0], ob.p[1], lo, ld, near, far, t);
+    case kShapeAABox: return aabox_hit(ob.p, lo, ld, near, far, t, k);
+    default: return plane_hit(lo, ld, near, far, t);
+  }
 }
 
-// Scene::find_nearest: the top-level query narrows its interval to every adopted hit and
-// offers each object [near, min_t]; a candidate is adopted only when strictly nearer.
-PBRT_DEV bool scene_closest(const SceneView& s, const F3& o, const F3& d, float near, float far, float& t_out,
-                            uint32_t& obj_out, uint32_t& prim_out, uint32_t* err) {
-  const PRay r = prepare_ray(o, d);
+// ---- primitives (a leaf or a compound) -----------------------------------------------------
+// A compound asks every member over the same [near, far] and keeps the strictly nearest hit,
+// the earlier member on a tie (compound.rs:21-38).
+PBRT_DEV bool prim_closest(const SceneView& s, uint32_t ref, const F3& o, const F3& d, float near, float far,
+                           float& t, uint32_t& leaf, uint32_t& prim, uint32_t* err) {
+  if (!(ref & kGroupBit)) {
+    leaf = ref;
+    return leaf_closest(s, ref, o, d, near, far, t, prim, err);
+  }
+  const GroupRec g = s.groups[ref & ~kGroupBit];
+  bool have = false;
+  for (uint32_t k = 0; k < g.count; ++k) {
+    float tk;
+    uint32_t pk;
+    if (leaf_closest(s, g.first + k, o, d, near, far, tk, pk, err) && (!have || tk < t)) {
+      have = true;
+      t = tk;
+      leaf = g.first + k;
+      prim = pk;
+    }
+  }
+  return have;
+}
+
+PBRT_DEV bool prim_any(const SceneView& s, uint32_t ref, const F3& o, const F3& d, float near, float far,
+                       uint32_t* err) {
+  if (!(ref & kGroupBit)) return leaf_any(s, ref, o, d, near, far, err);
+  const GroupRec g = s.groups[ref & ~kGroupBit];
+  for (uint32_t k = 0; k < g.count; ++k)
+    if (leaf_any(s, g.first + k, o, d, near, far, err)) return true;  // compound.rs:47-49
+  return false;
+}
+
+// Scene::find_nearest: the unbounded primitives first, each over [near, far]; then the
+// top-level query over [near, nearest so far], narrowing to every adopted hit and offering
+// each primitive [near, min_t]; a candidate is adopted only when strictly nearer.
+template <bool kCount>
+PBRT_DEV bool scene_closest_t(const SceneView& s, const F3& o, const F3& d, float near, float far, float& t_out,
+                              uint32_t& leaf_out, uint32_t& prim_out, uint32_t* err, SceneCount* cnt) {
   float min_t = far;
   bool have = false;
+  for (uint32_t k = 0; k < s.unbounded_count; ++k) {  // nearest_among + closer (scene.rs:222-249)
+    if (kCount) cnt->objects++;
+    float t;
+    uint32_t leaf, prim;
+    if (prim_closest(s, __ldg(&s.unbounded[k]), o, d, near, far, t, leaf, prim, err) && (!have || t < min_t)) {
+      have = true;
+      min_t = t;
+      leaf_out = leaf;
+      prim_out = prim;
+    }
+  }
+  if (s.top_node_count == 0) {
+    if (have) t_out = min_t;
+    return have;
+  }
+  const PRay r = prepare_ray(o, d);
   const float4 rlo = __ldg(&s.top[0]);
   const float4 rhi = __ldg(&s.top[1]);
   float entry;
-  if (!box_hit(r, rlo, rhi, near, min_t, entry)) return false;
+  if (kCount) cnt->boxes++;
+  if (!box_hit(r, rlo, rhi, near, min_t, entry)) {
+    if (have) t_out = min_t;
+    return have;
+  }
   uint32_t stk_lf[kTraceStack], stk_cnt[kTraceStack];
   float stk_e[kTraceStack];
   int sp = 0;
@@ -191,15 +341,17 @@ PBRT_DEV bool scene_closest(const SceneView& s, const F3& o, const F3& d, float 
     }
     bool pop = true;
     if (cur_e < min_t) {
+      if (kCount) cnt->nodes++;
       if (count > 0) {
         for (uint32_t k = lf; k < lf + count; ++k) {
-          const uint32_t oi = __ldg(&s.order[k]);
+          if (kCount) cnt->objects++;
+          const uint32_t ref = __ldg(&s.order[k]);
           float t;
-          uint32_t prim;
-          if (object_closest(s, oi, o, d, near, min_t, t, prim, err) && (!have || t < min_t)) {
+          uint32_t leaf, prim;
+          if (prim_closest(s, ref, o, d, near, min_t, t, leaf, prim, err) && (!have || t < min_t)) {
             have = true;
             min_t = t;
-            obj_out = oi;
+            leaf_out = leaf;
             prim_out = prim;
           }
         }
@@ -207,6 +359,7 @@ PBRT_DEV bool scene_closest(const SceneView& s, const F3& o, const F3& d, float 
         const float4 l0 = __ldg(&s.top[2 * lf]), l1 = __ldg(&s.top[2 * lf + 1]);
         const float4 r0 = __ldg(&s.top[2 * lf + 2]), r1 = __ldg(&s.top[2 * lf + 3]);
         float dl, dr;
+        if (kCount) cnt->boxes += 2;
         const bool hl = box_hit(r, l0, l1, near, min_t, dl);
         const bool hr = box_hit(r, r0, r1, near, min_t, dr);
         const bool swap = hl && hr && dr < dl;
@@ -242,8 +395,21 @@ PBRT_DEV bool scene_closest(const SceneView& s, const F3& o, const F3& d, float 
   return have;
 }
 
-// Scene::any_hit: unordered, the box tested at pop, right pushed before left (bvh.rs:269-270).
-PBRT_DEV bool scene_any(const SceneView& s, const F3& o, const F3& d, float near, float far, uint32_t* err) {
+PBRT_DEV bool scene_closest(const SceneView& s, const F3& o, const F3& d, float near, float far, float& t_out,
+                            uint32_t& leaf_out, uint32_t& prim_out, uint32_t* err) {
+  return scene_closest_t<false>(s, o, d, near, far, t_out, leaf_out, prim_out, err, nullptr);
+}
+
+// Scene::any_hit: the unbounded primitives first; then unordered, the box tested at pop,
+// right pushed before left (bvh.rs:269-270).
+template <bool kCount>
+PBRT_DEV bool scene_any_t(const SceneView& s, const F3& o, const F3& d, float near, float far, uint32_t* err,
+                          SceneCount* cnt) {
+  for (uint32_t k = 0; k < s.unbounded_count; ++k) {  // any_blocks (scene.rs:170-184)
+    if (kCount) cnt->objects++;
+    if (prim_any(s, __ldg(&s.unbounded[k]), o, d, near, far, err)) return true;
+  }
+  if (s.top_node_count == 0) return false;
   const PRay r = prepare_ray(o, d);
   uint32_t stk[kTraceStack];
   int sp = 0;
@@ -257,11 +423,15 @@ PBRT_DEV bool scene_any(const SceneView& s, const F3& o, const F3& d, float near
     const uint32_t ni = stk[--sp];
     const float4 lo = __ldg(&s.top[2 * ni]), hi = __ldg(&s.top[2 * ni + 1]);
     float e;
+    if (kCount) cnt->boxes++;
     if (!box_hit(r, lo, hi, near, far, e)) continue;
+    if (kCount) cnt->nodes++;
     const uint32_t lf = __float_as_uint(lo.w), count = __float_as_uint(hi.w);
     if (count > 0) {
-      for (uint32_t k = lf; k < lf + count; ++k)
-        if (object_any(s, __ldg(&s.order[k]), o, d, near, far, err)) return true;
+      for (uint32_t k = lf; k < lf + count; ++k) {
+        if (kCount) cnt->objects++;
+        if (prim_any(s, __ldg(&s.order[k]), o, d, near, far, err)) return true;
+      }
     } else {
       if (sp + 2 > kTraceStack) {
         atomicOr(err, kErrStack);
@@ -274,14 +444,16 @@ PBRT_DEV bool scene_any(const SceneView& s, const F3& o, const F3& d, float near
   return false;
 }
 
+PBRT_DEV bool scene_any(const SceneView& s, const F3& o, const F3& d, float near, float far, uint32_t* err) {
+  return scene_any_t<false>(s, o, d, near, far, err, nullptr);
+}
+
 // ---- the interaction of an adopted hit -----------------------------------------------------
 PBRT_DEV F3 vtx(const MeshShade& m, uint32_t i) { return mk3(m.v[3 * i], m.v[3 * i + 1], m.v[3 * i + 2]); }
 
-// World-space shading record of object `oi` hit at distance t (recomputed from the same
-// local ray and the same arithmetic as the hit itself).
 // The material of a hit: the triangle's own when its mesh carries per-face materials.
-PBRT_DEV uint32_t material_index(const SceneView& s, uint32_t oi, uint32_t prim) {
-  const ObjRec& ob = s.objects[oi];
+PBRT_DEV uint32_t material_index(const SceneView& s, uint32_t li, uint32_t prim) {
+  const ObjRec& ob = s.objects[li];
   if (ob.shape == kShapeMesh) {
     const uint32_t* fm = s.shade[ob.mesh].fmat;
     if (fm) return fm[prim];
@@ -289,55 +461,135 @@ PBRT_DEV uint32_t material_index(const SceneView& s, uint32_t oi, uint32_t prim)
   return ob.material;
 }
 
-PBRT_DEV Isect interaction(const SceneView& s, uint32_t oi, uint32_t prim, const F3& o, const F3& d, float t) {
-  const ObjRec& ob = s.objects[oi];
+// AABox face frames (aabox.rs:29-63): normal, du, dv
+static __constant__ float kBoxFace[6][9] = {
+    {-1.f, 0.f, 0.f, 0.f, 0.f, -1.f, 0.f, 1.f, 0.f}, {1.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f, 1.f, 0.f},
+    {0.f, -1.f, 0.f, -1.f, 0.f, 0.f, 0.f, 0.f, 1.f}, {0.f, 1.f, 0.f, 1.f, 0.f, 0.f, 0.f, 0.f, 1.f},
+    {0.f, 0.f, -1.f, 0.f, -1.f, 0.f, 1.f, 0.f, 0.f}, {0.f, 0.f, 1.f, 0.f, 1.f, 0.f, 1.f, 0.f, 0.f}};
+
+// World-space shading record of leaf `li` hit at distance t (recomputed from the same local
+// ray and the same arithmetic as the hit itself). With uv = false the texture coordinates of
+// mesh and sphere hits are left 0 (only textured materials read them).
+PBRT_DEV Isect interaction(const SceneView& s, uint32_t li, uint32_t prim, const F3& o, const F3& d, float t,
+                           bool uv = false) {
+  const ObjRec& ob = s.objects[li];
   F3 lo, ld;
-  local_ray(ob, o, d, lo, ld);
+  local_ray(s, ob, o, d, lo, ld);
   Isect h;
   h.d = t;
+  h.u = 0.f;
+  h.v = 0.f;
+  h.wo = mul3(ld, -1.f);
   F3 dpdv;
-  if (ob.shape == kShapeMesh) {
-    const MeshShade& m = s.shade[ob.mesh];
-    const F3 p0 = vtx(m, m.idx[3 * prim]), p1 = vtx(m, m.idx[3 * prim + 1]), p2 = vtx(m, m.idx[3 * prim + 2]);
-    h.p = add3(lo, mul3(ld, t));
-    // compute_texture_derivatives with the default uvs (0,0), (1,0), (1,1)
-    const float d02x = fs(0.f, 1.f), d02y = fs(0.f, 1.f), d12x = fs(1.f, 1.f), d12y = fs(0.f, 1.f);
-    const F3 dp02 = sub3(p0, p2), dp12 = sub3(p1, p2);
-    const float det = fs(fm(d12x, d02y), fm(d12y, d02x));
-    const float inv = frcp(det);
-    h.dpdu = mul3(sub3(mul3(dp12, d02y), mul3(dp02, d12y)), inv);
-    dpdv = mul3(sub3(mul3(dp02, d12x), mul3(dp12, d02x)), inv);
-    h.n = normalize3(cross3(dpdv, h.dpdu));
-    h.wo = mul3(ld, -1.f);
-  } else if (ob.shape == kShapeSphere) {
-    const F3 hit = add3(lo, mul3(ld, t));
-    h.p = hit;
-    h.n = normalize3(hit);
-    h.dpdu = mul3(mk3(-hit.y, hit.x, 0.f), fm(2.f, 3.14159265358979323846f));
-    dpdv = mk3(0.f, 0.f, 0.f);  // not used by the shading frame
-    h.wo = mul3(ld, -1.f);
-  } else {
-    const F3 p = add3(lo, mul3(ld, t));
-    h.p = p;
-    h.wo = mul3(ld, -1.f);
-    dpdv = mk3(0.f, 1.f, 0.f);
-    const uint32_t piece = prim;  // object_closest reports the piece in prim
-    if (piece == 0) {
-      h.n = normalize3(mk3(p.x, 0.f, p.z));
-      h.dpdu = mul3(mk3(-p.z, 0.f, p.x), fm(2.f, 3.14159265358979323846f));
-    } else {
-      const bool top = piece == 2;
-      h.n = mk3(0.f, top ? 1.f : -1.f, 0.f);
-      h.dpdu = mk3(top ? 1.f : -1.f, 0.f, 0.f);
+  const float kTwoPi = fm(2.f, 3.14159265358979323846f);
+  switch (ob.shape) {
+    case kShapeMesh: {
+      const MeshShade& m = s.shade[ob.mesh];
+      const F3 p0 = vtx(m, m.idx[3 * prim]), p1 = vtx(m, m.idx[3 * prim + 1]), p2 = vtx(m, m.idx[3 * prim + 2]);
+      h.p = add3(lo, mul3(ld, t));
+      // compute_texture_derivatives with the default uvs (0,0), (1,0), (1,1)
+      const float d02x = fs(0.f, 1.f), d02y = fs(0.f, 1.f), d12x = fs(1.f, 1.f), d12y = fs(0.f, 1.f);
+      const F3 dp02 = sub3(p0, p2), dp12 = sub3(p1, p2);
+      const float det = fs(fm(d12x, d02y), fm(d12y, d02x));
+      const float inv = frcp(det);
+      h.dpdu = mul3(sub3(mul3(dp12, d02y), mul3(dp02, d12y)), inv);
+      dpdv = mul3(sub3(mul3(dp02, d12x), mul3(dp12, d02x)), inv);
+      h.n = normalize3(cross3(dpdv, h.dpdu));
+      if (uv) {  // interpolate_texture_coords (triangle_mesh.rs:219-224) from Möller–Trumbore's u, v
+        const F3 e1 = sub3(p1, p0), e2 = sub3(p2, p0);
+        const F3 pv = cross3(ld, e2);
+        const float idet = frcp(dot3(e1, pv));
+        const F3 sv = sub3(lo, p0);
+        const float bu = fm(idet, dot3(sv, pv));
+        const float bv = fm(idet, dot3(ld, cross3(sv, e1)));
+        const float bw = fs(fs(1.f, bu), bv);
+        h.u = fa(fa(fm(bw, 0.f), fm(bu, 1.f)), fm(bv, 1.f));
+        h.v = fa(fa(fm(bw, 0.f), fm(bu, 0.f)), fm(bv, 1.f));
+      }
+      break;
+    }
+    case kShapeSphere: {
+      const F3 hit = add3(lo, mul3(ld, t));
+      h.p = hit;
+      h.n = normalize3(hit);
+      h.dpdu = mul3(mk3(-hit.y, hit.x, 0.f), kTwoPi);
+      dpdv = mk3(0.f, 0.f, 0.f);  // not used by the shading frame
+      if (uv) {  // compute_intersection_details (sphere.rs:152-172)
+        float phi = atan2f(hit.y, hit.x);
+        if (phi < 0.f) phi = fa(phi, kTwoPi);
+        h.u = fdv(phi, kTwoPi);
+        const float theta = acosf(fminf(fmaxf(fdv(hit.z, ob.p[0]), -1.f), 1.f));
+        h.v = fdv(theta, 3.14159265358979323846f);
+      }
+      break;
+    }
+    case kShapeCylinder: {
+      const F3 p = add3(lo, mul3(ld, t));
+      h.p = p;
+      dpdv = mk3(0.f, 1.f, 0.f);
+      const uint32_t piece = prim;  // leaf_closest reports the piece in prim
+      if (piece == 0) {
+        h.n = normalize3(mk3(p.x, 0.f, p.z));
+        h.dpdu = mul3(mk3(-p.z, 0.f, p.x), kTwoPi);
+        if (uv) {
+          float phi = atan2f(p.z, p.x);
+          if (phi < 0.f) phi = fa(phi, kTwoPi);
+          h.u = fdv(phi, kTwoPi);
+          h.v = p.y;
+        }
+      } else {
+        const bool top = piece == 2;
+        h.n = mk3(0.f, top ? 1.f : -1.f, 0.f);
+        h.dpdu = mk3(top ? 1.f : -1.f, 0.f, 0.f);
+        h.u = p.x;
+        h.v = p.z;
+      }
+      break;
+    }
+    case kShapeAABox: {
+      const float* f = kBoxFace[prim < 6 ? prim : 0];
+      const F3 p = add3(lo, mul3(ld, t));
+      h.p = p;
+      h.n = mk3(f[0], f[1], f[2]);
+      h.dpdu = mk3(f[3], f[4], f[5]);
+      dpdv = mk3(f[6], f[7], f[8]);
+      h.u = dot3(p, h.dpdu);
+      h.v = dot3(p, dpdv);
+      break;
+    }
+    default: {  // rectangle, plane: p on y = 0, n = +y, u = p.x, v = p.z
+      F3 p = add3(lo, mul3(ld, t));
+      p.y = 0.f;
+      h.p = p;
+      h.n = mk3(0.f, 1.f, 0.f);
+      h.dpdu = mk3(1.f, 0.f, 0.f);
+      dpdv = mk3(0.f, 0.f, 1.f);
+      h.u = p.x;
+      h.v = p.z;
+      break;
     }
   }
-  if (ob.transformed) {  // transform_interaction_to_world (transform.rs:105-116)
-    h.n = xf_normal(ob.to_local, h.n);
-    h.p = xf_point(ob.to_world, h.p);
-    h.wo = xf_dir(ob.to_world, h.wo);
-    h.dpdu = xf_dir(ob.to_world, h.dpdu);
+  // transform_interaction_to_world (transform.rs:105-116), innermost level first
+  for (uint32_t k = ob.xf_count; k-- > 0;) {
+    const float* w = leaf_to_world(s, ob, k);
+    h.n = xf_normal(leaf_to_local(s, ob, k), h.n);
+    h.p = xf_point(w, h.p);
+    h.wo = xf_dir(w, h.wo);
+    h.dpdu = xf_dir(w, h.dpdu);
   }
+  (void)dpdv;
   return h;
+}
+
+// Texture::shade at a hit: PlainColor, or CheckerBoard::shade (checker_board.rs:17-28) on the
+// record's u, v (`%` is fmod, exact; signum(+-0) = +-1).
+PBRT_DEV F3 texel(const MatRec& m, const Isect& it) {
+  if (m.texture == kTexColor) return mk3(m.color[0], m.color[1], m.color[2]);
+  const float su = fmodf(fm(fabsf(it.u), m.scale), 1.f);
+  const float sv = fmodf(fm(fabsf(it.v), m.scale), 1.f);
+  const bool use_color = (su < 0.5f && sv < 0.5f) || (su >= 0.5f && sv >= 0.5f);
+  const bool positive = !isnan(it.u) && !isnan(it.v) && fm(copysignf(1.f, it.u), copysignf(1.f, it.v)) >= 0.f;
+  return (use_color != positive) ? mk3(m.color[0], m.color[1], m.color[2]) : mk3(m.color2[0], m.color2[1], m.color2[2]);
 }
 
 // Shading frame: ss = normalize(dpdu), ts = n x ss, ns = n (intersectable.rs:92-144)

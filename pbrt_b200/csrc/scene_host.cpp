@@ -199,12 +199,211 @@ class TopBuilder {
 
 }  // namespace
 
+namespace {
+
+// aabound.rs:68-75: an empty box counts as bounded; otherwise every extent must be finite
+bool is_bounded(const Box3& b) {
+  for (int a = 0; a < 3; ++a)
+    if (b.lo[a] > b.hi[a]) return true;
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(b.hi[a] - b.lo[a])) return false;
+  return true;
+}
+
+// AABoundingBox::transform (aabound.rs:437-468)
+Box3 transform_box(const Box3& b, const float* to_world) {
+  Box3 t;
+  if (!is_bounded(b)) {
+    for (int a = 0; a < 3; ++a) { t.lo[a] = -INFINITY; t.hi[a] = INFINITY; }
+    return t;
+  }
+  const float* lo = b.lo;
+  const float* hi = b.hi;
+  const V3f c[8] = {{lo[0], lo[1], lo[2]}, {lo[0], lo[1], hi[2]}, {lo[0], hi[1], lo[2]}, {lo[0], hi[1], hi[2]},
+                    {hi[0], hi[1], hi[2]}, {hi[0], hi[1], lo[2]}, {hi[0], lo[1], hi[2]}, {hi[0], lo[1], lo[2]}};
+  t.set_empty();
+  for (const V3f& p0 : c) {
+    const V3f p = xf_point(to_world, p0);
+    t.lo[0] = std::fmin(t.lo[0], p.x); t.lo[1] = std::fmin(t.lo[1], p.y); t.lo[2] = std::fmin(t.lo[2], p.z);
+    t.hi[0] = std::fmax(t.hi[0], p.x); t.hi[1] = std::fmax(t.hi[1], p.y); t.hi[2] = std::fmax(t.hi[2], p.z);
+  }
+  return t;
+}
+
+struct Xf {
+  const float* to_world;
+  const float* to_local;
+};
+
+// Flattens the object tree: every placed Simple becomes a leaf with its chain of transforms.
+class Flattener {
+ public:
+  Flattener(const pbrt_scene_desc& d, const std::vector<Box3>& shape_boxes, FlatScene* out)
+      : d_(d), shape_boxes_(shape_boxes), out_(out) {}
+
+  // Acyclic, in range, of known kinds.
+  bool check_tree(std::string* err) {
+    if (!d_.nodes) return true;
+    for (uint32_t i = 0; i < d_.node_count; ++i) {
+      const pbrt_node_desc& n = d_.nodes[i];
+      if (n.kind == PBRT_NODE_SIMPLE) {
+        if (n.object >= d_.object_count) { *err = "node " + std::to_string(i) + ": bad object"; return false; }
+      } else if (n.kind == PBRT_NODE_TRANSFORMED || n.kind == PBRT_NODE_COMPOUND) {
+        const uint64_t cnt = n.kind == PBRT_NODE_TRANSFORMED ? 1 : n.count;
+        if (uint64_t(n.first) + cnt > d_.child_count || (cnt && !d_.node_children)) {
+          *err = "node " + std::to_string(i) + ": children out of range";
+          return false;
+        }
+        for (uint64_t k = 0; k < cnt; ++k)
+          if (d_.node_children[n.first + k] >= d_.node_count) {
+            *err = "node " + std::to_string(i) + ": bad child";
+            return false;
+          }
+      } else {
+        *err = "node " + std::to_string(i) + ": unknown kind";
+        return false;
+      }
+    }
+    if (d_.root_count && !d_.roots) { *err = "roots is NULL"; return false; }
+    for (uint32_t r = 0; r < d_.root_count; ++r)
+      if (d_.roots[r] >= d_.node_count) { *err = "root " + std::to_string(r) + ": bad node"; return false; }
+    std::vector<uint8_t> state(d_.node_count, 0);
+    std::vector<std::pair<uint32_t, uint32_t>> stack;  // node, next child
+    for (uint32_t r = 0; r < d_.root_count; ++r) {
+      if (state[d_.roots[r]] == 2) continue;
+      stack.push_back({d_.roots[r], 0});
+      state[d_.roots[r]] = 1;
+      while (!stack.empty()) {
+        auto& top = stack.back();
+        const pbrt_node_desc& n = d_.nodes[top.first];
+        const uint32_t cnt = n.kind == PBRT_NODE_TRANSFORMED ? 1u : (n.kind == PBRT_NODE_COMPOUND ? n.count : 0u);
+        if (top.second == cnt) {
+          state[top.first] = 2;
+          stack.pop_back();
+          continue;
+        }
+        const uint32_t c = d_.node_children[n.first + top.second++];
+        if (state[c] == 1) { *err = "the object tree has a cycle"; return false; }
+        if (state[c] == 0) {
+          state[c] = 1;
+          stack.push_back({c, 0});
+        }
+      }
+    }
+    return true;
+  }
+
+  // The scene's primitives in order: (reference, box).
+  bool run(std::vector<uint32_t>* refs, std::vector<Box3>* boxes, std::vector<uint8_t>* grouped, std::string* err) {
+    grouped_ = grouped;
+    const uint32_t n = d_.nodes ? d_.root_count : d_.object_count;
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t first = uint32_t(out_->objects.size());
+      std::vector<Xf> chain;
+      Box3 box;
+      if (d_.nodes) {
+        if (!node(d_.roots[i], &chain, 0, err)) return false;
+        box = node_box(d_.roots[i]);
+      } else {
+        if (!leaf(i, &chain, err)) return false;
+        box = object_box(i);
+      }
+      const uint32_t count = uint32_t(out_->objects.size()) - first;
+      if (count == 1) {
+        refs->push_back(first);
+      } else {
+        refs->push_back(kGroupBit | uint32_t(out_->groups.size()));
+        out_->groups.push_back(GroupRec{first, count});
+        for (uint32_t k = first; k < first + count; ++k) (*grouped_)[k] = 1;
+      }
+      boxes->push_back(box);
+    }
+    return true;
+  }
+
+ private:
+  Box3 object_box(uint32_t oi) const {
+    const pbrt_object_desc& o = d_.objects[oi];
+    return o.transformed ? transform_box(shape_boxes_[oi], o.to_world) : shape_boxes_[oi];
+  }
+
+  // get_bounding_box of a node (transformed.rs:70-74, compound.rs:57-64)
+  Box3 node_box(uint32_t ni) const {
+    const pbrt_node_desc& n = d_.nodes[ni];
+    if (n.kind == PBRT_NODE_SIMPLE) return object_box(n.object);
+    if (n.kind == PBRT_NODE_TRANSFORMED) return transform_box(node_box(d_.node_children[n.first]), n.to_world);
+    Box3 u;
+    u.set_empty();
+    for (uint32_t k = 0; k < n.count; ++k) u.grow(node_box(d_.node_children[n.first + k]));
+    return u;
+  }
+
+  bool node(uint32_t ni, std::vector<Xf>* chain, int depth, std::string* err) {
+    if (depth > 64) { *err = "the object tree is deeper than 64 levels"; return false; }
+    const pbrt_node_desc& n = d_.nodes[ni];
+    if (n.kind == PBRT_NODE_SIMPLE) return leaf(n.object, chain, err);
+    if (n.kind == PBRT_NODE_TRANSFORMED) {
+      chain->push_back(Xf{n.to_world, n.to_local});
+      const bool ok = node(d_.node_children[n.first], chain, depth + 1, err);
+      chain->pop_back();
+      return ok;
+    }
+    for (uint32_t k = 0; k < n.count; ++k)
+      if (!node(d_.node_children[n.first + k], chain, depth + 1, err)) return false;
+    return true;
+  }
+
+  bool leaf(uint32_t oi, std::vector<Xf>* chain, std::string* err) {
+    const pbrt_object_desc& o = d_.objects[oi];
+    if (out_->objects.size() >= (1u << 26)) { *err = "the object tree places more than 2^26 objects"; return false; }
+    std::vector<Xf> c = *chain;
+    if (o.transformed) c.push_back(Xf{o.to_world, o.to_local});
+    ObjRec r{};
+    r.shape = o.shape;
+    r.mesh = o.mesh;
+    r.material = o.material;
+    r.desc_id = oi;
+    r.xf_count = uint32_t(c.size());
+    switch (o.shape) {
+      case PBRT_SHAPE_SPHERE: r.p[0] = o.radius; break;
+      case PBRT_SHAPE_CYLINDER: r.p[0] = o.radius; r.p[1] = o.height / 2.0f; break;  // Cylinder::new
+      case PBRT_SHAPE_RECTANGLE: r.p[0] = o.radius / 2.0f; r.p[1] = o.height / 2.0f; break;  // Rectangle::new
+      case PBRT_SHAPE_AABOX:
+        for (int a = 0; a < 3; ++a) r.p[a] = o.extent[a] * 0.5f;  // AABox::new
+        break;
+      default: break;
+    }
+    if (!c.empty()) {
+      std::memcpy(r.to_world, c[0].to_world, sizeof(r.to_world));
+      std::memcpy(r.to_local, c[0].to_local, sizeof(r.to_local));
+    }
+    r.xf_rest = uint32_t(out_->xforms.size());
+    for (size_t k = 1; k < c.size(); ++k) {
+      XfRec x;
+      std::memcpy(x.to_world, c[k].to_world, sizeof(x.to_world));
+      std::memcpy(x.to_local, c[k].to_local, sizeof(x.to_local));
+      out_->xforms.push_back(x);
+    }
+    out_->objects.push_back(r);
+    grouped_->push_back(0);
+    return true;
+  }
+
+  const pbrt_scene_desc& d_;
+  const std::vector<Box3>& shape_boxes_;
+  FlatScene* out_;
+  std::vector<uint8_t>* grouped_ = nullptr;
+};
+
+}  // namespace
+
 bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err) {
   if (d.object_count == 0) { *err = "a scene needs at least one object"; return false; }
   if (!d.objects) { *err = "objects is NULL"; return false; }
   if (d.mesh_count && !d.meshes) { *err = "meshes is NULL"; return false; }
   if (d.material_count == 0 || !d.materials) { *err = "a scene needs at least one material"; return false; }
   if (d.light_count && !d.lights) { *err = "lights is NULL"; return false; }
+  if (d.nodes && d.root_count == 0) { *err = "a scene with an object tree needs at least one root"; return false; }
   MeshBuildParams bp;
   bp.bins = d.bvh_bins ? int(d.bvh_bins) : 8;
   bp.max_leaf = d.bvh_max_leaf ? d.bvh_max_leaf : 1;
@@ -235,69 +434,111 @@ bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err) {
   for (uint32_t i = 0; i < d.material_count; ++i) {
     const pbrt_material_desc& m = d.materials[i];
     if (m.kind > PBRT_MAT_DIFFUSE_LIGHT) { *err = "material " + std::to_string(i) + ": unknown kind"; return false; }
+    if (m.texture > PBRT_TEXTURE_CHECKERBOARD) {
+      *err = "material " + std::to_string(i) + ": unknown texture";
+      return false;
+    }
     MatRec r{};
     r.kind = m.kind;
+    r.texture = m.texture;
     r.fuzz = m.fuzz;
     r.ior = m.ior;
-    for (int c = 0; c < 3; ++c) r.color[c] = m.color[c];
+    for (int c = 0; c < 3; ++c) {
+      r.color[c] = m.color[c];
+      r.color2[c] = m.color2[c];
+    }
+    r.scale = m.scale;
     out->materials.push_back(r);
     if (m.kind == PBRT_MAT_DIFFUSE_LIGHT)
-      for (int c = 0; c < 3; ++c) out->max_radiance = std::max(out->max_radiance, m.color[c]);
+      for (int c = 0; c < 3; ++c) {
+        out->max_radiance = std::max(out->max_radiance, m.color[c]);
+        if (m.texture == PBRT_TEXTURE_CHECKERBOARD) out->max_radiance = std::max(out->max_radiance, m.color2[c]);
+      }
     if (m.kind == PBRT_MAT_DIELECTRIC) out->has_dielectric = true;
   }
 
-  std::vector<Box3> boxes(d.object_count);
+  // every object's shape box, before any transform
+  std::vector<Box3> shape_boxes(d.object_count);
   for (uint32_t i = 0; i < d.object_count; ++i) {
     const pbrt_object_desc& o = d.objects[i];
-    ObjRec r{};
-    r.shape = o.shape;
-    r.mesh = o.mesh;
-    r.material = o.material;
-    r.transformed = o.transformed ? 1u : 0u;
-    r.radius = o.radius;
-    r.half_height = o.height / 2.0f;  // Cylinder::new (cylinder.rs:12-19)
-    std::memcpy(r.to_world, o.to_world, sizeof(r.to_world));
-    std::memcpy(r.to_local, o.to_local, sizeof(r.to_local));
-    if (o.material >= d.material_count) { *err = "object " + std::to_string(i) + ": bad material"; return false; }
-    Box3 b;
-    if (o.shape == PBRT_SHAPE_MESH) {
-      if (o.mesh >= d.mesh_count) { *err = "object " + std::to_string(i) + ": bad mesh"; return false; }
-      const FlatMesh& fm = out->meshes[o.mesh];
-      for (int a = 0; a < 3; ++a) { b.lo[a] = fm.bounds_min[a]; b.hi[a] = fm.bounds_max[a]; }
-    } else if (o.shape == PBRT_SHAPE_SPHERE) {
-      if (!(o.radius > 0.0f)) { *err = "object " + std::to_string(i) + ": sphere radius must be > 0"; return false; }
-      for (int a = 0; a < 3; ++a) { b.lo[a] = -o.radius; b.hi[a] = o.radius; }
-    } else if (o.shape == PBRT_SHAPE_CYLINDER) {
-      if (!(o.radius > 0.0f) || !(o.height > 0.0f)) { *err = "object " + std::to_string(i) + ": bad cylinder"; return false; }
-      b.lo[0] = -o.radius; b.lo[1] = -r.half_height; b.lo[2] = -o.radius;
-      b.hi[0] = o.radius; b.hi[1] = r.half_height; b.hi[2] = o.radius;
-    } else {
-      *err = "object " + std::to_string(i) + ": unknown shape";
-      return false;
-    }
-    if (o.transformed) {  // the eight corners (aabound.rs:437-468)
-      const float* lo = b.lo;
-      const float* hi = b.hi;
-      const V3f c[8] = {{lo[0], lo[1], lo[2]}, {lo[0], lo[1], hi[2]}, {lo[0], hi[1], lo[2]}, {lo[0], hi[1], hi[2]},
-                        {hi[0], hi[1], hi[2]}, {hi[0], hi[1], lo[2]}, {hi[0], lo[1], hi[2]}, {hi[0], lo[1], lo[2]}};
-      Box3 t;
-      t.set_empty();
-      for (const V3f& p0 : c) {
-        const V3f p = xf_point(o.to_world, p0);
-        t.lo[0] = std::fmin(t.lo[0], p.x); t.lo[1] = std::fmin(t.lo[1], p.y); t.lo[2] = std::fmin(t.lo[2], p.z);
-        t.hi[0] = std::fmax(t.hi[0], p.x); t.hi[1] = std::fmax(t.hi[1], p.y); t.hi[2] = std::fmax(t.hi[2], p.z);
+    const std::string who = "object " + std::to_string(i) + ": ";
+    if (o.material >= d.material_count) { *err = who + "bad material"; return false; }
+    Box3& b = shape_boxes[i];
+    switch (o.shape) {
+      case PBRT_SHAPE_MESH: {
+        if (o.mesh >= d.mesh_count) { *err = who + "bad mesh"; return false; }
+        const FlatMesh& fm = out->meshes[o.mesh];
+        for (int a = 0; a < 3; ++a) { b.lo[a] = fm.bounds_min[a]; b.hi[a] = fm.bounds_max[a]; }
+        break;
       }
-      b = t;
-    }
-    for (int a = 0; a < 3; ++a)
-      if (!std::isfinite(b.lo[a]) || !std::isfinite(b.hi[a])) {
-        *err = "object " + std::to_string(i) + ": unbounded objects are not supported";
-        return false;
+      case PBRT_SHAPE_SPHERE:
+        if (!(o.radius > 0.0f) || !std::isfinite(o.radius)) { *err = who + "sphere radius must be > 0"; return false; }
+        for (int a = 0; a < 3; ++a) { b.lo[a] = -o.radius; b.hi[a] = o.radius; }
+        break;
+      case PBRT_SHAPE_CYLINDER: {
+        if (!(o.radius > 0.0f) || !(o.height > 0.0f)) { *err = who + "bad cylinder"; return false; }
+        const float hh = o.height / 2.0f;
+        b.lo[0] = -o.radius; b.lo[1] = -hh; b.lo[2] = -o.radius;
+        b.hi[0] = o.radius; b.hi[1] = hh; b.hi[2] = o.radius;
+        break;
       }
-    boxes[i] = b;
-    out->objects.push_back(r);
+      case PBRT_SHAPE_RECTANGLE: {  // rectangle.rs:63-69: flat at y = 0
+        if (!(o.radius >= 0.0f) || !(o.height >= 0.0f) || !std::isfinite(o.radius) || !std::isfinite(o.height)) {
+          *err = who + "rectangle sides must be finite and >= 0";
+          return false;
+        }
+        const float hw = o.radius / 2.0f, hh = o.height / 2.0f;
+        b.lo[0] = -hw; b.lo[1] = 0.0f; b.lo[2] = -hh;
+        b.hi[0] = hw; b.hi[1] = 0.0f; b.hi[2] = hh;
+        break;
+      }
+      case PBRT_SHAPE_AABOX:
+        for (int a = 0; a < 3; ++a) {
+          if (!(o.extent[a] >= 0.0f) || !std::isfinite(o.extent[a])) {
+            *err = who + "box extents must be finite and >= 0";
+            return false;
+          }
+          const float h = o.extent[a] * 0.5f;
+          b.lo[a] = 0.0f - h;
+          b.hi[a] = h;
+        }
+        break;
+      case PBRT_SHAPE_PLANE:  // plane.rs:89-93: the half-space below y = 0
+        for (int a = 0; a < 3; ++a) { b.lo[a] = -INFINITY; b.hi[a] = INFINITY; }
+        b.hi[1] = 0.0f;
+        break;
+      default: *err = who + "unknown shape"; return false;
+    }
   }
-  TopBuilder(boxes).run(&out->top, &out->order, &out->top_depth);
+
+  Flattener fl(d, shape_boxes, out);
+  if (!fl.check_tree(err)) return false;
+  std::vector<uint32_t> refs;
+  std::vector<Box3> boxes;
+  std::vector<uint8_t> grouped;
+  if (!fl.run(&refs, &boxes, &grouped, err)) return false;
+  out->primitive_count = refs.size();
+  // Scene::commit: the unbounded primitives stay out of the tree, in scene order
+  std::vector<uint32_t> bounded_refs;
+  std::vector<Box3> bounded_boxes;
+  for (size_t i = 0; i < refs.size(); ++i) {
+    if (is_bounded(boxes[i])) {
+      bounded_refs.push_back(refs[i]);
+      bounded_boxes.push_back(boxes[i]);
+    } else {
+      out->unbounded.push_back(refs[i]);
+    }
+  }
+  if (!bounded_boxes.empty()) {
+    std::vector<uint32_t> slot;
+    TopBuilder(bounded_boxes).run(&out->top, &slot, &out->top_depth);
+    out->order.resize(slot.size());
+    for (size_t k = 0; k < slot.size(); ++k) out->order[k] = bounded_refs[slot[k]];
+  }
+  if (refs.size() == 1 && out->unbounded.empty() && !(refs[0] & kGroupBit)) {
+    const ObjRec& r = out->objects[refs[0]];
+    if (r.shape == PBRT_SHAPE_MESH && r.xf_count == 0) out->single_mesh = int(r.mesh);
+  }
 
   for (uint32_t i = 0; i < d.light_count; ++i) {
     const pbrt_light_desc& l = d.lights[i];
@@ -310,17 +551,30 @@ bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err) {
       r.bottom[c] = l.bottom[c];
       r.top[c] = l.top[c];
     }
-    if (l.kind > PBRT_LIGHT_AREA) { *err = "light " + std::to_string(i) + ": unknown kind"; return false; }
+    const std::string who = "light " + std::to_string(i) + ": ";
+    if (l.kind > PBRT_LIGHT_AREA) { *err = who + "unknown kind"; return false; }
     if (l.kind == PBRT_LIGHT_AREA) {
-      if (l.object >= d.object_count) { *err = "light " + std::to_string(i) + ": bad object"; return false; }
-      const pbrt_object_desc& o = d.objects[l.object];
-      if (d.materials[o.material].kind != PBRT_MAT_DIFFUSE_LIGHT) {
-        *err = "light " + std::to_string(i) + ": an area light's object must have a diffuse-light material";
+      if (l.object >= d.object_count) { *err = who + "bad object"; return false; }
+      // the emitter: the one leaf placing the object, a primitive of its own under at most one transform
+      uint32_t leaf = 0, found = 0;
+      for (uint32_t k = 0; k < out->objects.size(); ++k)
+        if (out->objects[k].desc_id == l.object) { leaf = k; ++found; }
+      if (found != 1 || grouped[leaf] || out->objects[leaf].xf_count > 1) {
+        *err = who + "an area light's object must be placed once, as a primitive of the scene under at most one "
+                     "transform";
         return false;
       }
-      if (o.shape == PBRT_SHAPE_MESH) {
-        const std::vector<float>& v = out->mesh_v[o.mesh];
-        const std::vector<uint32_t>& ix = out->mesh_idx[o.mesh];
+      const ObjRec& ob = out->objects[leaf];
+      r.object = leaf;
+      const pbrt_material_desc& em = d.materials[ob.material];
+      if (em.kind != PBRT_MAT_DIFFUSE_LIGHT) {
+        *err = who + "an area light's object must have a diffuse-light material";
+        return false;
+      }
+      if (em.texture != PBRT_TEXTURE_COLOR) { *err = who + "an area light's emission must be a plain colour"; return false; }
+      if (ob.shape == PBRT_SHAPE_MESH) {
+        const std::vector<float>& v = out->mesh_v[ob.mesh];
+        const std::vector<uint32_t>& ix = out->mesh_idx[ob.mesh];
         r.tri_first = uint32_t(out->light_cdf.size());
         r.tri_count = uint32_t(ix.size() / 3);
         float run = 0.0f;
@@ -329,7 +583,7 @@ bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err) {
           for (int k = 0; k < 3; ++k) {
             const uint32_t vi = ix[3 * t + k];
             const V3f q{v[3 * size_t(vi)], v[3 * size_t(vi) + 1], v[3 * size_t(vi) + 2]};
-            p[k] = o.transformed ? xf_point(o.to_world, q) : q;
+            p[k] = ob.xf_count ? xf_point(ob.to_world, q) : q;
             out->light_tris.push_back(p[k].x);
             out->light_tris.push_back(p[k].y);
             out->light_tris.push_back(p[k].z);
@@ -340,13 +594,13 @@ bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err) {
           out->light_cdf.push_back(run);
         }
         r.area = run;
-      } else if (o.shape == PBRT_SHAPE_SPHERE) {
-        r.area = 4.0f * kPi * o.radius * o.radius;
+      } else if (ob.shape == PBRT_SHAPE_SPHERE) {
+        r.area = 4.0f * kPi * ob.p[0] * ob.p[0];
       } else {
-        *err = "light " + std::to_string(i) + ": area lights are triangle meshes or spheres";
+        *err = who + "area lights are triangle meshes or spheres";
         return false;
       }
-      if (!(r.area > 0.0f)) { *err = "light " + std::to_string(i) + ": zero area"; return false; }
+      if (!(r.area > 0.0f)) { *err = who + "zero area"; return false; }
     }
     out->lights.push_back(r);
     if (l.kind == PBRT_LIGHT_POINT) out->max_radiance = INFINITY;

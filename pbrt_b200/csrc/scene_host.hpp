@@ -1,10 +1,15 @@
 // scene_host.hpp — host-side build of a whole scene for the GPU (no device code here).
 //
-// The top-level BVH is the reference's scene accelerator (src/bvh.rs:109-132, 291-388):
-// median split on the widest centroid axis after a stable sort, one object per leaf, boxes
-// combined bottom-up; object boxes are the shape's box, transformed corner by corner for
-// Transformed objects (src/geom/aabound.rs:437-468). Everything is FP32, compiled with
-// -ffp-contract=off, in the reference's operation order.
+// The scene's primitives are its objects, or the roots of its object tree (Simple,
+// Transformed, Compound nodes: src/objects/*.rs). Scene::commit (src/scene.rs:101-115) keeps
+// the unbounded ones (a Plane's box is infinite) in a list and builds the top-level BVH over
+// the rest, as the reference's scene accelerator does (src/bvh.rs:109-132, 291-388): median
+// split on the widest centroid axis after a stable sort, one primitive per leaf, boxes
+// combined bottom-up. A primitive's box is its get_bounding_box: the shape's box, transformed
+// corner by corner under every Transformed (src/geom/aabound.rs:437-468), the union over a
+// Compound's members. Everything is FP32, compiled with -ffp-contract=off, in the
+// reference's operation order. The tree is flattened for the GPU into leaves (a placed
+// Simple with the chain of transforms above it) and groups (a Compound's leaves).
 #pragma once
 
 #include <string>
@@ -21,10 +26,16 @@ struct FlatScene {
   std::vector<std::vector<float>> mesh_v;       // original vertices (shading)
   std::vector<std::vector<uint32_t>> mesh_idx;  // original indices (shading)
   std::vector<std::vector<uint32_t>> mesh_fmat; // per-triangle material, empty when absent
-  std::vector<ObjRec> objects;
-  std::vector<GpuNode> top;                     // GPU numbering (root 0, padding 1)
-  std::vector<uint32_t> order;                  // leaf slot -> object
+  std::vector<ObjRec> objects;                  // leaves: placed Simple objects
+  std::vector<XfRec> xforms;                    // transform chains beyond each leaf's first
+  std::vector<GroupRec> groups;                 // compounds (consecutive leaves)
+  std::vector<uint32_t> unbounded;              // primitives kept out of the BVH, in scene order
+  std::vector<GpuNode> top;                     // GPU numbering (root 0, padding 1); empty when no
+                                                // primitive is bounded
+  std::vector<uint32_t> order;                  // leaf slot -> primitive (leaf, or kGroupBit | group)
   uint32_t top_depth = 0;
+  uint64_t primitive_count = 0;                 // bounded + unbounded
+  int single_mesh = -1;                         // the mesh, when the scene is one untransformed mesh
   std::vector<MatRec> materials;
   std::vector<LightRec> lights;
   std::vector<float> light_tris;                // 9 floats per area-light triangle (world space)

@@ -5,25 +5,47 @@
 
 namespace pbrt {
 
-enum : uint32_t { kShapeMesh = 0, kShapeSphere = 1, kShapeCylinder = 2 };
+enum : uint32_t { kShapeMesh = 0, kShapeSphere = 1, kShapeCylinder = 2, kShapeRectangle = 3, kShapeAABox = 4,
+                  kShapePlane = 5 };
 enum : uint32_t { kMatLambertian = 0, kMatMetal = 1, kMatDielectric = 2, kMatDiffuseLight = 3 };
 enum : uint32_t { kLightPoint = 0, kLightUniform = 1, kLightBackground = 2, kLightArea = 3 };
+enum : uint32_t { kTexColor = 0, kTexChecker = 1 };
 
-// One object (Simple or Transformed(Simple)): 128 bytes, read as eight float4.
+// A scene primitive, as the top-level BVH's leaves and the unbounded list name it: one
+// placed object (a leaf index), or with kGroupBit set a group of leaves (a Compound).
+constexpr uint32_t kGroupBit = 0x80000000u;
+
+// One placed Simple object (a "leaf"): its shape and material, and the chain of transforms
+// between it and the world (xf_count of them, outermost first: the first inline here, the
+// rest at xforms[xf_rest ..]). 144 bytes.
 struct alignas(16) ObjRec {
-  uint32_t shape, mesh, material, transformed;
-  float radius, half_height, pad0, pad1;
-  float to_world[12];  // row-major 3x4 of Transform::mat
+  uint32_t shape, mesh, material, xf_count;
+  float p[3];        // sphere: r; cylinder: r, h/2; rectangle: w/2, h/2; aabox: extent/2 (x, y, z)
+  uint32_t desc_id;  // the object's index in the caller's description (reported as object_id)
+  uint32_t xf_rest, pad0, pad1, pad2;
+  float to_world[12];  // row-major 3x4 of Transform::mat (outermost transform)
   float to_local[12];  // row-major 3x4 of Transform::inv_mat
 };
-static_assert(sizeof(ObjRec) == 128, "ObjRec is 128 bytes");
+static_assert(sizeof(ObjRec) == 144, "ObjRec is 144 bytes");
+
+struct alignas(16) XfRec {
+  float to_world[12], to_local[12];
+};
+static_assert(sizeof(XfRec) == 96, "XfRec is 96 bytes");
+
+// A Compound's members: leaves [first, first + count), in member order.
+struct GroupRec {
+  uint32_t first, count;
+};
 
 struct alignas(16) MatRec {
-  uint32_t kind, pad;
+  uint32_t kind, texture;
   float fuzz, ior;
   float color[4];
+  float color2[3];
+  float scale;
 };
-static_assert(sizeof(MatRec) == 32, "MatRec is 32 bytes");
+static_assert(sizeof(MatRec) == 48, "MatRec is 48 bytes");
 
 struct alignas(16) LightRec {
   uint32_t kind, object, tri_first, tri_count;

@@ -4,14 +4,20 @@ Names and argument meanings follow the Rust crate:
   TriangleMesh::new(vertices, indices, ..)   src/shapes/triangle_mesh/triangle_mesh.rs:27-41
   Sphere::new(r)                             src/shapes/sphere.rs:16-18
   Cylinder::new(radius, height)              src/shapes/cylinder.rs:13-19
+  Rectangle::new(width, height)              src/shapes/rectangle.rs:14-21
+  AABox::new(extent)                         src/shapes/aabox.rs:14-22
+  Plane::new()                               src/shapes/plane.rs:11-15
+  PlainColor / CheckerBoard::new(c1, c2, scale)   src/textures/*.rs
   Simple::new(shape, material)               src/objects/simple.rs:16-21
   Transformed::new(object, transform)        src/objects/transformed.rs:15-20
+  Compound::new(objects)                     src/objects/compound.rs:15-19
   Transform::translation / rotation_*        src/geom/transform.rs:43-72
   Lambertian / Metal / Dielectric / DiffuseLight   src/materials/*.rs
   PointLight / UniformInfiniteLight / BackgroundInfiniteLight   src/lights/*.rs
   AreaLight — the reference's planned light (ideas/area_light.md), on an emissive object
   Scene::new / add_object / add_light / commit     src/scene.rs:80-115
   Scene::intersect / intersect_p (batched)         src/scene.rs:118-150
+  Scene::intersect[_p]_instrumented (batched)      src/scene.rs:124-153
   renderers::mt::render (mean radiance film)       src/renderers/mt.rs:23-130
 Errors the reference reports by panicking (an empty mesh, an index out of range) raise
 PbrtError here; "no hit" is PBRT_MISS in the returned id array, as `None` is in Rust.
@@ -145,11 +151,25 @@ class Transform:
         return Transform._rot(2, a)
 
     def __mul__(self, o: "Transform") -> "Transform":  # transform.rs:119-127
-        return Transform(self.mat @ o.mat, o.inv @ self.inv)
+        return Transform(_matmul4(self.mat, o.mat), _matmul4(o.inv, self.inv))
 
     def rows(self):
-        """(to_world, to_local) as 12 FP32 values each (row-major 3x4)."""
-        return (self.mat[:3, :].astype(np.float32).reshape(-1), self.inv[:3, :].astype(np.float32).reshape(-1))
+        """(to_world, to_local) as 12 float64 values each (row-major 3x4); the scene
+        description rounds them to FP32."""
+        return (self.mat[:3, :].reshape(-1).copy(), self.inv[:3, :].reshape(-1).copy())
+
+
+def _matmul4(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Matrix4 * Matrix4 as the reference sums it (matrix4.rs:216-232): m[i][j] starts at 0 and
+    adds a[i][k] * b[k][j] for k = 0..3 in turn (no fused or reordered sums)."""
+    m = np.zeros((4, 4))
+    for i in range(4):
+        for j in range(4):
+            acc = 0.0
+            for k in range(4):
+                acc += float(a[i, k]) * float(b[k, j])
+            m[i, j] = acc
+    return m
 
 
 # ------------------------------------------------------------------------------------------
@@ -191,6 +211,32 @@ class Cylinder:
 
 
 @dataclass
+class Rectangle:
+    """Rectangle::new(width, height): y = 0, |x| <= width/2, |z| <= height/2, facing +y."""
+    width: float
+    height: float
+
+
+@dataclass
+class AABox:
+    """AABox::new(extent): the box [-extent/2, extent/2]."""
+    extent: Sequence[float]
+
+
+@dataclass
+class Plane:
+    """The y = 0 plane (unbounded: kept out of the scene's BVH, tested first)."""
+
+
+@dataclass
+class CheckerBoard:
+    """CheckerBoard::new(c1, c2, scale): a texture usable wherever a material takes a colour."""
+    c1: Sequence[float]
+    c2: Sequence[float]
+    scale: float
+
+
+@dataclass
 class Lambertian:
     albedo: Sequence[float]
 
@@ -220,8 +266,14 @@ class Simple:
 
 @dataclass
 class Transformed:
-    object: Simple
+    object: object  # Simple, Transformed or Compound
     transform: Transform
+
+
+@dataclass
+class Compound:
+    """Several objects as one primitive: the nearest member's hit, the first on a tie."""
+    objects: List[object]
 
 
 @dataclass
@@ -250,15 +302,21 @@ class AreaLight:
     object: object
 
 
+def _texture(c) -> dict:
+    if isinstance(c, CheckerBoard):
+        return dict(color=tuple(c.c1), texture=_capi.TEXTURE_CHECKERBOARD, color2=tuple(c.c2), scale=float(c.scale))
+    return dict(color=tuple(c))
+
+
 def _material_desc(m) -> dict:
     if isinstance(m, Lambertian):
-        return dict(kind=_capi.MAT_LAMBERTIAN, color=tuple(m.albedo), fuzz=0.0, ior=1.0)
+        return dict(kind=_capi.MAT_LAMBERTIAN, fuzz=0.0, ior=1.0, **_texture(m.albedo))
     if isinstance(m, Metal):
-        return dict(kind=_capi.MAT_METAL, color=tuple(m.albedo), fuzz=float(m.fuzz), ior=1.0)
+        return dict(kind=_capi.MAT_METAL, fuzz=float(m.fuzz), ior=1.0, **_texture(m.albedo))
     if isinstance(m, Dielectric):
-        return dict(kind=_capi.MAT_DIELECTRIC, color=tuple(m.albedo), fuzz=0.0, ior=float(m.ref_idx))
+        return dict(kind=_capi.MAT_DIELECTRIC, fuzz=0.0, ior=float(m.ref_idx), **_texture(m.albedo))
     if isinstance(m, DiffuseLight):
-        return dict(kind=_capi.MAT_DIFFUSE_LIGHT, color=tuple(m.emitted), fuzz=0.0, ior=1.0)
+        return dict(kind=_capi.MAT_DIFFUSE_LIGHT, fuzz=0.0, ior=1.0, **_texture(m.emitted))
     raise TypeError(f"unknown material {m!r}")
 
 
@@ -332,17 +390,20 @@ class Scene:
         return self
 
     def describe(self, bvh_bins: int = 8, bvh_max_leaf: int = 1) -> dict:
-        """The plain description dict of this scene (see the module docstring)."""
+        """The plain description dict of this scene (see the module docstring). Scenes whose
+        objects are all Simple or Transformed(Simple) list them as objects; any other nesting
+        (Compound, Transformed of a Transformed) adds the object tree (nodes, roots)."""
         if self._desc is not None:
             return self._desc
         meshes, mesh_ids, materials, mat_ids, objs, obj_ids = [], {}, [], {}, [], {}
-        for o in self.objects:
-            xf = None
-            top = o
-            if isinstance(o, Transformed):
-                xf, o = o.transform, o.object
-            if not isinstance(o, Simple):
-                raise TypeError("objects are Simple or Transformed(Simple)")
+
+        def mat_index(m):
+            if id(m) not in mat_ids:
+                mat_ids[id(m)] = len(materials)
+                materials.append(_material_desc(m))
+            return mat_ids[id(m)]
+
+        def simple_desc(o: Simple) -> dict:
             d = dict(shape=0, mesh=0, radius=0.0, height=0.0, material=0, to_world=None, to_local=None)
             shp = o.shape
             if isinstance(shp, TriangleMesh):
@@ -350,12 +411,7 @@ class Scene:
                     mesh_ids[id(shp)] = len(meshes)
                     md = dict(vertices=shp.vertices, indices=shp.indices)
                     if shp.face_materials is not None:
-                        glob = []
-                        for m in shp.face_materials[0]:
-                            if id(m) not in mat_ids:
-                                mat_ids[id(m)] = len(materials)
-                                materials.append(_material_desc(m))
-                            glob.append(mat_ids[id(m)])
+                        glob = [mat_index(m) for m in shp.face_materials[0]]
                         md["face_materials"] = np.asarray(glob, np.uint32)[shp.face_materials[1]]
                     meshes.append(md)
                 d.update(shape=_capi.SHAPE_MESH, mesh=mesh_ids[id(shp)])
@@ -363,16 +419,57 @@ class Scene:
                 d.update(shape=_capi.SHAPE_SPHERE, radius=float(shp.r))
             elif isinstance(shp, Cylinder):
                 d.update(shape=_capi.SHAPE_CYLINDER, radius=float(shp.radius), height=float(shp.height))
+            elif isinstance(shp, Rectangle):
+                d.update(shape=_capi.SHAPE_RECTANGLE, radius=float(shp.width), height=float(shp.height))
+            elif isinstance(shp, AABox):
+                d.update(shape=_capi.SHAPE_AABOX, extent=tuple(float(x) for x in shp.extent))
+            elif isinstance(shp, Plane):
+                d.update(shape=_capi.SHAPE_PLANE)
             else:
                 raise TypeError(f"unknown shape {shp!r}")
-            if id(o.material) not in mat_ids:
-                mat_ids[id(o.material)] = len(materials)
-                materials.append(_material_desc(o.material))
-            d["material"] = mat_ids[id(o.material)]
-            if xf is not None:
-                d["to_world"], d["to_local"] = xf.rows()
-            obj_ids[id(top)] = len(objs)
-            objs.append(d)
+            d["material"] = mat_index(o.material)
+            return d
+
+        flat = all(isinstance(o, Simple) or (isinstance(o, Transformed) and isinstance(o.object, Simple))
+                   for o in self.objects)
+        nodes, roots = None, None
+        if flat:
+            for o in self.objects:
+                top, xf = o, None
+                if isinstance(o, Transformed):
+                    xf, o = o.transform, o.object
+                d = simple_desc(o)
+                if xf is not None:
+                    d["to_world"], d["to_local"] = xf.rows()
+                obj_ids[id(top)] = len(objs)
+                objs.append(d)
+        else:
+            nodes, node_ids, simple_ids = [], {}, {}
+
+            def node(o) -> int:
+                if id(o) in node_ids:  # a shared object stays one node
+                    return node_ids[id(o)]
+                if isinstance(o, Simple):
+                    if id(o) not in simple_ids:
+                        simple_ids[id(o)] = len(objs)
+                        objs.append(simple_desc(o))
+                    n = dict(kind=_capi.NODE_SIMPLE, object=simple_ids[id(o)])
+                elif isinstance(o, Transformed):
+                    w, l = o.transform.rows()
+                    n = dict(kind=_capi.NODE_TRANSFORMED, children=[node(o.object)], to_world=w, to_local=l)
+                elif isinstance(o, Compound):
+                    n = dict(kind=_capi.NODE_COMPOUND, children=[node(c) for c in o.objects])
+                else:
+                    raise TypeError(f"unknown object {o!r}")
+                node_ids[id(o)] = len(nodes)
+                nodes.append(n)
+                return node_ids[id(o)]
+
+            roots = [node(o) for o in self.objects]
+            for o in self.objects:  # an area light names a top-level Simple or Transformed(Simple)
+                inner = o.object if isinstance(o, Transformed) else o
+                if isinstance(inner, Simple) and id(inner) in simple_ids:
+                    obj_ids[id(o)] = simple_ids[id(inner)]
         lights = []
         for l in self.lights:
             if isinstance(l, PointLight):
@@ -387,8 +484,11 @@ class Scene:
                 lights.append(dict(kind=_capi.LIGHT_AREA, object=obj_ids[id(l.object)]))
             else:
                 raise TypeError(f"unknown light {l!r}")
-        return dict(meshes=meshes, materials=materials, objects=objs, lights=lights, bvh_bins=bvh_bins,
-                    bvh_max_leaf=bvh_max_leaf)
+        out = dict(meshes=meshes, materials=materials, objects=objs, lights=lights, bvh_bins=bvh_bins,
+                   bvh_max_leaf=bvh_max_leaf)
+        if nodes is not None:
+            out.update(nodes=nodes, roots=roots)
+        return out
 
     def commit(self, bvh_bins: int = 8, bvh_max_leaf: int = 1) -> "Scene":
         if self.ctx is None:
@@ -438,6 +538,27 @@ class Scene:
         occ = _empty_like(r, n, "u8")
         self.ctx.check(self.ctx.lib.pbrt_trace_any(self.h, _ptr(r), n, _ptr(occ)), "pbrt_trace_any")
         return occ
+
+    def intersect_counted(self, rays):
+        """Scene::intersect_instrumented over a batch: (prim_id, t, object_id, {nodes, boxes,
+        objects}) with the scene accelerator's counters summed over the rays."""
+        self._need()
+        r, n = _as_rays(rays)
+        prim, t, obj = _empty_like(r, n, "u32"), _empty_like(r, n, "f32"), _empty_like(r, n, "u32")
+        stats = (C.c_uint64 * 3)()
+        self.ctx.check(self.ctx.lib.pbrt_trace_closest_counted(self.h, _ptr(r), n, _ptr(prim), _ptr(t), _ptr(obj),
+                                                               stats), "pbrt_trace_closest_counted")
+        return prim, t, obj, dict(nodes=stats[0], boxes=stats[1], objects=stats[2])
+
+    def intersect_p_counted(self, rays):
+        """Scene::intersect_p_instrumented over a batch: (occluded, {nodes, boxes, objects})."""
+        self._need()
+        r, n = _as_rays(rays)
+        occ = _empty_like(r, n, "u8")
+        stats = (C.c_uint64 * 3)()
+        self.ctx.check(self.ctx.lib.pbrt_trace_any_counted(self.h, _ptr(r), n, _ptr(occ), stats),
+                       "pbrt_trace_any_counted")
+        return occ, dict(nodes=stats[0], boxes=stats[1], objects=stats[2])
 
     def render(self, camera: dict, spp: int, max_depth: int, seed: int = 1, rr_start: int = 0,
                sample_offset: int = 0, integrator: str = "path", film=None, pixel_stride: int = 1):
@@ -503,18 +624,38 @@ def _lower_description(desc: dict, bvh_bins: int = 8, bvh_max_leaf: int = 1):
         d.kind = int(m["kind"])
         d.color[:] = [float(c) for c in m["color"]]
         d.fuzz, d.ior = float(m.get("fuzz", 0.0)), float(m.get("ior", 1.0))
+        d.texture = int(m.get("texture", 0))
+        d.color2[:] = [float(c) for c in m.get("color2", (0.0, 0.0, 0.0))]
+        d.scale = float(m.get("scale", 1.0))
         mats.append(d)
+
+    def xf(dst, m):  # float64 (or float32) 3x4 rows, rounded to FP32
+        dst[:] = [float(x) for x in np.asarray(np.asarray(m, np.float64).reshape(-1)[:12], np.float32)]
+
     objs = []
     for o in desc["objects"]:
         d = _capi.ObjectDesc()
         d.shape, d.mesh = int(o["shape"]), int(o.get("mesh", 0))
         d.radius, d.height = float(o.get("radius", 0.0)), float(o.get("height", 0.0))
+        d.extent[:] = [float(x) for x in o.get("extent", (0.0, 0.0, 0.0))]
         d.material = int(o["material"])
         if o.get("to_world") is not None:
             d.transformed = 1
-            d.to_world[:] = [float(x) for x in np.asarray(o["to_world"], np.float32).reshape(-1)[:12]]
-            d.to_local[:] = [float(x) for x in np.asarray(o["to_local"], np.float32).reshape(-1)[:12]]
+            xf(d.to_world, o["to_world"])
+            xf(d.to_local, o["to_local"])
         objs.append(d)
+    nodes, kids = [], []
+    for n in desc.get("nodes") or []:
+        d = _capi.NodeDesc()
+        d.kind, d.object = int(n["kind"]), int(n.get("object", 0))
+        ch = [int(c) for c in n.get("children", [])]
+        d.first, d.count = len(kids), len(ch)
+        kids += ch
+        if n.get("to_world") is not None:
+            xf(d.to_world, n["to_world"])
+            xf(d.to_local, n["to_local"])
+        nodes.append(d)
+    roots = [int(r) for r in desc.get("roots", [])] if nodes else []
     lights = []
     for l in desc["lights"]:
         d = _capi.LightDesc()
@@ -531,6 +672,13 @@ def _lower_description(desc: dict, bvh_bins: int = 8, bvh_max_leaf: int = 1):
     sd.objects, sd.object_count = C.cast(arrays[2], C.POINTER(_capi.ObjectDesc)), len(objs)
     sd.lights, sd.light_count = C.cast(arrays[3], C.POINTER(_capi.LightDesc)), len(lights)
     sd.bvh_bins, sd.bvh_max_leaf = int(desc.get("bvh_bins", bvh_bins)), int(desc.get("bvh_max_leaf", bvh_max_leaf))
+    if nodes:
+        tree = ((_capi.NodeDesc * len(nodes))(*nodes), (C.c_uint32 * max(1, len(kids)))(*kids),
+                (C.c_uint32 * max(1, len(roots)))(*roots))
+        sd.nodes, sd.node_count = C.cast(tree[0], C.POINTER(_capi.NodeDesc)), len(nodes)
+        sd.node_children, sd.child_count = C.cast(tree[1], C.POINTER(C.c_uint32)), len(kids)
+        sd.roots, sd.root_count = C.cast(tree[2], C.POINTER(C.c_uint32)), len(roots)
+        keep.append(tree)
     keep.append(arrays)
     return sd, keep
 

@@ -62,6 +62,31 @@ def fixture_mesh_loader(meshes: dict, reference_dir=None):
     return load
 
 
+def write_ply(path, v, i):
+    """An ASCII PLY whose float text reads back to exactly these float32 values."""
+    v = np.asarray(v, np.float32).reshape(-1, 3)
+    i = np.asarray(i, np.uint32).reshape(-1, 3)
+    with open(path, "w") as f:
+        f.write(f"ply\nformat ascii 1.0\ncomment written by the tests\nelement vertex {len(v)}\n"
+                "property float x\nproperty float y\nproperty float z\n"
+                f"element face {len(i)}\nproperty list uchar int vertex_indices\nend_header\n")
+        for p in v:
+            f.write(" ".join(repr(float(x)) for x in p) + "\n")
+        for t in i:
+            f.write("3 " + " ".join(str(int(x)) for x in t) + "\n")
+
+
+@pytest.fixture(scope="session")
+def mesh_dir(tmp_path_factory, golden_meshes):
+    """A directory with test_files/cube.ply and test_files/bun_zipper_res4.ply written from the
+    fixtures, for scene files that name them."""
+    d = tmp_path_factory.mktemp("stage")
+    os.makedirs(d / "test_files")
+    for key in ("cube", "bun_zipper_res4"):
+        write_ply(d / "test_files" / f"{key}.ply", golden_meshes[key + "_vertices"], golden_meshes[key + "_indices"])
+    return str(d)
+
+
 @pytest.fixture(scope="session")
 def reference_test_files():
     p = os.path.join(REFERENCE_ROOT, "test_files")

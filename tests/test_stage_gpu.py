@@ -1,0 +1,176 @@
+"""The reference's scene files through the library's loader and the GPU, against the oracle.
+
+Scene mode of the reference's traversal benchmark (src/bin/bvh_stats.rs:254-286) on its own
+scene files: the GPU's nearest-hit and any-hit scene queries must give the FP32 oracle's
+answers bit for bit — object, primitive (triangle, box face, cylinder piece), distance,
+occlusion — and the same scene-accelerator counters (nodes visited, box tests, object tests).
+(The FP64 oracle reproduces the published counters exactly; tests/test_stage_oracle.py.)
+Rendered images of the files match the oracle's renders of the same sample streams.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+import pbrt_b200 as pb
+from conftest import fixture_mesh_loader, stage_text
+from oracle.stage import load_stage
+
+pytestmark = pytest.mark.gpu
+
+TRACE_SCENES = ["cornell_box_canonical.stage", "many_spheres.stage", "many_meshes.stage", "default.stage",
+                "cube_mesh.stage", "cornell_box.stage"]
+
+TREE_SCENE = """camera pin_hole pos 0.3 1.5 6 look 0 0 0 up 0 1 0
+scene
+  object transformed object simple aabox 1 2 1.5 lambertian color 0.5 0.5 0.5
+    transform { rotate_y 0.7 rotate_x 0.2 translate -1 0.2 0 }
+  object transformed object transformed object simple rectangle 2 1 metal 0.1 color 0.9 0.9 0.9
+    transform { rotate_z 0.3 } transform { translate 1.2 0.5 -0.5 rotate_x 1.2 }
+  object transformed object compound {
+      object simple sphere 0.4 dielectric 1.5 color 1 1 1
+      object transformed object simple cylinder 0.3 0.8 lambertian color 0.2 0.8 0.2
+        transform { translate 0.5 0 0 } }
+    transform { translate 0 1.2 0.8 }
+  object transformed object simple mesh file "test_files/cube.ply" reverse
+      lambertian checkerboard 0.9 0.1 0.1 0.1 0.1 0.9 3
+    transform { rotate_y 0.4 translate 1.5 -0.4 1 }
+  object transformed object simple plane lambertian checkerboard 0.8 0.8 0.8 0.2 0.2 0.2 1.5
+    transform { translate 0 -1 0 }
+  object transformed object simple rectangle 1 1 diffuse_light color 4 4 4
+    transform { rotate_x 3.14159 translate 0 3 0 }
+"""
+
+
+def relmse(x, ref):
+    return float(np.mean((x - ref) ** 2 / (ref * ref + 1e-2)))
+
+
+def _pair(text, golden_meshes, mesh_dir, **opts):
+    st = pb.Stage(text, base_dir=mesh_dir, **opts)
+    want = load_stage(text, fixture_mesh_loader(golden_meshes), **opts)
+    return st, st.scene(), want, oracle.Scene(want, np.float32)
+
+
+def _check_scene_mode(st, scene, want, osc):
+    rays = oracle.camera_rays(want["camera"], np.float32)
+    prim, t, obj, gst = scene.intersect_counted(rays)
+    oprim, oobj, ot, ost = osc.trace_instrumented(rays)
+    np.testing.assert_array_equal(obj, oobj)
+    np.testing.assert_array_equal(prim, oprim)
+    np.testing.assert_array_equal(t, ot)
+    assert gst == ost
+    res, srays = osc.cast_sets(want["camera"], shadow_rays=True)
+    sr = np.ascontiguousarray(srays[:, ~np.isnan(srays[0])])
+    occ, gsst = scene.intersect_p_counted(sr)
+    oocc, osst = osc.occluded_instrumented(sr)
+    np.testing.assert_array_equal(occ, oocc)
+    assert gsst == osst
+    assert int(occ.sum()) == res["shadow"]["hits"]
+    assert (obj != pb.PBRT_MISS).sum() == res["primary"]["hits"]
+    # the plain queries agree with the counted ones
+    p2, t2, o2 = scene.intersect(rays, with_object=True)
+    np.testing.assert_array_equal(o2, obj)
+    np.testing.assert_array_equal(t2, t)
+    np.testing.assert_array_equal(scene.intersect_p(sr), occ)
+    return gst, gsst, rays.shape[1], sr.shape[1]
+
+
+@pytest.mark.parametrize("name", TRACE_SCENES)
+def test_scene_mode_bit_exact(name, golden_meshes, mesh_dir, published_scenes):
+    st, scene, want, osc = _pair(stage_text(name), golden_meshes, mesh_dir, width=200, height=150)
+    gp, gs, n, m = _check_scene_mode(st, scene, want, osc)
+    if name in published_scenes:  # FP32 against the published FP64 figures, for the record
+        pub = published_scenes[name]
+        print(name, "primary", [round(v / n, 2) for v in gp.values()], pub["primary"],
+              "shadow", [round(v / m, 2) for v in gs.values()], pub["shadow"])
+
+
+def test_object_tree_bit_exact(golden_meshes, mesh_dir):
+    """Compound, nested Transformed, AABox, Rectangle, Cylinder, a reversed mesh and an
+    unbounded Plane, on rays from inside and outside the scene."""
+    st, scene, want, osc = _pair(TREE_SCENE, golden_meshes, mesh_dir, width=96, height=72)
+    assert scene.info()["object_count"] == 6
+    _check_scene_mode(st, scene, want, osc)
+    rng = np.random.default_rng(3)
+    n = 20000
+    o = rng.uniform(-3, 3, (3, n)).astype(np.float32)
+    d = rng.normal(size=(3, n))
+    d = (d / np.linalg.norm(d, axis=0)).astype(np.float32)
+    dn = d * (np.float32(1) / np.sqrt((d * d).sum(0, dtype=np.float32)))
+    rays = np.concatenate([o, dn, np.full((1, n), 1e-4, np.float32), np.full((1, n), 1e3, np.float32)])
+    prim, t, obj, gst = scene.intersect_counted(rays)
+    oprim, oobj, ot, ost = osc.trace_instrumented(rays)
+    np.testing.assert_array_equal(obj, oobj)
+    np.testing.assert_array_equal(prim, oprim)
+    np.testing.assert_array_equal(t, ot)
+    assert gst == ost
+    occ, g2 = scene.intersect_p_counted(rays)
+    oocc, o2 = osc.occluded_instrumented(rays)
+    np.testing.assert_array_equal(occ, oocc)
+    assert g2 == o2
+
+
+@pytest.mark.parametrize("name,opts,spp,depth,tol", [
+    ("cornell_box_canonical.stage", dict(fov_deg=60.0, far=2000.0), 64, 8, 5e-3),
+    ("default.stage", dict(), 32, 8, 5e-3),
+    ("many_spheres.stage", dict(), 16, 8, 5e-3),
+])
+def test_render_matches_oracle(name, opts, spp, depth, tol, golden_meshes, mesh_dir):
+    st, scene, want, osc = _pair(stage_text(name), golden_meshes, mesh_dir, width=64, height=48, **opts)
+    img = scene.render(st.camera, spp=spp, max_depth=depth, seed=4)
+    ref = osc.render(want["camera"], spp, depth, seed=4)
+    assert np.all(np.isfinite(img)) and img.mean() > 0
+    err = relmse(img, ref)
+    print(name, "relMSE", err)
+    assert err < tol, err
+
+
+def test_tree_scene_render_matches_oracle(golden_meshes, mesh_dir):
+    st, scene, want, osc = _pair(TREE_SCENE, golden_meshes, mesh_dir, width=64, height=48)
+    img = scene.render(st.camera, spp=32, max_depth=8, seed=9)
+    ref = osc.render(want["camera"], 32, 8, seed=9)
+    assert relmse(img, ref) < 5e-3
+
+
+def test_load_scene_one_call(golden_meshes, mesh_dir):
+    scene, cam = pb.load_scene(stage_text("cornell_box_canonical.stage"), base_dir=mesh_dir, width=40, height=30,
+                               fov_deg=60.0, far=2000.0)
+    img = scene.render(cam, spp=4, max_depth=4, seed=1)
+    assert img.shape == (30, 40, 3) and np.all(np.isfinite(img)) and img.mean() > 0
+
+
+def test_api_built_tree_equals_loaded(golden_meshes, mesh_dir):
+    """The Python mirror (Compound, Transformed, Rectangle, AABox, Plane, CheckerBoard) lowers
+    to the same scene as the loader: identical hits."""
+    T = pb.Transform
+    box = pb.Simple(pb.AABox((1.0, 2.0, 1.5)), pb.Lambertian((0.5, 0.5, 0.5)))
+    rect = pb.Simple(pb.Rectangle(2.0, 1.0), pb.Metal(0.1, (0.9, 0.9, 0.9)))
+    ball = pb.Simple(pb.Sphere(0.4), pb.Dielectric(1.5, (1.0, 1.0, 1.0)))
+    cyl = pb.Simple(pb.Cylinder(0.3, 0.8), pb.Lambertian((0.2, 0.8, 0.2)))
+    v, i = golden_meshes["cube_vertices"], golden_meshes["cube_indices"][:, ::-1]
+    cube = pb.Simple(pb.TriangleMesh(v, i), pb.Lambertian(pb.CheckerBoard((0.9, 0.1, 0.1), (0.1, 0.1, 0.9), 3.0)))
+    floor = pb.Simple(pb.Plane(), pb.Lambertian(pb.CheckerBoard((0.8, 0.8, 0.8), (0.2, 0.2, 0.2), 1.5)))
+    lamp = pb.Simple(pb.Rectangle(1.0, 1.0), pb.DiffuseLight((4.0, 4.0, 4.0)))
+    s = pb.Scene()
+    I = T.identity()  # a transform block folds its steps onto the identity
+    # scene files list objects in reverse; add them in the loaded order
+    s.add_object(pb.Transformed(lamp, I * T.translation((0, 3, 0)) * T.rotation_x(3.14159)))
+    s.add_object(pb.Transformed(floor, I * T.translation((0, -1, 0))))
+    s.add_object(pb.Transformed(cube, I * T.translation((1.5, -0.4, 1)) * T.rotation_y(0.4)))
+    s.add_object(pb.Transformed(pb.Compound([pb.Transformed(cyl, I * T.translation((0.5, 0, 0))), ball]),
+                                I * T.translation((0, 1.2, 0.8))))
+    s.add_object(pb.Transformed(pb.Transformed(rect, I * T.rotation_z(0.3)),
+                                I * T.rotation_x(1.2) * T.translation((1.2, 0.5, -0.5))))
+    s.add_object(pb.Transformed(box, I * T.translation((-1, 0.2, 0)) * T.rotation_x(0.2) * T.rotation_y(0.7)))
+    s.commit()
+    loaded = pb.Stage(TREE_SCENE, base_dir=mesh_dir, width=96, height=72)
+    ls = loaded.scene()
+    rays = oracle.camera_rays(load_stage(TREE_SCENE, fixture_mesh_loader(golden_meshes), width=96, height=72)["camera"],
+                              np.float32)
+    a = s.intersect_counted(rays)
+    b = ls.intersect_counted(rays)
+    np.testing.assert_array_equal(a[1], b[1])
+    np.testing.assert_array_equal(a[0], b[0])
+    assert a[3] == b[3]
