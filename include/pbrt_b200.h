@@ -281,19 +281,26 @@ int pbrt_trace_any_counted(pbrt_scene* scene, const float* rays, uint64_t n, uin
 /* ---------------------------------------------------------------------------------- */
 
 /* PinHoleCamera::new(resolution, fov, near, far, Matrix4::look_at(position, look_at, up))
- * (src/cameras/pin_hole.rs:17-38, src/geom/matrix4.rs:70-98). near/far are also every
- * ray's [near, far] interval, as the reference passes Config::near/far to li(). */
+ * (src/cameras/pin_hole.rs:17-38, src/geom/matrix4.rs:70-98), or with thin_lens = 1
+ * ThinLensCamera::new(.., lens_radius, focal_distance, ..) (src/cameras/thin_lens.rs:21-75),
+ * whose rays start on a disk of lens_radius (random_in_unit_disk, drawn after the pixel
+ * jitter) and pass through the point at focal_distance along the pinhole ray. near/far are
+ * also every ray's [near, far] interval, as the reference passes Config::near/far to li(). */
 typedef struct pbrt_camera_desc {
   uint32_t width, height;
   float fov; /* full field of view, radians */
   float near, far;
   float position[3], look_at[3], up[3];
+  uint32_t thin_lens;
+  float lens_radius, focal_distance;
 } pbrt_camera_desc;
 
 typedef enum pbrt_integrator {
-  PBRT_INTEGRATOR_PATH = 0, /* PathIntegrator (src/integrators/path.rs:48-115) + area-light NEE */
-  PBRT_INTEGRATOR_NAIVE = 1 /* NaiveIntegrator (src/integrators/naive.rs:29-52), background = the
-                               scene's infinite lights */
+  PBRT_INTEGRATOR_PATH = 0,  /* PathIntegrator (src/integrators/path.rs:48-115) + area-light NEE */
+  PBRT_INTEGRATOR_NAIVE = 1, /* NaiveIntegrator (src/integrators/naive.rs:29-52), background = the
+                                scene's infinite lights */
+  PBRT_INTEGRATOR_NORMAL = 2 /* NormalIntegrator (src/integrators/normal.rs:17-30): (n + 1) / 2 of the
+                                first hit, the infinite lights on a miss */
 } pbrt_integrator;
 
 typedef struct pbrt_render_params {
@@ -446,10 +453,10 @@ typedef struct pbrt_stage_options {
 int pbrt_stage_parse(const char* text, const pbrt_stage_options* options, pbrt_stage** out, char* err,
                      size_t err_len);
 /* The scene description (pointing into arrays the stage owns, valid until
- * pbrt_stage_destroy) and the camera (PinHoleCamera from the file's pos/look/up and the
- * options; a thin_lens camera is described by its pinhole, see camera_lens). Either output
- * may be NULL. camera_lens (2 floats, may be NULL) receives the thin lens' radius and focal
- * distance (0, 0 for a pin_hole camera). */
+ * pbrt_stage_destroy) and the camera (the file's pos/look/up, pin_hole or thin_lens, with
+ * the options' resolution, field of view and planes). Either output may be NULL.
+ * camera_lens (2 floats, may be NULL) receives the thin lens' radius and focal distance
+ * (0, 0 for a pin_hole camera). */
 int pbrt_stage_describe(const pbrt_stage* stage, pbrt_scene_desc* desc, pbrt_camera_desc* camera,
                         float* camera_lens);
 void pbrt_stage_destroy(pbrt_stage* stage);
@@ -467,6 +474,11 @@ void pbrt_free(void* p);
  * [0, 1], truncate to 8 bits, alpha 255, as image_write stores it (mt.rs:152-167). Host
  * buffers; no GPU work. */
 int pbrt_film_to_rgba8(const double* film_rgb, uint32_t width, uint32_t height, uint8_t* rgba);
+
+/* image_write (src/renderers/mt.rs:152-167): an 8-bit RGBA PNG of width x height pixels
+ * (row-major, row 0 at the top) at `path`. The pixels decode to exactly `rgba`; the
+ * compressed bytes are the library's own (stored deflate blocks). Host only. */
+int pbrt_write_png(const char* path, const uint8_t* rgba, uint32_t width, uint32_t height);
 
 #ifdef __cplusplus
 }

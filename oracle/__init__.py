@@ -255,7 +255,8 @@ class _OScene(C.Structure):
 class _OCamera(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("fov", C.c_double), ("near", C.c_double),
                 ("far", C.c_double), ("position", C.c_double * 3), ("look_at", C.c_double * 3),
-                ("up", C.c_double * 3)]
+                ("up", C.c_double * 3), ("thin_lens", C.c_uint32), ("lens_radius", C.c_double),
+                ("focal_distance", C.c_double)]
 
 
 class _ORender(C.Structure):
@@ -270,6 +271,9 @@ def _camera(cam: dict) -> _OCamera:
     c.position[:] = [float(x) for x in cam["position"]]
     c.look_at[:] = [float(x) for x in cam["look_at"]]
     c.up[:] = [float(x) for x in cam["up"]]
+    if cam.get("kind") == "thin_lens":  # ThinLensCamera (src/cameras/thin_lens.rs)
+        c.thin_lens = 1
+        c.lens_radius, c.focal_distance = float(cam["lens_radius"]), float(cam["focal_distance"])
     return c
 
 
@@ -460,7 +464,7 @@ class Scene:
         p = _ORender()
         p.camera = _camera(camera)
         p.spp, p.max_depth, p.rr_start, p.sample_offset = spp, max_depth, rr_start, sample_offset
-        p.seed, p.integrator = seed, 1 if integrator == "naive" else 0
+        p.seed, p.integrator = seed, {"path": 0, "naive": 1, "normal": 2}[integrator]
         film = np.zeros((int(camera["height"]), int(camera["width"]), 3), np.float64)
         if getattr(lib(), f"oracle_render_{self.suf}")(self._h, C.byref(p), _ptr(film), threads) != 0:
             raise RuntimeError(lib().oracle_last_error().decode())

@@ -356,7 +356,7 @@ int scene_occluded(const OScene<R>* s, const R* rays, size_t n, uint8_t* occ, in
 template <class R>
 void scene_cast_sets(const OScene<R>* s, const OCameraDesc* c, const double* target, double near, double far,
                      double shadow_near, uint64_t* out, R* shadow_rays) {
-  const PinHoleCamera<R> cam = make_camera<R>(*c);
+  const PinHoleCamera<R> cam = make_camera<R>(*c).pin;
   const V3<R> tgt{R(target[0]), R(target[1]), R(target[2])};
   SceneStats ps, ss;
   uint64_t np = 0, hp = 0, ns = 0, hs = 0;
@@ -390,7 +390,7 @@ void scene_cast_sets(const OScene<R>* s, const OCameraDesc* c, const double* tar
 // camera, mean radiance per pixel (accumulated in f64, the film the judge image needs).
 template <class R>
 int render(const OScene<R>* s, const ORenderParams* p, double* film, int threads, const CacheHook* cache = nullptr) {
-  const PinHoleCamera<R> cam = make_camera<R>(p->camera);
+  const Camera<R> cam = make_camera<R>(p->camera);
   const uint32_t w = p->camera.width, h = p->camera.height;
   const size_t npix = size_t(w) * h;
   parallel_for(npix, threads, [&](size_t b, size_t e) {
@@ -400,10 +400,11 @@ int render(const OScene<R>* s, const ORenderParams* p, double* film, int threads
       for (uint32_t k = 0; k < p->spp; ++k) {
         Pcg32 rng = path_rng(p->seed, uint32_t(pix), p->sample_offset + k);
         const R jx = R(rng.uniform()), jy = R(rng.uniform());  // Sampler2::sample (mt.rs:145-150)
-        const Ray<R> ray = cam.get_ray(R(x) + jx, R(y) + jy);
-        const V3<R> L = p->integrator == 1 ? s->li_naive(ray, R(p->camera.near), R(p->camera.far), p->max_depth, rng)
-                                           : s->li_path(ray, R(p->camera.near), R(p->camera.far), p->max_depth,
-                                                        p->rr_start, rng, cache);
+        const Ray<R> ray = cam.get_ray(R(x) + jx, R(y) + jy, rng);
+        const R near = R(p->camera.near), far = R(p->camera.far);
+        const V3<R> L = p->integrator == 1   ? s->li_naive(ray, near, far, p->max_depth, rng)
+                        : p->integrator == 2 ? s->li_normal(ray, near, far)
+                                             : s->li_path(ray, near, far, p->max_depth, p->rr_start, rng, cache);
         acc[0] += double(L.x);
         acc[1] += double(L.y);
         acc[2] += double(L.z);
@@ -439,7 +440,7 @@ CacheHook cache_hook(const float* weights, const float* b6, uint32_t term_hit) {
 
 template <class R>
 void camera_rays(const OCameraDesc* c, R* out) {
-  const PinHoleCamera<R> cam = make_camera<R>(*c);
+  const PinHoleCamera<R> cam = make_camera<R>(*c).pin;
   const size_t n = size_t(c->width) * c->height;
   for (size_t pix = 0; pix < n; ++pix) {
     const Ray<R> r = cam.get_ray(R(pix % c->width) + R(0.5), R(pix / c->width) + R(0.5));

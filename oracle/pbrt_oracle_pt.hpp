@@ -181,6 +181,8 @@ struct OCameraDesc {
   uint32_t width, height;
   double fov, near, far;
   double position[3], look_at[3], up[3];
+  uint32_t thin_lens;  // 1: ThinLensCamera with the two values below
+  double lens_radius, focal_distance;
 };
 struct ORenderParams {
   OCameraDesc camera;
@@ -1226,6 +1228,15 @@ class OScene {
     return L;
   }
 
+  // NormalIntegrator::li (normal.rs:17-27): (n + (1, 1, 1)) * 0.5 at the first hit; a miss is
+  // black (the trait's default background, integrators.rs:9-11)
+  V3<R> li_normal(const Ray<R>& ray, R near, R far) const {
+    Isect<R> it;
+    uint32_t obj, prim;
+    if (!intersect(ray, near, far, &it, &obj, &prim)) return V3<R>{R(0), R(0), R(0)};
+    return (it.n + V3<R>{R(1), R(1), R(1)}) * R(0.5);
+  }
+
   // NaiveIntegrator::li (naive.rs:29-52), written as a loop, background = infinite lights
   V3<R> li_naive(Ray<R> ray, R near, R far, uint32_t max_depth, Pcg32& rng) const {
     V3<R> beta{R(1), R(1), R(1)}, L{R(0), R(0), R(0)};
@@ -1266,12 +1277,41 @@ class OScene {
   std::vector<BNode> bnodes;
 };
 
+// PinHoleCamera, or ThinLensCamera::get_ray (thin_lens.rs:60-75): the lens sample
+// (random_in_unit_disk, utils.rs:9-17, bounded at 64 draws) is drawn after the pixel jitter.
 template <class R>
-PinHoleCamera<R> make_camera(const OCameraDesc& c) {
+struct Camera {
+  PinHoleCamera<R> pin;
+  bool thin = false;
+  R lens_radius = R(0), focal_distance = R(0);
+  Ray<R> get_ray(R px, R py, Pcg32& rng) const {
+    if (!thin) return pin.get_ray(px, py);
+    const V3<R> cv = normalized(pin.raster_to_screen.point(V3<R>{px, py, R(0)}));
+    const Ray<R> ray = make_ray(V3<R>{R(0), R(0), R(0)}, cv);
+    R x = R(0), y = R(0);
+    for (int k = 0; k < 64; ++k) {
+      x = R(rng.uniform()) * R(2) - R(1);
+      y = R(rng.uniform()) * R(2) - R(1);
+      if (x * x + y * y < R(1)) break;
+      if (k == 63) { x = x * R(0.5); y = y * R(0.5); }
+    }
+    const V3<R> lens{x * lens_radius, y * lens_radius, R(0)};
+    const R ft = focal_distance / cv.z;
+    const V3<R> dir = normalized((ray.o + ray.d * ft) - lens);
+    return make_ray(pin.cam_to_world.point(lens), pin.cam_to_world.direction(dir));
+  }
+};
+
+template <class R>
+Camera<R> make_camera(const OCameraDesc& c) {
   const V3<R> pos{R(c.position[0]), R(c.position[1]), R(c.position[2])};
   const V3<R> look{R(c.look_at[0]), R(c.look_at[1]), R(c.look_at[2])};
   const V3<R> up{R(c.up[0]), R(c.up[1]), R(c.up[2])};
-  return PinHoleCamera<R>(c.width, c.height, R(c.fov), R(c.near), R(c.far), M4<R>::look_at(pos, look, up));
+  Camera<R> cam{PinHoleCamera<R>(c.width, c.height, R(c.fov), R(c.near), R(c.far), M4<R>::look_at(pos, look, up))};
+  cam.thin = c.thin_lens != 0;
+  cam.lens_radius = R(c.lens_radius);
+  cam.focal_distance = R(c.focal_distance);
+  return cam;
 }
 
 }  // namespace oracle

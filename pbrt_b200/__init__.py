@@ -32,7 +32,9 @@ from .scene import (  # noqa: F401
     TriangleMesh,
     UniformInfiniteLight,
     default_context,
+    film_to_png,
     film_to_rgba8,
+    write_png,
 )
 from .stage import Stage, load_scene, read_ply  # noqa: F401
 
@@ -40,5 +42,5 @@ __all__ = [
     "PBRT_MISS", "PbrtError", "load", "Context", "default_context", "Scene", "TriangleMesh", "Sphere", "Cylinder",
     "Simple", "Transformed", "Transform", "Lambertian", "Metal", "Dielectric", "DiffuseLight", "PointLight",
     "UniformInfiniteLight", "BackgroundInfiniteLight", "AreaLight", "film_to_rgba8", "Rectangle", "AABox", "Plane",
-    "CheckerBoard", "Compound", "Stage", "load_scene", "read_ply",
+    "CheckerBoard", "Compound", "Stage", "load_scene", "read_ply", "write_png", "film_to_png",
 ]

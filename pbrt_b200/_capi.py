@@ -74,7 +74,8 @@ class SceneInfo(C.Structure):
 
 class CameraDesc(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("fov", C.c_float), ("near", C.c_float),
-                ("far", C.c_float), ("position", C.c_float * 3), ("look_at", C.c_float * 3), ("up", C.c_float * 3)]
+                ("far", C.c_float), ("position", C.c_float * 3), ("look_at", C.c_float * 3), ("up", C.c_float * 3),
+                ("thin_lens", C.c_uint32), ("lens_radius", C.c_float), ("focal_distance", C.c_float)]
 
 
 class RenderParams(C.Structure):
@@ -151,6 +152,7 @@ SIGNATURES = {
     "pbrt_batch_destroy": (None, [C.c_void_p]),
     "pbrt_render_batch": (C.c_int, [C.c_void_p, C.POINTER(RenderParams), C.c_uint32, C.c_void_p]),
     "pbrt_film_to_rgba8": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
+    "pbrt_write_png": (C.c_int, [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint32]),
 }
 
 _lib = None

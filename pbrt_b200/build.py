@@ -17,6 +17,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libpbrt_b200.so")
+CLI_SRC = os.path.join(HERE, "cli", "pbrt_main.cpp")
+CLI = os.path.join(HERE, "pbrt")  # the command-line renderer (src/main.rs), linked to the library
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC = os.environ.get("PBRT_NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
@@ -82,6 +84,15 @@ def build(force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"linking libpbrt_b200.so failed:\n{r.stdout}\n{r.stderr}")
+    if force or not os.path.exists(CLI) or os.path.getmtime(CLI) < max(os.path.getmtime(LIB),
+                                                                       os.path.getmtime(CLI_SRC)):
+        cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-I", INCLUDE, CLI_SRC, "-o", CLI, "-L", HERE, "-l:libpbrt_b200.so",
+               "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"building the pbrt command failed:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

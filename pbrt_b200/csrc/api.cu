@@ -571,9 +571,11 @@ int pbrt::api::check_render_params(pbrt_ctx* c, const pbrt_render_params* p, boo
   if (p->spp == 0 && !allow_no_samples) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "spp must be >= 1");
   if (p->max_depth == 0 || p->max_depth > 0xFFFF)
     return c->fail(PBRT_ERR_INVALID_ARGUMENT, "max_depth must be in [1, 65535]");
-  if (p->integrator > PBRT_INTEGRATOR_NAIVE) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "unknown integrator");
+  if (p->integrator > PBRT_INTEGRATOR_NORMAL) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "unknown integrator");
   if (!(cd.fov > 0.f) || !(cd.fov < 3.14159265f) || !(cd.far > cd.near))
     return c->fail(PBRT_ERR_INVALID_ARGUMENT, "bad camera");
+  if (cd.thin_lens && (!(cd.lens_radius >= 0.f) || !std::isfinite(cd.lens_radius) || !std::isfinite(cd.focal_distance)))
+    return c->fail(PBRT_ERR_INVALID_ARGUMENT, "bad thin lens");
   if (uint64_t(cd.width) * cd.height > 0xFFFFFFFFull) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "image too large");
   if (p->pixel_stride > cd.width || p->pixel_stride > cd.height)
     return c->fail(PBRT_ERR_INVALID_ARGUMENT, "pixel_stride exceeds the image");
@@ -585,9 +587,9 @@ RenderSettings pbrt::api::settings_of(pbrt_ctx* c, const pbrt_render_params* p) 
   rs.stats = c->d_counters + 8;
   rs.shape = c->shape;
   rs.max_depth = p->max_depth;
-  rs.rr_start = p->integrator == PBRT_INTEGRATOR_NAIVE ? 0u : p->rr_start;
+  rs.rr_start = p->integrator == PBRT_INTEGRATOR_PATH ? p->rr_start : 0u;
   rs.sample_offset = p->sample_offset;
-  rs.naive = p->integrator == PBRT_INTEGRATOR_NAIVE ? 1u : 0u;
+  rs.integrator = p->integrator;
   rs.seed = p->seed;
   rs.stride = p->pixel_stride > 1 ? p->pixel_stride : 1u;
   rs.film_w = (p->camera.width + rs.stride - 1) / rs.stride;

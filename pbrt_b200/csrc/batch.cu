@@ -100,7 +100,7 @@ int pbrt_batch_create(pbrt_ctx* c, pbrt_scene* const* scenes, const pbrt_render_
     e.max_depth = rs.max_depth;
     e.rr_start = rs.rr_start;
     e.sample_offset = p->sample_offset;
-    e.naive = rs.naive;
+    e.integrator = rs.integrator;
     e.stride = rs.stride;
     e.film_w = rs.film_w;
     const unsigned long long paths = (unsigned long long)e.npix * e.spp;
@@ -110,7 +110,7 @@ int pbrt_batch_create(pbrt_ctx* c, pbrt_scene* const* scenes, const pbrt_render_
     b->table.push_back(e);
     b->film_n.push_back(size_t(e.npix) * 3);
     b->max_depth = std::max(b->max_depth, e.max_depth);
-    b->any_path = b->any_path || !e.naive;
+    b->any_path = b->any_path || !e.integrator;
   }
   int rc = PBRT_OK;
   for (uint32_t i = 0; i < n && rc == PBRT_OK; ++i) {

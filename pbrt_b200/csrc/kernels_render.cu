@@ -256,9 +256,24 @@ PBRT_DEV bool scatter(const MatRec& m, const F3& col, const Isect& it, unsigned 
 }
 
 // ---- the camera ------------------------------------------------------------------------------
+// random_in_unit_disk (utils.rs:9-17): rejection on [-1, 1)^2, bounded at 64 draws
+PBRT_DEV void in_unit_disk(unsigned long long& st, unsigned long long inc, float& x, float& y) {
+  for (int k = 0; k < 64; ++k) {
+    x = fs(fm(pcg_uniform(st, inc), 2.f), 1.f);
+    y = fs(fm(pcg_uniform(st, inc), 2.f), 1.f);
+    if (fa(fm(x, x), fm(y, y)) < 1.f) return;
+  }
+  x = fm(x, 0.5f);
+  y = fm(y, 0.5f);
+}
+
 // PinHoleCamera::get_ray (pin_hole.rs:42-50): raster -> screen through the inverse
 // perspective (w != 1 divides), normalise, camera -> world, Ray::new normalises again.
-PBRT_DEV void camera_ray(const CameraRec& c, float px, float py, F3& o, F3& d) {
+// ThinLensCamera::get_ray (thin_lens.rs:60-75): from a point of the lens disk through the
+// pinhole ray's point at focal_distance / cv.z, both to world (the lens sample is drawn after
+// the pixel jitter).
+PBRT_DEV void camera_ray(const CameraRec& c, float px, float py, unsigned long long& st, unsigned long long inc,
+                         F3& o, F3& d) {
   const float* m = c.raster_to_screen;
   F3 v = mk3(fa(fa(fa(fm(m[0], px), fm(m[1], py)), fm(m[2], 0.f)), m[3]),
              fa(fa(fa(fm(m[4], px), fm(m[5], py)), fm(m[6], 0.f)), m[7]),
@@ -266,8 +281,19 @@ PBRT_DEV void camera_ray(const CameraRec& c, float px, float py, F3& o, F3& d) {
   const float w = fa(fa(fa(fm(m[12], px), fm(m[13], py)), fm(m[14], 0.f)), m[15]);
   if (w != 1.f) v = mul3(v, frcp(w));
   const F3 cv = normalize3(v);
-  o = xf_point(c.cam_to_world, mk3(0.f, 0.f, 0.f));
-  d = normalize3(xf_dir(c.cam_to_world, cv));
+  if (!c.thin_lens) {
+    o = xf_point(c.cam_to_world, mk3(0.f, 0.f, 0.f));
+    d = normalize3(xf_dir(c.cam_to_world, cv));
+    return;
+  }
+  const F3 rd = normalize3(cv);  // Ray::new(0, camera_vector)
+  float lx, ly;
+  in_unit_disk(st, inc, lx, ly);
+  const F3 lens = mk3(fm(lx, c.lens_radius), fm(ly, c.lens_radius), 0.f);
+  const float ft = fdv(c.focal_distance, cv.z);
+  const F3 dir = normalize3(sub3(add3(mk3(0.f, 0.f, 0.f), mul3(rd, ft)), lens));  // ray.point_at(ft) - origin
+  o = xf_point(c.cam_to_world, lens);
+  d = normalize3(xf_dir(c.cam_to_world, dir));
 }
 
 // ---- the radiance cache's records ---------------------------------------------------------------
@@ -283,7 +309,7 @@ PBRT_DEV void write_record(float* rec, const F3& p, float rough, const F3& wo, c
 // The wavefront kernels are written once over a scene source: one scene passed as a kernel
 // parameter (pbrt_render, the cached render), or the batch table indexed by the path's scene.
 struct PathSettings {
-  uint32_t max_depth, rr_start, naive;
+  uint32_t max_depth, rr_start, integrator;  // integrator: 0 path, 1 naive, 2 normal
   float near, far;
 };
 
@@ -299,7 +325,7 @@ struct ManyScenes {
   PBRT_DEV const SceneView& view(const WaveBuffers& w, uint32_t p) const { return b[w.scene[p]].view; }
   PBRT_DEV PathSettings settings(const WaveBuffers& w, uint32_t p) const {
     const BatchScene& e = b[w.scene[p]];
-    return PathSettings{e.max_depth, e.rr_start, e.naive, e.cam.near, e.cam.far};
+    return PathSettings{e.max_depth, e.rr_start, e.integrator, e.cam.near, e.cam.far};
   }
 };
 
@@ -311,7 +337,7 @@ PBRT_DEV void start_path(const WaveBuffers& w, uint32_t i, const CameraRec& cam,
   unsigned long long st = pcg_seed(seed, pixel, sample);
   const float jx = pcg_uniform(st, inc), jy = pcg_uniform(st, inc);  // Sampler2::sample (mt.rs:145-150)
   F3 o, d;
-  camera_ray(cam, fa(float(pixel % cam.width), jx), fa(float(pixel / cam.width), jy), o, d);
+  camera_ray(cam, fa(float(pixel % cam.width), jx), fa(float(pixel / cam.width), jy), st, inc, o, d);
   w.ox[i] = o.x; w.oy[i] = o.y; w.oz[i] = o.z;
   w.dx[i] = d.x; w.dy[i] = d.y; w.dz[i] = d.z;
   w.br[i] = 1.f; w.bg[i] = 1.f; w.bb[i] = 1.f;
@@ -406,7 +432,8 @@ __global__ void __launch_bounds__(256) k_shade(WaveBuffers w, Src src, const uin
       p = q[k];
       const SceneView& s = src.view(w, p);
       const PathSettings ps = src.settings(w, p);
-      const uint32_t max_depth = ps.max_depth, rr_start = ps.rr_start, naive = ps.naive;
+      const uint32_t max_depth = ps.max_depth, rr_start = ps.rr_start, naive = ps.integrator;
+      const bool normal_only = ps.integrator == 2u;
       F3 o = mk3(w.ox[p], w.oy[p], w.oz[p]), d = mk3(w.dx[p], w.dy[p], w.dz[p]);
       F3 beta = mk3(w.br[p], w.bg[p], w.bb[p]);
       F3 L = mk3(w.lr[p], w.lg[p], w.lb[p]);
@@ -419,7 +446,7 @@ __global__ void __launch_bounds__(256) k_shade(WaveBuffers w, Src src, const uin
       const uint32_t obj = w.hobj[p];
       bool alive = false;
       if (obj == 0xFFFFFFFFu) {
-        if (spec) {
+        if (spec && !normal_only) {  // NormalIntegrator's background is black (integrators.rs:9-11)
           const F3 bg = background(s, d);
           L = add3(L, mk3(fm(bg.x, beta.x), fm(bg.y, beta.y), fm(bg.z, beta.z)));
         }
@@ -427,7 +454,13 @@ __global__ void __launch_bounds__(256) k_shade(WaveBuffers w, Src src, const uin
         const MatRec m = s.materials[material_index(s, obj, w.hprim[p])];
         const Isect it = interaction(s, obj, w.hprim[p], o, d, w.ht[p], m.texture != kTexColor);
         const F3 alb = texel(m, it);  // albedo, or emitted radiance (DiffuseLight::emit)
-        if (spec && m.kind == kMatDiffuseLight) L = add3(L, mk3(fm(alb.x, beta.x), fm(alb.y, beta.y), fm(alb.z, beta.z)));
+        if (normal_only) {  // NormalIntegrator::li (normal.rs:17-27): (n + (1, 1, 1)) * 0.5, one hit
+          const F3 nn = add3(it.n, mk3(1.f, 1.f, 1.f));
+          L = mul3(nn, 0.5f);
+          bounce = max_depth - 1u;  // the hit ends the path
+        }
+        if (spec && !normal_only && m.kind == kMatDiffuseLight)
+          L = add3(L, mk3(fm(alb.x, beta.x), fm(alb.y, beta.y), fm(alb.z, beta.z)));
         bounce++;
         // PathIntegrator stops at the max_depth-th hit, before sampling a light (path.rs:64-67);
         // the naive estimator also ends there, its emission counted: after max_depth hits its
@@ -769,8 +802,8 @@ cudaError_t trace_wave(const SceneView& s, const WaveBuffers& w, const CacheWave
                                                              rs.random_pixels, rs.stride,
                                                              rs.film_w ? rs.film_w : cam.width, rs.stats);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  const OneScene src{s, PathSettings{rs.max_depth, rs.rr_start, rs.naive, cam.near, cam.far}};
-  return bounce_loop(w, src, cw, rs.loop_depth ? rs.loop_depth : rs.max_depth, !rs.naive, rs.cache_mode, rs.term_hit,
+  const OneScene src{s, PathSettings{rs.max_depth, rs.rr_start, rs.integrator, cam.near, cam.far}};
+  return bounce_loop(w, src, cw, rs.loop_depth ? rs.loop_depth : rs.max_depth, !rs.integrator, rs.cache_mode, rs.term_hit,
                      rs.shape, rs.stats, err, sm_count, st);
 }
 

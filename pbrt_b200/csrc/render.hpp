@@ -57,7 +57,8 @@ struct LaunchShape {
 };
 
 struct RenderSettings {
-  uint32_t max_depth, rr_start, sample_offset, naive;
+  uint32_t max_depth, rr_start, sample_offset;
+  uint32_t integrator;  // pbrt_integrator: 0 path, 1 naive, 2 normal
   unsigned long long seed;
   uint32_t cache_mode = kCacheOff;
   uint32_t term_hit = 0;       // the hit at which paths end into the cache
@@ -78,7 +79,7 @@ struct BatchScene {
   CameraRec cam;
   double* film;       // sums; scaled by 1 / spp at the end
   unsigned long long begin, seed;
-  uint32_t npix, spp, max_depth, rr_start, sample_offset, naive, stride, film_w;
+  uint32_t npix, spp, max_depth, rr_start, sample_offset, integrator, stride, film_w;
 };
 
 // A batched frame: waves of `wave` paths over all scenes' paths (scenes in table order); the

@@ -632,6 +632,9 @@ CameraRec build_camera(const pbrt_camera_desc& c) {
   r.height = c.height;
   r.near = c.near;
   r.far = c.far;
+  r.thin_lens = c.thin_lens ? 1u : 0u;
+  r.lens_radius = c.lens_radius;
+  r.focal_distance = c.focal_distance;
   return r;
 }
 

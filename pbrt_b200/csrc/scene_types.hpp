@@ -54,12 +54,15 @@ struct alignas(16) LightRec {
 };
 static_assert(sizeof(LightRec) == 96, "LightRec is 96 bytes");
 
-// PinHoleCamera (src/cameras/pin_hole.rs:17-50), evaluated on the host in FP32.
+// PinHoleCamera (src/cameras/pin_hole.rs:17-50) or ThinLensCamera (src/cameras/thin_lens.rs),
+// evaluated on the host in FP32.
 struct CameraRec {
   float raster_to_screen[16];  // row-major 4x4 (the inverse perspective makes w != 1)
   float cam_to_world[12];      // row-major 3x4
   uint32_t width, height;
   float near, far;
+  uint32_t thin_lens;
+  float lens_radius, focal_distance;
 };
 
 }  // namespace pbrt

@@ -421,13 +421,16 @@ class StageParser {
     vector(look);
     expect_kw("up");
     vector(up);
-    if (k == "thin_lens") {
+    pbrt_camera_desc& c = st_->camera;
+    if (k == "thin_lens") {  // visit_camera_thin_lens: the file's radius and focal length
       expect_kw("radius");
       st_->lens[0] = float(number());
       expect_kw("focal_length");
       st_->lens[1] = float(number());
+      c.thin_lens = 1;
+      c.lens_radius = st_->lens[0];
+      c.focal_distance = st_->lens[1];
     }
-    pbrt_camera_desc& c = st_->camera;
     c.width = opt_.width ? opt_.width : 800;
     c.height = opt_.height ? opt_.height : 600;
     const double fov_deg = opt_.fov_deg != 0.0 ? opt_.fov_deg : 90.0;

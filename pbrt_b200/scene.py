@@ -353,13 +353,21 @@ def _empty_like(ref, n: int, dtype: str):
 
 
 def camera_desc(camera: dict) -> _capi.CameraDesc:
+    """A camera dict: width, height, fov (radians), near, far, position, look_at, up; with
+    kind = "thin_lens" also lens_radius and focal_distance (ThinLensCamera)."""
     c = _capi.CameraDesc()
     c.width, c.height = int(camera["width"]), int(camera["height"])
     c.fov, c.near, c.far = float(camera["fov"]), float(camera["near"]), float(camera["far"])
     c.position[:] = [float(x) for x in camera["position"]]
     c.look_at[:] = [float(x) for x in camera["look_at"]]
     c.up[:] = [float(x) for x in camera["up"]]
+    if camera.get("kind") == "thin_lens":
+        c.thin_lens = 1
+        c.lens_radius, c.focal_distance = float(camera["lens_radius"]), float(camera["focal_distance"])
     return c
+
+
+INTEGRATORS = {"path": 0, "naive": 1, "normal": 2}
 
 
 # ------------------------------------------------------------------------------------------
@@ -569,7 +577,7 @@ class Scene:
         p = _capi.RenderParams()
         p.camera = camera_desc(camera)
         p.spp, p.max_depth, p.rr_start, p.sample_offset = int(spp), int(max_depth), int(rr_start), int(sample_offset)
-        p.seed, p.integrator, p.pixel_stride = int(seed), 1 if integrator == "naive" else 0, int(pixel_stride)
+        p.seed, p.integrator, p.pixel_stride = int(seed), INTEGRATORS[integrator], int(pixel_stride)
         if film is None:
             film = np.zeros(film_shape(camera, pixel_stride), np.float64)
         self.ctx.check(self.ctx.lib.pbrt_render(self.h, C.byref(p), _ptr(film)), "pbrt_render")
@@ -705,7 +713,7 @@ def render_params(camera: dict, spp: int, max_depth: int, seed: int = 1, rr_star
     p = _capi.RenderParams()
     p.camera = camera_desc(camera)
     p.spp, p.max_depth, p.rr_start, p.sample_offset = int(spp), int(max_depth), int(rr_start), int(sample_offset)
-    p.seed, p.integrator, p.pixel_stride = int(seed), 1 if integrator == "naive" else 0, int(pixel_stride)
+    p.seed, p.integrator, p.pixel_stride = int(seed), INTEGRATORS[integrator], int(pixel_stride)
     return p
 
 
@@ -757,6 +765,19 @@ def film_shape(camera: dict, pixel_stride: int = 1):
     """(rows, columns, 3) of the film a render with this camera and pixel stride fills."""
     s = max(1, int(pixel_stride))
     return (-(-int(camera["height"]) // s), -(-int(camera["width"]) // s), 3)
+
+
+def write_png(path: str, rgba: np.ndarray):
+    """image_write (src/renderers/mt.rs:152-167): an (h, w, 4) uint8 image as an RGBA PNG."""
+    a = np.ascontiguousarray(rgba, np.uint8)
+    rc = _capi.load().pbrt_write_png(path.encode(), a.ctypes.data, a.shape[1], a.shape[0])
+    if rc != 0:
+        raise PbrtError(rc, f"pbrt_write_png({path})")
+
+
+def film_to_png(film: np.ndarray, path: str):
+    """The renderer's output file: gamma, clip, 8 bits (film_to_rgba8), then write_png."""
+    write_png(path, film_to_rgba8(film))
 
 
 def film_to_rgba8(film: np.ndarray) -> np.ndarray:

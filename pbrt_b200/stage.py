@@ -34,8 +34,11 @@ def _options(base_dir, width, height, fov_deg, near, far, loader_lights, bvh_bin
 
 
 def _camera_dict(c: _capi.CameraDesc) -> dict:
-    return dict(width=c.width, height=c.height, fov=c.fov, near=c.near, far=c.far, position=tuple(c.position),
-                look_at=tuple(c.look_at), up=tuple(c.up))
+    d = dict(width=c.width, height=c.height, fov=c.fov, near=c.near, far=c.far, position=tuple(c.position),
+             look_at=tuple(c.look_at), up=tuple(c.up))
+    if c.thin_lens:
+        d.update(kind="thin_lens", lens_radius=c.lens_radius, focal_distance=c.focal_distance)
+    return d
 
 
 class Stage:
@@ -59,7 +62,8 @@ class Stage:
 
     @property
     def camera(self) -> dict:
-        """The camera as a dict for Scene.render (a thin_lens camera by its pinhole; see lens)."""
+        """The camera as a dict for Scene.render (kind "thin_lens" with lens_radius and
+        focal_distance for a thin_lens camera)."""
         return _camera_dict(self.cam)
 
     @property
