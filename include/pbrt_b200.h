@@ -188,6 +188,9 @@ typedef struct pbrt_scene_desc {
   uint32_t child_count;
   const uint32_t* roots;
   uint32_t root_count;
+  /* 1: build the meshes' BVHs on the GPU (the same trees and triangle order as the host
+   * build); mesh arrays (vertices, indices, face_materials) may then be device memory. */
+  uint32_t device_build;
 } pbrt_scene_desc;
 
 /* Builds the acceleration structures on the host and uploads the scene. Replaces
@@ -211,6 +214,15 @@ int pbrt_scene_create_many(pbrt_ctx* ctx, const pbrt_scene_desc* descs, uint32_t
  * (src/shapes/triangle_mesh/bvh.rs:179-230) for callers that inspect the tree. */
 int pbrt_mesh_bvh_build_host(const pbrt_mesh_desc* mesh, uint32_t bvh_bins, uint32_t bvh_max_leaf, void* nodes,
                              uint64_t node_capacity, uint32_t* tri_order, uint64_t* node_count);
+/* pbrt_mesh_bvh_build_host on the context's GPU: the binned-SAH build of
+ * src/shapes/triangle_mesh/bvh.rs:221-309, 609-735 with every node split level by level by
+ * many thread blocks (small subtrees by one thread each); it yields the same nodes, in the
+ * same numbering, and the same triangle order. The mesh arrays may be host or device
+ * memory; nodes and tri_order are host memory. build_ms (may be NULL) receives the device
+ * time of the build, input copies included. */
+int pbrt_mesh_bvh_build_device(pbrt_ctx* ctx, const pbrt_mesh_desc* mesh, uint32_t bvh_bins, uint32_t bvh_max_leaf,
+                               void* nodes, uint64_t node_capacity, uint32_t* tri_order, uint64_t* node_count,
+                               float* build_ms);
 
 typedef struct pbrt_scene_info {
   uint64_t triangle_count;

@@ -63,7 +63,7 @@ class SceneDesc(C.Structure):
                 ("bvh_bins", C.c_uint32), ("bvh_max_leaf", C.c_uint32),
                 ("nodes", C.POINTER(NodeDesc)), ("node_count", C.c_uint32),
                 ("node_children", C.POINTER(C.c_uint32)), ("child_count", C.c_uint32),
-                ("roots", C.POINTER(C.c_uint32)), ("root_count", C.c_uint32)]
+                ("roots", C.POINTER(C.c_uint32)), ("root_count", C.c_uint32), ("device_build", C.c_uint32)]
 
 
 class SceneInfo(C.Structure):
@@ -115,6 +115,8 @@ SIGNATURES = {
     "pbrt_scene_get_info": (C.c_int, [C.c_void_p, C.POINTER(SceneInfo)]),
     "pbrt_mesh_bvh_build_host": (C.c_int, [C.POINTER(MeshDesc), C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64,
                                            C.c_void_p, C.POINTER(C.c_uint64)]),
+    "pbrt_mesh_bvh_build_device": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.c_uint32, C.c_uint32, C.c_void_p,
+                                             C.c_uint64, C.c_void_p, C.POINTER(C.c_uint64), C.c_void_p]),
     "pbrt_trace_closest": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]),
     "pbrt_trace_closest_instrumented": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
                                                   C.c_void_p]),

@@ -21,6 +21,7 @@
 #include "mesh_bvh.hpp"
 #include "render.hpp"
 #include "scene_device.cuh"
+#include "bvh_build_gpu.hpp"
 #include "scene_host.hpp"
 #include "trace_mesh.cuh"
 #include "context.hpp"
@@ -150,7 +151,9 @@ int pbrt_ctx_sync(pbrt_ctx* c) {
 namespace {
 
 // The device half of scene creation: checks the built structure, uploads it, fills the view.
-int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbrt_scene** out) {
+// Meshes listed in `dev` (non-null nodes) were built on the GPU: their arrays are taken over.
+int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbrt_scene** out,
+                 std::vector<DeviceMeshBuild>* dev = nullptr) {
   for (uint32_t i = 0; i < fs.meshes.size(); ++i)
     if (fs.meshes[i].stats.max_depth >= uint32_t(kTraceStack))
       return c->fail(PBRT_ERR_CAPACITY, "mesh " + std::to_string(i) + ": BVH depth " +
@@ -168,16 +171,29 @@ int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbr
   for (uint32_t i = 0; i < fs.meshes.size() && rc == PBRT_OK; ++i) {
     const FlatMesh& fm = fs.meshes[i];
     DeviceMesh& dm = s->meshes[i];
-    rc = upload(c, &dm.nodes, fm.nodes.data(), fm.nodes.size() * sizeof(GpuNode), &dm.bytes);
-    if (rc == PBRT_OK) rc = upload(c, &dm.tri_a, fm.tri_a.data(), fm.tri_a.size() * sizeof(float), &dm.bytes);
-    if (rc == PBRT_OK) rc = upload(c, &dm.tri_b, fm.tri_b.data(), fm.tri_b.size() * sizeof(float), &dm.bytes);
-    if (rc == PBRT_OK) rc = upload(c, &dm.tri_c, fm.tri_c.data(), fm.tri_c.size() * sizeof(float), &dm.bytes);
-    if (rc != PBRT_OK) break;
+    const uint64_t ntri = d->meshes[i].triangle_count;
+    if (dev && i < dev->size() && (*dev)[i].nodes) {  // built on the GPU: take its arrays
+      DeviceMeshBuild& b = (*dev)[i];
+      dm.nodes = b.nodes;
+      dm.tri_a = b.tri_a;
+      dm.tri_b = b.tri_b;
+      dm.tri_c = b.tri_c;
+      dm.bytes = b.node_slots * sizeof(GpuNode) + ntri * 40;
+      dm.view.node_count = uint32_t(b.node_slots);
+      cudaFree(b.tri_index);
+      b = DeviceMeshBuild{};
+    } else {
+      rc = upload(c, &dm.nodes, fm.nodes.data(), fm.nodes.size() * sizeof(GpuNode), &dm.bytes);
+      if (rc == PBRT_OK) rc = upload(c, &dm.tri_a, fm.tri_a.data(), fm.tri_a.size() * sizeof(float), &dm.bytes);
+      if (rc == PBRT_OK) rc = upload(c, &dm.tri_b, fm.tri_b.data(), fm.tri_b.size() * sizeof(float), &dm.bytes);
+      if (rc == PBRT_OK) rc = upload(c, &dm.tri_c, fm.tri_c.data(), fm.tri_c.size() * sizeof(float), &dm.bytes);
+      if (rc != PBRT_OK) break;
+      dm.view.node_count = uint32_t(fm.nodes.size());
+    }
     dm.view.nodes = (const float4*)dm.nodes;
     dm.view.tri_a = (const float4*)dm.tri_a;
     dm.view.tri_b = (const float4*)dm.tri_b;
     dm.view.tri_c = (const float2*)dm.tri_c;
-    dm.view.node_count = uint32_t(fm.nodes.size());
     views[i] = dm.view;
     void* pv = nullptr;
     void* pi = nullptr;
@@ -187,7 +203,7 @@ int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbr
     if (rc == PBRT_OK && !fs.mesh_fmat[i].empty())
       rc = s->upload(&pf, fs.mesh_fmat[i].data(), fs.mesh_fmat[i].size() * sizeof(uint32_t));
     shades[i] = MeshShade{(const float*)pv, (const uint32_t*)pi, (const uint32_t*)pf};
-    s->info.triangle_count += fm.tri_index.size();
+    s->info.triangle_count += ntri;
     s->info.mesh_node_count += fm.stats.node_count;
     s->info.mesh_leaf_count += fm.stats.leaf_count;
     s->info.mesh_max_depth = std::max(s->info.mesh_max_depth, fm.stats.max_depth);
@@ -249,6 +265,80 @@ int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbr
   return PBRT_OK;
 }
 
+// The meshes' BVHs built on the GPU (pbrt_scene_desc::device_build). Mesh arrays in device
+// memory are copied to the host for the scene build's host part (validation of face
+// materials, area-light triangles, the shading copies); `md` receives the description's
+// meshes pointing at host memory.
+int build_meshes_on_device(pbrt_ctx* c, const pbrt_scene_desc* d, std::vector<pbrt_mesh_desc>* md,
+                           std::vector<std::vector<float>>* hv, std::vector<std::vector<uint32_t>>* hi,
+                           std::vector<std::vector<uint32_t>>* hf, std::vector<MeshPrebuilt>* pre,
+                           std::vector<DeviceMeshBuild>* builds) {
+  const uint32_t n = d->mesh_count;
+  md->assign(d->meshes, d->meshes + n);
+  hv->resize(n);
+  hi->resize(n);
+  hf->resize(n);
+  pre->resize(n);
+  builds->resize(n);
+  MeshBuildParams bp;
+  bp.bins = d->bvh_bins ? int(d->bvh_bins) : 8;
+  bp.max_leaf = d->bvh_max_leaf ? d->bvh_max_leaf : 1;
+  cudaStream_t st = c->stream;
+  for (uint32_t i = 0; i < n; ++i) {
+    const pbrt_mesh_desc& m = d->meshes[i];
+    if (!m.vertices || !m.indices || m.triangle_count == 0)
+      return c->fail(PBRT_ERR_INVALID_ARGUMENT, "mesh " + std::to_string(i) + ": a TriangleMesh needs triangles");
+    const size_t vb = size_t(m.vertex_count) * 3 * sizeof(float), ib = size_t(m.triangle_count) * 3 * sizeof(uint32_t);
+    const bool vdev = mem_kind(m.vertices) == MemKind::Device, idev = mem_kind(m.indices) == MemKind::Device;
+    float* dv = nullptr;
+    uint32_t* di = nullptr;
+    int rc = PBRT_OK;
+    if (vdev) {
+      dv = const_cast<float*>(m.vertices);
+      (*hv)[i].resize(size_t(m.vertex_count) * 3);
+      rc = c->cuda(cudaMemcpyAsync((*hv)[i].data(), m.vertices, vb, cudaMemcpyDeviceToHost, st), "cudaMemcpy(vertices)");
+      (*md)[i].vertices = (*hv)[i].data();
+    } else {
+      rc = c->cuda(cudaMalloc(&dv, std::max<size_t>(vb, 4)), "cudaMalloc(build vertices)");
+      if (rc == PBRT_OK) rc = c->cuda(cudaMemcpyAsync(dv, m.vertices, vb, cudaMemcpyHostToDevice, st), "cudaMemcpy");
+    }
+    if (rc == PBRT_OK && idev) {
+      di = const_cast<uint32_t*>(m.indices);
+      (*hi)[i].resize(size_t(m.triangle_count) * 3);
+      rc = c->cuda(cudaMemcpyAsync((*hi)[i].data(), m.indices, ib, cudaMemcpyDeviceToHost, st), "cudaMemcpy(indices)");
+      (*md)[i].indices = (*hi)[i].data();
+    } else if (rc == PBRT_OK) {
+      rc = c->cuda(cudaMalloc(&di, std::max<size_t>(ib, 4)), "cudaMalloc(build indices)");
+      if (rc == PBRT_OK) rc = c->cuda(cudaMemcpyAsync(di, m.indices, ib, cudaMemcpyHostToDevice, st), "cudaMemcpy");
+    }
+    if (rc == PBRT_OK && m.face_materials && mem_kind(m.face_materials) == MemKind::Device) {
+      (*hf)[i].resize(m.triangle_count);
+      rc = c->cuda(cudaMemcpyAsync((*hf)[i].data(), m.face_materials, size_t(m.triangle_count) * 4,
+                                   cudaMemcpyDeviceToHost, st),
+                   "cudaMemcpy(face materials)");
+      (*md)[i].face_materials = (*hf)[i].data();
+    }
+    std::string e;
+    if (rc == PBRT_OK &&
+        !build_mesh_bvh_device(dv, m.vertex_count, di, m.triangle_count, bp, st, c->sm_count, &(*builds)[i], &e))
+      rc = c->fail(PBRT_ERR_INVALID_ARGUMENT, "mesh " + std::to_string(i) + ": " + e);
+    if (!vdev) cudaFree(dv);
+    if (!idev) cudaFree(di);
+    if (rc != PBRT_OK) {
+      for (DeviceMeshBuild& b : *builds) free_device_mesh_build(&b);
+      return rc;
+    }
+    MeshPrebuilt& p = (*pre)[i];
+    p.used = true;
+    p.stats = (*builds)[i].stats;
+    for (int a = 0; a < 3; ++a) {
+      p.bounds_min[a] = (*builds)[i].bounds_min[a];
+      p.bounds_max[a] = (*builds)[i].bounds_max[a];
+    }
+  }
+  return c->cuda(cudaStreamSynchronize(st), "device BVH build");
+}
+
 int check_scene_desc(pbrt_ctx* c, const pbrt_scene_desc* d) {
   if (!d) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "scene description is NULL");
   if (d->object_count == 0) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "a scene needs at least one object");
@@ -268,6 +358,21 @@ int pbrt_scene_create(pbrt_ctx* c, const pbrt_scene_desc* d, pbrt_scene** out) {
   PBRT_TRY(check_scene_desc(c, d));
   FlatScene fs;
   std::string e;
+  if (d->device_build && d->mesh_count) {
+    std::vector<pbrt_mesh_desc> md;
+    std::vector<std::vector<float>> hv;
+    std::vector<std::vector<uint32_t>> hi, hf;
+    std::vector<MeshPrebuilt> pre;
+    std::vector<DeviceMeshBuild> builds;
+    PBRT_TRY(build_meshes_on_device(c, d, &md, &hv, &hi, &hf, &pre, &builds));
+    pbrt_scene_desc d2 = *d;
+    d2.meshes = md.data();
+    int rc = PBRT_OK;
+    if (!build_scene(d2, &fs, &e, &pre)) rc = c->fail(PBRT_ERR_INVALID_ARGUMENT, e);
+    if (rc == PBRT_OK) rc = upload_scene(c, &d2, fs, out, &builds);
+    for (DeviceMeshBuild& b : builds) free_device_mesh_build(&b);  // those not taken over
+    return rc;
+  }
   if (!build_scene(*d, &fs, &e)) return c->fail(PBRT_ERR_INVALID_ARGUMENT, e);
   return upload_scene(c, d, fs, out);
 }
@@ -315,6 +420,47 @@ void pbrt_scene_destroy(pbrt_scene* s) {
   for (auto& m : s->meshes) free_mesh(m);
   for (void* p : s->allocs) cudaFree(p);
   delete s;
+}
+
+int pbrt_mesh_bvh_build_device(pbrt_ctx* c, const pbrt_mesh_desc* md, uint32_t bins, uint32_t max_leaf, void* nodes,
+                               uint64_t node_capacity, uint32_t* tri_order, uint64_t* node_count, float* build_ms) {
+  if (!c || !md || !node_count) return PBRT_ERR_INVALID_ARGUMENT;
+  DeviceGuard g(c->device);
+  pbrt_scene_desc d{};
+  d.meshes = md;
+  d.mesh_count = 1;
+  d.bvh_bins = bins;
+  d.bvh_max_leaf = max_leaf;
+  std::vector<pbrt_mesh_desc> m2;
+  std::vector<std::vector<float>> hv;
+  std::vector<std::vector<uint32_t>> hi, hf;
+  std::vector<MeshPrebuilt> pre;
+  std::vector<DeviceMeshBuild> b;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (build_ms) {
+    PBRT_TRY(c->cuda(cudaEventCreate(&e0), "cudaEventCreate"));
+    PBRT_TRY(c->cuda(cudaEventCreate(&e1), "cudaEventCreate"));
+    PBRT_TRY(c->cuda(cudaEventRecord(e0, c->stream), "cudaEventRecord"));
+  }
+  int rc = build_meshes_on_device(c, &d, &m2, &hv, &hi, &hf, &pre, &b);
+  if (rc == PBRT_OK && build_ms) {
+    rc = c->cuda(cudaEventRecord(e1, c->stream), "cudaEventRecord");
+    if (rc == PBRT_OK) rc = c->cuda(cudaEventSynchronize(e1), "cudaEventSynchronize");
+    if (rc == PBRT_OK) rc = c->cuda(cudaEventElapsedTime(build_ms, e0, e1), "cudaEventElapsedTime");
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (rc != PBRT_OK) return rc;
+  DeviceMeshBuild& r = b[0];
+  *node_count = r.node_slots;  // 32-byte records, the padding slot included (as the host variant)
+  if (nodes && node_capacity < r.node_slots) rc = PBRT_ERR_CAPACITY;
+  if (rc == PBRT_OK && nodes)
+    rc = c->cuda(cudaMemcpy(nodes, r.nodes, r.node_slots * sizeof(GpuNode), cudaMemcpyDeviceToHost), "cudaMemcpy(nodes)");
+  if (rc == PBRT_OK && nodes && tri_order)
+    rc = c->cuda(cudaMemcpy(tri_order, r.tri_index, size_t(md->triangle_count) * 4, cudaMemcpyDeviceToHost),
+                 "cudaMemcpy(order)");
+  free_device_mesh_build(&r);
+  return rc;
 }
 
 int pbrt_mesh_bvh_build_host(const pbrt_mesh_desc* md, uint32_t bins, uint32_t max_leaf, void* nodes,

@@ -16,6 +16,10 @@ namespace {
 // which only matters for the sign of a zero); inputs are finite (checked before the build).
 inline float mn(float x, float y) { return y < x ? y : x; }
 inline float mx(float x, float y) { return x < y ? y : x; }
+// Stored boxes hold +0 for a zero bound: the sign of a zero bound depends on the order the
+// triangles were met in, and no slab test can tell the two apart (near > 0), so both
+// builders (this one and the GPU's) store the same canonical value.
+inline float canon(float x) { return x == 0.0f ? 0.0f : x; }
 
 struct Box {
   float lo[3], hi[3];
@@ -245,7 +249,7 @@ bool build_mesh_bvh(const float* vertices, uint32_t vertex_count, const uint32_t
   for (size_t k = 0; k < ref.size(); ++k) {
     const RefNode& r = ref[k];
     GpuNode& g = out->nodes[k == 0 ? 0 : k + 1];
-    for (int a = 0; a < 3; ++a) { g.bmin[a] = r.box.lo[a]; g.bmax[a] = r.box.hi[a]; }
+    for (int a = 0; a < 3; ++a) { g.bmin[a] = canon(r.box.lo[a]); g.bmax[a] = canon(r.box.hi[a]); }
     if (r.count > 0) {
       g.left_first = r.left_first;
       g.count = r.count;
@@ -284,6 +288,10 @@ bool build_mesh_bvh(const float* vertices, uint32_t vertex_count, const uint32_t
       out->bounds_min[a] = std::fmin(vertices[3 * size_t(i) + a], out->bounds_min[a]);
       out->bounds_max[a] = std::fmax(vertices[3 * size_t(i) + a], out->bounds_max[a]);
     }
+  for (int a = 0; a < 3; ++a) {
+    out->bounds_min[a] = canon(out->bounds_min[a]);
+    out->bounds_max[a] = canon(out->bounds_max[a]);
+  }
   return true;
 }
 

@@ -397,7 +397,7 @@ class Flattener {
 
 }  // namespace
 
-bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err) {
+bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err, const std::vector<MeshPrebuilt>* pre) {
   if (d.object_count == 0) { *err = "a scene needs at least one object"; return false; }
   if (!d.objects) { *err = "objects is NULL"; return false; }
   if (d.mesh_count && !d.meshes) { *err = "meshes is NULL"; return false; }
@@ -415,7 +415,15 @@ bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err) {
   for (uint32_t i = 0; i < d.mesh_count; ++i) {
     const pbrt_mesh_desc& md = d.meshes[i];
     std::string e;
-    if (!build_mesh_bvh(md.vertices, md.vertex_count, md.indices, md.triangle_count, bp, &out->meshes[i], &e)) {
+    if (pre && i < pre->size() && (*pre)[i].used) {  // built on the GPU: its bounds and statistics
+      const MeshPrebuilt& pb = (*pre)[i];
+      for (int a = 0; a < 3; ++a) {
+        out->meshes[i].bounds_min[a] = pb.bounds_min[a];
+        out->meshes[i].bounds_max[a] = pb.bounds_max[a];
+      }
+      out->meshes[i].stats = pb.stats;
+    } else if (!build_mesh_bvh(md.vertices, md.vertex_count, md.indices, md.triangle_count, bp, &out->meshes[i],
+                               &e)) {
       *err = "mesh " + std::to_string(i) + ": " + e;
       return false;
     }

@@ -46,7 +46,16 @@ struct FlatScene {
   bool has_dielectric = false;  // a dielectric lets paths go on past a cache hit
 };
 
-bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err);
+// A mesh whose BVH was built elsewhere (on the GPU): the scene build takes its bounds and
+// statistics instead of building it.
+struct MeshPrebuilt {
+  bool used = false;
+  float bounds_min[3] = {0, 0, 0}, bounds_max[3] = {0, 0, 0};
+  MeshBuildStats stats;
+};
+
+bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err,
+                 const std::vector<MeshPrebuilt>* prebuilt = nullptr);
 
 // PinHoleCamera::new + Matrix4::look_at in FP32 (src/cameras/pin_hole.rs:17-38,
 // src/geom/matrix4.rs:70-175).

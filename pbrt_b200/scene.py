@@ -498,11 +498,14 @@ class Scene:
             out.update(nodes=nodes, roots=roots)
         return out
 
-    def commit(self, bvh_bins: int = 8, bvh_max_leaf: int = 1) -> "Scene":
+    def commit(self, bvh_bins: int = 8, bvh_max_leaf: int = 1, device_build: bool = False) -> "Scene":
+        """Scene::commit: builds (the meshes' BVHs on the GPU with device_build) and uploads."""
         if self.ctx is None:
             self.ctx = default_context()
         self.release()
         desc = self.describe(bvh_bins, bvh_max_leaf)
+        if device_build:
+            desc = dict(desc, device_build=True)
         sd, keep = _lower_description(desc, bvh_bins, bvh_max_leaf)
         h = C.c_void_p()
         self.ctx.check(self.ctx.lib.pbrt_scene_create(self.ctx.h, C.byref(sd), C.byref(h)), "pbrt_scene_create")
@@ -680,6 +683,7 @@ def _lower_description(desc: dict, bvh_bins: int = 8, bvh_max_leaf: int = 1):
     sd.objects, sd.object_count = C.cast(arrays[2], C.POINTER(_capi.ObjectDesc)), len(objs)
     sd.lights, sd.light_count = C.cast(arrays[3], C.POINTER(_capi.LightDesc)), len(lights)
     sd.bvh_bins, sd.bvh_max_leaf = int(desc.get("bvh_bins", bvh_bins)), int(desc.get("bvh_max_leaf", bvh_max_leaf))
+    sd.device_build = 1 if desc.get("device_build") else 0
     if nodes:
         tree = ((_capi.NodeDesc * len(nodes))(*nodes), (C.c_uint32 * max(1, len(kids)))(*kids),
                 (C.c_uint32 * max(1, len(roots)))(*roots))
@@ -796,6 +800,36 @@ def film_to_rgba8(film: np.ndarray) -> np.ndarray:
 # ------------------------------------------------------------------------------------------
 GPU_NODE_DTYPE = np.dtype([("bmin", np.float32, 3), ("left_first", np.uint32), ("bmax", np.float32, 3),
                            ("count", np.uint32)])
+
+
+def build_mesh_bvh_device(vertices, indices, bvh_bins: int = 8, bvh_max_leaf: int = 1,
+                          ctx: Optional["Context"] = None):
+    """build_mesh_bvh_host on the GPU (pbrt_mesh_bvh_build_device): (nodes, tri_order,
+    build milliseconds). vertices / indices may be numpy arrays or CUDA tensors."""
+    ctx = ctx or default_context()
+    if _is_torch(vertices):
+        v = vertices.contiguous()
+        nv = v.numel() // 3
+    else:
+        v = np.ascontiguousarray(np.asarray(vertices, np.float32).reshape(-1, 3))
+        nv = v.shape[0]
+    if _is_torch(indices):
+        i = indices.contiguous()
+        nt = i.numel() // 3
+    else:
+        i = np.ascontiguousarray(np.asarray(indices, np.uint32).reshape(-1, 3))
+        nt = i.shape[0]
+    md = _capi.MeshDesc(_ptr(v), nv, _ptr(i), nt)
+    cnt = C.c_uint64()
+    ms = C.c_float()
+    ctx.check(ctx.lib.pbrt_mesh_bvh_build_device(ctx.h, C.byref(md), bvh_bins, bvh_max_leaf, None, 0, None,
+                                                 C.byref(cnt), None), "pbrt_mesh_bvh_build_device")
+    nodes = np.zeros(cnt.value, GPU_NODE_DTYPE)
+    order = np.zeros(nt, np.uint32)
+    ctx.check(ctx.lib.pbrt_mesh_bvh_build_device(ctx.h, C.byref(md), bvh_bins, bvh_max_leaf, nodes.ctypes.data,
+                                                 cnt.value, order.ctypes.data, C.byref(cnt), C.byref(ms)),
+              "pbrt_mesh_bvh_build_device")
+    return nodes, order, float(ms.value)
 
 
 def build_mesh_bvh_host(vertices, indices, bvh_bins: int = 8, bvh_max_leaf: int = 1):
