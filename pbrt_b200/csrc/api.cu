@@ -383,6 +383,30 @@ int pbrt_scene_create_many(pbrt_ctx* c, const pbrt_scene_desc* descs, uint32_t n
   DeviceGuard g(c->device);
   for (uint32_t i = 0; i < n; ++i) out[i] = nullptr;
   for (uint32_t i = 0; i < n; ++i) PBRT_TRY(check_scene_desc(c, descs + i));
+  // GPU mesh builds first (device_build scenes), one scene after another on the context's stream
+  struct DevParts {
+    std::vector<pbrt_mesh_desc> md;
+    std::vector<std::vector<float>> hv;
+    std::vector<std::vector<uint32_t>> hi, hf;
+    std::vector<MeshPrebuilt> pre;
+    std::vector<DeviceMeshBuild> builds;
+  };
+  std::vector<DevParts> parts(n);
+  std::vector<pbrt_scene_desc> d2(descs, descs + n);
+  auto free_builds = [&]() {
+    for (DevParts& p : parts)
+      for (DeviceMeshBuild& b : p.builds) free_device_mesh_build(&b);
+  };
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!descs[i].device_build || !descs[i].mesh_count) continue;
+    DevParts& p = parts[i];
+    const int rc = build_meshes_on_device(c, descs + i, &p.md, &p.hv, &p.hi, &p.hf, &p.pre, &p.builds);
+    if (rc != PBRT_OK) {
+      free_builds();
+      return rc;
+    }
+    d2[i].meshes = p.md.data();
+  }
   // host builds on a pool of threads (no device calls), then uploads in order
   std::vector<FlatScene> flat(n);
   std::vector<std::string> errs(n);
@@ -391,25 +415,31 @@ int pbrt_scene_create_many(pbrt_ctx* c, const pbrt_scene_desc* descs, uint32_t n
   unsigned T = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
   T = std::min<unsigned>(T, n);
   auto work = [&]() {
-    for (uint32_t i = next++; i < n; i = next++) ok[i] = build_scene(descs[i], &flat[i], &errs[i]) ? 1 : 0;
+    for (uint32_t i = next++; i < n; i = next++)
+      ok[i] = build_scene(d2[i], &flat[i], &errs[i], parts[i].pre.empty() ? nullptr : &parts[i].pre) ? 1 : 0;
   };
   std::vector<std::thread> pool;
   for (unsigned t = 1; t < T; ++t) pool.emplace_back(work);
   work();
   for (std::thread& t : pool) t.join();
   for (uint32_t i = 0; i < n; ++i)
-    if (!ok[i]) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "scene " + std::to_string(i) + ": " + errs[i]);
+    if (!ok[i]) {
+      free_builds();
+      return c->fail(PBRT_ERR_INVALID_ARGUMENT, "scene " + std::to_string(i) + ": " + errs[i]);
+    }
   for (uint32_t i = 0; i < n; ++i) {
-    const int rc = upload_scene(c, descs + i, flat[i], out + i);
+    const int rc = upload_scene(c, &d2[i], flat[i], out + i, parts[i].builds.empty() ? nullptr : &parts[i].builds);
     if (rc != PBRT_OK) {
       for (uint32_t j = 0; j < i; ++j) {
         pbrt_scene_destroy(out[j]);
         out[j] = nullptr;
       }
+      free_builds();
       return rc;
     }
     FlatScene().meshes.swap(flat[i].meshes);  // release host copies as we go
   }
+  free_builds();  // anything not taken over
   return PBRT_OK;
 }
 

@@ -33,7 +33,7 @@ namespace pbrt {
 namespace {
 
 constexpr uint32_t kNone = 0xFFFFFFFFu;
-constexpr uint32_t kSmall = 512;     // subtrees of at most this many triangles: one thread each
+constexpr uint32_t kSmall = 96;      // subtrees of at most this many triangles: one thread each
 constexpr uint32_t kChunk = 2048;    // elements per block in the level kernels
 constexpr int kLevelThreads = 256;
 constexpr int kMaxBins = 64;
@@ -67,6 +67,10 @@ struct Chunk {
 
 struct SmallJob {
   uint32_t pool, first, count, depth, buf;
+};
+
+struct LevelResult {  // what the host needs back from a level: the split and the children
+  uint32_t split, nl, child, pad;
 };
 
 // ---- FP32 helpers (the host builder's expressions) ----------------------------------------
@@ -385,10 +389,11 @@ __global__ void k_classify(const TriRec* __restrict__ t, const LevelNode* __rest
 
 // per node: the chunks' offsets in the lefts' order and nl; the children's places
 __global__ void k_chunk_offsets(LevelNode* nodes, uint32_t nn, const uint32_t* __restrict__ cfirst,
-                                uint32_t* chunk_tot, PoolNode* pool, uint32_t* pool_count) {
+                                uint32_t* chunk_tot, PoolNode* pool, uint32_t* pool_count, LevelResult* res) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nn) return;
   LevelNode& nd = nodes[j];
+  res[j] = LevelResult{0, 0, kNone, 0};
   uint32_t run = 0;
   for (uint32_t c = cfirst[j]; c < cfirst[j + 1]; ++c) {
     const uint32_t v = chunk_tot[c];
@@ -407,6 +412,7 @@ __global__ void k_chunk_offsets(LevelNode* nodes, uint32_t nn, const uint32_t* _
   }
   const uint32_t c = atomicAdd(pool_count, 2u);
   nd.child = c;
+  res[j] = LevelResult{1, run, c, 0};
   pool[nd.pool].child = c;
   pool[nd.pool].count = 0;
   PoolNode l{}, r{};
@@ -773,6 +779,7 @@ bool build_mesh_bvh_device(const float* d_v, uint32_t nv, const uint32_t* d_idx,
     small.push_back(SmallJob{0, 0, n, 1, 0});
   }
   LevelNode* d_nodes = nullptr;
+  LevelResult* d_res = nullptr;
   Chunk* d_chunks = nullptr;
   uint32_t *d_cfirst = nullptr, *d_ctot = nullptr, *d_bins = nullptr;
   size_t cap_nodes = 0, cap_chunks = 0;
@@ -792,6 +799,7 @@ bool build_mesh_bvh_device(const float* d_v, uint32_t nv, const uint32_t* d_idx,
     if (nn > cap_nodes) {
       cap_nodes = std::max<size_t>(nn, 2 * cap_nodes);
       BUILD_TRY(s.alloc(&d_nodes, cap_nodes));
+      BUILD_TRY(s.alloc(&d_res, cap_nodes));
       BUILD_TRY(s.alloc(&d_cfirst, cap_nodes + 1));
       BUILD_TRY(s.alloc(&d_bins, cap_nodes * 3 * B * 7));
     }
@@ -810,7 +818,7 @@ bool build_mesh_bvh_device(const float* d_v, uint32_t nv, const uint32_t* d_idx,
     k_bins<<<nc, kLevelThreads, 0, st>>>(tc, d_nodes, d_chunks, d_bins, B);
     k_sah<<<(nn + 63) / 64, 64, 0, st>>>(d_nodes, nn, d_bins, B, p.max_leaf, pool);
     k_classify<<<nc, kLevelThreads, 0, st>>>(tc, d_nodes, d_chunks, ord, d_ctot, B);
-    k_chunk_offsets<<<(nn + 127) / 128, 128, 0, st>>>(d_nodes, nn, d_cfirst, d_ctot, pool, flags + 1);
+    k_chunk_offsets<<<(nn + 127) / 128, 128, 0, st>>>(d_nodes, nn, d_cfirst, d_ctot, pool, flags + 1, d_res);
     k_scatter<<<nc, kLevelThreads, 0, st>>>(d_nodes, d_chunks, d_ctot, ord, pos);
     BUILD_TRY(cudaGetLastError());
     for (int round = 0; round < 40; ++round) {
@@ -826,23 +834,26 @@ bool build_mesh_bvh_device(const float* d_v, uint32_t nv, const uint32_t* d_idx,
     k_child_box<<<nc, kLevelThreads, 0, st>>>(tn, d_nodes, d_chunks);
     k_child_finalize<<<(nn + 127) / 128, 128, 0, st>>>(d_nodes, nn, pool);
     BUILD_TRY(cudaGetLastError());
-    BUILD_TRY(cudaMemcpyAsync(level.data(), d_nodes, nn * sizeof(LevelNode), cudaMemcpyDeviceToHost, st));
+    std::vector<LevelResult> res(nn);
+    BUILD_TRY(cudaMemcpyAsync(res.data(), d_res, nn * sizeof(LevelResult), cudaMemcpyDeviceToHost, st));
     BUILD_TRY(cudaStreamSynchronize(st));
     std::vector<LevelNode> next;
-    for (const LevelNode& nd : level) {
-      if (!nd.split) continue;
-      const uint32_t cnt[2] = {nd.nl, nd.count - nd.nl};
-      const uint32_t fst[2] = {nd.first, nd.first + nd.nl};
+    for (uint32_t j = 0; j < nn; ++j) {
+      const LevelNode& nd = level[j];
+      const LevelResult& r = res[j];
+      if (!r.split) continue;
+      const uint32_t cnt[2] = {r.nl, nd.count - r.nl};
+      const uint32_t fst[2] = {nd.first, nd.first + r.nl};
       for (int side = 0; side < 2; ++side) {
         if (cnt[side] > kSmall && cnt[side] > p.max_leaf) {
           LevelNode c{};
-          c.pool = nd.child + side;
+          c.pool = r.child + side;
           c.first = fst[side];
           c.count = cnt[side];
           c.depth = nd.depth + 1;
           next.push_back(c);
         } else {
-          small.push_back(SmallJob{nd.child + uint32_t(side), fst[side], cnt[side], nd.depth + 1, uint32_t(cur ^ 1)});
+          small.push_back(SmallJob{r.child + uint32_t(side), fst[side], cnt[side], nd.depth + 1, uint32_t(cur ^ 1)});
         }
       }
     }

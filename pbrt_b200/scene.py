@@ -696,10 +696,13 @@ def _lower_description(desc: dict, bvh_bins: int = 8, bvh_max_leaf: int = 1):
 
 
 def create_scenes(descs, ctx: Optional[Context] = None, threads: int = 0, bvh_bins: int = 8,
-                  bvh_max_leaf: int = 1) -> list:
+                  bvh_max_leaf: int = 1, device_build: bool = False) -> list:
     """Committed Scenes of many descriptions at once: the host-side BVH builds run on
-    `threads` threads (0: all cores) inside pbrt_scene_create_many."""
+    `threads` threads (0: all cores) inside pbrt_scene_create_many; with device_build the
+    meshes' BVHs are built on the GPU instead."""
     ctx = ctx or default_context()
+    if device_build:
+        descs = [dict(d, device_build=True) for d in descs]
     lowered = [_lower_description(d, bvh_bins, bvh_max_leaf) for d in descs]
     arr = (_capi.SceneDesc * len(lowered))(*[sd for sd, _ in lowered])
     hs = (C.c_void_p * len(lowered))()

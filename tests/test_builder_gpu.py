@@ -101,3 +101,12 @@ def test_scene_device_build_renders_identically():
     np.testing.assert_array_equal(t1, t2)
     assert st1 == st2
     assert s1.info()["mesh_node_count"] == s2.info()["mesh_node_count"]
+
+
+def test_create_scenes_with_device_builds():
+    from pbrt_b200.scene import create_scenes
+    specs = workloads.batch_scenes(3, seed=11, width=32, height=32, levels=(3, 6))
+    host = create_scenes([d for d, _, _ in specs], bvh_max_leaf=2)
+    dev = create_scenes([d for d, _, _ in specs], bvh_max_leaf=2, device_build=True)
+    for a, b, (_, cam, spp) in zip(host, dev, specs):
+        np.testing.assert_array_equal(a.render(cam, spp=2, max_depth=4, seed=1), b.render(cam, spp=2, max_depth=4, seed=1))
