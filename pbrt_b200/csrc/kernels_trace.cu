@@ -190,8 +190,11 @@ PBRT_DEV bool pop_next(TraversalStack& s, int& sp, float min_t, uint32_t& lf, ui
   return false;
 }
 
+// 12 resident blocks of 128 threads per SM (at most 40 registers a thread): the traversal is
+// latency-bound, and the extra warps hide more of it than the few spilled registers cost
+// (measured: 1.01 ms against 1.10 ms at the compiler's 72 registers for the 16M-ray step).
 template <bool kRec>
-__global__ void __launch_bounds__(128) k_mesh_closest_persistent(MeshView m, const float* __restrict__ rays,
+__global__ void __launch_bounds__(128, 12) k_mesh_closest_persistent(MeshView m, const float* __restrict__ rays,
                                                                  uint64_t stride, const uint32_t* __restrict__ queue,
                                                                  const unsigned long long* __restrict__ queue_count,
                                                                  uint32_t* __restrict__ prim,
