@@ -80,9 +80,28 @@ typedef enum pbrt_shape_kind {
   PBRT_SHAPE_RECTANGLE = 3, /* Rectangle::new(width = `radius`, height = `height`): the y = 0 plane within
                                |x| <= width/2, |z| <= height/2, facing +y (src/shapes/rectangle.rs:9-70) */
   PBRT_SHAPE_AABOX = 4,     /* AABox::new(`extent`): the box [-extent/2, extent/2] (src/shapes/aabox.rs:9-203) */
-  PBRT_SHAPE_PLANE = 5      /* Plane: the y = 0 plane, unbounded (src/shapes/plane.rs:9-94); an unbounded
+  PBRT_SHAPE_PLANE = 5,     /* Plane: the y = 0 plane, unbounded (src/shapes/plane.rs:9-94); an unbounded
                                primitive is kept out of the scene BVH and tested first (src/scene.rs:101-115) */
+  PBRT_SHAPE_CSG = 6        /* a constructive solid over csg_elems[csg_first .. + csg_count) with csg_op
+                               (src/shapes/csg.rs, csg/{union,intersection,substraction}.rs) */
 } pbrt_shape_kind;
+
+typedef enum pbrt_csg_op {
+  PBRT_CSG_UNION = 0,        /* hits of each element outside every other element */
+  PBRT_CSG_INTERSECTION = 1, /* hits of each element inside every other element */
+  PBRT_CSG_SUBTRACTION = 2   /* the first element's hits outside the others, the others' hits inside the
+                                first and outside the rest, their normals reversed */
+} pbrt_csg_op;
+
+/* One element of a constructive solid (csg::Elem, src/shapes/csg.rs:7-10): a plain shape
+ * (not PBRT_SHAPE_CSG) with the sizes of pbrt_object_desc, placed by its transform. */
+typedef struct pbrt_csg_elem_desc {
+  uint32_t shape;
+  uint32_t mesh;
+  float radius, height;
+  float extent[3];
+  float to_world[12], to_local[12];
+} pbrt_csg_elem_desc;
 
 typedef enum pbrt_texture_kind {
   PBRT_TEXTURE_COLOR = 0,       /* PlainColor(color) (src/textures/plain_color.rs) */
@@ -142,6 +161,7 @@ typedef struct pbrt_object_desc {
   float to_world[12];      /* row-major 3x4 of Transform::mat (src/geom/transform.rs:7-10) */
   float to_local[12];      /* row-major 3x4 of Transform::inv_mat */
   float extent[3];         /* aabox: full size along x, y, z */
+  uint32_t csg_op, csg_first, csg_count; /* PBRT_SHAPE_CSG: pbrt_csg_op and the elements */
 } pbrt_object_desc;
 
 /* One node of an object tree (the Object trait objects a scene file builds,
@@ -191,6 +211,9 @@ typedef struct pbrt_scene_desc {
   /* 1: build the meshes' BVHs on the GPU (the same trees and triangle order as the host
    * build); mesh arrays (vertices, indices, face_materials) may then be device memory. */
   uint32_t device_build;
+  /* The elements of the constructive solids among the objects. */
+  const pbrt_csg_elem_desc* csg_elems;
+  uint32_t csg_elem_count;
 } pbrt_scene_desc;
 
 /* Builds the acceleration structures on the host and uploads the scene. Replaces
@@ -242,7 +265,9 @@ int pbrt_scene_get_info(const pbrt_scene* scene, pbrt_scene_info* info);
 /* Nearest hit per ray: replaces Scene::intersect (src/scene.rs:118-120, 186-220) and, for
  * a scene made of one untransformed mesh, TriangleMesh::intersect / BVHTree::query
  * (src/shapes/triangle_mesh/triangle_mesh.rs:73-132, bvh.rs:350-352, 450-526).
- * prim_id: triangle index within its mesh (or 0 for an analytic shape), PBRT_MISS on a miss.
+ * prim_id: triangle index within its mesh, cylinder piece (0 wall, 1 bottom, 2 top), box face
+ * (0..5: -x, +x, -y, +y, -z, +z), for a constructive solid element << 24 | that element's
+ * prim_id; 0 for the other shapes; PBRT_MISS on a miss.
  * t: hit distance, +inf on a miss. object_id may be NULL. */
 int pbrt_trace_closest(pbrt_scene* scene, const float* rays, uint64_t n, uint32_t* prim_id, float* t,
                        uint32_t* object_id);
@@ -460,8 +485,8 @@ typedef struct pbrt_stage_options {
 } pbrt_stage_options;
 
 /* Parses `text` (a whole scene file) and reads its meshes. On failure returns
- * PBRT_ERR_INVALID_ARGUMENT (a file the reference's parser rejects, or a shape outside the
- * ported set: constructive solids) or PBRT_ERR_UNSUPPORTED, with a message in err. */
+ * PBRT_ERR_INVALID_ARGUMENT (a file the reference's parser rejects) or PBRT_ERR_UNSUPPORTED
+ * (a constructive solid nested in another), with a message in err. */
 int pbrt_stage_parse(const char* text, const pbrt_stage_options* options, pbrt_stage** out, char* err,
                      size_t err_len);
 /* The scene description (pointing into arrays the stage owns, valid until

@@ -203,9 +203,12 @@ def make_ray(origin, direction, dtype=np.float64):
 #   materials: [{"kind": 0 lambertian | 1 metal | 2 dielectric | 3 diffuse light,
 #                "color": (3,), "fuzz": f, "ior": f,
 #                optional "texture": 1 checkerboard with "color2": (3,), "scale": f}]
-#   objects:   [{"shape": 0 mesh | 1 sphere | 2 cylinder | 3 rectangle | 4 aabox | 5 plane,
+#   objects:   [{"shape": 0 mesh | 1 sphere | 2 cylinder | 3 rectangle | 4 aabox | 5 plane | 6 csg,
 #                "mesh": i, "radius": r, "height": h, "extent": (3,), "material": i,
-#                "to_world": (12,) or None, "to_local": (12,) or None}]
+#                "to_world": (12,) or None, "to_local": (12,) or None,
+#                csg: "csg": {"op": 0 union | 1 intersection | 2 subtraction,
+#                             "elements": [{"shape", "mesh", "radius", "height", "extent",
+#                                           "to_world", "to_local"}]}}]
 #              (rectangle: radius = width, height = height; aabox: extent = full size)
 #   lights:    [{"kind": 0 point | 1 uniform infinite | 2 background | 3 area, "position": (3,),
 #                "radiance": (3,), "bottom": (3,), "top": (3,), "object": i}]
@@ -230,7 +233,13 @@ class _OMaterial(C.Structure):
 class _OObject(C.Structure):
     _fields_ = [("shape", C.c_uint32), ("mesh", C.c_uint32), ("radius", C.c_double), ("height", C.c_double),
                 ("extent", C.c_double * 3), ("material", C.c_uint32), ("transformed", C.c_uint32),
-                ("to_world", C.c_double * 12), ("to_local", C.c_double * 12)]
+                ("to_world", C.c_double * 12), ("to_local", C.c_double * 12), ("csg_op", C.c_uint32),
+                ("csg_first", C.c_uint32), ("csg_count", C.c_uint32)]
+
+
+class _OCsgElem(C.Structure):
+    _fields_ = [("shape", C.c_uint32), ("mesh", C.c_uint32), ("radius", C.c_double), ("height", C.c_double),
+                ("extent", C.c_double * 3), ("to_world", C.c_double * 12), ("to_local", C.c_double * 12)]
 
 
 class _ONode(C.Structure):
@@ -249,7 +258,7 @@ class _OScene(C.Structure):
                 ("lights", C.c_void_p), ("light_count", C.c_uint32), ("bvh_bins", C.c_uint32),
                 ("bvh_max_leaf", C.c_uint32), ("nodes", C.c_void_p), ("node_count", C.c_uint32),
                 ("children", C.c_void_p), ("child_count", C.c_uint32), ("roots", C.c_void_p),
-                ("root_count", C.c_uint32)]
+                ("root_count", C.c_uint32), ("csg_elems", C.c_void_p), ("csg_elem_count", C.c_uint32)]
 
 
 class _OCamera(C.Structure):
@@ -337,7 +346,7 @@ class Scene:
             d.color2[:] = [float(c) for c in m.get("color2", (0, 0, 0))]
             d.scale = float(m.get("scale", 1.0))
             mats.append(d)
-        objs = []
+        objs, celems = [], []
         for o in desc.get("objects", []):
             d = _OObject()
             d.shape, d.mesh = int(o["shape"]), int(o.get("mesh", 0))
@@ -348,6 +357,16 @@ class Scene:
                 d.transformed = 1
                 d.to_world[:] = _xf12(o["to_world"])
                 d.to_local[:] = _xf12(o["to_local"])
+            if o.get("csg") is not None:
+                d.csg_op, d.csg_first, d.csg_count = int(o["csg"]["op"]), len(celems), len(o["csg"]["elements"])
+                for e in o["csg"]["elements"]:
+                    c = _OCsgElem()
+                    c.shape, c.mesh = int(e["shape"]), int(e.get("mesh", 0))
+                    c.radius, c.height = float(e.get("radius", 0.0)), float(e.get("height", 0.0))
+                    c.extent[:] = [float(x) for x in e.get("extent", (0.0, 0.0, 0.0))]
+                    c.to_world[:] = _xf12(e["to_world"])
+                    c.to_local[:] = _xf12(e["to_local"])
+                    celems.append(c)
             objs.append(d)
         nodes, kids = [], []
         for n in desc.get("nodes", []) or []:
@@ -373,12 +392,12 @@ class Scene:
         arrs = [(_OMesh * max(1, len(ms)))(*ms), (_OMaterial * max(1, len(mats)))(*mats),
                 (_OObject * max(1, len(objs)))(*objs), (_OLight * max(1, len(lts)))(*lts),
                 (_ONode * max(1, len(nodes)))(*nodes), (C.c_uint32 * max(1, len(kids)))(*kids),
-                (C.c_uint32 * max(1, len(roots)))(*roots)]
+                (C.c_uint32 * max(1, len(roots)))(*roots), (_OCsgElem * max(1, len(celems)))(*celems)]
         self._keep += arrs
         sd = _OScene(C.addressof(arrs[0]), len(ms), C.addressof(arrs[1]), len(mats), C.addressof(arrs[2]), len(objs),
                      C.addressof(arrs[3]), len(lts), int(desc.get("bvh_bins", 8)), int(desc.get("bvh_max_leaf", 1)),
                      C.addressof(arrs[4]) if nodes else None, len(nodes), C.addressof(arrs[5]), len(kids),
-                     C.addressof(arrs[6]), len(roots))
+                     C.addressof(arrs[6]), len(roots), C.addressof(arrs[7]), len(celems))
         self._h = getattr(L, f"oracle_scene_new_{self.suf}")(C.byref(sd))
         if not self._h:
             raise ValueError(L.oracle_last_error().decode())

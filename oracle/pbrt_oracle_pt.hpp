@@ -117,7 +117,8 @@ struct Affine {
 // product's C description)
 // ---------------------------------------------------------------------------------------
 enum { O_SHAPE_MESH = 0, O_SHAPE_SPHERE = 1, O_SHAPE_CYLINDER = 2, O_SHAPE_RECTANGLE = 3, O_SHAPE_AABOX = 4,
-       O_SHAPE_PLANE = 5 };
+       O_SHAPE_PLANE = 5, O_SHAPE_CSG = 6 };
+enum { O_CSG_UNION = 0, O_CSG_INTERSECTION = 1, O_CSG_SUBTRACTION = 2 };
 enum { O_MAT_LAMBERTIAN = 0, O_MAT_METAL = 1, O_MAT_DIELECTRIC = 2, O_MAT_DIFFUSE_LIGHT = 3 };
 enum { O_LIGHT_POINT = 0, O_LIGHT_UNIFORM = 1, O_LIGHT_BACKGROUND = 2, O_LIGHT_AREA = 3 };
 enum { O_TEX_PLAIN = 0, O_TEX_CHECKERBOARD = 1 };
@@ -146,6 +147,15 @@ struct OObjectDesc {
   double radius, height;
   double extent[3];
   uint32_t material, transformed;
+  double to_world[12], to_local[12];
+  uint32_t csg_op, csg_first, csg_count;  // O_SHAPE_CSG: csg_elems[csg_first .. + csg_count)
+};
+// One element of a constructive solid (csg::Elem, src/shapes/csg.rs:7-10): a shape (any but
+// O_SHAPE_CSG) placed by its transform.
+struct OCsgElemDesc {
+  uint32_t shape, mesh;
+  double radius, height;
+  double extent[3];
   double to_world[12], to_local[12];
 };
 // Object tree of a scene file (src/objects/*.rs): SIMPLE names an object; TRANSFORMED wraps
@@ -176,6 +186,8 @@ struct OSceneDesc {
   uint32_t child_count;
   const uint32_t* roots;  // the scene's primitives in Scene::add_object order
   uint32_t root_count;
+  const OCsgElemDesc* csg_elems;
+  uint32_t csg_elem_count;
 };
 struct OCameraDesc {
   uint32_t width, height;
@@ -226,6 +238,7 @@ class OScene {
     V3<R> amin, amax;               // aabox (AABox::new: min = 0 - extent/2, max = extent/2)
     bool transformed;
     Affine<R> mat, inv;
+    uint32_t csg_op = 0, csg_first = 0, csg_count = 0;
   };
   struct Material {
     uint32_t kind;
@@ -284,25 +297,29 @@ class OScene {
           if (m.texture == O_TEX_CHECKERBOARD) max_radiance = std::max(max_radiance, m.color2[c]);
         }
     }
+    for (uint32_t i = 0; i < d.csg_elem_count; ++i) {
+      const OCsgElemDesc& e = d.csg_elems[i];
+      Object ob = shape_object(e.shape, e.mesh, e.radius, e.height, e.extent);
+      ob.transformed = true;
+      ob.mat = affine(e.to_world);
+      ob.inv = affine(e.to_local);
+      if (ob.shape > O_SHAPE_PLANE) throw std::invalid_argument("a csg element is a plain shape");
+      celems.push_back(ob);
+    }
     for (uint32_t i = 0; i < d.object_count; ++i) {
       const OObjectDesc& o = d.objects[i];
-      Object ob{};
-      ob.shape = o.shape;
-      ob.mesh = o.mesh;
+      Object ob = shape_object(o.shape, o.mesh, o.radius, o.height, o.extent);
       ob.material = o.material;
-      ob.radius = R(o.radius);
-      ob.height = R(o.height);
-      ob.half_height = R(o.height) / R(2);  // Cylinder::new (cylinder.rs:12-19)
-      ob.half_w = R(o.radius) / R(2);       // Rectangle::new(width, height) (rectangle.rs:15-20)
-      ob.half_h = R(o.height) / R(2);
-      const V3<R> half = V3<R>{R(o.extent[0]), R(o.extent[1]), R(o.extent[2])} * R(0.5);  // AABox::new
-      ob.amin = V3<R>{R(0), R(0), R(0)} - half;
-      ob.amax = half;
       ob.transformed = o.transformed != 0;
       ob.mat = affine(o.to_world);
       ob.inv = affine(o.to_local);
-      if (ob.shape > O_SHAPE_PLANE) throw std::invalid_argument("unknown shape");
-      if (ob.shape == O_SHAPE_MESH && ob.mesh >= meshes.size()) throw std::invalid_argument("bad mesh index");
+      ob.csg_op = o.csg_op;
+      ob.csg_first = o.csg_first;
+      ob.csg_count = o.csg_count;
+      if (ob.shape > O_SHAPE_CSG) throw std::invalid_argument("unknown shape");
+      if (ob.shape == O_SHAPE_CSG &&
+          (o.csg_op > O_CSG_SUBTRACTION || uint64_t(o.csg_first) + o.csg_count > celems.size()))
+        throw std::invalid_argument("bad csg object");
       if (ob.material >= materials.size()) throw std::invalid_argument("bad material index");
       objects.push_back(ob);
     }
@@ -362,6 +379,22 @@ class OScene {
     commit();
   }
 
+  Object shape_object(uint32_t shape, uint32_t mesh, double radius, double height, const double* extent) const {
+    Object ob{};
+    ob.shape = shape;
+    ob.mesh = mesh;
+    ob.radius = R(radius);
+    ob.height = R(height);
+    ob.half_height = R(height) / R(2);  // Cylinder::new (cylinder.rs:12-19)
+    ob.half_w = R(radius) / R(2);       // Rectangle::new(width, height) (rectangle.rs:15-20)
+    ob.half_h = R(height) / R(2);
+    const V3<R> half = V3<R>{R(extent[0]), R(extent[1]), R(extent[2])} * R(0.5);  // AABox::new
+    ob.amin = V3<R>{R(0), R(0), R(0)} - half;
+    ob.amax = half;
+    if (shape == O_SHAPE_MESH && mesh >= meshes.size()) throw std::invalid_argument("bad mesh index");
+    return ob;
+  }
+
   // A node may be shared (the reference holds objects in Arc), but the tree may not loop.
   void check_acyclic() const {
     std::vector<int> state(nodes.size(), 0);
@@ -403,8 +436,205 @@ class OScene {
         return AABB<R>{{-o.radius, -o.half_height, -o.radius}, {o.radius, o.half_height, o.radius}};
       case O_SHAPE_RECTANGLE: return AABB<R>{{-o.half_w, R(0), -o.half_h}, {o.half_w, R(0), o.half_h}};
       case O_SHAPE_AABOX: return AABB<R>{o.amin, o.amax};
+      case O_SHAPE_CSG: return csg_box(o);
       default: return AABB<R>{{-inf, -inf, -inf}, {inf, R(0), inf}};  // Plane (plane.rs:89-93)
     }
+  }
+
+  // get_bounding_box of a constructive solid: Union the union of its elements' boxes
+  // (union.rs:56-70), Intersection their intersection (intersection.rs:57-71), Subtraction the
+  // first element's (substraction.rs:97-108); no element: the point box at the origin
+  AABB<R> csg_box(const Object& o) const {
+    if (o.csg_count == 0) return AABB<R>{{R(0), R(0), R(0)}, {R(0), R(0), R(0)}};
+    const Object& e0 = celems[o.csg_first];
+    AABB<R> b = transform_box(shape_box(e0), e0.mat);
+    if (o.csg_op == O_CSG_SUBTRACTION) return b;
+    for (uint32_t k = 1; k < o.csg_count; ++k) {
+      const Object& e = celems[o.csg_first + k];
+      const AABB<R> x = transform_box(shape_box(e), e.mat);
+      if (o.csg_op == O_CSG_UNION) {
+        b.combine(x);
+      } else {  // intersect_with (aabound.rs:397-401): maximize the mins, minimize the maxes
+        b.bmin = {rmax(b.bmin.x, x.bmin.x), rmax(b.bmin.y, x.bmin.y), rmax(b.bmin.z, x.bmin.z)};
+        b.bmax = {rmin(b.bmax.x, x.bmax.x), rmin(b.bmax.y, x.bmax.y), rmin(b.bmax.z, x.bmax.z)};
+      }
+    }
+    return b;
+  }
+
+  // contain_point of a plain shape: sphere.rs:146-148, cylinder.rs:119-124, aabox.rs:192-199,
+  // plane.rs:47-52; a rectangle and a mesh enclose nothing
+  static bool contains(const Object& s, const V3<R>& p) {
+    switch (s.shape) {
+      case O_SHAPE_SPHERE: return dot(p, p) <= s.radius * s.radius;
+      case O_SHAPE_CYLINDER:
+        return p.x * p.x + p.z * p.z <= s.radius * s.radius && p.y >= -s.half_height && p.y <= s.half_height;
+      case O_SHAPE_AABOX:
+        return p.x >= s.amin.x && p.x <= s.amax.x && p.y >= s.amin.y && p.y <= s.amax.y && p.z >= s.amin.z &&
+               p.z <= s.amax.z;
+      case O_SHAPE_PLANE: return p.y <= R(0);
+      default: return false;
+    }
+  }
+
+  // Every hit a plain shape lists (its IntersectionResult, in order): distances and pieces
+  // (triangle, cylinder piece, box face)
+  int shape_hits(const Object& s, const Ray<R>& r, R near, R far, R* ts, uint32_t* ps) const {
+    R t;
+    int piece;
+    switch (s.shape) {
+      case O_SHAPE_MESH: {
+        TriHit<R> th;
+        uint32_t tri;
+        TraversalStats st;
+        if (!meshes[s.mesh].bvh->traverse(r, near, far, &th, &tri, &st)) return 0;
+        ts[0] = th.t;
+        ps[0] = tri;
+        return 1;
+      }
+      case O_SHAPE_SPHERE: {  // sphere.rs:108-144: the entry beyond near, the exit inside (near, far)
+        const V3<R> l = r.o * R(-1);
+        const R tca = dot(l, r.d);
+        if (tca < R(0)) return 0;
+        const R r2 = s.radius * s.radius;
+        const R d2 = dot(l, l) - tca * tca;
+        if (d2 > r2) return 0;
+        const R thc = std::sqrt(r2 - d2);
+        const R t0 = tca - thc, t1 = tca + thc;
+        const R tmin = rmin(t0, t1), tmax = rmax(t0, t1);
+        if (tmax < near || tmin > far) return 0;
+        int n = 0;
+        if (tmin > near) { ts[n] = tmin; ps[n] = 0; ++n; }
+        if (tmax > near && tmax < far) { ts[n] = tmax; ps[n] = 0; ++n; }
+        return n;
+      }
+      case O_SHAPE_CYLINDER: {  // cylinder.rs:28-110, the list sorted by distance (stable)
+        const V3<R>& org = r.o;
+        const V3<R>& dir = r.d;
+        const R a = dir.x * dir.x + dir.z * dir.z;
+        const R b = R(2) * (org.x * dir.x + org.z * dir.z);
+        const R c = org.x * org.x + org.z * org.z - s.radius * s.radius;
+        const R disc = b * b - R(4) * a * c;
+        if (disc < R(0)) return 0;
+        const R rd = std::sqrt(disc);
+        const R q = b < R(0) ? R(-0.5) * (b - rd) : R(-0.5) * (b + rd);
+        const R q0 = q / a, q1 = c / q;
+        const R tmin = rmin(q0, q1), tmax = rmax(q0, q1);
+        if (tmax < near || tmin > far) return 0;
+        int n = 0;
+        if (tmin > near) {
+          const V3<R> p = org + dir * tmin;
+          if (p.y > -s.half_height && p.y < s.half_height) { ts[n] = tmin; ps[n] = 0; n++; }
+        }
+        if (tmax > near && tmax < far) {
+          const V3<R> p = org + dir * tmax;
+          if (p.y > -s.half_height && p.y < s.half_height) { ts[n] = tmax; ps[n] = 0; n++; }
+        }
+        if (n < 2) {
+          const R iy = R(1) / dir.y;
+          const R c0 = (-s.half_height - org.y) * iy;
+          if (c0 > near && c0 < far) {
+            const V3<R> p = org + dir * c0;
+            if (p.x * p.x + p.z * p.z <= s.radius * s.radius) { ts[n] = c0; ps[n] = 1; n++; }
+          }
+          const R c1 = (s.half_height - org.y) * iy;
+          if (c1 > near && c1 < far) {
+            const V3<R> p = org + dir * c1;
+            if (p.x * p.x + p.z * p.z <= s.radius * s.radius) { ts[n] = c1; ps[n] = 2; n++; }
+          }
+        }
+        for (int i = 1; i < n; ++i)  // insertion sort: stable
+          for (int j = i; j > 0 && ts[j] < ts[j - 1]; --j) {
+            std::swap(ts[j], ts[j - 1]);
+            std::swap(ps[j], ps[j - 1]);
+          }
+        return n;
+      }
+      case O_SHAPE_RECTANGLE:
+        if (!rectangle_hit(s, r, near, far, &t)) return 0;
+        ts[0] = t;
+        ps[0] = 0;
+        return 1;
+      case O_SHAPE_PLANE:
+        if (!plane_hit(r, near, far, &t)) return 0;
+        ts[0] = t;
+        ps[0] = 0;
+        return 1;
+      default: {  // AABox (aabox.rs:76-190): the entry beyond near, the exit before far
+        (void)piece;
+        R tmin, tmax;
+        int fmin, fmax;
+        if (!aabox_span(s, r, &tmin, &tmax, &fmin, &fmax)) return 0;
+        if (tmax < near || tmin > far) return 0;
+        int n = 0;
+        if (tmin > near) { ts[n] = tmin; ps[n] = uint32_t(fmin); ++n; }
+        if (tmax < far) { ts[n] = tmax; ps[n] = uint32_t(fmax); ++n; }
+        return n;
+      }
+    }
+  }
+
+  // The record of one listed hit of a plain shape, in the shape's frame.
+  Isect<R> shape_details(const Object& s, const Ray<R>& r, R t, uint32_t piece) const {
+    Isect<R> h{};
+    switch (s.shape) {
+      case O_SHAPE_MESH: {
+        const Mesh& m = meshes[s.mesh];
+        const uint32_t i0 = m.idx[3 * size_t(piece)], i1 = m.idx[3 * size_t(piece) + 1],
+                       i2 = m.idx[3 * size_t(piece) + 2];
+        const V3<R> p0{m.v[3 * size_t(i0)], m.v[3 * size_t(i0) + 1], m.v[3 * size_t(i0) + 2]};
+        const V3<R> p1{m.v[3 * size_t(i1)], m.v[3 * size_t(i1) + 1], m.v[3 * size_t(i1) + 2]};
+        const V3<R> p2{m.v[3 * size_t(i2)], m.v[3 * size_t(i2) + 1], m.v[3 * size_t(i2) + 2]};
+        TriHit<R> th;
+        intersect_ray(r, p0, p1, p2, &th);
+        th.t = t;
+        mesh_details(m, piece, r, th, &h);
+        break;
+      }
+      case O_SHAPE_SPHERE: sphere_details(s, r, t, &h); break;
+      case O_SHAPE_CYLINDER: cylinder_details(s, r, t, int(piece), &h); break;
+      case O_SHAPE_AABOX: aabox_details(r, t, int(piece), &h); break;
+      default: flat_details(r, t, &h); break;
+    }
+    return h;
+  }
+
+  // Union / Intersection / Substraction::intersect (src/shapes/csg/*.rs): every element's
+  // hits, moved out of the element's frame, kept by the operation's inside tests, sorted by
+  // distance (stable); Simple keeps the first. prim = element << 24 | piece.
+  bool csg_closest(const Object& o, const Ray<R>& ray, R near, R far, Isect<R>* out, uint32_t* prim) const {
+    bool have = false;
+    for (uint32_t e = 0; e < o.csg_count; ++e) {
+      const Object& E = celems[o.csg_first + e];
+      const Ray<R> lr = make_ray(E.inv.point(ray.o), E.inv.direction(ray.d));
+      R ts[4];
+      uint32_t ps[4];
+      const int n = shape_hits(E, lr, near, far, ts, ps);
+      for (int k = 0; k < n; ++k) {
+        if (have && !(ts[k] < out->d)) continue;
+        Isect<R> w = to_world_isect(shape_details(E, lr, ts[k], ps[k]), E.mat, E.inv);
+        bool keep;
+        if (o.csg_op == O_CSG_UNION) {  // outside every other element (union.rs:76-93)
+          keep = true;
+          for (uint32_t j = 0; j < o.csg_count && keep; ++j)
+            if (j != e && contains(celems[o.csg_first + j], celems[o.csg_first + j].inv.point(w.p))) keep = false;
+        } else if (o.csg_op == O_CSG_INTERSECTION) {  // inside every other (intersection.rs:74-91)
+          keep = true;
+          for (uint32_t j = 0; j < o.csg_count && keep; ++j)
+            if (j != e && !contains(celems[o.csg_first + j], celems[o.csg_first + j].inv.point(w.p))) keep = false;
+        } else {  // the base outside the subtracted; a subtracted one inside the base, outside the others
+          keep = e == 0 || contains(celems[o.csg_first], celems[o.csg_first].inv.point(w.p));
+          for (uint32_t j = 1; j < o.csg_count && keep; ++j)
+            if (j != e && contains(celems[o.csg_first + j], celems[o.csg_first + j].inv.point(w.p))) keep = false;
+          if (e > 0) w.n = w.n * R(-1);
+        }
+        if (!keep) continue;
+        have = true;
+        *out = w;
+        *prim = (e << 24) | ps[k];
+      }
+    }
+    return have;
   }
 
   AABB<R> object_box(const Object& o) const {
@@ -511,6 +741,35 @@ class OScene {
     return true;
   }
 
+  // The slab span of AABox::intersect (aabox.rs:76-160) with its entering / leaving faces;
+  // false when the slabs do not overlap.
+  static bool aabox_span(const Object& o, const Ray<R>& ray, R* tmin_out, R* tmax_out, int* fmin_out, int* fmax_out) {
+    const V3<R> inv{R(1) / ray.d.x, R(1) / ray.d.y, R(1) / ray.d.z};
+    R tmin, tmax;
+    int fmin, fmax;
+    if (inv.x >= R(0)) { tmin = (o.amin.x - ray.o.x) * inv.x; tmax = (o.amax.x - ray.o.x) * inv.x; fmin = 0; fmax = 1; }
+    else { tmin = (o.amax.x - ray.o.x) * inv.x; tmax = (o.amin.x - ray.o.x) * inv.x; fmin = 1; fmax = 0; }
+    R tymin, tymax;
+    int fymin, fymax;
+    if (inv.y >= R(0)) { tymin = (o.amin.y - ray.o.y) * inv.y; tymax = (o.amax.y - ray.o.y) * inv.y; fymin = 2; fymax = 3; }
+    else { tymin = (o.amax.y - ray.o.y) * inv.y; tymax = (o.amin.y - ray.o.y) * inv.y; fymin = 3; fymax = 2; }
+    if ((tmin > tymax) || (tymin > tmax)) return false;
+    if (tymin > tmin) { tmin = tymin; fmin = fymin; }
+    if (tymax < tmax) { tmax = tymax; fmax = fymax; }
+    R tzmin, tzmax;
+    int fzmin, fzmax;
+    if (inv.z >= R(0)) { tzmin = (o.amin.z - ray.o.z) * inv.z; tzmax = (o.amax.z - ray.o.z) * inv.z; fzmin = 4; fzmax = 5; }
+    else { tzmin = (o.amax.z - ray.o.z) * inv.z; tzmax = (o.amin.z - ray.o.z) * inv.z; fzmin = 5; fzmax = 4; }
+    if ((tmin > tzmax) || (tzmin > tmax)) return false;
+    if (tzmin > tmin) { tmin = tzmin; fmin = fzmin; }
+    if (tzmax < tmax) { tmax = tzmax; fmax = fzmax; }
+    *tmin_out = tmin;
+    *tmax_out = tmax;
+    *fmin_out = fmin;
+    *fmax_out = fmax;
+    return true;
+  }
+
   // AABox::intersect (aabox.rs:76-190): slabs with the entering/leaving face tracked; the
   // first listed hit is the entry when it lies beyond near, else the exit. face: 0..5 for
   // X_NEG, X_POS, Y_NEG, Y_POS, Z_NEG, Z_POS.
@@ -585,11 +844,13 @@ class OScene {
         return false;
       flat_details(lr, t, &h);
       *prim = 0;
-    } else {
+    } else if (o.shape == O_SHAPE_AABOX) {
       int face;
       if (!aabox_hit(o, lr, near, far, &t, &face)) return false;
       aabox_details(lr, t, face, &h);
       *prim = uint32_t(face);
+    } else {
+      if (!csg_closest(o, lr, near, far, &h, prim)) return false;
     }
     *out = o.transformed ? to_world_isect(h, o.mat, o.inv) : h;
     return true;
@@ -608,6 +869,11 @@ class OScene {
       case O_SHAPE_CYLINDER: return cylinder_hit(o, lr, near, far, &t, &piece);
       case O_SHAPE_RECTANGLE: return rectangle_hit(o, lr, near, far, &t);
       case O_SHAPE_AABOX: return aabox_hit(o, lr, near, far, &t, &piece);
+      case O_SHAPE_CSG: {  // the default intersect_p: any hit listed (intersectable.rs:48-50)
+        Isect<R> h;
+        uint32_t prim;
+        return csg_closest(o, lr, near, far, &h, &prim);
+      }
       default: return plane_hit(lr, near, far, &t);
     }
   }
@@ -1268,6 +1534,7 @@ class OScene {
   std::vector<Object> objects;
   std::vector<Material> materials;
   std::vector<Light> lights;
+  std::vector<Object> celems;       // constructive solids' elements
   std::vector<Node> nodes;
   std::vector<uint32_t> roots;      // the scene's primitives (tree nodes), in add order
   std::vector<uint32_t> unbounded;  // roots kept out of the BVH (Scene::commit)

@@ -180,7 +180,8 @@ class Xf:
 # ------------------------------------------------------------------------------------------
 # Parser + scene builder
 # ------------------------------------------------------------------------------------------
-SHAPE = dict(mesh=0, sphere=1, cylinder=2, rectangle=3, aabox=4, plane=5)
+SHAPE = dict(mesh=0, sphere=1, cylinder=2, rectangle=3, aabox=4, plane=5, csg=6)
+CSG_OP = dict(union=0, intersection=1, substraction=2)
 MAT = dict(lambertian=0, metal=1, dielectric=2, diffuse_light=3)
 
 
@@ -297,8 +298,26 @@ class _Parser:
                 self.meshes.append(dict(vertices=np.asarray(v, np.float32).reshape(-1, 3),
                                         indices=np.asarray(idx, np.uint32).reshape(-1, 3), file=name, reverse=rev))
             return dict(shape=SHAPE["mesh"], mesh=self.mesh_ids[key])
-        if k == "csg":
-            raise StageError("csg shapes are not supported")
+        if k == "csg":  # parser.rs:157-196, scene_builder.rs:118-143
+            op = self.kw()
+            if op not in CSG_OP:
+                raise StageError("expected intersection, union or subtraction")
+            self.expect("sym", "{")
+            elems = []
+            while True:
+                t = self.next()
+                if t == ("kw", "elem"):
+                    e = self.shape()
+                    if e["shape"] == SHAPE["csg"]:
+                        raise StageError("a csg element is a plain shape")
+                    w, l = self.transform().rows()
+                    e.update(to_world=w, to_local=l)
+                    elems.append(e)
+                elif t == ("sym", "}"):
+                    break
+                else:
+                    raise StageError("expected } or elem")
+            return dict(shape=SHAPE["csg"], csg=dict(op=CSG_OP[op], elements=elems[::-1]))  # popped: reversed
         raise StageError("expected a shape")
 
     def material(self):

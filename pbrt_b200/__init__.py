@@ -16,6 +16,7 @@ from .scene import (  # noqa: F401
     CheckerBoard,
     Compound,
     Context,
+    Csg,
     Cylinder,
     Dielectric,
     DiffuseLight,
@@ -42,5 +43,5 @@ __all__ = [
     "PBRT_MISS", "PbrtError", "load", "Context", "default_context", "Scene", "TriangleMesh", "Sphere", "Cylinder",
     "Simple", "Transformed", "Transform", "Lambertian", "Metal", "Dielectric", "DiffuseLight", "PointLight",
     "UniformInfiniteLight", "BackgroundInfiniteLight", "AreaLight", "film_to_rgba8", "Rectangle", "AABox", "Plane",
-    "CheckerBoard", "Compound", "Stage", "load_scene", "read_ply", "write_png", "film_to_png",
+    "CheckerBoard", "Compound", "Csg", "Stage", "load_scene", "read_ply", "write_png", "film_to_png",
 ]

@@ -22,7 +22,8 @@ STATUS = {
     6: "PBRT_ERR_UNSUPPORTED",
 }
 
-SHAPE_MESH, SHAPE_SPHERE, SHAPE_CYLINDER, SHAPE_RECTANGLE, SHAPE_AABOX, SHAPE_PLANE = 0, 1, 2, 3, 4, 5
+SHAPE_MESH, SHAPE_SPHERE, SHAPE_CYLINDER, SHAPE_RECTANGLE, SHAPE_AABOX, SHAPE_PLANE, SHAPE_CSG = 0, 1, 2, 3, 4, 5, 6
+CSG_UNION, CSG_INTERSECTION, CSG_SUBTRACTION = 0, 1, 2
 TEXTURE_COLOR, TEXTURE_CHECKERBOARD = 0, 1
 NODE_SIMPLE, NODE_TRANSFORMED, NODE_COMPOUND = 0, 1, 2
 MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_DIFFUSE_LIGHT = 0, 1, 2, 3
@@ -42,7 +43,13 @@ class MaterialDesc(C.Structure):
 class ObjectDesc(C.Structure):
     _fields_ = [("shape", C.c_uint32), ("mesh", C.c_uint32), ("radius", C.c_float), ("height", C.c_float),
                 ("material", C.c_uint32), ("transformed", C.c_uint32), ("to_world", C.c_float * 12),
-                ("to_local", C.c_float * 12), ("extent", C.c_float * 3)]
+                ("to_local", C.c_float * 12), ("extent", C.c_float * 3), ("csg_op", C.c_uint32),
+                ("csg_first", C.c_uint32), ("csg_count", C.c_uint32)]
+
+
+class CsgElemDesc(C.Structure):
+    _fields_ = [("shape", C.c_uint32), ("mesh", C.c_uint32), ("radius", C.c_float), ("height", C.c_float),
+                ("extent", C.c_float * 3), ("to_world", C.c_float * 12), ("to_local", C.c_float * 12)]
 
 
 class NodeDesc(C.Structure):
@@ -63,7 +70,8 @@ class SceneDesc(C.Structure):
                 ("bvh_bins", C.c_uint32), ("bvh_max_leaf", C.c_uint32),
                 ("nodes", C.POINTER(NodeDesc)), ("node_count", C.c_uint32),
                 ("node_children", C.POINTER(C.c_uint32)), ("child_count", C.c_uint32),
-                ("roots", C.POINTER(C.c_uint32)), ("root_count", C.c_uint32), ("device_build", C.c_uint32)]
+                ("roots", C.POINTER(C.c_uint32)), ("root_count", C.c_uint32), ("device_build", C.c_uint32),
+                ("csg_elems", C.POINTER(CsgElemDesc)), ("csg_elem_count", C.c_uint32)]
 
 
 class SceneInfo(C.Structure):

@@ -211,7 +211,8 @@ int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbr
     s->info.device_bytes += dm.bytes;
   }
   void *top = nullptr, *order = nullptr, *objs = nullptr, *mviews = nullptr, *mshades = nullptr, *mats = nullptr,
-       *lights = nullptr, *ltris = nullptr, *lcdf = nullptr, *unb = nullptr, *xfs = nullptr, *grps = nullptr;
+       *lights = nullptr, *ltris = nullptr, *lcdf = nullptr, *unb = nullptr, *xfs = nullptr, *grps = nullptr,
+       *csgs = nullptr;
   if (rc == PBRT_OK && !fs.top.empty()) rc = s->upload(&top, fs.top.data(), fs.top.size() * sizeof(GpuNode));
   if (rc == PBRT_OK && !fs.order.empty()) rc = s->upload(&order, fs.order.data(), fs.order.size() * sizeof(uint32_t));
   if (rc == PBRT_OK) rc = s->upload(&objs, fs.objects.data(), fs.objects.size() * sizeof(ObjRec));
@@ -219,6 +220,7 @@ int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbr
     rc = s->upload(&unb, fs.unbounded.data(), fs.unbounded.size() * sizeof(uint32_t));
   if (rc == PBRT_OK && !fs.xforms.empty()) rc = s->upload(&xfs, fs.xforms.data(), fs.xforms.size() * sizeof(XfRec));
   if (rc == PBRT_OK && !fs.groups.empty()) rc = s->upload(&grps, fs.groups.data(), fs.groups.size() * sizeof(GroupRec));
+  if (rc == PBRT_OK && !fs.csg.empty()) rc = s->upload(&csgs, fs.csg.data(), fs.csg.size() * sizeof(CsgRec));
   if (rc == PBRT_OK && !views.empty()) rc = s->upload(&mviews, views.data(), views.size() * sizeof(MeshView));
   if (rc == PBRT_OK && !shades.empty()) rc = s->upload(&mshades, shades.data(), shades.size() * sizeof(MeshShade));
   if (rc == PBRT_OK) rc = s->upload(&mats, fs.materials.data(), fs.materials.size() * sizeof(MatRec));
@@ -240,6 +242,7 @@ int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbr
   v.objects = (const ObjRec*)objs;
   v.xforms = (const XfRec*)xfs;
   v.groups = (const GroupRec*)grps;
+  v.csg = (const CsgRec*)csgs;
   v.meshes = (const MeshView*)mviews;
   v.shade = (const MeshShade*)mshades;
   v.materials = (const MatRec*)mats;

@@ -39,6 +39,7 @@ struct SceneView {
   uint32_t unbounded_count;
   const ObjRec* objects;    // leaves
   const XfRec* xforms;      // transform chains beyond each leaf's first
+  const CsgRec* csg;        // constructive solids' elements
   const GroupRec* groups;   // compounds
   const MeshView* meshes;   // traversal views
   const MeshShade* shade;   // shading views
@@ -192,6 +193,170 @@ PBRT_DEV bool aabox_hit(const float* h, const F3& o, const F3& d, float near, fl
   return false;
 }
 
+// ---- constructive solids (src/shapes/csg/*.rs) ---------------------------------------------
+// contain_point of a plain shape: sphere.rs:146-148, cylinder.rs:119-124, aabox.rs:192-199,
+// plane.rs:47-52; a rectangle and a mesh enclose nothing
+PBRT_DEV bool shape_contains(uint32_t shape, const float* p, const F3& q) {
+  switch (shape) {
+    case kShapeSphere: return dot3(q, q) <= fm(p[0], p[0]);
+    case kShapeCylinder:
+      return fa(fm(q.x, q.x), fm(q.z, q.z)) <= fm(p[0], p[0]) && q.y >= -p[1] && q.y <= p[1];
+    case kShapeAABox: {
+      const float lx = fs(0.f, p[0]), ly = fs(0.f, p[1]), lz = fs(0.f, p[2]);
+      return q.x >= lx && q.x <= p[0] && q.y >= ly && q.y <= p[1] && q.z >= lz && q.z <= p[2];
+    }
+    case kShapePlane: return q.y <= 0.f;
+    default: return false;
+  }
+}
+
+// Every hit a plain shape lists (its IntersectionResult, in order): distances and pieces
+PBRT_DEV int shape_hits(const SceneView& s, uint32_t shape, uint32_t mesh, const float* p, const F3& o, const F3& d,
+                        float near, float far, float* ts, uint32_t* ps, uint32_t* err) {
+  float t;
+  switch (shape) {
+    case kShapeMesh: {
+      TraceCounters c;
+      const uint32_t id = mesh_closest<false>(s.meshes[mesh], prepare_ray(o, d), near, far, &t, &c, err);
+      if (id == 0xFFFFFFFFu) return 0;
+      ts[0] = t;
+      ps[0] = id;
+      return 1;
+    }
+    case kShapeSphere: {  // sphere.rs:108-144: the entry beyond near, the exit inside (near, far)
+      const F3 l = mul3(o, -1.f);
+      const float tca = dot3(l, d);
+      if (tca < 0.f) return 0;
+      const float r2 = fm(p[0], p[0]);
+      const float d2 = fs(dot3(l, l), fm(tca, tca));
+      if (d2 > r2) return 0;
+      const float thc = fsq(fs(r2, d2));
+      const float t0 = fs(tca, thc), t1 = fa(tca, thc);
+      const float tmin = fminf(t0, t1), tmax = fmaxf(t0, t1);
+      if (tmax < near || tmin > far) return 0;
+      int n = 0;
+      if (tmin > near) { ts[n] = tmin; ps[n] = 0; ++n; }
+      if (tmax > near && tmax < far) { ts[n] = tmax; ps[n] = 0; ++n; }
+      return n;
+    }
+    case kShapeCylinder: {  // cylinder.rs:28-110, sorted by distance (stable)
+      const float radius = p[0], hh = p[1];
+      const float a = fa(fm(d.x, d.x), fm(d.z, d.z));
+      const float b = fm(2.f, fa(fm(o.x, d.x), fm(o.z, d.z)));
+      const float c = fs(fa(fm(o.x, o.x), fm(o.z, o.z)), fm(radius, radius));
+      const float disc = fs(fm(b, b), fm(fm(4.f, a), c));
+      if (disc < 0.f) return 0;
+      const float rd = fsq(disc);
+      const float q = b < 0.f ? fm(-0.5f, fs(b, rd)) : fm(-0.5f, fa(b, rd));
+      const float q0 = fdv(q, a), q1 = fdv(c, q);
+      const float tmin = fminf(q0, q1), tmax = fmaxf(q0, q1);
+      if (tmax < near || tmin > far) return 0;
+      int n = 0;
+      if (tmin > near) {
+        const F3 h = add3(o, mul3(d, tmin));
+        if (h.y > -hh && h.y < hh) { ts[n] = tmin; ps[n] = 0; ++n; }
+      }
+      if (tmax > near && tmax < far) {
+        const F3 h = add3(o, mul3(d, tmax));
+        if (h.y > -hh && h.y < hh) { ts[n] = tmax; ps[n] = 0; ++n; }
+      }
+      if (n < 2) {
+        const float iy = frcp(d.y);
+        const float c0 = fm(fs(-hh, o.y), iy);
+        if (c0 > near && c0 < far) {
+          const F3 h = add3(o, mul3(d, c0));
+          if (fa(fm(h.x, h.x), fm(h.z, h.z)) <= fm(radius, radius)) { ts[n] = c0; ps[n] = 1; ++n; }
+        }
+        const float c1 = fm(fs(hh, o.y), iy);
+        if (c1 > near && c1 < far) {
+          const F3 h = add3(o, mul3(d, c1));
+          if (fa(fm(h.x, h.x), fm(h.z, h.z)) <= fm(radius, radius)) { ts[n] = c1; ps[n] = 2; ++n; }
+        }
+      }
+      for (int i = 1; i < n; ++i)  // insertion sort: stable
+        for (int j = i; j > 0 && ts[j] < ts[j - 1]; --j) {
+          const float tt = ts[j]; ts[j] = ts[j - 1]; ts[j - 1] = tt;
+          const uint32_t pp = ps[j]; ps[j] = ps[j - 1]; ps[j - 1] = pp;
+        }
+      return n;
+    }
+    case kShapeRectangle:
+      if (!rectangle_hit(p[0], p[1], o, d, near, far, t)) return 0;
+      ts[0] = t;
+      ps[0] = 0;
+      return 1;
+    case kShapePlane:
+      if (!plane_hit(o, d, near, far, t)) return 0;
+      ts[0] = t;
+      ps[0] = 0;
+      return 1;
+    default: {  // AABox: the entry beyond near, the exit before far (aabox.rs:76-190)
+      float tmin, tmax, tymin, tymax, tzmin, tzmax;
+      int fmin, fmax, fymin, fymax, fzmin, fzmax;
+      aabox_axis(o.x, frcp(d.x), fs(0.f, p[0]), p[0], 0, tmin, tmax, fmin, fmax);
+      aabox_axis(o.y, frcp(d.y), fs(0.f, p[1]), p[1], 2, tymin, tymax, fymin, fymax);
+      if ((tmin > tymax) || (tymin > tmax)) return 0;
+      if (tymin > tmin) { tmin = tymin; fmin = fymin; }
+      if (tymax < tmax) { tmax = tymax; fmax = fymax; }
+      aabox_axis(o.z, frcp(d.z), fs(0.f, p[2]), p[2], 4, tzmin, tzmax, fzmin, fzmax);
+      if ((tmin > tzmax) || (tzmin > tmax)) return 0;
+      if (tzmin > tmin) { tmin = tzmin; fmin = fzmin; }
+      if (tzmax < tmax) { tmax = tzmax; fmax = fzmax; }
+      if (tmax < near || tmin > far) return 0;
+      int n = 0;
+      if (tmin > near) { ts[n] = tmin; ps[n] = uint32_t(fmin); ++n; }
+      if (tmax < far) { ts[n] = tmax; ps[n] = uint32_t(fmax); ++n; }
+      return n;
+    }
+  }
+}
+
+PBRT_DEV bool csg_point_in(const CsgRec& e, const F3& q) {
+  return shape_contains(e.shape, e.p, xf_point(e.to_local, q));
+}
+
+// Union / Intersection / Substraction::intersect: every element's listed hits, each moved out
+// of its element (the hit point as the element's record places it: on y = 0 for the flat
+// shapes), kept by the operation's inside tests; the nearest kept, the earliest listed on a
+// tie (the results are sorted stably). prim = element << 24 | the element's piece.
+PBRT_DEV bool csg_closest(const SceneView& s, const ObjRec& ob, const F3& o, const F3& d, float near, float far,
+                          float& t_out, uint32_t& prim_out, uint32_t* err) {
+  bool have = false;
+  for (uint32_t e = 0; e < ob.csg_count; ++e) {
+    const CsgRec& E = s.csg[ob.csg_first + e];
+    const F3 lo = xf_point(E.to_local, o);
+    const F3 ld = normalize3(xf_dir(E.to_local, d));
+    float ts[4];
+    uint32_t ps[4];
+    const int n = shape_hits(s, E.shape, E.mesh, E.p, lo, ld, near, far, ts, ps, err);
+    for (int k = 0; k < n; ++k) {
+      if (have && !(ts[k] < t_out)) continue;
+      F3 hp = add3(lo, mul3(ld, ts[k]));
+      if (E.shape == kShapeRectangle || E.shape == kShapePlane) hp.y = 0.f;
+      const F3 w = xf_point(E.to_world, hp);
+      bool keep;
+      if (ob.csg_op == kCsgUnion) {
+        keep = true;
+        for (uint32_t j = 0; j < ob.csg_count && keep; ++j)
+          if (j != e && csg_point_in(s.csg[ob.csg_first + j], w)) keep = false;
+      } else if (ob.csg_op == kCsgIntersection) {
+        keep = true;
+        for (uint32_t j = 0; j < ob.csg_count && keep; ++j)
+          if (j != e && !csg_point_in(s.csg[ob.csg_first + j], w)) keep = false;
+      } else {
+        keep = e == 0 || csg_point_in(s.csg[ob.csg_first], w);
+        for (uint32_t j = 1; j < ob.csg_count && keep; ++j)
+          if (j != e && csg_point_in(s.csg[ob.csg_first + j], w)) keep = false;
+      }
+      if (!keep) continue;
+      have = true;
+      t_out = ts[k];
+      prim_out = (e << 24) | ps[k];
+    }
+  }
+  return have;
+}
+
 // ---- leaves --------------------------------------------------------------------------------
 PBRT_DEV const float* leaf_to_local(const SceneView& s, const ObjRec& ob, uint32_t k) {
   return k == 0 ? ob.to_local : s.xforms[ob.xf_rest + k - 1].to_local;
@@ -242,6 +407,7 @@ PBRT_DEV bool leaf_closest(const SceneView& s, uint32_t li, const F3& o, const F
       prim = uint32_t(face);
       return hit;
     }
+    case kShapeCsg: return csg_closest(s, ob, lo, ld, near, far, t, prim, err);
     default: return plane_hit(lo, ld, near, far, t);
   }
 }
@@ -259,6 +425,10 @@ PBRT_DEV bool leaf_any(const SceneView& s, uint32_t li, const F3& o, const F3& d
     case kShapeCylinder: return cylinder_hit(ob.p[0], ob.p[1], lo, ld, near, far, t, k);
     case kShapeRectangle: return rectangle_hit(ob.p[0], ob.p[1], lo, ld, near, far, t);
     case kShapeAABox: return aabox_hit(ob.p, lo, ld, near, far, t, k);
+    case kShapeCsg: {  // the default intersect_p: any listed hit (intersectable.rs:48-50)
+      uint32_t prim;
+      return csg_closest(s, ob, lo, ld, near, far, t, prim, err);
+    }
     default: return plane_hit(lo, ld, near, far, t);
   }
 }
@@ -470,11 +640,11 @@ static __constant__ float kBoxFace[6][9] = {
 // World-space shading record of leaf `li` hit at distance t (recomputed from the same local
 // ray and the same arithmetic as the hit itself). With uv = false the texture coordinates of
 // mesh and sphere hits are left 0 (only textured materials read them).
-PBRT_DEV Isect interaction(const SceneView& s, uint32_t li, uint32_t prim, const F3& o, const F3& d, float t,
-                           bool uv = false) {
-  const ObjRec& ob = s.objects[li];
-  F3 lo, ld;
-  local_ray(s, ob, o, d, lo, ld);
+// The record of a hit on a plain shape, in its own frame (the shape's details functions:
+// triangle_mesh.rs:73-132, 219-258; sphere.rs:152-187; cylinder.rs:266-344; aabox.rs:165-190;
+// rectangle.rs:46-55; plane.rs:31-40).
+PBRT_DEV Isect shape_isect(const SceneView& s, uint32_t shape, uint32_t mesh, const float* pr, uint32_t prim,
+                           const F3& lo, const F3& ld, float t, bool uv) {
   Isect h;
   h.d = t;
   h.u = 0.f;
@@ -482,9 +652,9 @@ PBRT_DEV Isect interaction(const SceneView& s, uint32_t li, uint32_t prim, const
   h.wo = mul3(ld, -1.f);
   F3 dpdv;
   const float kTwoPi = fm(2.f, 3.14159265358979323846f);
-  switch (ob.shape) {
+  switch (shape) {
     case kShapeMesh: {
-      const MeshShade& m = s.shade[ob.mesh];
+      const MeshShade& m = s.shade[mesh];
       const F3 p0 = vtx(m, m.idx[3 * prim]), p1 = vtx(m, m.idx[3 * prim + 1]), p2 = vtx(m, m.idx[3 * prim + 2]);
       h.p = add3(lo, mul3(ld, t));
       // compute_texture_derivatives with the default uvs (0,0), (1,0), (1,1)
@@ -518,7 +688,7 @@ PBRT_DEV Isect interaction(const SceneView& s, uint32_t li, uint32_t prim, const
         float phi = atan2f(hit.y, hit.x);
         if (phi < 0.f) phi = fa(phi, kTwoPi);
         h.u = fdv(phi, kTwoPi);
-        const float theta = acosf(fminf(fmaxf(fdv(hit.z, ob.p[0]), -1.f), 1.f));
+        const float theta = acosf(fminf(fmaxf(fdv(hit.z, pr[0]), -1.f), 1.f));
         h.v = fdv(theta, 3.14159265358979323846f);
       }
       break;
@@ -527,7 +697,7 @@ PBRT_DEV Isect interaction(const SceneView& s, uint32_t li, uint32_t prim, const
       const F3 p = add3(lo, mul3(ld, t));
       h.p = p;
       dpdv = mk3(0.f, 1.f, 0.f);
-      const uint32_t piece = prim;  // leaf_closest reports the piece in prim
+      const uint32_t piece = prim;  // the piece: 0 wall, 1 bottom cap, 2 top cap
       if (piece == 0) {
         h.n = normalize3(mk3(p.x, 0.f, p.z));
         h.dpdu = mul3(mk3(-p.z, 0.f, p.x), kTwoPi);
@@ -569,6 +739,33 @@ PBRT_DEV Isect interaction(const SceneView& s, uint32_t li, uint32_t prim, const
       break;
     }
   }
+  (void)dpdv;
+  return h;
+}
+
+// World-space shading record of leaf `li` hit at distance t (recomputed from the same local
+// ray and the same arithmetic as the hit itself). With uv = false the texture coordinates of
+// mesh and sphere hits are left 0 (only textured materials read them).
+PBRT_DEV Isect interaction(const SceneView& s, uint32_t li, uint32_t prim, const F3& o, const F3& d, float t,
+                           bool uv = false) {
+  const ObjRec& ob = s.objects[li];
+  F3 lo, ld;
+  local_ray(s, ob, o, d, lo, ld);
+  Isect h;
+  if (ob.shape == kShapeCsg) {  // the element's record, moved out of the element (csg/*.rs)
+    const uint32_t e = prim >> 24;
+    const CsgRec& E = s.csg[ob.csg_first + e];
+    const F3 elo = xf_point(E.to_local, lo);
+    const F3 eld = normalize3(xf_dir(E.to_local, ld));
+    h = shape_isect(s, E.shape, E.mesh, E.p, prim & 0xFFFFFFu, elo, eld, t, uv);
+    h.n = xf_normal(E.to_local, h.n);
+    h.p = xf_point(E.to_world, h.p);
+    h.wo = xf_dir(E.to_world, h.wo);
+    h.dpdu = xf_dir(E.to_world, h.dpdu);
+    if (ob.csg_op == kCsgSubtraction && e > 0) h.n = mul3(h.n, -1.f);  // substraction.rs:73-76
+  } else {
+    h = shape_isect(s, ob.shape, ob.mesh, ob.p, prim, lo, ld, t, uv);
+  }
   // transform_interaction_to_world (transform.rs:105-116), innermost level first
   for (uint32_t k = ob.xf_count; k-- > 0;) {
     const float* w = leaf_to_world(s, ob, k);
@@ -577,7 +774,6 @@ PBRT_DEV Isect interaction(const SceneView& s, uint32_t li, uint32_t prim, const
     h.wo = xf_dir(w, h.wo);
     h.dpdu = xf_dir(w, h.dpdu);
   }
-  (void)dpdv;
   return h;
 }
 

@@ -364,6 +364,11 @@ class Flattener {
     r.material = o.material;
     r.desc_id = oi;
     r.xf_count = uint32_t(c.size());
+    if (o.shape == PBRT_SHAPE_CSG) {
+      r.csg_op = o.csg_op;
+      r.csg_first = o.csg_first;
+      r.csg_count = o.csg_count;
+    }
     switch (o.shape) {
       case PBRT_SHAPE_SPHERE: r.p[0] = o.radius; break;
       case PBRT_SHAPE_CYLINDER: r.p[0] = o.radius; r.p[1] = o.height / 2.0f; break;  // Cylinder::new
@@ -394,6 +399,58 @@ class Flattener {
   FlatScene* out_;
   std::vector<uint8_t>* grouped_ = nullptr;
 };
+
+// The box of a plain shape before any transform (its get_bounding_box), with its sizes checked.
+bool plain_shape_box(const pbrt_object_desc& o, const pbrt_scene_desc& d, const FlatScene* out, const std::string& who,
+                   Box3* bp, std::string* err) {
+  Box3& b = *bp;
+  switch (o.shape) {
+    case PBRT_SHAPE_MESH: {
+      if (o.mesh >= d.mesh_count) { *err = who + "bad mesh"; return false; }
+      const FlatMesh& fm = out->meshes[o.mesh];
+      for (int a = 0; a < 3; ++a) { b.lo[a] = fm.bounds_min[a]; b.hi[a] = fm.bounds_max[a]; }
+      break;
+    }
+    case PBRT_SHAPE_SPHERE:
+      if (!(o.radius > 0.0f) || !std::isfinite(o.radius)) { *err = who + "sphere radius must be > 0"; return false; }
+      for (int a = 0; a < 3; ++a) { b.lo[a] = -o.radius; b.hi[a] = o.radius; }
+      break;
+    case PBRT_SHAPE_CYLINDER: {
+      if (!(o.radius > 0.0f) || !(o.height > 0.0f)) { *err = who + "bad cylinder"; return false; }
+      const float hh = o.height / 2.0f;
+      b.lo[0] = -o.radius; b.lo[1] = -hh; b.lo[2] = -o.radius;
+      b.hi[0] = o.radius; b.hi[1] = hh; b.hi[2] = o.radius;
+      break;
+    }
+    case PBRT_SHAPE_RECTANGLE: {  // rectangle.rs:63-69: flat at y = 0
+      if (!(o.radius >= 0.0f) || !(o.height >= 0.0f) || !std::isfinite(o.radius) || !std::isfinite(o.height)) {
+        *err = who + "rectangle sides must be finite and >= 0";
+        return false;
+      }
+      const float hw = o.radius / 2.0f, hh = o.height / 2.0f;
+      b.lo[0] = -hw; b.lo[1] = 0.0f; b.lo[2] = -hh;
+      b.hi[0] = hw; b.hi[1] = 0.0f; b.hi[2] = hh;
+      break;
+    }
+    case PBRT_SHAPE_AABOX:
+      for (int a = 0; a < 3; ++a) {
+        if (!(o.extent[a] >= 0.0f) || !std::isfinite(o.extent[a])) {
+          *err = who + "box extents must be finite and >= 0";
+          return false;
+        }
+        const float h = o.extent[a] * 0.5f;
+        b.lo[a] = 0.0f - h;
+        b.hi[a] = h;
+      }
+      break;
+    case PBRT_SHAPE_PLANE:  // plane.rs:89-93: the half-space below y = 0
+      for (int a = 0; a < 3; ++a) { b.lo[a] = -INFINITY; b.hi[a] = INFINITY; }
+      b.hi[1] = 0.0f;
+      break;
+    default: *err = who + "unknown shape"; return false;
+    }
+  return true;
+}
 
 }  // namespace
 
@@ -465,6 +522,43 @@ bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err, con
     if (m.kind == PBRT_MAT_DIELECTRIC) out->has_dielectric = true;
   }
 
+  // the elements of the constructive solids: plain shapes placed by their transforms
+  if (d.csg_elem_count && !d.csg_elems) { *err = "csg_elems is NULL"; return false; }
+  std::vector<Box3> elem_boxes(d.csg_elem_count);
+  for (uint32_t i = 0; i < d.csg_elem_count; ++i) {
+    const pbrt_csg_elem_desc& e = d.csg_elems[i];
+    pbrt_object_desc as{};
+    as.shape = e.shape;
+    as.mesh = e.mesh;
+    as.radius = e.radius;
+    as.height = e.height;
+    for (int a = 0; a < 3; ++a) as.extent[a] = e.extent[a];
+    const std::string who = "csg element " + std::to_string(i) + ": ";
+    if (e.shape >= PBRT_SHAPE_CSG) { *err = who + "an element is a plain shape"; return false; }
+    Box3 b;
+    if (!plain_shape_box(as, d, out, who, &b, err)) return false;
+    if (e.shape == PBRT_SHAPE_MESH && d.meshes[e.mesh].triangle_count > (1u << 24)) {
+      *err = who + "a mesh inside a constructive solid has at most 2^24 triangles";
+      return false;
+    }
+    elem_boxes[i] = transform_box(b, e.to_world);
+    CsgRec r{};
+    r.shape = e.shape;
+    r.mesh = e.mesh;
+    switch (e.shape) {
+      case PBRT_SHAPE_SPHERE: r.p[0] = e.radius; break;
+      case PBRT_SHAPE_CYLINDER: r.p[0] = e.radius; r.p[1] = e.height / 2.0f; break;
+      case PBRT_SHAPE_RECTANGLE: r.p[0] = e.radius / 2.0f; r.p[1] = e.height / 2.0f; break;
+      case PBRT_SHAPE_AABOX:
+        for (int a = 0; a < 3; ++a) r.p[a] = e.extent[a] * 0.5f;
+        break;
+      default: break;
+    }
+    std::memcpy(r.to_world, e.to_world, sizeof(r.to_world));
+    std::memcpy(r.to_local, e.to_local, sizeof(r.to_local));
+    out->csg.push_back(r);
+  }
+
   // every object's shape box, before any transform
   std::vector<Box3> shape_boxes(d.object_count);
   for (uint32_t i = 0; i < d.object_count; ++i) {
@@ -472,51 +566,32 @@ bool build_scene(const pbrt_scene_desc& d, FlatScene* out, std::string* err, con
     const std::string who = "object " + std::to_string(i) + ": ";
     if (o.material >= d.material_count) { *err = who + "bad material"; return false; }
     Box3& b = shape_boxes[i];
-    switch (o.shape) {
-      case PBRT_SHAPE_MESH: {
-        if (o.mesh >= d.mesh_count) { *err = who + "bad mesh"; return false; }
-        const FlatMesh& fm = out->meshes[o.mesh];
-        for (int a = 0; a < 3; ++a) { b.lo[a] = fm.bounds_min[a]; b.hi[a] = fm.bounds_max[a]; }
-        break;
+    if (o.shape == PBRT_SHAPE_CSG) {  // Union / Intersection / Substraction::get_bounding_box
+      if (o.csg_op > PBRT_CSG_SUBTRACTION || uint64_t(o.csg_first) + o.csg_count > d.csg_elem_count ||
+          o.csg_count > 256) {
+        *err = who + "bad constructive solid (operation, element range, at most 256 elements)";
+        return false;
       }
-      case PBRT_SHAPE_SPHERE:
-        if (!(o.radius > 0.0f) || !std::isfinite(o.radius)) { *err = who + "sphere radius must be > 0"; return false; }
-        for (int a = 0; a < 3; ++a) { b.lo[a] = -o.radius; b.hi[a] = o.radius; }
-        break;
-      case PBRT_SHAPE_CYLINDER: {
-        if (!(o.radius > 0.0f) || !(o.height > 0.0f)) { *err = who + "bad cylinder"; return false; }
-        const float hh = o.height / 2.0f;
-        b.lo[0] = -o.radius; b.lo[1] = -hh; b.lo[2] = -o.radius;
-        b.hi[0] = o.radius; b.hi[1] = hh; b.hi[2] = o.radius;
-        break;
+      if (o.csg_count == 0) {
+        for (int a = 0; a < 3; ++a) { b.lo[a] = 0.0f; b.hi[a] = 0.0f; }
+        continue;
       }
-      case PBRT_SHAPE_RECTANGLE: {  // rectangle.rs:63-69: flat at y = 0
-        if (!(o.radius >= 0.0f) || !(o.height >= 0.0f) || !std::isfinite(o.radius) || !std::isfinite(o.height)) {
-          *err = who + "rectangle sides must be finite and >= 0";
-          return false;
-        }
-        const float hw = o.radius / 2.0f, hh = o.height / 2.0f;
-        b.lo[0] = -hw; b.lo[1] = 0.0f; b.lo[2] = -hh;
-        b.hi[0] = hw; b.hi[1] = 0.0f; b.hi[2] = hh;
-        break;
-      }
-      case PBRT_SHAPE_AABOX:
-        for (int a = 0; a < 3; ++a) {
-          if (!(o.extent[a] >= 0.0f) || !std::isfinite(o.extent[a])) {
-            *err = who + "box extents must be finite and >= 0";
-            return false;
+      b = elem_boxes[o.csg_first];
+      if (o.csg_op == PBRT_CSG_SUBTRACTION) continue;
+      for (uint32_t k = 1; k < o.csg_count; ++k) {
+        const Box3& x = elem_boxes[o.csg_first + k];
+        if (o.csg_op == PBRT_CSG_UNION) {
+          b.grow(x);
+        } else {  // intersect_with (aabound.rs:397-401)
+          for (int a = 0; a < 3; ++a) {
+            b.lo[a] = std::fmax(b.lo[a], x.lo[a]);
+            b.hi[a] = std::fmin(b.hi[a], x.hi[a]);
           }
-          const float h = o.extent[a] * 0.5f;
-          b.lo[a] = 0.0f - h;
-          b.hi[a] = h;
         }
-        break;
-      case PBRT_SHAPE_PLANE:  // plane.rs:89-93: the half-space below y = 0
-        for (int a = 0; a < 3; ++a) { b.lo[a] = -INFINITY; b.hi[a] = INFINITY; }
-        b.hi[1] = 0.0f;
-        break;
-      default: *err = who + "unknown shape"; return false;
+      }
+      continue;
     }
+    if (!plain_shape_box(o, d, out, who, &b, err)) return false;
   }
 
   Flattener fl(d, shape_boxes, out);

@@ -28,6 +28,7 @@ struct FlatScene {
   std::vector<std::vector<uint32_t>> mesh_fmat; // per-triangle material, empty when absent
   std::vector<ObjRec> objects;                  // leaves: placed Simple objects
   std::vector<XfRec> xforms;                    // transform chains beyond each leaf's first
+  std::vector<CsgRec> csg;                      // constructive solids' elements
   std::vector<GroupRec> groups;                 // compounds (consecutive leaves)
   std::vector<uint32_t> unbounded;              // primitives kept out of the BVH, in scene order
   std::vector<GpuNode> top;                     // GPU numbering (root 0, padding 1); empty when no

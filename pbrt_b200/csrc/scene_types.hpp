@@ -6,7 +6,8 @@
 namespace pbrt {
 
 enum : uint32_t { kShapeMesh = 0, kShapeSphere = 1, kShapeCylinder = 2, kShapeRectangle = 3, kShapeAABox = 4,
-                  kShapePlane = 5 };
+                  kShapePlane = 5, kShapeCsg = 6 };
+enum : uint32_t { kCsgUnion = 0, kCsgIntersection = 1, kCsgSubtraction = 2 };
 enum : uint32_t { kMatLambertian = 0, kMatMetal = 1, kMatDielectric = 2, kMatDiffuseLight = 3 };
 enum : uint32_t { kLightPoint = 0, kLightUniform = 1, kLightBackground = 2, kLightArea = 3 };
 enum : uint32_t { kTexColor = 0, kTexChecker = 1 };
@@ -22,7 +23,8 @@ struct alignas(16) ObjRec {
   uint32_t shape, mesh, material, xf_count;
   float p[3];        // sphere: r; cylinder: r, h/2; rectangle: w/2, h/2; aabox: extent/2 (x, y, z)
   uint32_t desc_id;  // the object's index in the caller's description (reported as object_id)
-  uint32_t xf_rest, pad0, pad1, pad2;
+  uint32_t xf_rest;
+  uint32_t csg_op, csg_first, csg_count;  // a constructive solid: its elements in the CsgRec array
   float to_world[12];  // row-major 3x4 of Transform::mat (outermost transform)
   float to_local[12];  // row-major 3x4 of Transform::inv_mat
 };
@@ -32,6 +34,14 @@ struct alignas(16) XfRec {
   float to_world[12], to_local[12];
 };
 static_assert(sizeof(XfRec) == 96, "XfRec is 96 bytes");
+
+// One element of a constructive solid: a plain shape (sizes as ObjRec::p) and its transform.
+struct alignas(16) CsgRec {
+  uint32_t shape, mesh, pad0, pad1;
+  float p[4];
+  float to_world[12], to_local[12];
+};
+static_assert(sizeof(CsgRec) == 128, "CsgRec is 128 bytes");
 
 // A Compound's members: leaves [first, first + count), in member order.
 struct GroupRec {

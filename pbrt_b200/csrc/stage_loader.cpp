@@ -346,6 +346,7 @@ void rows(const M4d& m, float* out) {
 
 // ---- the stage -------------------------------------------------------------------------------
 struct pbrt_stage {
+  std::vector<pbrt_csg_elem_desc> csg;
   std::vector<std::vector<float>> mesh_v;
   std::vector<std::vector<uint32_t>> mesh_i;
   std::vector<pbrt_mesh_desc> meshes;
@@ -527,8 +528,41 @@ class StageParser {
       }
       o->shape = PBRT_SHAPE_MESH;
       o->mesh = mesh(f.s, rev);
-    } else if (k == "csg") {
-      throw StageError("constructive solid (csg) shapes are not supported", PBRT_ERR_UNSUPPORTED);
+    } else if (k == "csg") {  // parser.rs:157-196, scene_builder.rs:118-143
+      const std::string op = kw();
+      o->shape = PBRT_SHAPE_CSG;
+      if (op == "union") o->csg_op = PBRT_CSG_UNION;
+      else if (op == "intersection") o->csg_op = PBRT_CSG_INTERSECTION;
+      else if (op == "substraction") o->csg_op = PBRT_CSG_SUBTRACTION;
+      else throw StageError("expected intersection, union or subtraction");
+      expect_sym('{');
+      std::vector<pbrt_csg_elem_desc> elems;
+      for (;;) {
+        const Tok& t = next();
+        if (t.kind == Tok::Kw && t.s == "elem") {
+          pbrt_object_desc e{};
+          shape(&e);
+          if (e.shape == PBRT_SHAPE_CSG)
+            throw StageError("a constructive solid nested in another is not supported", PBRT_ERR_UNSUPPORTED);
+          const Xfd x = transform();
+          pbrt_csg_elem_desc d{};
+          d.shape = e.shape;
+          d.mesh = e.mesh;
+          d.radius = e.radius;
+          d.height = e.height;
+          for (int a = 0; a < 3; ++a) d.extent[a] = e.extent[a];
+          rows(x.mat, d.to_world);
+          rows(x.inv, d.to_local);
+          elems.push_back(d);
+        } else if (t.kind == Tok::Sym && t.s == "}") {
+          break;
+        } else {
+          throw StageError("expected } or elem");
+        }
+      }
+      o->csg_first = uint32_t(st_->csg.size());
+      o->csg_count = uint32_t(elems.size());
+      st_->csg.insert(st_->csg.end(), elems.rbegin(), elems.rend());  // popped: reverse order
     } else {
       throw StageError("expected a shape");
     }
@@ -692,6 +726,8 @@ int pbrt_stage_describe(const pbrt_stage* st, pbrt_scene_desc* d, pbrt_camera_de
     d->child_count = uint32_t(st->children.size());
     d->roots = st->roots.data();
     d->root_count = uint32_t(st->roots.size());
+    d->csg_elems = st->csg.data();
+    d->csg_elem_count = uint32_t(st->csg.size());
   }
   if (camera) *camera = st->camera;
   if (camera_lens) {

@@ -229,6 +229,17 @@ class Plane:
 
 
 @dataclass
+class Csg:
+    """csg::Union / Intersection / Substraction (src/shapes/csg/*.rs): op is "union",
+    "intersection" or "subtraction"; elements are (plain shape, Transform) pairs (csg::Elem) in
+    the order the solid holds them: elements[0] is the piece the others are subtracted from. A
+    scene file lists a solid's elements in the reverse of that order (the scene builder pops
+    them, loader/visitors/scene_builder.rs:117-143)."""
+    op: str
+    elements: List[tuple]
+
+
+@dataclass
 class CheckerBoard:
     """CheckerBoard::new(c1, c2, scale): a texture usable wherever a material takes a colour."""
     c1: Sequence[float]
@@ -300,6 +311,9 @@ class AreaLight:
     """The emissive surface of an object already added to the scene (its material is a
     DiffuseLight); sampled by area for next-event estimation (ideas/area_light.md)."""
     object: object
+
+
+_NO_MATERIAL = object()  # a csg element's shape carries no material of its own
 
 
 def _texture(c) -> dict:
@@ -411,7 +425,7 @@ class Scene:
                 materials.append(_material_desc(m))
             return mat_ids[id(m)]
 
-        def simple_desc(o: Simple) -> dict:
+        def simple_desc(o: Simple) -> dict:  # noqa: C901
             d = dict(shape=0, mesh=0, radius=0.0, height=0.0, material=0, to_world=None, to_local=None)
             shp = o.shape
             if isinstance(shp, TriangleMesh):
@@ -433,10 +447,25 @@ class Scene:
                 d.update(shape=_capi.SHAPE_AABOX, extent=tuple(float(x) for x in shp.extent))
             elif isinstance(shp, Plane):
                 d.update(shape=_capi.SHAPE_PLANE)
+            elif isinstance(shp, Csg):
+                ops = {"union": _capi.CSG_UNION, "intersection": _capi.CSG_INTERSECTION,
+                       "subtraction": _capi.CSG_SUBTRACTION}
+                elems = []
+                for es, ex in shp.elements:
+                    if isinstance(es, Csg):
+                        raise TypeError("a csg element is a plain shape")
+                    e = plain(es)
+                    e["to_world"], e["to_local"] = ex.rows()
+                    elems.append(e)
+                d.update(shape=_capi.SHAPE_CSG, csg=dict(op=ops[shp.op], elements=elems))
             else:
                 raise TypeError(f"unknown shape {shp!r}")
-            d["material"] = mat_index(o.material)
+            if o.material is not _NO_MATERIAL:
+                d["material"] = mat_index(o.material)
             return d
+
+        def plain(shp) -> dict:
+            return simple_desc(Simple(shp, _NO_MATERIAL))
 
         flat = all(isinstance(o, Simple) or (isinstance(o, Transformed) and isinstance(o.object, Simple))
                    for o in self.objects)
@@ -643,7 +672,7 @@ def _lower_description(desc: dict, bvh_bins: int = 8, bvh_max_leaf: int = 1):
     def xf(dst, m):  # float64 (or float32) 3x4 rows, rounded to FP32
         dst[:] = [float(x) for x in np.asarray(np.asarray(m, np.float64).reshape(-1)[:12], np.float32)]
 
-    objs = []
+    objs, celems = [], []
     for o in desc["objects"]:
         d = _capi.ObjectDesc()
         d.shape, d.mesh = int(o["shape"]), int(o.get("mesh", 0))
@@ -654,6 +683,16 @@ def _lower_description(desc: dict, bvh_bins: int = 8, bvh_max_leaf: int = 1):
             d.transformed = 1
             xf(d.to_world, o["to_world"])
             xf(d.to_local, o["to_local"])
+        if o.get("csg") is not None:
+            d.csg_op, d.csg_first, d.csg_count = int(o["csg"]["op"]), len(celems), len(o["csg"]["elements"])
+            for e in o["csg"]["elements"]:
+                c = _capi.CsgElemDesc()
+                c.shape, c.mesh = int(e["shape"]), int(e.get("mesh", 0))
+                c.radius, c.height = float(e.get("radius", 0.0)), float(e.get("height", 0.0))
+                c.extent[:] = [float(x) for x in e.get("extent", (0.0, 0.0, 0.0))]
+                xf(c.to_world, e["to_world"])
+                xf(c.to_local, e["to_local"])
+                celems.append(c)
         objs.append(d)
     nodes, kids = [], []
     for n in desc.get("nodes") or []:
@@ -684,6 +723,10 @@ def _lower_description(desc: dict, bvh_bins: int = 8, bvh_max_leaf: int = 1):
     sd.lights, sd.light_count = C.cast(arrays[3], C.POINTER(_capi.LightDesc)), len(lights)
     sd.bvh_bins, sd.bvh_max_leaf = int(desc.get("bvh_bins", bvh_bins)), int(desc.get("bvh_max_leaf", bvh_max_leaf))
     sd.device_build = 1 if desc.get("device_build") else 0
+    if celems:
+        ca = (_capi.CsgElemDesc * len(celems))(*celems)
+        sd.csg_elems, sd.csg_elem_count = C.cast(ca, C.POINTER(_capi.CsgElemDesc)), len(celems)
+        keep.append(ca)
     if nodes:
         tree = ((_capi.NodeDesc * len(nodes))(*nodes), (C.c_uint32 * max(1, len(kids)))(*kids),
                 (C.c_uint32 * max(1, len(roots)))(*roots))

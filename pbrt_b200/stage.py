@@ -96,6 +96,14 @@ class Stage:
                      material=o.material, to_world=None, to_local=None)
             if o.transformed:
                 d.update(to_world=np.array(o.to_world, np.float32), to_local=np.array(o.to_local, np.float32))
+            if o.shape == _capi.SHAPE_CSG:
+                elems = []
+                for k in range(o.csg_first, o.csg_first + o.csg_count):
+                    e = sd.csg_elems[k]
+                    elems.append(dict(shape=e.shape, mesh=e.mesh, radius=e.radius, height=e.height,
+                                      extent=tuple(e.extent), to_world=np.array(e.to_world, np.float32),
+                                      to_local=np.array(e.to_local, np.float32)))
+                d["csg"] = dict(op=o.csg_op, elements=elems)
             objs.append(d)
         nodes = []
         for i in range(sd.node_count):

@@ -20,7 +20,30 @@ from oracle.stage import load_stage
 pytestmark = pytest.mark.gpu
 
 TRACE_SCENES = ["cornell_box_canonical.stage", "many_spheres.stage", "many_meshes.stage", "default.stage",
-                "cube_mesh.stage", "cornell_box.stage"]
+                "cube_mesh.stage", "cornell_box.stage", "csg_union_spheres.stage"]
+
+CSG_SCENE = """camera pin_hole pos 0.5 1.2 5 look 0 0 0 up 0 1 0
+scene
+  object transformed object simple csg intersection {
+      elem sphere 1 transform { translate -0.3 0 0 }
+      elem aabox 1.2 1.2 1.2 transform { rotate_y 0.5 translate 0.2 0 0 }
+      elem cylinder 0.7 3 transform { rotate_x 0.4 } }
+    lambertian checkerboard 0.9 0.2 0.2 0.2 0.9 0.2 4
+    transform { translate -1.2 0.3 0 }
+  object transformed object simple csg substraction {
+      elem aabox 1.4 1.4 1.4 transform { }
+      elem sphere 0.9 transform { translate 0.4 0.4 0.4 }
+      elem cylinder 0.3 3 transform { rotate_z 1.5708 } }
+    metal 0.2 color 0.8 0.8 0.9
+    transform { rotate_y 0.6 translate 1.3 0.2 -0.5 }
+  object simple csg union {
+      elem mesh file "test_files/cube.ply" reverse transform { translate 0 -0.2 1.5 }
+      elem sphere 0.5 transform { translate 0.4 0.3 1.5 }
+      elem plane transform { translate 0 -1 0 } }
+    lambertian color 0.6 0.6 0.6
+  object transformed object simple rectangle 2 2 diffuse_light color 6 6 6
+    transform { rotate_x 3.14159 translate 0 3 0 }
+"""
 
 TREE_SCENE = """camera pin_hole pos 0.3 1.5 6 look 0 0 0 up 0 1 0
 scene
@@ -85,6 +108,17 @@ def test_scene_mode_bit_exact(name, golden_meshes, mesh_dir, published_scenes):
         pub = published_scenes[name]
         print(name, "primary", [round(v / n, 2) for v in gp.values()], pub["primary"],
               "shadow", [round(v / m, 2) for v in gs.values()], pub["shadow"])
+
+
+def test_csg_bit_exact_and_render(golden_meshes, mesh_dir):
+    """Union (with a mesh and an unbounded plane), Intersection and Substraction of mixed
+    shapes: identical hits, pieces and counters, and the image."""
+    st, scene, want, osc = _pair(CSG_SCENE, golden_meshes, mesh_dir, width=96, height=72)
+    assert scene.info()["object_count"] == 4
+    _check_scene_mode(st, scene, want, osc)
+    img = scene.render(st.camera, spp=32, max_depth=6, seed=2)
+    ref = osc.render(want["camera"], 32, 6, seed=2)
+    assert relmse(img, ref) < 5e-3
 
 
 def test_object_tree_bit_exact(golden_meshes, mesh_dir):
@@ -174,3 +208,29 @@ def test_api_built_tree_equals_loaded(golden_meshes, mesh_dir):
     np.testing.assert_array_equal(a[1], b[1])
     np.testing.assert_array_equal(a[0], b[0])
     assert a[3] == b[3]
+
+
+def test_api_built_csg_equals_loaded(golden_meshes, mesh_dir):
+    T = pb.Transform
+    I = T.identity()
+    text = """camera pin_hole pos 0 0.5 4 look 0 0 0 up 0 1 0
+    scene
+      object simple csg substraction {
+          elem sphere 1 transform { translate 0.5 0.5 0.5 }
+          elem aabox 2 2 2 transform { rotate_y 0.3 } }
+        lambertian color 0.5 0.5 0.5
+    """
+    # the file's elements, popped by the scene builder, come out reversed: the box is the base piece
+    shp = pb.Csg("subtraction", [(pb.AABox((2.0, 2.0, 2.0)), I * T.rotation_y(0.3)),
+                                 (pb.Sphere(1.0), I * T.translation((0.5, 0.5, 0.5)))])
+    s = pb.Scene().add_object(pb.Simple(shp, pb.Lambertian((0.5, 0.5, 0.5)))).commit()
+    loaded = pb.Stage(text, width=64, height=48)
+    rays = oracle.camera_rays(load_stage(text, fixture_mesh_loader(golden_meshes), width=64, height=48)["camera"],
+                              np.float32)
+    a = s.intersect_counted(rays)
+    b = loaded.scene().intersect_counted(rays)
+    for k in range(3):
+        np.testing.assert_array_equal(a[k], b[k])
+    assert a[3] == b[3]
+    hit = a[0] != pb.PBRT_MISS
+    assert hit.mean() > 0.04 and set(np.unique(a[0][hit] >> 24)) == {0, 1}  # box faces and the cavity

@@ -20,7 +20,7 @@ from oracle.stage import load_stage
 from pbrt_b200 import PbrtError
 
 SCENES = ["cornell_box_canonical.stage", "cornell_box.stage", "default.stage", "cube_mesh.stage",
-          "many_spheres.stage", "many_meshes.stage"]
+          "many_spheres.stage", "many_meshes.stage", "csg_union_spheres.stage"]
 
 
 def _f32(x):
@@ -50,6 +50,14 @@ def _compare(got: dict, want: dict):
         for k in ("radius", "height"):
             assert np.float32(a[k]) == np.float32(b.get(k, 0.0))
         np.testing.assert_array_equal(_f32(a["extent"]), _f32(b.get("extent", (0, 0, 0))))
+        assert ("csg" in a) == ("csg" in b)
+        if "csg" in b:
+            assert a["csg"]["op"] == b["csg"]["op"]
+            assert len(a["csg"]["elements"]) == len(b["csg"]["elements"])
+            for ea, eb in zip(a["csg"]["elements"], b["csg"]["elements"]):
+                assert ea["shape"] == eb["shape"] and np.float32(ea["radius"]) == np.float32(eb.get("radius", 0))
+                np.testing.assert_array_equal(ea["to_world"], _f32(eb["to_world"]))
+                np.testing.assert_array_equal(ea["to_local"], _f32(eb["to_local"]))
     assert len(got["nodes"]) == len(want["nodes"])
     for a, b in zip(got["nodes"], want["nodes"]):
         assert a["kind"] == b["kind"]
@@ -112,9 +120,11 @@ def test_loader_rejects_what_the_reference_rejects(text):
         pb.Stage(text)
 
 
-def test_csg_is_refused_as_unsupported(mesh_dir):
+def test_nested_csg_is_refused_as_unsupported():
+    text = ("camera pin_hole pos 0 0 5 look 0 0 0 up 0 1 0 scene object simple csg union { elem csg union { "
+            "elem sphere 1 transform { } } transform { } } lambertian color 1 1 1")
     with pytest.raises(PbrtError) as e:
-        pb.Stage(stage_text("csg_union_spheres.stage"), base_dir=mesh_dir)
+        pb.Stage(text)
     assert e.value.code == 6  # PBRT_ERR_UNSUPPORTED
 
 

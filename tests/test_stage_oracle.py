@@ -123,8 +123,9 @@ def test_every_fixture_scene_loads(golden_meshes):
         d = load_stage(stage_text(name), fixture_mesh_loader(golden_meshes))
         s = oracle.Scene(d, np.float32)
         assert s.counts()["primitives"] == len(d["roots"])
-    with pytest.raises(StageError):  # constructive solids are outside the ported shapes
-        load_stage(stage_text("csg_union_spheres.stage"), fixture_mesh_loader(golden_meshes))
+    d = load_stage(stage_text("csg_union_spheres.stage"), fixture_mesh_loader(golden_meshes))
+    csg = [o for o in d["objects"] if o["shape"] == 6]
+    assert len(csg) == 1 and csg[0]["csg"]["op"] == 0 and len(csg[0]["csg"]["elements"]) == 9
 
 
 def test_shapes_against_brute_force(golden_meshes):
@@ -168,3 +169,62 @@ def test_shapes_against_brute_force(golden_meshes):
         np.testing.assert_array_equal(t[hit], best_t[hit].astype(dt))
         occ = s.occluded(rays)
         np.testing.assert_array_equal(occ.astype(bool), hit)
+
+
+def _csg_scene(op, elements, extra=()):
+    """One constructive solid (and optional plain spheres) as a scene description."""
+    objs = [dict(shape=6, material=0, csg=dict(op=op, elements=[
+        dict(shape=sh, radius=r, to_world=w, to_local=l) for sh, r, (w, l) in elements]))]
+    for r, xf in extra:
+        w, l = xf.rows()
+        objs.append(dict(shape=1, radius=r, material=0, to_world=w, to_local=l))
+    return dict(meshes=[], materials=[dict(kind=0, color=(0.5, 0.5, 0.5))], objects=objs, lights=[])
+
+
+def _rays(n, seed, dt):
+    rng = np.random.default_rng(seed)
+    o = rng.uniform(-3, 3, (3, n))
+    d = rng.normal(size=(3, n))
+    d /= np.linalg.norm(d, axis=0)
+    return np.concatenate([o, d, np.full((1, n), 1e-4), np.full((1, n), 1e3)]).astype(dt)
+
+
+def test_csg_bound_of_a_sphere_cut_by_a_plane():
+    """intersection.rs:  the half-sphere is bounded by the sphere's box, in either order."""
+    ident = Xf.identity().rows()
+    for els in ([(1, 1.0, ident), (5, 0.0, ident)], [(5, 0.0, ident), (1, 1.0, ident)]):
+        s = oracle.Scene(_csg_scene(1, els), np.float64)
+        assert s.counts() == dict(primitives=1, unbounded=0, nodes=1)
+        boxes = s.bvh()[0]
+        np.testing.assert_array_equal(boxes[0], [-1, -1, -1, 1, 1, 1])
+
+
+def test_csg_union_of_disjoint_spheres_is_their_compound():
+    xs = [Xf.translation(x, 0.0, 0.0) for x in (-1.5, 0.0, 1.5)]
+    u = oracle.Scene(_csg_scene(0, [(1, 0.5, x.rows()) for x in xs]), np.float64)
+    c = oracle.Scene(_csg_scene(0, [], extra=[(0.5, x) for x in xs]), np.float64)
+    rays = _rays(20000, 3, np.float64)
+    _, ou, tu = u.trace(rays)
+    _, oc, tc = c.trace(rays)
+    hit = oc != oracle.MISS
+    np.testing.assert_array_equal(ou != oracle.MISS, hit)
+    np.testing.assert_array_equal(tu[hit], tc[hit])
+
+
+def test_csg_intersection_and_subtraction_geometry():
+    a, b = Xf.translation(-0.3, 0, 0).rows(), Xf.translation(0.3, 0, 0).rows()
+    rays = _rays(60000, 4, np.float64)
+    o, d = rays[0:3], rays[3:6]
+    for op in (1, 2):
+        s = oracle.Scene(_csg_scene(op, [(1, 1.0, a), (1, 0.8, b)]), np.float64)
+        _, obj, t = s.trace(rays)
+        hit = obj != oracle.MISS
+        assert hit.sum() > 300
+        p = o[:, hit] + d[:, hit] * t[hit]
+        da = np.linalg.norm(p - np.array([[-0.3], [0], [0]]), axis=0)
+        db = np.linalg.norm(p - np.array([[0.3], [0], [0]]), axis=0)
+        if op == 1:  # on one sphere, inside the other
+            assert np.all(((np.abs(da - 1) < 1e-9) & (db <= 0.8 + 1e-9)) | ((np.abs(db - 0.8) < 1e-9) & (da <= 1 + 1e-9)))
+        else:  # on the base outside the hole, or on the hole inside the base
+            assert np.all(((np.abs(da - 1) < 1e-9) & (db >= 0.8 - 1e-9)) | ((np.abs(db - 0.8) < 1e-9) & (da <= 1 + 1e-9)))
+        assert np.array_equal(s.occluded(rays).astype(bool), hit)
