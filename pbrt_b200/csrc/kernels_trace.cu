@@ -266,10 +266,9 @@ __global__ void __launch_bounds__(128, 12) k_mesh_closest_persistent(MeshView m,
           done = true;
           break;
         }
-        const float4 l0 = __ldg(&m.nodes[2 * lf]);
-        const float4 l1 = __ldg(&m.nodes[2 * lf + 1]);
-        const float4 r0 = __ldg(&m.nodes[2 * lf + 2]);
-        const float4 r1 = __ldg(&m.nodes[2 * lf + 3]);
+        float4 l0, l1, r0, r1;
+        load_node(&m.nodes[2 * lf], l0, l1);
+        load_node(&m.nodes[2 * lf + 2], r0, r1);
         float dl, dr;
         const bool hl = box_hit(r, l0, l1, near, far, dl);
         const bool hr = box_hit(r, r0, r1, near, far, dr);

@@ -526,8 +526,9 @@ PBRT_DEV bool scene_closest_t(const SceneView& s, const F3& o, const F3& d, floa
           }
         }
       } else {
-        const float4 l0 = __ldg(&s.top[2 * lf]), l1 = __ldg(&s.top[2 * lf + 1]);
-        const float4 r0 = __ldg(&s.top[2 * lf + 2]), r1 = __ldg(&s.top[2 * lf + 3]);
+        float4 l0, l1, r0, r1;
+        load_node(&s.top[2 * lf], l0, l1);
+        load_node(&s.top[2 * lf + 2], r0, r1);
         float dl, dr;
         if (kCount) cnt->boxes += 2;
         const bool hl = box_hit(r, l0, l1, near, min_t, dl);

@@ -13,7 +13,8 @@
 // and t are bit-identical to the FP32 restatement of the reference.
 //
 // Layout (mesh_bvh.hpp): nodes are 32-byte records read as two float4 (bmin|left_first,
-// bmax|count); a sibling pair is one aligned 64-byte read; triangles are three SoA
+// bmax|count); a sibling pair is one aligned 64-byte read
+// (two 256-bit loads); triangles are three SoA
 // streams in leaf order.
 #pragma once
 
@@ -29,6 +30,14 @@ enum DeviceError : uint32_t {
   kErrBudget = 1u,  // a traversal exceeded its iteration budget (malformed tree)
   kErrStack = 2u,   // a traversal stack would have overflowed
 };
+
+// One 32-byte node record (bmin|left_first, bmax|count) as a single 256-bit load. Node
+// arrays come from cudaMalloc and records are 32 bytes, so every record is 32-byte aligned.
+PBRT_DEV void load_node(const float4* p, float4& lo, float4& hi) {
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(lo.x), "=f"(lo.y), "=f"(lo.z), "=f"(lo.w), "=f"(hi.x), "=f"(hi.y), "=f"(hi.z), "=f"(hi.w)
+      : "l"(p));
+}
 
 struct MeshView {
   const float4* nodes;  // 2 float4 per node
@@ -164,10 +173,9 @@ PBRT_DEV uint32_t mesh_closest(const MeshView& m, const PRay& r, float near, flo
           }
         }
       } else {
-        const float4 l0 = __ldg(&m.nodes[2 * lf]);
-        const float4 l1 = __ldg(&m.nodes[2 * lf + 1]);
-        const float4 r0 = __ldg(&m.nodes[2 * lf + 2]);
-        const float4 r1 = __ldg(&m.nodes[2 * lf + 3]);
+        float4 l0, l1, r0, r1;
+        load_node(&m.nodes[2 * lf], l0, l1);
+        load_node(&m.nodes[2 * lf + 2], r0, r1);
         float dl, dr;
         if (kCount) cnt->box_tests += 2;
         const bool hl = box_hit(r, l0, l1, near, far, dl);
@@ -243,10 +251,9 @@ PBRT_DEV bool mesh_any(const MeshView& m, const PRay& r, float near, float far, 
         if (tri_hit(r, A, B, C.x, t) && t >= near && t <= far) return true;
       }
     } else {
-      const float4 l0 = __ldg(&m.nodes[2 * lf]);
-      const float4 l1 = __ldg(&m.nodes[2 * lf + 1]);
-      const float4 r0 = __ldg(&m.nodes[2 * lf + 2]);
-      const float4 r1 = __ldg(&m.nodes[2 * lf + 3]);
+      float4 l0, l1, r0, r1;
+      load_node(&m.nodes[2 * lf], l0, l1);
+      load_node(&m.nodes[2 * lf + 2], r0, r1);
       float dl, dr;
       const bool hl = box_hit(r, l0, l1, near, far, dl);
       const bool hr = box_hit(r, r0, r1, near, far, dr);

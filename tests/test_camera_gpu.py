@@ -56,7 +56,9 @@ def test_thin_lens_of_radius_zero_is_a_pinhole_up_to_rounding(golden_meshes):
     assert np.abs(a - b).mean() < 1e-3
 
 
-@pytest.mark.parametrize("name", ["default.stage", "cornell_box_canonical.stage", "cube_mesh.stage"])
+# many_spheres.stage (445 objects) takes the persistent extend walk, the others one thread per path
+@pytest.mark.parametrize("name", ["default.stage", "cornell_box_canonical.stage", "cube_mesh.stage",
+                                  "many_spheres.stage"])
 def test_normal_integrator_matches_oracle(name, golden_meshes, mesh_dir):
     opts = dict(width=64, height=48, fov_deg=60.0, far=2000.0)
     st = pb.Stage(stage_text(name), base_dir=mesh_dir, **opts)
