@@ -524,6 +524,31 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def _copy_floor_ms(rays_pin, rays_d, prim_pin, t_pin, prim_d, t_d, reps=5):
+    """Wall time of the host path's bare copies: the rays host->device on one stream while the
+    ids and t come back device->host on another (PCIe moves both directions at once)."""
+    import torch
+
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    flat_d = rays_d.view(-1)
+    flat_h = rays_pin.view(-1)
+
+    def once():
+        with torch.cuda.stream(s_in):
+            flat_d.copy_(flat_h, non_blocking=True)
+        with torch.cuda.stream(s_out):
+            prim_pin.copy_(prim_d, non_blocking=True)
+            t_pin.copy_(t_d, non_blocking=True)
+
+    once()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        once()
+    torch.cuda.synchronize()
+    return (time.perf_counter() - t0) / reps * 1e3
+
+
 def main():
     global N_RAYS
     ap = argparse.ArgumentParser()
@@ -655,6 +680,8 @@ def main():
     e2e_value = whole_job_rate(ws, N_RAYS, max_over_ranks(e2e_s, dist, rays_d.device)) / 1e6
     # the host path must agree with the device path
     assert torch.equal(prim_pin, prim_d.cpu()), "host-buffer results differ from device-buffer results"
+    # The bound of the host path: the same bytes copied bare (rays in, id + t out, concurrently).
+    copy_floor_ms = _copy_floor_ms(rays_pin, rays_d, prim_pin, t_pin, prim_d, t_d)
 
     if rank == 0:
         peak, peak_kind = _peaks()
@@ -671,7 +698,9 @@ def main():
                              "by design", "parallelism": f"replicas x{ws}"},
             "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": 32 * N_RAYS,
                     "d2h_bytes_per_step": 8 * N_RAYS, "steps": e2e_steps,
-                    "path": "pbrt_trace_closest with pinned host buffers, 3-slot pipelined H2D/kernel/D2H"},
+                    "path": "pbrt_trace_closest with pinned host buffers, 3-slot pipelined H2D/kernel/D2H",
+                    "copy_floor_ms": round(copy_floor_ms, 3),
+                    "frac_of_copy_floor": round(copy_floor_ms / (N_RAYS / (e2e_value * 1e6 / ws) * 1e3), 3)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": round(traffic) if traffic else None,
                          "peak_kind": peak_kind, "kernel": "k_mesh_closest",

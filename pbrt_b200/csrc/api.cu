@@ -607,7 +607,8 @@ int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, flo
 
   // Host buffers: pipeline chunks through three staging slots, each on its own stream, so
   // the copy engines and the SMs overlap (H2D of chunk k+1 and D2H of k-1 run under the
-  // kernel of chunk k).
+  // kernel of chunk k). With 1M-ray chunks and one 2D copy per chunk a 16M-ray call takes the
+  // time of its bare copies (512 MiB in, 128 MiB out concurrently: 10.3 ms on PCIe 5).
   PBRT_TRY(ensure_slots(c));
   if (c->user) PBRT_TRY(c->cuda(cudaStreamSynchronize(c->user), "cudaStreamSynchronize"));
   if (stats)
@@ -616,10 +617,10 @@ int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, flo
   for (uint64_t base = 0; base < n; base += kSlotRays, ++chunk) {
     Slot& sl = c->slots[chunk % kSlots];
     const uint64_t m = std::min<uint64_t>(kSlotRays, n - base);
-    for (int p = 0; p < 8; ++p)
-      PBRT_TRY(c->cuda(cudaMemcpyAsync(sl.rays + p * kSlotRays, rays + p * n + base, m * sizeof(float),
-                                       cudaMemcpyHostToDevice, sl.s),
-                       "cudaMemcpyAsync(rays)"));
+    // the chunk's eight planes as one 2D copy (rows = planes): one DMA job instead of eight
+    PBRT_TRY(c->cuda(cudaMemcpy2DAsync(sl.rays, kSlotRays * sizeof(float), rays + base, n * sizeof(float),
+                                       m * sizeof(float), 8, cudaMemcpyHostToDevice, sl.s),
+                     "cudaMemcpy2DAsync(rays)"));
     PBRT_TRY(c->cuda(launch(sl.rays, kSlotRays, m, sl.prim, sl.t, obj ? sl.obj : nullptr, occ ? sl.occ : nullptr,
                             counters, sl.queue, sl.fetch, sl.rec, sl.s),
                      "kernel launch"));

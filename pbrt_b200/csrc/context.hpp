@@ -17,7 +17,7 @@
 namespace pbrt {
 namespace api {
 
-constexpr uint64_t kSlotRays = uint64_t(1) << 21;  // rays per pipelined chunk (64 MiB of rays)
+constexpr uint64_t kSlotRays = uint64_t(1) << 20;  // rays per pipelined chunk (32 MiB of rays)
 constexpr int kSlots = 3;
 constexpr uint64_t kDevChunk = uint64_t(1) << 24;  // rays per launch pair on device buffers
 

@@ -81,7 +81,7 @@ def test_displaced_icosphere_incoherent(bins, max_leaf):
 
 def test_host_and_device_buffers_agree_across_chunks():
     v, f = W.displaced_icosphere(5, seed=21)
-    n = (1 << 21) * 2 + 12345  # three pipelined chunks, the last one partial
+    n = (1 << 21) * 2 + 12345  # five 1M-ray pipelined chunks over three staging slots, the last one partial
     rays = W.incoherent_rays(n, v.min(0), v.max(0), seed=22)
     s = _scene(v, f, 16, 4)
     hp, ht = s.intersect(rays)
