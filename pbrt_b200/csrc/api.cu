@@ -250,6 +250,8 @@ int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbr
   v.light_count = uint32_t(fs.lights.size());
   v.light_tris = (const float*)ltris;
   v.light_cdf = (const float*)lcdf;
+  v.has_csg = 0;
+  for (const ObjRec& ob : fs.objects) v.has_csg |= ob.shape == kShapeCsg ? 1u : 0u;
   s->info.object_count = fs.primitive_count;
   s->info.device_bytes += s->extra_bytes;
   s->max_radiance = fs.max_radiance;

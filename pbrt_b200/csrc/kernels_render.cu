@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(256) k_generate_batch(WaveBuffers w, const Bat
 // resident 256-thread blocks per SM (at most 64 registers a thread) for the traversal kernels:
 // measured 2-4% faster than the compiler's 86 registers on the Cornell, many-spheres and
 // torus-knot renders.
-template <class Src>
+template <class Src, bool kCsg>
 __global__ void __launch_bounds__(256, 4) k_extend(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
                                                 const uint32_t* __restrict__ qcount, uint32_t* err,
                                                 unsigned long long* stats) {
@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(256, 4) k_extend(WaveBuffers w, Src src, const
     const F3 o = mk3(w.ox[p], w.oy[p], w.oz[p]), d = mk3(w.dx[p], w.dy[p], w.dz[p]);
     float t = 0.f;
     uint32_t obj = 0xFFFFFFFFu, prim = 0;
-    if (!scene_closest(s, o, d, ps.near, ps.far, t, obj, prim, err)) obj = 0xFFFFFFFFu;
+    if (!scene_closest<kCsg>(s, o, d, ps.near, ps.far, t, obj, prim, err)) obj = 0xFFFFFFFFu;
     w.ht[p] = t;
     w.hobj[p] = obj;
     w.hprim[p] = prim;
@@ -423,7 +423,7 @@ __global__ void __launch_bounds__(256, 4) k_extend(WaveBuffers w, Src src, const
 // scene_closest: the same boxes, the same order, the same adoptions. It pays where the
 // top-level tree is deep (10,000 spheres: 259 -> 177 ms a frame) and costs where a path's
 // query is a few nodes (a 4-object box: 2.7 -> 3.1 ms), hence kWalkMinTopNodes.
-template <class Src>
+template <class Src, bool kCsg>
 __global__ void __launch_bounds__(256, 4) k_extend_walk(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
                                                      const uint32_t* __restrict__ qcount, uint32_t* __restrict__ fetch,
                                                 uint32_t* err, unsigned long long* stats) {
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(256, 4) k_extend_walk(WaveBuffers w, Src src, 
         for (uint32_t u = 0; u < s.unbounded_count; ++u) {  // nearest_among + closer (scene.rs:222-249)
           float t;
           uint32_t leaf, prim;
-          if (prim_closest(s, __ldg(&s.unbounded[u]), o, d, near, ps.far, t, leaf, prim, err) &&
+          if (prim_closest<kCsg>(s, __ldg(&s.unbounded[u]), o, d, near, ps.far, t, leaf, prim, err) &&
               (!have || t < min_t)) {
             have = true;
             min_t = t;
@@ -553,7 +553,7 @@ __global__ void __launch_bounds__(256, 4) k_extend_walk(WaveBuffers w, Src src, 
           const uint32_t ref = __ldg(&s.order[k]);
           float t;
           uint32_t leaf, prim;
-          if (prim_closest(s, ref, o, d, near, min_t, t, leaf, prim, err) && (!have || t < min_t)) {
+          if (prim_closest<kCsg>(s, ref, o, d, near, min_t, t, leaf, prim, err) && (!have || t < min_t)) {
             have = true;
             min_t = t;
             leaf_out = leaf;
@@ -771,7 +771,7 @@ __global__ void __launch_bounds__(256) k_train_batch(WaveBuffers w, CacheWave cw
   }
 }
 
-template <class Src>
+template <class Src, bool kCsg>
 __global__ void __launch_bounds__(256, 4) k_shadow(WaveBuffers w, Src src, uint32_t* err, unsigned long long* stats) {
   const uint32_t n = w.counts[2];
   if (stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(stats + 1, (unsigned long long)n);
@@ -779,7 +779,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow(WaveBuffers w, Src src, uint3
     const uint32_t p = w.s_path[k];
     const SceneView& s = src.view(w, p);
     const F3 o = mk3(w.s_ox[k], w.s_oy[k], w.s_oz[k]), d = mk3(w.s_dx[k], w.s_dy[k], w.s_dz[k]);
-    if (!scene_any(s, o, d, kShadowEps, w.s_tmax[k], err)) {  // VisibilityTester::unoccluded (lights.rs:67-69)
+    if (!scene_any<kCsg>(s, o, d, kShadowEps, w.s_tmax[k], err)) {  // VisibilityTester::unoccluded (lights.rs:67-69)
       w.lr[p] = fa(w.lr[p], w.s_cr[k]);
       w.lg[p] = fa(w.lg[p], w.s_cg[k]);
       w.lb[p] = fa(w.lb[p], w.s_cb[k]);
@@ -836,7 +836,7 @@ PBRT_DEV void flush_counts(const SceneCount& c, unsigned long long* cnt) {
 
 // Nearest hit per ray; object ids are the description's (the leaf's desc_id). kCount adds
 // the scene accelerator's counters (Scene::intersect_instrumented) into cnt.
-template <bool kCount>
+template <bool kCount, bool kCsg>
 __global__ void __launch_bounds__(128) k_scene_closest(SceneView s, const float* __restrict__ rays, uint64_t stride,
                                                        uint64_t n, uint32_t* __restrict__ prim, float* __restrict__ tout,
                                                        uint32_t* __restrict__ obj, unsigned long long* cnt,
@@ -853,7 +853,7 @@ __global__ void __launch_bounds__(128) k_scene_closest(SceneView s, const float*
     const float near = __ldcs(rays + 6 * stride + i), far = __ldcs(rays + 7 * stride + i);
     float t = 0.f;
     uint32_t leaf = 0, pr = 0;
-    const bool hit = scene_closest_t<kCount>(s, o, d, near, far, t, leaf, pr, err, &c);
+    const bool hit = scene_closest_t<kCount, kCsg>(s, o, d, near, far, t, leaf, pr, err, &c);
     __stcs(prim + i, hit ? pr : 0xFFFFFFFFu);
     __stcs(tout + i, hit ? t : __int_as_float(0x7f800000));
     if (obj) __stcs(obj + i, hit ? s.objects[leaf].desc_id : 0xFFFFFFFFu);
@@ -861,7 +861,7 @@ __global__ void __launch_bounds__(128) k_scene_closest(SceneView s, const float*
   if (kCount) flush_counts(c, cnt);
 }
 
-template <bool kCount>
+template <bool kCount, bool kCsg>
 __global__ void __launch_bounds__(128) k_scene_any(SceneView s, const float* __restrict__ rays, uint64_t stride,
                                                    uint64_t n, uint8_t* __restrict__ occ, unsigned long long* cnt,
                                                    uint32_t* err) {
@@ -873,7 +873,9 @@ __global__ void __launch_bounds__(128) k_scene_any(SceneView s, const float* __r
     if (i >= n) continue;
     const F3 o = mk3(__ldcs(rays + i), __ldcs(rays + stride + i), __ldcs(rays + 2 * stride + i));
     const F3 d = mk3(__ldcs(rays + 3 * stride + i), __ldcs(rays + 4 * stride + i), __ldcs(rays + 5 * stride + i));
-    occ[i] = scene_any_t<kCount>(s, o, d, __ldcs(rays + 6 * stride + i), __ldcs(rays + 7 * stride + i), err, &c) ? 1 : 0;
+    occ[i] = scene_any_t<kCount, kCsg>(s, o, d, __ldcs(rays + 6 * stride + i), __ldcs(rays + 7 * stride + i), err, &c)
+                 ? 1
+                 : 0;
   }
   if (kCount) flush_counts(c, cnt);
 }
@@ -890,8 +892,9 @@ cudaError_t launch_scene_closest(const SceneView& s, const float* rays, uint64_t
                                  cudaStream_t st) {
   if (n == 0) return cudaSuccess;
   const unsigned g = grid_cap(n, 128, sm_count, 32);
-  if (cnt) k_scene_closest<true><<<g, 128, 0, st>>>(s, rays, stride, n, prim, t, obj, cnt, err);
-  else k_scene_closest<false><<<g, 128, 0, st>>>(s, rays, stride, n, prim, t, obj, nullptr, err);
+  if (cnt) k_scene_closest<true, true><<<g, 128, 0, st>>>(s, rays, stride, n, prim, t, obj, cnt, err);
+  else if (s.has_csg) k_scene_closest<false, true><<<g, 128, 0, st>>>(s, rays, stride, n, prim, t, obj, nullptr, err);
+  else k_scene_closest<false, false><<<g, 128, 0, st>>>(s, rays, stride, n, prim, t, obj, nullptr, err);
   return cudaGetLastError();
 }
 
@@ -899,8 +902,9 @@ cudaError_t launch_scene_any(const SceneView& s, const float* rays, uint64_t str
                              unsigned long long* cnt, uint32_t* err, int sm_count, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
   const unsigned g = grid_cap(n, 128, sm_count, 32);
-  if (cnt) k_scene_any<true><<<g, 128, 0, st>>>(s, rays, stride, n, occ, cnt, err);
-  else k_scene_any<false><<<g, 128, 0, st>>>(s, rays, stride, n, occ, nullptr, err);
+  if (cnt) k_scene_any<true, true><<<g, 128, 0, st>>>(s, rays, stride, n, occ, cnt, err);
+  else if (s.has_csg) k_scene_any<false, true><<<g, 128, 0, st>>>(s, rays, stride, n, occ, nullptr, err);
+  else k_scene_any<false, false><<<g, 128, 0, st>>>(s, rays, stride, n, occ, nullptr, err);
   return cudaGetLastError();
 }
 
@@ -909,11 +913,13 @@ cudaError_t launch_scene_any(const SceneView& s, const float* rays, uint64_t str
 constexpr uint32_t kWalkMinTopNodes = 64;
 
 // extend -> shade -> shadow, `loops` times, over the ping-pong queues. `top_nodes`: the largest
-// top-level tree among the scenes rendered.
+// top-level tree among the scenes rendered; `csg`: some scene holds a constructive solid (the
+// traversal kernels are also built without the solids' code, which takes registers and spills
+// from every other query).
 template <class Src>
 static cudaError_t bounce_loop(const WaveBuffers& w, const Src& src, const CacheWave& cw, uint32_t loops, bool shadows,
                                uint32_t cache_mode, uint32_t term_hit, const LaunchShape& sh, unsigned long long* stats,
-                               uint32_t* err, int sm_count, cudaStream_t st, uint32_t top_nodes) {
+                               uint32_t* err, int sm_count, cudaStream_t st, uint32_t top_nodes, bool csg) {
   cudaError_t e;
   const unsigned gt = unsigned(sm_count) * sh.trace_blocks_per_sm, gs = unsigned(sm_count) * sh.shade_blocks_per_sm;
   for (uint32_t b = 0; b < loops; ++b) {
@@ -924,14 +930,19 @@ static cudaError_t bounce_loop(const WaveBuffers& w, const Src& src, const Cache
     if ((e = cudaMemsetAsync(cout, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
     // counts[2]: shadow rays queued by k_shade; counts[3]: k_extend_walk's fetch position
     if ((e = cudaMemsetAsync(w.counts + 2, 0, 2 * sizeof(uint32_t), st)) != cudaSuccess) return e;
-    if (top_nodes >= kWalkMinTopNodes)
-      k_extend_walk<Src><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, w.counts + 3, err, stats);
+    if (top_nodes >= kWalkMinTopNodes && csg)
+      k_extend_walk<Src, true><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, w.counts + 3, err, stats);
+    else if (top_nodes >= kWalkMinTopNodes)
+      k_extend_walk<Src, false><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, w.counts + 3, err, stats);
+    else if (csg)
+      k_extend<Src, true><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, err, stats);
     else
-      k_extend<Src><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, err, stats);
+      k_extend<Src, false><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, err, stats);
     k_shade<Src><<<gs, sh.shade_threads, 0, st>>>(w, src, qin, cin, qout, cout, cw, cache_mode, term_hit);
     // (a persistent walk for the shadow rays measured 2.6% slower on 10,000 spheres: any-hit
     // rays end early, so one thread per ray wastes little)
-    if (shadows) k_shadow<Src><<<gt, sh.trace_threads, 0, st>>>(w, src, err, stats);
+    if (shadows && csg) k_shadow<Src, true><<<gt, sh.trace_threads, 0, st>>>(w, src, err, stats);
+    else if (shadows) k_shadow<Src, false><<<gt, sh.trace_threads, 0, st>>>(w, src, err, stats);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -952,15 +963,18 @@ cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, 
       host_table[nscenes - 1].begin + (unsigned long long)host_table[nscenes - 1].npix * host_table[nscenes - 1].spp;
   const ManyScenes src{table};
   uint32_t top_nodes = 0;
-  for (uint32_t i = 0; i < nscenes; ++i)
+  bool csg = false;
+  for (uint32_t i = 0; i < nscenes; ++i) {
     top_nodes = top_nodes > host_table[i].view.top_node_count ? top_nodes : host_table[i].view.top_node_count;
+    csg = csg || host_table[i].view.has_csg;
+  }
   uint32_t next_done = 0;
   for (unsigned long long base = 0; base < total; base += wave) {
     const uint32_t n = uint32_t(total - base < wave ? total - base : wave);
     k_generate_batch<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, table, nscenes, base, n, frame, stats);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = bounce_loop(w, src, CacheWave{}, max_depth, any_path_integrator, kCacheOff, 0, shape, stats, err, sm_count,
-                         st, top_nodes)) != cudaSuccess)
+                         st, top_nodes, csg)) != cudaSuccess)
       return e;
     k_accumulate_batch<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, n, table);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -986,7 +1000,7 @@ cudaError_t trace_wave(const SceneView& s, const WaveBuffers& w, const CacheWave
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const OneScene src{s, PathSettings{rs.max_depth, rs.rr_start, rs.integrator, cam.near, cam.far}};
   return bounce_loop(w, src, cw, rs.loop_depth ? rs.loop_depth : rs.max_depth, !rs.integrator, rs.cache_mode, rs.term_hit,
-                     rs.shape, rs.stats, err, sm_count, st, s.top_node_count);
+                     rs.shape, rs.stats, err, sm_count, st, s.top_node_count, s.has_csg != 0);
 }
 
 cudaError_t accumulate_wave(const WaveBuffers& w, uint32_t n, double* film, uint32_t image_w, const RenderSettings& rs,

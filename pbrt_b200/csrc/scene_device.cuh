@@ -48,6 +48,7 @@ struct SceneView {
   uint32_t light_count;
   const float* light_tris;  // area lights: 9 floats per world-space triangle
   const float* light_cdf;   // running area per triangle
+  uint32_t has_csg;         // some leaf is a constructive solid: only the kernels built with CSG may run it
 };
 
 struct Isect {
@@ -379,6 +380,7 @@ PBRT_DEV void local_ray(const SceneView& s, const ObjRec& ob, const F3& o, const
 
 // Object::intersect distance of one leaf within [near, far]; prim = triangle index, cylinder
 // piece or box face (0 for the other shapes).
+template <bool kCsg = true>
 PBRT_DEV bool leaf_closest(const SceneView& s, uint32_t li, const F3& o, const F3& d, float near, float far,
                            float& t, uint32_t& prim, uint32_t* err) {
   const ObjRec& ob = s.objects[li];
@@ -407,11 +409,14 @@ PBRT_DEV bool leaf_closest(const SceneView& s, uint32_t li, const F3& o, const F
       prim = uint32_t(face);
       return hit;
     }
-    case kShapeCsg: return csg_closest(s, ob, lo, ld, near, far, t, prim, err);
+    case kShapeCsg:
+      if (kCsg) return csg_closest(s, ob, lo, ld, near, far, t, prim, err);
+      return false;
     default: return plane_hit(lo, ld, near, far, t);
   }
 }
 
+template <bool kCsg = true>
 PBRT_DEV bool leaf_any(const SceneView& s, uint32_t li, const F3& o, const F3& d, float near, float far,
                        uint32_t* err) {
   const ObjRec& ob = s.objects[li];
@@ -426,6 +431,7 @@ PBRT_DEV bool leaf_any(const SceneView& s, uint32_t li, const F3& o, const F3& d
     case kShapeRectangle: return rectangle_hit(ob.p[0], ob.p[1], lo, ld, near, far, t);
     case kShapeAABox: return aabox_hit(ob.p, lo, ld, near, far, t, k);
     case kShapeCsg: {  // the default intersect_p: any listed hit (intersectable.rs:48-50)
+      if (!kCsg) return false;
       uint32_t prim;
       return csg_closest(s, ob, lo, ld, near, far, t, prim, err);
     }
@@ -436,18 +442,19 @@ PBRT_DEV bool leaf_any(const SceneView& s, uint32_t li, const F3& o, const F3& d
 // ---- primitives (a leaf or a compound) -----------------------------------------------------
 // A compound asks every member over the same [near, far] and keeps the strictly nearest hit,
 // the earlier member on a tie (compound.rs:21-38).
+template <bool kCsg = true>
 PBRT_DEV bool prim_closest(const SceneView& s, uint32_t ref, const F3& o, const F3& d, float near, float far,
                            float& t, uint32_t& leaf, uint32_t& prim, uint32_t* err) {
   if (!(ref & kGroupBit)) {
     leaf = ref;
-    return leaf_closest(s, ref, o, d, near, far, t, prim, err);
+    return leaf_closest<kCsg>(s, ref, o, d, near, far, t, prim, err);
   }
   const GroupRec g = s.groups[ref & ~kGroupBit];
   bool have = false;
   for (uint32_t k = 0; k < g.count; ++k) {
     float tk;
     uint32_t pk;
-    if (leaf_closest(s, g.first + k, o, d, near, far, tk, pk, err) && (!have || tk < t)) {
+    if (leaf_closest<kCsg>(s, g.first + k, o, d, near, far, tk, pk, err) && (!have || tk < t)) {
       have = true;
       t = tk;
       leaf = g.first + k;
@@ -457,19 +464,20 @@ PBRT_DEV bool prim_closest(const SceneView& s, uint32_t ref, const F3& o, const 
   return have;
 }
 
+template <bool kCsg = true>
 PBRT_DEV bool prim_any(const SceneView& s, uint32_t ref, const F3& o, const F3& d, float near, float far,
                        uint32_t* err) {
-  if (!(ref & kGroupBit)) return leaf_any(s, ref, o, d, near, far, err);
+  if (!(ref & kGroupBit)) return leaf_any<kCsg>(s, ref, o, d, near, far, err);
   const GroupRec g = s.groups[ref & ~kGroupBit];
   for (uint32_t k = 0; k < g.count; ++k)
-    if (leaf_any(s, g.first + k, o, d, near, far, err)) return true;  // compound.rs:47-49
+    if (leaf_any<kCsg>(s, g.first + k, o, d, near, far, err)) return true;  // compound.rs:47-49
   return false;
 }
 
 // Scene::find_nearest: the unbounded primitives first, each over [near, far]; then the
 // top-level query over [near, nearest so far], narrowing to every adopted hit and offering
 // each primitive [near, min_t]; a candidate is adopted only when strictly nearer.
-template <bool kCount>
+template <bool kCount, bool kCsg = true>
 PBRT_DEV bool scene_closest_t(const SceneView& s, const F3& o, const F3& d, float near, float far, float& t_out,
                               uint32_t& leaf_out, uint32_t& prim_out, uint32_t* err, SceneCount* cnt) {
   float min_t = far;
@@ -478,7 +486,7 @@ PBRT_DEV bool scene_closest_t(const SceneView& s, const F3& o, const F3& d, floa
     if (kCount) cnt->objects++;
     float t;
     uint32_t leaf, prim;
-    if (prim_closest(s, __ldg(&s.unbounded[k]), o, d, near, far, t, leaf, prim, err) && (!have || t < min_t)) {
+    if (prim_closest<kCsg>(s, __ldg(&s.unbounded[k]), o, d, near, far, t, leaf, prim, err) && (!have || t < min_t)) {
       have = true;
       min_t = t;
       leaf_out = leaf;
@@ -518,7 +526,7 @@ PBRT_DEV bool scene_closest_t(const SceneView& s, const F3& o, const F3& d, floa
           const uint32_t ref = __ldg(&s.order[k]);
           float t;
           uint32_t leaf, prim;
-          if (prim_closest(s, ref, o, d, near, min_t, t, leaf, prim, err) && (!have || t < min_t)) {
+          if (prim_closest<kCsg>(s, ref, o, d, near, min_t, t, leaf, prim, err) && (!have || t < min_t)) {
             have = true;
             min_t = t;
             leaf_out = leaf;
@@ -566,19 +574,20 @@ PBRT_DEV bool scene_closest_t(const SceneView& s, const F3& o, const F3& d, floa
   return have;
 }
 
+template <bool kCsg = true>
 PBRT_DEV bool scene_closest(const SceneView& s, const F3& o, const F3& d, float near, float far, float& t_out,
                             uint32_t& leaf_out, uint32_t& prim_out, uint32_t* err) {
-  return scene_closest_t<false>(s, o, d, near, far, t_out, leaf_out, prim_out, err, nullptr);
+  return scene_closest_t<false, kCsg>(s, o, d, near, far, t_out, leaf_out, prim_out, err, nullptr);
 }
 
 // Scene::any_hit: the unbounded primitives first; then unordered, the box tested at pop,
 // right pushed before left (bvh.rs:269-270).
-template <bool kCount>
+template <bool kCount, bool kCsg = true>
 PBRT_DEV bool scene_any_t(const SceneView& s, const F3& o, const F3& d, float near, float far, uint32_t* err,
                           SceneCount* cnt) {
   for (uint32_t k = 0; k < s.unbounded_count; ++k) {  // any_blocks (scene.rs:170-184)
     if (kCount) cnt->objects++;
-    if (prim_any(s, __ldg(&s.unbounded[k]), o, d, near, far, err)) return true;
+    if (prim_any<kCsg>(s, __ldg(&s.unbounded[k]), o, d, near, far, err)) return true;
   }
   if (s.top_node_count == 0) return false;
   const PRay r = prepare_ray(o, d);
@@ -601,7 +610,7 @@ PBRT_DEV bool scene_any_t(const SceneView& s, const F3& o, const F3& d, float ne
     if (count > 0) {
       for (uint32_t k = lf; k < lf + count; ++k) {
         if (kCount) cnt->objects++;
-        if (prim_any(s, __ldg(&s.order[k]), o, d, near, far, err)) return true;
+        if (prim_any<kCsg>(s, __ldg(&s.order[k]), o, d, near, far, err)) return true;
       }
     } else {
       if (sp + 2 > kTraceStack) {
@@ -615,8 +624,9 @@ PBRT_DEV bool scene_any_t(const SceneView& s, const F3& o, const F3& d, float ne
   return false;
 }
 
+template <bool kCsg = true>
 PBRT_DEV bool scene_any(const SceneView& s, const F3& o, const F3& d, float near, float far, uint32_t* err) {
-  return scene_any_t<false>(s, o, d, near, far, err, nullptr);
+  return scene_any_t<false, kCsg>(s, o, d, near, far, err, nullptr);
 }
 
 // ---- the interaction of an adopted hit -----------------------------------------------------
