@@ -12,21 +12,20 @@
 
 namespace {
 
-uint32_t crc_table[256];
-
-void init_crc() {
-  static bool done = false;
-  if (done) return;
-  for (uint32_t n = 0; n < 256; ++n) {  // CRC-32, polynomial 0xEDB88320 (PNG spec, ISO 3309)
-    uint32_t c = n;
-    for (int k = 0; k < 8; ++k) c = (c & 1u) ? 0xEDB88320u ^ (c >> 1) : c >> 1;
-    crc_table[n] = c;
+struct CrcTable {
+  uint32_t v[256];
+  CrcTable() {
+    for (uint32_t n = 0; n < 256; ++n) {  // CRC-32, polynomial 0xEDB88320 (PNG spec, ISO 3309)
+      uint32_t c = n;
+      for (int k = 0; k < 8; ++k) c = (c & 1u) ? 0xEDB88320u ^ (c >> 1) : c >> 1;
+      v[n] = c;
+    }
   }
-  done = true;
-}
+};
+const CrcTable crc_table;  // built at load time, read-only afterwards
 
 uint32_t crc(const uint8_t* p, size_t n, uint32_t c = 0xFFFFFFFFu) {
-  for (size_t i = 0; i < n; ++i) c = crc_table[(c ^ p[i]) & 0xFFu] ^ (c >> 8);
+  for (size_t i = 0; i < n; ++i) c = crc_table.v[(c ^ p[i]) & 0xFFu] ^ (c >> 8);
   return c;
 }
 
@@ -50,7 +49,6 @@ void chunk(std::vector<uint8_t>& out, const char* type, const std::vector<uint8_
 extern "C" int pbrt_write_png(const char* path, const uint8_t* rgba, uint32_t width, uint32_t height) {
   if (!path || !rgba || width == 0 || height == 0) return PBRT_ERR_INVALID_ARGUMENT;
   if (uint64_t(width) * 4 + 1 > 0x7FFFFFFFull || uint64_t(height) > 0x7FFFFFFFull) return PBRT_ERR_INVALID_ARGUMENT;
-  init_crc();
   // scanlines: filter type 0, then the row's RGBA bytes
   const size_t row = size_t(width) * 4;
   std::vector<uint8_t> raw;

@@ -350,17 +350,24 @@ cudaError_t launch_mesh_closest(const MeshView& m, const float* rays, uint64_t s
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// Resident 128-thread blocks per SM of the persistent traversal (the same on every B200);
+// computed once, thread-safely, by the first launch.
+template <bool kRec>
+static int persistent_blocks_per_sm() {
+  static const int v = [] {
+    int b = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_mesh_closest_persistent<kRec>, 128, 0);
+    return e == cudaSuccess && b > 0 ? b : 8;
+  }();
+  return v;
+}
+
 cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays, uint64_t stride, uint64_t n,
                                            uint32_t* prim, float* t, uint32_t* obj, uint32_t* queue,
                                            unsigned long long* counters, uint32_t* err, int sm_count, cudaStream_t s,
                                            float4* rec) {
   if (n == 0) return cudaSuccess;
-  static int blocks_per_sm = 0;
-  if (blocks_per_sm == 0) {
-    cudaError_t e =
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_mesh_closest_persistent<true>, 128, 0);
-    if (e != cudaSuccess || blocks_per_sm <= 0) blocks_per_sm = 8;
-  }
+  const int blocks_per_sm = persistent_blocks_per_sm<true>();
   cudaError_t e = cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;
   const bool vec = stride % 4 == 0 && aligned16(rays) && aligned16(prim) && aligned16(t) && (!obj || aligned16(obj));
@@ -432,11 +439,7 @@ cudaError_t launch_mesh_closest_noalloc(const MeshView& m, const float* rays, ui
   unsigned long long* counters = reinterpret_cast<unsigned long long*>(scratch);
   uint32_t* err = scratch + 4;
   uint32_t* queue = scratch + 64;
-  static int blocks_per_sm = 0;
-  if (blocks_per_sm == 0) {
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_mesh_closest_persistent<false>, 128, 0);
-    if (e != cudaSuccess || blocks_per_sm <= 0) blocks_per_sm = 8;
-  }
+  const int blocks_per_sm = persistent_blocks_per_sm<false>();
   const bool vec = n % 4 == 0 && aligned16(rays) && aligned16(prim) && aligned16(t);
   const uint64_t per_block = uint64_t(kCullThreads) * kCullRays;
   const uint64_t cull_need = (n + per_block - 1) / per_block, cull_cap = uint64_t(sm_count) * 8;

@@ -16,6 +16,7 @@
 // second kernel and Adam updates the FP32 master weights and rewrites both BF16 packs.
 #include <cuda_bf16.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "mlp.hpp"
@@ -380,15 +381,25 @@ cudaError_t launch_infer(const Net& net, const Bounds& b, const float* records, 
   return launch_infer_dev(net, b, records, nullptr, n, out, err, sm_count, s);
 }
 
+// The dynamic shared-memory limit of a kernel is a per-device attribute: set it once on each
+// device the kernel runs on (one bit per device; setting it twice is harmless).
+static cudaError_t allow_smem(std::atomic<uint64_t>& done, const void* kernel, size_t bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t bit = dev >= 0 && dev < 64 ? uint64_t(1) << dev : 0;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+  if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+  return e;
+}
+
 cudaError_t launch_infer_dev(const Net& net, const Bounds& b, const float* records, const uint32_t* n_dev,
                              uint64_t n, float* out, uint32_t* err, int sm_count, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, int(infer_smem_bytes()));
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  static std::atomic<uint64_t> configured{0};
+  cudaError_t e = allow_smem(configured, reinterpret_cast<const void*>(k_mlp_infer), infer_smem_bytes());
+  if (e != cudaSuccess) return e;
   const uint64_t tiles = (n + kTile - 1) / kTile;
   const uint64_t cap = uint64_t(sm_count) * 2;
   k_mlp_infer<<<unsigned(tiles < cap ? tiles : cap), kTile, infer_smem_bytes(), s>>>(net, b, records, n, n_dev, out,
@@ -399,12 +410,9 @@ cudaError_t launch_infer_dev(const Net& net, const Bounds& b, const float* recor
 cudaError_t launch_grad_tiles(const Net& net, const Bounds& b, const float* records, const float* targets, uint64_t n,
                               float grad_scale, float* partials, float* tile_loss, uint32_t* err, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, int(train_smem_bytes()));
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  static std::atomic<uint64_t> configured{0};
+  cudaError_t e = allow_smem(configured, reinterpret_cast<const void*>(k_mlp_grad), train_smem_bytes());
+  if (e != cudaSuccess) return e;
   const uint64_t tiles = (n + kTile - 1) / kTile;
   k_mlp_grad<<<unsigned(tiles), kTile, train_smem_bytes(), s>>>(net, b, records, targets, n, grad_scale, partials,
                                                                  tile_loss, err);
