@@ -16,6 +16,8 @@ import oracle
 import pbrt_b200 as pb
 from conftest import fixture_mesh_loader, stage_text
 from oracle.stage import load_stage
+from pbrt_b200 import workloads as W
+from pbrt_b200.scene import Batch, render_params
 
 pytestmark = pytest.mark.gpu
 
@@ -234,3 +236,20 @@ def test_api_built_csg_equals_loaded(golden_meshes, mesh_dir):
     assert a[3] == b[3]
     hit = a[0] != pb.PBRT_MISS
     assert hit.mean() > 0.04 and set(np.unique(a[0][hit] >> 24)) == {0, 1}  # box faces and the cavity
+
+
+def test_batch_mixing_solids_and_plain_scenes_equals_single_renders(mesh_dir):
+    """A batch that holds a scene with constructive solids runs every scene through the
+    kernels built with the solids' code, while a scene without solids rendered alone takes
+    the build without it: the films must still be equal."""
+    st = pb.Stage(CSG_SCENE, base_dir=mesh_dir, width=48, height=36)
+    csg = st.scene()
+    d, cam = W.cornell_box(32, 24)
+    plain = pb.Scene.from_description(d).commit()
+    kw = dict(spp=3, max_depth=5, seed=4)
+    singles = [csg.render(st.camera, **kw), plain.render(cam, **kw)]
+    b = Batch([csg, plain], [render_params(st.camera, **kw), render_params(cam, **kw)])
+    films = b.render(0)
+    for f, s in zip(films, singles):
+        np.testing.assert_allclose(f, s, rtol=1e-12, atol=1e-15)
+    b.close()
