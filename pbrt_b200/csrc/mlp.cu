@@ -31,6 +31,7 @@ constexpr uint32_t kXBytes = kTile * kInPad * 2;    // 24,576
 constexpr uint32_t kHBytes = kTile * kHidden * 2;   // 16,384
 constexpr uint32_t kG16Bytes = kTile * kOutPad * 2;  // 4,096
 constexpr uint32_t kTmemCols = 64;
+static_assert(kXBytes >= kHBytes, "the inference kernel stores the hidden tile over the input tile");
 
 __device__ __forceinline__ uint16_t to_bf16(float f) { return __bfloat16_as_ushort(__float2bfloat16_rn(f)); }
 __device__ __forceinline__ float from_bf16(uint16_t b) { return __uint_as_float(uint32_t(b) << 16); }
@@ -134,7 +135,11 @@ __device__ __forceinline__ void release_tmem(uint32_t tmem, uint64_t* mbar, uint
   if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(tmem, kTmemCols);
 }
 
-__global__ void __launch_bounds__(kTile, 1) k_mlp_infer(Net net, Bounds b, const float* __restrict__ rec, uint64_t n,
+// Three CTAs per SM (shared memory: the weights and one activation tile each; TMEM: 64 columns
+// each): while one CTA waits on its GEMM, the others encode, read TMEM or store activations.
+constexpr int kInferCtasPerSm = 3;
+
+__global__ void __launch_bounds__(kTile, kInferCtasPerSm) k_mlp_infer(Net net, Bounds b, const float* __restrict__ rec, uint64_t n,
                                                          const uint32_t* __restrict__ n_dev, float* __restrict__ out,
                                                          uint32_t* err) {
   if (n_dev) n = min(n, uint64_t(*n_dev));  // a count the previous kernel left on the device
@@ -142,8 +147,11 @@ __global__ void __launch_bounds__(kTile, 1) k_mlp_infer(Net net, Bounds b, const
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* sW = smem;
   uint8_t* sX = sW + kWBytes;
-  uint8_t* sH = sX + kXBytes;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(sH + kHBytes);
+  // The hidden activations overwrite the input tile: a layer's GEMM has finished reading its
+  // A operand (wait_gemm) before any thread stores the next layer's, and the next tile's
+  // features are stored only after the last layer's GEMM has completed.
+  uint8_t* sH = sX;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sX + kXBytes);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
   load_smem(sW, net.wpk_fwd, kWBytes);
   setup_tmem(mbar, tslot);
@@ -373,7 +381,7 @@ __global__ void k_pack(const float* __restrict__ w, uint16_t* fwd, uint16_t* bwd
   if (p < uint32_t(kParams)) pack_one(p, w[p], fwd, bwd);
 }
 
-size_t infer_smem_bytes() { return kWBytes + kXBytes + kHBytes + 64; }
+size_t infer_smem_bytes() { return kWBytes + kXBytes + 64; }
 size_t train_smem_bytes() { return 2 * kWBytes + kXBytes + 5 * kHBytes + kHBytes + kG16Bytes + 64; }
 
 cudaError_t launch_infer(const Net& net, const Bounds& b, const float* records, uint64_t n, float* out, uint32_t* err,
@@ -401,7 +409,7 @@ cudaError_t launch_infer_dev(const Net& net, const Bounds& b, const float* recor
   cudaError_t e = allow_smem(configured, reinterpret_cast<const void*>(k_mlp_infer), infer_smem_bytes());
   if (e != cudaSuccess) return e;
   const uint64_t tiles = (n + kTile - 1) / kTile;
-  const uint64_t cap = uint64_t(sm_count) * 2;
+  const uint64_t cap = uint64_t(sm_count) * kInferCtasPerSm;
   k_mlp_infer<<<unsigned(tiles < cap ? tiles : cap), kTile, infer_smem_bytes(), s>>>(net, b, records, n, n_dev, out,
                                                                                      err);
   return cudaGetLastError();
