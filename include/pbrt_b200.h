@@ -417,8 +417,11 @@ int pbrt_cache_load(pbrt_cache* cache, const void* buf, uint64_t size);
  * its throughput times the network's output clamped to [0, Lmax]. Lmax is the largest
  * radiance an emitter of the scene gives off (diffuse-light materials, infinite lights;
  * unbounded with a point light): no energy-conserving surface reflects more. Training
- * targets are clamped the same way. spp = 0 only trains (film may be NULL). The
- * integrator must be PBRT_INTEGRATOR_PATH. A cache whose scene box is empty (scene_min ==
+ * targets are clamped the same way. spp = 0 only trains (film may be NULL). A call that
+ * both trains (train_rounds > 0) and renders (spp > 0) runs its rounds beside the frame, on
+ * a second stream: the frame reads the weights the cache held when the call started, and
+ * the call's work ends with the weights its rounds trained. The integrator must be
+ * PBRT_INTEGRATOR_PATH. A cache whose scene box is empty (scene_min ==
  * scene_max) takes the scene's bounds on first use. */
 int pbrt_render_cached(pbrt_scene* scene, pbrt_cache* cache, const pbrt_render_params* params, uint32_t train_rounds,
                        double* film_rgb);

@@ -124,6 +124,12 @@ void pbrt_ctx_destroy(pbrt_ctx* c) {
     cudaFree(s.rec);
     if (s.s) cudaStreamDestroy(s.s);
   }
+  if (c->side) {
+    cudaStreamSynchronize(c->side);
+    cudaStreamDestroy(c->side);
+  }
+  if (c->fork) cudaEventDestroy(c->fork);
+  if (c->join) cudaEventDestroy(c->join);
   cudaFree(c->d_err);
   cudaFree(c->d_counters);
   cudaFree(c->queue);
@@ -786,6 +792,7 @@ uint64_t pbrt::api::film_pixels(const pbrt_render_params* p, const RenderSetting
 namespace {
 
 WaveAlloc g_waves[kMaxDevices];  // per device; a context serialises its own calls
+WaveAlloc g_train_waves[kMaxDevices];  // a cached render's training paths beside its frame
 
 // Training paths of the cached render go this many hits past the render's cache hit before
 // they end into the cache themselves.
@@ -878,6 +885,31 @@ int pbrt_render_cached(pbrt_scene* s, pbrt_cache* k, const pbrt_render_params* p
   const CacheWave& cw = k->cw;
   PBRT_TRY(c->cuda(cudaMemsetAsync(rs.stats, 0, 3 * sizeof(unsigned long long), st), "cudaMemset"));
 
+  // A call that trains and renders runs its rounds beside the frame: the rounds on the
+  // context's side stream with their own wave, the frame on `st` with its own query buffers,
+  // reading a snapshot of the weights the call started with. The rounds' few thousand paths
+  // leave most of the GPU idle; this way the frame's work fills it.
+  const bool beside = train_rounds > 0 && p->spp > 0;
+  cudaStream_t ts = st;            // the training rounds' stream
+  WaveAlloc* twa = &wa;            // and their wave
+  mlp::Net fnet{k->wfwd, k->wbwd};  // the weights the frame reads
+  const CacheWave* fcw = &cw;      // and its query buffers
+  if (beside) {
+    if (!c->side) PBRT_TRY(c->cuda(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking), "cudaStreamCreate"));
+    if (!c->fork) PBRT_TRY(c->cuda(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming), "cudaEventCreate"));
+    if (!c->join) PBRT_TRY(c->cuda(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming), "cudaEventCreate"));
+    twa = &g_train_waves[c->device];
+    PBRT_TRY(ensure_wave(c, twa, train_paths));
+    PBRT_TRY(k->ensure_frame_buffers(wave));
+    PBRT_TRY(c->cuda(cudaMemcpyAsync(k->wsnap, k->wfwd, mlp::kParams * 2, cudaMemcpyDeviceToDevice, st),
+                     "cudaMemcpy(weight snapshot)"));
+    PBRT_TRY(c->cuda(cudaEventRecord(c->fork, st), "cudaEventRecord"));
+    PBRT_TRY(c->cuda(cudaStreamWaitEvent(c->side, c->fork, 0), "cudaStreamWaitEvent"));
+    ts = c->side;
+    fnet.wpk_fwd = k->wsnap;
+    fcw = &k->fcw;
+  }
+
   // Online training. Training paths start at random pixels, go kTrainTail hits past the
   // render's cache hit and end into the cache there; their earlier Lambertian and metal
   // vertices become training samples. No host synchronisation: counts stay on the device.
@@ -885,28 +917,43 @@ int pbrt_render_cached(pbrt_scene* s, pbrt_cache* k, const pbrt_render_params* p
   const uint32_t tail_hit = term_hit + kTrainTail;
   const mlp::Net net{k->wfwd, k->wbwd};
   const mlp::Bounds nb = k->bounds();
-  for (uint32_t r = 0; r < train_rounds; ++r) {
-    RenderSettings tr = rs;
-    tr.cache_mode = kCacheRecord;
-    tr.term_hit = tail_hit;
-    tr.random_pixels = 1;
-    tr.sample_offset = 0;
-    tr.seed = host_mix64(p->seed ^ host_mix64(0x747261696e696e67ULL + k->rounds));
-    if (!s->has_dielectric) tr.loop_depth = std::min(rs.max_depth, tail_hit);
-    PBRT_TRY(c->cuda(cudaMemsetAsync(cw.counts, 0, 3 * sizeof(uint32_t), st), "cudaMemset(cache counts)"));
-    PBRT_TRY(c->cuda(trace_wave(s->view, wa.w, cw, cam, 0, train_paths, uint32_t(npix), tr, c->d_err, c->sm_count, st),
-                     "cache training paths"));
-    PBRT_TRY(c->cuda(mlp::launch_infer_dev(net, nb, cw.qrec, cw.counts, train_paths, cw.qout, c->d_err, c->sm_count,
-                                           st),
-                     "cache training tails"));
-    PBRT_TRY(c->cuda(apply_cache(wa.w, cw, train_paths, s->max_radiance, c->sm_count, st), "cache training tails"));
-    for (uint32_t step = 0; step < steps; ++step) {
-      PBRT_TRY(c->cuda(train_batch(wa.w, cw, batch, step, tr.seed, s->max_radiance, k->brec, k->btgt, c->sm_count, st),
-                       "cache training batch"));
-      PBRT_TRY(k->gradient_device(k->brec, k->btgt, batch, st));
-      PBRT_TRY(k->adam_device(st, cw.counts + 2));
-    }
-    ++k->rounds;
+  int trc = PBRT_OK;
+  {
+    auto train = [&]() -> int {
+      for (uint32_t r = 0; r < train_rounds; ++r) {
+        RenderSettings tr = rs;
+        tr.cache_mode = kCacheRecord;
+        tr.term_hit = tail_hit;
+        tr.random_pixels = 1;
+        tr.sample_offset = 0;
+        tr.seed = host_mix64(p->seed ^ host_mix64(0x747261696e696e67ULL + k->rounds));
+        if (!s->has_dielectric) tr.loop_depth = std::min(rs.max_depth, tail_hit);
+        PBRT_TRY(c->cuda(cudaMemsetAsync(cw.counts, 0, 3 * sizeof(uint32_t), ts), "cudaMemset(cache counts)"));
+        PBRT_TRY(c->cuda(trace_wave(s->view, twa->w, cw, cam, 0, train_paths, uint32_t(npix), tr, c->d_err, c->sm_count, ts),
+                         "cache training paths"));
+        PBRT_TRY(c->cuda(mlp::launch_infer_dev(net, nb, cw.qrec, cw.counts, train_paths, cw.qout, c->d_err, c->sm_count,
+                                               ts),
+                         "cache training tails"));
+        PBRT_TRY(c->cuda(apply_cache(twa->w, cw, train_paths, s->max_radiance, c->sm_count, ts), "cache training tails"));
+        for (uint32_t step = 0; step < steps; ++step) {
+          PBRT_TRY(c->cuda(train_batch(twa->w, cw, batch, step, tr.seed, s->max_radiance, k->brec, k->btgt, c->sm_count, ts),
+                           "cache training batch"));
+          PBRT_TRY(k->gradient_device(k->brec, k->btgt, batch, ts));
+          PBRT_TRY(k->adam_device(ts, cw.counts + 2));
+        }
+        ++k->rounds;
+      }
+      return PBRT_OK;
+    };
+    trc = train();
+  }
+  if (beside) {  // the call ends when its rounds have: `st` waits for them at the end
+    const int jr = c->cuda(cudaEventRecord(c->join, c->side), "cudaEventRecord");
+    if (trc == PBRT_OK) trc = jr;
+  }
+  if (trc != PBRT_OK) {
+    if (beside) cudaStreamWaitEvent(st, c->join, 0);
+    return trc;
   }
   if (p->spp == 0) {
     if (c->user) return PBRT_OK;
@@ -925,17 +972,21 @@ int pbrt_render_cached(pbrt_scene* s, pbrt_cache* k, const pbrt_render_params* p
   int rc = c->cuda(cudaMemsetAsync(dfilm, 0, film_n * sizeof(double), st), "cudaMemset(film)");
   for (uint64_t base = 0; base < total && rc == PBRT_OK; base += wave) {
     const uint32_t n = uint32_t(std::min<uint64_t>(wave, total - base));
-    rc = c->cuda(cudaMemsetAsync(cw.counts, 0, sizeof(uint32_t), st), "cudaMemset(cache counts)");
+    rc = c->cuda(cudaMemsetAsync(fcw->counts, 0, sizeof(uint32_t), st), "cudaMemset(cache counts)");
     if (rc == PBRT_OK)
-      rc = c->cuda(trace_wave(s->view, wa.w, cw, cam, base, n, uint32_t(npix), qr, c->d_err, c->sm_count, st),
+      rc = c->cuda(trace_wave(s->view, wa.w, *fcw, cam, base, n, uint32_t(npix), qr, c->d_err, c->sm_count, st),
                    "cached render");
     if (rc == PBRT_OK)
-      rc = c->cuda(mlp::launch_infer_dev(net, nb, cw.qrec, cw.counts, n, cw.qout, c->d_err, c->sm_count, st),
+      rc = c->cuda(mlp::launch_infer_dev(fnet, nb, fcw->qrec, fcw->counts, n, fcw->qout, c->d_err, c->sm_count, st),
                    "cache query");
-    if (rc == PBRT_OK) rc = c->cuda(apply_cache(wa.w, cw, n, s->max_radiance, c->sm_count, st), "cache apply");
+    if (rc == PBRT_OK) rc = c->cuda(apply_cache(wa.w, *fcw, n, s->max_radiance, c->sm_count, st), "cache apply");
     if (rc == PBRT_OK) rc = c->cuda(accumulate_wave(wa.w, n, dfilm, cd.width, qr, c->sm_count, st), "cached render");
   }
   if (rc == PBRT_OK) rc = c->cuda(scale_film(dfilm, film_n, 1.0 / double(p->spp), c->sm_count, st), "render");
+  if (beside) {
+    const int jr = c->cuda(cudaStreamWaitEvent(st, c->join, 0), "cudaStreamWaitEvent");
+    if (rc == PBRT_OK) rc = jr;
+  }
   if (host_film) {
     if (rc == PBRT_OK)
       rc = c->cuda(cudaMemcpyAsync(film, dfilm, film_n * sizeof(double), cudaMemcpyDeviceToHost, st), "cudaMemcpy(film)");

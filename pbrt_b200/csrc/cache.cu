@@ -151,9 +151,32 @@ int pbrt_cache::ensure_render_buffers(uint32_t queries, uint32_t train_vertices,
   return PBRT_OK;
 }
 
+int pbrt_cache::ensure_frame_buffers(uint32_t queries) {
+  if (frame_block && fqcap >= queries) return PBRT_OK;
+  cudaFree(frame_block);
+  frame_block = nullptr;
+  fqcap = 0;
+  fcw = pbrt::CacheWave{};
+  const size_t R = pbrt::kCacheRecordFloats * 4;
+  auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t bytes =
+      up(64) + up(size_t(queries) * R) + up(size_t(queries) * 12) + up(size_t(queries) * 4) + up(mlp::kParams * 2);
+  PBRT_TRY(ctx->cuda(cudaMalloc(&frame_block, bytes), "cudaMalloc(cache frame buffers)"));
+  char* p = static_cast<char*>(frame_block);
+  auto take = [&](size_t b) { char* r = p; p += up(b); return r; };
+  fcw.counts = reinterpret_cast<uint32_t*>(take(64));
+  fcw.qrec = reinterpret_cast<float*>(take(size_t(queries) * R));
+  fcw.qout = reinterpret_cast<float*>(take(size_t(queries) * 12));
+  fcw.qpath = reinterpret_cast<uint32_t*>(take(size_t(queries) * 4));
+  fcw.qcap = queries;  // no training vertices: the frame only queries
+  wsnap = reinterpret_cast<uint16_t*>(take(mlp::kParams * 2));
+  fqcap = queries;
+  return PBRT_OK;
+}
+
 void pbrt_cache::release() {
   for (void* p : {(void*)w, (void*)m, (void*)v, (void*)grad, (void*)wfwd, (void*)wbwd, (void*)loss, (void*)partials,
-                  (void*)tile_loss, render_block})
+                  (void*)tile_loss, render_block, frame_block})
     cudaFree(p);
 }
 

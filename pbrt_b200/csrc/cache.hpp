@@ -27,6 +27,14 @@ struct pbrt_cache {
   float *brec = nullptr, *btgt = nullptr;
   int ensure_render_buffers(uint32_t queries, uint32_t train_vertices, uint32_t batch);
 
+  // A call that trains and renders: the frame's own query buffers and the snapshot of the
+  // forward weights it reads, while the training rounds (with `cw`) update the weights.
+  void* frame_block = nullptr;
+  uint32_t fqcap = 0;
+  pbrt::CacheWave fcw{};
+  uint16_t* wsnap = nullptr;
+  int ensure_frame_buffers(uint32_t queries);
+
   int device_arrays();
   int ensure_tiles(uint32_t tiles);
   int reset();

@@ -122,3 +122,23 @@ def test_knot_scene_face_materials():
     ref = oracle.Scene(desc, np.float32).render(cam, 16, 8, seed=1)
     assert np.all(np.isfinite(img))
     assert relmse(img, ref) < 5e-3
+
+
+def test_training_beside_the_frame(cornell):
+    """A call that trains and renders runs its rounds beside the frame: the frame reads the
+    weights the call started with (so its film is that of a render-only call with those
+    weights), and the call leaves the weights its rounds trained. The rounds' training
+    vertices are recorded in whatever order the GPU schedules them, so their weights are not
+    compared bit for bit with a separate training call."""
+    desc, cam, scene = cornell
+    lo, hi = _box_bounds(desc)
+    kw = dict(terminate_bounce=TERM, train_samples=4096, train_steps=4, seed=7)
+    a, b = RadianceCache(lo, hi, **kw), RadianceCache(lo, hi, **kw)
+    for frame in range(3):
+        w0 = a.weights()
+        b.set_weights(w0)
+        got = scene.render_cached(a, cam, spp=4, max_depth=16, seed=20 + frame, train_rounds=1)
+        want = scene.render_cached(b, cam, spp=4, max_depth=16, seed=20 + frame, train_rounds=0)
+        np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-15)
+        w1 = a.weights()
+        assert np.isfinite(w1).all() and not np.array_equal(w1, w0)
