@@ -625,13 +625,27 @@ __global__ void __launch_bounds__(64) k_small(const SmallJob* __restrict__ jobs,
 }
 
 // ---- depth-first renumbering and the GPU layout -----------------------------------------------
+// Nodes grouped by depth. Every node adds to one of a few dozen counters, so the lanes of a
+// warp that share a depth (neighbouring nodes usually do) add once, together; the order
+// within a depth does not matter to the sizes and numbers computed from it.
 __global__ void k_depth_hist(const PoolNode* __restrict__ pool, uint32_t n, uint32_t* hist) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    atomicAdd(hist + min(pool[i].depth, 255u), 1u);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t dep = min(pool[i].depth, 255u);
+    const unsigned peers = __match_any_sync(__activemask(), dep);
+    if ((threadIdx.x & 31u) == unsigned(__ffs(peers) - 1)) atomicAdd(hist + dep, uint32_t(__popc(peers)));
+  }
 }
 __global__ void k_depth_scatter(const PoolNode* __restrict__ pool, uint32_t n, uint32_t* cursor, uint32_t* by_depth) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    by_depth[atomicAdd(cursor + min(pool[i].depth, 255u), 1u)] = i;
+  const unsigned lane = threadIdx.x & 31u;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t dep = min(pool[i].depth, 255u);
+    const unsigned peers = __match_any_sync(__activemask(), dep);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (int(lane) == leader) base = atomicAdd(cursor + dep, uint32_t(__popc(peers)));
+    base = __shfl_sync(peers, base, leader);
+    by_depth[base + __popc(peers & ((1u << lane) - 1u))] = i;
+  }
 }
 // subtree sizes, deepest level first
 __global__ void k_sizes(const PoolNode* __restrict__ pool, const uint32_t* __restrict__ ids, uint32_t n,
