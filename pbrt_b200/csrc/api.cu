@@ -130,6 +130,8 @@ void pbrt_ctx_destroy(pbrt_ctx* c) {
   }
   if (c->fork) cudaEventDestroy(c->fork);
   if (c->join) cudaEventDestroy(c->join);
+  cudaFree(c->waves.block);
+  cudaFree(c->train_waves.block);
   cudaFree(c->d_err);
   cudaFree(c->d_counters);
   cudaFree(c->queue);
@@ -791,9 +793,6 @@ uint64_t pbrt::api::film_pixels(const pbrt_render_params* p, const RenderSetting
 
 namespace {
 
-WaveAlloc g_waves[kMaxDevices];  // per device; a context serialises its own calls
-WaveAlloc g_train_waves[kMaxDevices];  // a cached render's training paths beside its frame
-
 // Training paths of the cached render go this many hits past the render's cache hit before
 // they end into the cache themselves.
 constexpr uint32_t kTrainTail = 3;
@@ -821,7 +820,7 @@ int pbrt_render(pbrt_scene* s, const pbrt_render_params* p, double* film) {
   const uint64_t npix = film_pixels(p, rs);
   const uint64_t total = npix * p->spp;
 
-  WaveAlloc& wa = g_waves[c->device];
+  WaveAlloc& wa = c->waves;
   const uint32_t wave = uint32_t(std::min<uint64_t>(total, c->wave_paths));
   PBRT_TRY(ensure_wave(c, &wa, wave));
   cudaStream_t st = c->work_stream();
@@ -877,7 +876,7 @@ int pbrt_render_cached(pbrt_scene* s, pbrt_cache* k, const pbrt_render_params* p
   const uint32_t batch = std::max(128u, cp.train_samples / steps);
   const uint32_t wave = uint32_t(std::min<uint64_t>(total, c->wave_paths));
 
-  WaveAlloc& wa = g_waves[c->device];
+  WaveAlloc& wa = c->waves;
   PBRT_TRY(ensure_wave(c, &wa, std::max(wave, train_paths)));
   // one query per path at most: the render wave's and the training paths'
   PBRT_TRY(k->ensure_render_buffers(std::max(wave, train_paths), cp.train_samples, batch));
@@ -898,7 +897,7 @@ int pbrt_render_cached(pbrt_scene* s, pbrt_cache* k, const pbrt_render_params* p
     if (!c->side) PBRT_TRY(c->cuda(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking), "cudaStreamCreate"));
     if (!c->fork) PBRT_TRY(c->cuda(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming), "cudaEventCreate"));
     if (!c->join) PBRT_TRY(c->cuda(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming), "cudaEventCreate"));
-    twa = &g_train_waves[c->device];
+    twa = &c->train_waves;
     PBRT_TRY(ensure_wave(c, twa, train_paths));
     PBRT_TRY(k->ensure_frame_buffers(wave));
     PBRT_TRY(c->cuda(cudaMemcpyAsync(k->wsnap, k->wfwd, mlp::kParams * 2, cudaMemcpyDeviceToDevice, st),

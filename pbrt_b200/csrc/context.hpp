@@ -58,7 +58,7 @@ struct Slot {
   unsigned long long* fetch = nullptr;  // [queue length, fetch position] of that pass
 };
 
-// The wave's SoA state, grown on demand (one per device for pbrt_render / pbrt_render_cached,
+// The wave's SoA state, grown on demand (one per context for pbrt_render / pbrt_render_cached,
 // one per batch).
 struct WaveAlloc {
   void* block = nullptr;
@@ -89,6 +89,9 @@ struct pbrt_ctx {
   // a cached render's training rounds beside its frame: their stream, the fork and join
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  // the path state of pbrt_render / pbrt_render_cached (grown on demand), and of a cached
+  // render's training paths; per context, so contexts on one device may render at once
+  pbrt::api::WaveAlloc waves, train_waves;
 
   int fail(int code, const std::string& msg) {
     err = msg;
