@@ -161,3 +161,26 @@ def test_render_stats_count_the_work():
     # every path traces its camera ray, at most max_depth rays in all, one shadow ray per hit
     assert st["paths"] <= st["rays"] <= 5 * st["paths"]
     assert 0 < st["shadow_rays"] <= 4 * st["paths"]
+
+
+def test_two_contexts_render_at_once():
+    """Each context owns its path state: two contexts on one GPU, driven from two host
+    threads at the same time, render what either renders alone."""
+    import threading
+
+    desc, cam = W.cornell_box(32, 24)
+    scenes = [pb.Scene.from_description(desc, pb.Context(0)).commit() for _ in range(2)]
+    want = scenes[0].render(cam, spp=4, max_depth=6, seed=3)
+    for _ in range(3):
+        out = [None, None]
+
+        def run(k):
+            out[k] = scenes[k].render(cam, spp=4, max_depth=6, seed=3)
+
+        threads = [threading.Thread(target=run, args=(k,)) for k in range(2)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        for o in out:
+            np.testing.assert_allclose(o, want, rtol=1e-12, atol=1e-15)
