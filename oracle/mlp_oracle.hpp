@@ -1,7 +1,7 @@
 // mlp_oracle.hpp — TEST INFRASTRUCTURE, NOT THE PRODUCT.
 //
 // CPU restatement of the radiance cache's network (the reference has no learned component;
-// this is the checker the north star asks for: "gradients checked against the CPU oracle").
+// this is the checker the GPU's forward pass, gradients and Adam steps are compared with).
 // Two modes:
 //   emulate = true : the GPU's arithmetic — BF16 inputs, weights, activations and layer
 //                    gradients (round to nearest even), FP32 results of each dot product;
