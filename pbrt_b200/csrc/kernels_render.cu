@@ -422,12 +422,12 @@ __global__ void __launch_bounds__(256, 4) k_extend(WaveBuffers w, Src src, const
 // queued one (one atomicAdd on `fetch` per warp). Hit t / object / primitive are those of
 // scene_closest: the same boxes, the same order, the same adoptions. It pays where the
 // top-level tree is deep (10,000 spheres: 259 -> 177 ms a frame) and costs where a path's
-// query is a few nodes (a 4-object box: 2.7 -> 3.1 ms), hence kWalkMinTopNodes. Built
-// without the solids' code it keeps its whole walk state in registers at 2 resident blocks
-// per SM (91 registers, no spills): 10,000 spheres 170 -> 148 ms a frame against 4 blocks
-// (64 registers, 318 bytes spilled).
+// query is a few nodes (a 4-object box: 2.7 -> 3.1 ms), hence kWalkMinTopNodes. At 2
+// resident blocks per SM it keeps its whole walk state in registers (91 without the solids'
+// code, 108 with it; no spills): 10,000 spheres 170 -> 148 ms a frame against 4 blocks (64
+// registers, 318 bytes spilled); 48 solids 2.45 -> 2.31 ms.
 template <class Src, bool kCsg>
-__global__ void __launch_bounds__(256, kCsg ? 4 : 2) k_extend_walk(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
+__global__ void __launch_bounds__(256, 2) k_extend_walk(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
                                                      const uint32_t* __restrict__ qcount, uint32_t* __restrict__ fetch,
                                                 uint32_t* err, unsigned long long* stats) {
   const uint32_t n = *qcount;
@@ -774,10 +774,10 @@ __global__ void __launch_bounds__(256) k_train_batch(WaveBuffers w, CacheWave cw
   }
 }
 
-// Built without the solids' code: 3 resident blocks per SM (the torus-knot frame 54.1 ->
-// 52.9 ms against 4; 2 gained nothing more).
+// 3 resident blocks per SM (the torus-knot frame 54.1 -> 52.9 ms against 4; 2 gained nothing
+// more; with the solids' code, 48 of 770 bytes still spill).
 template <class Src, bool kCsg>
-__global__ void __launch_bounds__(256, kCsg ? 4 : 3) k_shadow(WaveBuffers w, Src src, uint32_t* err, unsigned long long* stats) {
+__global__ void __launch_bounds__(256, 3) k_shadow(WaveBuffers w, Src src, uint32_t* err, unsigned long long* stats) {
   const uint32_t n = w.counts[2];
   if (stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(stats + 1, (unsigned long long)n);
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
