@@ -524,6 +524,26 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def headline_parity(scene, m, rays_h, rays_d, prim_d, t_d, oprim, ot, threads):
+    """The GPU's answers for the timed rays against the FP32 oracle's (untimed): nearest
+    triangle ids bit-exact, t bit-exact on hits and +inf on misses, and the any-hit answer of
+    every ray (pbrt_trace_any against the oracle's BVHTree::intersect_p restatement)."""
+    import torch
+
+    gp = prim_d.cpu().numpy().view(np.uint32)
+    gt = t_d.cpu().numpy()
+    hit = oprim != 0xFFFFFFFF
+    occ_d = scene.intersect_p(rays_d)
+    torch.cuda.synchronize()
+    occ_g = occ_d.cpu().numpy().astype(bool)
+    occ_o = m.occluded(rays_h, threads=threads).astype(bool)
+    return {"ids_equal": bool(np.array_equal(gp, oprim)),
+            "t_equal_on_hits": bool(np.array_equal(gt[hit], ot[hit]) and np.all(np.isinf(gt[~hit]))),
+            "occluded_equal": bool(np.array_equal(occ_g, occ_o)), "rays": int(oprim.size), "hits": int(hit.sum()),
+            "ids_differing": int((gp != oprim).sum()), "occluded_rays": int(occ_o.sum()),
+            "oracle": "FP32 C++ restatement of BVHTree::traverse / intersect_p (same tree, same operation order)"}
+
+
 def _copy_floor_ms(rays_pin, rays_d, prim_pin, t_pin, prim_d, t_d, reps=5):
     """Wall time of the host path's bare copies: the rays host->device on one stream while the
     ids and t come back device->host on another (PCIe moves both directions at once)."""
@@ -720,12 +740,15 @@ def main():
             m = oracle.MeshBVH(v, f, np.float32, bins=BINS, max_leaf=MAX_LEAF)
             sample = N_RAYS
             t0 = time.perf_counter()
-            m.trace(rays_h[:, :sample], threads=threads)
+            oprim, ot, _ = m.trace(rays_h[:, :sample], threads=threads)
             cs = time.perf_counter() - t0
             line["cpu_baseline"] = {"value": round(sample / cs / 1e6, 3), "unit": UNIT, "cores": threads, "kind": "port",
                                     "sample": f"the full {sample}-ray step once, C++ restatement of the reference "
                                               "traversal (oracle), all host threads"}
+            line["parity"] = headline_parity(scene, m, rays_h, rays_d, prim_d, t_d, oprim, ot, threads)
         print(json.dumps(line), flush=True)
+        if "parity" in line and not all(line["parity"][k] for k in ("ids_equal", "t_equal_on_hits", "occluded_equal")):
+            raise SystemExit(f"parity failed on the headline rays: {line['parity']}")
     if dist:
         dist.barrier()
         dist.destroy_process_group()

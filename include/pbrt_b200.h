@@ -5,8 +5,8 @@
  * traversal (Möller–Trumbore triangles, analytic spheres and cylinders) and the path
  * integrator's bounce loop with BSDF sampling/evaluation and light sampling. The reference
  * is a Rust crate whose seams are traits; a Rust binding would declare exactly these
- * functions in an `extern "C"` block. Each entry point names the
- * reference interface it replaces, as `path:line` inside nmichel/pbrt.
+ * functions in an `extern "C"` block. Each entry point names the reference interface it
+ * replaces, as `path:line` inside nmichel/pbrt.
  *
  * Conventions
  *   - Every function returns a pbrt_status; 0 is success. pbrt_last_error() gives a
@@ -289,12 +289,16 @@ int pbrt_trace_closest_instrumented(pbrt_scene* scene, const float* rays, uint64
  * every GPU which loads the library holds until the process exits.
  *   - rays, prim_id and t must be device memory of the context's GPU; n must not exceed
  *     PBRT_NOALLOC_MAX_RAYS (PBRT_ERR_CAPACITY otherwise; split larger batches).
- *   - The first call on a device looks the array's address up there; make that first call
- *     before any stream capture.
+ *   - pbrt_ctx_create looks the array's address up on its device; that also loads the
+ *     trace kernels there, so the array's memory is committed when the context is created
+ *     (a context that cannot get it fails to create) and never inside this call.
  *   - Every call shares the one array: calls that overlap on the GPU (other streams, other
  *     threads, other contexts on the same device) race and corrupt each other's results.
  *   - It runs on the context's stream (pbrt_ctx_set_stream) and returns when its results
- *     are complete, with device-side errors reported in its status.
+ *     are complete, with device-side errors reported in its status. Because it waits for
+ *     them, it refuses a stream that is being captured (PBRT_ERR_UNSUPPORTED, nothing
+ *     enqueued) instead of invalidating the capture.
+ *   - n = 0 returns PBRT_OK whatever the scene, as pbrt_trace_closest does.
  * Results are identical to pbrt_trace_closest's. */
 #define PBRT_NOALLOC_MAX_RAYS 1048576u
 int pbrt_trace_closest_noalloc(pbrt_scene* scene, const float* rays, uint64_t n, uint32_t* prim_id, float* t);

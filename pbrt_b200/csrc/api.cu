@@ -103,6 +103,10 @@ int pbrt_ctx_create(int device, pbrt_ctx** out) {
   if (c->cuda(cudaMemsetAsync(c->d_counters, 0, 16 * sizeof(unsigned long long), c->stream), "cudaMemset") !=
       PBRT_OK)
     return PBRT_ERR_CUDA;
+  // The allocation-free trace's scratch array: its address on this device (which loads the
+  // trace kernels' module now, under lazy loading, so its 4 MiB are committed here and not
+  // inside a later call).
+  if (c->cuda(noalloc_scratch_lookup(&c->noalloc_scratch), "cudaGetSymbolAddress") != PBRT_OK) return PBRT_ERR_CUDA;
   if (c->cuda(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize") != PBRT_OK) return PBRT_ERR_CUDA;
   *out = c.release();
   return PBRT_OK;
@@ -674,32 +678,38 @@ int pbrt_trace_closest_instrumented(pbrt_scene* s, const float* rays, uint64_t n
 static_assert(kNoAllocMaxRays == PBRT_NOALLOC_MAX_RAYS, "header and kernels disagree on the no-alloc capacity");
 
 // For callers that cannot call cudaMalloc (see the header): the same two kernels as the
-// device-buffer path of pbrt_trace_closest, with their scratch in a static __device__ array.
+// device-buffer path of pbrt_trace_closest, with their scratch in a static __device__ array
+// whose address the context looked up when it was created.
 int pbrt_trace_closest_noalloc(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim_id, float* t) {
   if (!s) return PBRT_ERR_INVALID_ARGUMENT;
   pbrt_ctx* c = s->ctx;
+  if (n == 0) return PBRT_OK;  // as pbrt_trace_closest: nothing to do, whatever the scene
   DeviceGuard g(c->device);
   if (n > kNoAllocMaxRays)
     return c->fail(PBRT_ERR_CAPACITY, "pbrt_trace_closest_noalloc: n = " + std::to_string(n) +
                                           " exceeds its fixed scratch capacity of " + std::to_string(kNoAllocMaxRays) +
                                           " rays; split the batch or use pbrt_trace_closest");
-  if (n > 0) {
-    if (!rays || !prim_id || !t) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "ray or result buffer is NULL");
-    if (mem_kind(rays) != MemKind::Device || mem_kind(prim_id) != MemKind::Device || mem_kind(t) != MemKind::Device)
-      return c->fail(PBRT_ERR_INVALID_ARGUMENT,
-                     "pbrt_trace_closest_noalloc takes device buffers only (host buffers need staging memory)");
-  }
+  cudaStream_t st = c->work_stream();
+  // The call waits for its results (it reads the error word back), which a stream under
+  // capture cannot do: refuse before any other CUDA call, so the caller's capture survives.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  PBRT_TRY(c->cuda(cudaStreamIsCapturing(st, &cap), "cudaStreamIsCapturing"));
+  if (cap != cudaStreamCaptureStatusNone)
+    return c->fail(PBRT_ERR_UNSUPPORTED,
+                   "pbrt_trace_closest_noalloc waits for its results and cannot run on a stream being captured");
+  if (!rays || !prim_id || !t) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "ray or result buffer is NULL");
+  if (mem_kind(rays) != MemKind::Device || mem_kind(prim_id) != MemKind::Device || mem_kind(t) != MemKind::Device)
+    return c->fail(PBRT_ERR_INVALID_ARGUMENT,
+                   "pbrt_trace_closest_noalloc takes device buffers only (host buffers need staging memory)");
   if (s->single_mesh < 0)
     return c->fail(PBRT_ERR_UNSUPPORTED, "pbrt_trace_closest_noalloc traces scenes made of one untransformed mesh");
   const MeshView& mv = s->meshes[s->single_mesh].view;
-  cudaStream_t st = c->work_stream();
-  uint32_t* scratch = nullptr;
-  PBRT_TRY(c->cuda(launch_mesh_closest_noalloc(mv, rays, n, prim_id, t, c->device, c->sm_count, st, &scratch),
+  uint32_t* scratch = c->noalloc_scratch;
+  PBRT_TRY(c->cuda(launch_mesh_closest_noalloc(mv, rays, n, prim_id, t, scratch, c->sm_count, st),
                    "pbrt_trace_closest_noalloc"));
-  if (n == 0) return PBRT_OK;
+  uint32_t h = 0;  // the error word, read back on the same stream (no legacy-stream wait)
+  PBRT_TRY(c->cuda(cudaMemcpyAsync(&h, scratch + 4, sizeof(h), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync"));
   PBRT_TRY(c->cuda(cudaStreamSynchronize(st), "kernel execution"));
-  uint32_t h = 0;
-  PBRT_TRY(c->cuda(cudaMemcpy(&h, scratch + 4, sizeof(h), cudaMemcpyDeviceToHost), "cudaMemcpy(error word)"));
   if (h & kErrStack) return c->fail(PBRT_ERR_CAPACITY, "traversal stack capacity exceeded");
   if (h) return c->fail(PBRT_ERR_DEVICE_BUDGET, "a traversal exceeded its iteration budget (malformed tree)");
   return PBRT_OK;

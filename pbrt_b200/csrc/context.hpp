@@ -81,6 +81,8 @@ struct pbrt_ctx {
   uint32_t* queue = nullptr;                  // survivor queue for device-buffer calls (kDevChunk entries)
   float4* queue_rec = nullptr;                // and their ray records (kDevChunk x 32 bytes)
   bool persistent = true;                     // persistent dynamic-fetch traversal (default)
+  uint32_t* noalloc_scratch = nullptr;        // device address of pbrt_trace_closest_noalloc's static
+                                              // scratch array on this device, looked up at creation
   pbrt::api::Slot slots[pbrt::api::kSlots];
   bool slots_ready = false;
   std::vector<void*> allocs;

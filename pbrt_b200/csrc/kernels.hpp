@@ -24,13 +24,15 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
                                            float4* rec = nullptr);
 // Allocation-free form of launch_mesh_closest_persistent for device buffers (plane stride
 // = n): its scratch is a file-scope __device__ array of kNoAllocMaxRays queue entries
-// shared by every call on a device. Looks the array's address up on `device` (which must be
-// current) on its first use there and returns it in *scratch (word 4 is the error word).
-// cudaErrorInvalidValue when n > kNoAllocMaxRays. Calls that overlap on the GPU race.
+// shared by every call on a device. `scratch` is that array's device address on the current
+// device, from noalloc_scratch_lookup (word 4 is the error word). cudaErrorInvalidValue when
+// n > kNoAllocMaxRays. Calls that overlap on the GPU race.
 constexpr uint64_t kNoAllocMaxRays = uint64_t(1) << 20;
-constexpr int kMaxDevices = 64;
 cudaError_t launch_mesh_closest_noalloc(const MeshView& m, const float* rays, uint64_t n, uint32_t* prim, float* t,
-                                        int device, int sm_count, cudaStream_t s, uint32_t** scratch);
+                                        uint32_t* scratch, int sm_count, cudaStream_t s);
+// Device address of the allocation-free pass's scratch array on the current device. The
+// lookup loads this file's module there (under lazy loading), which commits the array.
+cudaError_t noalloc_scratch_lookup(uint32_t** scratch);
 cudaError_t launch_mesh_any(const MeshView& m, const float* rays, uint64_t stride, uint64_t n, uint8_t* occ,
                             uint32_t* err, int sm_count, cudaStream_t s);
 

@@ -17,7 +17,6 @@
 // k_mesh_closest (one thread per ray) is the instrumented form that counts the work.
 #include <cfloat>
 #include <cstdint>
-#include <mutex>
 
 #include "kernels.hpp"
 #include "trace_mesh.cuh"
@@ -403,38 +402,24 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
 // ---------------------------------------------------------------------------------------
 static __device__ __align__(256) uint32_t g_noalloc_scratch[64 + kNoAllocMaxRays];
 
-// Device address of g_noalloc_scratch on `device`, looked up once per device with that
-// device current (host code cannot use the symbol itself as a device address).
-static cudaError_t noalloc_scratch_address(int device, uint32_t** out) {
-  static std::mutex mu;
-  static uint32_t* addr[kMaxDevices] = {};
-  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(mu);
-  if (!addr[device]) {
-    int cur = -1;
-    cudaError_t e = cudaGetDevice(&cur);
-    if (e != cudaSuccess) return e;
-    if (cur != device) return cudaErrorInvalidDevice;  // the caller makes `device` current
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    addr[device] = static_cast<uint32_t*>(p);
-  }
-  *out = addr[device];
+// Device address of g_noalloc_scratch on the current device (host code cannot use the
+// symbol itself as a device address). The context looks it up when it is created, with its
+// device current, and keeps it: a context made after a device reset gets the new address.
+cudaError_t noalloc_scratch_lookup(uint32_t** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  *out = static_cast<uint32_t*>(p);
   return cudaSuccess;
 }
 
 cudaError_t launch_mesh_closest_noalloc(const MeshView& m, const float* rays, uint64_t n, uint32_t* prim, float* t,
-                                        int device, int sm_count, cudaStream_t s, uint32_t** scratch_out) {
-  uint32_t* scratch = nullptr;
-  cudaError_t e = noalloc_scratch_address(device, &scratch);
-  if (e != cudaSuccess) return e;
-  *scratch_out = scratch;
+                                        uint32_t* scratch, int sm_count, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  if (n > kNoAllocMaxRays) return cudaErrorInvalidValue;
+  if (n > kNoAllocMaxRays || !scratch) return cudaErrorInvalidValue;
   // The array keeps the previous call's contents: the counters and the error word must
   // start at zero; the queue is written before it is read.
-  e = cudaMemsetAsync(scratch, 0, 64 * sizeof(uint32_t), s);
+  cudaError_t e = cudaMemsetAsync(scratch, 0, 64 * sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
   unsigned long long* counters = reinterpret_cast<unsigned long long*>(scratch);
   uint32_t* err = scratch + 4;

@@ -4,11 +4,14 @@ Run from the repository root, in a container where the reference is mounted:
 
     python tests/golden/make_golden.py /path/to/nmichel-pbrt
 
+(or with the checkout's location in PBRT_REFERENCE_ROOT and no argument).
+
 Writes:
-  meshes.npz — the two smallest PLY meshes of the reference's test_files/ (cube.ply,
-      bun_zipper_res4.ply) parsed with the reference's PLY semantics (f32 text widened to
-      f64, src/loader/ply/ply_loader.rs:137 and :40), so GPU tests can use real reference
-      geometry on a machine without the reference.
+  meshes.npz — the three smallest PLY meshes of the reference's test_files/ (cube.ply,
+      bun_zipper_res4.ply, dragon_vrip_res4.ply) parsed with the reference's PLY semantics
+      (f32 text widened to f64, src/loader/ply/ply_loader.rs:137 and :40), so the oracle's
+      known-answer tests and the GPU tests use real reference geometry on a machine without
+      the reference.
   bvh_stats_published.json — the mesh-mode figures the reference publishes for its own
       traversal benchmark (docs/mesures_bvh.md:706-713, produced by
       src/bin/bvh_stats.rs:345-401): hit counts (exact), box and triangle tests per ray
@@ -62,7 +65,7 @@ STAGES = ("cornell_box_canonical.stage", "bunny_mesh.stage", "many_spheres.stage
 
 def main(ref_root: str):
     out = {}
-    for name in ("cube.ply", "bun_zipper_res4.ply"):
+    for name in ("cube.ply", "bun_zipper_res4.ply", "dragon_vrip_res4.ply"):
         v, i = oracle.read_ply(os.path.join(ref_root, "test_files", name))
         key = name.replace(".ply", "")
         out[key + "_vertices"] = v
@@ -84,4 +87,7 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PBRT_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py <reference checkout> (or set PBRT_REFERENCE_ROOT)")
+    main(root)

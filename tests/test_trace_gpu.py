@@ -79,6 +79,29 @@ def test_displaced_icosphere_incoherent(bins, max_leaf):
     assert hit.sum() > 100_000
 
 
+def test_headline_mesh_level7_incoherent():
+    """The ray-cast workload's own mesh and tree (icosphere level 7, 327,680 triangles, 16
+    bins, leaves of at most 4) with 4M incoherent rays of its distribution plus 1M rays aimed
+    into the mesh: ids, t, occlusion and work counters identical to the FP32 oracle's."""
+    v, f = W.displaced_icosphere(7, seed=1)
+    assert f.shape[0] == 327_680
+    rays = W.incoherent_rays(1 << 22, v.min(0), v.max(0), seed=71)
+    rng = np.random.default_rng(72)
+    aim = rays[:, : 1 << 20].copy()
+    tgt = (rng.random((3, aim.shape[1])) - 0.5).astype(np.float32)
+    aim[3:6] = W.normalize_f32(tgt - aim[0:3])
+    rays = np.concatenate([rays, aim], axis=1)
+    m = oracle.MeshBVH(v, f, np.float32, bins=16, max_leaf=4)
+    s = _scene(v, f, 16, 4)
+    hit = _assert_parity(s, m, rays)
+    assert hit.sum() > 1_000_000
+    # the timed path (persistent traversal over device buffers) gives the same answers
+    dp, dt = s.intersect(torch.from_numpy(rays).cuda())
+    oprim, ot, _ = m.trace(rays)
+    assert np.array_equal(dp.cpu().numpy().view(np.uint32), oprim)
+    assert np.array_equal(dt.cpu().numpy()[hit], ot[hit])
+
+
 def test_host_and_device_buffers_agree_across_chunks():
     v, f = W.displaced_icosphere(5, seed=21)
     n = (1 << 21) * 2 + 12345  # five 1M-ray pipelined chunks over three staging slots, the last one partial

@@ -59,7 +59,7 @@ def test_noalloc_matches_trace_closest_on_consecutive_calls():
         ctx.check(lib.pbrt_trace_closest_noalloc(scene.h, r.data_ptr(), r.shape[1], p.data_ptr(), t.data_ptr()),
                   "pbrt_trace_closest_noalloc")
 
-    noalloc(order[0], outs[0])  # first call on this device: looks the scratch array up
+    noalloc(order[0], outs[0])  # first call: its kernels may load now (lazy module loading)
     free_before = _free_bytes()
     noalloc(order[1], outs[1])  # two more calls in a row reuse the array as the last one left it
     noalloc(order[2], outs[2])
@@ -90,3 +90,38 @@ def test_noalloc_rejects_oversized_and_host_batches():
     rc = lib.pbrt_trace_closest_noalloc(scene.h, hr.ctypes.data, 16, hp.ctypes.data, ht.ctypes.data)
     assert rc == 1  # PBRT_ERR_INVALID_ARGUMENT: device buffers only
     assert lib.pbrt_trace_closest_noalloc(scene.h, None, 0, None, None) == 0
+
+
+def test_noalloc_refuses_a_capturing_stream_and_accepts_empty_batches():
+    """The entry point waits for its results, so on a stream under capture it must refuse
+    before enqueuing anything and leave the caller's capture intact; n = 0 is a no-op on any
+    scene, as for pbrt_trace_closest."""
+    v, f = W.displaced_icosphere(3, seed=45)
+    ctx = pb.Context(0)
+    scene = pb.Scene(ctx).add_object(pb.Simple(pb.TriangleMesh(v, f))).commit()
+    lib = ctx.lib
+    n = 1024
+    rays = torch.from_numpy(W.incoherent_rays(n, v.min(0), v.max(0), seed=46)).cuda()
+    p = torch.empty(n, dtype=torch.int32, device="cuda")
+    t = torch.empty(n, dtype=torch.float32, device="cuda")
+    x = torch.zeros(4, device="cuda")
+    s = torch.cuda.Stream()
+    ctx.set_stream(s.cuda_stream)
+    g = torch.cuda.CUDAGraph()
+    rcs = []
+    with torch.cuda.graph(g, stream=s):
+        x.add_(1.0)
+        rcs.append(lib.pbrt_trace_closest_noalloc(scene.h, rays.data_ptr(), n, p.data_ptr(), t.data_ptr()))
+    assert rcs == [6]  # PBRT_ERR_UNSUPPORTED
+    assert b"stream being captured" in lib.pbrt_last_error(ctx.h)
+    g.replay()  # the capture survived the refusal
+    torch.cuda.synchronize()
+    assert torch.equal(x.cpu(), torch.ones(4))
+    del g
+    # outside a capture the same call on the same stream works
+    ctx.check(lib.pbrt_trace_closest_noalloc(scene.h, rays.data_ptr(), n, p.data_ptr(), t.data_ptr()), "noalloc")
+    ctx.set_stream(None)
+    # n = 0 returns PBRT_OK even on a scene the entry point does not trace (two meshes)
+    two = pb.Scene(ctx).add_object(pb.Simple(pb.TriangleMesh(v, f))).add_object(
+        pb.Simple(pb.TriangleMesh(v + 3.0, f))).commit()
+    assert lib.pbrt_trace_closest_noalloc(two.h, None, 0, None, None) == 0
