@@ -10,6 +10,8 @@
 // the end of a wave, accumulate adds every path's FP32 radiance into the FP64 film.
 #include <cfloat>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "kernels.hpp"
@@ -416,24 +418,23 @@ __global__ void __launch_bounds__(256, 4) k_extend(WaveBuffers w, Src src, const
 }
 
 // Scene::find_nearest for the queued paths (scene_closest_t, visit for visit), restated as a
-// persistent while-while walk: each lane walks the top-level BVH until it stands on a leaf it
-// must visit, then the lanes on leaves test their primitives together, so one lane's leaf
-// does not stall the others at every step; a lane whose path is finished takes the next
-// queued one (one atomicAdd on `fetch` per warp). Hit t / object / primitive are those of
-// scene_closest: the same boxes, the same order, the same adoptions. It pays where the
-// top-level tree is deep (10,000 spheres: 259 -> 177 ms a frame) and costs where a path's
-// query is a few nodes (a 4-object box: 2.7 -> 3.1 ms), hence kWalkMinTopNodes. At 2
-// resident blocks per SM it keeps its whole walk state in registers (91 without the solids'
-// code, 108 with it; no spills): 10,000 spheres 170 -> 148 ms a frame against 4 blocks (64
-// registers, 318 bytes spilled); 48 solids 2.45 -> 2.31 ms.
+// persistent walk of the top-level BVH with one warp-voted step per iteration: a node step
+// (or a pop) for the lanes not standing on a leaf, or, once at least `leaf_min` lanes stand on
+// a leaf they must visit (or no lane has anything else to do), a leaf step for those; idle
+// lanes take the next queued paths (one atomicAdd on `fetch` per warp) once at least
+// `refill_min` of them are idle. Hit t / object / primitive are those of scene_closest: the
+// same boxes, the same order, the same adoptions. It pays where the top-level tree is deep
+// (10,000 spheres) and costs where a path's query is a few nodes (a 4-object box), hence
+// kWalkMinTopNodes. At 2 resident blocks per SM it keeps its walk state in registers.
 template <class Src, bool kCsg>
 __global__ void __launch_bounds__(256, 2) k_extend_walk(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
                                                      const uint32_t* __restrict__ qcount, uint32_t* __restrict__ fetch,
-                                                uint32_t* err, unsigned long long* stats) {
+                                                     uint32_t* err, unsigned long long* stats, int leaf_min,
+                                                     int refill_min) {
   const uint32_t n = *qcount;
   if (stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(stats, (unsigned long long)n);
   const unsigned lane = threadIdx.x & 31u, lt_mask = (1u << lane) - 1u;
-  bool active = false;
+  bool active = false, exhausted = false;  // exhausted is warp-uniform
   uint32_t p = 0;
   F3 o = mk3(0.f, 0.f, 0.f), d = o;
   PRay r;
@@ -445,8 +446,7 @@ __global__ void __launch_bounds__(256, 2) k_extend_walk(WaveBuffers w, Src src, 
   float stk_e[kTraceStack];
   for (;;) {
     const unsigned idle = __ballot_sync(0xffffffffu, !active);
-    bool exhausted = false;
-    if (idle) {
+    if (!exhausted && idle && (__popc(idle) >= refill_min || idle == 0xffffffffu)) {
       const int leader = __ffs(idle) - 1;
       uint32_t base = 0;
       if (int(lane) == leader) base = atomicAdd(fetch, uint32_t(__popc(idle)));
@@ -498,60 +498,22 @@ __global__ void __launch_bounds__(256, 2) k_extend_walk(WaveBuffers w, Src src, 
         }
       }
     }
-    if (__ballot_sync(0xffffffffu, active) == 0) {
+    const unsigned act = __ballot_sync(0xffffffffu, active);
+    if (act == 0) {
       if (exhausted) break;
-      continue;
+      continue;  // all idle and the queue not yet drained: the next iteration refills
     }
-    if (active) {
+    const bool at_leaf = active && cur_e < min_t && count > 0;  // a leaf this lane must visit
+    const unsigned on_leaf = __ballot_sync(0xffffffffu, at_leaf);
+    const bool leaf_step = __popc(on_leaf) >= leaf_min || on_leaf == act;
+    bool done = false;
+    if (active && at_leaf == leaf_step) {
       const SceneView& s = src.view(w, p);
-      bool done = false;
-      // Walk until standing on a leaf to visit (cur_e < min_t), or until the stack is empty.
-      for (;;) {
-        if (budget-- == 0) {
-          atomicOr(err, kErrBudget);
-          done = true;
-          break;
-        }
-        if (cur_e < min_t) {
-          if (count > 0) break;
-          float4 l0, l1, r0, r1;
-          load_node(&s.top[2 * lf], l0, l1);
-          load_node(&s.top[2 * lf + 2], r0, r1);
-          float dl, dr;
-          const bool hl = box_hit(r, l0, l1, near, min_t, dl);
-          const bool hr = box_hit(r, r0, r1, near, min_t, dr);
-          const bool swap = hl && hr && dr < dl;
-          const bool hn = swap ? hr : hl, hf = swap ? hl : hr;
-          const float dn = swap ? dr : dl, df = swap ? dl : dr;
-          if (hf) {
-            if (sp >= kTraceStack) {
-              atomicOr(err, kErrStack);
-              done = true;
-              break;
-            }
-            stk_lf[sp] = __float_as_uint(swap ? l0.w : r0.w);
-            stk_cnt[sp] = __float_as_uint(swap ? l1.w : r1.w);
-            stk_e[sp] = df;
-            ++sp;
-          }
-          if (hn) {
-            lf = __float_as_uint(swap ? r0.w : l0.w);
-            count = __float_as_uint(swap ? r1.w : l1.w);
-            cur_e = dn;
-            continue;
-          }
-        }
-        if (sp == 0) {
-          done = true;
-          break;
-        }
-        --sp;
-        lf = stk_lf[sp];
-        count = stk_cnt[sp];
-        cur_e = stk_e[sp];
-      }
-      // A leaf: its primitives over [near, min_t], a candidate adopted only when strictly nearer.
-      if (!done) {
+      if (budget-- == 0) {
+        atomicOr(err, kErrBudget);
+        done = true;
+      } else if (leaf_step) {
+        // A leaf: its primitives over [near, min_t], a candidate adopted only when strictly nearer.
         for (uint32_t k = lf; k < lf + count; ++k) {
           const uint32_t ref = __ldg(&s.order[k]);
           float t;
@@ -571,22 +533,72 @@ __global__ void __launch_bounds__(256, 2) k_extend_walk(WaveBuffers w, Src src, 
           count = stk_cnt[sp];
           cur_e = stk_e[sp];
         }
+      } else {
+        // One node of the walk: an interior node's children (the farther pushed, the nearer
+        // taken), or a pop when the current entry is dropped (>= min_t) or no child was hit.
+        bool pop = true;
+        if (cur_e < min_t) {
+          float4 l0, l1, r0, r1;
+          load_node(&s.top[2 * lf], l0, l1);
+          load_node(&s.top[2 * lf + 2], r0, r1);
+          float dl, dr;
+          const bool hl = box_hit(r, l0, l1, near, min_t, dl);
+          const bool hr = box_hit(r, r0, r1, near, min_t, dr);
+          const bool swap = hl && hr && dr < dl;
+          const bool hn = swap ? hr : hl, hf = swap ? hl : hr;
+          const float dn = swap ? dr : dl, df = swap ? dl : dr;
+          if (hf) {
+            if (sp >= kTraceStack) {
+              atomicOr(err, kErrStack);
+              done = true;
+            } else {
+              stk_lf[sp] = __float_as_uint(swap ? l0.w : r0.w);
+              stk_cnt[sp] = __float_as_uint(swap ? l1.w : r1.w);
+              stk_e[sp] = df;
+              ++sp;
+            }
+          }
+          if (hn) {
+            lf = __float_as_uint(swap ? r0.w : l0.w);
+            count = __float_as_uint(swap ? r1.w : l1.w);
+            cur_e = dn;
+            pop = false;
+          }
+        }
+        if (pop && !done) {
+          if (sp == 0) {
+            done = true;
+          } else {
+            --sp;
+            lf = stk_lf[sp];
+            count = stk_cnt[sp];
+            cur_e = stk_e[sp];
+          }
+        }
       }
-      if (done) {
-        w.ht[p] = have ? min_t : 0.f;  // the adopted hit's distance (min_t = c.d)
-        w.hobj[p] = have ? leaf_out : 0xFFFFFFFFu;
-        w.hprim[p] = prim_out;
-        active = false;
-      }
+    }
+    if (done) {
+      w.ht[p] = have ? min_t : 0.f;  // the adopted hit's distance (min_t = c.d)
+      w.hobj[p] = have ? leaf_out : 0xFFFFFFFFu;
+      w.hprim[p] = prim_out;
+      active = false;
     }
   }
 }
 
-template <class Src>
+// kStage: the path and shadow queues are pushed per block instead of per warp: a block-wide
+// scan of the warps' ballots and one atomicAdd per block and queue, the path indices written
+// as one contiguous run, and the shadow records (11 planes) staged in shared memory and
+// copied out as one contiguous SoA run per block (thread t writes entry t of each plane).
+template <class Src, bool kStage>
 __global__ void __launch_bounds__(256) k_shade(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
                                                const uint32_t* __restrict__ qcount, uint32_t* __restrict__ qout,
                                                uint32_t* __restrict__ qout_count, CacheWave cw, uint32_t cache_mode,
                                                uint32_t term_hit) {
+  constexpr int kMaxThreads = 256, kMaxWarps = kMaxThreads / 32;
+  __shared__ uint32_t st_off[2][kMaxWarps], st_base[2], st_total[2];
+  __shared__ uint32_t st_path[kStage ? kMaxThreads : 1];
+  __shared__ float st_rec[kStage ? 10 : 1][kStage ? kMaxThreads : 1];
   const uint32_t n = *qcount;
   // every lane runs the same trip count so the warp-aggregated pushes see full warps
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -705,15 +717,56 @@ __global__ void __launch_bounds__(256) k_shade(WaveBuffers w, Src src, const uin
         push_path = true;
       }
     }
-    const uint32_t qi = warp_push(qout_count, push_path);
-    if (push_path) qout[qi] = p;
-    const uint32_t si = warp_push(w.counts + 2, push_shadow);
-    if (push_shadow) {
-      w.s_path[si] = p;
-      w.s_ox[si] = sro.x; w.s_oy[si] = sro.y; w.s_oz[si] = sro.z;
-      w.s_dx[si] = srd.x; w.s_dy[si] = srd.y; w.s_dz[si] = srd.z;
-      w.s_tmax[si] = stmax;
-      w.s_cr[si] = contrib.x; w.s_cg[si] = contrib.y; w.s_cb[si] = contrib.z;
+    if (kStage) {
+      const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, lt = (1u << lane) - 1u;
+      const unsigned bp = __ballot_sync(0xffffffffu, push_path), bs = __ballot_sync(0xffffffffu, push_shadow);
+      if (lane == 0) {
+        st_off[0][warp] = __popc(bp);
+        st_off[1][warp] = __popc(bs);
+      }
+      __syncthreads();
+      if (threadIdx.x < 2) {  // exclusive scan over the warps, one atomicAdd per queue
+        uint32_t run = 0;
+        for (uint32_t v = 0; v < blockDim.x / 32u; ++v) {
+          const uint32_t c = st_off[threadIdx.x][v];
+          st_off[threadIdx.x][v] = run;
+          run += c;
+        }
+        st_total[threadIdx.x] = run;
+        st_base[threadIdx.x] = run ? atomicAdd(threadIdx.x == 0 ? qout_count : w.counts + 2, run) : 0u;
+      }
+      __syncthreads();
+      if (push_path) qout[st_base[0] + st_off[0][warp] + __popc(bp & lt)] = p;
+      if (push_shadow) {
+        const uint32_t slot = st_off[1][warp] + __popc(bs & lt);
+        st_path[slot] = p;
+        st_rec[0][slot] = sro.x; st_rec[1][slot] = sro.y; st_rec[2][slot] = sro.z;
+        st_rec[3][slot] = srd.x; st_rec[4][slot] = srd.y; st_rec[5][slot] = srd.z;
+        st_rec[6][slot] = stmax;
+        st_rec[7][slot] = contrib.x; st_rec[8][slot] = contrib.y; st_rec[9][slot] = contrib.z;
+      }
+      __syncthreads();
+      const uint32_t total = st_total[1], base = st_base[1];
+      for (uint32_t t = threadIdx.x; t < total; t += blockDim.x) {
+        const uint32_t si = base + t;
+        w.s_path[si] = st_path[t];
+        w.s_ox[si] = st_rec[0][t]; w.s_oy[si] = st_rec[1][t]; w.s_oz[si] = st_rec[2][t];
+        w.s_dx[si] = st_rec[3][t]; w.s_dy[si] = st_rec[4][t]; w.s_dz[si] = st_rec[5][t];
+        w.s_tmax[si] = st_rec[6][t];
+        w.s_cr[si] = st_rec[7][t]; w.s_cg[si] = st_rec[8][t]; w.s_cb[si] = st_rec[9][t];
+      }
+      __syncthreads();  // the staging arrays are reused by the next iteration
+    } else {
+      const uint32_t qi = warp_push(qout_count, push_path);
+      if (push_path) qout[qi] = p;
+      const uint32_t si = warp_push(w.counts + 2, push_shadow);
+      if (push_shadow) {
+        w.s_path[si] = p;
+        w.s_ox[si] = sro.x; w.s_oy[si] = sro.y; w.s_oz[si] = sro.z;
+        w.s_dx[si] = srd.x; w.s_dy[si] = srd.y; w.s_dz[si] = srd.z;
+        w.s_tmax[si] = stmax;
+        w.s_cr[si] = contrib.x; w.s_cg[si] = contrib.y; w.s_cb[si] = contrib.z;
+      }
     }
     if (cache_mode != kCacheOff) {  // uniform over the grid, so the pushes see whole warps
       const uint32_t ci = warp_push(cw.counts, push_query);
@@ -917,6 +970,39 @@ cudaError_t launch_scene_any(const SceneView& s, const float* rays, uint64_t str
 // nodes; one thread per path (k_extend) below it.
 constexpr uint32_t kWalkMinTopNodes = 64;
 
+// The walk's step schedule: a leaf step once `leaf_min` lanes of a warp stand on a leaf, a
+// refill once `refill_min` lanes are idle. PBRT_WALK_SCHEDULE="leaf_min,refill_min" (each in
+// 1..32) overrides the default for measurements; films do not depend on it.
+struct WalkSchedule {
+  int leaf_min = 8, refill_min = 8;
+};
+
+static WalkSchedule walk_schedule() {
+  static const WalkSchedule v = [] {
+    WalkSchedule d;
+    if (const char* e = std::getenv("PBRT_WALK_SCHEDULE")) {
+      int a = 0, b = 0;
+      if (std::sscanf(e, "%d,%d", &a, &b) == 2 && a >= 1 && a <= 32 && b >= 1 && b <= 32) {
+        d.leaf_min = a;
+        d.refill_min = b;
+      }
+    }
+    return d;
+  }();
+  return v;
+}
+
+// Queue pushes of the shading kernel per block through shared memory (k_shade<.., true>)
+// instead of per warp: PBRT_SHADE_STAGING=1 / 0 selects it for measurements; films do not
+// depend on it beyond the order of queue entries.
+static bool shade_staging() {
+  static const bool v = [] {
+    const char* e = std::getenv("PBRT_SHADE_STAGING");
+    return e && e[0] == '1';
+  }();
+  return v;
+}
+
 // extend -> shade -> shadow, `loops` times, over the ping-pong queues. `top_nodes`: the largest
 // top-level tree among the scenes rendered; `csg`: some scene holds a constructive solid (the
 // traversal kernels are also built without the solids' code, which takes registers and spills
@@ -935,15 +1021,21 @@ static cudaError_t bounce_loop(const WaveBuffers& w, const Src& src, const Cache
     if ((e = cudaMemsetAsync(cout, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
     // counts[2]: shadow rays queued by k_shade; counts[3]: k_extend_walk's fetch position
     if ((e = cudaMemsetAsync(w.counts + 2, 0, 2 * sizeof(uint32_t), st)) != cudaSuccess) return e;
+    const WalkSchedule ws = walk_schedule();
     if (top_nodes >= kWalkMinTopNodes && csg)
-      k_extend_walk<Src, true><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, w.counts + 3, err, stats);
+      k_extend_walk<Src, true><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, w.counts + 3, err, stats,
+                                                                ws.leaf_min, ws.refill_min);
     else if (top_nodes >= kWalkMinTopNodes)
-      k_extend_walk<Src, false><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, w.counts + 3, err, stats);
+      k_extend_walk<Src, false><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, w.counts + 3, err, stats,
+                                                                 ws.leaf_min, ws.refill_min);
     else if (csg)
       k_extend<Src, true><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, err, stats);
     else
       k_extend<Src, false><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, err, stats);
-    k_shade<Src><<<gs, sh.shade_threads, 0, st>>>(w, src, qin, cin, qout, cout, cw, cache_mode, term_hit);
+    if (shade_staging())
+      k_shade<Src, true><<<gs, sh.shade_threads, 0, st>>>(w, src, qin, cin, qout, cout, cw, cache_mode, term_hit);
+    else
+      k_shade<Src, false><<<gs, sh.shade_threads, 0, st>>>(w, src, qin, cin, qout, cout, cw, cache_mode, term_hit);
     // (a persistent walk for the shadow rays measured 2.6% slower on 10,000 spheres: any-hit
     // rays end early, so one thread per ray wastes little)
     if (shadows && csg) k_shadow<Src, true><<<gt, sh.trace_threads, 0, st>>>(w, src, err, stats);

@@ -10,13 +10,15 @@
 //      index (when a record buffer is given), so that stage 2 reads its rays coalesced
 //      instead of gathering eight planes per ray;
 //   2. k_mesh_closest_persistent runs persistent warps over the queue, refilling idle lanes
-//      with ballot/popc and one atomicAdd per warp, and walks interior nodes until each lane
-//      reaches a leaf before any lane tests triangles (so a leaf of one lane does not
-//      serialise the warp at every step). Each lane still visits its nodes in the
-//      reference's order, so ids and t stay bit-exact.
+//      with ballot/popc and one atomicAdd per warp; each iteration is one warp-voted step,
+//      a node step for the lanes on interior nodes or, once enough lanes stand on a leaf, a
+//      leaf step for those (so leaves are tested in batches and interior lanes rarely wait).
+//      Each lane still visits its nodes in the reference's order, so ids and t stay bit-exact.
 // k_mesh_closest (one thread per ray) is the instrumented form that counts the work.
 #include <cfloat>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 
 #include "kernels.hpp"
 #include "trace_mesh.cuh"
@@ -189,22 +191,31 @@ PBRT_DEV bool pop_next(TraversalStack& s, int& sp, float min_t, uint32_t& lf, ui
   return false;
 }
 
+// One warp-voted step per iteration: either a node step for the lanes standing on an
+// interior node or a leaf step for the lanes standing on a leaf, never both. A leaf step is
+// taken once at least `leaf_min` lanes stand on a leaf (or no lane has interior work left);
+// until then the lanes on a leaf wait and the others keep descending. Idle lanes are refilled
+// from the queue once at least `refill_min` of them are idle (or all are). Waiting for every
+// lane to reach a leaf before any leaf is tested (the classic while-while loop) left 3/4 of
+// the lanes idle on this workload; this schedule keeps most lanes on interior nodes, where
+// the work is. Each lane still visits its nodes in the reference's order, so ids and t are
+// unchanged.
+//
 // 12 resident blocks of 128 threads per SM (at most 40 registers a thread): the traversal is
-// latency-bound, and the extra warps hide more of it than the few spilled registers cost
-// (measured: 1.01 ms against 1.10 ms at the compiler's 72 registers for the 16M-ray step).
+// latency-bound, and the extra warps hide more of it than the few spilled registers cost.
+#ifndef PBRT_TRAVERSAL_MIN_BLOCKS
+#define PBRT_TRAVERSAL_MIN_BLOCKS 12
+#endif
 template <bool kRec>
-__global__ void __launch_bounds__(128, 12) k_mesh_closest_persistent(MeshView m, const float* __restrict__ rays,
-                                                                 uint64_t stride, const uint32_t* __restrict__ queue,
-                                                                 const unsigned long long* __restrict__ queue_count,
-                                                                 uint32_t* __restrict__ prim,
-                                                                 float* __restrict__ tout, uint32_t* __restrict__ obj,
-                                                                 unsigned long long* __restrict__ next_ray,
-                                                                 uint32_t* __restrict__ err,
-                                                                 const float4* __restrict__ rec) {
+__global__ void __launch_bounds__(128, PBRT_TRAVERSAL_MIN_BLOCKS) k_mesh_closest_persistent(
+    MeshView m, const float* __restrict__ rays, uint64_t stride, const uint32_t* __restrict__ queue,
+    const unsigned long long* __restrict__ queue_count, uint32_t* __restrict__ prim, float* __restrict__ tout,
+    uint32_t* __restrict__ obj, unsigned long long* __restrict__ next_ray, uint32_t* __restrict__ err,
+    const float4* __restrict__ rec, int leaf_min, int refill_min) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
   const uint64_t n = *queue_count;
-  bool active = false;
+  bool active = false, exhausted = false;  // exhausted is warp-uniform
   uint32_t idx = 0;
   PRay r;
   float near = 0.f, far = 0.f, min_t = FLT_MAX;
@@ -215,10 +226,9 @@ __global__ void __launch_bounds__(128, 12) k_mesh_closest_persistent(MeshView m,
   const uint32_t root_cnt = __float_as_uint(__ldg(&m.nodes[1]).w);
 
   for (;;) {
-    // Refill the lanes whose ray is finished: one atomicAdd per warp.
+    // Refill the idle lanes: one atomicAdd per warp.
     const unsigned idle = __ballot_sync(0xffffffffu, !active);
-    bool exhausted = false;
-    if (idle) {
+    if (!exhausted && idle && (__popc(idle) >= refill_min || idle == 0xffffffffu)) {
       const int leader = __ffs(idle) - 1;
       unsigned long long base = 0;
       if (int(lane) == leader) base = atomicAdd(next_ray, (unsigned long long)__popc(idle));
@@ -252,19 +262,31 @@ __global__ void __launch_bounds__(128, 12) k_mesh_closest_persistent(MeshView m,
         }
       }
     }
-    if (__ballot_sync(0xffffffffu, active) == 0) {
+    const unsigned act = __ballot_sync(0xffffffffu, active);
+    if (act == 0) {
       if (exhausted) break;
-      continue;
+      continue;  // all idle and the queue not yet drained: the next iteration refills
     }
-    if (active) {
-      bool done = false;
-      // Interior walk until this lane stands on a leaf (or its ray is finished).
-      while (count == 0) {
-        if (budget-- == 0) {
-          atomicOr(err, kErrBudget);
-          done = true;
-          break;
+    const unsigned on_leaf = __ballot_sync(0xffffffffu, active && count > 0);
+    const bool leaf_step = __popc(on_leaf) >= leaf_min || on_leaf == act;
+    bool done = false;
+    if (active && (count > 0) == leaf_step) {
+      if (budget-- == 0) {
+        atomicOr(err, kErrBudget);
+        done = true;
+      } else if (leaf_step) {
+        for (uint32_t k = lf; k < lf + count; ++k) {
+          const float4 A = __ldg(&m.tri_a[k]);
+          const float4 B = __ldg(&m.tri_b[k]);
+          const float2 C = __ldg(&m.tri_c[k]);
+          float t;
+          if (tri_hit(r, A, B, C.x, t) && t < min_t && t >= near && t <= far) {
+            min_t = t;
+            best = __float_as_uint(C.y);
+          }
         }
+        if (!pop_next(stk, sp, min_t, lf, count)) done = true;
+      } else {
         float4 l0, l1, r0, r1;
         load_node(&m.nodes[2 * lf], l0, l1);
         load_node(&m.nodes[2 * lf + 2], r0, r1);
@@ -281,12 +303,12 @@ __global__ void __launch_bounds__(128, 12) k_mesh_closest_persistent(MeshView m,
             if (sp >= kTraceStack) {
               atomicOr(err, kErrStack);
               done = true;
-              break;
+            } else {
+              stk.lf[sp] = __float_as_uint(swap ? l0.w : r0.w);
+              stk.cnt[sp] = __float_as_uint(swap ? l1.w : r1.w);
+              stk.e[sp] = df;
+              ++sp;
             }
-            stk.lf[sp] = __float_as_uint(swap ? l0.w : r0.w);
-            stk.cnt[sp] = __float_as_uint(swap ? l1.w : r1.w);
-            stk.e[sp] = df;
-            ++sp;
           }
           lf = __float_as_uint(swap ? r0.w : l0.w);
           count = __float_as_uint(swap ? r1.w : l1.w);
@@ -295,38 +317,40 @@ __global__ void __launch_bounds__(128, 12) k_mesh_closest_persistent(MeshView m,
           count = __float_as_uint(swap ? l1.w : r1.w);
         } else if (!pop_next(stk, sp, min_t, lf, count)) {
           done = true;
-          break;
         }
-      }
-      // Leaf: every lane that reached one tests its triangles in the same pass.
-      if (!done) {
-        if (budget-- == 0) {
-          atomicOr(err, kErrBudget);
-          done = true;
-        } else {
-          for (uint32_t k = lf; k < lf + count; ++k) {
-            const float4 A = __ldg(&m.tri_a[k]);
-            const float4 B = __ldg(&m.tri_b[k]);
-            const float2 C = __ldg(&m.tri_c[k]);
-            float t;
-            if (tri_hit(r, A, B, C.x, t) && t < min_t && t >= near && t <= far) {
-              min_t = t;
-              best = __float_as_uint(C.y);
-            }
-          }
-          if (!pop_next(stk, sp, min_t, lf, count)) done = true;
-        }
-      }
-      if (done) {
-        if (best != 0xFFFFFFFFu) {  // stage 1 already wrote the miss answer
-          __stcs(prim + idx, best);
-          __stcs(tout + idx, min_t);
-          if (obj) __stcs(obj + idx, 0u);
-        }
-        active = false;
       }
     }
+    if (done) {
+      if (best != 0xFFFFFFFFu) {  // stage 1 already wrote the miss answer
+        __stcs(prim + idx, best);
+        __stcs(tout + idx, min_t);
+        if (obj) __stcs(obj + idx, 0u);
+      }
+      active = false;
+    }
   }
+}
+
+// The persistent traversal's step schedule: a leaf step once `leaf_min` lanes of a warp stand
+// on a leaf, a refill once `refill_min` lanes are idle. PBRT_TRACE_SCHEDULE="leaf_min,refill_min"
+// (each in 1..32) overrides the default for measurements; results do not depend on it.
+struct TraversalSchedule {
+  int leaf_min = 8, refill_min = 8;
+};
+
+static TraversalSchedule traversal_schedule() {
+  static const TraversalSchedule v = [] {
+    TraversalSchedule d;
+    if (const char* e = std::getenv("PBRT_TRACE_SCHEDULE")) {
+      int a = 0, b = 0;
+      if (std::sscanf(e, "%d,%d", &a, &b) == 2 && a >= 1 && a <= 32 && b >= 1 && b <= 32) {
+        d.leaf_min = a;
+        d.refill_min = b;
+      }
+    }
+    return d;
+  }();
+  return v;
 }
 
 static unsigned grid_for(uint64_t n, int threads, int sm_count) {
@@ -382,12 +406,13 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
   const uint64_t full = uint64_t(sm_count) * blocks_per_sm;
   const uint64_t need = (n + 127) / 128;
   const unsigned g = unsigned(need < full ? need : full);
+  const TraversalSchedule ts = traversal_schedule();
   if (rec)
     k_mesh_closest_persistent<true><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj, counters + 1, err,
-                                                      rec);
+                                                      rec, ts.leaf_min, ts.refill_min);
   else
     k_mesh_closest_persistent<false><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj, counters + 1,
-                                                       err, nullptr);
+                                                       err, nullptr, ts.leaf_min, ts.refill_min);
   return cudaGetLastError();
 }
 
@@ -438,8 +463,9 @@ cudaError_t launch_mesh_closest_noalloc(const MeshView& m, const float* rays, ui
   const uint64_t full = uint64_t(sm_count) * blocks_per_sm;
   const uint64_t need = (n + 127) / 128;
   const unsigned g = unsigned(need < full ? need : full);
+  const TraversalSchedule ts = traversal_schedule();
   k_mesh_closest_persistent<false><<<g, 128, 0, s>>>(m, rays, n, queue, counters, prim, t, nullptr, counters + 1, err,
-                                                     nullptr);
+                                                     nullptr, ts.leaf_min, ts.refill_min);
   return cudaGetLastError();
 }
 
