@@ -295,6 +295,7 @@ def _declare_scene(L):
         getattr(L, f"oracle_scene_trace_{suf}").argtypes = [vp, vp, sz, vp, vp, vp, C.c_int]
         getattr(L, f"oracle_scene_occluded_{suf}").argtypes = [vp, vp, sz, vp, C.c_int]
         getattr(L, f"oracle_render_{suf}").argtypes = [vp, C.POINTER(_ORender), vp, C.c_int]
+        getattr(L, f"oracle_render_counted_{suf}").argtypes = [vp, C.POINTER(_ORender), vp, C.c_int, vp]
         getattr(L, f"oracle_render_cached_{suf}").argtypes = [vp, C.POINTER(_ORender), vp, vp, C.c_uint32, vp,
                                                               C.c_int]
         getattr(L, f"oracle_camera_rays_{suf}").argtypes = [C.POINTER(_OCamera), vp]
@@ -489,6 +490,22 @@ class Scene:
             raise RuntimeError(lib().oracle_last_error().decode())
         return film
 
+    def render_counted(self, camera: dict, spp: int, max_depth: int, seed: int = 1, rr_start: int = 0,
+                       sample_offset: int = 0, threads: int = os.cpu_count() or 1):
+        """render() with the path integrator, plus its work summed over every scene query:
+        (film, {rays, shadow_rays, top_boxes, objects, mesh_boxes, triangles, shapes})."""
+        p = _ORender()
+        p.camera = _camera(camera)
+        p.spp, p.max_depth, p.rr_start, p.sample_offset = spp, max_depth, rr_start, sample_offset
+        p.seed, p.integrator = seed, 0
+        film = np.zeros((int(camera["height"]), int(camera["width"]), 3), np.float64)
+        out = np.zeros(7, np.uint64)
+        if getattr(lib(), f"oracle_render_counted_{self.suf}")(self._h, C.byref(p), _ptr(film), threads,
+                                                                _ptr(out)) != 0:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        keys = ("rays", "shadow_rays", "top_boxes", "objects", "mesh_boxes", "triangles", "shapes")
+        return film, {k: int(v) for k, v in zip(keys, out)}
+
     def render_cached(self, camera: dict, spp: int, max_depth: int, weights, bounds, terminate_bounce: int = 2,
                       seed: int = 1, rr_start: int = 0, sample_offset: int = 0,
                       threads: int = os.cpu_count() or 1):
@@ -532,6 +549,7 @@ def _declare_mlp(L):
     L.oracle_mlp_forward.argtypes = [vp, vp, vp, C.c_size_t, vp, C.c_int, C.c_int]
     L.oracle_mlp_gradient.argtypes = [vp, vp, vp, vp, C.c_size_t, vp, vp, C.c_int]
     L.oracle_mlp_forward_f64.argtypes = [vp, vp, vp, C.c_size_t, vp]
+    L.oracle_mlp_forward_margins.argtypes = [vp, vp, vp, C.c_size_t, vp, vp, vp, C.c_int]
     L.oracle_mlp_adam.argtypes = [vp, vp, vp, vp, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float]
 
 
@@ -551,6 +569,21 @@ def mlp_forward(weights, bounds, records, emulate=True, threads: int = os.cpu_co
     out = np.zeros((r.shape[0], 3), np.float32)
     _mlp_lib().oracle_mlp_forward(_ptr(w), _ptr(b), _ptr(r), r.shape[0], _ptr(out), int(emulate), threads)
     return out
+
+
+def mlp_forward_margins(weights, bounds, records, threads: int = os.cpu_count() or 1):
+    """BF16-emulating outputs (n, 3), per record the smallest BF16 rounding margin of its
+    forward pass (distance of a BF16-rounded value to a rounding boundary, in units of 2^-24
+    times the magnitude sum of the terms that formed it), and the outputs' magnitude sums (n, 3)."""
+    w = np.ascontiguousarray(weights, np.float32)
+    b = np.ascontiguousarray(bounds, np.float32).reshape(6)
+    r = np.ascontiguousarray(records, np.float32).reshape(-1, 16)
+    n = r.shape[0]
+    out = np.zeros((n, 3), np.float32)
+    margin = np.zeros(n, np.float64)
+    scale = np.zeros((n, 3), np.float64)
+    _mlp_lib().oracle_mlp_forward_margins(_ptr(w), _ptr(b), _ptr(r), n, _ptr(out), _ptr(margin), _ptr(scale), threads)
+    return out, margin, scale
 
 
 def mlp_forward_f64(weights, bounds, records):

@@ -11,6 +11,7 @@
 // Loss: mean over samples and channels of (o - t)^2 / (o^2 + 0.01), denominator constant.
 #pragma once
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -39,14 +40,30 @@ inline float bf16(float f) {
   return r;
 }
 
+// sin(pi x) and cos(pi x) rounded to FP32: x is first reduced exactly modulo 2 (an FP32 x is
+// exact in double, and so is the remainder), multiples of 1/2 give exact 0 / +-1, any other x
+// the double-precision sine and cosine of pi times the remainder.
+inline void sincospi_f32(float x, double* s, double* c) {
+  double r = std::fmod(double(x), 2.0);
+  if (r < 0.0) r += 2.0;
+  if (r * 2.0 == std::floor(r * 2.0)) {  // r in {0, 0.5, 1, 1.5}
+    static const double ks[4] = {0.0, 1.0, 0.0, -1.0}, kc[4] = {1.0, 0.0, -1.0, 0.0};
+    const int q = int(r * 2.0);
+    *s = ks[q];
+    *c = kc[q];
+    return;
+  }
+  *s = double(float(std::sin(M_PI * r)));
+  *c = double(float(std::cos(M_PI * r)));
+}
+
 // Features of one record: sin/cos(pi * x * 2^j) of the normalised position, j < 12, then
 // wo, n, albedo, roughness.
 inline void encode(const float* rec, const float* lo, const float* inv_ext, double* f) {
   for (int a = 0; a < 3; ++a) {
     float x = (rec[a] - lo[a]) * inv_ext[a];
     for (int j = 0; j < 12; ++j) {
-      f[a * 24 + 2 * j] = double(float(std::sin(M_PI * double(x))));
-      f[a * 24 + 2 * j + 1] = double(float(std::cos(M_PI * double(x))));
+      sincospi_f32(x, &f[a * 24 + 2 * j], &f[a * 24 + 2 * j + 1]);
       x = x * 2.0f;
     }
   }
@@ -66,26 +83,64 @@ struct Net {
   double q(double x) const { return emulate ? double(bf16(float(x))) : x; }
   double fin(double x) const { return emulate ? double(float(x)) : x; }
 
-  // acts[l] = input of layer l (acts[0] = features), out = 16 outputs
-  void forward(const double* feat, std::vector<std::vector<double>>& acts, double* out) const {
+  // How far an FP32 value v lies from the nearest BF16 rounding boundary (the midpoint
+  // between the two BF16 neighbours of v), in units of 2^-24 * s: s is the sum of the
+  // magnitudes of the terms that produced v (|v| for a single rounded value), so an FP32
+  // result computed in another order, within k * 2^-24 * s of this one, rounds to the same
+  // BF16 value whenever the margin exceeds k.
+  static double bf16_margin(double v, double s) {
+    const float f = float(v);
+    if (f == 0.f || !std::isfinite(f) || s <= 0.0) return 1e300;
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    const uint32_t lo_bits = u & 0xFFFF0000u, hi_bits = lo_bits + 0x10000u;
+    float lo, hi;
+    std::memcpy(&lo, &lo_bits, 4);
+    std::memcpy(&hi, &hi_bits, 4);
+    const double mid = 0.5 * (double(lo) + double(hi));
+    return std::fabs(v - mid) / (std::ldexp(1.0, -24) * s);
+  }
+
+  // acts[l] = input of layer l (acts[0] = features), out = 16 outputs. In emulate mode,
+  // `margin` (optional) receives the smallest bf16_margin of every value the forward pass
+  // rounds to BF16 (the features and the five hidden layers' pre-activations that pass the
+  // ReLU), and `out_scale` (optional, 16) the sums of the output terms' magnitudes.
+  void forward(const double* feat, std::vector<std::vector<double>>& acts, double* out, double* margin = nullptr,
+               double* out_scale = nullptr) const {
     acts.assign(kLayers, {});
     acts[0].resize(kInPad);
-    for (int k = 0; k < kInPad; ++k) acts[0][k] = q(feat[k]);
+    double mg = 1e300;
+    for (int k = 0; k < kInPad; ++k) {
+      acts[0][k] = q(feat[k]);
+      if (margin) mg = std::min(mg, bf16_margin(feat[k], std::fabs(feat[k])));
+    }
     for (int l = 0; l < kLayers; ++l) {
       const int K = layer_k(l), N = layer_n(l);
-      std::vector<double> y(N);
+      std::vector<double> y(N), mag(N);
       for (int o = 0; o < N; ++o) {
-        double s = 0.0;
-        for (int i = 0; i < K; ++i) s += w[layer_off(l) + o * K + i] * acts[l][i];
+        double s = 0.0, m = 0.0;
+        for (int i = 0; i < K; ++i) {
+          const double t = w[layer_off(l) + o * K + i] * acts[l][i];
+          s += t;
+          m += std::fabs(t);
+        }
         y[o] = fin(s);
+        mag[o] = m;
       }
       if (l + 1 < kLayers) {
         acts[l + 1].resize(N);
-        for (int o = 0; o < N; ++o) acts[l + 1][o] = q(y[o] > 0.0 ? y[o] : 0.0);
+        for (int o = 0; o < N; ++o) {
+          acts[l + 1][o] = q(y[o] > 0.0 ? y[o] : 0.0);
+          if (margin && y[o] > 0.0) mg = std::min(mg, bf16_margin(y[o], mag[o]));
+        }
       } else {
-        for (int o = 0; o < N; ++o) out[o] = y[o];
+        for (int o = 0; o < N; ++o) {
+          out[o] = y[o];
+          if (out_scale) out_scale[o] = mag[o];
+        }
       }
     }
+    if (margin) *margin = mg;
   }
 
   // Adds this sample's gradient (scaled) to grad; returns its loss sum over channels.

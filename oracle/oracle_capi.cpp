@@ -9,6 +9,7 @@
 #include <cstring>
 #include <fstream>
 #include <memory>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <thread>
@@ -388,12 +389,17 @@ void scene_cast_sets(const OScene<R>* s, const OCameraDesc* c, const double* tar
 
 // renderers::mt::compute_pixel (mt.rs:112-130): spp jittered samples through the pinhole
 // camera, mean radiance per pixel (accumulated in f64, the film the judge image needs).
+// `tally` (optional) receives the render's work counters summed over all threads.
 template <class R>
-int render(const OScene<R>* s, const ORenderParams* p, double* film, int threads, const CacheHook* cache = nullptr) {
+int render(const OScene<R>* s, const ORenderParams* p, double* film, int threads, const CacheHook* cache = nullptr,
+           WorkTally* tally = nullptr) {
   const Camera<R> cam = make_camera<R>(p->camera);
   const uint32_t w = p->camera.width, h = p->camera.height;
   const size_t npix = size_t(w) * h;
+  std::mutex tally_mu;
   parallel_for(npix, threads, [&](size_t b, size_t e) {
+    WorkTally local;
+    work_tally = tally ? &local : nullptr;
     for (size_t pix = b; pix < e; ++pix) {
       const uint32_t x = uint32_t(pix % w), y = uint32_t(pix / w);
       double acc[3] = {0, 0, 0};
@@ -410,6 +416,11 @@ int render(const OScene<R>* s, const ORenderParams* p, double* film, int threads
         acc[2] += double(L.z);
       }
       for (int c = 0; c < 3; ++c) film[3 * pix + c] = acc[c] / double(p->spp);
+    }
+    work_tally = nullptr;
+    if (tally) {
+      std::lock_guard<std::mutex> lock(tally_mu);
+      tally->add(local);
     }
   });
   return 0;
@@ -496,6 +507,21 @@ extern "C" {
       return -1;                                                                                            \
     }                                                                                                       \
   }                                                                                                         \
+  /* the render with its work counters: rays, shadow rays, top-level boxes, objects, mesh boxes,     \
+     triangles, analytic shape tests */                                                                     \
+  int oracle_render_counted_##SUF(void* s, const ORenderParams* p, double* film, int th, uint64_t* out7) {   \
+    try {                                                                                                   \
+      WorkTally t;                                                                                          \
+      const int rc = render((OScene<R>*)s, p, film, th, nullptr, &t);                                       \
+      const uint64_t v[7] = {t.rays, t.shadow_rays, t.top_boxes, t.objects, t.mesh_boxes, t.triangles,      \
+                             t.shapes};                                                                     \
+      for (int k = 0; k < 7; ++k) out7[k] = v[k];                                                           \
+      return rc;                                                                                            \
+    } catch (const std::exception& e) {                                                                     \
+      g_err = e.what();                                                                                     \
+      return -1;                                                                                            \
+    }                                                                                                       \
+  }                                                                                                         \
   int oracle_render_cached_##SUF(void* s, const ORenderParams* p, const float* weights, const float* bounds6,  \
                                  uint32_t term_hit, double* film, int th) {                                 \
     try {                                                                                                   \
@@ -549,6 +575,28 @@ int oracle_mlp_forward(const float* weights, const float* bounds6, const float* 
       oracle::mlp::encode(records + i * oracle::mlp::kRecord, lo, inv, f);
       net.forward(f, acts, o);
       for (int c = 0; c < 3; ++c) out[3 * i + c] = float(o[c]);
+    }
+  });
+  return 0;
+}
+
+// BF16-emulating outputs with, per record, the smallest BF16 rounding margin of its forward
+// pass (Net::forward) and the three outputs' term-magnitude sums.
+int oracle_mlp_forward_margins(const float* weights, const float* bounds6, const float* records, size_t n,
+                               float* out, double* margin, double* out_scale, int threads) {
+  const oracle::mlp::Net net(weights, true);
+  float lo[3], inv[3];
+  mlp_bounds(bounds6, lo, inv);
+  parallel_for(n, threads, [&](size_t b, size_t e) {
+    for (size_t i = b; i < e; ++i) {
+      double f[oracle::mlp::kInPad], o[oracle::mlp::kOutPad], sc[oracle::mlp::kOutPad];
+      std::vector<std::vector<double>> acts;
+      oracle::mlp::encode(records + i * oracle::mlp::kRecord, lo, inv, f);
+      net.forward(f, acts, o, margin + i, sc);
+      for (int c = 0; c < 3; ++c) {
+        out[3 * i + c] = float(o[c]);
+        out_scale[3 * i + c] = sc[c];
+      }
     }
   });
   return 0;

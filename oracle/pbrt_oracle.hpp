@@ -314,23 +314,28 @@ class MeshBVH {
   }
 
   // BVHTree::intersect_p (bvh.rs:381-420): unordered, fixed interval, first hit wins.
-  bool intersect_p(const Ray<R>& ray, R near, R far) const {
+  // `st` (optional) counts the work as traverse() does: nodes visited, box and triangle tests.
+  bool intersect_p(const Ray<R>& ray, R near, R far, TraversalStats* st = nullptr) const {
     R dist;
+    if (st) st->box_tests++;
     if (!box_hit(nodes_[0].box, ray, near, far, &dist)) return false;
     uint64_t stack[256];
     int sp = 0;
     stack[sp++] = 0;
     while (sp > 0) {
       const Node& n = nodes_[stack[--sp]];
+      if (st) st->nodes_visited++;
       if (n.count > 0) {
         for (uint64_t i = 0; i < n.count; ++i) {
           const Tri& t = tris_[tri_idx_[n.left_first + i]];
           TriHit<R> h;
+          if (st) st->triangle_tests++;
           if (intersect_ray(ray, vertex(t.v0), vertex(t.v1), vertex(t.v2), &h))
             if (h.t >= near && h.t <= far) return true;
         }
       } else {
         for (uint64_t c = n.left_first; c <= n.left_first + 1; ++c) {
+          if (st) st->box_tests++;
           if (box_hit(nodes_[c].box, ray, near, far, &dist)) {
             if (sp >= 256) throw std::runtime_error("oracle stack overflow");
             stack[sp++] = c;

@@ -222,6 +222,19 @@ struct SceneStats {
   uint64_t nodes_visited = 0, box_tests = 0, object_tests = 0;
 };
 
+// The work of a render, summed over its scene queries (for the render path's algorithmic
+// bytes): rays and shadow rays traced, top-level box tests and objects tested, the meshes'
+// own box and triangle tests, and analytic shape tests (spheres, cylinders, rectangles,
+// boxes, planes, solids). A render thread points work_tally at its own tally.
+struct WorkTally {
+  uint64_t rays = 0, shadow_rays = 0, top_boxes = 0, objects = 0, mesh_boxes = 0, triangles = 0, shapes = 0;
+  void add(const WorkTally& o) {
+    rays += o.rays; shadow_rays += o.shadow_rays; top_boxes += o.top_boxes; objects += o.objects;
+    mesh_boxes += o.mesh_boxes; triangles += o.triangles; shapes += o.shapes;
+  }
+};
+inline thread_local WorkTally* work_tally = nullptr;
+
 template <class R>
 class OScene {
  public:
@@ -822,12 +835,18 @@ class OScene {
     const Ray<R> lr = local_ray(o, ray);
     Isect<R> h;
     R t;
+    if (work_tally && o.shape != O_SHAPE_MESH) work_tally->shapes++;
     if (o.shape == O_SHAPE_MESH) {
       const Mesh& m = meshes[o.mesh];
       TriHit<R> th;
       uint32_t tri;
       TraversalStats st;
-      if (!m.bvh->traverse(lr, near, far, &th, &tri, &st)) return false;
+      const bool hit = m.bvh->traverse(lr, near, far, &th, &tri, &st);
+      if (work_tally) {
+        work_tally->mesh_boxes += st.box_tests;
+        work_tally->triangles += st.triangle_tests;
+      }
+      if (!hit) return false;
       mesh_details(m, tri, lr, th, &h);
       *prim = tri;
     } else if (o.shape == O_SHAPE_SPHERE) {
@@ -863,8 +882,17 @@ class OScene {
     const Ray<R> lr = local_ray(o, ray);
     R t;
     int piece;
+    if (work_tally && o.shape != O_SHAPE_MESH) work_tally->shapes++;
     switch (o.shape) {
-      case O_SHAPE_MESH: return meshes[o.mesh].bvh->intersect_p(lr, near, far);
+      case O_SHAPE_MESH: {
+        TraversalStats st;
+        const bool hit = meshes[o.mesh].bvh->intersect_p(lr, near, far, work_tally ? &st : nullptr);
+        if (work_tally) {
+          work_tally->mesh_boxes += st.box_tests;
+          work_tally->triangles += st.triangle_tests;
+        }
+        return hit;
+      }
       case O_SHAPE_SPHERE: return sphere_hit(o, lr, near, far, &t);
       case O_SHAPE_CYLINDER: return cylinder_hit(o, lr, near, far, &t, &piece);
       case O_SHAPE_RECTANGLE: return rectangle_hit(o, lr, near, far, &t);
@@ -1091,6 +1119,14 @@ class OScene {
   // (bvh.rs:153-230) over [near, nearest so far], adopting only strictly nearer hits.
   bool intersect(const Ray<R>& ray, R near, R far, Isect<R>* out, uint32_t* obj_out, uint32_t* prim_out,
                  SceneStats* st = nullptr) const {
+    if (work_tally && !st) {  // count this query into the render's tally
+      SceneStats local;
+      const bool h = intersect(ray, near, far, out, obj_out, prim_out, &local);
+      work_tally->rays++;
+      work_tally->top_boxes += local.box_tests;
+      work_tally->objects += local.object_tests;
+      return h;
+    }
     bool have = false;
     Isect<R> nearest{};
     for (uint32_t r : unbounded) {  // nearest_among + closer (scene.rs:222-249)
@@ -1152,6 +1188,14 @@ class OScene {
   // Scene::any_hit (scene.rs:157-184): the unbounded primitives first, then BVH::query_p
   // (bvh.rs:239-275): unordered, the box tested at pop, left popped first.
   bool occluded(const Ray<R>& ray, R near, R far, SceneStats* st = nullptr) const {
+    if (work_tally && !st) {
+      SceneStats local;
+      const bool h = occluded(ray, near, far, &local);
+      work_tally->shadow_rays++;
+      work_tally->top_boxes += local.box_tests;
+      work_tally->objects += local.object_tests;
+      return h;
+    }
     for (uint32_t r : unbounded) {
       if (st) st->object_tests++;
       if (occluded_node(r, ray, near, far)) return true;
