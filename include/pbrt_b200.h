@@ -449,9 +449,11 @@ int pbrt_ctx_get_tuning(pbrt_ctx* ctx, pbrt_tuning* tuning);
 
 /* Many scenes rendered together (no counterpart in the reference, whose renderer takes one
  * scene): the paths of all scenes share the waves, queues and kernel launches of one
- * wavefront, scene by scene in the given order, and the launch sequence of one frame is
- * recorded once in a CUDA graph that pbrt_batch_render replays. The scenes must belong to
- * ctx and outlive the batch; params[i] (integrator path or naive) renders scenes[i]. */
+ * wavefront, scene by scene, cheapest first (pixels x spp x max depth; ties keep the given
+ * order, which minimises the frame's mean completion time), and the launch sequence of one
+ * frame is recorded once in a CUDA graph that pbrt_batch_render replays. The scenes must
+ * belong to ctx and outlive the batch; params[i] (integrator path or naive) renders
+ * scenes[i]; films and times are reported per caller index i. */
 typedef struct pbrt_batch pbrt_batch;
 int pbrt_batch_create(pbrt_ctx* ctx, pbrt_scene* const* scenes, const pbrt_render_params* params, uint32_t n,
                       pbrt_batch** out);

@@ -19,6 +19,7 @@ struct pbrt_batch {
   pbrt_ctx* ctx = nullptr;
   std::vector<BatchScene> table;  // host copy (film pointers are the batch's device films)
   std::vector<size_t> film_n;     // doubles per film
+  std::vector<uint32_t> slot;     // the table position of the caller's scene i (cheapest first)
   BatchScene* d_table = nullptr;
   uint32_t* d_frame = nullptr;
   uint32_t frame_host = 0;
@@ -82,8 +83,22 @@ int pbrt_batch_create(pbrt_ctx* c, pbrt_scene* const* scenes, const pbrt_render_
   std::unique_ptr<pbrt_batch> b(new pbrt_batch);
   b->ctx = c;
   b->shape = c->shape;
-  unsigned long long begin = 0;
+  // Scenes run cheapest first (pixels x spp x max depth; ties keep the given order), which
+  // minimises the mean completion time of a frame; films and times stay per caller index.
+  std::vector<uint32_t> order(n);
+  std::vector<unsigned long long> cost(n, 0);
   for (uint32_t i = 0; i < n; ++i) {
+    order[i] = i;
+    const pbrt_render_params* p = params + i;
+    const unsigned long long px = (unsigned long long)p->camera.width * p->camera.height;
+    cost[i] = px * p->spp * std::max<uint32_t>(1u, p->max_depth);
+  }
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b2) { return cost[a] < cost[b2]; });
+  b->slot.assign(n, 0);
+  unsigned long long begin = 0;
+  for (uint32_t pos = 0; pos < n; ++pos) {
+    const uint32_t i = order[pos];
+    b->slot[i] = pos;
     const pbrt_scene* s = scenes[i];
     const pbrt_render_params* p = params + i;
     if (!s || s->ctx != c) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "scene " + std::to_string(i) + " is NULL or "
@@ -154,14 +169,16 @@ int pbrt_batch_render(pbrt_batch* b, uint32_t frame, double* const* films, float
   PBRT_TRY(c->cuda(cudaEventRecord(b->start, st), "cudaEventRecord"));
   PBRT_TRY(c->cuda(cudaGraphLaunch(b->exec, st), "cudaGraphLaunch"));
   if (films)
-    for (size_t i = 0; i < b->films.size(); ++i)
-      if (films[i])
-        PBRT_TRY(c->cuda(cudaMemcpyAsync(films[i], b->films[i], b->film_n[i] * sizeof(double), cudaMemcpyDefault, st),
+    for (size_t i = 0; i < b->slot.size(); ++i)
+      if (films[i]) {
+        const uint32_t k = b->slot[i];
+        PBRT_TRY(c->cuda(cudaMemcpyAsync(films[i], b->films[k], b->film_n[k] * sizeof(double), cudaMemcpyDefault, st),
                          "cudaMemcpy(batch film)"));
+      }
   PBRT_TRY(check_device_error(c, st));
   if (scene_ms)
-    for (size_t i = 0; i < b->done.size(); ++i)
-      PBRT_TRY(c->cuda(cudaEventElapsedTime(scene_ms + i, b->start, b->done[i]), "cudaEventElapsedTime"));
+    for (size_t i = 0; i < b->slot.size(); ++i)
+      PBRT_TRY(c->cuda(cudaEventElapsedTime(scene_ms + i, b->start, b->done[b->slot[i]]), "cudaEventElapsedTime"));
   return PBRT_OK;
 }
 
