@@ -174,17 +174,20 @@ CACHE_W, CACHE_H, CACHE_DEPTH = 1920, 1080, 32
 JUDGE_SPP, JUDGE_STRIDE, JUDGE_CHUNK = 32768, 4, 256
 TARGET = 1e-3
 PLAIN_SPP_PER_FRAME, CACHED_SPP_PER_FRAME, CACHE_WARMUP_ROUNDS = 8, 4, 50
-RACE_LIMIT_S = 90.0
+RACE_LIMIT_S = 75.0
+TRIMS = (("trim_0.01%", 1e-4), ("trim_0.1%", 1e-3), ("trim_1%", 1e-2))
 
 
 def cache_race(pb, W, ctx, device):
     """Both arms render the full 1920x1080 image frame after frame into a running FP64 mean;
     the error is measured on every JUDGE_STRIDE-th pixel in x and y against a plain render
     of those pixels (same pixel footprints) with JUDGE_SPP samples. relMSE =
-    mean((x - ref)^2 / (ref^2 + 0.01)); `trimmed` drops the 0.1% largest per-pixel terms
-    (caustic fireflies of the glossy faces, which even the judge has not averaged out).
-    Times are device times (CUDA events) of the render calls, training included; error
-    evaluation is outside them."""
+    mean((x - ref)^2 / (ref^2 + 0.01)) over the grid ("raw"); the trimmed forms drop the
+    0.01% / 0.1% / 1% largest per-pixel terms (caustic fireflies of the glossy faces, which
+    even the judge has not averaged out); "block4" averages 4x4 blocks of the grid first and
+    drops nothing. Every metric is recorded after every frame (the error curve) with its own
+    time to TARGET. Times are device times (CUDA events) of the render calls, training
+    included; error evaluation is outside them."""
     import torch
     from pbrt_b200.cache import RadianceCache
     from pbrt_b200.scene import film_shape
@@ -212,24 +215,45 @@ def cache_race(pb, W, ctx, device):
     def terms(x, ref):
         return ((x - ref) ** 2 / (ref * ref + 1e-2)).reshape(-1)
 
-    def trimmed(e):
-        k = int(e.numel() * 0.999)
-        return float(torch.sort(e).values[:k].mean())
+    def blocks(x):
+        """Means of 4x4 blocks of the judge grid (16 pixels 4 apart): fireflies are averaged with
+        their neighbours instead of dropped."""
+        h, w = (x.shape[0] // 4) * 4, (x.shape[1] // 4) * 4
+        return x[:h, :w].reshape(h // 4, 4, w // 4, 4, 3).mean(dim=(1, 3))
 
-    half = terms(ja, jb)
-    judge_err = {"raw": float(half.mean()) / 4, "trimmed": trimmed(half) / 4}
+    judge_blocks = blocks(judge)
+
+    def metrics(x, ref=judge, ref_blocks=judge_blocks):
+        """relMSE of the image x (on the judge grid) against ref: raw (every pixel), trimmed
+        (the largest 0.01% / 0.1% / 1% of per-pixel terms dropped) and block4 (4x4-block means
+        of the grid, nothing dropped)."""
+        e = terms(x, ref)
+        srt = torch.sort(e).values
+        n = e.numel()
+        out = {"raw": float(e.mean())}
+        for name, frac in TRIMS:
+            out[name] = float(srt[: int(n * (1.0 - frac))].mean())
+        out["block4"] = float(terms(blocks(x), ref_blocks).mean())
+        return out
+
+    # the judge's own error: half against half, scaled to the full judge (4x fewer samples each)
+    judge_err = {k: v / 4 for k, v in metrics(ja, jb, blocks(jb)).items()}
 
     def race(frame, spp_per_frame, setup=None):
+        """Renders frame after frame into a running mean until every metric but the raw one has
+        reached TARGET or RACE_LIMIT_S of wall time has passed; records every metric after
+        every frame (the error curve) and each metric's own time to TARGET."""
         full = torch.zeros((CACHE_H, CACHE_W, 3), dtype=torch.float64, device=device)
         acc = torch.zeros_like(full)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        dev_ms, n, hit, hist = 0.0, 0, None, []
+        dev_ms, n, curve = 0.0, 0, []
         if setup:
             ev0.record(stream)
             setup()
             ev1.record(stream)
             torch.cuda.synchronize()
             dev_ms += ev0.elapsed_time(ev1)
+        reached = {}
         wall0 = time.perf_counter()
         while time.perf_counter() - wall0 < RACE_LIMIT_S:
             ev0.record(stream)
@@ -239,21 +263,25 @@ def cache_race(pb, W, ctx, device):
             n += spp_per_frame
             torch.cuda.synchronize()
             dev_ms += ev0.elapsed_time(ev1)
-            e = terms(acc[::JUDGE_STRIDE, ::JUDGE_STRIDE] / n, judge)
-            tr = trimmed(e)
-            hist.append((n, dev_ms))
-            if tr <= TARGET:
-                mean = acc / n
-                hit = {"seconds": round(dev_ms / 1e3, 3), "spp": n, "relmse_trimmed": tr, "relmse_raw": float(e.mean()),
-                       "energy_bias": float(mean[::JUDGE_STRIDE, ::JUDGE_STRIDE].mean() / judge.mean() - 1.0)}
+            m = metrics(acc[::JUDGE_STRIDE, ::JUDGE_STRIDE] / n)
+            curve.append({"seconds": round(dev_ms / 1e3, 3), "spp": n, **m})
+            for k, v in m.items():
+                if v <= TARGET and k not in reached:
+                    reached[k] = {"seconds": round(dev_ms / 1e3, 3), "spp": n}
+            if all(k in reached for k in m if k != "raw"):
                 break
-        if hit is None:
-            mean = acc / max(n, 1)
-            e = terms(mean[::JUDGE_STRIDE, ::JUDGE_STRIDE], judge)
-            hit = {"seconds": None, "spp": n, "device_seconds_spent": round(dev_ms / 1e3, 3),
-                   "relmse_trimmed": trimmed(e), "relmse_raw": float(e.mean())}
-        hit["ms_per_spp"] = round(dev_ms / max(n, 1), 3)
-        return hit
+        mean = acc / max(n, 1)
+        keys = [k for k in curve[-1] if k not in ("seconds", "spp")]
+        out = {"seconds_to_target": {k: (reached[k]["seconds"] if k in reached else None) for k in keys},
+               "spp_to_target": {k: (reached[k]["spp"] if k in reached else None) for k in keys},
+               "device_seconds_spent": round(dev_ms / 1e3, 3), "spp": n, "final": curve[-1],
+               "energy_bias": float(mean[::JUDGE_STRIDE, ::JUDGE_STRIDE].mean() / judge.mean() - 1.0),
+               "ms_per_spp": round(dev_ms / max(n, 1), 3)}
+        # the error curve, thinned to about a dozen points (log-spaced, the last one kept)
+        keep = sorted({int(round(x)) for x in np.geomspace(1, len(curve), 12)} | {len(curve)})
+        out["curve"] = [curve[i - 1] for i in keep]
+        out["seconds"] = out["seconds_to_target"]["trim_0.1%"]  # the headline metric
+        return out
 
     sampler = ClockSampler(device.index or 0)
     sampler.start()
@@ -271,8 +299,18 @@ def cache_race(pb, W, ctx, device):
     speedup = None
     if plain["seconds"] and cached["seconds"]:
         speedup = round(plain["seconds"] / cached["seconds"], 3)
+    per_metric = {}
+    for k, pv in plain["seconds_to_target"].items():
+        cv = cached["seconds_to_target"][k]
+        per_metric[k] = round(pv / cv, 3) if pv and cv else None
     return {
         "metric": "seconds to relMSE 1e-3 (trimmed: 0.1% largest per-pixel terms dropped), cached vs plain PT",
+        "speedup_by_metric": per_metric,
+        "metrics": {"raw": "mean over the judge grid of (x - ref)^2 / (ref^2 + 0.01), nothing dropped",
+                    "trim_0.01% / trim_0.1% / trim_1%": "the same with that fraction of the largest per-pixel "
+                                                          "terms dropped",
+                    "block4": "the same on 4x4-block means of the judge grid (16 pixels 4 apart), nothing dropped",
+                    "target": TARGET},
         "workload": "displaced torus knot (871,414 triangles, glossy/diffuse per face) in the closed box with its "
                     f"area light; {CACHE_W}x{CACHE_H}, max depth {CACHE_DEPTH}",
         "plain": plain, "cached": cached, "speedup_plain_over_cached": speedup,
@@ -298,13 +336,19 @@ RENDER_CASES = {
 }
 
 
-def render_case(pb, W, ctx, case, reps=3, cpu=False, nvtx=False):
+def render_case(pb, W, ctx, case, reps=3, cpu=False, nvtx=False, frame=None, spp=None):
     """Device time of one full render of a path-tracing workload (CUDA events on the
-    context's stream, after one warm-up render), with the rays it traced."""
+    context's stream, after one warm-up render), with the rays it traced. `frame` (w, h) and
+    `spp` shrink the workload for profiling captures (same scene and camera)."""
     import torch
 
     what, make, kw = RENDER_CASES[case]
     desc, cam = make(W)
+    if frame:
+        cam = dict(cam, width=int(frame[0]), height=int(frame[1]))
+        what += f" [reduced: {frame[0]}x{frame[1]}" + (f", {spp} spp]" if spp else "]")
+    if spp:
+        kw = dict(kw, spp=int(spp))
     scene = pb.Scene.from_description(desc, ctx).commit(bvh_bins=desc.get("bvh_bins", 8),
                                                        bvh_max_leaf=desc.get("bvh_max_leaf", 1))
     stream = torch.cuda.current_stream()
@@ -336,13 +380,34 @@ def render_case(pb, W, ctx, case, reps=3, cpu=False, nvtx=False):
         threads = os.cpu_count() or 1
         o = oracle.Scene(desc, np.float32)
         t0 = time.perf_counter()
-        o.render(cam, 1, kw["max_depth"], seed=1, rr_start=kw["rr_start"], threads=threads)
+        _, work = o.render_counted(cam, 1, kw["max_depth"], seed=1, rr_start=kw["rr_start"], threads=threads)
         cs = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": round(cam["width"] * cam["height"] / cs, 1), "unit": "samples/s",
                                "cores": threads, "kind": "port",
                                "sample": "1 spp of the same image, FP32 C++ restatement of the reference's path "
                                          "integrator and scene traversal (oracle), all host threads"}
+        out["roofline"] = render_roofline(work, rays, ms)
     return out
+
+
+def render_roofline(work, gpu_rays, ms):
+    """Traversal roofline of a render: algorithmic bytes per traced ray (extension and shadow
+    rays) = 32 (ray) + 8 (hit) + 32 per box test (top-level and mesh nodes) + 36 per
+    triangle test + 16 per analytic shape test, with the tests per ray counted by the oracle
+    rendering the same image with the same sample streams (1 spp), times the rays the GPU
+    traced per frame, over the GPU's frame time, against the measured HBM copy bandwidth."""
+    peak, peak_kind = _peaks()
+    n = work["rays"] + work["shadow_rays"]
+    boxes = (work["top_boxes"] + work["mesh_boxes"]) / n
+    tris, shapes = work["triangles"] / n, work["shapes"] / n
+    bpr = 32 + 8 + 32 * boxes + 36 * tris + 16 * shapes
+    achieved = bpr * gpu_rays / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
+            "algorithmic_bytes_per_ray": round(bpr, 2), "box_tests_per_ray": round(boxes, 3),
+            "triangle_tests_per_ray": round(tris, 3), "shape_tests_per_ray": round(shapes, 3),
+            "objects_per_ray": round(work["objects"] / n, 3),
+            "counted_by": "oracle render of the same image at 1 spp (same scene, trees and sample streams)"}
 
 
 def batch_race(pb, W, ctx, device):
@@ -384,11 +449,15 @@ def batch_race(pb, W, ctx, device):
     batch.close()
     best = min(frames, key=max)
     frame_ms = max(best)
-    # the same scenes one after another, each its own pbrt_render
+    # the same scenes one after another, each its own pbrt_render, in the batch's order
+    # (cheapest first: pixels x spp x max depth)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     seq = []
-    for sc, p, (_, cam, spp) in zip(scenes, params, specs):
+    cost = [cam["width"] * cam["height"] * spp * 8 for _, cam, spp in specs]
+    order = sorted(range(len(specs)), key=lambda i: (cost[i], i))
+    for i in order:
+        sc, p, (_, cam, spp) = scenes[i], params[i], specs[i]
         film = torch.empty((cam["height"], cam["width"], 3), dtype=torch.float64, device=device)
         sc.render(cam, spp=spp, max_depth=8, seed=p.seed, film=film)  # warm-up (this scene's first launch)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -413,7 +482,8 @@ def batch_race(pb, W, ctx, device):
                     "graph_launches_per_frame": 1},
         "sequential": {"total_ms": round(float(cum[-1]), 2), "samples_per_s": round(samples / (cum[-1] * 1e-3), 1),
                        "scene_latency_ms": {"mean": round(float(np.mean(cum)), 2), "max": round(float(cum[-1]), 2)},
-                       "note": "same scenes and tuning, one pbrt_render each (launches not captured)"},
+                       "note": "same scenes, tuning and order (cheapest first), one pbrt_render each "
+                               "(launches not captured)"},
         "speedup_aggregate": round(cum[-1] / frame_ms, 3),
         "tuning": {k: tune[k] for k in ("leaf", "wave_paths", "trace_threads", "trace_blocks_per_sm",
                                           "shade_threads", "shade_blocks_per_sm")},
@@ -423,6 +493,54 @@ def batch_race(pb, W, ctx, device):
                     "note": "host: BVHs on all host cores (pbrt_scene_create_many); gpu: device_build, the "
                             "same trees; both include the uploads"},
     }
+
+
+def batch_small(pb, W, ctx, device, n=64, width=128, height=128):
+    """Where batching is meant to pay: n small scenes (displaced icosphere of level U{3..6} in
+    the closed box, 128x128, U{2..8} spp, max depth 8: 33K-131K paths each, far fewer than one
+    B200 keeps in flight) rendered as one graph frame against one pbrt_render each in the same
+    order (cheapest first); device time of both (CUDA events), per-scene completion times."""
+    import torch
+    from pbrt_b200.scene import Batch, create_scenes, render_params
+
+    specs = W.batch_scenes(n, seed=5, width=width, height=height, levels=(3, 6), spp=(2, 8))
+    scenes = create_scenes([d for d, _, _ in specs], ctx)
+    params = [render_params(cam, spp, 8, seed=200 + i) for i, (_, cam, spp) in enumerate(specs)]
+    samples = sum(cam["width"] * cam["height"] * spp for _, cam, spp in specs)
+    batch = Batch(scenes, params, ctx)
+    none = [None] * len(scenes)
+    batch.render(0, none)
+    frames = [batch.render(f, none, scene_times=True)[1] for f in (1, 2)]
+    batch.close()
+    best = min(frames, key=max)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    cost = [cam["width"] * cam["height"] * spp * 8 for _, cam, spp in specs]
+    order = sorted(range(len(specs)), key=lambda i: (cost[i], i))
+    films = [torch.empty((cam["height"], cam["width"], 3), dtype=torch.float64, device=device) for _, cam, _ in specs]
+    for i in order:  # warm-up: every scene once
+        scenes[i].render(specs[i][1], spp=specs[i][2], max_depth=8, seed=params[i].seed, film=films[i])
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(order) + 1)]
+    ev[0].record(stream)
+    for k, i in enumerate(order):
+        scenes[i].render(specs[i][1], spp=specs[i][2], max_depth=8, seed=params[i].seed, film=films[i])
+        ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    done = [ev[0].elapsed_time(e) for e in ev[1:]]
+    ctx.set_stream(None)
+    for sc in scenes:
+        sc.release()
+    total = done[-1]
+    return {"workload": f"{n} scenes: displaced icosphere level U{{3..6}} in the closed box, {width}x{height}, "
+                        "U{2..8} spp, max depth 8 (seeded)",
+            "samples_per_frame": samples,
+            "batched": {"frame_ms": round(max(best), 3), "samples_per_s": round(samples / (max(best) * 1e-3), 1),
+                        "scene_latency_ms": {"mean": round(float(np.mean(best)), 3), "max": round(float(max(best)), 3)}},
+            "sequential": {"total_ms": round(total, 3), "samples_per_s": round(samples / (total * 1e-3), 1),
+                           "scene_latency_ms": {"mean": round(float(np.mean(done)), 3), "max": round(total, 3)},
+                           "note": "one pbrt_render each, cheapest first, back to back on one stream"},
+            "speedup_aggregate": round(total / max(best), 3),
+            "speedup_mean_latency": round(float(np.mean(done)) / float(np.mean(best)), 3)}
 
 
 MLP_FLOP_PER_QUERY = 2 * (96 * 64 + 4 * 64 * 64 + 64 * 3)  # 45,440: forward multiply-adds x 2
@@ -579,10 +697,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cache-race", action="store_true")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays per step (smaller cases for profiling)")
-    ap.add_argument("--workload", default="raycast", choices=["raycast", "mlp", "render", "batch"],
+    ap.add_argument("--workload", default="raycast", choices=["raycast", "mlp", "render", "batch", "cache"],
                     help="mlp: the radiance cache's network alone; render: one path-tracing case (--case); "
                          "neither is the headline line")
     ap.add_argument("--case", default="c0", choices=sorted(RENDER_CASES))
+    ap.add_argument("--frame", default=None, help="WxH: a reduced frame for --workload render (profiling)")
+    ap.add_argument("--spp", type=int, default=None, help="samples per pixel for --workload render (profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = _dist()
@@ -597,7 +717,19 @@ def main():
         from pbrt_b200 import workloads as W
 
         torch.cuda.set_device(local)
-        print(json.dumps(batch_race(pb, W, pb.Context(local), torch.device("cuda", local))), flush=True)
+        ctx = pb.Context(local)
+        res = batch_race(pb, W, ctx, torch.device("cuda", local))
+        res["small_scenes"] = batch_small(pb, W, ctx, torch.device("cuda", local))
+        print(json.dumps(res), flush=True)
+        return
+    if args.workload == "cache":
+        import torch
+
+        import pbrt_b200 as pb
+        from pbrt_b200 import workloads as W
+
+        torch.cuda.set_device(local)
+        print(json.dumps(cache_race(pb, W, pb.Context(local), torch.device("cuda", local))), flush=True)
         return
     if args.workload == "render":
         import torch
@@ -606,7 +738,9 @@ def main():
         from pbrt_b200 import workloads as W
 
         torch.cuda.set_device(local)
-        res = render_case(pb, W, pb.Context(local), args.case, reps=max(1, args.steps), nvtx=True)
+        frame = tuple(int(x) for x in args.frame.split("x")) if args.frame else None
+        res = render_case(pb, W, pb.Context(local), args.case, reps=max(1, args.steps), nvtx=True, frame=frame,
+                          spp=args.spp)
         print(json.dumps({"metric": f"path tracing {args.case}", **res}), flush=True)
         return
 
@@ -730,9 +864,10 @@ def main():
             "clocks": clocks,
         }
         if ws == 1 and not args.no_cache_race:
-            line["renders"] = {c: render_case(pb, W, ctx, c, cpu=not args.no_cpu_baseline) for c in ("c0", "c2")}
+            line["renders"] = {c: render_case(pb, W, ctx, c, cpu=not args.no_cpu_baseline) for c in ("c0", "c2", "c4")}
             line["cache"] = cache_race(pb, W, ctx, rays_d.device)
             line["batch"] = batch_race(pb, W, ctx, rays_d.device)
+            line["batch"]["small_scenes"] = batch_small(pb, W, ctx, rays_d.device)
         if ws == 1 and not args.no_cpu_baseline:
             import oracle
 
