@@ -10,10 +10,12 @@
 // resident in shared memory for the CTA's lifetime.
 //
 // Training: the same forward keeps every layer's activations; the loss gradient dO is
-// written as a BF16 tile; for each layer the data gradient dA = G·W runs on the tensor cores
-// (W transposed in its own pack) while the weight gradient dW = Gᵀ·A runs on the CUDA
-// cores from the same shared-memory tiles; per-tile partial gradients are reduced by a
-// second kernel and Adam updates the FP32 master weights and rewrites both BF16 packs.
+// written as a BF16 tile; for each layer both products run on the tensor cores, issued back
+// to back and committed once: the data gradient dA = G·W (W transposed in its own pack) and
+// the weight gradient dW = Gᵀ·A, which reduces over the tile's 128 samples by reading the
+// resident G and A tiles as MN-major operands (M = 64; the output layer's 16-row dW is
+// formed transposed, dWᵀ = Aᵀ·G). Per-tile partial gradients are reduced by a second kernel
+// and Adam updates the FP32 master weights and rewrites both BF16 packs.
 #include <cuda_bf16.h>
 
 #include <atomic>
@@ -30,7 +32,9 @@ constexpr uint32_t kWBytes = kParams * 2;           // 47,104
 constexpr uint32_t kXBytes = kTile * kInPad * 2;    // 24,576
 constexpr uint32_t kHBytes = kTile * kHidden * 2;   // 16,384
 constexpr uint32_t kG16Bytes = kTile * kOutPad * 2;  // 4,096
-constexpr uint32_t kTmemCols = 64;
+constexpr uint32_t kTmemCols = 64;       // one 64-column accumulator
+constexpr uint32_t kTrainTmemCols = 256;  // training: dA in columns 0-63, dW from column 64 (up to 96 wide)
+constexpr uint32_t kWgradCol = 64;
 static_assert(kXBytes >= kHBytes, "the inference kernel stores the hidden tile over the input tile");
 
 __device__ __forceinline__ uint16_t to_bf16(float f) { return __bfloat16_as_ushort(__float2bfloat16_rn(f)); }
@@ -83,6 +87,7 @@ __device__ __forceinline__ float tile_at(const uint8_t* tile, uint32_t r, uint32
 }
 
 // D[128 x n] = A[128 x k] · B[n x k]^T, both K-major in the core-matrix layout; thread 0 only.
+// Commits to mbar unless mbar is null.
 __device__ __forceinline__ void issue_gemm(const uint8_t* a, const uint8_t* b, uint32_t n, uint32_t k, uint32_t tmem,
                                            uint64_t* mbar) {
   const uint32_t a_addr = tc::smem_u32(a), b_addr = tc::smem_u32(b);
@@ -90,6 +95,22 @@ __device__ __forceinline__ void issue_gemm(const uint8_t* a, const uint8_t* b, u
   const uint32_t idesc = tc::idesc_bf16(kTile, n);
   for (uint32_t s = 0; s < k / 16; ++s)
     tc::mma_bf16(tmem, tc::make_desc(a_addr + s * 2 * lbo_a, lbo_a, 128), tc::make_desc(b_addr + s * 2 * lbo_b, lbo_b, 128),
+                 idesc, s > 0 ? 1u : 0u);
+  if (mbar) tc::mma_commit(mbar);  // null: a later issue commits both
+}
+
+// D[64 x n] = P^T · Q over the 128 samples of two resident 128-row tiles: the 64 columns of P
+// become D's rows, the n columns of Q its columns, and the tiles' row (sample) index is the
+// reduction. Both tiles are read MN-major (SBO = 16 core matrices down the tile = 2048 bytes
+// between 8-column blocks, LBO = 128 bytes between 8-sample blocks); K steps of 16 samples
+// advance 256 bytes. Thread 0 only; commits to mbar.
+__device__ __forceinline__ void issue_gemm_tn(const uint8_t* p, const uint8_t* q, uint32_t n, uint32_t tmem,
+                                              uint64_t* mbar) {
+  const uint32_t p_addr = tc::smem_u32(p), q_addr = tc::smem_u32(q);
+  constexpr uint32_t sbo = (kTile / 8) * 128, lbo = 128;
+  const uint32_t idesc = tc::idesc_bf16_mn(64, n);
+  for (uint32_t s = 0; s < kTile / 16; ++s)
+    tc::mma_bf16(tmem, tc::make_desc(p_addr + s * 2 * lbo, lbo, sbo), tc::make_desc(q_addr + s * 2 * lbo, lbo, sbo),
                  idesc, s > 0 ? 1u : 0u);
   tc::mma_commit(mbar);
 }
@@ -117,10 +138,10 @@ __device__ __forceinline__ void load_smem(uint8_t* dst, const uint16_t* src, uin
   for (uint32_t i = threadIdx.x; i < bytes / 16; i += blockDim.x) d[i] = __ldg(s + i);
 }
 
-__device__ __forceinline__ void setup_tmem(uint64_t* mbar, uint32_t* tslot) {
+__device__ __forceinline__ void setup_tmem(uint64_t* mbar, uint32_t* tslot, uint32_t ncols = kTmemCols) {
   if (threadIdx.x == 0) tc::mbar_init(mbar, 1);
   if ((threadIdx.x >> 5) == 0) {
-    tc::tmem_alloc(tslot, kTmemCols);
+    tc::tmem_alloc(tslot, ncols);
     tc::tmem_relinquish();
   }
   tc::fence_before_sync();
@@ -128,11 +149,12 @@ __device__ __forceinline__ void setup_tmem(uint64_t* mbar, uint32_t* tslot) {
   tc::fence_after_sync();
 }
 
-__device__ __forceinline__ void release_tmem(uint32_t tmem, uint64_t* mbar, uint32_t phase, bool ok) {
+__device__ __forceinline__ void release_tmem(uint32_t tmem, uint64_t* mbar, uint32_t phase, bool ok,
+                                             uint32_t ncols = kTmemCols) {
   if (!ok) tc::mbar_wait(mbar, phase, 1u << 20);  // one more bounded wait for a GEMM still in flight
   tc::fence_before_sync();
   __syncthreads();
-  if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(tmem, kTmemCols);
+  if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(tmem, ncols);
 }
 
 // Three CTAs per SM (shared memory: the weights and one activation tile each; TMEM: 64 columns
@@ -220,7 +242,7 @@ __global__ void __launch_bounds__(kTile, 1) k_mlp_grad(Net net, Bounds b, const 
   load_smem(sWf, net.wpk_fwd, kWBytes);
   load_smem(sWb, net.wpk_bwd, kWBytes);
   if (threadIdx.x == 0) *s_loss = 0.f;
-  setup_tmem(mbar, tslot);
+  setup_tmem(mbar, tslot, kTrainTmemCols);
   const uint32_t tmem = *tslot;
   uint32_t phase = 0;
   bool ok = true;
@@ -288,48 +310,58 @@ __global__ void __launch_bounds__(kTile, 1) k_mlp_grad(Net net, Bounds b, const 
     __syncthreads();
   }
   // backward
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t quarter = (warp * 32u) << 16;  // this warp's TMEM lanes
   for (int l = kLayers - 1; l >= 0 && ok; --l) {
     const int N = layer_n(l), K = layer_k(l);
     const uint8_t* G = (l == kLayers - 1) ? sG16 : sG;
     const uint8_t* A = act(l);
-    if (l > 0 && threadIdx.x == 0) {  // dA_l = G_l · W_l on the tensor cores, (128 x K) with K = 64
+    if (threadIdx.x == 0) {
       tc::fence_after_sync();
-      issue_gemm(G, sWb + 2 * layer_off(l), uint32_t(K), uint32_t(N), tmem, mbar);
+      // dA_l = G_l · W_l, (128 x K) with K = 64, into columns 0-63
+      if (l > 0) issue_gemm(G, sWb + 2 * layer_off(l), uint32_t(K), uint32_t(N), tmem, nullptr);
+      // dW_l = G_lᵀ · A_l (64 x K), or for the 16-row output layer dW_lᵀ = A_lᵀ · G_l (64 x 16)
+      if (l < kLayers - 1)
+        issue_gemm_tn(G, A, uint32_t(K), tmem + kWgradCol, mbar);
+      else
+        issue_gemm_tn(A, G, uint32_t(N), tmem + kWgradCol, mbar);
     }
-    // dW_l = G_lᵀ · A_l on the CUDA cores: thread t owns outputs o in [o0, o0 + ob), i in [i0, i0 + ib)
+    ok = wait_gemm(mbar, phase, err);
+    if (!ok) break;
     {
-      const int groups_o = 16, groups_i = 8;  // 128 threads
-      const int ob = N / groups_o, ib = K / groups_i;
-      const int o0 = (threadIdx.x / groups_i) * ob, i0 = (threadIdx.x % groups_i) * ib;
-      float acc[4 * 12];
-      for (int j = 0; j < ob * ib; ++j) acc[j] = 0.f;
-      for (int bb = 0; bb < kTile; ++bb) {
-        float gv[4], av[12];
-        for (int j = 0; j < ob; ++j) gv[j] = tile_at(G, uint32_t(bb), uint32_t(o0 + j), kTile);
-        for (int k = 0; k < ib; ++k) av[k] = tile_at(A, uint32_t(bb), uint32_t(i0 + k), kTile);
-        for (int j = 0; j < ob; ++j)
-          for (int k = 0; k < ib; ++k) acc[j * ib + k] += gv[j] * av[k];
-      }
+      // M = 64 accumulator: lanes 0-15 of warp q hold rows 16q .. 16q + 15
+      const uint32_t row = warp * 16u + lane;
       float* dst = partials + tile * uint64_t(kParams) + layer_off(l);
-      for (int j = 0; j < ob; ++j)
-        for (int k = 0; k < ib; ++k) dst[(o0 + j) * K + (i0 + k)] = acc[j * ib + k];
+      const int cols = l < kLayers - 1 ? K : N;
+      for (int c = 0; c < cols; c += 16) {
+        float v[16];
+        tc::tmem_ld16(tmem + quarter + kWgradCol + uint32_t(c), v);
+        if (lane < 16) {
+          if (l < kLayers - 1) {  // row = output unit o, columns = inputs i
+#pragma unroll
+            for (int j = 0; j < 16; j += 4)
+              *reinterpret_cast<float4*>(dst + row * uint32_t(K) + uint32_t(c + j)) =
+                  make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+          } else {  // transposed: row = input i, columns = outputs o
+#pragma unroll
+            for (int j = 0; j < 16; ++j) dst[uint32_t(c + j) * uint32_t(K) + row] = v[j];
+          }
+        }
+      }
     }
-    __syncthreads();  // every thread is done reading G_l
     if (l > 0) {
-      ok = wait_gemm(mbar, phase, err);
-      if (!ok) break;
       float v[64];
       read_acc64(tmem, v);
 #pragma unroll
       for (int c = 0; c < 64; ++c) v[c] = tile_at(A, r, uint32_t(c), kTile) > 0.f ? v[c] : 0.f;
       store_row(sG, r, v, 64);
-      tc::fence_before_sync();
       tc::fence_smem_to_async();
-      __syncthreads();
     }
+    tc::fence_before_sync();
+    __syncthreads();
   }
   if (threadIdx.x == 0) tile_loss[tile] = *s_loss;
-  release_tmem(tmem, mbar, phase, ok);
+  release_tmem(tmem, mbar, phase, ok, kTrainTmemCols);
 }
 
 __global__ void k_reduce(const float* __restrict__ partials, const float* __restrict__ tile_loss, uint32_t tiles,

@@ -40,6 +40,16 @@ __device__ __forceinline__ uint64_t make_desc(uint32_t smem_addr, uint32_t lbo_b
 __host__ __device__ constexpr uint32_t idesc_bf16(uint32_t m, uint32_t n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
 }
+// The same with both operands MN-major (bit 15: A, bit 16: B). An MN-major operand without
+// swizzle is built of the same 128-byte core matrices, read the other way round: 8 MN-
+// consecutive elements per 16-byte row, 8 rows = 8 consecutive K; the descriptor's SBO is then
+// the step between 8-element MN blocks and its LBO the step between 8-deep K blocks. So an
+// R-row K-major tile of the layout above (element (r, c) at tile_offset(r, c, R)) is also
+// the MN-major operand whose MN index is c and whose K index is r, with SBO = R/8 * 128 and
+// LBO = 128: a product over the tile's rows needs no transposed copy.
+__host__ __device__ constexpr uint32_t idesc_bf16_mn(uint32_t m, uint32_t n) {
+  return idesc_bf16(m, n) | (1u << 15) | (1u << 16);
+}
 
 __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                          uint32_t accumulate) {
@@ -95,7 +105,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint3
 }
 
 // 16 consecutive FP32 columns of this thread's TMEM lane (32x32b shape: the warp reads its
-// own 32-lane quarter, lane = warp_quarter * 32 + lane id). The wait sits in the same asm
+// own 32-lane quarter, lane = warp_quarter * 32 + lane id). An M = 128 accumulator has row r
+// in lane r; an M = 64 one (one CTA) has row 16q + j in lane 32q + j (j < 16), so lanes 0-15
+// of warp q hold rows 16q .. 16q + 15. The wait sits in the same asm
 // statement, so no use of the registers can be scheduled before the data has arrived.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   uint32_t r[16];
