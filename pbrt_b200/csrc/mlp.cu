@@ -157,72 +157,163 @@ __device__ __forceinline__ void release_tmem(uint32_t tmem, uint64_t* mbar, uint
   if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(tmem, ncols);
 }
 
-// Three CTAs per SM (shared memory: the weights and one activation tile each; TMEM: 64 columns
-// each): while one CTA waits on its GEMM, the others encode, read TMEM or store activations.
-constexpr int kInferCtasPerSm = 3;
+// Inference: one CTA per SM holds the weights once and runs kInferGroups independent tile
+// groups of 128 threads (four warps), each with its own activation tile, mbarrier, named
+// barrier and 64 TMEM columns, so six tiles' GEMM chains are in flight per SM: while one
+// group waits on its GEMM the others encode, read TMEM or store activations. (Three CTAs of
+// one tile each, every CTA with its own copy of the weights, was the shared-memory limit.)
+constexpr int kInferGroups = 6;
+constexpr int kInferThreads = kInferGroups * kTile;  // 768
+constexpr uint32_t kInferTmemCols = 512;             // 6 x 64 columns, rounded up to a power of two
+static_assert(kInferGroups * kTmemCols <= kInferTmemCols, "the groups' accumulators must fit the allocation");
 
-__global__ void __launch_bounds__(kTile, kInferCtasPerSm) k_mlp_infer(Net net, Bounds b, const float* __restrict__ rec, uint64_t n,
-                                                         const uint32_t* __restrict__ n_dev, float* __restrict__ out,
-                                                         uint32_t* err) {
+// Named barrier g + 1 over the 128 threads of tile group g (barrier 0 is __syncthreads).
+__device__ __forceinline__ void group_sync(uint32_t g) {
+  asm volatile("bar.sync %0, %1;" ::"r"(g + 1u), "r"(uint32_t(kTile)) : "memory");
+}
+// The same barrier, returning whether `v` holds in every thread of the group.
+__device__ __forceinline__ bool group_and(uint32_t g, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, %3, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"(uint32_t(v)), "r"(g + 1u), "r"(uint32_t(kTile))
+      : "memory");
+  return r != 0;
+}
+
+__global__ void __launch_bounds__(kInferThreads, 1) k_mlp_infer(Net net, Bounds b, const float* __restrict__ rec,
+                                                                uint64_t n, const uint32_t* __restrict__ n_dev,
+                                                                float* __restrict__ out, uint32_t* err) {
   if (n_dev) n = min(n, uint64_t(*n_dev));  // a count the previous kernel left on the device
-  if (uint64_t(blockIdx.x) * kTile >= n) return;  // before any barrier or TMEM allocation
+  if (uint64_t(blockIdx.x) * kInferGroups * kTile >= n) return;  // before any barrier or TMEM allocation
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* sW = smem;
-  uint8_t* sX = sW + kWBytes;
-  // The hidden activations overwrite the input tile: a layer's GEMM has finished reading its
-  // A operand (wait_gemm) before any thread stores the next layer's, and the next tile's
-  // features are stored only after the last layer's GEMM has completed.
-  uint8_t* sH = sX;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(sX + kXBytes);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+  const uint32_t g = threadIdx.x / kTile, r = threadIdx.x % kTile;
+  // The group's tile: the hidden activations overwrite the input features (a layer's GEMM has
+  // finished reading its A operand before any thread stores the next layer's, and the next
+  // tile's features are stored only after the last layer's GEMM has completed).
+  uint8_t* sX = sW + kWBytes + g * kXBytes;
+  uint64_t* mbars = reinterpret_cast<uint64_t*>(sW + kWBytes + kInferGroups * kXBytes);
+  uint64_t* mbar = mbars + g;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbars + kInferGroups);
   load_smem(sW, net.wpk_fwd, kWBytes);
-  setup_tmem(mbar, tslot);
-  const uint32_t tmem = *tslot;
+  if (r == 0) tc::mbar_init(mbar, 1);
+  if (threadIdx.x < 32) {
+    tc::tmem_alloc(tslot, kInferTmemCols);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tslot + g * kTmemCols;                // this group's 64 columns
+  const uint32_t lane_base = ((threadIdx.x >> 5) & 3u) * 32u;  // this warp's TMEM lanes = rows
   uint32_t phase = 0;
   bool ok = true;
   const uint64_t tiles = (n + kTile - 1) / kTile;
-  for (uint64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-    const uint64_t row = tile * kTile + threadIdx.x;
-    float f[kInPad];
-    if (row < n) {
-      encode(rec + row * kRecord, b, f);
-    } else {
-#pragma unroll
-      for (int k = 0; k < kInPad; ++k) f[k] = 0.f;
-    }
-    store_row(sX, threadIdx.x, f, kInPad);
-    tc::fence_smem_to_async();
-    __syncthreads();
-    for (int l = 0; l < kLayers && ok; ++l) {
-      if (threadIdx.x == 0) {
-        tc::fence_after_sync();
-        issue_gemm(l == 0 ? sX : sH, sW + 2 * layer_off(l), uint32_t(layer_n(l)), uint32_t(layer_k(l)), tmem, mbar);
+  for (uint64_t tile = uint64_t(blockIdx.x) * kInferGroups + g; tile < tiles && ok;
+       tile += uint64_t(gridDim.x) * kInferGroups) {
+    const uint64_t row = tile * kTile + r;
+    {
+      // encode(): the features in 8-column chunks, 3 axes x 3 chunks of sin/cos bands, then the
+      // 10 record values, without a 96-value array in registers
+      float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = q0, q2 = q0, q3 = q0;
+      const bool valid = row < n;
+      if (valid) {
+        const float4* qr = reinterpret_cast<const float4*>(rec + row * kRecord);
+        q0 = __ldg(qr);
+        q1 = __ldg(qr + 1);
+        q2 = __ldg(qr + 2);
+        q3 = __ldg(qr + 3);
       }
-      ok = wait_gemm(mbar, phase, err);
-      if (!ok) break;
-      if (l < kLayers - 1) {
-        float v[64];
-        read_acc64(tmem, v);
+      const float p[3] = {q0.x, q0.y, q0.z};
 #pragma unroll
-        for (int c = 0; c < 64; ++c) v[c] = fmaxf(v[c], 0.f);
-        store_row(sH, threadIdx.x, v, 64);
+      for (int a = 0; a < 3; ++a) {
+        float x = (p[a] - b.lo[a]) * b.inv_extent[a];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float v[8];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            float sn, cs;
+            sincospif(x, &sn, &cs);
+            v[2 * j] = valid ? sn : 0.f;
+            v[2 * j + 1] = valid ? cs : 0.f;
+            x = x * 2.0f;
+          }
+          uint4 qq;
+          qq.x = pack2(v[0], v[1]);
+          qq.y = pack2(v[2], v[3]);
+          qq.z = pack2(v[4], v[5]);
+          qq.w = pack2(v[6], v[7]);
+          *reinterpret_cast<uint4*>(sX + tc::tile_offset(r, uint32_t(a * 24 + c * 8), kTile)) = qq;
+        }
+      }
+      uint4 qa, qb;
+      const uint4 qz = make_uint4(0u, 0u, 0u, 0u);
+      qa.x = pack2(q1.x, q1.y);
+      qa.y = pack2(q1.z, q2.x);
+      qa.z = pack2(q2.y, q2.z);
+      qa.w = pack2(q3.x, q3.y);
+      qb.x = pack2(q3.z, q0.w);
+      qb.y = 0u;
+      qb.z = 0u;
+      qb.w = 0u;
+      *reinterpret_cast<uint4*>(sX + tc::tile_offset(r, 72u, kTile)) = qa;
+      *reinterpret_cast<uint4*>(sX + tc::tile_offset(r, 80u, kTile)) = qb;
+      *reinterpret_cast<uint4*>(sX + tc::tile_offset(r, 88u, kTile)) = qz;
+    }
+    tc::fence_smem_to_async();
+    group_sync(g);
+    for (int l = 0; l < kLayers && ok; ++l) {
+      if (r == 0) {
+        tc::fence_after_sync();
+        issue_gemm(sX, sW + 2 * layer_off(l), uint32_t(layer_n(l)), uint32_t(layer_k(l)), tmem, mbar);
+      }
+      ok = group_and(g, tc::mbar_wait(mbar, phase));
+      if (!ok) {
+        if (r == 0) atomicOr(err, kErrMma);
+        break;
+      }
+      phase ^= 1u;
+      tc::fence_after_sync();
+      if (l < kLayers - 1) {
+#pragma unroll
+        for (int c = 0; c < 64; c += 16) {
+          float v[16];
+          tc::tmem_ld16(tmem + (lane_base << 16) + uint32_t(c), v);
+          uint4 lo, hi;
+          lo.x = pack2(fmaxf(v[0], 0.f), fmaxf(v[1], 0.f));
+          lo.y = pack2(fmaxf(v[2], 0.f), fmaxf(v[3], 0.f));
+          lo.z = pack2(fmaxf(v[4], 0.f), fmaxf(v[5], 0.f));
+          lo.w = pack2(fmaxf(v[6], 0.f), fmaxf(v[7], 0.f));
+          hi.x = pack2(fmaxf(v[8], 0.f), fmaxf(v[9], 0.f));
+          hi.y = pack2(fmaxf(v[10], 0.f), fmaxf(v[11], 0.f));
+          hi.z = pack2(fmaxf(v[12], 0.f), fmaxf(v[13], 0.f));
+          hi.w = pack2(fmaxf(v[14], 0.f), fmaxf(v[15], 0.f));
+          *reinterpret_cast<uint4*>(sX + tc::tile_offset(r, uint32_t(c), kTile)) = lo;
+          *reinterpret_cast<uint4*>(sX + tc::tile_offset(r, uint32_t(c + 8), kTile)) = hi;
+        }
         tc::fence_before_sync();
         tc::fence_smem_to_async();
-        __syncthreads();
+        group_sync(g);
       } else {
         float v[16];
-        tc::tmem_ld16(tmem + (((threadIdx.x >> 5) * 32u) << 16), v);
+        tc::tmem_ld16(tmem + (lane_base << 16), v);
         if (row < n) {
           out[3 * row] = v[0];
           out[3 * row + 1] = v[1];
           out[3 * row + 2] = v[2];
         }
         tc::fence_before_sync();
-        __syncthreads();
+        group_sync(g);
       }
     }
   }
-  release_tmem(tmem, mbar, phase, ok);
+  if (!ok) tc::mbar_wait(mbar, phase, 1u << 20);  // one more bounded wait for a GEMM still in flight
+  tc::fence_before_sync();
+  __syncthreads();
+  if (threadIdx.x < 32) tc::tmem_dealloc(*tslot, kInferTmemCols);
 }
 
 __global__ void __launch_bounds__(kTile, 1) k_mlp_grad(Net net, Bounds b, const float* __restrict__ rec,
@@ -413,7 +504,7 @@ __global__ void k_pack(const float* __restrict__ w, uint16_t* fwd, uint16_t* bwd
   if (p < uint32_t(kParams)) pack_one(p, w[p], fwd, bwd);
 }
 
-size_t infer_smem_bytes() { return kWBytes + kXBytes + 64; }
+size_t infer_smem_bytes() { return kWBytes + kInferGroups * kXBytes + kInferGroups * 8 + 16; }
 size_t train_smem_bytes() { return 2 * kWBytes + kXBytes + 5 * kHBytes + kHBytes + kG16Bytes + 64; }
 
 cudaError_t launch_infer(const Net& net, const Bounds& b, const float* records, uint64_t n, float* out, uint32_t* err,
@@ -440,10 +531,10 @@ cudaError_t launch_infer_dev(const Net& net, const Bounds& b, const float* recor
   static std::atomic<uint64_t> configured{0};
   cudaError_t e = allow_smem(configured, reinterpret_cast<const void*>(k_mlp_infer), infer_smem_bytes());
   if (e != cudaSuccess) return e;
-  const uint64_t tiles = (n + kTile - 1) / kTile;
-  const uint64_t cap = uint64_t(sm_count) * kInferCtasPerSm;
-  k_mlp_infer<<<unsigned(tiles < cap ? tiles : cap), kTile, infer_smem_bytes(), s>>>(net, b, records, n, n_dev, out,
-                                                                                     err);
+  const uint64_t ctas = (n + uint64_t(kInferGroups) * kTile - 1) / (uint64_t(kInferGroups) * kTile);
+  const uint64_t cap = uint64_t(sm_count);  // one CTA (six tile groups) per SM
+  k_mlp_infer<<<unsigned(ctas < cap ? ctas : cap), kInferThreads, infer_smem_bytes(), s>>>(net, b, records, n, n_dev,
+                                                                                           out, err);
   return cudaGetLastError();
 }
 
