@@ -280,6 +280,7 @@ def cache_race(pb, W, ctx, device):
         # the error curve, thinned to about a dozen points (log-spaced, the last one kept)
         keep = sorted({int(round(x)) for x in np.geomspace(1, len(curve), 12)} | {len(curve)})
         out["curve"] = [curve[i - 1] for i in keep]
+        out["_curve"] = curve  # every frame, for the comparisons below (not printed)
         out["seconds"] = out["seconds_to_target"]["trim_0.1%"]  # the headline metric
         return out
 
@@ -303,9 +304,22 @@ def cache_race(pb, W, ctx, device):
     for k, pv in plain["seconds_to_target"].items():
         cv = cached["seconds_to_target"][k]
         per_metric[k] = round(pv / cv, 3) if pv and cv else None
+    # Raw relMSE (no sample dropped) compared without a fixed target: both arms at the cached
+    # arm's last time, and the plain arm's time to first match the cached arm's final error.
+    pc, cc = plain.pop("_curve"), cached.pop("_curve")
+    t_c, raw_c = cc[-1]["seconds"], cc[-1]["raw"]
+    at_t = [e for e in pc if e["seconds"] <= t_c]
+    match = next((e for e in pc if e["raw"] <= raw_c), None)
+    raw_cmp = {"cached_seconds": t_c, "cached_raw": raw_c,
+               "plain_raw_at_same_seconds": at_t[-1]["raw"] if at_t else None,
+               "plain_seconds_to_cached_raw": match["seconds"] if match else None,
+               "plain_seconds_spent": pc[-1]["seconds"], "plain_final_raw": pc[-1]["raw"],
+               "time_ratio": round(match["seconds"] / t_c, 3) if match else
+               f"> {round(pc[-1]['seconds'] / t_c, 2)} (the plain arm never reached it)"}
     return {
         "metric": "seconds to relMSE 1e-3 (trimmed: 0.1% largest per-pixel terms dropped), cached vs plain PT",
         "speedup_by_metric": per_metric,
+        "raw_comparison": raw_cmp,
         "metrics": {"raw": "mean over the judge grid of (x - ref)^2 / (ref^2 + 0.01), nothing dropped",
                     "trim_0.01% / trim_0.1% / trim_1%": "the same with that fraction of the largest per-pixel "
                                                           "terms dropped",

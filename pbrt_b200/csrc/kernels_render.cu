@@ -1065,14 +1065,27 @@ cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, 
     top_nodes = top_nodes > host_table[i].view.top_node_count ? top_nodes : host_table[i].view.top_node_count;
     csg = csg || host_table[i].view.has_csg;
   }
-  uint32_t next_done = 0;
+  uint32_t next_done = 0, first = 0;
   for (unsigned long long base = 0; base < total; base += wave) {
     const uint32_t n = uint32_t(total - base < wave ? total - base : wave);
+    // the scenes holding the wave's first and last paths (the table is in path order)
+    while (host_table[first].begin + (unsigned long long)host_table[first].npix * host_table[first].spp <= base) ++first;
+    uint32_t last = first;
+    while (last + 1 < nscenes && host_table[last + 1].begin < base + n) ++last;
     k_generate_batch<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, table, nscenes, base, n, frame, stats);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = bounce_loop(w, src, CacheWave{}, max_depth, any_path_integrator, kCacheOff, 0, shape, stats, err, sm_count,
-                         st, top_nodes, csg)) != cudaSuccess)
-      return e;
+    if (first == last) {
+      // a wave of one scene runs the single-scene kernels: its view is a kernel parameter
+      // instead of a per-path table lookup, and the bounce loop stops at its own depth
+      const BatchScene& h = host_table[first];
+      const OneScene one{h.view, PathSettings{h.max_depth, h.rr_start, h.integrator, h.cam.near, h.cam.far}};
+      e = bounce_loop(w, one, CacheWave{}, h.max_depth, !h.integrator, kCacheOff, 0, shape, stats, err, sm_count, st,
+                      h.view.top_node_count, h.view.has_csg != 0);
+    } else {
+      e = bounce_loop(w, src, CacheWave{}, max_depth, any_path_integrator, kCacheOff, 0, shape, stats, err, sm_count,
+                      st, top_nodes, csg);
+    }
+    if (e != cudaSuccess) return e;
     k_accumulate_batch<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, n, table);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // scenes whose last path was in this wave are done
