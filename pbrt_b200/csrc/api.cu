@@ -162,6 +162,8 @@ int pbrt_ctx_sync(pbrt_ctx* c) {
 
 namespace {
 
+constexpr uint64_t kDeferMinTriangles = 4096;
+
 // The device half of scene creation: checks the built structure, uploads it, fills the view.
 // Meshes listed in `dev` (non-null nodes) were built on the GPU: their arrays are taken over.
 int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbrt_scene** out,
@@ -264,6 +266,20 @@ int upload_scene(pbrt_ctx* c, const pbrt_scene_desc* d, const FlatScene& fs, pbr
   v.light_cdf = (const float*)lcdf;
   v.has_csg = 0;
   for (const ObjRec& ob : fs.objects) v.has_csg |= ob.shape == kShapeCsg ? 1u : 0u;
+  // The leaf the renderer answers in passes of its own: the largest untransformed mesh placed
+  // directly in the top-level tree, of at least kDeferMinTriangles triangles.
+  v.defer_leaf = kNoLeaf;
+  uint64_t defer_tris = kDeferMinTriangles - 1;
+  for (const uint32_t ref : fs.order) {
+    if (ref & kGroupBit) continue;
+    const ObjRec& ob = fs.objects[ref];
+    if (ob.shape != kShapeMesh || ob.xf_count != 0) continue;
+    const uint64_t nt = d->meshes[ob.mesh].triangle_count;
+    if (nt > defer_tris) {
+      defer_tris = nt;
+      v.defer_leaf = ref;
+    }
+  }
   s->info.object_count = fs.primitive_count;
   s->info.device_bytes += s->extra_bytes;
   s->max_radiance = fs.max_radiance;

@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(256) k_generate_batch(WaveBuffers w, const Bat
 template <class Src, bool kCsg>
 __global__ void __launch_bounds__(256, 4) k_extend(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
                                                 const uint32_t* __restrict__ qcount, uint32_t* err,
-                                                unsigned long long* stats) {
+                                                unsigned long long* stats, uint32_t defer) {
   const uint32_t n = *qcount;
   if (stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(stats, (unsigned long long)n);
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -410,7 +410,8 @@ __global__ void __launch_bounds__(256, 4) k_extend(WaveBuffers w, Src src, const
     const F3 o = mk3(w.ox[p], w.oy[p], w.oz[p]), d = mk3(w.dx[p], w.dy[p], w.dz[p]);
     float t = 0.f;
     uint32_t obj = 0xFFFFFFFFu, prim = 0;
-    if (!scene_closest<kCsg>(s, o, d, ps.near, ps.far, t, obj, prim, err)) obj = 0xFFFFFFFFu;
+    if (!scene_closest<kCsg>(s, o, d, ps.near, ps.far, t, obj, prim, err, defer ? s.defer_leaf : kNoLeaf))
+      obj = 0xFFFFFFFFu;
     w.ht[p] = t;
     w.hobj[p] = obj;
     w.hprim[p] = prim;
@@ -430,7 +431,7 @@ template <class Src, bool kCsg>
 __global__ void __launch_bounds__(256, 2) k_extend_walk(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
                                                      const uint32_t* __restrict__ qcount, uint32_t* __restrict__ fetch,
                                                      uint32_t* err, unsigned long long* stats, int leaf_min,
-                                                     int refill_min) {
+                                                     int refill_min, uint32_t defer) {
   const uint32_t n = *qcount;
   if (stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(stats, (unsigned long long)n);
   const unsigned lane = threadIdx.x & 31u, lt_mask = (1u << lane) - 1u;
@@ -516,6 +517,7 @@ __global__ void __launch_bounds__(256, 2) k_extend_walk(WaveBuffers w, Src src, 
         // A leaf: its primitives over [near, min_t], a candidate adopted only when strictly nearer.
         for (uint32_t k = lf; k < lf + count; ++k) {
           const uint32_t ref = __ldg(&s.order[k]);
+          if (defer && ref == s.defer_leaf) continue;  // answered by k_defer_closest
           float t;
           uint32_t leaf, prim;
           if (prim_closest<kCsg>(s, ref, o, d, near, min_t, t, leaf, prim, err) && (!have || t < min_t)) {
@@ -829,18 +831,310 @@ __global__ void __launch_bounds__(256) k_train_batch(WaveBuffers w, CacheWave cw
 
 // 3 resident blocks per SM (the torus-knot frame 54.1 -> 52.9 ms against 4; 2 gained nothing
 // more; with the solids' code, 48 of 770 bytes still spill).
+// With `defer`, a scene's deferred leaf is left out: an occluded entry is resolved (its t_max
+// set to -1), an unoccluded one of a scene without a deferred leaf adds its light sample and
+// is resolved, and the others wait for k_defer_any.
 template <class Src, bool kCsg>
-__global__ void __launch_bounds__(256, 3) k_shadow(WaveBuffers w, Src src, uint32_t* err, unsigned long long* stats) {
+__global__ void __launch_bounds__(256, 3) k_shadow(WaveBuffers w, Src src, uint32_t* err, unsigned long long* stats,
+                                                uint32_t defer) {
   const uint32_t n = w.counts[2];
   if (stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(stats + 1, (unsigned long long)n);
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const uint32_t p = w.s_path[k];
     const SceneView& s = src.view(w, p);
     const F3 o = mk3(w.s_ox[k], w.s_oy[k], w.s_oz[k]), d = mk3(w.s_dx[k], w.s_dy[k], w.s_dz[k]);
-    if (!scene_any<kCsg>(s, o, d, kShadowEps, w.s_tmax[k], err)) {  // VisibilityTester::unoccluded (lights.rs:67-69)
+    const uint32_t skip = defer ? s.defer_leaf : kNoLeaf;
+    if (scene_any<kCsg>(s, o, d, kShadowEps, w.s_tmax[k], err, skip)) {
+      if (defer) w.s_tmax[k] = -1.f;
+    } else if (skip == kNoLeaf) {  // VisibilityTester::unoccluded (lights.rs:67-69)
       w.lr[p] = fa(w.lr[p], w.s_cr[k]);
       w.lg[p] = fa(w.lg[p], w.s_cg[k]);
       w.lb[p] = fa(w.lb[p], w.s_cb[k]);
+      if (defer) w.s_tmax[k] = -1.f;
+    }
+  }
+}
+
+// ---- the deferred leaf ----------------------------------------------------------------------
+// A scene's largest mesh, when it is placed untransformed in the top-level tree, is left out
+// of the per-path queries above and answered here for all queued paths at once by persistent
+// warps over the paths (the ray-cast kernel's while-while schedule: idle lanes refilled with
+// one atomicAdd per warp, interior nodes walked until every lane stands on a leaf, the leaves
+// of all lanes tested in one pass). Each lane walks its own scene's mesh (batches mix scenes).
+//
+// Nearest hit: the mesh is offered [near, nearest hit so far] and its hit adopted only when
+// strictly nearer, which is what Scene::find_nearest does with it wherever it comes in the
+// top-level order (scene.rs:186-220); an object's own answer does not depend on the interval
+// it is offered as long as its hit lies inside, so the result is the per-path query's, up to
+// which of two objects hit at exactly the same distance is kept.
+template <class Src>
+__global__ void __launch_bounds__(128, 8) k_defer_closest(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
+                                                       const uint32_t* __restrict__ qcount,
+                                                       uint32_t* __restrict__ fetch, uint32_t* err) {
+  const uint32_t n = *qcount;
+  const unsigned lane = threadIdx.x & 31u, lt_mask = (1u << lane) - 1u;
+  bool active = false;
+  uint32_t p = 0, leaf = 0, best = 0xFFFFFFFFu, lf = 0, count = 0, budget = 0;
+  MeshView m{};
+  PRay r;
+  float near = 0.f, far = 0.f, min_t = FLT_MAX;
+  bool have = false;
+  int sp = 0;
+  uint32_t stk_lf[kTraceStack], stk_cnt[kTraceStack];
+  float stk_e[kTraceStack];
+  for (;;) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    bool exhausted = false;
+    if (idle) {
+      const int leader = __ffs(idle) - 1;
+      uint32_t base = 0;
+      if (int(lane) == leader) base = atomicAdd(fetch, uint32_t(__popc(idle)));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      exhausted = uint64_t(base) + __popc(idle) >= n;
+      const uint64_t k = uint64_t(base) + __popc(idle & lt_mask);
+      if (!active && k < n) {
+        p = q[k];
+        const SceneView& s = src.view(w, p);
+        leaf = s.defer_leaf;
+        if (leaf != kNoLeaf) {
+          const PathSettings ps = src.settings(w, p);
+          m = s.meshes[s.objects[leaf].mesh];
+          r = prepare_ray(mk3(w.ox[p], w.oy[p], w.oz[p]), mk3(w.dx[p], w.dy[p], w.dz[p]));
+          near = ps.near;
+          have = w.hobj[p] != 0xFFFFFFFFu;
+          far = have ? w.ht[p] : ps.far;
+          const float4 rlo = __ldg(&m.nodes[0]);
+          const float4 rhi = __ldg(&m.nodes[1]);
+          float entry;
+          // the root is pushed, then dropped at pop if its entry is >= min_t = FLT_MAX (bvh.rs:462-472)
+          if (box_hit(r, rlo, rhi, near, far, entry) && entry < FLT_MAX) {
+            lf = __float_as_uint(rlo.w);
+            count = __float_as_uint(rhi.w);
+            min_t = FLT_MAX;
+            best = 0xFFFFFFFFu;
+            sp = 0;
+            budget = m.node_count;
+            active = true;
+          }
+        }
+      }
+    }
+    if (__ballot_sync(0xffffffffu, active) == 0) {
+      if (exhausted) break;
+      continue;
+    }
+    if (active) {
+      bool done = false;
+      while (count == 0) {  // interior nodes until this lane stands on a leaf
+        if (budget-- == 0) {
+          atomicOr(err, kErrBudget);
+          done = true;
+          break;
+        }
+        float4 l0, l1, r0, r1;
+        load_node(&m.nodes[2 * lf], l0, l1);
+        load_node(&m.nodes[2 * lf + 2], r0, r1);
+        float dl, dr;
+        const bool hl = box_hit(r, l0, l1, near, far, dl);
+        const bool hr = box_hit(r, r0, r1, near, far, dr);
+        const bool swap = hl && hr && dr < dl;  // right first only when strictly nearer
+        const bool hn = swap ? hr : hl, hf = swap ? hl : hr;
+        const float dn = swap ? dr : dl, df = swap ? dl : dr;
+        const bool take_f = hf && df < min_t, take_n = hn && dn < min_t;
+        if (take_n) {
+          if (take_f) {
+            if (sp >= kTraceStack) {
+              atomicOr(err, kErrStack);
+              done = true;
+              break;
+            }
+            stk_lf[sp] = __float_as_uint(swap ? l0.w : r0.w);
+            stk_cnt[sp] = __float_as_uint(swap ? l1.w : r1.w);
+            stk_e[sp] = df;
+            ++sp;
+          }
+          lf = __float_as_uint(swap ? r0.w : l0.w);
+          count = __float_as_uint(swap ? r1.w : l1.w);
+        } else if (take_f) {
+          lf = __float_as_uint(swap ? l0.w : r0.w);
+          count = __float_as_uint(swap ? l1.w : r1.w);
+        } else {
+          bool found = false;  // pop, dropping entries at or beyond the nearest hit (bvh.rs:470-472)
+          while (sp > 0) {
+            --sp;
+            if (stk_e[sp] < min_t) {
+              lf = stk_lf[sp];
+              count = stk_cnt[sp];
+              found = true;
+              break;
+            }
+          }
+          if (!found) {
+            done = true;
+            break;
+          }
+        }
+      }
+      if (!done) {  // the leaves of every lane standing on one
+        if (budget-- == 0) {
+          atomicOr(err, kErrBudget);
+          done = true;
+        } else {
+          for (uint32_t k = lf; k < lf + count; ++k) {
+            const float4 A = __ldg(&m.tri_a[k]);
+            const float4 B = __ldg(&m.tri_b[k]);
+            const float2 C = __ldg(&m.tri_c[k]);
+            float t;
+            if (tri_hit(r, A, B, C.x, t) && t < min_t && t >= near && t <= far) {
+              min_t = t;
+              best = __float_as_uint(C.y);
+            }
+          }
+          bool found = false;
+          while (sp > 0) {
+            --sp;
+            if (stk_e[sp] < min_t) {
+              lf = stk_lf[sp];
+              count = stk_cnt[sp];
+              found = true;
+              break;
+            }
+          }
+          if (!found) done = true;
+        }
+      }
+      if (done) {
+        if (best != 0xFFFFFFFFu && (!have || min_t < far)) {  // adopted only when strictly nearer
+          w.ht[p] = min_t;
+          w.hobj[p] = leaf;
+          w.hprim[p] = best;
+        }
+        active = false;
+      }
+    }
+  }
+}
+
+// Shadow rays against the deferred leaf: the entries k_shadow left open (t_max >= 0) add their
+// light sample when the mesh does not block [kShadowEps, t_max]; any hit ends the walk.
+template <class Src>
+__global__ void __launch_bounds__(128, 8) k_defer_any(WaveBuffers w, Src src, uint32_t* __restrict__ fetch,
+                                                   uint32_t* err) {
+  const uint32_t n = w.counts[2];
+  const unsigned lane = threadIdx.x & 31u, lt_mask = (1u << lane) - 1u;
+  bool active = false;
+  uint32_t k = 0, p = 0, lf = 0, count = 0, budget = 0;
+  MeshView m{};
+  PRay r;
+  float far = 0.f;
+  int sp = 0;
+  uint32_t stk_lf[kTraceStack], stk_cnt[kTraceStack];
+  for (;;) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    bool exhausted = false;
+    if (idle) {
+      const int leader = __ffs(idle) - 1;
+      uint32_t base = 0;
+      if (int(lane) == leader) base = atomicAdd(fetch, uint32_t(__popc(idle)));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      exhausted = uint64_t(base) + __popc(idle) >= n;
+      const uint64_t kk = uint64_t(base) + __popc(idle & lt_mask);
+      if (!active && kk < n) {
+        k = uint32_t(kk);
+        far = w.s_tmax[k];
+        if (far >= 0.f) {  // still open
+          p = w.s_path[k];
+          const SceneView& s = src.view(w, p);
+          m = s.meshes[s.objects[s.defer_leaf].mesh];
+          r = prepare_ray(mk3(w.s_ox[k], w.s_oy[k], w.s_oz[k]), mk3(w.s_dx[k], w.s_dy[k], w.s_dz[k]));
+          const float4 rlo = __ldg(&m.nodes[0]);
+          const float4 rhi = __ldg(&m.nodes[1]);
+          float entry;
+          if (box_hit(r, rlo, rhi, kShadowEps, far, entry)) {
+            lf = __float_as_uint(rlo.w);
+            count = __float_as_uint(rhi.w);
+            sp = 0;
+            budget = m.node_count;
+            active = true;
+          } else {  // misses the mesh: unoccluded
+            w.lr[p] = fa(w.lr[p], w.s_cr[k]);
+            w.lg[p] = fa(w.lg[p], w.s_cg[k]);
+            w.lb[p] = fa(w.lb[p], w.s_cb[k]);
+          }
+        }
+      }
+    }
+    if (__ballot_sync(0xffffffffu, active) == 0) {
+      if (exhausted) break;
+      continue;
+    }
+    if (active) {
+      bool done = false, hit = false;
+      while (count == 0) {
+        if (budget-- == 0) {
+          atomicOr(err, kErrBudget);
+          done = true;
+          hit = true;  // a malformed tree: reported, the sample dropped
+          break;
+        }
+        float4 l0, l1, r0, r1;
+        load_node(&m.nodes[2 * lf], l0, l1);
+        load_node(&m.nodes[2 * lf + 2], r0, r1);
+        float dl, dr;
+        const bool hl = box_hit(r, l0, l1, kShadowEps, far, dl);
+        const bool hr = box_hit(r, r0, r1, kShadowEps, far, dr);
+        const bool swap = hl && hr && dr < dl;  // the nearer child first: the likelier blocker
+        const bool hn = swap ? hr : hl, hf = swap ? hl : hr;
+        if (hn) {
+          if (hf) {
+            if (sp >= kTraceStack) {
+              atomicOr(err, kErrStack);
+              done = true;
+              hit = true;
+              break;
+            }
+            stk_lf[sp] = __float_as_uint(swap ? l0.w : r0.w);
+            stk_cnt[sp] = __float_as_uint(swap ? l1.w : r1.w);
+            ++sp;
+          }
+          lf = __float_as_uint(swap ? r0.w : l0.w);
+          count = __float_as_uint(swap ? r1.w : l1.w);
+        } else if (hf) {
+          lf = __float_as_uint(swap ? l0.w : r0.w);
+          count = __float_as_uint(swap ? l1.w : r1.w);
+        } else if (sp > 0) {
+          --sp;
+          lf = stk_lf[sp];
+          count = stk_cnt[sp];
+        } else {
+          done = true;
+          break;
+        }
+      }
+      if (!done) {
+        for (uint32_t j = lf; j < lf + count && !hit; ++j) {
+          const float4 A = __ldg(&m.tri_a[j]);
+          const float4 B = __ldg(&m.tri_b[j]);
+          const float2 C = __ldg(&m.tri_c[j]);
+          float t;
+          if (tri_hit(r, A, B, C.x, t) && t >= kShadowEps && t <= far) hit = true;
+        }
+        if (hit || sp == 0) {
+          done = true;
+        } else {
+          --sp;
+          lf = stk_lf[sp];
+          count = stk_cnt[sp];
+        }
+      }
+      if (done) {
+        if (!hit) {
+          w.lr[p] = fa(w.lr[p], w.s_cr[k]);
+          w.lg[p] = fa(w.lg[p], w.s_cg[k]);
+          w.lb[p] = fa(w.lb[p], w.s_cb[k]);
+        }
+        active = false;
+      }
     }
   }
 }
@@ -1007,39 +1301,56 @@ static bool shade_staging() {
 // top-level tree among the scenes rendered; `csg`: some scene holds a constructive solid (the
 // traversal kernels are also built without the solids' code, which takes registers and spills
 // from every other query).
+// Scenes' deferred leaves are answered by their own passes (k_defer_closest, k_defer_any)
+// unless PBRT_DEFER=0 (for measurements; the films differ at most where two objects are hit
+// at exactly the same distance).
+static bool defer_enabled() {
+  static const bool v = [] {
+    const char* e = std::getenv("PBRT_DEFER");
+    return !(e && e[0] == '0');
+  }();
+  return v;
+}
+
 template <class Src>
 static cudaError_t bounce_loop(const WaveBuffers& w, const Src& src, const CacheWave& cw, uint32_t loops, bool shadows,
                                uint32_t cache_mode, uint32_t term_hit, const LaunchShape& sh, unsigned long long* stats,
-                               uint32_t* err, int sm_count, cudaStream_t st, uint32_t top_nodes, bool csg) {
+                               uint32_t* err, int sm_count, cudaStream_t st, uint32_t top_nodes, bool csg,
+                               bool defer) {
   cudaError_t e;
   const unsigned gt = unsigned(sm_count) * sh.trace_blocks_per_sm, gs = unsigned(sm_count) * sh.shade_blocks_per_sm;
+  const unsigned gd = unsigned(sm_count) * 8u;  // the deferred passes: persistent, 8 blocks of 128 per SM
+  const uint32_t df = defer ? 1u : 0u;
   for (uint32_t b = 0; b < loops; ++b) {
     uint32_t* qin = (b & 1) ? w.qb : w.qa;
     uint32_t* qout = (b & 1) ? w.qa : w.qb;
     uint32_t* cin = w.counts + (b & 1);
     uint32_t* cout = w.counts + ((b + 1) & 1);
     if ((e = cudaMemsetAsync(cout, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
-    // counts[2]: shadow rays queued by k_shade; counts[3]: k_extend_walk's fetch position
-    if ((e = cudaMemsetAsync(w.counts + 2, 0, 2 * sizeof(uint32_t), st)) != cudaSuccess) return e;
+    // counts[2]: shadow rays queued by k_shade; counts[3]: k_extend_walk's fetch position;
+    // counts[4], [5]: the deferred passes' fetch positions
+    if ((e = cudaMemsetAsync(w.counts + 2, 0, 4 * sizeof(uint32_t), st)) != cudaSuccess) return e;
     const WalkSchedule ws = walk_schedule();
     if (top_nodes >= kWalkMinTopNodes && csg)
       k_extend_walk<Src, true><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, w.counts + 3, err, stats,
-                                                                ws.leaf_min, ws.refill_min);
+                                                                ws.leaf_min, ws.refill_min, df);
     else if (top_nodes >= kWalkMinTopNodes)
       k_extend_walk<Src, false><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, w.counts + 3, err, stats,
-                                                                 ws.leaf_min, ws.refill_min);
+                                                                 ws.leaf_min, ws.refill_min, df);
     else if (csg)
-      k_extend<Src, true><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, err, stats);
+      k_extend<Src, true><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, err, stats, df);
     else
-      k_extend<Src, false><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, err, stats);
+      k_extend<Src, false><<<gt, sh.trace_threads, 0, st>>>(w, src, qin, cin, err, stats, df);
+    if (defer) k_defer_closest<Src><<<gd, 128, 0, st>>>(w, src, qin, cin, w.counts + 4, err);
     if (shade_staging())
       k_shade<Src, true><<<gs, sh.shade_threads, 0, st>>>(w, src, qin, cin, qout, cout, cw, cache_mode, term_hit);
     else
       k_shade<Src, false><<<gs, sh.shade_threads, 0, st>>>(w, src, qin, cin, qout, cout, cw, cache_mode, term_hit);
     // (a persistent walk for the shadow rays measured 2.6% slower on 10,000 spheres: any-hit
     // rays end early, so one thread per ray wastes little)
-    if (shadows && csg) k_shadow<Src, true><<<gt, sh.trace_threads, 0, st>>>(w, src, err, stats);
-    else if (shadows) k_shadow<Src, false><<<gt, sh.trace_threads, 0, st>>>(w, src, err, stats);
+    if (shadows && csg) k_shadow<Src, true><<<gt, sh.trace_threads, 0, st>>>(w, src, err, stats, df);
+    else if (shadows) k_shadow<Src, false><<<gt, sh.trace_threads, 0, st>>>(w, src, err, stats, df);
+    if (shadows && defer) k_defer_any<Src><<<gd, 128, 0, st>>>(w, src, w.counts + 5, err);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -1080,10 +1391,12 @@ cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, 
       const BatchScene& h = host_table[first];
       const OneScene one{h.view, PathSettings{h.max_depth, h.rr_start, h.integrator, h.cam.near, h.cam.far}};
       e = bounce_loop(w, one, CacheWave{}, h.max_depth, !h.integrator, kCacheOff, 0, shape, stats, err, sm_count, st,
-                      h.view.top_node_count, h.view.has_csg != 0);
+                      h.view.top_node_count, h.view.has_csg != 0, defer_enabled() && h.view.defer_leaf != kNoLeaf);
     } else {
+      bool defer = false;
+      for (uint32_t i = first; i <= last; ++i) defer = defer || host_table[i].view.defer_leaf != kNoLeaf;
       e = bounce_loop(w, src, CacheWave{}, max_depth, any_path_integrator, kCacheOff, 0, shape, stats, err, sm_count,
-                      st, top_nodes, csg);
+                      st, top_nodes, csg, defer_enabled() && defer);
     }
     if (e != cudaSuccess) return e;
     k_accumulate_batch<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, n, table);
@@ -1110,7 +1423,8 @@ cudaError_t trace_wave(const SceneView& s, const WaveBuffers& w, const CacheWave
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const OneScene src{s, PathSettings{rs.max_depth, rs.rr_start, rs.integrator, cam.near, cam.far}};
   return bounce_loop(w, src, cw, rs.loop_depth ? rs.loop_depth : rs.max_depth, !rs.integrator, rs.cache_mode, rs.term_hit,
-                     rs.shape, rs.stats, err, sm_count, st, s.top_node_count, s.has_csg != 0);
+                     rs.shape, rs.stats, err, sm_count, st, s.top_node_count, s.has_csg != 0,
+                     defer_enabled() && s.defer_leaf != kNoLeaf);
 }
 
 cudaError_t accumulate_wave(const WaveBuffers& w, uint32_t n, double* film, uint32_t image_w, const RenderSettings& rs,

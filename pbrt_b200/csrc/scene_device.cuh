@@ -49,7 +49,11 @@ struct SceneView {
   const float* light_tris;  // area lights: 9 floats per world-space triangle
   const float* light_cdf;   // running area per triangle
   uint32_t has_csg;         // some leaf is a constructive solid: only the kernels built with CSG may run it
+  // A leaf the renderer's scene queries may leave out and answer in a pass of their own (the
+  // scene's largest untransformed mesh placed directly in the top-level tree); kNoLeaf: none.
+  uint32_t defer_leaf;
 };
+constexpr uint32_t kNoLeaf = 0xFFFFFFFFu;
 
 struct Isect {
   F3 p, n, wo, dpdu;
@@ -477,9 +481,11 @@ PBRT_DEV bool prim_any(const SceneView& s, uint32_t ref, const F3& o, const F3& 
 // Scene::find_nearest: the unbounded primitives first, each over [near, far]; then the
 // top-level query over [near, nearest so far], narrowing to every adopted hit and offering
 // each primitive [near, min_t]; a candidate is adopted only when strictly nearer.
+// `skip` (a leaf index, or kNoLeaf) is a primitive the query leaves out.
 template <bool kCount, bool kCsg = true>
 PBRT_DEV bool scene_closest_t(const SceneView& s, const F3& o, const F3& d, float near, float far, float& t_out,
-                              uint32_t& leaf_out, uint32_t& prim_out, uint32_t* err, SceneCount* cnt) {
+                              uint32_t& leaf_out, uint32_t& prim_out, uint32_t* err, SceneCount* cnt,
+                              uint32_t skip = kNoLeaf) {
   float min_t = far;
   bool have = false;
   for (uint32_t k = 0; k < s.unbounded_count; ++k) {  // nearest_among + closer (scene.rs:222-249)
@@ -524,6 +530,7 @@ PBRT_DEV bool scene_closest_t(const SceneView& s, const F3& o, const F3& d, floa
         for (uint32_t k = lf; k < lf + count; ++k) {
           if (kCount) cnt->objects++;
           const uint32_t ref = __ldg(&s.order[k]);
+          if (ref == skip) continue;
           float t;
           uint32_t leaf, prim;
           if (prim_closest<kCsg>(s, ref, o, d, near, min_t, t, leaf, prim, err) && (!have || t < min_t)) {
@@ -576,15 +583,15 @@ PBRT_DEV bool scene_closest_t(const SceneView& s, const F3& o, const F3& d, floa
 
 template <bool kCsg = true>
 PBRT_DEV bool scene_closest(const SceneView& s, const F3& o, const F3& d, float near, float far, float& t_out,
-                            uint32_t& leaf_out, uint32_t& prim_out, uint32_t* err) {
-  return scene_closest_t<false, kCsg>(s, o, d, near, far, t_out, leaf_out, prim_out, err, nullptr);
+                            uint32_t& leaf_out, uint32_t& prim_out, uint32_t* err, uint32_t skip = kNoLeaf) {
+  return scene_closest_t<false, kCsg>(s, o, d, near, far, t_out, leaf_out, prim_out, err, nullptr, skip);
 }
 
 // Scene::any_hit: the unbounded primitives first; then unordered, the box tested at pop,
 // right pushed before left (bvh.rs:269-270).
 template <bool kCount, bool kCsg = true>
 PBRT_DEV bool scene_any_t(const SceneView& s, const F3& o, const F3& d, float near, float far, uint32_t* err,
-                          SceneCount* cnt) {
+                          SceneCount* cnt, uint32_t skip = kNoLeaf) {
   for (uint32_t k = 0; k < s.unbounded_count; ++k) {  // any_blocks (scene.rs:170-184)
     if (kCount) cnt->objects++;
     if (prim_any<kCsg>(s, __ldg(&s.unbounded[k]), o, d, near, far, err)) return true;
@@ -610,7 +617,8 @@ PBRT_DEV bool scene_any_t(const SceneView& s, const F3& o, const F3& d, float ne
     if (count > 0) {
       for (uint32_t k = lf; k < lf + count; ++k) {
         if (kCount) cnt->objects++;
-        if (prim_any<kCsg>(s, __ldg(&s.order[k]), o, d, near, far, err)) return true;
+        const uint32_t ref = __ldg(&s.order[k]);
+        if (ref != skip && prim_any<kCsg>(s, ref, o, d, near, far, err)) return true;
       }
     } else {
       if (sp + 2 > kTraceStack) {
@@ -625,8 +633,9 @@ PBRT_DEV bool scene_any_t(const SceneView& s, const F3& o, const F3& d, float ne
 }
 
 template <bool kCsg = true>
-PBRT_DEV bool scene_any(const SceneView& s, const F3& o, const F3& d, float near, float far, uint32_t* err) {
-  return scene_any_t<false, kCsg>(s, o, d, near, far, err, nullptr);
+PBRT_DEV bool scene_any(const SceneView& s, const F3& o, const F3& d, float near, float far, uint32_t* err,
+                        uint32_t skip = kNoLeaf) {
+  return scene_any_t<false, kCsg>(s, o, d, near, far, err, nullptr, skip);
 }
 
 // ---- the interaction of an adopted hit -----------------------------------------------------
