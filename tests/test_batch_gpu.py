@@ -129,3 +129,25 @@ def test_batch_render_stats(built):
     want = sum(int(np.prod(sh[:2])) * p.spp for sh, p in zip(b.film_shapes(), params))
     assert st["paths"] == want
     b.close()
+
+
+def test_batch_with_deferred_meshes_equals_single_renders():
+    """Scenes whose large mesh is answered by the deferred passes, mixed with plain ones, in
+    waves small enough that some span several scenes (per-path scene lookup) and some hold
+    one scene (the single-scene kernels): every film equals the scene's own render."""
+    specs = [(d, c, dict(spp=s, max_depth=6)) for d, c, s in
+             W.batch_scenes(3, seed=13, width=40, height=30, levels=(5, 6), spp=(2, 4))]
+    d0, c0 = W.cornell_box(24, 20)
+    specs.insert(1, (d0, c0, dict(spp=3, max_depth=6)))
+    scenes = create_scenes([d for d, _, _ in specs])
+    singles = [s.render(cam, seed=5, **kw) for s, (_, cam, kw) in zip(scenes, specs)]
+    params = [render_params(cam, seed=5, **kw) for _, cam, kw in specs]
+    ctx = scenes[0].ctx
+    ctx.set_tuning(wave_paths=3000)
+    try:
+        b = Batch(scenes, params)
+        for f, s in zip(b.render(0), singles):
+            _close(f, s)
+        b.close()
+    finally:
+        ctx.set_tuning()
