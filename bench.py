@@ -637,8 +637,8 @@ def run_mlp(args, local):
                          "frac": round(tflops / peak, 4), "peak_kind": "measured burst bf16", "kernel": "k_mlp_infer"},
             "train_step": {"samples": MLP_TRAIN_BATCH, "ms": round(t_ms, 4),
                            "samples_per_s": round(MLP_TRAIN_BATCH / (t_ms * 1e-3), 1),
-                           "includes": "forward + backward (tcgen05 data gradients, CUDA-core weight gradients), "
-                                       "tile reduction, Adam"},
+                           "includes": "forward + backward (tcgen05 data and weight gradients), tile reduction, "
+                                       "Adam"},
             "clocks": clocks}
     print(json.dumps(line), flush=True)
 
