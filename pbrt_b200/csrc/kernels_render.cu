@@ -858,27 +858,10 @@ __global__ void __launch_bounds__(256, 3) k_shadow(WaveBuffers w, Src src, uint3
 // ---- the deferred leaf ----------------------------------------------------------------------
 // A scene's largest mesh, when it is placed untransformed in the top-level tree, is left out
 // of the per-path queries above and answered here for all queued paths at once by persistent
-// warps over the paths, with the ray-cast kernel's voted schedule: idle lanes are refilled
-// (one atomicAdd per warp) once 8 are idle, and each iteration is either a burst of up to 8
-// interior nodes for the lanes on interior nodes or, once 8 lanes stand on a leaf (or no lane
-// has interior work), a leaf step for those. Each lane walks its own scene's mesh (batches
-// mix scenes).
-constexpr int kDeferLeafMin = 8, kDeferRefillMin = 8, kDeferBurst = 8;
-
-// Pops the next node worth visiting (entry < min_t); false when the stack is empty.
-PBRT_DEV bool defer_pop(const uint32_t* stk_lf, const uint32_t* stk_cnt, const float* stk_e, int& sp, float min_t,
-                        uint32_t& lf, uint32_t& count) {
-  while (sp > 0) {
-    --sp;
-    if (stk_e[sp] < min_t) {  // entries at or beyond the nearest hit are dropped (bvh.rs:470-472)
-      lf = stk_lf[sp];
-      count = stk_cnt[sp];
-      return true;
-    }
-  }
-  return false;
-}
-
+// warps over the paths (the ray-cast kernel's while-while schedule: idle lanes refilled with
+// one atomicAdd per warp, interior nodes walked until every lane stands on a leaf, the leaves
+// of all lanes tested in one pass). Each lane walks its own scene's mesh (batches mix scenes).
+//
 // Nearest hit: the mesh is offered [near, nearest hit so far] and its hit adopted only when
 // strictly nearer, which is what Scene::find_nearest does with it wherever it comes in the
 // top-level order (scene.rs:186-220); an object's own answer does not depend on the interval
@@ -890,7 +873,7 @@ __global__ void __launch_bounds__(128, 8) k_defer_closest(WaveBuffers w, Src src
                                                        uint32_t* __restrict__ fetch, uint32_t* err) {
   const uint32_t n = *qcount;
   const unsigned lane = threadIdx.x & 31u, lt_mask = (1u << lane) - 1u;
-  bool active = false, exhausted = false;  // exhausted is warp-uniform
+  bool active = false;
   uint32_t p = 0, leaf = 0, best = 0xFFFFFFFFu, lf = 0, count = 0, budget = 0;
   MeshView m{};
   PRay r;
@@ -901,7 +884,8 @@ __global__ void __launch_bounds__(128, 8) k_defer_closest(WaveBuffers w, Src src
   float stk_e[kTraceStack];
   for (;;) {
     const unsigned idle = __ballot_sync(0xffffffffu, !active);
-    if (!exhausted && idle && (__popc(idle) >= kDeferRefillMin || idle == 0xffffffffu)) {
+    bool exhausted = false;
+    if (idle) {
       const int leader = __ffs(idle) - 1;
       uint32_t base = 0;
       if (int(lane) == leader) base = atomicAdd(fetch, uint32_t(__popc(idle)));
@@ -935,16 +919,63 @@ __global__ void __launch_bounds__(128, 8) k_defer_closest(WaveBuffers w, Src src
         }
       }
     }
-    const unsigned act = __ballot_sync(0xffffffffu, active);
-    if (act == 0) {
+    if (__ballot_sync(0xffffffffu, active) == 0) {
       if (exhausted) break;
-      continue;  // all idle and the queue not yet drained: the next iteration refills
+      continue;
     }
-    const unsigned on_leaf = __ballot_sync(0xffffffffu, active && count > 0);
-    const bool leaf_step = __popc(on_leaf) >= kDeferLeafMin || on_leaf == act;
-    bool done = false;
-    if (active && (count > 0) == leaf_step) {
-      if (leaf_step) {
+    if (active) {
+      bool done = false;
+      while (count == 0) {  // interior nodes until this lane stands on a leaf
+        if (budget-- == 0) {
+          atomicOr(err, kErrBudget);
+          done = true;
+          break;
+        }
+        float4 l0, l1, r0, r1;
+        load_node(&m.nodes[2 * lf], l0, l1);
+        load_node(&m.nodes[2 * lf + 2], r0, r1);
+        float dl, dr;
+        const bool hl = box_hit(r, l0, l1, near, far, dl);
+        const bool hr = box_hit(r, r0, r1, near, far, dr);
+        const bool swap = hl && hr && dr < dl;  // right first only when strictly nearer
+        const bool hn = swap ? hr : hl, hf = swap ? hl : hr;
+        const float dn = swap ? dr : dl, df = swap ? dl : dr;
+        const bool take_f = hf && df < min_t, take_n = hn && dn < min_t;
+        if (take_n) {
+          if (take_f) {
+            if (sp >= kTraceStack) {
+              atomicOr(err, kErrStack);
+              done = true;
+              break;
+            }
+            stk_lf[sp] = __float_as_uint(swap ? l0.w : r0.w);
+            stk_cnt[sp] = __float_as_uint(swap ? l1.w : r1.w);
+            stk_e[sp] = df;
+            ++sp;
+          }
+          lf = __float_as_uint(swap ? r0.w : l0.w);
+          count = __float_as_uint(swap ? r1.w : l1.w);
+        } else if (take_f) {
+          lf = __float_as_uint(swap ? l0.w : r0.w);
+          count = __float_as_uint(swap ? l1.w : r1.w);
+        } else {
+          bool found = false;  // pop, dropping entries at or beyond the nearest hit (bvh.rs:470-472)
+          while (sp > 0) {
+            --sp;
+            if (stk_e[sp] < min_t) {
+              lf = stk_lf[sp];
+              count = stk_cnt[sp];
+              found = true;
+              break;
+            }
+          }
+          if (!found) {
+            done = true;
+            break;
+          }
+        }
+      }
+      if (!done) {  // the leaves of every lane standing on one
         if (budget-- == 0) {
           atomicOr(err, kErrBudget);
           done = true;
@@ -959,55 +990,27 @@ __global__ void __launch_bounds__(128, 8) k_defer_closest(WaveBuffers w, Src src
               best = __float_as_uint(C.y);
             }
           }
-          if (!defer_pop(stk_lf, stk_cnt, stk_e, sp, min_t, lf, count)) done = true;
-        }
-      } else {
-        for (int b = 0; b < kDeferBurst && !done && count == 0; ++b) {
-          if (budget-- == 0) {
-            atomicOr(err, kErrBudget);
-            done = true;
-            break;
-          }
-          float4 l0, l1, r0, r1;
-          load_node(&m.nodes[2 * lf], l0, l1);
-          load_node(&m.nodes[2 * lf + 2], r0, r1);
-          float dl, dr;
-          const bool hl = box_hit(r, l0, l1, near, far, dl);
-          const bool hr = box_hit(r, r0, r1, near, far, dr);
-          const bool swap = hl && hr && dr < dl;  // right first only when strictly nearer
-          const bool hn = swap ? hr : hl, hf = swap ? hl : hr;
-          const float dn = swap ? dr : dl, df = swap ? dl : dr;
-          const bool take_f = hf && df < min_t, take_n = hn && dn < min_t;
-          if (take_n) {
-            if (take_f) {
-              if (sp >= kTraceStack) {
-                atomicOr(err, kErrStack);
-                done = true;
-                break;
-              }
-              stk_lf[sp] = __float_as_uint(swap ? l0.w : r0.w);
-              stk_cnt[sp] = __float_as_uint(swap ? l1.w : r1.w);
-              stk_e[sp] = df;
-              ++sp;
+          bool found = false;
+          while (sp > 0) {
+            --sp;
+            if (stk_e[sp] < min_t) {
+              lf = stk_lf[sp];
+              count = stk_cnt[sp];
+              found = true;
+              break;
             }
-            lf = __float_as_uint(swap ? r0.w : l0.w);
-            count = __float_as_uint(swap ? r1.w : l1.w);
-          } else if (take_f) {
-            lf = __float_as_uint(swap ? l0.w : r0.w);
-            count = __float_as_uint(swap ? l1.w : r1.w);
-          } else if (!defer_pop(stk_lf, stk_cnt, stk_e, sp, min_t, lf, count)) {
-            done = true;
           }
+          if (!found) done = true;
         }
       }
-    }
-    if (done) {
-      if (best != 0xFFFFFFFFu && (!have || min_t < far)) {  // adopted only when strictly nearer
-        w.ht[p] = min_t;
-        w.hobj[p] = leaf;
-        w.hprim[p] = best;
+      if (done) {
+        if (best != 0xFFFFFFFFu && (!have || min_t < far)) {  // adopted only when strictly nearer
+          w.ht[p] = min_t;
+          w.hobj[p] = leaf;
+          w.hprim[p] = best;
+        }
+        active = false;
       }
-      active = false;
     }
   }
 }
@@ -1019,7 +1022,7 @@ __global__ void __launch_bounds__(128, 8) k_defer_any(WaveBuffers w, Src src, ui
                                                    uint32_t* err) {
   const uint32_t n = w.counts[2];
   const unsigned lane = threadIdx.x & 31u, lt_mask = (1u << lane) - 1u;
-  bool active = false, exhausted = false;  // exhausted is warp-uniform
+  bool active = false;
   uint32_t k = 0, p = 0, lf = 0, count = 0, budget = 0;
   MeshView m{};
   PRay r;
@@ -1028,7 +1031,8 @@ __global__ void __launch_bounds__(128, 8) k_defer_any(WaveBuffers w, Src src, ui
   uint32_t stk_lf[kTraceStack], stk_cnt[kTraceStack];
   for (;;) {
     const unsigned idle = __ballot_sync(0xffffffffu, !active);
-    if (!exhausted && idle && (__popc(idle) >= kDeferRefillMin || idle == 0xffffffffu)) {
+    bool exhausted = false;
+    if (idle) {
       const int leader = __ffs(idle) - 1;
       uint32_t base = 0;
       if (int(lane) == leader) base = atomicAdd(fetch, uint32_t(__popc(idle)));
@@ -1060,16 +1064,54 @@ __global__ void __launch_bounds__(128, 8) k_defer_any(WaveBuffers w, Src src, ui
         }
       }
     }
-    const unsigned act = __ballot_sync(0xffffffffu, active);
-    if (act == 0) {
+    if (__ballot_sync(0xffffffffu, active) == 0) {
       if (exhausted) break;
       continue;
     }
-    const unsigned on_leaf = __ballot_sync(0xffffffffu, active && count > 0);
-    const bool leaf_step = __popc(on_leaf) >= kDeferLeafMin || on_leaf == act;
-    bool done = false, hit = false;
-    if (active && (count > 0) == leaf_step) {
-      if (leaf_step) {
+    if (active) {
+      bool done = false, hit = false;
+      while (count == 0) {
+        if (budget-- == 0) {
+          atomicOr(err, kErrBudget);
+          done = true;
+          hit = true;  // a malformed tree: reported, the sample dropped
+          break;
+        }
+        float4 l0, l1, r0, r1;
+        load_node(&m.nodes[2 * lf], l0, l1);
+        load_node(&m.nodes[2 * lf + 2], r0, r1);
+        float dl, dr;
+        const bool hl = box_hit(r, l0, l1, kShadowEps, far, dl);
+        const bool hr = box_hit(r, r0, r1, kShadowEps, far, dr);
+        const bool swap = hl && hr && dr < dl;  // the nearer child first: the likelier blocker
+        const bool hn = swap ? hr : hl, hf = swap ? hl : hr;
+        if (hn) {
+          if (hf) {
+            if (sp >= kTraceStack) {
+              atomicOr(err, kErrStack);
+              done = true;
+              hit = true;
+              break;
+            }
+            stk_lf[sp] = __float_as_uint(swap ? l0.w : r0.w);
+            stk_cnt[sp] = __float_as_uint(swap ? l1.w : r1.w);
+            ++sp;
+          }
+          lf = __float_as_uint(swap ? r0.w : l0.w);
+          count = __float_as_uint(swap ? r1.w : l1.w);
+        } else if (hf) {
+          lf = __float_as_uint(swap ? l0.w : r0.w);
+          count = __float_as_uint(swap ? l1.w : r1.w);
+        } else if (sp > 0) {
+          --sp;
+          lf = stk_lf[sp];
+          count = stk_cnt[sp];
+        } else {
+          done = true;
+          break;
+        }
+      }
+      if (!done) {
         for (uint32_t j = lf; j < lf + count && !hit; ++j) {
           const float4 A = __ldg(&m.tri_a[j]);
           const float4 B = __ldg(&m.tri_b[j]);
@@ -1084,56 +1126,15 @@ __global__ void __launch_bounds__(128, 8) k_defer_any(WaveBuffers w, Src src, ui
           lf = stk_lf[sp];
           count = stk_cnt[sp];
         }
-      } else {
-        for (int b = 0; b < kDeferBurst && !done && count == 0; ++b) {
-          if (budget-- == 0) {
-            atomicOr(err, kErrBudget);
-            done = true;
-            hit = true;  // a malformed tree: reported, the sample dropped
-            break;
-          }
-          float4 l0, l1, r0, r1;
-          load_node(&m.nodes[2 * lf], l0, l1);
-          load_node(&m.nodes[2 * lf + 2], r0, r1);
-          float dl, dr;
-          const bool hl = box_hit(r, l0, l1, kShadowEps, far, dl);
-          const bool hr = box_hit(r, r0, r1, kShadowEps, far, dr);
-          const bool swap = hl && hr && dr < dl;  // the nearer child first: the likelier blocker
-          const bool hn = swap ? hr : hl, hf = swap ? hl : hr;
-          if (hn) {
-            if (hf) {
-              if (sp >= kTraceStack) {
-                atomicOr(err, kErrStack);
-                done = true;
-                hit = true;
-                break;
-              }
-              stk_lf[sp] = __float_as_uint(swap ? l0.w : r0.w);
-              stk_cnt[sp] = __float_as_uint(swap ? l1.w : r1.w);
-              ++sp;
-            }
-            lf = __float_as_uint(swap ? r0.w : l0.w);
-            count = __float_as_uint(swap ? r1.w : l1.w);
-          } else if (hf) {
-            lf = __float_as_uint(swap ? l0.w : r0.w);
-            count = __float_as_uint(swap ? l1.w : r1.w);
-          } else if (sp > 0) {
-            --sp;
-            lf = stk_lf[sp];
-            count = stk_cnt[sp];
-          } else {
-            done = true;
-          }
+      }
+      if (done) {
+        if (!hit) {
+          w.lr[p] = fa(w.lr[p], w.s_cr[k]);
+          w.lg[p] = fa(w.lg[p], w.s_cg[k]);
+          w.lb[p] = fa(w.lb[p], w.s_cb[k]);
         }
+        active = false;
       }
-    }
-    if (done) {
-      if (!hit) {
-        w.lr[p] = fa(w.lr[p], w.s_cr[k]);
-        w.lg[p] = fa(w.lg[p], w.s_cg[k]);
-        w.lb[p] = fa(w.lb[p], w.s_cb[k]);
-      }
-      active = false;
     }
   }
 }
