@@ -31,6 +31,23 @@ using namespace pbrt::api;
 
 namespace {
 
+// The dense-result scratch for `cap` rays: a (id, t) pair per queue slot, one mask bit per
+// ray, one queue base per 1,024-ray chunk.
+int alloc_dense(pbrt_ctx* c, DenseScratch* d, uint64_t cap) {
+  if (!d->res) PBRT_TRY(c->cuda(cudaMalloc(&d->res, sizeof(uint2) * cap), "cudaMalloc(dense results)"));
+  const uint64_t chunks = (cap + kDenseChunk - 1) / kDenseChunk;
+  if (!d->mask) PBRT_TRY(c->cuda(cudaMalloc(&d->mask, sizeof(uint32_t) * 32 * chunks), "cudaMalloc(dense mask)"));
+  if (!d->bases) PBRT_TRY(c->cuda(cudaMalloc(&d->bases, sizeof(uint32_t) * chunks), "cudaMalloc(dense bases)"));
+  return PBRT_OK;
+}
+
+void free_dense(DenseScratch* d) {
+  cudaFree(d->res);
+  cudaFree(d->mask);
+  cudaFree(d->bases);
+  *d = DenseScratch{};
+}
+
 int ensure_slots(pbrt_ctx* c) {
   if (c->slots_ready) return PBRT_OK;
   for (Slot& s : c->slots) {
@@ -42,6 +59,7 @@ int ensure_slots(pbrt_ctx* c) {
     PBRT_TRY(c->cuda(cudaMalloc(&s.occ, kSlotRays), "cudaMalloc(staging)"));
     PBRT_TRY(c->cuda(cudaMalloc(&s.queue, sizeof(uint32_t) * kSlotRays), "cudaMalloc(staging)"));
     PBRT_TRY(c->cuda(cudaMalloc(&s.rec, sizeof(float4) * 2 * kSlotRays), "cudaMalloc(staging)"));
+    PBRT_TRY(alloc_dense(c, &s.dense, kSlotRays));
     PBRT_TRY(c->cuda(cudaMalloc(&s.fetch, 2 * sizeof(unsigned long long)), "cudaMalloc(staging)"));
   }
   c->slots_ready = true;
@@ -49,11 +67,12 @@ int ensure_slots(pbrt_ctx* c) {
 }
 
 int ensure_queue(pbrt_ctx* c) {
-  if (c->queue && c->queue_rec) return PBRT_OK;
+  if (c->queue && c->queue_rec && c->queue_dense.bases) return PBRT_OK;
   if (!c->queue) PBRT_TRY(c->cuda(cudaMalloc(&c->queue, sizeof(uint32_t) * kDevChunk), "cudaMalloc(survivor queue)"));
-  return c->cuda(cudaMalloc(&c->queue_rec, sizeof(float4) * 2 * kDevChunk), "cudaMalloc(survivor records)");
+  if (!c->queue_rec)
+    PBRT_TRY(c->cuda(cudaMalloc(&c->queue_rec, sizeof(float4) * 2 * kDevChunk), "cudaMalloc(survivor records)"));
+  return alloc_dense(c, &c->queue_dense, kDevChunk);
 }
-
 
 // Host-to-device copies go on the context's own stream: a plain cudaMemcpy from pageable
 // memory may return before its DMA lands, and kernels on a non-blocking stream would not wait
@@ -126,6 +145,7 @@ void pbrt_ctx_destroy(pbrt_ctx* c) {
     cudaFree(s.queue);
     cudaFree(s.fetch);
     cudaFree(s.rec);
+    free_dense(&s.dense);
     if (s.s) cudaStreamDestroy(s.s);
   }
   if (c->side) {
@@ -140,6 +160,7 @@ void pbrt_ctx_destroy(pbrt_ctx* c) {
   cudaFree(c->d_counters);
   cudaFree(c->queue);
   cudaFree(c->queue_rec);
+  free_dense(&c->queue_dense);
   cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -587,13 +608,14 @@ int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, flo
   // Nearest hit / any hit of one chunk of `m` rays (planes `stride` apart) on `st`.
   auto launch = [&](const float* r, uint64_t stride, uint64_t m, uint32_t* p, float* tt, uint32_t* ob, uint8_t* oc,
                     unsigned long long* cnt, uint32_t* queue, unsigned long long* qc, float4* rec,
-                    cudaStream_t st) -> cudaError_t {
+                    cudaStream_t st, const DenseScratch* dense = nullptr) -> cudaError_t {
     if (!one_mesh)
       return oc ? launch_scene_any(s->view, r, stride, m, oc, cnt, c->d_err, c->sm_count, st)
                 : launch_scene_closest(s->view, r, stride, m, p, tt, ob, cnt, c->d_err, c->sm_count, st);
     if (oc) return launch_mesh_any(mv, r, stride, m, oc, c->d_err, c->sm_count, st);
     if (c->persistent && !cnt)
-      return launch_mesh_closest_persistent(mv, r, stride, m, p, tt, ob, queue, qc, c->d_err, c->sm_count, st, rec);
+      return launch_mesh_closest_persistent(mv, r, stride, m, p, tt, ob, queue, qc, c->d_err, c->sm_count, st, rec,
+                                            dense);
     return launch_mesh_closest(mv, r, stride, m, p, tt, ob, cnt, c->d_err, c->sm_count, st);
   };
 
@@ -618,7 +640,7 @@ int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, flo
       for (uint64_t base = 0; base < n; base += kDevChunk) {
         const uint64_t m = std::min<uint64_t>(kDevChunk, n - base);
         PBRT_TRY(c->cuda(launch(rays + base, n, m, prim + base, t + base, obj ? obj + base : nullptr, nullptr, nullptr,
-                                c->queue, c->d_counters + 4, c->queue_rec, st),
+                                c->queue, c->d_counters + 4, c->queue_rec, st, &c->queue_dense),
                          "kernel launch"));
       }
     } else {
@@ -652,7 +674,7 @@ int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, flo
                                        m * sizeof(float), 8, cudaMemcpyHostToDevice, sl.s),
                      "cudaMemcpy2DAsync(rays)"));
     PBRT_TRY(c->cuda(launch(sl.rays, kSlotRays, m, sl.prim, sl.t, obj ? sl.obj : nullptr, occ ? sl.occ : nullptr,
-                            counters, sl.queue, sl.fetch, sl.rec, sl.s),
+                            counters, sl.queue, sl.fetch, sl.rec, sl.s, &sl.dense),
                      "kernel launch"));
     if (occ) {
       PBRT_TRY(c->cuda(cudaMemcpyAsync(occ + base, sl.occ, m, cudaMemcpyDeviceToHost, sl.s), "cudaMemcpyAsync"));

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/pbrt_b200.h"
+#include "kernels.hpp"
 #include "render.hpp"
 #include "scene_device.cuh"
 #include "trace_mesh.cuh"
@@ -55,6 +56,7 @@ struct Slot {
   uint8_t* occ = nullptr;
   uint32_t* queue = nullptr;            // survivor queue of the two-stage nearest-hit pass
   float4* rec = nullptr;                // the survivors' ray records (32 bytes each)
+  pbrt::DenseScratch dense;             // dense results: per-slot (id, t), survivor bitmask, chunk bases
   unsigned long long* fetch = nullptr;  // [queue length, fetch position] of that pass
 };
 
@@ -80,6 +82,7 @@ struct pbrt_ctx {
                                              // [8..10] rays / shadow rays / paths of the last render
   uint32_t* queue = nullptr;                  // survivor queue for device-buffer calls (kDevChunk entries)
   float4* queue_rec = nullptr;                // and their ray records (kDevChunk x 32 bytes)
+  pbrt::DenseScratch queue_dense;             // and the dense-result scratch for kDevChunk rays
   bool persistent = true;                     // persistent dynamic-fetch traversal (default)
   uint32_t* noalloc_scratch = nullptr;        // device address of pbrt_trace_closest_noalloc's static
                                               // scratch array on this device, looked up at creation

@@ -82,13 +82,19 @@ constexpr int kCullRays = 4;  // rays per thread and iteration
 
 // kVec: every plane and every output pointer is 16-byte aligned and the plane stride is a
 // multiple of 4, so a thread's four rays are one float4 per plane.
-template <bool kVec>
-__global__ void __launch_bounds__(kCullThreads) k_cull_root(MeshView m, const float* __restrict__ rays, uint64_t stride,
+// kDense: no miss answers; instead each block iteration (one 1,024-ray chunk) writes the
+// chunk's survivor bitmask (32 words, bit i = ray chunk * 1024 + i entered the root) and the
+// queue position of its first survivor; the queue itself is not needed (the traversal writes
+// results by queue position and k_dense_finalize maps them back to rays).
+static_assert(kDenseChunk == uint64_t(kCullThreads) * kCullRays, "a dense chunk is one cull block iteration");
+template <bool kVec, bool kDense>
+__global__ void __launch_bounds__(kCullThreads, 4) k_cull_root(MeshView m, const float* __restrict__ rays, uint64_t stride,
                                                             uint64_t n, uint32_t* __restrict__ prim,
                                                             float* __restrict__ tout, uint32_t* __restrict__ obj,
                                                             uint32_t* __restrict__ queue,
                                                             unsigned long long* __restrict__ queue_count,
-                                                            float4* __restrict__ rec) {
+                                                            float4* __restrict__ rec, uint32_t* __restrict__ mask,
+                                                            uint32_t* __restrict__ bases) {
   __shared__ uint32_t warp_off[2][kCullThreads / 32];
   __shared__ unsigned long long blk_base[2];
   const float4 rlo = __ldg(&m.nodes[0]);
@@ -122,14 +128,20 @@ __global__ void __launch_bounds__(kCullThreads) k_cull_root(MeshView m, const fl
         if (box_hit(r, rlo, rhi, v[6][j], v[7][j], entry) && entry < FLT_MAX) enter |= 1u << j;
       }
     }
-    // Every ray gets the miss answer now; stage 2 overwrites the rays it traverses.
-    if (kVec && full) {
+    const uint64_t chunk = it * gridDim.x + blockIdx.x;
+    if (kDense) {  // the 4-bit survivor nibbles of 8 lanes form one mask word
+      uint32_t word = uint32_t(enter) << ((lane & 7u) * 4u);
+      word |= __shfl_xor_sync(0xffffffffu, word, 1);
+      word |= __shfl_xor_sync(0xffffffffu, word, 2);
+      word |= __shfl_xor_sync(0xffffffffu, word, 4);
+      if ((lane & 7u) == 0 && chunk * kDenseChunk < n) mask[chunk * 32 + warp * 4 + (lane >> 3)] = word;
+    } else if (kVec && full) {  // every ray gets the miss answer now; stage 2 overwrites the rays it traverses
       __stcs(reinterpret_cast<uint4*>(prim + i0), make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu));
       const float inf = __int_as_float(0x7f800000);
       __stcs(reinterpret_cast<float4*>(tout + i0), make_float4(inf, inf, inf, inf));
       if (obj)
         __stcs(reinterpret_cast<uint4*>(obj + i0), make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu));
-    } else {
+    } else if (!kDense) {
       for (int j = 0; j < kCullRays; ++j)
         if (i0 + j < n) {
           __stcs(prim + i0 + j, 0xFFFFFFFFu);
@@ -156,6 +168,7 @@ __global__ void __launch_bounds__(kCullThreads) k_cull_root(MeshView m, const fl
         run += t;
       }
       blk_base[buf] = run ? atomicAdd(queue_count, (unsigned long long)run) : 0ull;
+      if (kDense && chunk * kDenseChunk < n) bases[chunk] = uint32_t(blk_base[buf]);
     }
     __syncthreads();
     uint64_t pos = blk_base[buf] + warp_off[buf][warp] + (incl - c);
@@ -166,7 +179,8 @@ __global__ void __launch_bounds__(kCullThreads) k_cull_root(MeshView m, const fl
           rec[2 * pos] = make_float4(v[0][j], v[1][j], v[2][j], v[6][j]);
           rec[2 * pos + 1] = make_float4(v[3][j], v[4][j], v[5][j], v[7][j]);
         }
-        queue[pos++] = uint32_t(i0 + j);
+        if (!kDense) queue[pos] = uint32_t(i0 + j);
+        ++pos;
       }
   }
 }
@@ -353,12 +367,15 @@ __global__ void __launch_bounds__(128, PBRT_TRAVERSAL_MIN_BLOCKS) k_mesh_closest
 //
 // 12 resident blocks of 128 threads per SM (at most 40 registers a thread): the traversal is
 // latency-bound, and the extra warps hide more of it than the few spilled registers cost.
-template <bool kRec>
+// kDense (with records): a lane's result goes to its queue slot in `res` (every survivor, hit
+// or miss) instead of to its ray's place in prim / tout; the queue's ray indices are not read.
+template <bool kRec, bool kDense>
 __global__ void __launch_bounds__(128, PBRT_TRAVERSAL_MIN_BLOCKS) k_mesh_closest_persistent(
     MeshView m, const float* __restrict__ rays, uint64_t stride, const uint32_t* __restrict__ queue,
     const unsigned long long* __restrict__ queue_count, uint32_t* __restrict__ prim, float* __restrict__ tout,
     uint32_t* __restrict__ obj, unsigned long long* __restrict__ next_ray, uint32_t* __restrict__ err,
-    const float4* __restrict__ rec, int leaf_min, int refill_min, int burst) {
+    const float4* __restrict__ rec, int leaf_min, int refill_min, int burst, uint2* __restrict__ res) {
+  static_assert(kRec || !kDense, "dense results need the ray records");
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
   const uint64_t n = *queue_count;
@@ -384,7 +401,7 @@ __global__ void __launch_bounds__(128, PBRT_TRAVERSAL_MIN_BLOCKS) k_mesh_closest
       if (!active) {
         const uint64_t k = base + __popc(idle & lt_mask);
         if (k < n) {
-          idx = __ldg(queue + k);
+          idx = kDense ? uint32_t(k) : __ldg(queue + k);  // dense: the queue slot (results go there)
           F3 o, d;
           if (kRec) {  // the copy stage 1 wrote: consecutive lanes read consecutive records
             const float4 a = __ldcs(rec + 2 * k), b = __ldcs(rec + 2 * k + 1);
@@ -476,7 +493,9 @@ __global__ void __launch_bounds__(128, PBRT_TRAVERSAL_MIN_BLOCKS) k_mesh_closest
       }
     }
     if (done) {
-      if (best != 0xFFFFFFFFu) {  // stage 1 already wrote the miss answer
+      if (kDense) {
+        res[idx] = make_uint2(best, best != 0xFFFFFFFFu ? __float_as_uint(min_t) : 0x7f800000u);
+      } else if (best != 0xFFFFFFFFu) {  // stage 1 already wrote the miss answer
         __stcs(prim + idx, best);
         __stcs(tout + idx, min_t);
         if (obj) __stcs(obj + idx, 0u);
@@ -492,9 +511,10 @@ __global__ void __launch_bounds__(128, PBRT_TRAVERSAL_MIN_BLOCKS) k_mesh_closest
 // against 1.021 ms for the while-while kernel and 1.052 ms for single-node steps), or the
 // while-while kernel (voted = false). PBRT_TRACE_SCHEDULE="ww" or
 // "leaf_min,refill_min[,burst]" (each in 1..32) overrides it for measurements; results do
-// not depend on it.
+// not depend on it. `dense`: the voted kernel's results go out through the dense pass when
+// the caller gives its scratch (PBRT_TRACE_DENSE=0: scattered stores by ray index instead).
 struct TraversalSchedule {
-  bool voted = true;
+  bool voted = true, dense = true;
   int leaf_min = 8, refill_min = 8, burst = 8;
 };
 
@@ -512,9 +532,73 @@ static TraversalSchedule traversal_schedule() {
         d.burst = got == 3 ? c : 1;
       }
     }
+    if (const char* e = std::getenv("PBRT_TRACE_DENSE")) d.dense = std::strcmp(e, "0") != 0;
     return d;
   }();
   return v;
+}
+
+// Stage 3 of the dense form: every ray's answer in ray order. One block per 1,024-ray chunk:
+// the chunk's 32 mask words and their exclusive prefix popcounts in shared memory; thread t
+// owns rays 4t .. 4t + 3 of the chunk, finds its survivors' ranks and reads their results
+// from consecutive queue slots, and writes 4 ids and 4 distances as one 16-byte store each.
+template <bool kVec>
+__global__ void __launch_bounds__(kCullThreads) k_dense_finalize(const uint2* __restrict__ res,
+                                                                 const uint32_t* __restrict__ mask,
+                                                                 const uint32_t* __restrict__ bases, uint64_t n,
+                                                                 uint32_t* __restrict__ prim, float* __restrict__ tout,
+                                                                 uint32_t* __restrict__ obj) {
+  __shared__ uint32_t msk[32], pre[32];
+  const uint64_t chunks = (n + kDenseChunk - 1) / kDenseChunk;
+  const uint32_t t = threadIdx.x, lane = t & 31u;
+  for (uint64_t ch = blockIdx.x; ch < chunks; ch += gridDim.x) {
+    if (t < 32) {
+      const uint32_t w = __ldg(mask + ch * 32 + t);
+      const uint32_t c = __popc(w);
+      uint32_t incl = c;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= unsigned(off)) incl += y;
+      }
+      msk[t] = w;
+      pre[t] = incl - c;
+    }
+    __syncthreads();
+    const uint32_t w = t >> 3, sh = (t & 7u) * 4u;
+    const uint32_t word = msk[w], bits = (word >> sh) & 0xFu;
+    uint64_t rank = uint64_t(__ldg(bases + ch)) + pre[w] + __popc(word & ((1u << sh) - 1u));
+    const uint64_t i0 = ch * kDenseChunk + 4u * t;
+    uint32_t p[4];
+    float tt[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      p[j] = 0xFFFFFFFFu;
+      tt[j] = __int_as_float(0x7f800000);
+      if (bits & (1u << j)) {
+        const uint2 r = __ldg(res + rank);
+        ++rank;
+        p[j] = r.x;
+        tt[j] = __uint_as_float(r.y);
+      }
+    }
+    if (kVec && i0 + 4 <= n) {
+      __stcs(reinterpret_cast<uint4*>(prim + i0), make_uint4(p[0], p[1], p[2], p[3]));
+      __stcs(reinterpret_cast<float4*>(tout + i0), make_float4(tt[0], tt[1], tt[2], tt[3]));
+      if (obj)
+        __stcs(reinterpret_cast<uint4*>(obj + i0),
+               make_uint4(p[0] != 0xFFFFFFFFu ? 0u : 0xFFFFFFFFu, p[1] != 0xFFFFFFFFu ? 0u : 0xFFFFFFFFu,
+                          p[2] != 0xFFFFFFFFu ? 0u : 0xFFFFFFFFu, p[3] != 0xFFFFFFFFu ? 0u : 0xFFFFFFFFu));
+    } else {
+      for (int j = 0; j < 4; ++j)
+        if (i0 + j < n) {
+          __stcs(prim + i0 + j, p[j]);
+          __stcs(tout + i0 + j, tt[j]);
+          if (obj) __stcs(obj + i0 + j, p[j] != 0xFFFFFFFFu ? 0u : 0xFFFFFFFFu);
+        }
+    }
+    __syncthreads();  // msk and pre are reused by the next chunk
+  }
 }
 
 static unsigned grid_for(uint64_t n, int threads, int sm_count) {
@@ -543,7 +627,8 @@ template <bool kRec>
 static int persistent_blocks_per_sm() {
   static const int v = [] {
     int b = 0;
-    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_mesh_closest_persistent<kRec>, 128, 0);
+    const cudaError_t e =
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_mesh_closest_persistent<kRec, false>, 128, 0);
     return e == cudaSuccess && b > 0 ? b : 8;
   }();
   return v;
@@ -552,7 +637,7 @@ static int persistent_blocks_per_sm() {
 cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays, uint64_t stride, uint64_t n,
                                            uint32_t* prim, float* t, uint32_t* obj, uint32_t* queue,
                                            unsigned long long* counters, uint32_t* err, int sm_count, cudaStream_t s,
-                                           float4* rec) {
+                                           float4* rec, const DenseScratch* dense) {
   if (n == 0) return cudaSuccess;
   const int blocks_per_sm = persistent_blocks_per_sm<true>();
   cudaError_t e = cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), s);
@@ -561,16 +646,29 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
   const uint64_t per_block = uint64_t(kCullThreads) * kCullRays;
   const uint64_t cull_need = (n + per_block - 1) / per_block, cull_cap = uint64_t(sm_count) * 8;
   const unsigned cg = unsigned(cull_need < cull_cap ? cull_need : cull_cap);
-  if (vec)
-    k_cull_root<true><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec);
-  else
-    k_cull_root<false><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
   const uint64_t full = uint64_t(sm_count) * blocks_per_sm;
   const uint64_t need = (n + 127) / 128;
   const unsigned g = unsigned(need < full ? need : full);
   const TraversalSchedule ts = traversal_schedule();
+  if (ts.voted && ts.dense && rec && vec && dense && dense->res && dense->mask && dense->bases) {
+    // dense results: cull (bitmask, chunk bases, records), traversal (results by queue slot),
+    // then every ray's answer in ray order
+    k_cull_root<true, true><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec,
+                                                         dense->mask, dense->bases);
+    k_mesh_closest_persistent<true, true><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj,
+                                                            counters + 1, err, rec, ts.leaf_min, ts.refill_min,
+                                                            ts.burst, dense->res);
+    k_dense_finalize<true><<<cg, kCullThreads, 0, s>>>(dense->res, dense->mask, dense->bases, n, prim, t, obj);
+    return cudaGetLastError();
+  }
+  if (vec)
+    k_cull_root<true, false><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec,
+                                                          nullptr, nullptr);
+  else
+    k_cull_root<false, false><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec,
+                                                           nullptr, nullptr);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
   if (!ts.voted) {
     if (rec)
       k_mesh_closest_ww<true><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj, counters + 1, err, rec);
@@ -578,11 +676,13 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
       k_mesh_closest_ww<false><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj, counters + 1, err,
                                                  nullptr);
   } else if (rec) {
-    k_mesh_closest_persistent<true><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj, counters + 1, err,
-                                                      rec, ts.leaf_min, ts.refill_min, ts.burst);
+    k_mesh_closest_persistent<true, false><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj,
+                                                             counters + 1, err, rec, ts.leaf_min, ts.refill_min,
+                                                             ts.burst, nullptr);
   } else {
-    k_mesh_closest_persistent<false><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj, counters + 1,
-                                                       err, nullptr, ts.leaf_min, ts.refill_min, ts.burst);
+    k_mesh_closest_persistent<false, false><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj,
+                                                              counters + 1, err, nullptr, ts.leaf_min, ts.refill_min,
+                                                              ts.burst, nullptr);
   }
   return cudaGetLastError();
 }
@@ -626,9 +726,11 @@ cudaError_t launch_mesh_closest_noalloc(const MeshView& m, const float* rays, ui
   const uint64_t cull_need = (n + per_block - 1) / per_block, cull_cap = uint64_t(sm_count) * 8;
   const unsigned cg = unsigned(cull_need < cull_cap ? cull_need : cull_cap);
   if (vec)
-    k_cull_root<true><<<cg, kCullThreads, 0, s>>>(m, rays, n, n, prim, t, nullptr, queue, counters, nullptr);
+    k_cull_root<true, false><<<cg, kCullThreads, 0, s>>>(m, rays, n, n, prim, t, nullptr, queue, counters, nullptr,
+                                                          nullptr, nullptr);
   else
-    k_cull_root<false><<<cg, kCullThreads, 0, s>>>(m, rays, n, n, prim, t, nullptr, queue, counters, nullptr);
+    k_cull_root<false, false><<<cg, kCullThreads, 0, s>>>(m, rays, n, n, prim, t, nullptr, queue, counters, nullptr,
+                                                           nullptr, nullptr);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const uint64_t full = uint64_t(sm_count) * blocks_per_sm;
@@ -639,8 +741,9 @@ cudaError_t launch_mesh_closest_noalloc(const MeshView& m, const float* rays, ui
     k_mesh_closest_ww<false><<<g, 128, 0, s>>>(m, rays, n, queue, counters, prim, t, nullptr, counters + 1, err,
                                                nullptr);
   else
-    k_mesh_closest_persistent<false><<<g, 128, 0, s>>>(m, rays, n, queue, counters, prim, t, nullptr, counters + 1,
-                                                       err, nullptr, ts.leaf_min, ts.refill_min, ts.burst);
+    k_mesh_closest_persistent<false, false><<<g, 128, 0, s>>>(m, rays, n, queue, counters, prim, t, nullptr,
+                                                              counters + 1, err, nullptr, ts.leaf_min, ts.refill_min,
+                                                              ts.burst, nullptr);
   return cudaGetLastError();
 }
 
