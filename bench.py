@@ -892,10 +892,10 @@ def main():
                          "peak_kind": peak_kind, "kernel": "k_mesh_closest",
                          "algorithmic_bytes_per_ray": round(bytes_per_ray, 2), "box_tests_per_ray": round(box_pr, 4),
                          "triangle_tests_per_ray": round(tri_pr, 4), "avg_launch_ms": round(launch_ms, 4)},
-            # per pbrt_trace_closest: the root cull, the persistent traversal and (unless switched
-            # off) the dense result pass
-            "gpu_launches": (2 if os.environ.get("PBRT_TRACE_DENSE") == "0"
-                             or os.environ.get("PBRT_TRACE_SCHEDULE") == "ww" else 3) * args.steps,
+            # per pbrt_trace_closest: the root cull, the persistent traversal and (when selected)
+            # the dense result pass
+            "gpu_launches": (3 if os.environ.get("PBRT_TRACE_DENSE") == "1"
+                             and os.environ.get("PBRT_TRACE_SCHEDULE") != "ww" else 2) * args.steps,
             "clocks": clocks,
         }
         if ws == 1 and not args.no_cache_race:

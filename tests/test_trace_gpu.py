@@ -151,3 +151,52 @@ def test_unsupported_and_invalid_inputs_raise():
     bad[0, 0] = 9999
     with pytest.raises(pb.PbrtError):
         pb.Scene().add_object(pb.Simple(pb.TriangleMesh(v, bad))).commit()
+
+
+_DENSE_SCRIPT = """
+import sys, numpy as np, torch
+sys.path.insert(0, {root!r})
+import pbrt_b200 as pb
+from pbrt_b200 import workloads as W
+v, f = W.displaced_icosphere(6, seed=41)
+s = pb.Scene()
+s.add_object(pb.Simple(pb.TriangleMesh(v, f)))
+s = s.commit(bvh_bins=16, bvh_max_leaf=4)
+n = (1 << 21) + 1028  # device buffers: 2,050 chunks of 1,024 rays, the last one of 4
+rays = W.incoherent_rays(n, v.min(0), v.max(0), seed=42)
+rng = np.random.default_rng(43)
+aim = rays[:, : 1 << 18]
+aim[3:6] = W.normalize_f32((rng.random((3, aim.shape[1])) - 0.5).astype(np.float32) - aim[0:3])
+dp, dt = s.intersect(torch.from_numpy(rays).cuda())
+hp, ht = s.intersect(rays[:, : (1 << 20) + 3 * 1024 + 8])  # host buffers: two pipelined chunks, the second ragged
+np.savez({out!r}, rays=rays, dp=dp.cpu().numpy().view(np.uint32), dt=dt.cpu().numpy(), hp=hp, ht=ht)
+"""
+
+
+@pytest.mark.parametrize("dense", ["0", "1"])
+def test_dense_result_pass_matches_oracle(tmp_path, dense):
+    """Both result forms of the two-stage pass (the cull's miss answers plus scattered hit
+    stores, or the survivor bitmask, results by queue slot and the ray-order pass) give the
+    oracle's ids and t, on device buffers with a partial last chunk and on host buffers. The
+    switch is read once per process: a child per form."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = str(tmp_path / f"dense_{dense}.npz")
+    env = dict(os.environ, PBRT_TRACE_DENSE=dense)
+    subprocess.run([sys.executable, "-c", _DENSE_SCRIPT.format(root=root, out=out)], env=env, check=True,
+                   timeout=600)
+    z = np.load(out)
+    rays = z["rays"]
+    v, f = W.displaced_icosphere(6, seed=41)
+    m = oracle.MeshBVH(v, f, np.float32, bins=16, max_leaf=4)
+    op, ot, _ = m.trace(rays)
+    hit = op != oracle.MISS
+    assert hit.sum() > 200_000
+    assert np.array_equal(z["dp"], op), f"{int((z['dp'] != op).sum())} ids differ"
+    assert np.array_equal(z["dt"][hit], ot[hit]) and np.all(np.isinf(z["dt"][~hit]))
+    k = z["hp"].shape[0]
+    assert np.array_equal(z["hp"], op[:k]) and np.array_equal(z["ht"][hit[:k]], ot[:k][hit[:k]])
+    assert np.all(np.isinf(z["ht"][~hit[:k]]))
