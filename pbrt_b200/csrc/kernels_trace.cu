@@ -738,12 +738,11 @@ static int pipelined_traversal_blocks(int want) {
   return b < full ? b : full;
 }
 
-// PBRT_TRACE_PARTS="K[,B[,G[,P[,T]]]]": K parts, B traversal blocks per SM (of 128 threads
-// worth of registers), G cull blocks per SM for the parts after the first (default 1), P
-// stream priorities (0: culls high, traversals low; 1: all equal; 2: culls low, traversals
-// high), T threads per traversal block (32, 64 or 128; the grid scales to keep the warps).
+// PBRT_TRACE_PARTS="K[,B[,G[,P]]]": K parts, B traversal blocks per SM, G cull blocks per SM
+// for the parts after the first (default 1), P stream priorities (0: culls high, traversals
+// low; 1: all equal; 2: culls low, traversals high).
 struct PipelineShape {
-  int parts = 1, trav_blocks = 10, cull_blocks = 1, priorities = 0, trav_threads = 128;
+  int parts = 1, trav_blocks = 10, cull_blocks = 1, priorities = 0;
 };
 
 static PipelineShape pipeline_shape() {
@@ -751,9 +750,8 @@ static PipelineShape pipeline_shape() {
     PipelineShape d;
     if (traversal_schedule().dense) return d;  // the dense result pass runs unpipelined
     if (const char* e = std::getenv("PBRT_TRACE_PARTS")) {
-      int a = 0, b = 0, g = 0, pr = 0, th = 0;
-      const int got = std::sscanf(e, "%d,%d,%d,%d,%d", &a, &b, &g, &pr, &th);
-      if (got >= 5 && (th == 32 || th == 64 || th == 128)) d.trav_threads = th;
+      int a = 0, b = 0, g = 0, pr = 0;
+      const int got = std::sscanf(e, "%d,%d,%d,%d", &a, &b, &g, &pr);
       if (got >= 1 && a >= 1 && a <= kPipeMaxParts) d.parts = a;
       if (got >= 2 && b >= 1 && b <= 16) d.trav_blocks = b;
       if (got >= 3 && g >= 1 && g <= 8) d.cull_blocks = g;
@@ -801,16 +799,15 @@ cudaError_t launch_mesh_closest_pipelined(const MeshView& m, const float* rays, 
     cudaStream_t ts_j = p.trav[j & 1];
     if (e == cudaSuccess) e = cudaStreamWaitEvent(ts_j, p.culled[j], 0);
     if (e != cudaSuccess) break;
-    const int th = pipeline_shape().trav_threads;
-    const uint64_t need = (mj + th - 1) / th, cap = uint64_t(sm_count) * tb * (128 / th);
+    const uint64_t need = (mj + 127) / 128, cap = uint64_t(sm_count) * tb;
     const unsigned g = unsigned(need < cap ? need : cap);
     if (ts.voted)
-      k_mesh_closest_persistent<true, false><<<g, th, 0, ts_j>>>(m, rays + b, stride, queue + b, cnt, prim + b,
+      k_mesh_closest_persistent<true, false><<<g, 128, 0, ts_j>>>(m, rays + b, stride, queue + b, cnt, prim + b,
                                                                   t + b, obj ? obj + b : nullptr, cnt + 1, err,
                                                                   rec + 2 * b, ts.leaf_min, ts.refill_min, ts.burst,
                                                                   nullptr);
     else
-      k_mesh_closest_ww<true><<<g, th, 0, ts_j>>>(m, rays + b, stride, queue + b, cnt, prim + b, t + b,
+      k_mesh_closest_ww<true><<<g, 128, 0, ts_j>>>(m, rays + b, stride, queue + b, cnt, prim + b, t + b,
                                                    obj ? obj + b : nullptr, cnt + 1, err, rec + 2 * b);
     e = cudaGetLastError();
   }
