@@ -74,12 +74,10 @@ int ensure_pipeline(pbrt_ctx* c) {
   TracePipeline& p = c->pipe;
   int least = 0, greatest = 0;
   PBRT_TRY(c->cuda(cudaDeviceGetStreamPriorityRange(&least, &greatest), "cudaDeviceGetStreamPriorityRange"));
-  const int mode = trace_pipeline_priorities();
-  const int cull_pri = mode == 0 ? greatest : least, trav_pri = mode == 2 ? greatest : least;
   if (!p.cull)
-    PBRT_TRY(c->cuda(cudaStreamCreateWithPriority(&p.cull, cudaStreamNonBlocking, cull_pri), "cudaStreamCreate"));
+    PBRT_TRY(c->cuda(cudaStreamCreateWithPriority(&p.cull, cudaStreamNonBlocking, greatest), "cudaStreamCreate"));
   for (cudaStream_t& t : p.trav)
-    if (!t) PBRT_TRY(c->cuda(cudaStreamCreateWithPriority(&t, cudaStreamNonBlocking, trav_pri), "cudaStreamCreate"));
+    if (!t) PBRT_TRY(c->cuda(cudaStreamCreateWithPriority(&t, cudaStreamNonBlocking, least), "cudaStreamCreate"));
   if (!p.fork) PBRT_TRY(c->cuda(cudaEventCreateWithFlags(&p.fork, cudaEventDisableTiming), "cudaEventCreate"));
   for (cudaEvent_t& e : p.culled)
     if (!e) PBRT_TRY(c->cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate"));

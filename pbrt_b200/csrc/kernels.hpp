@@ -56,9 +56,6 @@ cudaError_t launch_mesh_closest_pipelined(const MeshView& m, const float* rays, 
 // The part count and traversal blocks per SM of the pipelined pass on this build (1 part: the
 // plain two-stage pass); PBRT_TRACE_PARTS="K[,B]" overrides them for measurements.
 void trace_pipeline_shape(int* parts, int* trav_blocks_per_sm);
-// Stream priorities of the pipelined pass: 0 culls high and traversals low, 1 all equal, 2
-// culls low and traversals high.
-int trace_pipeline_priorities();
 // Allocation-free form of launch_mesh_closest_persistent for device buffers (plane stride
 // = n): its scratch is a file-scope __device__ array of kNoAllocMaxRays queue entries
 // shared by every call on a device. `scratch` is that array's device address on the current

@@ -738,37 +738,21 @@ static int pipelined_traversal_blocks(int want) {
   return b < full ? b : full;
 }
 
-// PBRT_TRACE_PARTS="K[,B[,G[,P]]]": K parts, B traversal blocks per SM, G cull blocks per SM
-// for the parts after the first (default 1), P stream priorities (0: culls high, traversals
-// low; 1: all equal; 2: culls low, traversals high).
-struct PipelineShape {
-  int parts = 1, trav_blocks = 10, cull_blocks = 1, priorities = 0;
-};
-
-static PipelineShape pipeline_shape() {
-  static const PipelineShape v = [] {
-    PipelineShape d;
+void trace_pipeline_shape(int* parts, int* trav_blocks_per_sm) {
+  static const int2 v = [] {
+    int2 d = make_int2(1, 10);
     if (traversal_schedule().dense) return d;  // the dense result pass runs unpipelined
     if (const char* e = std::getenv("PBRT_TRACE_PARTS")) {
-      int a = 0, b = 0, g = 0, pr = 0;
-      const int got = std::sscanf(e, "%d,%d,%d,%d", &a, &b, &g, &pr);
-      if (got >= 1 && a >= 1 && a <= kPipeMaxParts) d.parts = a;
-      if (got >= 2 && b >= 1 && b <= 16) d.trav_blocks = b;
-      if (got >= 3 && g >= 1 && g <= 8) d.cull_blocks = g;
-      if (got >= 4 && pr >= 0 && pr <= 2) d.priorities = pr;
+      int a = 0, b = 0;
+      const int got = std::sscanf(e, "%d,%d", &a, &b);
+      if (got >= 1 && a >= 1 && a <= kPipeMaxParts) d.x = a;
+      if (got == 2 && b >= 1 && b <= 16) d.y = b;
     }
     return d;
   }();
-  return v;
+  *parts = v.x;
+  *trav_blocks_per_sm = v.y;
 }
-
-void trace_pipeline_shape(int* parts, int* trav_blocks_per_sm) {
-  const PipelineShape v = pipeline_shape();
-  *parts = v.parts;
-  *trav_blocks_per_sm = v.trav_blocks;
-}
-
-int trace_pipeline_priorities() { return pipeline_shape().priorities; }
 
 cudaError_t launch_mesh_closest_pipelined(const MeshView& m, const float* rays, uint64_t stride, uint64_t n,
                                           uint32_t* prim, float* t, uint32_t* obj, uint32_t* queue, float4* rec,
@@ -789,7 +773,7 @@ cudaError_t launch_mesh_closest_pipelined(const MeshView& m, const float* rays, 
     unsigned long long* cnt = p.counters + 2 * j;
     const uint64_t per_block = uint64_t(kCullThreads) * kCullRays;
     const uint64_t cull_need = (mj + per_block - 1) / per_block;
-    const uint64_t cull_cap = uint64_t(sm_count) * (j == 0 ? 8 : pipeline_shape().cull_blocks);
+    const uint64_t cull_cap = uint64_t(sm_count) * (j == 0 ? 8 : 1);
     const unsigned cg = unsigned(cull_need < cull_cap ? cull_need : cull_cap);
     k_cull_root<true, false><<<cg, kCullThreads, 0, p.cull>>>(m, rays + b, stride, mj, prim + b, t + b,
                                                                obj ? obj + b : nullptr, queue + b, cnt, rec + 2 * b,
