@@ -157,26 +157,6 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-TRACE_PARTS_DEFAULT = 1  # the library's default part count of the pipelined pass
-
-
-def _launches_per_call(n_rays: int) -> int:
-    """Kernels one pbrt_trace_closest call on device buffers launches: the root cull and the
-    persistent traversal per part (PBRT_TRACE_PARTS, parts of whole 1,024-ray blocks), or
-    the cull, the traversal and the ray-order pass of the dense form (PBRT_TRACE_DENSE=1)."""
-    if os.environ.get("PBRT_TRACE_DENSE") == "1" and os.environ.get("PBRT_TRACE_SCHEDULE") != "ww":
-        return 3
-    parts = TRACE_PARTS_DEFAULT
-    try:
-        k = int(os.environ.get("PBRT_TRACE_PARTS", "").split(",")[0])
-        if 1 <= k <= 16:
-            parts = k
-    except ValueError:
-        pass
-    per = -(-(-(-n_rays // parts)) // 1024) * 1024
-    return 2 * -(-n_rays // per)
-
-
 def _traffic_per_launch(n_rays: int):
     """DRAM bytes per launch of the nearest-hit kernel from the committed ncu summary, scaled
     by rays when the capture used a smaller ray count (the tree is L2-resident, so traffic
@@ -912,7 +892,10 @@ def main():
                          "peak_kind": peak_kind, "kernel": "k_mesh_closest",
                          "algorithmic_bytes_per_ray": round(bytes_per_ray, 2), "box_tests_per_ray": round(box_pr, 4),
                          "triangle_tests_per_ray": round(tri_pr, 4), "avg_launch_ms": round(launch_ms, 4)},
-            "gpu_launches": _launches_per_call(N_RAYS) * args.steps,
+            # per pbrt_trace_closest: the root cull, the persistent traversal and (when selected)
+            # the dense result pass
+            "gpu_launches": (3 if os.environ.get("PBRT_TRACE_DENSE") == "1"
+                             and os.environ.get("PBRT_TRACE_SCHEDULE") != "ww" else 2) * args.steps,
             "clocks": clocks,
         }
         if ws == 1 and not args.no_cache_race:

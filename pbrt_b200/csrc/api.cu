@@ -66,46 +66,6 @@ int ensure_slots(pbrt_ctx* c) {
   return PBRT_OK;
 }
 
-// The pipelined pass's streams (culls at the device's highest priority, so a cull block takes
-// the first free slot beside the running traversals; traversals at the lowest), events and
-// per-part counters.
-int ensure_pipeline(pbrt_ctx* c) {
-  if (c->pipe_ready) return PBRT_OK;
-  TracePipeline& p = c->pipe;
-  int least = 0, greatest = 0;
-  PBRT_TRY(c->cuda(cudaDeviceGetStreamPriorityRange(&least, &greatest), "cudaDeviceGetStreamPriorityRange"));
-  if (!p.cull)
-    PBRT_TRY(c->cuda(cudaStreamCreateWithPriority(&p.cull, cudaStreamNonBlocking, greatest), "cudaStreamCreate"));
-  for (cudaStream_t& t : p.trav)
-    if (!t) PBRT_TRY(c->cuda(cudaStreamCreateWithPriority(&t, cudaStreamNonBlocking, least), "cudaStreamCreate"));
-  if (!p.fork) PBRT_TRY(c->cuda(cudaEventCreateWithFlags(&p.fork, cudaEventDisableTiming), "cudaEventCreate"));
-  for (cudaEvent_t& e : p.culled)
-    if (!e) PBRT_TRY(c->cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate"));
-  for (cudaEvent_t& e : p.joined)
-    if (!e) PBRT_TRY(c->cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate"));
-  if (!p.counters)
-    PBRT_TRY(c->cuda(cudaMalloc(&p.counters, 2 * sizeof(unsigned long long) * kPipeMaxParts), "cudaMalloc(counters)"));
-  c->pipe_ready = true;
-  return PBRT_OK;
-}
-
-void free_pipeline(TracePipeline* p) {
-  for (cudaStream_t s : {p->cull, p->trav[0], p->trav[1]})
-    if (s) {
-      cudaStreamSynchronize(s);
-      cudaStreamDestroy(s);
-    }
-  if (p->fork) cudaEventDestroy(p->fork);
-  for (cudaEvent_t e : p->culled)
-    if (e) cudaEventDestroy(e);
-  for (cudaEvent_t e : p->joined)
-    if (e) cudaEventDestroy(e);
-  cudaFree(p->counters);
-  *p = TracePipeline{};
-}
-
-bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
-
 int ensure_queue(pbrt_ctx* c) {
   if (c->queue && c->queue_rec && c->queue_dense.bases) return PBRT_OK;
   if (!c->queue) PBRT_TRY(c->cuda(cudaMalloc(&c->queue, sizeof(uint32_t) * kDevChunk), "cudaMalloc(survivor queue)"));
@@ -201,7 +161,6 @@ void pbrt_ctx_destroy(pbrt_ctx* c) {
   cudaFree(c->queue);
   cudaFree(c->queue_rec);
   free_dense(&c->queue_dense);
-  free_pipeline(&c->pipe);
   cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -678,21 +637,11 @@ int trace_impl(pbrt_scene* s, const float* rays, uint64_t n, uint32_t* prim, flo
     if (one_mesh && !occ && c->persistent && !counters) {
       // Chunks of at most kDevChunk rays bound the survivor queue (scratch) to 64 MiB.
       PBRT_TRY(ensure_queue(c));
-      int parts = 1, trav_blocks = 0;
-      trace_pipeline_shape(&parts, &trav_blocks);
-      const bool vec = n % 4 == 0 && aligned16(rays) && aligned16(prim) && aligned16(t) && (!obj || aligned16(obj));
-      if (parts > 1 && vec) PBRT_TRY(ensure_pipeline(c));
       for (uint64_t base = 0; base < n; base += kDevChunk) {
         const uint64_t m = std::min<uint64_t>(kDevChunk, n - base);
-        if (parts > 1 && vec)
-          PBRT_TRY(c->cuda(launch_mesh_closest_pipelined(mv, rays + base, n, m, prim + base, t + base,
-                                                         obj ? obj + base : nullptr, c->queue, c->queue_rec, c->d_err,
-                                                         c->sm_count, st, c->pipe, parts, trav_blocks),
-                           "kernel launch"));
-        else
-          PBRT_TRY(c->cuda(launch(rays + base, n, m, prim + base, t + base, obj ? obj + base : nullptr, nullptr,
-                                  nullptr, c->queue, c->d_counters + 4, c->queue_rec, st, &c->queue_dense),
-                           "kernel launch"));
+        PBRT_TRY(c->cuda(launch(rays + base, n, m, prim + base, t + base, obj ? obj + base : nullptr, nullptr, nullptr,
+                                c->queue, c->d_counters + 4, c->queue_rec, st, &c->queue_dense),
+                         "kernel launch"));
       }
     } else {
       PBRT_TRY(c->cuda(launch(rays, n, n, prim, t, obj, occ, counters, nullptr, nullptr, nullptr, st), "kernel launch"));

@@ -83,8 +83,6 @@ struct pbrt_ctx {
   uint32_t* queue = nullptr;                  // survivor queue for device-buffer calls (kDevChunk entries)
   float4* queue_rec = nullptr;                // and their ray records (kDevChunk x 32 bytes)
   pbrt::DenseScratch queue_dense;             // and the dense-result scratch for kDevChunk rays
-  pbrt::TracePipeline pipe;                   // streams, events and counters of the pipelined pass
-  bool pipe_ready = false;
   bool persistent = true;                     // persistent dynamic-fetch traversal (default)
   uint32_t* noalloc_scratch = nullptr;        // device address of pbrt_trace_closest_noalloc's static
                                               // scratch array on this device, looked up at creation

@@ -32,30 +32,6 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
                                            uint32_t* prim, float* t, uint32_t* obj, uint32_t* queue,
                                            unsigned long long* counters, uint32_t* err, int sm_count, cudaStream_t s,
                                            float4* rec = nullptr, const DenseScratch* dense = nullptr);
-// The two-stage pass over `n` rays in up to kPipeMaxParts parts, the cull of part j + 1
-// running beside the traversal of part j: culls on `cull` (the first with a full grid, the
-// rest with one block per SM), part j's traversal on trav[j % 2] after part j's cull, at
-// `trav_blocks_per_sm` resident blocks per SM so that a cull block fits beside them. Part j
-// uses queue / records from its first ray's index on, and counters 2j, 2j + 1 (zeroed on
-// `s`). `s` forks into the three streams through `fork` and waits for the ones it used
-// through `joined`; the plane stride must be a multiple of 4 and every pointer 16-byte aligned.
-// Stream ordering alone orders the parts (no kernel waits on another).
-constexpr int kPipeMaxParts = 16;
-struct TracePipeline {
-  cudaStream_t cull = nullptr;
-  cudaStream_t trav[2] = {nullptr, nullptr};
-  cudaEvent_t fork = nullptr;
-  cudaEvent_t culled[kPipeMaxParts] = {};
-  cudaEvent_t joined[3] = {nullptr, nullptr, nullptr};  // the cull stream, trav[0], trav[1]
-  unsigned long long* counters = nullptr;  // 2 * kPipeMaxParts words
-};
-cudaError_t launch_mesh_closest_pipelined(const MeshView& m, const float* rays, uint64_t stride, uint64_t n,
-                                          uint32_t* prim, float* t, uint32_t* obj, uint32_t* queue, float4* rec,
-                                          uint32_t* err, int sm_count, cudaStream_t s, const TracePipeline& p,
-                                          int parts, int trav_blocks_per_sm);
-// The part count and traversal blocks per SM of the pipelined pass on this build (1 part: the
-// plain two-stage pass); PBRT_TRACE_PARTS="K[,B]" overrides them for measurements.
-void trace_pipeline_shape(int* parts, int* trav_blocks_per_sm);
 // Allocation-free form of launch_mesh_closest_persistent for device buffers (plane stride
 // = n): its scratch is a file-scope __device__ array of kNoAllocMaxRays queue entries
 // shared by every call on a device. `scratch` is that array's device address on the current

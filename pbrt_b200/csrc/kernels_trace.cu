@@ -87,11 +87,8 @@ constexpr int kCullRays = 4;  // rays per thread and iteration
 // queue position of its first survivor; the queue itself is not needed (the traversal writes
 // results by queue position and k_dense_finalize maps them back to rays).
 static_assert(kDenseChunk == uint64_t(kCullThreads) * kCullRays, "a dense chunk is one cull block iteration");
-// Registers: the plain form is left unbounded (54: one block, 14,336 registers, fits beside
-// 10 resident traversal blocks in the pipelined pass; an explicit minimum of one block per SM
-// lets ptxas take 77); the dense form is bounded to 4 blocks per SM (64).
 template <bool kVec, bool kDense>
-__global__ void __launch_bounds__(kCullThreads, kDense ? 4 : 0) k_cull_root(MeshView m, const float* __restrict__ rays, uint64_t stride,
+__global__ void __launch_bounds__(kCullThreads, 4) k_cull_root(MeshView m, const float* __restrict__ rays, uint64_t stride,
                                                             uint64_t n, uint32_t* __restrict__ prim,
                                                             float* __restrict__ tout, uint32_t* __restrict__ obj,
                                                             uint32_t* __restrict__ queue,
@@ -714,99 +711,6 @@ cudaError_t noalloc_scratch_lookup(uint32_t** out) {
   if (e != cudaSuccess) return e;
   *out = static_cast<uint32_t*>(p);
   return cudaSuccess;
-}
-
-// Registers a block of `threads` threads holds on an SM (whole 256-register units per warp).
-static int block_registers(const void* fn, int threads) {
-  cudaFuncAttributes a{};
-  if (cudaFuncGetAttributes(&a, fn) != cudaSuccess) return 65536;
-  const int per_warp = (a.numRegs * 32 + 255) / 256 * 256;
-  return per_warp * ((threads + 31) / 32);
-}
-
-// Traversal blocks per SM for the pipelined pass: at most `want`, and few enough that one
-// cull block still fits in the SM's 65,536 registers beside them.
-static int pipelined_traversal_blocks(int want) {
-  static const int fit = [] {
-    const int cull = block_registers(reinterpret_cast<const void*>(k_cull_root<true, false>), kCullThreads);
-    const int trav = block_registers(reinterpret_cast<const void*>(k_mesh_closest_persistent<true, false>), 128);
-    const int f = (65536 - cull) / trav;
-    return f > 1 ? f : 1;
-  }();
-  const int full = persistent_blocks_per_sm<true>();
-  int b = want < fit ? want : fit;
-  return b < full ? b : full;
-}
-
-void trace_pipeline_shape(int* parts, int* trav_blocks_per_sm) {
-  static const int2 v = [] {
-    int2 d = make_int2(1, 10);
-    if (traversal_schedule().dense) return d;  // the dense result pass runs unpipelined
-    if (const char* e = std::getenv("PBRT_TRACE_PARTS")) {
-      int a = 0, b = 0;
-      const int got = std::sscanf(e, "%d,%d", &a, &b);
-      if (got >= 1 && a >= 1 && a <= kPipeMaxParts) d.x = a;
-      if (got == 2 && b >= 1 && b <= 16) d.y = b;
-    }
-    return d;
-  }();
-  *parts = v.x;
-  *trav_blocks_per_sm = v.y;
-}
-
-cudaError_t launch_mesh_closest_pipelined(const MeshView& m, const float* rays, uint64_t stride, uint64_t n,
-                                          uint32_t* prim, float* t, uint32_t* obj, uint32_t* queue, float4* rec,
-                                          uint32_t* err, int sm_count, cudaStream_t s, const TracePipeline& p,
-                                          int parts, int trav_blocks_per_sm) {
-  if (n == 0) return cudaSuccess;
-  if (parts < 1 || parts > kPipeMaxParts || stride % 4 != 0) return cudaErrorInvalidValue;
-  // parts of whole 1,024-ray blocks, so every part starts 16-byte aligned
-  const uint64_t per = ((n + parts - 1) / parts + kDenseChunk - 1) / kDenseChunk * kDenseChunk;
-  const int np = int((n + per - 1) / per);
-  const TraversalSchedule ts = traversal_schedule();
-  const int tb = pipelined_traversal_blocks(trav_blocks_per_sm);
-  cudaError_t e = cudaMemsetAsync(p.counters, 0, 2 * sizeof(unsigned long long) * np, s);
-  if (e == cudaSuccess) e = cudaEventRecord(p.fork, s);
-  if (e == cudaSuccess) e = cudaStreamWaitEvent(p.cull, p.fork, 0);
-  for (int j = 0; j < np && e == cudaSuccess; ++j) {
-    const uint64_t b = uint64_t(j) * per, mj = n - b < per ? n - b : per;
-    unsigned long long* cnt = p.counters + 2 * j;
-    const uint64_t per_block = uint64_t(kCullThreads) * kCullRays;
-    const uint64_t cull_need = (mj + per_block - 1) / per_block;
-    const uint64_t cull_cap = uint64_t(sm_count) * (j == 0 ? 8 : 1);
-    const unsigned cg = unsigned(cull_need < cull_cap ? cull_need : cull_cap);
-    k_cull_root<true, false><<<cg, kCullThreads, 0, p.cull>>>(m, rays + b, stride, mj, prim + b, t + b,
-                                                               obj ? obj + b : nullptr, queue + b, cnt, rec + 2 * b,
-                                                               nullptr, nullptr);
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaEventRecord(p.culled[j], p.cull);
-    cudaStream_t ts_j = p.trav[j & 1];
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(ts_j, p.culled[j], 0);
-    if (e != cudaSuccess) break;
-    const uint64_t need = (mj + 127) / 128, cap = uint64_t(sm_count) * tb;
-    const unsigned g = unsigned(need < cap ? need : cap);
-    if (ts.voted)
-      k_mesh_closest_persistent<true, false><<<g, 128, 0, ts_j>>>(m, rays + b, stride, queue + b, cnt, prim + b,
-                                                                  t + b, obj ? obj + b : nullptr, cnt + 1, err,
-                                                                  rec + 2 * b, ts.leaf_min, ts.refill_min, ts.burst,
-                                                                  nullptr);
-    else
-      k_mesh_closest_ww<true><<<g, 128, 0, ts_j>>>(m, rays + b, stride, queue + b, cnt, prim + b, t + b,
-                                                   obj ? obj + b : nullptr, cnt + 1, err, rec + 2 * b);
-    e = cudaGetLastError();
-  }
-  // join: the caller's stream waits for the cull stream and each traversal stream this call
-  // used (a stream under capture may wait only on work captured with it); also after a
-  // failed launch, so no stream is left forked
-  const cudaError_t rc = cudaEventRecord(p.joined[0], p.cull);
-  const cudaError_t wc = rc == cudaSuccess ? cudaStreamWaitEvent(s, p.joined[0], 0) : rc;
-  if (e == cudaSuccess) e = wc;
-  for (int k = 0; k < 2 && k < np; ++k) {
-    const cudaError_t r1 = cudaEventRecord(p.joined[1 + k], p.trav[k]);
-    const cudaError_t r2 = r1 == cudaSuccess ? cudaStreamWaitEvent(s, p.joined[1 + k], 0) : r1;
-    if (e == cudaSuccess) e = r2;
-  }
-  return e;
 }
 
 cudaError_t launch_mesh_closest_noalloc(const MeshView& m, const float* rays, uint64_t n, uint32_t* prim, float* t,

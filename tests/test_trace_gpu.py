@@ -162,7 +162,7 @@ v, f = W.displaced_icosphere(6, seed=41)
 s = pb.Scene()
 s.add_object(pb.Simple(pb.TriangleMesh(v, f)))
 s = s.commit(bvh_bins=16, bvh_max_leaf=4)
-n = (1 << 21) + 4  # device buffers: 2,049 chunks of 1,024 rays, the last one of 4
+n = (1 << 21) + 1028  # device buffers: 2,050 chunks of 1,024 rays, the last one of 4
 rays = W.incoherent_rays(n, v.min(0), v.max(0), seed=42)
 rng = np.random.default_rng(43)
 aim = rays[:, : 1 << 18]
@@ -173,29 +173,19 @@ np.savez({out!r}, rays=rays, dp=dp.cpu().numpy().view(np.uint32), dt=dt.cpu().nu
 """
 
 
-_FORMS = {
-    "scattered, one part": {"PBRT_TRACE_DENSE": "0", "PBRT_TRACE_PARTS": "1"},
-    "dense results": {"PBRT_TRACE_DENSE": "1"},
-    "pipelined, 3 parts": {"PBRT_TRACE_DENSE": "0", "PBRT_TRACE_PARTS": "3"},
-    "pipelined, 16 parts, 2 traversal blocks per SM": {"PBRT_TRACE_DENSE": "0", "PBRT_TRACE_PARTS": "16,2"},
-}
-
-
-@pytest.mark.parametrize("form", list(_FORMS))
-def test_two_stage_forms_match_oracle(tmp_path, form):
-    """Every form of the two-stage pass gives the oracle's ids and t, on device buffers with a
-    partial last chunk and on host buffers: the cull's miss answers plus scattered hit stores;
-    the survivor bitmask, results by queue slot and the ray-order pass; and the pipelined
-    pass (the rays in parts, a part's cull beside the previous part's traversal; 2,097,156
-    rays in 3 parts are 699,392 + 699,392 + 698,372). The switches are read once per
-    process: a child per form."""
+@pytest.mark.parametrize("dense", ["0", "1"])
+def test_dense_result_pass_matches_oracle(tmp_path, dense):
+    """Both result forms of the two-stage pass (the cull's miss answers plus scattered hit
+    stores, or the survivor bitmask, results by queue slot and the ray-order pass) give the
+    oracle's ids and t, on device buffers with a partial last chunk and on host buffers. The
+    switch is read once per process: a child per form."""
     import os
     import subprocess
     import sys
 
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    out = str(tmp_path / "form.npz")
-    env = dict(os.environ, **_FORMS[form])
+    out = str(tmp_path / f"dense_{dense}.npz")
+    env = dict(os.environ, PBRT_TRACE_DENSE=dense)
     subprocess.run([sys.executable, "-c", _DENSE_SCRIPT.format(root=root, out=out)], env=env, check=True,
                    timeout=600)
     z = np.load(out)
