@@ -87,8 +87,10 @@ constexpr int kCullRays = 4;  // rays per thread and iteration
 // queue position of its first survivor; the queue itself is not needed (the traversal writes
 // results by queue position and k_dense_finalize maps them back to rays).
 static_assert(kDenseChunk == uint64_t(kCullThreads) * kCullRays, "a dense chunk is one cull block iteration");
+// Registers: the plain form is left unbounded (54; an explicit minimum of one block per SM
+// lets ptxas take 77); the dense form is bounded to 4 blocks per SM (64 instead of 78).
 template <bool kVec, bool kDense>
-__global__ void __launch_bounds__(kCullThreads, 4) k_cull_root(MeshView m, const float* __restrict__ rays, uint64_t stride,
+__global__ void __launch_bounds__(kCullThreads, kDense ? 4 : 0) k_cull_root(MeshView m, const float* __restrict__ rays, uint64_t stride,
                                                             uint64_t n, uint32_t* __restrict__ prim,
                                                             float* __restrict__ tout, uint32_t* __restrict__ obj,
                                                             uint32_t* __restrict__ queue,
