@@ -173,19 +173,29 @@ np.savez({out!r}, rays=rays, dp=dp.cpu().numpy().view(np.uint32), dt=dt.cpu().nu
 """
 
 
-@pytest.mark.parametrize("dense", ["0", "1"])
-def test_dense_result_pass_matches_oracle(tmp_path, dense):
-    """Both result forms of the two-stage pass (the cull's miss answers plus scattered hit
-    stores, or the survivor bitmask, results by queue slot and the ray-order pass) give the
-    oracle's ids and t, on device buffers with a partial last chunk and on host buffers. The
-    switch is read once per process: a child per form."""
+_FORMS = {
+    "default": {},
+    "dense results": {"PBRT_TRACE_DENSE": "1"},
+    "ordered queue": {"PBRT_TRACE_ORDER": "1"},
+    "drained-queue schedule": {"PBRT_TRACE_SCHEDULE": "8,8,8,1,2"},
+}
+
+
+@pytest.mark.parametrize("form", list(_FORMS))
+def test_two_stage_forms_match_oracle(tmp_path, form):
+    """Every form of the two-stage pass gives the oracle's ids and t, on device buffers with a
+    partial last chunk and on host buffers: the cull's miss answers plus scattered hit stores;
+    the survivor bitmask, results by queue slot and the ray-order pass; the queue ordered
+    (likely-long survivors from the front, the rest from the back); another schedule once the
+    queue is drained. The switches are read once per process: a child per form."""
     import os
     import subprocess
     import sys
 
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    out = str(tmp_path / f"dense_{dense}.npz")
-    env = dict(os.environ, PBRT_TRACE_DENSE=dense)
+    out = str(tmp_path / "form.npz")
+    env = {k: v for k, v in os.environ.items() if not k.startswith("PBRT_TRACE_")}
+    env.update(_FORMS[form])
     subprocess.run([sys.executable, "-c", _DENSE_SCRIPT.format(root=root, out=out)], env=env, check=True,
                    timeout=600)
     z = np.load(out)
