@@ -60,7 +60,7 @@ int ensure_slots(pbrt_ctx* c) {
     PBRT_TRY(c->cuda(cudaMalloc(&s.queue, sizeof(uint32_t) * kSlotRays), "cudaMalloc(staging)"));
     PBRT_TRY(c->cuda(cudaMalloc(&s.rec, sizeof(float4) * 2 * kSlotRays), "cudaMalloc(staging)"));
     PBRT_TRY(alloc_dense(c, &s.dense, kSlotRays));
-    PBRT_TRY(c->cuda(cudaMalloc(&s.fetch, 3 * sizeof(unsigned long long)), "cudaMalloc(staging)"));
+    PBRT_TRY(c->cuda(cudaMalloc(&s.fetch, 2 * sizeof(unsigned long long)), "cudaMalloc(staging)"));
   }
   c->slots_ready = true;
   return PBRT_OK;

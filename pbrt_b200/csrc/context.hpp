@@ -57,7 +57,7 @@ struct Slot {
   uint32_t* queue = nullptr;            // survivor queue of the two-stage nearest-hit pass
   float4* rec = nullptr;                // the survivors' ray records (32 bytes each)
   pbrt::DenseScratch dense;             // dense results: per-slot (id, t), survivor bitmask, chunk bases
-  unsigned long long* fetch = nullptr;  // [queue length, fetch position, back-end length] of that pass
+  unsigned long long* fetch = nullptr;  // [queue length, fetch position] of that pass
 };
 
 // The wave's SoA state, grown on demand (one per context for pbrt_render / pbrt_render_cached,
@@ -78,7 +78,7 @@ struct pbrt_ctx {
   cudaStream_t user = nullptr;    // caller's stream (asynchronous device-buffer calls)
   std::string err;
   uint32_t* d_err = nullptr;
-  unsigned long long* d_counters = nullptr;  // [0..2] traversal counters, [4..6] queue length / fetch position / back-end length,
+  unsigned long long* d_counters = nullptr;  // [0..2] traversal counters, [4..5] queue length / fetch position,
                                              // [8..10] rays / shadow rays / paths of the last render
   uint32_t* queue = nullptr;                  // survivor queue for device-buffer calls (kDevChunk entries)
   float4* queue_rec = nullptr;                // and their ray records (kDevChunk x 32 bytes)

@@ -15,8 +15,8 @@ cudaError_t launch_mesh_closest(const MeshView& m, const float* rays, uint64_t s
                                 cudaStream_t s);
 // Two-stage nearest hit: a streaming root-box cull that answers misses and compacts the
 // survivors' indices into `queue` (scratch, capacity >= n, n < 2^32), then the persistent
-// dynamic-fetch traversal over the queue. `counters` is three 64-bit words of scratch (queue
-// length, fetch position, length of the queue's back end), zeroed on `s` by the launcher. `rec` (optional scratch, 2 x n
+// dynamic-fetch traversal over the queue. `counters` is two 64-bit words of scratch (queue
+// length, fetch position), zeroed on `s` by the launcher. `rec` (optional scratch, 2 x n
 // float4): the survivors' rays copied beside their queue entries, read back coalesced.
 // Dense results (optional scratch, with `rec`): the cull writes no miss answers but a survivor
 // bitmask per ray (`mask`, n/32 words) and the queue position of each 1,024-ray chunk's first

@@ -96,17 +96,11 @@ __global__ void __launch_bounds__(kCullThreads, kDense ? 4 : 0) k_cull_root(Mesh
                                                             uint32_t* __restrict__ queue,
                                                             unsigned long long* __restrict__ queue_count,
                                                             float4* __restrict__ rec, uint32_t* __restrict__ mask,
-                                                            uint32_t* __restrict__ bases,
-                                                            unsigned long long* __restrict__ graze_count) {
+                                                            uint32_t* __restrict__ bases) {
   __shared__ uint32_t warp_off[2][kCullThreads / 32];
-  __shared__ unsigned long long blk_base[2], blk_graze[2];
+  __shared__ unsigned long long blk_base[2];
   const float4 rlo = __ldg(&m.nodes[0]);
   const float4 rhi = __ldg(&m.nodes[1]);
-  // queue order (graze_count given): survivors whose line passes within the sphere inscribed
-  // in the root box (likely long walks) from slot 0 up, the others from slot n - 1 down
-  const bool order = !kDense && graze_count != nullptr;
-  const float cx = 0.5f * (rlo.x + rhi.x), cy = 0.5f * (rlo.y + rhi.y), cz = 0.5f * (rlo.z + rhi.z);
-  const float rad = 0.5f * fminf(fminf(rhi.x - rlo.x, rhi.y - rlo.y), rhi.z - rlo.z), rad2 = rad * rad;
   const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint64_t per_iter = uint64_t(gridDim.x) * kCullThreads * kCullRays;
   const uint64_t iters = (n + per_iter - 1) / per_iter;  // uniform across the grid: __syncthreads is safe
@@ -126,23 +120,14 @@ __global__ void __launch_bounds__(kCullThreads, kDense ? 4 : 0) k_cull_root(Mesh
 #pragma unroll
         for (int j = 0; j < kCullRays; ++j) v[p][j] = (i0 + j < n) ? __ldcs(rays + p * stride + i0 + j) : 0.f;
     }
-    unsigned enter = 0, central = 0;
+    unsigned enter = 0;
 #pragma unroll
     for (int j = 0; j < kCullRays; ++j) {
       if (i0 + j < n) {
         float entry;
         const PRay r = prepare_ray(mk3(v[0][j], v[1][j], v[2][j]), mk3(v[3][j], v[4][j], v[5][j]));
         // entered, and not dropped at its first pop for entry >= min_t = FLT_MAX (bvh.rs:462-472)
-        if (box_hit(r, rlo, rhi, v[6][j], v[7][j], entry) && entry < FLT_MAX) {
-          enter |= 1u << j;
-          if (order) {  // |(c - o) x d|^2 <= rad^2 |d|^2: an ordering hint only, no effect on answers
-            const float wx = cx - v[0][j], wy = cy - v[1][j], wz = cz - v[2][j];
-            const float ex = wy * v[5][j] - wz * v[4][j], ey = wz * v[3][j] - wx * v[5][j],
-                        ez = wx * v[4][j] - wy * v[3][j];
-            const float dd = v[3][j] * v[3][j] + v[4][j] * v[4][j] + v[5][j] * v[5][j];
-            if (ex * ex + ey * ey + ez * ez <= rad2 * dd) central |= 1u << j;
-          }
-        }
+        if (box_hit(r, rlo, rhi, v[6][j], v[7][j], entry) && entry < FLT_MAX) enter |= 1u << j;
       }
     }
     const uint64_t chunk = it * gridDim.x + blockIdx.x;
@@ -166,9 +151,8 @@ __global__ void __launch_bounds__(kCullThreads, kDense ? 4 : 0) k_cull_root(Mesh
           if (obj) __stcs(obj + i0 + j, 0xFFFFFFFFu);
         }
     }
-    // Block-wide exclusive scan of the survivor counts: one atomicAdd per block (per end of
-    // the queue when ordering; the two counts packed in 16-bit halves, at most 1,024 each).
-    const uint32_t c = order ? (__popc(central) | (__popc(enter & ~central) << 16)) : __popc(enter);
+    // Block-wide exclusive scan of the survivor counts: one atomicAdd per block.
+    const uint32_t c = __popc(enter);
     uint32_t incl = c;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -185,33 +169,20 @@ __global__ void __launch_bounds__(kCullThreads, kDense ? 4 : 0) k_cull_root(Mesh
         warp_off[buf][w] = run;
         run += t;
       }
-      if (order) {
-        const uint32_t rc = run & 0xFFFFu, rg = run >> 16;
-        blk_base[buf] = rc ? atomicAdd(queue_count, (unsigned long long)rc) : 0ull;
-        blk_graze[buf] = rg ? atomicAdd(graze_count, (unsigned long long)rg) : 0ull;
-      } else {
-        blk_base[buf] = run ? atomicAdd(queue_count, (unsigned long long)run) : 0ull;
-      }
+      blk_base[buf] = run ? atomicAdd(queue_count, (unsigned long long)run) : 0ull;
       if (kDense && chunk * kDenseChunk < n) bases[chunk] = uint32_t(blk_base[buf]);
     }
     __syncthreads();
-    const uint32_t off = warp_off[buf][warp] + (incl - c);
-    uint64_t pos = blk_base[buf] + (order ? (off & 0xFFFFu) : off);
-    uint64_t gpos = order ? n - 1 - (blk_graze[buf] + (off >> 16)) : 0;  // counts down
+    uint64_t pos = blk_base[buf] + warp_off[buf][warp] + (incl - c);
 #pragma unroll
     for (int j = 0; j < kCullRays; ++j)
       if (enter & (1u << j)) {
-        const bool front = !order || (central & (1u << j));
-        const uint64_t slot = front ? pos : gpos;
         if (rec) {  // read back soon by stage 2: default caching, the planes stream past
-          rec[2 * slot] = make_float4(v[0][j], v[1][j], v[2][j], v[6][j]);
-          rec[2 * slot + 1] = make_float4(v[3][j], v[4][j], v[5][j], v[7][j]);
+          rec[2 * pos] = make_float4(v[0][j], v[1][j], v[2][j], v[6][j]);
+          rec[2 * pos + 1] = make_float4(v[3][j], v[4][j], v[5][j], v[7][j]);
         }
-        if (!kDense) queue[slot] = uint32_t(i0 + j);
-        if (front)
-          ++pos;
-        else
-          --gpos;
+        if (!kDense) queue[pos] = uint32_t(i0 + j);
+        ++pos;
       }
   }
 }
@@ -405,14 +376,11 @@ __global__ void __launch_bounds__(128, PBRT_TRAVERSAL_MIN_BLOCKS) k_mesh_closest
     MeshView m, const float* __restrict__ rays, uint64_t stride, const uint32_t* __restrict__ queue,
     const unsigned long long* __restrict__ queue_count, uint32_t* __restrict__ prim, float* __restrict__ tout,
     uint32_t* __restrict__ obj, unsigned long long* __restrict__ next_ray, uint32_t* __restrict__ err,
-    const float4* __restrict__ rec, int leaf_min, int refill_min, int burst, uint2* __restrict__ res,
-    const unsigned long long* __restrict__ graze_count, uint64_t back) {
+    const float4* __restrict__ rec, int leaf_min, int refill_min, int burst, uint2* __restrict__ res) {
   static_assert(kRec || !kDense, "dense results need the ray records");
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
-  // queue order (graze_count given): fetch k < nc is slot k, the rest count down from `back`
-  const uint64_t nc = *queue_count;
-  const uint64_t n = nc + (graze_count ? *graze_count : 0ull);
+  const uint64_t n = *queue_count;
   bool active = false, exhausted = false;  // exhausted is warp-uniform
   uint32_t idx = 0;
   PRay r;
@@ -435,11 +403,10 @@ __global__ void __launch_bounds__(128, PBRT_TRAVERSAL_MIN_BLOCKS) k_mesh_closest
       if (!active) {
         const uint64_t k = base + __popc(idle & lt_mask);
         if (k < n) {
-          const uint64_t slot = k < nc ? k : back - (k - nc);
-          idx = kDense ? uint32_t(k) : __ldg(queue + slot);  // dense: the queue slot (results go there)
+          idx = kDense ? uint32_t(k) : __ldg(queue + k);  // dense: the queue slot (results go there)
           F3 o, d;
           if (kRec) {  // the copy stage 1 wrote: consecutive lanes read consecutive records
-            const float4 a = __ldcs(rec + 2 * slot), b = __ldcs(rec + 2 * slot + 1);
+            const float4 a = __ldcs(rec + 2 * k), b = __ldcs(rec + 2 * k + 1);
             o = mk3(a.x, a.y, a.z);
             d = mk3(b.x, b.y, b.z);
             near = a.w;
@@ -547,18 +514,21 @@ __global__ void __launch_bounds__(128, PBRT_TRAVERSAL_MIN_BLOCKS) k_mesh_closest
 // lanes of a warp stand on a leaf, a refill once `refill_min` lanes are idle and up to
 // `burst` interior nodes per node step (default 8, 8, 8: 0.913 ms per 16,777,216-ray step
 // against 1.021 ms for the while-while kernel and 1.052 ms for single-node steps), or the
-// while-while kernel (voted = false). PBRT_TRACE_SCHEDULE="ww" or
-// "leaf_min,refill_min[,burst[,tail_leaf_min[,tail_burst]]]" (each in 1..32; the tail values
-// apply once the queue is drained) overrides it for measurements; results do not depend on it. `dense` (PBRT_TRACE_DENSE=1, when the caller gives its scratch): the
+// while-while kernel (voted = false). Once the queue is drained no refill can come, and a
+// lane waiting on a leaf only lengthens the tail: there a leaf step is taken as soon as one
+// lane stands on a leaf (tail_leaf_min 1: 1.7 % faster than keeping 8).
+// PBRT_TRACE_SCHEDULE="ww" or "leaf_min,refill_min[,burst[,tail_leaf_min[,tail_burst]]]"
+// (each in 1..32; without tail values the bulk's apply) overrides it for measurements;
+// results do not depend on it. `dense` (PBRT_TRACE_DENSE=1, when the caller gives its scratch): the
 // voted kernel's results go out through the dense pass instead of the cull's miss answers
 // plus scattered hit stores. On the 16,777,216-ray step it cuts DRAM traffic from 997 MB to
 // 851 MB but takes 0.923-0.926 ms against 0.916-0.920 ms: the cull saves 18 us by writing
 // no answers, the ray-order pass costs 37 us, and the hit stores it replaces were hidden
 // under the issue-bound traversal.
 struct TraversalSchedule {
-  bool voted = true, dense = false, order = false;
+  bool voted = true, dense = false;
   int leaf_min = 8, refill_min = 8, burst = 8;
-  int tail_leaf_min = 8, tail_burst = 8;  // once the queue is drained (no refill can come)
+  int tail_leaf_min = 1, tail_burst = 8;  // once the queue is drained (no refill can come)
   int leaf_arg() const { return leaf_min | (tail_leaf_min << 8); }
   int burst_arg() const { return burst | (tail_burst << 8); }
 };
@@ -580,7 +550,6 @@ static TraversalSchedule traversal_schedule() {
       }
     }
     if (const char* e = std::getenv("PBRT_TRACE_DENSE")) d.dense = std::strcmp(e, "1") == 0;
-    if (const char* e = std::getenv("PBRT_TRACE_ORDER")) d.order = std::strcmp(e, "1") == 0;
     return d;
   }();
   return v;
@@ -688,7 +657,7 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
                                            float4* rec, const DenseScratch* dense) {
   if (n == 0) return cudaSuccess;
   const int blocks_per_sm = persistent_blocks_per_sm<true>();
-  cudaError_t e = cudaMemsetAsync(counters, 0, 3 * sizeof(unsigned long long), s);
+  cudaError_t e = cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;
   const bool vec = stride % 4 == 0 && aligned16(rays) && aligned16(prim) && aligned16(t) && (!obj || aligned16(obj));
   const uint64_t per_block = uint64_t(kCullThreads) * kCullRays;
@@ -702,21 +671,19 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
     // dense results: cull (bitmask, chunk bases, records), traversal (results by queue slot),
     // then every ray's answer in ray order
     k_cull_root<true, true><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec,
-                                                         dense->mask, dense->bases, nullptr);
+                                                         dense->mask, dense->bases);
     k_mesh_closest_persistent<true, true><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj,
                                                             counters + 1, err, rec, ts.leaf_arg(), ts.refill_min,
-                                                            ts.burst_arg(), dense->res, nullptr, 0);
+                                                            ts.burst_arg(), dense->res);
     k_dense_finalize<true><<<cg, kCullThreads, 0, s>>>(dense->res, dense->mask, dense->bases, n, prim, t, obj);
     return cudaGetLastError();
   }
-  // queue order: the voted kernel with records only (counters[2] counts the back of the queue)
-  unsigned long long* graze = ts.order && ts.voted && rec ? counters + 2 : nullptr;
   if (vec)
     k_cull_root<true, false><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec,
-                                                          nullptr, nullptr, graze);
+                                                          nullptr, nullptr);
   else
     k_cull_root<false, false><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec,
-                                                           nullptr, nullptr, graze);
+                                                           nullptr, nullptr);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (!ts.voted) {
@@ -728,11 +695,11 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
   } else if (rec) {
     k_mesh_closest_persistent<true, false><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj,
                                                              counters + 1, err, rec, ts.leaf_arg(), ts.refill_min,
-                                                             ts.burst_arg(), nullptr, graze, n - 1);
+                                                             ts.burst_arg(), nullptr);
   } else {
     k_mesh_closest_persistent<false, false><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj,
                                                               counters + 1, err, nullptr, ts.leaf_arg(), ts.refill_min,
-                                                              ts.burst_arg(), nullptr, nullptr, 0);
+                                                              ts.burst_arg(), nullptr);
   }
   return cudaGetLastError();
 }
@@ -777,10 +744,10 @@ cudaError_t launch_mesh_closest_noalloc(const MeshView& m, const float* rays, ui
   const unsigned cg = unsigned(cull_need < cull_cap ? cull_need : cull_cap);
   if (vec)
     k_cull_root<true, false><<<cg, kCullThreads, 0, s>>>(m, rays, n, n, prim, t, nullptr, queue, counters, nullptr,
-                                                          nullptr, nullptr, nullptr);
+                                                          nullptr, nullptr);
   else
     k_cull_root<false, false><<<cg, kCullThreads, 0, s>>>(m, rays, n, n, prim, t, nullptr, queue, counters, nullptr,
-                                                           nullptr, nullptr, nullptr);
+                                                           nullptr, nullptr);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const uint64_t full = uint64_t(sm_count) * blocks_per_sm;
@@ -793,7 +760,7 @@ cudaError_t launch_mesh_closest_noalloc(const MeshView& m, const float* rays, ui
   else
     k_mesh_closest_persistent<false, false><<<g, 128, 0, s>>>(m, rays, n, queue, counters, prim, t, nullptr,
                                                               counters + 1, err, nullptr, ts.leaf_arg(), ts.refill_min,
-                                                              ts.burst_arg(), nullptr, nullptr, 0);
+                                                              ts.burst_arg(), nullptr);
   return cudaGetLastError();
 }
 

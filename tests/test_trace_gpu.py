@@ -176,8 +176,8 @@ np.savez({out!r}, rays=rays, dp=dp.cpu().numpy().view(np.uint32), dt=dt.cpu().nu
 _FORMS = {
     "default": {},
     "dense results": {"PBRT_TRACE_DENSE": "1"},
-    "ordered queue": {"PBRT_TRACE_ORDER": "1"},
-    "drained-queue schedule": {"PBRT_TRACE_SCHEDULE": "8,8,8,1,2"},
+    "drained-queue schedule as the bulk's": {"PBRT_TRACE_SCHEDULE": "8,8,8"},
+    "drained-queue schedule 1, 2": {"PBRT_TRACE_SCHEDULE": "8,8,8,1,2"},
 }
 
 
@@ -185,9 +185,8 @@ _FORMS = {
 def test_two_stage_forms_match_oracle(tmp_path, form):
     """Every form of the two-stage pass gives the oracle's ids and t, on device buffers with a
     partial last chunk and on host buffers: the cull's miss answers plus scattered hit stores;
-    the survivor bitmask, results by queue slot and the ray-order pass; the queue ordered
-    (likely-long survivors from the front, the rest from the back); another schedule once the
-    queue is drained. The switches are read once per process: a child per form."""
+    the survivor bitmask, results by queue slot and the ray-order pass; other schedules once
+    the queue is drained. The switches are read once per process: a child per form."""
     import os
     import subprocess
     import sys
