@@ -481,6 +481,7 @@ def batch_race(pb, W, ctx, device):
     batch.close()
     best = min(frames, key=max)
     frame_ms = max(best)
+    pers = _persistent_frame(ctx, scenes, params, samples, frame_ms)
     # the same scenes one after another, each its own pbrt_render, in the batch's order
     # (cheapest first: pixels x spp x max depth)
     stream = torch.cuda.current_stream()
@@ -517,6 +518,7 @@ def batch_race(pb, W, ctx, device):
                        "note": "same scenes, tuning and order (cheapest first), one pbrt_render each "
                                "(launches not captured)"},
         "speedup_aggregate": round(cum[-1] / frame_ms, 3),
+        "persistent": pers,
         "tuning": {k: tune[k] for k in ("leaf", "wave_paths", "trace_threads", "trace_blocks_per_sm",
                                           "shade_threads", "shade_blocks_per_sm")},
         "autotune": {"trials": len(tune["trials"]), "sample_scenes": tune["sample_scenes"], "seconds": round(tune_s, 1)},
@@ -525,6 +527,27 @@ def batch_race(pb, W, ctx, device):
                     "note": "host: BVHs on all host cores (pbrt_scene_create_many); gpu: device_build, the "
                             "same trees; both include the uploads"},
     }
+
+
+def _persistent_frame(ctx, scenes, params, samples, wavefront_ms):
+    """The same batch frame as one persistent launch (pbrt_ctx_set_batch_kernel): best of two
+    frames after a warm-up, each scene's completion on the GPU clock."""
+    from pbrt_b200.scene import Batch
+
+    ctx.set_batch_kernel("persistent")
+    try:
+        batch = Batch(scenes, params, ctx)
+        none = [None] * len(scenes)
+        batch.render(0, none)
+        frames = [batch.render(f, none, scene_times=True)[1] for f in (1, 2)]
+        batch.close()
+    finally:
+        ctx.set_batch_kernel("wavefront")
+    best = min(frames, key=max)
+    return {"frame_ms": round(max(best), 3), "samples_per_s": round(samples / (max(best) * 1e-3), 1),
+            "scene_latency_ms": {"mean": round(float(np.mean(best)), 3), "max": round(float(max(best)), 3)},
+            "speedup_vs_wavefront_batch": round(wavefront_ms / max(best), 3),
+            "kernel": "k_batch_paths: one launch, each lane runs a path to its end and takes the next"}
 
 
 def batch_small(pb, W, ctx, device, n=64, width=128, height=128):
@@ -545,6 +568,7 @@ def batch_small(pb, W, ctx, device, n=64, width=128, height=128):
     frames = [batch.render(f, none, scene_times=True)[1] for f in (1, 2)]
     batch.close()
     best = min(frames, key=max)
+    pers = _persistent_frame(ctx, scenes, params, samples, max(best))
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     cost = [cam["width"] * cam["height"] * spp * 8 for _, cam, spp in specs]
@@ -572,7 +596,8 @@ def batch_small(pb, W, ctx, device, n=64, width=128, height=128):
                            "scene_latency_ms": {"mean": round(float(np.mean(done)), 3), "max": round(total, 3)},
                            "note": "one pbrt_render each, cheapest first, back to back on one stream"},
             "speedup_aggregate": round(total / max(best), 3),
-            "speedup_mean_latency": round(float(np.mean(done)) / float(np.mean(best)), 3)}
+            "speedup_mean_latency": round(float(np.mean(done)) / float(np.mean(best)), 3),
+            "persistent": pers}
 
 
 MLP_FLOP_PER_QUERY = 2 * (96 * 64 + 4 * 64 * 64 + 64 * 3)  # 45,440: forward multiply-adds x 2

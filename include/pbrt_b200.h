@@ -449,9 +449,10 @@ int pbrt_ctx_get_tuning(pbrt_ctx* ctx, pbrt_tuning* tuning);
 
 /* Many scenes rendered together (no counterpart in the reference, whose renderer takes one
  * scene): the paths of all scenes share the waves, queues and kernel launches of one
- * wavefront, scene by scene, cheapest first (pixels x spp x max depth; ties keep the given
- * order, which minimises the frame's mean completion time), and the launch sequence of one
- * frame is recorded once in a CUDA graph that pbrt_batch_render replays. The scenes must
+ * wavefront (or one persistent launch, pbrt_ctx_set_batch_kernel), scene by scene, cheapest
+ * first (pixels x spp x max depth; ties keep the given order, which minimises the frame's
+ * mean completion time), and the launch sequence of one frame is recorded once in a CUDA
+ * graph that pbrt_batch_render replays. The scenes must
  * belong to ctx and outlive the batch; params[i] (integrator path or naive) renders
  * scenes[i]; films and times are reported per caller index i. */
 typedef struct pbrt_batch pbrt_batch;
@@ -460,9 +461,17 @@ int pbrt_batch_create(pbrt_ctx* ctx, pbrt_scene* const* scenes, const pbrt_rende
 /* Frame `frame`: scene i takes samples sample_offset + frame * spp ... + spp - 1 of every
  * pixel. films[i] (host or device, scene i's film size; films or films[i] may be NULL)
  * receives the mean radiance. scene_ms (optional, n floats): device milliseconds from the
- * frame's start until the wave holding scene i's last paths finished. */
+ * frame's start until the wave holding scene i's last paths finished (persistent batches:
+ * until its last path finished). */
 int pbrt_batch_render(pbrt_batch* batch, uint32_t frame, double* const* films, float* scene_ms);
 void pbrt_batch_destroy(pbrt_batch* batch);
+/* How batches created afterwards run a frame. PBRT_BATCH_WAVEFRONT (the default): waves of
+ * paths through the wavefront's queues, one kernel per stage and bounce. PBRT_BATCH_PERSISTENT:
+ * one persistent launch in which each warp lane runs a path to its end (nearest hit, shading,
+ * shadow ray, film) and takes the next; scene_ms then comes from the GPU clock at the moment a
+ * scene's last path finished. Films are the same either way. */
+enum { PBRT_BATCH_WAVEFRONT = 0, PBRT_BATCH_PERSISTENT = 1 };
+int pbrt_ctx_set_batch_kernel(pbrt_ctx* ctx, int kind);
 /* pbrt_batch_create + pbrt_batch_render(frame 0) + pbrt_batch_destroy. */
 int pbrt_render_batch(pbrt_scene* const* scenes, const pbrt_render_params* params, uint32_t n, double* const* films);
 

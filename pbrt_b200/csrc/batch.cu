@@ -1,10 +1,12 @@
-// batch.cu — many scenes rendered by one wavefront, its launch sequence recorded once in a
-// CUDA graph (pbrt_batch_* in include/pbrt_b200.h). Host code; the kernels are the wavefront
-// kernels of kernels_render.cu over the batch table.
+// batch.cu — many scenes rendered together, one frame's launches recorded once in a CUDA graph
+// (pbrt_batch_* in include/pbrt_b200.h): by one wavefront over the batch table (the wavefront
+// kernels of kernels_render.cu), or by one persistent launch that runs every path to its end
+// (k_batch_paths). Host code.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "../../include/pbrt_b200.h"
@@ -27,6 +29,9 @@ struct pbrt_batch {
   WaveAlloc wave;
   uint32_t wave_paths = 0, max_depth = 0;
   bool any_path = false;
+  bool persistent = false;                 // one persistent launch instead of the wavefront
+  unsigned long long* d_scratch = nullptr;  // its fetch position, clock stamps, completion counters
+  std::vector<unsigned long long> h_stamps;
   LaunchShape shape;
   cudaStream_t cap = nullptr;
   cudaGraph_t graph = nullptr;
@@ -43,6 +48,7 @@ struct pbrt_batch {
     for (double* f : films) cudaFree(f);
     cudaFree(d_table);
     cudaFree(d_frame);
+    cudaFree(d_scratch);
     cudaFree(wave.block);
   }
 };
@@ -55,7 +61,10 @@ int capture(pbrt_batch* b) {
   PBRT_TRY(c->cuda(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking), "cudaStreamCreate"));
   PBRT_TRY(c->cuda(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture"));
   cudaError_t e = cudaMemsetAsync(c->d_counters + 8, 0, 3 * sizeof(unsigned long long), b->cap);
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && b->persistent)
+    e = render_batch_persistent(b->d_table, b->table.data(), uint32_t(b->table.size()), b->d_frame, b->d_scratch,
+                                c->d_counters + 8, c->d_err, c->sm_count, b->cap);
+  else if (e == cudaSuccess)
     e = render_batch(b->d_table, b->table.data(), uint32_t(b->table.size()), b->wave.w, b->wave_paths, b->d_frame,
                      b->max_depth, b->any_path, b->shape, c->d_counters + 8, c->d_err, c->sm_count, b->cap,
                      b->done.data());
@@ -145,7 +154,15 @@ int pbrt_batch_create(pbrt_ctx* c, pbrt_scene* const* scenes, const pbrt_render_
   if (rc == PBRT_OK) rc = c->cuda(cudaMemsetAsync(b->d_frame, 0, sizeof(uint32_t), c->stream), "cudaMemset(batch frame)");
   if (rc == PBRT_OK) rc = c->cuda(cudaStreamSynchronize(c->stream), "batch upload");
   b->wave_paths = uint32_t(std::min<unsigned long long>(begin, c->wave_paths));
-  if (rc == PBRT_OK) rc = ensure_wave(c, &b->wave, b->wave_paths);
+  b->persistent = c->batch_kernel == PBRT_BATCH_PERSISTENT;
+  if (b->persistent) {
+    b->h_stamps.assign(2 + 2 * size_t(n), 0);
+    if (rc == PBRT_OK)
+      rc = c->cuda(cudaMalloc(&b->d_scratch, b->h_stamps.size() * sizeof(unsigned long long)),
+                   "cudaMalloc(batch counters)");
+  } else if (rc == PBRT_OK) {
+    rc = ensure_wave(c, &b->wave, b->wave_paths);
+  }
   if (rc == PBRT_OK) rc = c->cuda(cudaEventCreate(&b->start), "cudaEventCreate");
   b->done.assign(n, nullptr);
   for (uint32_t i = 0; i < n && rc == PBRT_OK; ++i) rc = c->cuda(cudaEventCreate(&b->done[i]), "cudaEventCreate");
@@ -175,10 +192,21 @@ int pbrt_batch_render(pbrt_batch* b, uint32_t frame, double* const* films, float
         PBRT_TRY(c->cuda(cudaMemcpyAsync(films[i], b->films[k], b->film_n[k] * sizeof(double), cudaMemcpyDefault, st),
                          "cudaMemcpy(batch film)"));
       }
+  if (scene_ms && b->persistent)  // the kernel's clock stamps: frame start, each scene's completion
+    PBRT_TRY(c->cuda(cudaMemcpyAsync(b->h_stamps.data(), b->d_scratch, b->h_stamps.size() * sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToHost, st),
+                     "cudaMemcpy(batch clock)"));
   PBRT_TRY(check_device_error(c, st));
-  if (scene_ms)
+  if (scene_ms && b->persistent) {
+    const size_t n = b->slot.size();
+    for (size_t i = 0; i < n; ++i) {
+      const unsigned long long t0 = b->h_stamps[1], t1 = b->h_stamps[2 + n + b->slot[i]];
+      scene_ms[i] = t1 >= t0 ? float(double(t1 - t0) * 1e-6) : 0.f;
+    }
+  } else if (scene_ms) {
     for (size_t i = 0; i < b->slot.size(); ++i)
       PBRT_TRY(c->cuda(cudaEventElapsedTime(scene_ms + i, b->start, b->done[b->slot[i]]), "cudaEventElapsedTime"));
+  }
   return PBRT_OK;
 }
 
@@ -188,6 +216,14 @@ void pbrt_batch_destroy(pbrt_batch* b) {
   cudaStreamSynchronize(b->ctx->work_stream());
   b->release();
   delete b;
+}
+
+int pbrt_ctx_set_batch_kernel(pbrt_ctx* c, int kind) {
+  if (!c) return PBRT_ERR_INVALID_ARGUMENT;
+  if (kind != PBRT_BATCH_WAVEFRONT && kind != PBRT_BATCH_PERSISTENT)
+    return c->fail(PBRT_ERR_INVALID_ARGUMENT, "unknown batch kernel " + std::to_string(kind));
+  c->batch_kernel = kind;
+  return PBRT_OK;
 }
 
 int pbrt_render_batch(pbrt_scene* const* scenes, const pbrt_render_params* params, uint32_t n, double* const* films) {

@@ -91,6 +91,7 @@ struct pbrt_ctx {
   std::vector<void*> allocs;
   pbrt::LaunchShape shape;          // wavefront launch shape (pbrt_ctx_set_tuning)
   uint32_t wave_paths = 1u << 22;   // paths per wave
+  int batch_kernel = 0;             // batches created afterwards: PBRT_BATCH_WAVEFRONT / _PERSISTENT
   // a cached render's training rounds beside its frame: their stream, the fork and join
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;

@@ -333,13 +333,19 @@ struct ManyScenes {
 
 // ---- kernels ---------------------------------------------------------------------------------
 // A new path for image pixel `pixel`, sample `sample`: jitter, camera ray, fresh state.
+PBRT_DEV void begin_path(const CameraRec& cam, unsigned long long seed, uint32_t pixel, uint32_t sample,
+                         F3& o, F3& d, unsigned long long& st) {
+  const unsigned long long inc = pcg_inc(pixel);
+  st = pcg_seed(seed, pixel, sample);
+  const float jx = pcg_uniform(st, inc), jy = pcg_uniform(st, inc);  // Sampler2::sample (mt.rs:145-150)
+  camera_ray(cam, fa(float(pixel % cam.width), jx), fa(float(pixel / cam.width), jy), st, inc, o, d);
+}
+
 PBRT_DEV void start_path(const WaveBuffers& w, uint32_t i, const CameraRec& cam, unsigned long long seed,
                          uint32_t pixel, uint32_t sample) {
-  const unsigned long long inc = pcg_inc(pixel);
-  unsigned long long st = pcg_seed(seed, pixel, sample);
-  const float jx = pcg_uniform(st, inc), jy = pcg_uniform(st, inc);  // Sampler2::sample (mt.rs:145-150)
   F3 o, d;
-  camera_ray(cam, fa(float(pixel % cam.width), jx), fa(float(pixel / cam.width), jy), st, inc, o, d);
+  unsigned long long st;
+  begin_path(cam, seed, pixel, sample, o, d, st);
   w.ox[i] = o.x; w.oy[i] = o.y; w.oz[i] = o.z;
   w.dx[i] = d.x; w.dy[i] = d.y; w.dz[i] = d.z;
   w.br[i] = 1.f; w.bg[i] = 1.f; w.bb[i] = 1.f;
@@ -348,6 +354,28 @@ PBRT_DEV void start_path(const WaveBuffers& w, uint32_t i, const CameraRec& cam,
   w.pixel[i] = pixel;
   w.flags[i] = kSpecularBit;  // is_last_bounce_specular starts true (path.rs:52)
   w.qa[i] = i;
+}
+
+// The table entry holding path g of a batch frame: the last scene whose range starts at or
+// before g (the table is in path order).
+PBRT_DEV uint32_t batch_scene_of(const BatchScene* __restrict__ b, uint32_t nscenes, unsigned long long g) {
+  uint32_t lo = 0, hi = nscenes - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (b[mid].begin <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Path g of a batch frame: its scene's pixel and sample (frame f takes samples
+// sample_offset + f * spp ... of every pixel).
+PBRT_DEV void batch_pixel_sample(const BatchScene& e, unsigned long long g, uint32_t f, uint32_t& pixel,
+                                 uint32_t& sample) {
+  const unsigned long long l = g - e.begin;
+  const uint32_t q = uint32_t(l % e.npix);
+  pixel = (q / e.film_w) * e.stride * e.cam.width + (q % e.film_w) * e.stride;
+  sample = e.sample_offset + f * e.spp + uint32_t(l / e.npix);
 }
 
 __global__ void __launch_bounds__(256) k_generate(WaveBuffers w, CameraRec cam, uint64_t wave_base, uint32_t n,
@@ -376,17 +404,10 @@ __global__ void __launch_bounds__(256) k_generate_batch(WaveBuffers w, const Bat
   const uint32_t f = *frame;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const unsigned long long g = wave_base + i;
-    uint32_t lo = 0, hi = nscenes - 1;  // the last scene whose range starts at or before g
-    while (lo < hi) {
-      const uint32_t mid = (lo + hi + 1) >> 1;
-      if (b[mid].begin <= g) lo = mid;
-      else hi = mid - 1;
-    }
+    const uint32_t lo = batch_scene_of(b, nscenes, g);
     const BatchScene& e = b[lo];
-    const unsigned long long l = g - e.begin;
-    const uint32_t q = uint32_t(l % e.npix);
-    const uint32_t pixel = (q / e.film_w) * e.stride * e.cam.width + (q % e.film_w) * e.stride;
-    const uint32_t sample = e.sample_offset + f * e.spp + uint32_t(l / e.npix);
+    uint32_t pixel, sample;
+    batch_pixel_sample(e, g, f, pixel, sample);
     start_path(w, i, e.cam, e.seed, pixel, sample);
     w.scene[i] = lo;
   }
@@ -592,6 +613,128 @@ __global__ void __launch_bounds__(256, 2) k_extend_walk(WaveBuffers w, Src src, 
 // scan of the warps' ballots and one atomicAdd per block and queue, the path indices written
 // as one contiguous run, and the shadow records (11 planes) staged in shared memory and
 // copied out as one contiguous SoA run per block (thread t writes entry t of each plane).
+// One path vertex of PathIntegrator::li (path.rs:48-115): the hit (obj 0xFFFFFFFF: the
+// background) of the path's ray, its emission, the light sample (a shadow ray to trace, with
+// the contribution it adds if unoccluded), the BSDF sample and Russian roulette. `P` is updated
+// in place (radiance always; ray, throughput, stream and flags when the path goes on: alive).
+// With the cache on, a cacheable vertex's record is returned and the path may end into it.
+struct PathState {
+  F3 o, d, beta, L;
+  unsigned long long st;
+  uint32_t pixel, flags;  // flags: bounce count | kSpecularBit
+};
+
+struct VertexOut {
+  bool alive = false, shadow = false, query = false, train = false;
+  F3 sro, srd, contrib;
+  float stmax = 0.f;
+  F3 cp, cwo, cn, calb, cL, cB;  // the cache record of this vertex
+  float crough = 0.f;
+};
+
+PBRT_DEV void shade_vertex(const SceneView& s, const PathSettings& ps, PathState& P, uint32_t obj, uint32_t prim,
+                           float t, uint32_t cache_mode, uint32_t term_hit, VertexOut& v) {
+  const uint32_t max_depth = ps.max_depth, rr_start = ps.rr_start, naive = ps.integrator;
+  const bool normal_only = ps.integrator == 2u;
+  F3 o = P.o, d = P.d;
+  F3 beta = P.beta;
+  F3 L = P.L;
+  unsigned long long st = P.st;
+  const unsigned long long inc = pcg_inc(P.pixel);
+  uint32_t flags = P.flags;
+  const bool spec = naive || (flags & kSpecularBit);
+  uint32_t bounce = flags & 0xFFFFu;
+  bool alive = false;
+  if (obj == 0xFFFFFFFFu) {
+    if (spec && !normal_only) {  // NormalIntegrator's background is black (integrators.rs:9-11)
+      const F3 bg = background(s, d);
+      L = add3(L, mk3(fm(bg.x, beta.x), fm(bg.y, beta.y), fm(bg.z, beta.z)));
+    }
+  } else {
+    const MatRec m = s.materials[material_index(s, obj, prim)];
+    const Isect it = interaction(s, obj, prim, o, d, t, m.texture != kTexColor);
+    const F3 alb = texel(m, it);  // albedo, or emitted radiance (DiffuseLight::emit)
+    if (normal_only) {  // NormalIntegrator::li (normal.rs:17-27): (n + (1, 1, 1)) * 0.5, one hit
+      const F3 nn = add3(it.n, mk3(1.f, 1.f, 1.f));
+      L = mul3(nn, 0.5f);
+      bounce = max_depth - 1u;  // the hit ends the path
+    }
+    if (spec && !normal_only && m.kind == kMatDiffuseLight)
+      L = add3(L, mk3(fm(alb.x, beta.x), fm(alb.y, beta.y), fm(alb.z, beta.z)));
+    bounce++;
+    // PathIntegrator stops at the max_depth-th hit, before sampling a light (path.rs:64-67);
+    // the naive estimator also ends there, its emission counted: after max_depth hits its
+    // recursion reaches li(.., 0), which is black (naive.rs:29-52). Paths of every scene of
+    // a batch stop at their own depth, whatever the number of bounce launches.
+    const bool depth_cut = bounce == max_depth;
+    const bool cacheable = m.kind == kMatLambertian || m.kind == kMatMetal;
+    if (!depth_cut && cacheable && cache_mode != kCacheOff) {
+      v.cp = it.p;
+      v.cwo = mul3(d, -1.f);
+      v.cn = dot3(it.n, v.cwo) < 0.f ? mul3(it.n, -1.f) : it.n;
+      v.calb = alb;
+      v.crough = m.kind == kMatMetal ? m.fuzz : 1.f;
+      v.cL = L;
+      v.cB = beta;
+      v.query = bounce >= term_hit;  // the path ends here, into the cache
+      v.train = cache_mode == kCacheRecord && !v.query;
+    }
+    if (!depth_cut && !v.query) {
+      if (!naive && s.light_count > 0) {  // sample_light (path.rs:31-44) and the light sample
+        const float cnt = float(s.light_count);
+        const float pick = fminf(fm(pcg_uniform(st, inc), cnt), fs(cnt, 1.f));
+        const uint32_t li = uint32_t(pick);
+        const float pl = fdv(1.f, cnt);
+        LiSample ls;
+        if (sample_li(s, s.lights[li], it, st, inc, ls)) {
+          const F3 f0 = bsdf_f(m, alb, mul3(d, -1.f), ls.wi, it);
+          const float ac = fabsf(dot3(ls.wi, it.n));
+          const F3 f = mk3(fm(f0.x, ac), fm(f0.y, ac), fm(f0.z, ac));
+          if (f.x != 0.f || f.y != 0.f || f.z != 0.f) {
+            const float den = fm(pl, ls.pdf);
+            v.contrib = mk3(fdv(fm(fm(ls.spectrum.x, f.x), beta.x), den),
+                            fdv(fm(fm(ls.spectrum.y, f.y), beta.y), den),
+                            fdv(fm(fm(ls.spectrum.z, f.z), beta.z), den));
+            v.sro = ls.ro;
+            v.srd = ls.rd;
+            v.stmax = ls.dist;
+            v.shadow = true;
+          }
+        }
+      }
+      ScatterOut sc;
+      if (scatter(m, alb, it, st, inc, sc)) {
+        const float ac = fabsf(dot3(sc.rd, it.n));
+        const F3 kk = mk3(fdv(fm(sc.att.x, ac), sc.pdf), fdv(fm(sc.att.y, ac), sc.pdf), fdv(fm(sc.att.z, ac), sc.pdf));
+        beta = mk3(fm(beta.x, kk.x), fm(beta.y, kk.y), fm(beta.z, kk.z));
+        o = sc.ro;
+        d = sc.rd;
+        const bool sp = m.kind == kMatMetal || m.kind == kMatDielectric;
+        alive = true;
+        if (rr_start && bounce >= rr_start) {  // Russian roulette (path.rs:92-101, q clamped to 1)
+          const float qq = fminf(1.f, fmaxf(fmaxf(beta.x, beta.y), beta.z));
+          if (pcg_uniform(st, inc) > qq) {
+            alive = false;
+          } else {
+            const float iq = frcp(qq);
+            beta = mul3(beta, iq);
+          }
+        }
+        flags = (sp ? kSpecularBit : 0u) | bounce;
+      }
+    }
+  }
+  P.L = L;
+  v.alive = alive;
+  if (alive) {
+    P.o = o;
+    P.d = d;
+    P.beta = beta;
+    P.st = st;
+    P.flags = flags;
+  }
+}
+
 template <class Src, bool kStage>
 __global__ void __launch_bounds__(256) k_shade(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
                                                const uint32_t* __restrict__ qcount, uint32_t* __restrict__ qout,
@@ -617,105 +760,28 @@ __global__ void __launch_bounds__(256) k_shade(WaveBuffers w, Src src, const uin
       p = q[k];
       const SceneView& s = src.view(w, p);
       const PathSettings ps = src.settings(w, p);
-      const uint32_t max_depth = ps.max_depth, rr_start = ps.rr_start, naive = ps.integrator;
-      const bool normal_only = ps.integrator == 2u;
-      F3 o = mk3(w.ox[p], w.oy[p], w.oz[p]), d = mk3(w.dx[p], w.dy[p], w.dz[p]);
-      F3 beta = mk3(w.br[p], w.bg[p], w.bb[p]);
-      F3 L = mk3(w.lr[p], w.lg[p], w.lb[p]);
-      unsigned long long st = w.rng[p];
-      const uint32_t pixel = w.pixel[p];
-      const unsigned long long inc = pcg_inc(pixel);
-      uint32_t flags = w.flags[p];
-      const bool spec = naive || (flags & kSpecularBit);
-      uint32_t bounce = flags & 0xFFFFu;
-      const uint32_t obj = w.hobj[p];
-      bool alive = false;
-      if (obj == 0xFFFFFFFFu) {
-        if (spec && !normal_only) {  // NormalIntegrator's background is black (integrators.rs:9-11)
-          const F3 bg = background(s, d);
-          L = add3(L, mk3(fm(bg.x, beta.x), fm(bg.y, beta.y), fm(bg.z, beta.z)));
-        }
-      } else {
-        const MatRec m = s.materials[material_index(s, obj, w.hprim[p])];
-        const Isect it = interaction(s, obj, w.hprim[p], o, d, w.ht[p], m.texture != kTexColor);
-        const F3 alb = texel(m, it);  // albedo, or emitted radiance (DiffuseLight::emit)
-        if (normal_only) {  // NormalIntegrator::li (normal.rs:17-27): (n + (1, 1, 1)) * 0.5, one hit
-          const F3 nn = add3(it.n, mk3(1.f, 1.f, 1.f));
-          L = mul3(nn, 0.5f);
-          bounce = max_depth - 1u;  // the hit ends the path
-        }
-        if (spec && !normal_only && m.kind == kMatDiffuseLight)
-          L = add3(L, mk3(fm(alb.x, beta.x), fm(alb.y, beta.y), fm(alb.z, beta.z)));
-        bounce++;
-        // PathIntegrator stops at the max_depth-th hit, before sampling a light (path.rs:64-67);
-        // the naive estimator also ends there, its emission counted: after max_depth hits its
-        // recursion reaches li(.., 0), which is black (naive.rs:29-52). Paths of every scene of
-        // a batch stop at their own depth, whatever the number of bounce launches.
-        const bool depth_cut = bounce == max_depth;
-        const bool cacheable = m.kind == kMatLambertian || m.kind == kMatMetal;
-        if (!depth_cut && cacheable && cache_mode != kCacheOff) {
-          cp = it.p;
-          cwo = mul3(d, -1.f);
-          cn = dot3(it.n, cwo) < 0.f ? mul3(it.n, -1.f) : it.n;
-          calb = alb;
-          crough = m.kind == kMatMetal ? m.fuzz : 1.f;
-          cL = L;
-          cB = beta;
-          push_query = bounce >= term_hit;  // the path ends here, into the cache
-          push_train = cache_mode == kCacheRecord && !push_query;
-        }
-        if (!depth_cut && !push_query) {
-          if (!naive && s.light_count > 0) {  // sample_light (path.rs:31-44) and the light sample
-            const float cnt = float(s.light_count);
-            const float pick = fminf(fm(pcg_uniform(st, inc), cnt), fs(cnt, 1.f));
-            const uint32_t li = uint32_t(pick);
-            const float pl = fdv(1.f, cnt);
-            LiSample ls;
-            if (sample_li(s, s.lights[li], it, st, inc, ls)) {
-              const F3 f0 = bsdf_f(m, alb, mul3(d, -1.f), ls.wi, it);
-              const float ac = fabsf(dot3(ls.wi, it.n));
-              const F3 f = mk3(fm(f0.x, ac), fm(f0.y, ac), fm(f0.z, ac));
-              if (f.x != 0.f || f.y != 0.f || f.z != 0.f) {
-                const float den = fm(pl, ls.pdf);
-                contrib = mk3(fdv(fm(fm(ls.spectrum.x, f.x), beta.x), den),
-                              fdv(fm(fm(ls.spectrum.y, f.y), beta.y), den),
-                              fdv(fm(fm(ls.spectrum.z, f.z), beta.z), den));
-                sro = ls.ro;
-                srd = ls.rd;
-                stmax = ls.dist;
-                push_shadow = true;
-              }
-            }
-          }
-          ScatterOut sc;
-          if (scatter(m, alb, it, st, inc, sc)) {
-            const float ac = fabsf(dot3(sc.rd, it.n));
-            const F3 kk = mk3(fdv(fm(sc.att.x, ac), sc.pdf), fdv(fm(sc.att.y, ac), sc.pdf), fdv(fm(sc.att.z, ac), sc.pdf));
-            beta = mk3(fm(beta.x, kk.x), fm(beta.y, kk.y), fm(beta.z, kk.z));
-            o = sc.ro;
-            d = sc.rd;
-            const bool sp = m.kind == kMatMetal || m.kind == kMatDielectric;
-            alive = true;
-            if (rr_start && bounce >= rr_start) {  // Russian roulette (path.rs:92-101, q clamped to 1)
-              const float qq = fminf(1.f, fmaxf(fmaxf(beta.x, beta.y), beta.z));
-              if (pcg_uniform(st, inc) > qq) {
-                alive = false;
-              } else {
-                const float iq = frcp(qq);
-                beta = mul3(beta, iq);
-              }
-            }
-            flags = (sp ? kSpecularBit : 0u) | bounce;
-          }
-        }
-      }
-      w.lr[p] = L.x; w.lg[p] = L.y; w.lb[p] = L.z;
-      if (alive) {
-        w.ox[p] = o.x; w.oy[p] = o.y; w.oz[p] = o.z;
-        w.dx[p] = d.x; w.dy[p] = d.y; w.dz[p] = d.z;
-        w.br[p] = beta.x; w.bg[p] = beta.y; w.bb[p] = beta.z;
-        w.rng[p] = st;
-        w.flags[p] = flags;
+      PathState P;
+      P.o = mk3(w.ox[p], w.oy[p], w.oz[p]);
+      P.d = mk3(w.dx[p], w.dy[p], w.dz[p]);
+      P.beta = mk3(w.br[p], w.bg[p], w.bb[p]);
+      P.L = mk3(w.lr[p], w.lg[p], w.lb[p]);
+      P.st = w.rng[p];
+      P.pixel = w.pixel[p];
+      P.flags = w.flags[p];
+      VertexOut v;
+      shade_vertex(s, ps, P, w.hobj[p], w.hprim[p], w.ht[p], cache_mode, term_hit, v);
+      push_shadow = v.shadow;
+      push_query = v.query;
+      push_train = v.train;
+      sro = v.sro; srd = v.srd; contrib = v.contrib; stmax = v.stmax;
+      cp = v.cp; cwo = v.cwo; cn = v.cn; calb = v.calb; cL = v.cL; cB = v.cB; crough = v.crough;
+      w.lr[p] = P.L.x; w.lg[p] = P.L.y; w.lb[p] = P.L.z;
+      if (v.alive) {
+        w.ox[p] = P.o.x; w.oy[p] = P.o.y; w.oz[p] = P.o.z;
+        w.dx[p] = P.d.x; w.dy[p] = P.d.y; w.dz[p] = P.d.z;
+        w.br[p] = P.beta.x; w.bg[p] = P.beta.y; w.bb[p] = P.beta.z;
+        w.rng[p] = P.st;
+        w.flags[p] = P.flags;
         push_path = true;
       }
     }
@@ -1150,15 +1216,128 @@ __global__ void __launch_bounds__(256) k_accumulate(WaveBuffers w, uint32_t n, d
   }
 }
 
+// A finished path's radiance into its scene's film (FP64 sums: the FP32 radiances of a pixel
+// add exactly, so the order of the adds does not matter).
+PBRT_DEV void batch_film_add(const BatchScene& e, uint32_t px, float r, float g, float bl) {
+  const uint32_t iw = e.cam.width;
+  const uint32_t pix = e.stride == 1 ? px : ((px / iw) / e.stride) * e.film_w + (px % iw) / e.stride;
+  double* film = e.film + 3 * size_t(pix);
+  atomicAdd(film, double(r));
+  atomicAdd(film + 1, double(g));
+  atomicAdd(film + 2, double(bl));
+}
+
 __global__ void __launch_bounds__(256) k_accumulate_batch(WaveBuffers w, uint32_t n, const BatchScene* __restrict__ b) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const BatchScene& e = b[w.scene[i]];
-    const uint32_t px = w.pixel[i], iw = e.cam.width;
-    const uint32_t pix = e.stride == 1 ? px : ((px / iw) / e.stride) * e.film_w + (px % iw) / e.stride;
-    double* film = e.film + 3 * size_t(pix);
-    atomicAdd(film, double(w.lr[i]));
-    atomicAdd(film + 1, double(w.lg[i]));
-    atomicAdd(film + 2, double(w.lb[i]));
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    batch_film_add(b[w.scene[i]], w.pixel[i], w.lr[i], w.lg[i], w.lb[i]);
+}
+
+// ---- batches: every path to its end in one persistent launch -------------------------------
+PBRT_DEV unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__global__ void k_batch_clock(unsigned long long* t) { *t = global_ns(); }
+
+// The batch frame as persistent warps over all scenes' paths (table order, cheapest scene
+// first): a lane takes path g (one atomicAdd on `fetch` per warp, once at least `refill_min`
+// lanes are idle or all are), and each iteration runs one vertex of its path: the nearest
+// hit (Scene::find_nearest, the full query), the vertex's shading (shade_vertex, the shading
+// kernel's code), the shadow ray (Scene::any_hit) and, when the path ends, the film add. The
+// arithmetic is the wavefront's, so films are the same. `done[s]` counts scene s's finished
+// paths (one atomicAdd per warp and scene); the lane that finishes a scene's last path stamps
+// `done_ns[s]` with the GPU clock. stats: rays, shadow rays, paths (one atomicAdd per warp).
+// kTight: at most 64 registers (8 resident blocks per SM, more spills) instead of the
+// compiler's choice (96: 5 blocks per SM).
+template <bool kCsg, bool kTight>
+__global__ void __launch_bounds__(128, kTight ? 8 : 0) k_batch_paths(const BatchScene* __restrict__ b, uint32_t nscenes,
+                                                     unsigned long long total, const uint32_t* __restrict__ frame,
+                                                     unsigned long long* __restrict__ fetch,
+                                                     unsigned long long* __restrict__ done,
+                                                     unsigned long long* __restrict__ done_ns, int refill_min,
+                                                     unsigned long long* stats, uint32_t* err) {
+  const unsigned lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+  const uint32_t f = *frame;
+  bool active = false, exhausted = false;  // exhausted is warp-uniform
+  PathState P;
+  uint32_t sc = 0, n_rays = 0, n_shadow = 0, n_paths = 0;
+  for (;;) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !active);
+    if (!exhausted && idle && (__popc(idle) >= refill_min || idle == 0xffffffffu)) {
+      const int leader = __ffs(idle) - 1;
+      unsigned long long base = 0;
+      if (int(lane) == leader) base = atomicAdd(fetch, (unsigned long long)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      exhausted = base + __popc(idle) >= total;
+      if (!active) {
+        const unsigned long long g = base + __popc(idle & lt);
+        if (g < total) {
+          sc = batch_scene_of(b, nscenes, g);
+          const BatchScene& e = b[sc];
+          uint32_t pixel, sample;
+          batch_pixel_sample(e, g, f, pixel, sample);
+          begin_path(e.cam, e.seed, pixel, sample, P.o, P.d, P.st);
+          P.beta = mk3(1.f, 1.f, 1.f);
+          P.L = mk3(0.f, 0.f, 0.f);
+          P.pixel = pixel;
+          P.flags = kSpecularBit;  // is_last_bounce_specular starts true (path.rs:52)
+          active = true;
+          ++n_paths;
+        }
+      }
+    }
+    if (__ballot_sync(0xffffffffu, active) == 0) {
+      if (exhausted) break;
+      continue;  // all idle and paths left: the next iteration refills
+    }
+    bool finished = false;
+    if (active) {
+      const BatchScene& e = b[sc];
+      const PathSettings ps{e.max_depth, e.rr_start, e.integrator, e.cam.near, e.cam.far};
+      float t = 0.f;
+      uint32_t obj = 0xFFFFFFFFu, prim = 0;
+      if (!scene_closest<kCsg>(e.view, P.o, P.d, ps.near, ps.far, t, obj, prim, err)) obj = 0xFFFFFFFFu;
+      ++n_rays;
+      VertexOut v;
+      shade_vertex(e.view, ps, P, obj, prim, t, kCacheOff, 0, v);
+      if (v.shadow) {  // VisibilityTester::unoccluded (lights.rs:67-69)
+        ++n_shadow;
+        if (!scene_any<kCsg>(e.view, v.sro, v.srd, kShadowEps, v.stmax, err)) {
+          P.L.x = fa(P.L.x, v.contrib.x);
+          P.L.y = fa(P.L.y, v.contrib.y);
+          P.L.z = fa(P.L.z, v.contrib.z);
+        }
+      }
+      if (!v.alive) {
+        batch_film_add(e, P.pixel, P.L.x, P.L.y, P.L.z);
+        active = false;
+        finished = true;
+      }
+    }
+    const unsigned fin = __ballot_sync(0xffffffffu, finished);
+    if (finished) {  // per scene: one count per warp, and the clock when the scene is complete
+      const unsigned same = __match_any_sync(fin, sc);
+      if (int(lane) == __ffs(same) - 1) {
+        const unsigned long long k = __popc(same);
+        const BatchScene& e = b[sc];
+        if (atomicAdd(done + sc, k) + k == (unsigned long long)e.npix * e.spp) done_ns[sc] = global_ns();
+      }
+    }
+  }
+  if (stats) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      n_rays += __shfl_xor_sync(0xffffffffu, n_rays, off);
+      n_shadow += __shfl_xor_sync(0xffffffffu, n_shadow, off);
+      n_paths += __shfl_xor_sync(0xffffffffu, n_paths, off);
+    }
+    if (lane == 0) {
+      atomicAdd(stats, (unsigned long long)n_rays);
+      atomicAdd(stats + 1, (unsigned long long)n_shadow);
+      atomicAdd(stats + 2, (unsigned long long)n_paths);
+    }
   }
 }
 
@@ -1409,6 +1588,79 @@ cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, 
       ++next_done;
     }
   }
+  k_films_batch<<<fgrid, 256, 0, st>>>(table, 0);
+  return cudaGetLastError();
+}
+
+// Resident 128-thread blocks per SM of the persistent batch kernel (computed once).
+template <bool kCsg, bool kTight>
+static int batch_paths_blocks_per_sm() {
+  static const int v = [] {
+    int b = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_paths<kCsg, kTight>, 128, 0);
+    return e == cudaSuccess && b > 0 ? b : 4;
+  }();
+  return v;
+}
+
+// PBRT_BATCH_REFILL (1..32, default 8): idle lanes of a warp before the persistent batch
+// kernel refills them; PBRT_BATCH_TIGHT=1: the 64-register build. For measurements.
+static int batch_refill_min() {
+  static const int v = [] {
+    const char* e = std::getenv("PBRT_BATCH_REFILL");
+    const int r = e ? std::atoi(e) : 8;
+    return r >= 1 && r <= 32 ? r : 8;
+  }();
+  return v;
+}
+
+static bool batch_tight() {
+  static const bool v = [] {
+    const char* e = std::getenv("PBRT_BATCH_TIGHT");
+    return e && e[0] == '1';
+  }();
+  return v;
+}
+
+template <bool kCsg, bool kTight>
+static void launch_batch_paths(const BatchScene* table, uint32_t nscenes, unsigned long long total,
+                               const uint32_t* frame, unsigned long long* scratch, int refill,
+                               unsigned long long* stats, uint32_t* err, int sm_count, cudaStream_t st) {
+  k_batch_paths<kCsg, kTight><<<unsigned(sm_count * batch_paths_blocks_per_sm<kCsg, kTight>()), 128, 0, st>>>(
+      table, nscenes, total, frame, scratch, scratch + 2, scratch + 2 + nscenes, refill, stats, err);
+}
+
+cudaError_t render_batch_persistent(const BatchScene* table, const BatchScene* host_table, uint32_t nscenes,
+                                    const uint32_t* frame, unsigned long long* scratch, unsigned long long* stats,
+                                    uint32_t* err, int sm_count, cudaStream_t st) {
+  cudaError_t e;
+  uint32_t max_npix = 0;
+  bool csg = false;
+  for (uint32_t i = 0; i < nscenes; ++i) {
+    max_npix = max_npix > host_table[i].npix ? max_npix : host_table[i].npix;
+    csg = csg || host_table[i].view.has_csg;
+  }
+  const dim3 fgrid(unsigned((size_t(max_npix) * 3 + 255) / 256 < 1024 ? (size_t(max_npix) * 3 + 255) / 256 : 1024),
+                   nscenes);
+  const unsigned long long total =
+      host_table[nscenes - 1].begin + (unsigned long long)host_table[nscenes - 1].npix * host_table[nscenes - 1].spp;
+  // scratch: [0] fetch position, [1] frame start (GPU clock), [2, 2 + n) finished paths per
+  // scene, [2 + n, 2 + 2n) each scene's completion time
+  if ((e = cudaMemsetAsync(scratch, 0, (2 + 2 * size_t(nscenes)) * sizeof(unsigned long long), st)) != cudaSuccess)
+    return e;
+  k_films_batch<<<fgrid, 256, 0, st>>>(table, 1);
+  k_batch_clock<<<1, 1, 0, st>>>(scratch + 1);
+  const int refill = batch_refill_min();
+  const bool tight = batch_tight();
+  if (csg && tight)
+    launch_batch_paths<true, true>(table, nscenes, total, frame, scratch, refill, stats, err, sm_count, st);
+  else if (csg)
+    launch_batch_paths<true, false>(table, nscenes, total, frame, scratch, refill, stats, err, sm_count, st);
+  else if (tight)
+    launch_batch_paths<false, true>(table, nscenes, total, frame, scratch, refill, stats, err, sm_count, st);
+  else
+    launch_batch_paths<false, false>(table, nscenes, total, frame, scratch, refill, stats, err, sm_count, st);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_films_batch<<<fgrid, 256, 0, st>>>(table, 0);
   return cudaGetLastError();
 }

@@ -91,6 +91,14 @@ cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, 
                          const LaunchShape& shape, unsigned long long* stats, uint32_t* err, int sm_count,
                          cudaStream_t st, cudaEvent_t* done);
 
+// A batched frame as one persistent launch: every path of every scene run to its end by
+// persistent warps (between the films' zeroing and scaling). `scratch`: 2 + 2 * nscenes
+// 64-bit words; words 1 and 2 + nscenes + s hold the frame's start and scene s's completion
+// on the GPU clock (ns) afterwards.
+cudaError_t render_batch_persistent(const BatchScene* table, const BatchScene* host_table, uint32_t nscenes,
+                                    const uint32_t* frame, unsigned long long* scratch, unsigned long long* stats,
+                                    uint32_t* err, int sm_count, cudaStream_t st);
+
 // One wave: generate, max_depth x (extend, shade, shadow), accumulate into `film` (sums).
 // `npix` is the number of film pixels (the image's, or the strided subset's).
 cudaError_t render_wave(const SceneView& s, const WaveBuffers& w, const CameraRec& cam, uint64_t wave_base,

@@ -75,6 +75,15 @@ class Context:
                          int(shade_blocks_per_sm))
         self.check(self.lib.pbrt_ctx_set_tuning(self.h, C.byref(t)), "pbrt_ctx_set_tuning")
 
+    def set_batch_kernel(self, kind: str):
+        """How batches created afterwards run a frame: "wavefront" (the default; waves of
+        paths through queues, one kernel per stage and bounce) or "persistent" (one
+        persistent launch, each lane running a path to its end). Films are the same."""
+        kinds = {"wavefront": 0, "persistent": 1}
+        if kind not in kinds:
+            raise ValueError(f"batch kernel must be one of {sorted(kinds)}")
+        self.check(self.lib.pbrt_ctx_set_batch_kernel(self.h, kinds[kind]), "pbrt_ctx_set_batch_kernel")
+
     def tuning(self) -> dict:
         t = _capi.Tuning()
         self.check(self.lib.pbrt_ctx_get_tuning(self.h, C.byref(t)), "pbrt_ctx_get_tuning")
@@ -769,8 +778,8 @@ def render_params(camera: dict, spp: int, max_depth: int, seed: int = 1, rr_star
 
 class Batch:
     """Many committed scenes rendered together (pbrt_batch): one wavefront over all their
-    paths, its launch sequence recorded once in a CUDA graph. `params` are render_params()
-    per scene."""
+    paths, or one persistent launch (Context.set_batch_kernel), a frame's launches recorded
+    once in a CUDA graph. `params` are render_params() per scene."""
 
     def __init__(self, scenes, params, ctx: Optional[Context] = None):
         self.ctx = ctx or scenes[0].ctx

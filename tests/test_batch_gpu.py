@@ -151,3 +151,76 @@ def test_batch_with_deferred_meshes_equals_single_renders():
         b.close()
     finally:
         ctx.set_tuning()
+    # the persistent launch answers the large meshes inside each path's query
+    ctx.set_batch_kernel("persistent")
+    try:
+        b = Batch(scenes, params)
+        for f, s in zip(b.render(0), singles):
+            _close(f, s)
+        b.close()
+    finally:
+        ctx.set_batch_kernel("wavefront")
+
+
+def test_persistent_batch_equals_single_renders(built):
+    """One persistent launch over the batch (each lane runs a path to its end with the
+    wavefront's shading code): every film equals the scene's own render, in later frames too;
+    the scenes complete cheapest first on the GPU clock; the work counters equal the
+    wavefront batch's."""
+    specs, scenes, singles, params = built
+    ctx = scenes[0].ctx
+    wave = Batch(scenes, params)
+    wave.render(0)
+    wave_stats = ctx.render_stats()
+    wave.close()
+    ctx.set_batch_kernel("persistent")
+    try:
+        b = Batch(scenes, params)
+        films, ms = b.render(0, scene_times=True)
+        for f, s in zip(films, singles):
+            _close(f, s)
+        assert ctx.render_stats() == wave_stats
+        # (paths are taken in table order, but a scene's last path may still finish after a
+        # later scene's, so the times are not ordered)
+        assert all(np.isfinite(t) and t > 0 for t in ms)
+        for sc, f, (_, cam, kw) in zip(scenes, b.render(2), specs):
+            _close(f, sc.render(cam, seed=5, sample_offset=2 * kw["spp"], **kw))
+        b.close()
+    finally:
+        ctx.set_batch_kernel("wavefront")
+    with pytest.raises(ValueError):
+        ctx.set_batch_kernel("megakernel")
+
+
+_TIGHT_SCRIPT = """
+import sys, numpy as np
+sys.path.insert(0, {root!r})
+import pbrt_b200 as pb
+from pbrt_b200 import workloads as W
+from pbrt_b200.scene import Batch, create_scenes, render_params
+(d0, c0), (d1, c1) = W.cornell_box(24, 20), W.many_spheres(200, width=32, height=24)
+scenes = create_scenes([d0, d1])
+params = [render_params(c0, spp=3, max_depth=6, seed=9), render_params(c1, spp=2, max_depth=8, rr_start=3, seed=9)]
+singles = [scenes[0].render(c0, spp=3, max_depth=6, seed=9), scenes[1].render(c1, spp=2, max_depth=8, rr_start=3, seed=9)]
+scenes[0].ctx.set_batch_kernel("persistent")
+films = Batch(scenes, params).render(0)
+np.savez({out!r}, f0=films[0], f1=films[1], s0=singles[0], s1=singles[1])
+"""
+
+
+@pytest.mark.parametrize("env", [{"PBRT_BATCH_TIGHT": "1"}, {"PBRT_BATCH_REFILL": "1"}, {"PBRT_BATCH_REFILL": "32"}])
+def test_persistent_batch_builds_and_refill(tmp_path, env):
+    """The 64-register build of the persistent batch kernel, and refills at every idle lane or
+    only when the whole warp is idle, give the scenes' own films (switches read once per
+    process: a child each)."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = str(tmp_path / "films.npz")
+    subprocess.run([sys.executable, "-c", _TIGHT_SCRIPT.format(root=root, out=out)], env=dict(os.environ, **env),
+                   check=True, timeout=300)
+    z = np.load(out)
+    _close(z["f0"], z["s0"])
+    _close(z["f1"], z["s1"])
