@@ -208,9 +208,9 @@ np.savez({out!r}, f0=films[0], f1=films[1], s0=singles[0], s1=singles[1])
 """
 
 
-@pytest.mark.parametrize("env", [{"PBRT_BATCH_TIGHT": "1"}, {"PBRT_BATCH_REFILL": "1"}, {"PBRT_BATCH_REFILL": "32"}])
+@pytest.mark.parametrize("env", [{"PBRT_BATCH_TIGHT": "0"}, {"PBRT_BATCH_REFILL": "1"}, {"PBRT_BATCH_REFILL": "32"}])
 def test_persistent_batch_builds_and_refill(tmp_path, env):
-    """The 64-register build of the persistent batch kernel, and refills at every idle lane or
+    """The 96-register build of the persistent batch kernel, and refills at every idle lane or
     only when the whole warp is idle, give the scenes' own films (switches read once per
     process: a child each)."""
     import os
