@@ -441,6 +441,12 @@ def render_case(pb, W, ctx, case, reps=3, cpu=False, nvtx=False, frame=None, spp
         torch.cuda.nvtx.range_pop()
     ms = e0.elapsed_time(e1) / reps
     st = ctx.render_stats()
+    g1 = None
+    if cpu:  # the frame at 1 spp with the oracle's seed, for the parity check below
+        g1t = torch.zeros_like(film)
+        scene.render(cam, seed=1, film=g1t, **dict(kw, spp=1))
+        torch.cuda.synchronize()
+        g1 = g1t.cpu().numpy()
     ctx.set_stream(None)
     samples = cam["width"] * cam["height"] * kw["spp"]
     rays = st["rays"] + st["shadow_rays"]
@@ -453,8 +459,15 @@ def render_case(pb, W, ctx, case, reps=3, cpu=False, nvtx=False, frame=None, spp
         threads = os.cpu_count() or 1
         o = oracle.Scene(desc, np.float32)
         t0 = time.perf_counter()
-        _, work = o.render_counted(cam, 1, kw["max_depth"], seed=1, rr_start=kw["rr_start"], threads=threads)
+        ofilm, work = o.render_counted(cam, 1, kw["max_depth"], seed=1, rr_start=kw["rr_start"], threads=threads)
         cs = time.perf_counter() - t0
+        # the same image, the same sample streams: pixels agree except where a path took
+        # another branch after a last-bit difference in a transcendental function
+        same = np.all(np.abs(g1 - ofilm) <= 1e-5 * np.maximum(1.0, np.abs(ofilm)), axis=2)
+        out["parity"] = {"relmse_vs_oracle": float(np.mean((g1 - ofilm) ** 2 / (ofilm ** 2 + 1e-2))),
+                         "pixels_equal_frac": round(float(same.mean()), 5),
+                         "mean_ratio": round(float(g1.mean() / ofilm.mean()), 5),
+                         "frame": "the full image at 1 spp, seed 1, against the FP32 oracle's render"}
         out["cpu_baseline"] = {"value": round(cam["width"] * cam["height"] / cs, 1), "unit": "samples/s",
                                "cores": threads, "kind": "port",
                                "sample": "1 spp of the same image, FP32 C++ restatement of the reference's path "

@@ -109,6 +109,18 @@ def test_spheres_render_matches_oracle():
     assert relmse(gpu, ref) < 5e-3, relmse(gpu, ref)
 
 
+def test_bench_sphere_scene_render_matches_oracle():
+    """The timed 10,000-sphere scene itself (the same seeded spheres, materials and lights as
+    the 1024x768 bench frame), at 256x192: the GPU frame against the oracle's, same streams."""
+    desc, cam = W.many_spheres(10_000, width=256, height=192)
+    assert len(desc["objects"]) >= 10_000
+    gpu = pb.Scene.from_description(desc).commit().render(cam, spp=4, max_depth=16, seed=3, rr_start=4)
+    ref = oracle.Scene(desc, np.float32).render(cam, 4, 16, seed=3, rr_start=4)
+    assert np.isfinite(gpu).all()
+    assert relmse(gpu, ref) < 5e-3, relmse(gpu, ref)
+    assert abs(gpu.mean() - ref.mean()) < 1e-2 * ref.mean()
+
+
 def test_naive_and_path_converge_to_the_same_image():
     """ideas/area_light.md:131-136: with the panel as the only light, the estimator that adds
     emission at every hit and the one that samples the light must agree."""
