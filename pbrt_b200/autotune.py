@@ -17,7 +17,7 @@ from typing import Optional
 from .scene import Batch, Context, create_scenes, default_context, render_params
 
 LEAF_SIZES = (1, 2, 4, 8)
-WAVES = (1 << 20, 1 << 21, 1 << 22, 1 << 23)
+WAVES = (1 << 22, 1 << 24, 1 << 26)
 SHAPES = ((64, 32), (128, 16), (256, 8), (128, 8), (256, 4))
 
 
@@ -42,7 +42,7 @@ def autotune(specs, ctx: Optional[Context] = None, sample: int = 8, trial_spp: i
     picked = [specs[i] for i in idx]
     params = [render_params(cam, trial_spp, d.get("max_depth", 8), seed=11) for d, cam, _ in picked]
     trials = []
-    best = {"wave_paths": 1 << 22, "trace_threads": 128, "trace_blocks_per_sm": 16, "shade_threads": 128,
+    best = {"wave_paths": 1 << 26, "trace_threads": 128, "trace_blocks_per_sm": 16, "shade_threads": 128,
             "shade_blocks_per_sm": 16}
 
     best_leaf, best_ms, best_scenes = None, None, None

@@ -1052,7 +1052,7 @@ int pbrt_ctx_set_tuning(pbrt_ctx* c, const pbrt_tuning* t) {
   pbrt_tuning d{};
   if (t) d = *t;
   LaunchShape sh;
-  const uint32_t wave = d.wave_paths ? d.wave_paths : (1u << 22);
+  const uint32_t wave = d.wave_paths ? d.wave_paths : (1u << 26);
   if (d.trace_threads) sh.trace_threads = d.trace_threads;
   if (d.trace_blocks_per_sm) sh.trace_blocks_per_sm = d.trace_blocks_per_sm;
   if (d.shade_threads) sh.shade_threads = d.shade_threads;
@@ -1063,7 +1063,7 @@ int pbrt_ctx_set_tuning(pbrt_ctx* c, const pbrt_tuning* t) {
     return c->fail(PBRT_ERR_INVALID_ARGUMENT, "threads per block must be a multiple of 32 in [32, 256]");
   if (bad_blocks(sh.trace_blocks_per_sm) || bad_blocks(sh.shade_blocks_per_sm))
     return c->fail(PBRT_ERR_INVALID_ARGUMENT, "blocks per SM must be in [1, 64]");
-  if (wave < 1024 || wave > (1u << 24)) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "wave_paths must be in [1024, 2^24]");
+  if (wave < 1024 || wave > (1u << 26)) return c->fail(PBRT_ERR_INVALID_ARGUMENT, "wave_paths must be in [1024, 2^26]");
   c->shape = sh;
   c->wave_paths = wave;
   return PBRT_OK;

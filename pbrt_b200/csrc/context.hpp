@@ -90,7 +90,7 @@ struct pbrt_ctx {
   bool slots_ready = false;
   std::vector<void*> allocs;
   pbrt::LaunchShape shape;          // wavefront launch shape (pbrt_ctx_set_tuning)
-  uint32_t wave_paths = 1u << 22;   // paths per wave
+  uint32_t wave_paths = 1u << 26;   // paths per wave (136 bytes of path state each, allocated on demand)
   int batch_kernel = 0;             // batches created afterwards: PBRT_BATCH_WAVEFRONT / _PERSISTENT
   // a cached render's training rounds beside its frame: their stream, the fork and join
   cudaStream_t side = nullptr;
