@@ -1541,6 +1541,37 @@ static cudaError_t bounce_loop(const WaveBuffers& w, const Src& src, const Cache
   return cudaSuccess;
 }
 
+// Paths from which a batch scene gets waves of its own (it fills a B200 alone: 148 SMs keep
+// about 0.3M threads resident).
+constexpr unsigned long long kBatchOwnWavePaths = 1ull << 20;
+
+// The waves of a batch frame, (first path, paths), in path order and covering every path,
+// none longer than `wave`: a scene of at least kBatchOwnWavePaths paths, or of more than
+// `wave`, gets waves of its own (the single-scene kernels, its own depth, its completion as
+// soon as it is done); smaller scenes are packed whole into shared waves.
+static std::vector<std::pair<unsigned long long, uint32_t>> batch_waves(const BatchScene* host_table,
+                                                                        uint32_t nscenes, uint32_t wave) {
+  std::vector<std::pair<unsigned long long, uint32_t>> waves;
+  unsigned long long pack_begin = 0, pack_n = 0;
+  auto flush = [&]() {
+    if (pack_n) waves.emplace_back(pack_begin, uint32_t(pack_n));
+    pack_n = 0;
+  };
+  for (uint32_t i = 0; i < nscenes; ++i) {
+    const unsigned long long b = host_table[i].begin, np = (unsigned long long)host_table[i].npix * host_table[i].spp;
+    if (np >= kBatchOwnWavePaths || np > wave) {
+      flush();
+      for (unsigned long long o = 0; o < np; o += wave) waves.emplace_back(b + o, uint32_t(np - o < wave ? np - o : wave));
+    } else {
+      if (pack_n + np > wave) flush();
+      if (!pack_n) pack_begin = b;
+      pack_n += np;
+    }
+  }
+  flush();
+  return waves;
+}
+
 cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, uint32_t nscenes, const WaveBuffers& w,
                          uint32_t wave, const uint32_t* frame, uint32_t max_depth, bool any_path_integrator,
                          const LaunchShape& shape, unsigned long long* stats, uint32_t* err, int sm_count,
@@ -1552,8 +1583,6 @@ cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, 
                    nscenes);
   k_films_batch<<<fgrid, 256, 0, st>>>(table, 1);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  const unsigned long long total =
-      host_table[nscenes - 1].begin + (unsigned long long)host_table[nscenes - 1].npix * host_table[nscenes - 1].spp;
   const ManyScenes src{table};
   uint32_t top_nodes = 0;
   bool csg = false;
@@ -1561,9 +1590,11 @@ cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, 
     top_nodes = top_nodes > host_table[i].view.top_node_count ? top_nodes : host_table[i].view.top_node_count;
     csg = csg || host_table[i].view.has_csg;
   }
+  const std::vector<std::pair<unsigned long long, uint32_t>> waves = batch_waves(host_table, nscenes, wave);
   uint32_t next_done = 0, first = 0;
-  for (unsigned long long base = 0; base < total; base += wave) {
-    const uint32_t n = uint32_t(total - base < wave ? total - base : wave);
+  for (const auto& wv : waves) {
+    const unsigned long long base = wv.first;
+    const uint32_t n = wv.second;
     // the scenes holding the wave's first and last paths (the table is in path order)
     while (host_table[first].begin + (unsigned long long)host_table[first].npix * host_table[first].spp <= base) ++first;
     uint32_t last = first;
