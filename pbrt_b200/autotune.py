@@ -1,6 +1,7 @@
 """Autotuner of the batched wavefront renderer: picks the BVH leaf size, the wave size
-(paths in flight, i.e. the queues' capacity) and the launch shape (threads per block and
-resident blocks per SM) of the traversal and shading kernels by timing trial batches.
+(paths in flight, i.e. the queues' capacity; by default only the largest is tried) and the
+launch shape (threads per block and resident blocks per SM) of the traversal and shading
+kernels by timing trial batches.
 
 Search: a sample of the batch's scenes (spread over the list), rendered at `trial_spp`
 samples per pixel as one graph-replayed batch; each trial's cost is the device time until the
@@ -17,7 +18,11 @@ from typing import Optional
 from .scene import Batch, Context, create_scenes, default_context, render_params
 
 LEAF_SIZES = (1, 2, 4, 8)
-WAVES = (1 << 22, 1 << 24, 1 << 26)
+# Wave size candidates: only the largest by default. A trial batch (a few scenes at 1-2 spp)
+# holds fewer paths than one wave, so it cannot show the wave size's effect; at frame scale
+# fewer, larger waves leave fewer per-bounce kernel tails (10,000 spheres at 1024x768x64 spp:
+# 139.7 ms a frame at 2^22 paths per wave, 103.7 ms at 2^26).
+WAVES = (1 << 26,)
 SHAPES = ((64, 32), (128, 16), (256, 8), (128, 8), (256, 4))
 
 
