@@ -39,8 +39,18 @@ static_assert(kXBytes >= kHBytes, "the inference kernel stores the hidden tile o
 
 __device__ __forceinline__ uint16_t to_bf16(float f) { return __bfloat16_as_ushort(__float2bfloat16_rn(f)); }
 __device__ __forceinline__ float from_bf16(uint16_t b) { return __uint_as_float(uint32_t(b) << 16); }
+// Two values to BF16 (round to nearest even), `a` in the low half: one cvt.rn.bf16x2.f32,
+// whose first source goes to the high half.
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
-  return uint32_t(to_bf16(a)) | (uint32_t(to_bf16(b)) << 16);
+  uint32_t d;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(b), "f"(a));
+  return d;
+}
+// The same after a ReLU (.relu clamps negative results to 0): the hidden layers' epilogue.
+__device__ __forceinline__ uint32_t pack2_relu(float a, float b) {
+  uint32_t d;
+  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(b), "f"(a));
+  return d;
 }
 
 // Encodes one query record into 96 features (82 used, zero padded).
@@ -283,14 +293,14 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_mlp_infer(Net net, Bounds 
           float v[16];
           tc::tmem_ld16(tmem + (lane_base << 16) + uint32_t(c), v);
           uint4 lo, hi;
-          lo.x = pack2(fmaxf(v[0], 0.f), fmaxf(v[1], 0.f));
-          lo.y = pack2(fmaxf(v[2], 0.f), fmaxf(v[3], 0.f));
-          lo.z = pack2(fmaxf(v[4], 0.f), fmaxf(v[5], 0.f));
-          lo.w = pack2(fmaxf(v[6], 0.f), fmaxf(v[7], 0.f));
-          hi.x = pack2(fmaxf(v[8], 0.f), fmaxf(v[9], 0.f));
-          hi.y = pack2(fmaxf(v[10], 0.f), fmaxf(v[11], 0.f));
-          hi.z = pack2(fmaxf(v[12], 0.f), fmaxf(v[13], 0.f));
-          hi.w = pack2(fmaxf(v[14], 0.f), fmaxf(v[15], 0.f));
+          lo.x = pack2_relu(v[0], v[1]);
+          lo.y = pack2_relu(v[2], v[3]);
+          lo.z = pack2_relu(v[4], v[5]);
+          lo.w = pack2_relu(v[6], v[7]);
+          hi.x = pack2_relu(v[8], v[9]);
+          hi.y = pack2_relu(v[10], v[11]);
+          hi.z = pack2_relu(v[12], v[13]);
+          hi.w = pack2_relu(v[14], v[15]);
           *reinterpret_cast<uint4*>(sX + tc::tile_offset(r, uint32_t(c), kTile)) = lo;
           *reinterpret_cast<uint4*>(sX + tc::tile_offset(r, uint32_t(c + 8), kTile)) = hi;
         }
