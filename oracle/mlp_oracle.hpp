@@ -40,31 +40,48 @@ inline float bf16(float f) {
   return r;
 }
 
-// sin(pi x) and cos(pi x) rounded to FP32: x is first reduced exactly modulo 2 (an FP32 x is
-// exact in double, and so is the remainder), multiples of 1/2 give exact 0 / +-1, any other x
-// the double-precision sine and cosine of pi times the remainder.
-inline void sincospi_f32(float x, double* s, double* c) {
-  double r = std::fmod(double(x), 2.0);
-  if (r < 0.0) r += 2.0;
-  if (r * 2.0 == std::floor(r * 2.0)) {  // r in {0, 0.5, 1, 1.5}
-    static const double ks[4] = {0.0, 1.0, 0.0, -1.0}, kc[4] = {1.0, 0.0, -1.0, 0.0};
-    const int q = int(r * 2.0);
-    *s = ks[q];
-    *c = kc[q];
-    return;
+// The network's sin(pi x) / cos(pi x) (the library's own method, restated): x reduced to
+// t in [-1/4, 1/4] and a quadrant q (k = rint(x / 2), r = x - 2k, q = rint(2r), t = r - q/2),
+// Taylor polynomials of sin(pi t) to t^9 and cos(pi t) to t^10 in Horner form with FP32
+// coefficients (-1)^k pi^(2k+1) / (2k+1)! and (-1)^k pi^(2k) / (2k)!, every product and sum
+// rounded to FP32 (no contraction: this file is built with -ffp-contract=off), then the
+// quadrant. The GPU performs the same operations, so the bits agree.
+inline void sincospi_poly(float x, float* s, float* c) {
+  const float k = std::rint(x * 0.5f);
+  const float r = x - k * 2.0f;
+  const float q = std::rint(r * 2.0f);
+  const float t = r - q * 0.5f;
+  const float t2 = t * t;
+  // (-1)^k pi^(2k+1) / (2k+1)!, k = 0..4, and (-1)^k pi^(2k) / (2k)!, k = 0..5, rounded to FP32
+  const float sc[5] = {0x1.921fb6p+1f, -0x1.4abbcep+2f, 0x1.466bc6p+1f, -0x1.32d2ccp-1f, 0x1.507834p-4f};
+  const float cc[6] = {1.0f, -0x1.3bd3ccp+2f, 0x1.03c1f0p+2f, -0x1.55d3c8p+0f, 0x1.e1f506p-3f, -0x1.a6d1f2p-6f};
+  float ps = sc[4];
+  for (int i = 3; i >= 0; --i) ps = ps * t2 + sc[i];
+  const float st = ps * t;
+  float pc = cc[5];
+  for (int i = 4; i >= 0; --i) pc = pc * t2 + cc[i];
+  const float ct = pc;
+  switch (int(q) & 3) {
+    case 0: *s = st; *c = ct; break;
+    case 1: *s = ct; *c = -st; break;
+    case 2: *s = -st; *c = -ct; break;
+    default: *s = -ct; *c = st; break;
   }
-  *s = double(float(std::sin(M_PI * r)));
-  *c = double(float(std::cos(M_PI * r)));
 }
 
-// Features of one record: sin/cos(pi * x * 2^j) of the normalised position, j < 12, then
-// wo, n, albedo, roughness.
+// Features of one record: sin/cos(pi * x * 2^j) of the normalised position, j < 12 (the
+// first band by sincospi_poly, each next one by the double-angle formulas sin 2a = 2 sin a
+// cos a, cos 2a = (cos a - sin a)(cos a + sin a) in FP32), then wo, n, albedo, roughness.
 inline void encode(const float* rec, const float* lo, const float* inv_ext, double* f) {
   for (int a = 0; a < 3; ++a) {
-    float x = (rec[a] - lo[a]) * inv_ext[a];
+    float s, c;
+    sincospi_poly((rec[a] - lo[a]) * inv_ext[a], &s, &c);
     for (int j = 0; j < 12; ++j) {
-      sincospi_f32(x, &f[a * 24 + 2 * j], &f[a * 24 + 2 * j + 1]);
-      x = x * 2.0f;
+      f[a * 24 + 2 * j] = s;
+      f[a * 24 + 2 * j + 1] = c;
+      const float s2 = (s * c) * 2.0f;
+      c = (c - s) * (c + s);
+      s = s2;
     }
   }
   f[72] = rec[4]; f[73] = rec[5]; f[74] = rec[6];

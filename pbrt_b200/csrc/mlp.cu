@@ -53,7 +53,49 @@ __device__ __forceinline__ uint32_t pack2_relu(float a, float b) {
   return d;
 }
 
-// Encodes one query record into 96 features (82 used, zero padded).
+// sin(pi x) and cos(pi x) in FP32, about 1.5 ulp: x reduced (k = rint(x / 2), r = x - 2k in
+// [-1, 1]; q = rint(2r), t = r - q / 2 in [-1/4, 1/4]), the Taylor polynomials of sin(pi t)
+// to t^9 and cos(pi t) to t^10 (truncation below 2e-9 there) in Horner form, each step one
+// rounded multiply and one rounded add (no fused multiply-add, so a host computes the same
+// bits), then the quadrant q. Coefficients: (-1)^k pi^(2k+1) / (2k+1)! and (-1)^k pi^(2k) /
+// (2k)!, rounded to FP32.
+__device__ __forceinline__ void sincospi_poly(float x, float& s, float& c) {
+  const float k = rintf(__fmul_rn(x, 0.5f));
+  const float r = __fsub_rn(x, __fmul_rn(k, 2.0f));
+  const float q = rintf(__fmul_rn(r, 2.0f));
+  const float t = __fsub_rn(r, __fmul_rn(q, 0.5f));
+  const float t2 = __fmul_rn(t, t);
+  float ps = 0x1.507834p-4f;
+  ps = __fadd_rn(__fmul_rn(ps, t2), -0x1.32d2ccp-1f);
+  ps = __fadd_rn(__fmul_rn(ps, t2), 0x1.466bc6p+1f);
+  ps = __fadd_rn(__fmul_rn(ps, t2), -0x1.4abbcep+2f);
+  ps = __fadd_rn(__fmul_rn(ps, t2), 0x1.921fb6p+1f);
+  const float st = __fmul_rn(ps, t);
+  float pc = -0x1.a6d1f2p-6f;
+  pc = __fadd_rn(__fmul_rn(pc, t2), 0x1.e1f506p-3f);
+  pc = __fadd_rn(__fmul_rn(pc, t2), -0x1.55d3c8p+0f);
+  pc = __fadd_rn(__fmul_rn(pc, t2), 0x1.03c1f0p+2f);
+  pc = __fadd_rn(__fmul_rn(pc, t2), -0x1.3bd3ccp+2f);
+  const float ct = __fadd_rn(__fmul_rn(pc, t2), 1.0f);
+  switch (int(q) & 3) {
+    case 0: s = st; c = ct; break;
+    case 1: s = ct; c = -st; break;
+    case 2: s = -st; c = -ct; break;
+    default: s = -ct; c = st; break;
+  }
+}
+
+// The next octave of a band: sin 2a = 2 sin a cos a, cos 2a = (cos a - sin a)(cos a + sin a),
+// each operation rounded (the error doubles per octave: 2e-4 at the twelfth band).
+__device__ __forceinline__ void next_octave(float& s, float& c) {
+  const float s2 = __fmul_rn(__fmul_rn(s, c), 2.0f);
+  c = __fmul_rn(__fsub_rn(c, s), __fadd_rn(c, s));
+  s = s2;
+}
+
+// Encodes one query record into 96 features (82 used, zero padded): sin / cos (pi 2^j x) of the
+// normalised position, j < 12 (the first band by sincospi_poly, the others by next_octave),
+// then wo, n, albedo, roughness.
 __device__ void encode(const float* __restrict__ rec, const Bounds& b, float* f) {
   const float4 q0 = __ldg(reinterpret_cast<const float4*>(rec));
   const float4 q1 = __ldg(reinterpret_cast<const float4*>(rec) + 1);
@@ -62,14 +104,13 @@ __device__ void encode(const float* __restrict__ rec, const Bounds& b, float* f)
   const float p[3] = {q0.x, q0.y, q0.z};
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    float x = (p[a] - b.lo[a]) * b.inv_extent[a];
+    float s, c;
+    sincospi_poly(__fmul_rn(__fsub_rn(p[a], b.lo[a]), b.inv_extent[a]), s, c);
 #pragma unroll
     for (int j = 0; j < 12; ++j) {
-      float s, c;
-      sincospif(x, &s, &c);
       f[a * 24 + 2 * j] = s;
       f[a * 24 + 2 * j + 1] = c;
-      x = x * 2.0f;
+      next_octave(s, c);
     }
   }
   f[72] = q1.x; f[73] = q1.y; f[74] = q1.z;
@@ -239,17 +280,16 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_mlp_infer(Net net, Bounds 
       const float p[3] = {q0.x, q0.y, q0.z};
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        float x = (p[a] - b.lo[a]) * b.inv_extent[a];
+        float sn, cs;
+        sincospi_poly(__fmul_rn(__fsub_rn(p[a], b.lo[a]), b.inv_extent[a]), sn, cs);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           float v[8];
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
-            float sn, cs;
-            sincospif(x, &sn, &cs);
             v[2 * j] = valid ? sn : 0.f;
             v[2 * j + 1] = valid ? cs : 0.f;
-            x = x * 2.0f;
+            next_octave(sn, cs);
           }
           uint4 qq;
           qq.x = pack2(v[0], v[1]);
