@@ -551,6 +551,7 @@ def _declare_mlp(L):
     L.oracle_mlp_forward_f64.argtypes = [vp, vp, vp, C.c_size_t, vp]
     L.oracle_mlp_forward_margins.argtypes = [vp, vp, vp, C.c_size_t, vp, vp, vp, C.c_int]
     L.oracle_mlp_adam.argtypes = [vp, vp, vp, vp, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float]
+    L.oracle_mlp_encode.argtypes = [vp, vp, C.c_size_t, vp]
 
 
 def _mlp_lib():
@@ -559,6 +560,15 @@ def _mlp_lib():
         _declare_mlp(L)
         L._mlp_declared = True
     return L
+
+
+def mlp_encode(bounds, records):
+    """The network's input features (n, 96) of query records (n, 16) (mlp_oracle.hpp encode)."""
+    b = np.ascontiguousarray(bounds, np.float32).reshape(6)
+    r = np.ascontiguousarray(records, np.float32).reshape(-1, 16)
+    out = np.zeros((r.shape[0], 96), np.float32)
+    _mlp_lib().oracle_mlp_encode(_ptr(b), _ptr(r), r.shape[0], _ptr(out))
+    return out
 
 
 def mlp_forward(weights, bounds, records, emulate=True, threads: int = os.cpu_count() or 1):

@@ -563,6 +563,18 @@ static void mlp_bounds(const float* b6, float* lo, float* inv) {
   }
 }
 
+// The network's input features of n records (kInPad per record, the encoding the forward pass uses).
+int oracle_mlp_encode(const float* bounds6, const float* records, size_t n, float* features) {
+  float lo[3], inv[3];
+  mlp_bounds(bounds6, lo, inv);
+  for (size_t i = 0; i < n; ++i) {
+    double f[oracle::mlp::kInPad];
+    oracle::mlp::encode(records + i * oracle::mlp::kRecord, lo, inv, f);
+    for (int k = 0; k < oracle::mlp::kInPad; ++k) features[i * oracle::mlp::kInPad + k] = float(f[k]);
+  }
+  return 0;
+}
+
 int oracle_mlp_forward(const float* weights, const float* bounds6, const float* records, size_t n, float* out,
                        int emulate, int threads) {
   const oracle::mlp::Net net(weights, emulate != 0);

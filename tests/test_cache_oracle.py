@@ -92,3 +92,54 @@ def test_adam_formula():
     np.testing.assert_array_equal(m, mm)
     np.testing.assert_array_equal(v, vv)
     np.testing.assert_allclose(w, w0 - f(1e-2) * (mm / c1) / (np.sqrt(vv / c2) + f(1e-8)), rtol=1e-6)
+
+
+def _emulated_bands(x):
+    """The position encoding's documented FP32 operations, emulated in numpy float32: one
+    polynomial sin / cos (pi x) (reduction to |t| <= 1/4 and a quadrant, Taylor coefficients
+    rounded to FP32, Horner with rounded multiplies and adds), then double-angle octaves."""
+    f = np.float32
+    sc = [f(float.fromhex(h)) for h in ("0x1.921fb6p+1", "-0x1.4abbcep+2", "0x1.466bc6p+1", "-0x1.32d2ccp-1",
+                                        "0x1.507834p-4")]
+    cc = [f(float.fromhex(h)) for h in ("0x1p+0", "-0x1.3bd3ccp+2", "0x1.03c1f0p+2", "-0x1.55d3c8p+0",
+                                        "0x1.e1f506p-3", "-0x1.a6d1f2p-6")]
+    x = x.astype(np.float32)
+    k = np.rint(x * f(0.5)).astype(np.float32)
+    r = (x - k * f(2)).astype(np.float32)
+    q = np.rint(r * f(2)).astype(np.float32)
+    t = (r - q * f(0.5)).astype(np.float32)
+    t2 = (t * t).astype(np.float32)
+    ps = np.full_like(t, sc[4])
+    for c in sc[3::-1]:
+        ps = ((ps * t2).astype(np.float32) + c).astype(np.float32)
+    st = (ps * t).astype(np.float32)
+    pc = np.full_like(t, cc[5])
+    for c in cc[4::-1]:
+        pc = ((pc * t2).astype(np.float32) + c).astype(np.float32)
+    qi = q.astype(np.int64) & 3
+    s = np.select([qi == 0, qi == 1, qi == 2], [st, pc, -st], -pc).astype(np.float32)
+    c = np.select([qi == 0, qi == 1, qi == 2], [pc, -st, -pc], st).astype(np.float32)
+    bands = []
+    for _ in range(12):
+        bands += [s, c]
+        s, c = ((s * c).astype(np.float32) * f(2)).astype(np.float32), ((c - s) * (c + s)).astype(np.float32)
+    return np.stack(bands, axis=1)
+
+
+def test_position_encoding_pinned():
+    """The oracle's position features equal, bit for bit, an independent numpy emulation of
+    the documented FP32 operations, and stay within 1.5e-7 of sin / cos (pi 2^j x) at the
+    first band and 2^j x 3e-7 at band j (each double-angle step doubles the error it carries
+    and adds about one rounding)."""
+    r = random_records(20000, BOUNDS[:3], BOUNDS[3:], seed=5)
+    r[:64, 0] = np.linspace(-1.0, 1.0, 64, dtype=np.float32)  # quadrant edges: x = 0, 1/4, 1/2, ...
+    feat = oracle.mlp_encode(BOUNDS, r)
+    x = ((r[:, :3] - BOUNDS[:3]) * (np.float32(1) / (BOUNDS[3:] - BOUNDS[:3]))).astype(np.float32)
+    for a in range(3):
+        got = feat[:, 24 * a:24 * a + 24]
+        assert np.array_equal(got.view(np.uint32), _emulated_bands(x[:, a]).view(np.uint32))
+        for j in range(12):
+            ang = np.pi * x[:, a].astype(np.float64) * 2.0 ** j
+            err = max(np.abs(got[:, 2 * j] - np.sin(ang)).max(), np.abs(got[:, 2 * j + 1] - np.cos(ang)).max())
+            assert err <= (1.5e-7 if j == 0 else 2.0 ** j * 3e-7), (a, j, err)
+    assert np.array_equal(feat[:, 72:75], r[:, 4:7]) and np.array_equal(feat[:, 81], r[:, 3])
