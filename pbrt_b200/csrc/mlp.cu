@@ -213,7 +213,7 @@ __device__ __forceinline__ void release_tmem(uint32_t tmem, uint64_t* mbar, uint
 // barrier and 64 TMEM columns, so six tiles' GEMM chains are in flight per SM: while one
 // group waits on its GEMM the others encode, read TMEM or store activations. (Three CTAs of
 // one tile each, every CTA with its own copy of the weights, was the shared-memory limit.)
-constexpr int kInferGroups = 6;
+constexpr int kInferGroups = 6;  // 7 (72 registers, spills) measured 4 % slower
 constexpr int kInferThreads = kInferGroups * kTile;  // 768
 constexpr uint32_t kInferTmemCols = 512;             // 6 x 64 columns, rounded up to a power of two
 static_assert(kInferGroups * kTmemCols <= kInferTmemCols, "the groups' accumulators must fit the allocation");
@@ -262,21 +262,31 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_mlp_infer(Net net, Bounds 
   uint32_t phase = 0;
   bool ok = true;
   const uint64_t tiles = (n + kTile - 1) / kTile;
-  for (uint64_t tile = uint64_t(blockIdx.x) * kInferGroups + g; tile < tiles && ok;
-       tile += uint64_t(gridDim.x) * kInferGroups) {
+  const uint64_t tile_step = uint64_t(gridDim.x) * kInferGroups;
+  // A row's record, loaded one tile ahead: the next tile's loads are in flight while this
+  // tile's features are encoded and its GEMM chain runs.
+  auto load_record = [&](uint64_t t, float4& a, float4& b1, float4& c1, float4& d1) {
+    const uint64_t rw = t * kTile + r;
+    if (t < tiles && rw < n) {
+      const float4* qr = reinterpret_cast<const float4*>(rec + rw * kRecord);
+      a = __ldg(qr);
+      b1 = __ldg(qr + 1);
+      c1 = __ldg(qr + 2);
+      d1 = __ldg(qr + 3);
+    } else {
+      a = b1 = c1 = d1 = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  };
+  float4 n0, n1, n2, n3;
+  load_record(uint64_t(blockIdx.x) * kInferGroups + g, n0, n1, n2, n3);
+  for (uint64_t tile = uint64_t(blockIdx.x) * kInferGroups + g; tile < tiles && ok; tile += tile_step) {
     const uint64_t row = tile * kTile + r;
     {
       // encode(): the features in 8-column chunks, 3 axes x 3 chunks of sin/cos bands, then the
       // 10 record values, without a 96-value array in registers
-      float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = q0, q2 = q0, q3 = q0;
+      const float4 q0 = n0, q1 = n1, q2 = n2, q3 = n3;
+      load_record(tile + tile_step, n0, n1, n2, n3);
       const bool valid = row < n;
-      if (valid) {
-        const float4* qr = reinterpret_cast<const float4*>(rec + row * kRecord);
-        q0 = __ldg(qr);
-        q1 = __ldg(qr + 1);
-        q2 = __ldg(qr + 2);
-        q3 = __ldg(qr + 3);
-      }
       const float p[3] = {q0.x, q0.y, q0.z};
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
