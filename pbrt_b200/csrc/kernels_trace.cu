@@ -102,10 +102,10 @@ __global__ void __launch_bounds__(kCullThreads, kDense ? 4 : 0) k_cull_root(Mesh
   const float4 rlo = __ldg(&m.nodes[0]);
   const float4 rhi = __ldg(&m.nodes[1]);
   const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const uint64_t per_iter = uint64_t(gridDim.x) * kCullThreads * kCullRays;
+  const uint64_t per_iter = uint64_t(gridDim.x) * blockDim.x * kCullRays;  // blockDim.x <= kCullThreads
   const uint64_t iters = (n + per_iter - 1) / per_iter;  // uniform across the grid: __syncthreads is safe
   for (uint64_t it = 0; it < iters; ++it) {
-    const uint64_t i0 = it * per_iter + (uint64_t(blockIdx.x) * kCullThreads + threadIdx.x) * kCullRays;
+    const uint64_t i0 = it * per_iter + (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) * kCullRays;
     float v[8][kCullRays];
     const bool full = i0 + kCullRays <= n;
     if (kVec && full) {
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(kCullThreads, kDense ? 4 : 0) k_cull_root(Mesh
     __syncthreads();
     if (threadIdx.x == 0) {
       uint32_t run = 0;
-      for (int w = 0; w < kCullThreads / 32; ++w) {
+      for (int w = 0; w < int(blockDim.x / 32); ++w) {
         const uint32_t t = warp_off[buf][w];
         warp_off[buf][w] = run;
         run += t;
@@ -678,12 +678,20 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
     k_dense_finalize<true><<<cg, kCullThreads, 0, s>>>(dense->res, dense->mask, dense->bases, n, prim, t, obj);
     return cudaGetLastError();
   }
+  // PBRT_CULL_THREADS=128: the cull in 128-thread blocks, twice as many (for measurements)
+  static const unsigned cull_threads = [] {
+    const char* e = std::getenv("PBRT_CULL_THREADS");
+    return e && std::strcmp(e, "128") == 0 ? 128u : unsigned(kCullThreads);
+  }();
+  const uint64_t cpb = uint64_t(cull_threads) * kCullRays;
+  const uint64_t cneed = (n + cpb - 1) / cpb, ccap = uint64_t(sm_count) * 8 * (kCullThreads / cull_threads);
+  const unsigned cgt = unsigned(cneed < ccap ? cneed : ccap);
   if (vec)
-    k_cull_root<true, false><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec,
-                                                          nullptr, nullptr);
-  else
-    k_cull_root<false, false><<<cg, kCullThreads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec,
+    k_cull_root<true, false><<<cgt, cull_threads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec,
                                                            nullptr, nullptr);
+  else
+    k_cull_root<false, false><<<cgt, cull_threads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec,
+                                                            nullptr, nullptr);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (!ts.voted) {
