@@ -162,6 +162,7 @@ inline int check_device_error(pbrt_ctx* c, cudaStream_t s) {
   PBRT_TRY(c->cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize"));
   if (h & kErrStack) return c->fail(PBRT_ERR_CAPACITY, "traversal stack capacity exceeded");
   if (h & 4u) return c->fail(PBRT_ERR_DEVICE_BUDGET, "a tensor-core completion wait ran out of its budget");
+  if (h & kErrCopy) return c->fail(PBRT_ERR_DEVICE_BUDGET, "a wait for a bulk copy into shared memory ran out of its budget");
   return c->fail(PBRT_ERR_DEVICE_BUDGET, "a traversal exceeded its iteration budget (malformed tree)");
 }
 

@@ -24,6 +24,7 @@
 #include <cstring>
 
 #include "kernels.hpp"
+#include "tcgen05.cuh"
 #include "trace_mesh.cuh"
 
 namespace pbrt {
@@ -182,6 +183,126 @@ __global__ void __launch_bounds__(kCullThreads, kDense ? 4 : 0) k_cull_root(Mesh
           rec[2 * pos + 1] = make_float4(v[3][j], v[4][j], v[5][j], v[7][j]);
         }
         if (!kDense) queue[pos] = uint32_t(i0 + j);
+        ++pos;
+      }
+  }
+}
+
+// The cull with its rays staged through shared memory by bulk asynchronous copies (the plain
+// cp.async.bulk, no tensor map, no multicast), double-buffered: while a block tests, scans and
+// compacts one 512-ray chunk, the next chunk's eight plane segments (2 KB each) are already on
+// their way. The answers are k_cull_root's (same tests, same compaction, same records).
+// Requires kVec's alignment (planes and outputs 16-byte aligned, stride a multiple of 4). The
+// last, partial chunk is read directly. A copy wait that runs out of its budget sets kErrCopy.
+constexpr int kBulkThreads = 128;
+constexpr uint32_t kBulkChunk = kBulkThreads * kCullRays;  // rays per chunk
+constexpr uint32_t kBulkPlaneBytes = kBulkChunk * 4;         // one plane's segment
+
+__global__ void __launch_bounds__(kBulkThreads) k_cull_root_bulk(MeshView m, const float* __restrict__ rays,
+                                                                 uint64_t stride, uint64_t n,
+                                                                 uint32_t* __restrict__ prim, float* __restrict__ tout,
+                                                                 uint32_t* __restrict__ obj, uint32_t* __restrict__ queue,
+                                                                 unsigned long long* __restrict__ queue_count,
+                                                                 float4* __restrict__ rec, uint32_t* __restrict__ err) {
+  __shared__ __align__(128) float sbuf[2][8][kBulkChunk];  // 32 KB
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t warp_off[2][kBulkThreads / 32];
+  __shared__ unsigned long long blk_base[2];
+  const float4 rlo = __ldg(&m.nodes[0]);
+  const float4 rhi = __ldg(&m.nodes[1]);
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint64_t full_chunks = n / kBulkChunk;  // chunks read by bulk copies
+  const uint64_t chunks = (n + kBulkChunk - 1) / kBulkChunk;
+  const uint64_t iters = (chunks + gridDim.x - 1) / gridDim.x;  // uniform across the grid
+  // thread 0 starts chunk c's copies into buffer b (c < full_chunks)
+  auto issue = [&](uint64_t c, int b) {
+    tc::fence_smem_to_async();  // the buffer's previous contents were read by ordinary loads
+    tc::mbar_arrive_expect_tx(&mbar[b], 8u * kBulkPlaneBytes);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) tc::bulk_g2s(&sbuf[b][p][0], rays + p * stride + c * kBulkChunk, kBulkPlaneBytes, &mbar[b]);
+  };
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&mbar[0], 1);
+    tc::mbar_init(&mbar[1], 1);
+    if (uint64_t(blockIdx.x) < full_chunks) issue(blockIdx.x, 0);
+  }
+  __syncthreads();
+  for (uint64_t it = 0; it < iters; ++it) {
+    const uint64_t c = uint64_t(blockIdx.x) + it * gridDim.x;
+    const int b = int(it & 1);
+    // The next chunk's copies go out now; its buffer was last read in the previous
+    // iteration, before that iteration's barriers.
+    if (threadIdx.x == 0 && c + gridDim.x < full_chunks) issue(c + gridDim.x, b ^ 1);
+    const uint64_t i0 = c * kBulkChunk + uint64_t(threadIdx.x) * kCullRays;
+    float v[8][kCullRays];
+    const bool bulk = c < full_chunks;
+    if (bulk) {
+      // buffer b's (it >> 1)-th use: full chunks come first, so every earlier use was a copy
+      if (!tc::mbar_wait(&mbar[b], uint32_t((it >> 1) & 1u))) atomicOr(err, kErrCopy);
+#pragma unroll
+      for (int p = 0; p < 8; ++p) {
+        const float4 q = *reinterpret_cast<const float4*>(&sbuf[b][p][threadIdx.x * kCullRays]);
+        v[p][0] = q.x; v[p][1] = q.y; v[p][2] = q.z; v[p][3] = q.w;
+      }
+    } else {
+#pragma unroll
+      for (int p = 0; p < 8; ++p)
+#pragma unroll
+        for (int j = 0; j < kCullRays; ++j) v[p][j] = (i0 + j < n) ? __ldcs(rays + p * stride + i0 + j) : 0.f;
+    }
+    unsigned enter = 0;
+#pragma unroll
+    for (int j = 0; j < kCullRays; ++j) {
+      if (i0 + j < n) {
+        float entry;
+        const PRay r = prepare_ray(mk3(v[0][j], v[1][j], v[2][j]), mk3(v[3][j], v[4][j], v[5][j]));
+        // entered, and not dropped at its first pop for entry >= min_t = FLT_MAX (bvh.rs:462-472)
+        if (box_hit(r, rlo, rhi, v[6][j], v[7][j], entry) && entry < FLT_MAX) enter |= 1u << j;
+      }
+    }
+    if (i0 + kCullRays <= n) {  // every ray gets the miss answer now; stage 2 overwrites the hits
+      __stcs(reinterpret_cast<uint4*>(prim + i0), make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu));
+      const float inf = __int_as_float(0x7f800000);
+      __stcs(reinterpret_cast<float4*>(tout + i0), make_float4(inf, inf, inf, inf));
+      if (obj)
+        __stcs(reinterpret_cast<uint4*>(obj + i0), make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu));
+    } else {
+      for (int j = 0; j < kCullRays; ++j)
+        if (i0 + j < n) {
+          __stcs(prim + i0 + j, 0xFFFFFFFFu);
+          __stcs(tout + i0 + j, __int_as_float(0x7f800000));
+          if (obj) __stcs(obj + i0 + j, 0xFFFFFFFFu);
+        }
+    }
+    // Block-wide exclusive scan of the survivor counts: one atomicAdd per block.
+    const uint32_t cnt = __popc(enter);
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= unsigned(off)) incl += y;
+    }
+    if (lane == 31) warp_off[b][warp] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t run = 0;
+      for (int w = 0; w < kBulkThreads / 32; ++w) {
+        const uint32_t t = warp_off[b][w];
+        warp_off[b][w] = run;
+        run += t;
+      }
+      blk_base[b] = run ? atomicAdd(queue_count, (unsigned long long)run) : 0ull;
+    }
+    __syncthreads();
+    uint64_t pos = blk_base[b] + warp_off[b][warp] + (incl - cnt);
+#pragma unroll
+    for (int j = 0; j < kCullRays; ++j)
+      if (enter & (1u << j)) {
+        if (rec) {  // read back soon by stage 2: default caching
+          rec[2 * pos] = make_float4(v[0][j], v[1][j], v[2][j], v[6][j]);
+          rec[2 * pos + 1] = make_float4(v[3][j], v[4][j], v[5][j], v[7][j]);
+        }
+        queue[pos] = uint32_t(i0 + j);
         ++pos;
       }
   }
@@ -678,6 +799,21 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
     k_dense_finalize<true><<<cg, kCullThreads, 0, s>>>(dense->res, dense->mask, dense->bases, n, prim, t, obj);
     return cudaGetLastError();
   }
+  // PBRT_CULL_BULK=1: the cull staged through shared memory by bulk copies (k_cull_root_bulk)
+  static const bool cull_bulk = [] {
+    const char* e = std::getenv("PBRT_CULL_BULK");
+    return e && std::strcmp(e, "1") == 0;
+  }();
+  if (vec && cull_bulk) {
+    static const int bulk_per_sm = [] {
+      int b = 0;
+      const cudaError_t oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cull_root_bulk, kBulkThreads, 0);
+      return oe == cudaSuccess && b > 0 ? b : 4;
+    }();
+    const uint64_t bneed = (n + kBulkChunk - 1) / kBulkChunk, bcap = uint64_t(sm_count) * bulk_per_sm;
+    k_cull_root_bulk<<<unsigned(bneed < bcap ? bneed : bcap), kBulkThreads, 0, s>>>(m, rays, stride, n, prim, t, obj,
+                                                                                   queue, counters, rec, err);
+  }
   // The cull in 128-thread blocks, twice as many as 256-thread ones: more independent
   // load / scan / atomicAdd chains per SM (0.5 % faster per 16M-ray step, three alternating
   // pairs). PBRT_CULL_THREADS=256 selects the larger blocks for measurements.
@@ -688,10 +824,10 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
   const uint64_t cpb = uint64_t(cull_threads) * kCullRays;
   const uint64_t cneed = (n + cpb - 1) / cpb, ccap = uint64_t(sm_count) * 8 * (kCullThreads / cull_threads);
   const unsigned cgt = unsigned(cneed < ccap ? cneed : ccap);
-  if (vec)
+  if (vec && !cull_bulk)
     k_cull_root<true, false><<<cgt, cull_threads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec,
                                                            nullptr, nullptr);
-  else
+  else if (!vec)
     k_cull_root<false, false><<<cgt, cull_threads, 0, s>>>(m, rays, stride, n, prim, t, obj, queue, counters, rec,
                                                             nullptr, nullptr);
   e = cudaGetLastError();

@@ -97,6 +97,23 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity) {
   return ok != 0;
 }
 
+// Arrives on the barrier (one of its expected arrivals) and adds `bytes` to the transaction
+// count its current phase waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes)
+               : "memory");
+}
+
+// Bulk asynchronous copy of `bytes` (a multiple of 16) from global memory to this CTA's shared
+// memory, both addresses 16-byte aligned; its bytes complete on `mbar`'s transaction count.
+// Plain form: no tensor map, no multicast.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(mbar))
+               : "memory");
+}
+
 // Waits for phase `parity` of the barrier; gives up after `budget` polls and returns false.
 __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t budget = 1u << 22) {
   for (uint32_t i = 0; i < budget; ++i)

@@ -29,6 +29,7 @@ constexpr int kTraceStack = 64;  // scenes whose trees are deeper are refused at
 enum DeviceError : uint32_t {
   kErrBudget = 1u,  // a traversal exceeded its iteration budget (malformed tree)
   kErrStack = 2u,   // a traversal stack would have overflowed
+  kErrCopy = 8u,    // a wait for a bulk copy into shared memory ran out of its budget
 };
 
 // One 32-byte node record (bmin|left_first, bmax|count) as a single 256-bit load. Node

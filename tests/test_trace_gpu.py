@@ -176,6 +176,8 @@ np.savez({out!r}, rays=rays, dp=dp.cpu().numpy().view(np.uint32), dt=dt.cpu().nu
 _FORMS = {
     "default": {},
     "dense results": {"PBRT_TRACE_DENSE": "1"},
+    "cull through bulk copies": {"PBRT_CULL_BULK": "1"},
+    "cull in 256-thread blocks": {"PBRT_CULL_THREADS": "256"},
     "drained-queue schedule as the bulk's": {"PBRT_TRACE_SCHEDULE": "8,8,8"},
     "drained-queue schedule 1, 2": {"PBRT_TRACE_SCHEDULE": "8,8,8,1,2"},
 }
@@ -185,15 +187,16 @@ _FORMS = {
 def test_two_stage_forms_match_oracle(tmp_path, form):
     """Every form of the two-stage pass gives the oracle's ids and t, on device buffers with a
     partial last chunk and on host buffers: the cull's miss answers plus scattered hit stores;
-    the survivor bitmask, results by queue slot and the ray-order pass; other schedules once
-    the queue is drained. The switches are read once per process: a child per form."""
+    the survivor bitmask, results by queue slot and the ray-order pass; the cull's rays
+    staged by bulk copies, or in 256-thread blocks; other schedules once the queue is
+    drained. The switches are read once per process: a child per form."""
     import os
     import subprocess
     import sys
 
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     out = str(tmp_path / "form.npz")
-    env = {k: v for k, v in os.environ.items() if not k.startswith("PBRT_TRACE_")}
+    env = {k: v for k, v in os.environ.items() if not k.startswith(("PBRT_TRACE_", "PBRT_CULL_"))}
     env.update(_FORMS[form])
     subprocess.run([sys.executable, "-c", _DENSE_SCRIPT.format(root=root, out=out)], env=env, check=True,
                    timeout=600)
