@@ -227,6 +227,7 @@ __global__ void __launch_bounds__(kBulkThreads) k_cull_root_bulk(MeshView m, con
     if (uint64_t(blockIdx.x) < full_chunks) issue(blockIdx.x, 0);
   }
   __syncthreads();
+  bool copies_ok = true;  // false after a wait ran out: this thread reads directly from then on
   for (uint64_t it = 0; it < iters; ++it) {
     const uint64_t c = uint64_t(blockIdx.x) + it * gridDim.x;
     const int b = int(it & 1);
@@ -235,10 +236,12 @@ __global__ void __launch_bounds__(kBulkThreads) k_cull_root_bulk(MeshView m, con
     if (threadIdx.x == 0 && c + gridDim.x < full_chunks) issue(c + gridDim.x, b ^ 1);
     const uint64_t i0 = c * kBulkChunk + uint64_t(threadIdx.x) * kCullRays;
     float v[8][kCullRays];
-    const bool bulk = c < full_chunks;
-    if (bulk) {
-      // buffer b's (it >> 1)-th use: full chunks come first, so every earlier use was a copy
-      if (!tc::mbar_wait(&mbar[b], uint32_t((it >> 1) & 1u))) atomicOr(err, kErrCopy);
+    // buffer b's (it >> 1)-th use: full chunks come first, so every earlier use was a copy
+    if (c < full_chunks && copies_ok && !tc::mbar_wait(&mbar[b], uint32_t((it >> 1) & 1u))) {
+      atomicOr(err, kErrCopy);
+      copies_ok = false;
+    }
+    if (c < full_chunks && copies_ok) {
 #pragma unroll
       for (int p = 0; p < 8; ++p) {
         const float4 q = *reinterpret_cast<const float4*>(&sbuf[b][p][threadIdx.x * kCullRays]);
