@@ -176,8 +176,8 @@ np.savez({out!r}, rays=rays, dp=dp.cpu().numpy().view(np.uint32), dt=dt.cpu().nu
 _FORMS = {
     "default": {},
     "dense results": {"PBRT_TRACE_DENSE": "1"},
-    "cull through bulk copies": {"PBRT_CULL_BULK": "1"},
-    "cull in 256-thread blocks": {"PBRT_CULL_THREADS": "256"},
+    "cull by direct loads": {"PBRT_CULL_BULK": "0"},
+    "cull by direct loads, 256-thread blocks": {"PBRT_CULL_BULK": "0", "PBRT_CULL_THREADS": "256"},
     "drained-queue schedule as the bulk's": {"PBRT_TRACE_SCHEDULE": "8,8,8"},
     "drained-queue schedule 1, 2": {"PBRT_TRACE_SCHEDULE": "8,8,8,1,2"},
 }
@@ -188,7 +188,7 @@ def test_two_stage_forms_match_oracle(tmp_path, form):
     """Every form of the two-stage pass gives the oracle's ids and t, on device buffers with a
     partial last chunk and on host buffers: the cull's miss answers plus scattered hit stores;
     the survivor bitmask, results by queue slot and the ray-order pass; the cull's rays
-    staged by bulk copies, or in 256-thread blocks; other schedules once the queue is
+    staged by bulk copies (the default) or read directly, in 128- or 256-thread blocks; other schedules once the queue is
     drained. The switches are read once per process: a child per form."""
     import os
     import subprocess
