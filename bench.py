@@ -170,14 +170,16 @@ def _kernel_profile():
 def _per_kernel(launch_ms: float, n_rays: int, box_pr: float, tri_pr: float, peak: float):
     """The call's two kernels apart: each one's time is the live call time times its share
     of the captured pass (ncu times are serialised and cold, so only their ratio is used).
-    k_cull_root streams rays: its figure is its captured DRAM bytes over that time.
+    The cull (k_cull_root_bulk, or k_cull_root) streams rays: its figure is its captured DRAM
+    bytes over that time.
     k_mesh_closest_persistent walks the survivors: its algorithmic bytes are the node and
     triangle fetches beyond the root test, 32 (box tests - 1) + 36 triangle tests per ray."""
     d = _kernel_profile()
     if not d:
         return None
     k = d["kernels"]
-    cull, trav = k["k_cull_root"], k["k_mesh_closest_persistent"]
+    cull_name = "k_cull_root_bulk" if "k_cull_root_bulk" in k else "k_cull_root"
+    cull, trav = k[cull_name], k["k_mesh_closest_persistent"]
     total_ns = float(cull["ns"] + trav["ns"])
     scale = n_rays / float(d["rays_per_launch"])
     cull_ms, trav_ms = launch_ms * cull["ns"] / total_ns, launch_ms * trav["ns"] / total_ns
@@ -185,7 +187,7 @@ def _per_kernel(launch_ms: float, n_rays: int, box_pr: float, tri_pr: float, pea
     trav_bytes = (32 * (box_pr - 1) + 36 * tri_pr) * n_rays
     trav_gbs = trav_bytes / (trav_ms * 1e-3) / 1e9
     return {
-        "k_cull_root": {"share": round(cull["ns"] / total_ns, 4), "ms": round(cull_ms, 4),
+        cull_name: {"share": round(cull["ns"] / total_ns, 4), "ms": round(cull_ms, 4),
                         "dram_gbs": round(cull_gbs, 1), "frac": round(cull_gbs / peak, 4),
                         "limiter": "HBM: streams the 32-byte rays and writes every answer"},
         "k_mesh_closest_persistent": {"share": round(trav["ns"] / total_ns, 4), "ms": round(trav_ms, 4),
