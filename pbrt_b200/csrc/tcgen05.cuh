@@ -1,7 +1,8 @@
 // tcgen05.cuh — the sm_100a tensor-core primitives the radiance-cache MLP uses, as inline
 // PTX: TMEM allocation, tcgen05.mma (kind::f16, BF16 in, FP32 accumulate, one CTA),
 // tcgen05.commit to an mbarrier, tcgen05.ld of the accumulator, and the fences that order
-// them against ordinary shared-memory traffic.
+// them against ordinary shared-memory traffic; plus the mbarrier transaction counts and the
+// plain bulk global-to-shared copy (cp.async.bulk) that the ray-cast cull stages rays with.
 //
 // Operand layout (both operands K-major, no swizzle): an R x K BF16 tile is stored as 8x8
 // "core matrices" (8 rows x 16 bytes, 128 contiguous bytes); core matrix (row block rb,
