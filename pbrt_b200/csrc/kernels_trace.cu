@@ -334,15 +334,17 @@ PBRT_DEV bool pop_next(TraversalStack& s, int& sp, float min_t, uint32_t& lf, ui
   return false;
 }
 
+// Resident 128-thread blocks per SM the traversal kernels are compiled for (the register cap
+// follows: 10 -> 48 registers a thread).
 #ifndef PBRT_TRAVERSAL_MIN_BLOCKS
-#define PBRT_TRAVERSAL_MIN_BLOCKS 12
+#define PBRT_TRAVERSAL_MIN_BLOCKS 10
 #endif
 
 // The while-while schedule: refill the idle lanes, walk interior nodes until every lane
 // stands on a leaf (or its ray is finished), then test the leaves of all lanes in one pass.
-// 12 resident blocks of 128 threads per SM (at most 40 registers a thread): the traversal is
-// latency-bound, and the extra warps hide more of it than the few spilled registers cost
-// (measured: 1.01 ms against 1.10 ms at the compiler's 72 registers for the 16M-ray step).
+// Compiled for PBRT_TRAVERSAL_MIN_BLOCKS resident blocks per SM: for this schedule 12 blocks
+// (40 registers) measured 1.01 ms against 1.10 ms at the compiler's 72 registers for the
+// 16M-ray step.
 template <bool kRec>
 __global__ void __launch_bounds__(128, PBRT_TRAVERSAL_MIN_BLOCKS) k_mesh_closest_ww(MeshView m, const float* __restrict__ rays,
                                                                  uint64_t stride, const uint32_t* __restrict__ queue,
@@ -491,8 +493,10 @@ __global__ void __launch_bounds__(128, PBRT_TRAVERSAL_MIN_BLOCKS) k_mesh_closest
 // bursts spread the vote's cost over several nodes (single-node steps lost to while-while).
 // Each lane still visits its nodes in the reference's order, so ids and t are unchanged.
 //
-// 12 resident blocks of 128 threads per SM (at most 40 registers a thread): the traversal is
-// latency-bound, and the extra warps hide more of it than the few spilled registers cost.
+// 10 resident blocks of 128 threads per SM (at most 48 registers a thread, 4 bytes spilled):
+// 0.882-0.887 ms per 16M-ray step against 0.888-0.894 at 9 blocks (56 registers), 0.897-0.900
+// at 8 (64, no spill), 0.928-0.932 at 12 (40, 64 bytes spilled) and 1.146-1.152 at 13-16
+// (32, 176 bytes spilled): the stack spills cost more than the extra warps hide.
 // kDense (with records): a lane's result goes to its queue slot in `res` (every survivor, hit
 // or miss) instead of to its ray's place in prim / tout; the queue's ray indices are not read.
 template <bool kRec, bool kDense>
