@@ -922,6 +922,12 @@ __global__ void __launch_bounds__(256, 3) k_shadow(WaveBuffers w, Src src, uint3
 }
 
 // ---- the deferred leaf ----------------------------------------------------------------------
+// Resident 128-thread blocks per SM the deferred passes are compiled for (8: at most 64
+// registers a thread).
+#ifndef PBRT_DEFER_MIN_BLOCKS
+#define PBRT_DEFER_MIN_BLOCKS 8
+#endif
+
 // A scene's largest mesh, when it is placed untransformed in the top-level tree, is left out
 // of the per-path queries above and answered here for all queued paths at once by persistent
 // warps over the paths (the ray-cast kernel's while-while schedule: idle lanes refilled with
@@ -934,7 +940,7 @@ __global__ void __launch_bounds__(256, 3) k_shadow(WaveBuffers w, Src src, uint3
 // it is offered as long as its hit lies inside, so the result is the per-path query's, up to
 // which of two objects hit at exactly the same distance is kept.
 template <class Src>
-__global__ void __launch_bounds__(128, 8) k_defer_closest(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
+__global__ void __launch_bounds__(128, PBRT_DEFER_MIN_BLOCKS) k_defer_closest(WaveBuffers w, Src src, const uint32_t* __restrict__ q,
                                                        const uint32_t* __restrict__ qcount,
                                                        uint32_t* __restrict__ fetch, uint32_t* err) {
   const uint32_t n = *qcount;
@@ -1084,7 +1090,7 @@ __global__ void __launch_bounds__(128, 8) k_defer_closest(WaveBuffers w, Src src
 // Shadow rays against the deferred leaf: the entries k_shadow left open (t_max >= 0) add their
 // light sample when the mesh does not block [kShadowEps, t_max]; any hit ends the walk.
 template <class Src>
-__global__ void __launch_bounds__(128, 8) k_defer_any(WaveBuffers w, Src src, uint32_t* __restrict__ fetch,
+__global__ void __launch_bounds__(128, PBRT_DEFER_MIN_BLOCKS) k_defer_any(WaveBuffers w, Src src, uint32_t* __restrict__ fetch,
                                                    uint32_t* err) {
   const uint32_t n = w.counts[2];
   const unsigned lane = threadIdx.x & 31u, lt_mask = (1u << lane) - 1u;
@@ -1504,7 +1510,8 @@ static cudaError_t bounce_loop(const WaveBuffers& w, const Src& src, const Cache
                                bool defer) {
   cudaError_t e;
   const unsigned gt = unsigned(sm_count) * sh.trace_blocks_per_sm, gs = unsigned(sm_count) * sh.shade_blocks_per_sm;
-  const unsigned gd = unsigned(sm_count) * 8u;  // the deferred passes: persistent, 8 blocks of 128 per SM
+  // the deferred passes: persistent, PBRT_DEFER_MIN_BLOCKS blocks of 128 per SM
+  const unsigned gd = unsigned(sm_count) * unsigned(PBRT_DEFER_MIN_BLOCKS);
   const uint32_t df = defer ? 1u : 0u;
   for (uint32_t b = 0; b < loops; ++b) {
     uint32_t* qin = (b & 1) ? w.qb : w.qa;
