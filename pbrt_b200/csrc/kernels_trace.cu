@@ -231,8 +231,6 @@ __global__ void __launch_bounds__(kBulkThreads) k_cull_root_bulk(MeshView m, con
   for (uint64_t it = 0; it < iters; ++it) {
     const uint64_t c = uint64_t(blockIdx.x) + it * gridDim.x;
     const int b = int(it & 1);
-    // at this block's last chunk, let a programmatic dependent (the traversal) begin launching
-    if (it + 1 == iters) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     // The next chunk's copies go out now; its buffer was last read in the previous
     // iteration, before that iteration's barriers.
     if (threadIdx.x == 0 && c + gridDim.x < full_chunks) issue(c + gridDim.x, b ^ 1);
@@ -510,9 +508,6 @@ __global__ void __launch_bounds__(128, PBRT_TRAVERSAL_MIN_BLOCKS) k_mesh_closest
   static_assert(kRec || !kDense, "dense results need the ray records");
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
-  // Launched as a programmatic dependent of the cull: wait here until the cull's grid has
-  // completed and its memory is visible (a no-op for an ordinary launch).
-  asm volatile("griddepcontrol.wait;" ::: "memory");
   const uint64_t n = *queue_count;
   bool active = false, exhausted = false;  // exhausted is warp-uniform
   uint32_t idx = 0;
@@ -853,27 +848,9 @@ cudaError_t launch_mesh_closest_persistent(const MeshView& m, const float* rays,
       k_mesh_closest_ww<false><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj, counters + 1, err,
                                                  nullptr);
   } else if (rec) {
-    // Programmatic dependent launch: the traversal grid is set up while the cull drains and
-    // its threads wait in griddepcontrol.wait for the cull's results (PBRT_TRACE_PDL=0: an
-    // ordinary launch).
-    static const bool pdl = [] {
-      const char* ev = std::getenv("PBRT_TRACE_PDL");
-      return !(ev && std::strcmp(ev, "0") == 0);
-    }();
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(g);
-    cfg.blockDim = dim3(128);
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = pdl ? 1 : 0;
-    e = cudaLaunchKernelEx(&cfg, k_mesh_closest_persistent<true, false>, m, rays, stride,
-                           static_cast<const uint32_t*>(queue), static_cast<const unsigned long long*>(counters), prim,
-                           t, obj, counters + 1, err, static_cast<const float4*>(rec), ts.leaf_arg(), ts.refill_min,
-                           ts.burst_arg(), static_cast<uint2*>(nullptr));
-    if (e != cudaSuccess) return e;
+    k_mesh_closest_persistent<true, false><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj,
+                                                             counters + 1, err, rec, ts.leaf_arg(), ts.refill_min,
+                                                             ts.burst_arg(), nullptr);
   } else {
     k_mesh_closest_persistent<false, false><<<g, 128, 0, s>>>(m, rays, stride, queue, counters, prim, t, obj,
                                                               counters + 1, err, nullptr, ts.leaf_arg(), ts.refill_min,
