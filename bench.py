@@ -193,8 +193,8 @@ def _per_kernel(launch_ms: float, n_rays: int, box_pr: float, tri_pr: float, pea
         "k_mesh_closest_persistent": {"share": round(trav["ns"] / total_ns, 4), "ms": round(trav_ms, 4),
                                       "algorithmic_bytes_per_ray": round(trav_bytes / n_rays, 2),
                                       "achieved_gbs": round(trav_gbs, 1), "frac": round(trav_gbs / peak, 4),
-                                      "limiter": "instruction issue and latency: 9.7 of 32 lanes active per warp "
-                                                 "instruction, 66 % issue active, 3 % of DRAM throughput; node "
+                                      "limiter": "instruction issue and latency: 10.0 of 32 lanes active per warp "
+                                                 "instruction, 63 % issue active, 3 % of DRAM throughput; node "
                                                  "and triangle reads are mostly L1/L2 hits"},
         "shares_from": "profiles/k_mesh_closest_raycast.json (ncu, full-size pass)",
     }
