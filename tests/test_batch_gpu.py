@@ -224,3 +224,28 @@ def test_persistent_batch_builds_and_refill(tmp_path, env):
     z = np.load(out)
     _close(z["f0"], z["s0"])
     _close(z["f1"], z["s1"])
+
+
+@pytest.mark.parametrize("wave_paths", [0, 1 << 19])
+def test_waves_along_scene_boundaries(wave_paths):
+    """A scene of at least 2^20 paths gets waves of its own (split in two by a 2^19-path wave
+    size), the small scenes around it are packed into shared waves: every film equals the
+    scene's own render, and each scene's completion time is reported."""
+    specs = [(W.cornell_box(32, 24), dict(spp=2, max_depth=5)),
+             (W.cornell_box(512, 512), dict(spp=4, max_depth=4)),  # 1,048,576 paths
+             (W.many_spheres(200, width=40, height=30), dict(spp=3, max_depth=6, rr_start=3)),
+             (W.cornell_box(20, 20), dict(spp=5, max_depth=6))]
+    scenes = create_scenes([d for (d, _), _ in specs])
+    singles = [s.render(cam, seed=9, **kw) for s, ((_, cam), kw) in zip(scenes, specs)]
+    params = [render_params(cam, seed=9, **kw) for (_, cam), kw in specs]
+    ctx = scenes[0].ctx
+    ctx.set_tuning(wave_paths=wave_paths)
+    try:
+        b = Batch(scenes, params)
+        films, ms = b.render(0, scene_times=True)
+        for f, s in zip(films, singles):
+            _close(f, s)
+        assert all(t > 0 for t in ms)
+        b.close()
+    finally:
+        ctx.set_tuning()
