@@ -537,6 +537,7 @@ def batch_race(pb, W, ctx, device):
     batch.close()
     best = min(frames, key=max)
     frame_ms = max(best)
+    branches = _branch_frames(ctx, scenes, params, samples, frame_ms)
     pers = _persistent_frame(ctx, scenes, params, samples, frame_ms)
     # the same scenes one after another, each its own pbrt_render, in the batch's order
     # (cheapest first: pixels x spp x max depth)
@@ -574,6 +575,7 @@ def batch_race(pb, W, ctx, device):
                        "note": "same scenes, tuning and order (cheapest first), one pbrt_render each "
                                "(launches not captured)"},
         "speedup_aggregate": round(cum[-1] / frame_ms, 3),
+        "branches": branches,
         "persistent": pers,
         "tuning": {k: tune[k] for k in ("leaf", "wave_paths", "trace_threads", "trace_blocks_per_sm",
                                           "shade_threads", "shade_blocks_per_sm")},
@@ -583,6 +585,30 @@ def batch_race(pb, W, ctx, device):
                     "note": "host: BVHs on all host cores (pbrt_scene_create_many); gpu: device_build, the "
                             "same trees; both include the uploads"},
     }
+
+
+def _branch_frames(ctx, scenes, params, samples, default_ms, branches=(1, 3, 4)):
+    """The same wavefront batch frame with its waves on k concurrent branches (streams inside
+    the graph, each with its own wave buffers; pbrt_ctx_set_batch_branches; the default is
+    2): best of two frames after a warm-up, for each k."""
+    from pbrt_b200.scene import Batch
+
+    out = {}
+    none = [None] * len(scenes)
+    try:
+        for k in branches:
+            ctx.set_batch_branches(k)
+            batch = Batch(scenes, params, ctx)
+            batch.render(0, none)
+            frames = [batch.render(f, none, scene_times=True)[1] for f in (1, 2)]
+            batch.close()
+            best = min(frames, key=max)
+            out[str(k)] = {"frame_ms": round(max(best), 3), "samples_per_s": round(samples / (max(best) * 1e-3), 1),
+                           "scene_latency_ms": {"mean": round(float(np.mean(best)), 3)},
+                           "speedup_vs_default": round(default_ms / max(best), 3)}
+    finally:
+        ctx.set_batch_branches(2)
+    return out
 
 
 def _persistent_frame(ctx, scenes, params, samples, wavefront_ms):
@@ -624,6 +650,7 @@ def batch_small(pb, W, ctx, device, n=64, width=128, height=128):
     frames = [batch.render(f, none, scene_times=True)[1] for f in (1, 2)]
     batch.close()
     best = min(frames, key=max)
+    branches = _branch_frames(ctx, scenes, params, samples, max(best))
     pers = _persistent_frame(ctx, scenes, params, samples, max(best))
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
@@ -653,6 +680,7 @@ def batch_small(pb, W, ctx, device, n=64, width=128, height=128):
                            "note": "one pbrt_render each, cheapest first, back to back on one stream"},
             "speedup_aggregate": round(total / max(best), 3),
             "speedup_mean_latency": round(float(np.mean(done)) / float(np.mean(best)), 3),
+            "branches": branches,
             "persistent": pers}
 
 

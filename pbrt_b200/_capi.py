@@ -162,6 +162,7 @@ SIGNATURES = {
     "pbrt_batch_destroy": (None, [C.c_void_p]),
     "pbrt_render_batch": (C.c_int, [C.c_void_p, C.POINTER(RenderParams), C.c_uint32, C.c_void_p]),
     "pbrt_ctx_set_batch_kernel": (C.c_int, [C.c_void_p, C.c_int]),
+    "pbrt_ctx_set_batch_branches": (C.c_int, [C.c_void_p, C.c_uint32]),
     "pbrt_film_to_rgba8": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
     "pbrt_write_png": (C.c_int, [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint32]),
 }

@@ -33,6 +33,14 @@ struct pbrt_batch {
   unsigned long long* d_scratch = nullptr;  // its fetch position, clock stamps, completion counters
   std::vector<unsigned long long> h_stamps;
   LaunchShape shape;
+  // concurrent branches of a wavefront frame: branch 0 runs on `cap`, branch k >= 1 on
+  // branch_st[k] with its own wave buffers extra[k - 1]
+  std::vector<BatchWave> plan;
+  uint32_t branches = 1;
+  std::vector<WaveAlloc> extra;
+  std::vector<cudaStream_t> branch_st;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> joins;
   cudaStream_t cap = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -43,6 +51,12 @@ struct pbrt_batch {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (cap) cudaStreamDestroy(cap);
+    for (size_t k = 1; k < branch_st.size(); ++k)
+      if (branch_st[k]) cudaStreamDestroy(branch_st[k]);
+    if (fork) cudaEventDestroy(fork);
+    for (cudaEvent_t e : joins)
+      if (e) cudaEventDestroy(e);
+    for (WaveAlloc& w : extra) cudaFree(w.block);
     if (start) cudaEventDestroy(start);
     for (cudaEvent_t e : done) cudaEventDestroy(e);
     for (double* f : films) cudaFree(f);
@@ -59,15 +73,26 @@ namespace {
 int capture(pbrt_batch* b) {
   pbrt_ctx* c = b->ctx;
   PBRT_TRY(c->cuda(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking), "cudaStreamCreate"));
+  std::vector<WaveBuffers> bw(b->branches);
+  b->branch_st.assign(b->branches, nullptr);
+  b->joins.assign(b->branches, nullptr);
+  b->branch_st[0] = b->cap;
+  bw[0] = b->wave.w;
+  for (uint32_t k = 1; k < b->branches; ++k) {
+    PBRT_TRY(c->cuda(cudaStreamCreateWithFlags(&b->branch_st[k], cudaStreamNonBlocking), "cudaStreamCreate"));
+    PBRT_TRY(c->cuda(cudaEventCreateWithFlags(&b->joins[k], cudaEventDisableTiming), "cudaEventCreate"));
+    bw[k] = b->extra[k - 1].w;
+  }
+  if (b->branches > 1) PBRT_TRY(c->cuda(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "cudaEventCreate"));
   PBRT_TRY(c->cuda(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture"));
   cudaError_t e = cudaMemsetAsync(c->d_counters + 8, 0, 3 * sizeof(unsigned long long), b->cap);
   if (e == cudaSuccess && b->persistent)
     e = render_batch_persistent(b->d_table, b->table.data(), uint32_t(b->table.size()), b->d_frame, b->d_scratch,
                                 c->d_counters + 8, c->d_err, c->sm_count, b->cap);
   else if (e == cudaSuccess)
-    e = render_batch(b->d_table, b->table.data(), uint32_t(b->table.size()), b->wave.w, b->wave_paths, b->d_frame,
-                     b->max_depth, b->any_path, b->shape, c->d_counters + 8, c->d_err, c->sm_count, b->cap,
-                     b->done.data());
+    e = render_batch(b->d_table, b->table.data(), uint32_t(b->table.size()), b->plan, bw.data(), b->branch_st.data(),
+                     b->branches, b->d_frame, b->max_depth, b->any_path, b->shape, c->d_counters + 8, c->d_err,
+                     c->sm_count, b->cap, b->fork, b->joins.data(), b->done.data());
   cudaGraph_t g = nullptr;
   const cudaError_t e2 = cudaStreamEndCapture(b->cap, &g);
   if (e != cudaSuccess || e2 != cudaSuccess) {
@@ -161,7 +186,17 @@ int pbrt_batch_create(pbrt_ctx* c, pbrt_scene* const* scenes, const pbrt_render_
       rc = c->cuda(cudaMalloc(&b->d_scratch, b->h_stamps.size() * sizeof(unsigned long long)),
                    "cudaMalloc(batch counters)");
   } else if (rc == PBRT_OK) {
-    rc = ensure_wave(c, &b->wave, b->wave_paths);
+    // each branch's wave buffers hold its largest wave
+    b->plan = batch_plan(b->table.data(), n, b->wave_paths, std::max<uint32_t>(1u, c->batch_branches));
+    std::vector<uint32_t> cap(1, 0);
+    for (const BatchWave& wv : b->plan) {
+      if (wv.branch >= cap.size()) cap.resize(wv.branch + 1, 0);
+      cap[wv.branch] = std::max(cap[wv.branch], wv.n);
+    }
+    b->branches = uint32_t(cap.size());
+    b->extra.resize(b->branches - 1);
+    rc = ensure_wave(c, &b->wave, cap[0]);
+    for (uint32_t k = 1; k < b->branches && rc == PBRT_OK; ++k) rc = ensure_wave(c, &b->extra[k - 1], cap[k]);
   }
   if (rc == PBRT_OK) rc = c->cuda(cudaEventCreate(&b->start), "cudaEventCreate");
   b->done.assign(n, nullptr);
@@ -223,6 +258,15 @@ int pbrt_ctx_set_batch_kernel(pbrt_ctx* c, int kind) {
   if (kind != PBRT_BATCH_WAVEFRONT && kind != PBRT_BATCH_PERSISTENT)
     return c->fail(PBRT_ERR_INVALID_ARGUMENT, "unknown batch kernel " + std::to_string(kind));
   c->batch_kernel = kind;
+  return PBRT_OK;
+}
+
+int pbrt_ctx_set_batch_branches(pbrt_ctx* c, uint32_t branches) {
+  if (!c) return PBRT_ERR_INVALID_ARGUMENT;
+  if (branches < 1 || branches > kMaxBatchBranches)
+    return c->fail(PBRT_ERR_INVALID_ARGUMENT, "batch branches must be in [1, " + std::to_string(kMaxBatchBranches) +
+                                                  "], not " + std::to_string(branches));
+  c->batch_branches = branches;
   return PBRT_OK;
 }
 

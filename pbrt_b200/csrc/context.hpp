@@ -21,6 +21,9 @@ namespace api {
 constexpr uint64_t kSlotRays = uint64_t(1) << 20;  // rays per pipelined chunk (32 MiB of rays)
 constexpr int kSlots = 3;
 constexpr uint64_t kDevChunk = uint64_t(1) << 24;  // rays per launch pair on device buffers
+// Concurrent branches of a wavefront batch frame (pbrt_ctx_set_batch_branches).
+constexpr uint32_t kMaxBatchBranches = 8;
+constexpr uint32_t kDefaultBatchBranches = 2;
 
 struct DeviceGuard {
   int prev = -1;
@@ -92,6 +95,7 @@ struct pbrt_ctx {
   pbrt::LaunchShape shape;          // wavefront launch shape (pbrt_ctx_set_tuning)
   uint32_t wave_paths = 1u << 26;   // paths per wave (136 bytes of path state each, allocated on demand)
   int batch_kernel = 0;             // batches created afterwards: PBRT_BATCH_WAVEFRONT / _PERSISTENT
+  uint32_t batch_branches = pbrt::api::kDefaultBatchBranches;  // concurrent branches of a wavefront batch frame
   // a cached render's training rounds beside its frame: their stream, the fork and join
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;

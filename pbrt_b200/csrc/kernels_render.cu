@@ -1579,10 +1579,37 @@ static std::vector<std::pair<unsigned long long, uint32_t>> batch_waves(const Ba
   return waves;
 }
 
-cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, uint32_t nscenes, const WaveBuffers& w,
-                         uint32_t wave, const uint32_t* frame, uint32_t max_depth, bool any_path_integrator,
+std::vector<BatchWave> batch_plan(const BatchScene* host_table, uint32_t nscenes, uint32_t wave, uint32_t branches) {
+  const std::vector<std::pair<unsigned long long, uint32_t>> waves = batch_waves(host_table, nscenes, wave);
+  std::vector<BatchWave> plan;
+  plan.reserve(waves.size());
+  std::vector<unsigned long long> load(branches ? branches : 1, 0);
+  uint32_t first = 0, prev_last = ~0u, branch = 0;
+  for (const auto& wv : waves) {
+    while (host_table[first].begin + (unsigned long long)host_table[first].npix * host_table[first].spp <= wv.first)
+      ++first;
+    uint32_t last = first, depth = host_table[first].max_depth;
+    while (last + 1 < nscenes && host_table[last + 1].begin < wv.first + wv.second) {
+      ++last;
+      depth = depth > host_table[last].max_depth ? depth : host_table[last].max_depth;
+    }
+    if (first != prev_last) {  // a new group of waves: the least loaded branch (lowest on ties)
+      branch = 0;
+      for (uint32_t k = 1; k < load.size(); ++k)
+        if (load[k] < load[branch]) branch = k;
+    }
+    load[branch] += (unsigned long long)wv.second * depth;
+    plan.push_back(BatchWave{wv.first, wv.second, branch});
+    prev_last = last;
+  }
+  return plan;
+}
+
+cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, uint32_t nscenes,
+                         const std::vector<BatchWave>& plan, const WaveBuffers* bw, const cudaStream_t* bst,
+                         uint32_t nbranch, const uint32_t* frame, uint32_t max_depth, bool any_path_integrator,
                          const LaunchShape& shape, unsigned long long* stats, uint32_t* err, int sm_count,
-                         cudaStream_t st, cudaEvent_t* done) {
+                         cudaStream_t st, cudaEvent_t fork, const cudaEvent_t* joins, cudaEvent_t* done) {
   cudaError_t e;
   uint32_t max_npix = 0;
   for (uint32_t i = 0; i < nscenes; ++i) max_npix = max_npix > host_table[i].npix ? max_npix : host_table[i].npix;
@@ -1590,6 +1617,11 @@ cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, 
                    nscenes);
   k_films_batch<<<fgrid, 256, 0, st>>>(table, 1);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (nbranch > 1) {
+    if ((e = cudaEventRecord(fork, st)) != cudaSuccess) return e;
+    for (uint32_t k = 1; k < nbranch; ++k)
+      if ((e = cudaStreamWaitEvent(bst[k], fork, 0)) != cudaSuccess) return e;
+  }
   const ManyScenes src{table};
   uint32_t top_nodes = 0;
   bool csg = false;
@@ -1597,39 +1629,43 @@ cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, 
     top_nodes = top_nodes > host_table[i].view.top_node_count ? top_nodes : host_table[i].view.top_node_count;
     csg = csg || host_table[i].view.has_csg;
   }
-  const std::vector<std::pair<unsigned long long, uint32_t>> waves = batch_waves(host_table, nscenes, wave);
-  uint32_t next_done = 0, first = 0;
-  for (const auto& wv : waves) {
-    const unsigned long long base = wv.first;
-    const uint32_t n = wv.second;
+  uint32_t first = 0;
+  for (const BatchWave& wv : plan) {
+    const unsigned long long base = wv.base;
+    const uint32_t n = wv.n;
+    const WaveBuffers& w = bw[wv.branch];
+    cudaStream_t s = bst[wv.branch];
     // the scenes holding the wave's first and last paths (the table is in path order)
     while (host_table[first].begin + (unsigned long long)host_table[first].npix * host_table[first].spp <= base) ++first;
     uint32_t last = first;
     while (last + 1 < nscenes && host_table[last + 1].begin < base + n) ++last;
-    k_generate_batch<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, table, nscenes, base, n, frame, stats);
+    k_generate_batch<<<grid_cap(n, 256, sm_count, 16), 256, 0, s>>>(w, table, nscenes, base, n, frame, stats);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (first == last) {
       // a wave of one scene runs the single-scene kernels: its view is a kernel parameter
       // instead of a per-path table lookup, and the bounce loop stops at its own depth
       const BatchScene& h = host_table[first];
       const OneScene one{h.view, PathSettings{h.max_depth, h.rr_start, h.integrator, h.cam.near, h.cam.far}};
-      e = bounce_loop(w, one, CacheWave{}, h.max_depth, !h.integrator, kCacheOff, 0, shape, stats, err, sm_count, st,
+      e = bounce_loop(w, one, CacheWave{}, h.max_depth, !h.integrator, kCacheOff, 0, shape, stats, err, sm_count, s,
                       h.view.top_node_count, h.view.has_csg != 0, defer_enabled() && h.view.defer_leaf != kNoLeaf);
     } else {
       bool defer = false;
       for (uint32_t i = first; i <= last; ++i) defer = defer || host_table[i].view.defer_leaf != kNoLeaf;
       e = bounce_loop(w, src, CacheWave{}, max_depth, any_path_integrator, kCacheOff, 0, shape, stats, err, sm_count,
-                      st, top_nodes, csg, defer_enabled() && defer);
+                      s, top_nodes, csg, defer_enabled() && defer);
     }
     if (e != cudaSuccess) return e;
-    k_accumulate_batch<<<grid_cap(n, 256, sm_count, 16), 256, 0, st>>>(w, n, table);
+    k_accumulate_batch<<<grid_cap(n, 256, sm_count, 16), 256, 0, s>>>(w, n, table);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    // scenes whose last path was in this wave are done
-    while (done && next_done < nscenes &&
-           host_table[next_done].begin + (unsigned long long)host_table[next_done].npix * host_table[next_done].spp <=
-               base + n) {
-      if ((e = cudaEventRecordWithFlags(done[next_done], st, cudaEventRecordExternal)) != cudaSuccess) return e;
-      ++next_done;
+    // the wave's scenes whose last path was in it are done
+    for (uint32_t i = first; done && i <= last; ++i)
+      if (host_table[i].begin + (unsigned long long)host_table[i].npix * host_table[i].spp <= base + n)
+        if ((e = cudaEventRecordWithFlags(done[i], s, cudaEventRecordExternal)) != cudaSuccess) return e;
+  }
+  if (nbranch > 1) {
+    for (uint32_t k = 1; k < nbranch; ++k) {
+      if ((e = cudaEventRecord(joins[k], bst[k])) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(st, joins[k], 0)) != cudaSuccess) return e;
     }
   }
   k_films_batch<<<fgrid, 256, 0, st>>>(table, 0);

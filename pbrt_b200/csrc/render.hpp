@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "scene_device.cuh"
@@ -82,14 +83,30 @@ struct BatchScene {
   uint32_t npix, spp, max_depth, rr_start, sample_offset, integrator, stride, film_w;
 };
 
-// A batched frame: waves of `wave` paths over all scenes' paths (scenes in table order); the
+// One wave of a batched frame: global paths [base, base + n), run on concurrent branch
+// `branch` (its own wave buffers and stream).
+struct BatchWave {
+  unsigned long long base;
+  uint32_t n, branch;
+};
+
+// The waves of a batched frame (scenes in table order, waves of at most `wave` paths along
+// scene boundaries) spread over `branches` concurrent branches: the waves that share a scene
+// stay on one branch (a scene's film and completion belong to one stream), and each group of
+// them goes to the branch with the least work so far (paths x max depth), in table order.
+std::vector<BatchWave> batch_plan(const BatchScene* host_table, uint32_t nscenes, uint32_t wave, uint32_t branches);
+
+// A batched frame: the planned waves, each on its branch's stream with its branch's wave
+// buffers (bw[k], bst[k]; bst[0] is `st`). The films are cleared on `st` before the branches
+// fork from it (event `fork`) and scaled after they join it again (events joins[1..]). The
 // kernels read the frame number from `frame` (device memory), so a captured graph of these
 // launches renders any frame. `done[s]`, when given, is recorded (as an external event, so it
-// survives stream capture) right after the wave that completes scene s.
-cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, uint32_t nscenes, const WaveBuffers& w,
-                         uint32_t wave, const uint32_t* frame, uint32_t max_depth, bool any_path_integrator,
+// survives stream capture) on scene s's branch right after the wave that completes it.
+cudaError_t render_batch(const BatchScene* table, const BatchScene* host_table, uint32_t nscenes,
+                         const std::vector<BatchWave>& plan, const WaveBuffers* bw, const cudaStream_t* bst,
+                         uint32_t nbranch, const uint32_t* frame, uint32_t max_depth, bool any_path_integrator,
                          const LaunchShape& shape, unsigned long long* stats, uint32_t* err, int sm_count,
-                         cudaStream_t st, cudaEvent_t* done);
+                         cudaStream_t st, cudaEvent_t fork, const cudaEvent_t* joins, cudaEvent_t* done);
 
 // A batched frame as one persistent launch: every path of every scene run to its end by
 // persistent warps (between the films' zeroing and scaling). `scratch`: 2 + 2 * nscenes

@@ -84,6 +84,12 @@ class Context:
             raise ValueError(f"batch kernel must be one of {sorted(kinds)}")
         self.check(self.lib.pbrt_ctx_set_batch_kernel(self.h, kinds[kind]), "pbrt_ctx_set_batch_kernel")
 
+    def set_batch_branches(self, branches: int):
+        """Concurrent branches (streams inside the frame's graph, each with its own wave
+        buffers) of the wavefront frame of batches created afterwards, 1..8. A scene's waves
+        stay on one branch; films are the same for any count."""
+        self.check(self.lib.pbrt_ctx_set_batch_branches(self.h, int(branches)), "pbrt_ctx_set_batch_branches")
+
     def tuning(self) -> dict:
         t = _capi.Tuning()
         self.check(self.lib.pbrt_ctx_get_tuning(self.h, C.byref(t)), "pbrt_ctx_get_tuning")

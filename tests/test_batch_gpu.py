@@ -145,11 +145,14 @@ def test_batch_with_deferred_meshes_equals_single_renders():
     ctx = scenes[0].ctx
     ctx.set_tuning(wave_paths=3000)
     try:
-        b = Batch(scenes, params)
-        for f, s in zip(b.render(0), singles):
-            _close(f, s)
-        b.close()
+        for branches in (1, 3):  # the deferred passes' fetch counters belong to each branch
+            ctx.set_batch_branches(branches)
+            b = Batch(scenes, params)
+            for f, s in zip(b.render(0), singles):
+                _close(f, s)
+            b.close()
     finally:
+        ctx.set_batch_branches(2)  # the default
         ctx.set_tuning()
     # the persistent launch answers the large meshes inside each path's query
     ctx.set_batch_kernel("persistent")
@@ -160,6 +163,40 @@ def test_batch_with_deferred_meshes_equals_single_renders():
         b.close()
     finally:
         ctx.set_batch_kernel("wavefront")
+
+
+@pytest.mark.parametrize("branches", [2, 3, 8])
+@pytest.mark.parametrize("wave_paths", [0, 3000])
+def test_concurrent_branches_equal_single_renders(built, branches, wave_paths):
+    """A frame whose waves run on several streams inside the graph (each branch its own wave
+    buffers): every film equals the scene's own render, in later frames too, whether each
+    scene is a group of its own waves (small waves) or scenes share waves; the work counters
+    equal the single-branch frame's; every scene reports a completion time."""
+    specs, scenes, singles, params = built
+    ctx = scenes[0].ctx
+    ctx.set_tuning(wave_paths=wave_paths)
+    try:
+        ctx.set_batch_branches(1)
+        one = Batch(scenes, params)
+        one.render(0)
+        one_stats = ctx.render_stats()
+        one.close()
+        ctx.set_batch_branches(branches)
+        b = Batch(scenes, params)
+        films, ms = b.render(0, scene_times=True)
+        for f, s in zip(films, singles):
+            _close(f, s)
+        assert ctx.render_stats() == one_stats
+        assert all(np.isfinite(t) and t > 0 for t in ms)
+        for sc, f, (_, cam, kw) in zip(scenes, b.render(2), specs):
+            _close(f, sc.render(cam, seed=5, sample_offset=2 * kw["spp"], **kw))
+        b.close()
+    finally:
+        ctx.set_batch_branches(2)  # the default
+        ctx.set_tuning()
+    for bad in (0, 9):
+        with pytest.raises(PbrtError):
+            ctx.set_batch_branches(bad)
 
 
 def test_persistent_batch_equals_single_renders(built):
