@@ -156,6 +156,15 @@ void pbrt_ctx_destroy(pbrt_ctx* c) {
   if (c->join) cudaEventDestroy(c->join);
   cudaFree(c->waves.block);
   cudaFree(c->train_waves.block);
+  for (uint32_t k = 0; k < kMaxBatchBranches; ++k) {
+    if (c->branch_st[k]) {
+      cudaStreamSynchronize(c->branch_st[k]);
+      cudaStreamDestroy(c->branch_st[k]);
+    }
+    if (c->branch_join[k]) cudaEventDestroy(c->branch_join[k]);
+    if (k + 1 < kMaxBatchBranches) cudaFree(c->branch_waves[k].block);
+  }
+  if (c->branch_fork) cudaEventDestroy(c->branch_fork);
   cudaFree(c->d_err);
   cudaFree(c->d_counters);
   cudaFree(c->queue);
@@ -845,6 +854,21 @@ namespace {
 // they end into the cache themselves.
 constexpr uint32_t kTrainTail = 3;
 
+// Concurrent branches of one pbrt_render: the frame's paths split into this many contiguous
+// parts, each a chain of waves on its own stream with its own wave buffers, so that one
+// part's per-bounce kernel tails overlap another part's work. PBRT_RENDER_BRANCHES (1..8)
+// overrides it for measurements; films do not depend on it.
+static_assert(pbrt_cache::kBranchSlots + 1 >= kMaxBatchBranches, "a cached frame's branches need query buffers");
+
+uint32_t render_branches(uint64_t total) {
+  static const uint32_t v = [] {
+    const char* e = std::getenv("PBRT_RENDER_BRANCHES");
+    const int k = e ? std::atoi(e) : int(kDefaultRenderBranches);
+    return uint32_t(k >= 1 && k <= int(kMaxBatchBranches) ? k : kDefaultRenderBranches);
+  }();
+  return uint32_t(std::min<uint64_t>(v, std::max<uint64_t>(1, total / 1024)));
+}
+
 unsigned long long host_mix64(unsigned long long x) {
   x += 0x9E3779B97F4A7C15ULL;
   x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
@@ -868,9 +892,20 @@ int pbrt_render(pbrt_scene* s, const pbrt_render_params* p, double* film) {
   const uint64_t npix = film_pixels(p, rs);
   const uint64_t total = npix * p->spp;
 
-  WaveAlloc& wa = c->waves;
-  const uint32_t wave = uint32_t(std::min<uint64_t>(total, c->wave_paths));
-  PBRT_TRY(ensure_wave(c, &wa, wave));
+  // the paths in `nb` contiguous parts [j * part, (j + 1) * part), part j on branch j
+  const uint32_t nb = render_branches(total);
+  const uint64_t part = (total + nb - 1) / nb;
+  const uint32_t wave = uint32_t(std::min<uint64_t>(part, c->wave_paths));
+  PBRT_TRY(ensure_wave(c, &c->waves, wave));
+  for (uint32_t j = 1; j < nb; ++j) {
+    PBRT_TRY(ensure_wave(c, &c->branch_waves[j - 1], wave));
+    if (!c->branch_st[j])
+      PBRT_TRY(c->cuda(cudaStreamCreateWithFlags(&c->branch_st[j], cudaStreamNonBlocking), "cudaStreamCreate"));
+    if (!c->branch_join[j])
+      PBRT_TRY(c->cuda(cudaEventCreateWithFlags(&c->branch_join[j], cudaEventDisableTiming), "cudaEventCreate"));
+  }
+  if (nb > 1 && !c->branch_fork)
+    PBRT_TRY(c->cuda(cudaEventCreateWithFlags(&c->branch_fork, cudaEventDisableTiming), "cudaEventCreate"));
   cudaStream_t st = c->work_stream();
   const size_t film_n = size_t(npix) * 3;
   double* dfilm = film;
@@ -878,10 +913,24 @@ int pbrt_render(pbrt_scene* s, const pbrt_render_params* p, double* film) {
   if (host_film) PBRT_TRY(c->cuda(cudaMalloc(&dfilm, film_n * sizeof(double)), "cudaMalloc(film)"));
   int rc = c->cuda(cudaMemsetAsync(dfilm, 0, film_n * sizeof(double), st), "cudaMemset(film)");
   if (rc == PBRT_OK) rc = c->cuda(cudaMemsetAsync(rs.stats, 0, 3 * sizeof(unsigned long long), st), "cudaMemset");
-  for (uint64_t base = 0; base < total && rc == PBRT_OK; base += wave) {
-    const uint32_t n = uint32_t(std::min<uint64_t>(wave, total - base));
-    rc = c->cuda(render_wave(s->view, wa.w, cam, base, n, uint32_t(npix), rs, dfilm, c->d_err, c->sm_count, st),
-                 "render");
+  if (rc == PBRT_OK && nb > 1) rc = c->cuda(cudaEventRecord(c->branch_fork, st), "cudaEventRecord");
+  for (uint32_t j = 1; j < nb && rc == PBRT_OK; ++j)
+    rc = c->cuda(cudaStreamWaitEvent(c->branch_st[j], c->branch_fork, 0), "cudaStreamWaitEvent");
+  for (uint32_t j = 0; j < nb && rc == PBRT_OK; ++j) {
+    cudaStream_t bs = j ? c->branch_st[j] : st;
+    const WaveBuffers& bw = j ? c->branch_waves[j - 1].w : c->waves.w;
+    const uint64_t end = std::min<uint64_t>(total, (j + 1) * part);
+    for (uint64_t base = j * part; base < end && rc == PBRT_OK; base += wave) {
+      const uint32_t n = uint32_t(std::min<uint64_t>(wave, end - base));
+      rc = c->cuda(render_wave(s->view, bw, cam, base, n, uint32_t(npix), rs, dfilm, c->d_err, c->sm_count, bs),
+                   "render");
+    }
+  }
+  // the branches join `st` again (also after a failed launch, so that no branch is left behind)
+  for (uint32_t j = 1; j < nb; ++j) {
+    const int jr = c->cuda(cudaEventRecord(c->branch_join[j], c->branch_st[j]), "cudaEventRecord");
+    if (jr == PBRT_OK) cudaStreamWaitEvent(st, c->branch_join[j], 0);
+    if (rc == PBRT_OK) rc = jr;
   }
   if (rc == PBRT_OK) rc = c->cuda(scale_film(dfilm, film_n, 1.0 / double(p->spp), c->sm_count, st), "render");
   if (host_film) {
@@ -1016,18 +1065,53 @@ int pbrt_render_cached(pbrt_scene* s, pbrt_cache* k, const pbrt_render_params* p
   double* dfilm = film;
   const bool host_film = mem_kind(film) != MemKind::Device;
   if (host_film) PBRT_TRY(c->cuda(cudaMalloc(&dfilm, film_n * sizeof(double)), "cudaMalloc(film)"));
-  int rc = c->cuda(cudaMemsetAsync(dfilm, 0, film_n * sizeof(double), st), "cudaMemset(film)");
-  for (uint64_t base = 0; base < total && rc == PBRT_OK; base += wave) {
-    const uint32_t n = uint32_t(std::min<uint64_t>(wave, total - base));
-    rc = c->cuda(cudaMemsetAsync(fcw->counts, 0, sizeof(uint32_t), st), "cudaMemset(cache counts)");
-    if (rc == PBRT_OK)
-      rc = c->cuda(trace_wave(s->view, wa.w, *fcw, cam, base, n, uint32_t(npix), qr, c->d_err, c->sm_count, st),
-                   "cached render");
-    if (rc == PBRT_OK)
-      rc = c->cuda(mlp::launch_infer_dev(fnet, nb, fcw->qrec, fcw->counts, n, fcw->qout, c->d_err, c->sm_count, st),
-                   "cache query");
-    if (rc == PBRT_OK) rc = c->cuda(apply_cache(wa.w, *fcw, n, s->max_radiance, c->sm_count, st), "cache apply");
-    if (rc == PBRT_OK) rc = c->cuda(accumulate_wave(wa.w, n, dfilm, cd.width, qr, c->sm_count, st), "cached render");
+  // the frame's paths in `nbr` contiguous parts on concurrent branches, as pbrt_render's;
+  // branch j >= 1 has its own wave buffers and query buffers
+  const uint32_t nbr = render_branches(total);
+  const uint64_t part = (total + nbr - 1) / nbr;
+  const uint32_t fwave = uint32_t(std::min<uint64_t>(part, wave));
+  int rc = PBRT_OK;
+  for (uint32_t j = 1; j < nbr && rc == PBRT_OK; ++j) {
+    rc = ensure_wave(c, &c->branch_waves[j - 1], fwave);
+    if (rc == PBRT_OK) rc = k->ensure_branch_buffers(j - 1, fwave);
+    if (rc == PBRT_OK && !c->branch_st[j])
+      rc = c->cuda(cudaStreamCreateWithFlags(&c->branch_st[j], cudaStreamNonBlocking), "cudaStreamCreate");
+    if (rc == PBRT_OK && !c->branch_join[j])
+      rc = c->cuda(cudaEventCreateWithFlags(&c->branch_join[j], cudaEventDisableTiming), "cudaEventCreate");
+  }
+  if (rc == PBRT_OK && nbr > 1 && !c->branch_fork)
+    rc = c->cuda(cudaEventCreateWithFlags(&c->branch_fork, cudaEventDisableTiming), "cudaEventCreate");
+  if (rc != PBRT_OK) {
+    if (beside) cudaStreamWaitEvent(st, c->join, 0);
+    if (host_film) cudaFree(dfilm);
+    return rc;
+  }
+  rc = c->cuda(cudaMemsetAsync(dfilm, 0, film_n * sizeof(double), st), "cudaMemset(film)");
+  if (rc == PBRT_OK && nbr > 1) rc = c->cuda(cudaEventRecord(c->branch_fork, st), "cudaEventRecord");
+  for (uint32_t j = 1; j < nbr && rc == PBRT_OK; ++j)
+    rc = c->cuda(cudaStreamWaitEvent(c->branch_st[j], c->branch_fork, 0), "cudaStreamWaitEvent");
+  for (uint32_t j = 0; j < nbr && rc == PBRT_OK; ++j) {
+    cudaStream_t bs = j ? c->branch_st[j] : st;
+    const WaveBuffers& bw = j ? c->branch_waves[j - 1].w : wa.w;
+    const CacheWave& q = j ? k->bcw[j - 1] : *fcw;
+    const uint64_t end = std::min<uint64_t>(total, (j + 1) * part);
+    for (uint64_t base = j * part; base < end && rc == PBRT_OK; base += fwave) {
+      const uint32_t n = uint32_t(std::min<uint64_t>(fwave, end - base));
+      rc = c->cuda(cudaMemsetAsync(q.counts, 0, sizeof(uint32_t), bs), "cudaMemset(cache counts)");
+      if (rc == PBRT_OK)
+        rc = c->cuda(trace_wave(s->view, bw, q, cam, base, n, uint32_t(npix), qr, c->d_err, c->sm_count, bs),
+                     "cached render");
+      if (rc == PBRT_OK)
+        rc = c->cuda(mlp::launch_infer_dev(fnet, nb, q.qrec, q.counts, n, q.qout, c->d_err, c->sm_count, bs),
+                     "cache query");
+      if (rc == PBRT_OK) rc = c->cuda(apply_cache(bw, q, n, s->max_radiance, c->sm_count, bs), "cache apply");
+      if (rc == PBRT_OK) rc = c->cuda(accumulate_wave(bw, n, dfilm, cd.width, qr, c->sm_count, bs), "cached render");
+    }
+  }
+  for (uint32_t j = 1; j < nbr; ++j) {  // the branches join `st` again
+    const int jr = c->cuda(cudaEventRecord(c->branch_join[j], c->branch_st[j]), "cudaEventRecord");
+    if (jr == PBRT_OK) cudaStreamWaitEvent(st, c->branch_join[j], 0);
+    if (rc == PBRT_OK) rc = jr;
   }
   if (rc == PBRT_OK) rc = c->cuda(scale_film(dfilm, film_n, 1.0 / double(p->spp), c->sm_count, st), "render");
   if (beside) {

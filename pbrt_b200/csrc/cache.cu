@@ -174,10 +174,34 @@ int pbrt_cache::ensure_frame_buffers(uint32_t queries) {
   return PBRT_OK;
 }
 
+int pbrt_cache::ensure_branch_buffers(uint32_t slot, uint32_t queries) {
+  if (slot >= kBranchSlots) return ctx->fail(PBRT_ERR_INVALID_ARGUMENT, "no such frame branch");
+  if (branch_block[slot] && branch_qcap[slot] >= queries) return PBRT_OK;
+  cudaFree(branch_block[slot]);
+  branch_block[slot] = nullptr;
+  branch_qcap[slot] = 0;
+  pbrt::CacheWave& q = bcw[slot];
+  q = pbrt::CacheWave{};
+  const size_t R = pbrt::kCacheRecordFloats * 4;
+  auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t bytes = up(64) + up(size_t(queries) * R) + up(size_t(queries) * 12) + up(size_t(queries) * 4);
+  PBRT_TRY(ctx->cuda(cudaMalloc(&branch_block[slot], bytes), "cudaMalloc(cache branch buffers)"));
+  char* p = static_cast<char*>(branch_block[slot]);
+  auto take = [&](size_t b) { char* r = p; p += up(b); return r; };
+  q.counts = reinterpret_cast<uint32_t*>(take(64));
+  q.qrec = reinterpret_cast<float*>(take(size_t(queries) * R));
+  q.qout = reinterpret_cast<float*>(take(size_t(queries) * 12));
+  q.qpath = reinterpret_cast<uint32_t*>(take(size_t(queries) * 4));
+  q.qcap = queries;  // queries only, like the frame's own buffers
+  branch_qcap[slot] = queries;
+  return PBRT_OK;
+}
+
 void pbrt_cache::release() {
   for (void* p : {(void*)w, (void*)m, (void*)v, (void*)grad, (void*)wfwd, (void*)wbwd, (void*)loss, (void*)partials,
                   (void*)tile_loss, render_block, frame_block})
     cudaFree(p);
+  for (void* p : branch_block) cudaFree(p);
 }
 
 namespace {

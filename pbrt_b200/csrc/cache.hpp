@@ -35,6 +35,13 @@ struct pbrt_cache {
   uint16_t* wsnap = nullptr;
   int ensure_frame_buffers(uint32_t queries);
 
+  // The query buffers of a frame's concurrent branches 1.. (branch 0 takes fcw or cw).
+  static constexpr uint32_t kBranchSlots = 7;
+  void* branch_block[kBranchSlots] = {};
+  uint32_t branch_qcap[kBranchSlots] = {};
+  pbrt::CacheWave bcw[kBranchSlots] = {};
+  int ensure_branch_buffers(uint32_t slot, uint32_t queries);
+
   int device_arrays();
   int ensure_tiles(uint32_t tiles);
   int reset();

@@ -24,6 +24,9 @@ constexpr uint64_t kDevChunk = uint64_t(1) << 24;  // rays per launch pair on de
 // Concurrent branches of a wavefront batch frame (pbrt_ctx_set_batch_branches).
 constexpr uint32_t kMaxBatchBranches = 8;
 constexpr uint32_t kDefaultBatchBranches = 2;
+// Concurrent branches of one render (pbrt_render, pbrt_render_cached); PBRT_RENDER_BRANCHES
+// overrides it for measurements.
+constexpr uint32_t kDefaultRenderBranches = 2;
 
 struct DeviceGuard {
   int prev = -1;
@@ -102,6 +105,10 @@ struct pbrt_ctx {
   // the path state of pbrt_render / pbrt_render_cached (grown on demand), and of a cached
   // render's training paths; per context, so contexts on one device may render at once
   pbrt::api::WaveAlloc waves, train_waves;
+  // concurrent branches of one pbrt_render (branch k >= 1: its stream, wave buffers and join)
+  pbrt::api::WaveAlloc branch_waves[pbrt::api::kMaxBatchBranches - 1];
+  cudaStream_t branch_st[pbrt::api::kMaxBatchBranches] = {};
+  cudaEvent_t branch_fork = nullptr, branch_join[pbrt::api::kMaxBatchBranches] = {};
 
   int fail(int code, const std::string& msg) {
     err = msg;
