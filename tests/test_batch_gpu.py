@@ -265,12 +265,14 @@ def test_persistent_batch_builds_and_refill(tmp_path, env):
 
 @pytest.mark.parametrize("wave_paths", [0, 1 << 19])
 def test_waves_along_scene_boundaries(wave_paths):
-    """A scene of at least 2^20 paths gets waves of its own (split in two by a 2^19-path wave
-    size), the small scenes around it are packed into shared waves: every film equals the
-    scene's own render, and each scene's completion time is reported."""
+    """Scenes of at least 2^20 paths get waves of their own (split into several by a
+    2^19-path wave size) on the least-loaded branch, the small scenes around them are packed
+    into shared waves: every film equals the scene's own render, and each scene's completion
+    time is reported."""
     specs = [(W.cornell_box(32, 24), dict(spp=2, max_depth=5)),
              (W.cornell_box(512, 512), dict(spp=4, max_depth=4)),  # 1,048,576 paths
              (W.many_spheres(200, width=40, height=30), dict(spp=3, max_depth=6, rr_start=3)),
+             (W.cornell_box(512, 512), dict(spp=8, max_depth=3)),  # 2,097,152 paths
              (W.cornell_box(20, 20), dict(spp=5, max_depth=6))]
     scenes = create_scenes([d for (d, _), _ in specs])
     singles = [s.render(cam, seed=9, **kw) for s, ((_, cam), kw) in zip(scenes, specs)]
